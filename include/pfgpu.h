@@ -1,0 +1,162 @@
+/*
+ * pfgpu.h — C ABI of the B200 NeoHookean assembly library (libpfgpu.so).
+ *
+ * Drop-in for PolyFEM's nonlinear-elasticity assembly path (iiiian/polyfem):
+ * the NLAssembler virtuals that ElasticForm calls, the SparseMatrixCache that
+ * ElasticForm owns, and the two ElasticForceDerivative adjoint terms.  Every
+ * entry point takes plain pointers and sizes; no C++ or torch types cross it.
+ *
+ * Conventions (identical to the reference):
+ *  - displacement / adjoint / gradient vectors are node-major: x[node*3 + d];
+ *  - conn is the host's Basis::global() table, E x n int32 (row-major);
+ *  - the Hessian is Eigen's ColMajor CSC (int32 outer/inner, sorted inner
+ *    indices, structural entries stored even when zero); because the pattern
+ *    is structurally symmetric these arrays are also the CSR arrays of H^T;
+ *  - values are unweighted: the caller applies Form::weight()/scale.
+ *  - NaN/inf from inverted elements (J <= 0) propagate exactly as in the
+ *    reference; they are not an error status.
+ *
+ * Memory spaces: every call takes `mem`.  With PFG_MEM_HOST the pointers are
+ * host memory, the call copies inputs to the device, runs, copies results
+ * back and returns after the stream has synchronised.  With PFG_MEM_DEVICE
+ * the pointers are device memory on the context's device and the call only
+ * enqueues work on the context's stream (pfg_set_stream), returning at once.
+ *
+ * Calls on one context are not re-entrant and must be serialised by the
+ * caller (as ElasticForm's mutable mat_cache_ requires in the reference).
+ */
+#ifndef PFGPU_H
+#define PFGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pfg_context pfg_context;
+
+enum pfg_status
+{
+	PFG_OK = 0,
+	PFG_ERR_INVALID = 1,     /* bad argument (null pointer, index out of range, bad enum) */
+	PFG_ERR_CUDA = 2,        /* a CUDA runtime call failed; see pfg_last_error */
+	PFG_ERR_OOM = 3,         /* device or host allocation failed */
+	PFG_ERR_UNSUPPORTED = 4, /* combination not implemented (e.g. project_to_psd) */
+	PFG_ERR_STATE = 5        /* call made in the wrong state (e.g. pattern not built) */
+};
+
+enum pfg_elem_type
+{
+	PFG_P1_TET = 1, /* 4-node tetrahedron, 1-point quadrature */
+	PFG_P2_TET = 2, /* 10-node tetrahedron on P1 geometry, 4-point quadrature */
+	PFG_Q1_HEX = 3  /* 8-node hexahedron, 2x2x2 Gauss quadrature */
+};
+
+enum pfg_precision
+{
+	PFG_FP64 = 0,    /* all arithmetic in FP64 (the drop-in) */
+	PFG_FP32 = 1,    /* FP32 arithmetic; det(F)/log J and reductions in FP64 */
+	PFG_SPLIT32 = 2  /* Hessian contraction on tcgen05 tensor cores with 3xTF32
+	                    split products and FP32 accumulation; det/log J in FP64;
+	                    FP64 CSC values.  Energy/gradient treat it as PFG_FP32. */
+};
+
+enum pfg_mem
+{
+	PFG_MEM_HOST = 0,
+	PFG_MEM_DEVICE = 1
+};
+
+/* Mesh and material description consumed by pfg_create.
+ * Replaces the inputs NLAssembler reads through ElementBases / AssemblyValsCache
+ * (assembler/Assembler.hpp:244-291, assembler/AssemblyValsCache.hpp) and
+ * LameParameters (assembler/MatParams.cpp:368-401). */
+typedef struct pfg_mesh_desc
+{
+	int elem_type;        /* enum pfg_elem_type */
+	int n_elements;       /* E >= 0 */
+	int n_nodes;          /* N: FE nodes (n_bases); dofs = 3N */
+	int n_geom_nodes;     /* N_g: geometric nodes (rows of X) */
+	const int *conn;      /* E x n FE node ids (Basis::global()[0].index), host */
+	const int *gconn;     /* E x n_g geometric node ids, host; NULL = conn (isoparametric) */
+	const double *X;      /* N_g x 3 rest positions of the geometric nodes, host */
+	const double *lambda; /* E per-element Lame lambda, host */
+	const double *mu;     /* E per-element Lame mu, host */
+	int device;           /* CUDA device ordinal */
+} pfg_mesh_desc;
+
+/* Creates a context: uploads the mesh in the device layout and validates
+ * every index.  Replaces AssemblyValsCache::init (assembler/AssemblyValsCache.cpp:11-32)
+ * and ElasticForm's constructor (solver/forms/ElasticForm.cpp:238-280). */
+int pfg_create(const pfg_mesh_desc *desc, pfg_context **out);
+int pfg_destroy(pfg_context *ctx);
+
+/* cudaStream_t as void*; NULL selects the legacy default stream. */
+int pfg_set_stream(pfg_context *ctx, void *stream);
+
+/* Per-element Lame parameters; replaces LameParameters::lambda_mat_/mu_mat_
+ * updates (NeoHookeanElasticity.hpp:58-62, update_lame_params). */
+int pfg_set_lame(pfg_context *ctx, const double *lambda, const double *mu, int mem);
+
+/* Rest positions of the geometric nodes (N_g x 3); shape optimisation moves them. */
+int pfg_set_rest_positions(pfg_context *ctx, const double *X, int mem);
+
+/* Total energy.  Replaces NLAssembler::assemble_energy (assembler/Assembler.cpp:495-531).
+ * `out` is one double in the `mem` space.  Deterministic for a fixed mesh. */
+int pfg_energy(pfg_context *ctx, const double *u, int mem, int prec, double *out);
+
+/* Energy of every element.  Replaces NLAssembler::assemble_energy_per_element
+ * (assembler/Assembler.cpp:533-572).  `out` holds E doubles. */
+int pfg_energy_per_element(pfg_context *ctx, const double *u, int mem, int prec, double *out);
+
+/* Gradient (3N doubles).  Replaces NLAssembler::assemble_gradient
+ * (assembler/Assembler.cpp:574-643).  Deterministic for a fixed mesh. */
+int pfg_gradient(pfg_context *ctx, const double *u, int mem, int prec, double *g);
+
+/* Builds the Hessian sparsity pattern and the element->slot map if they do not
+ * exist yet, and returns nnz.  Replaces the first-call branch of
+ * SparseMatrixCache::get_matrix (utils/MatrixCache.cpp:134-212). */
+int pfg_hessian_pattern(pfg_context *ctx, long long *nnz);
+
+/* Copies the CSC index arrays: outer (3N+1) and inner (nnz) int32. */
+int pfg_hessian_pattern_copy(pfg_context *ctx, int *outer, int *inner, int mem);
+
+/* Assembles the Hessian values (nnz doubles, CSC order) into `values`; with
+ * values == NULL they stay in the context's device buffer (pfg_hessian_device_csc).
+ * Builds the pattern on the first call.  Replaces NLAssembler::assemble_hessian
+ * (assembler/Assembler.cpp:645-771) and the later-call branch of
+ * SparseMatrixCache (utils/MatrixCache.cpp:88-113, 214-225).
+ * project_psd must be 0 (ipc::project_to_psd is not implemented). */
+int pfg_hessian(pfg_context *ctx, const double *u, int mem, int prec, int project_psd, double *values);
+
+/* Device pointers of the context-owned CSC arrays (valid until pfg_destroy). */
+int pfg_hessian_device_csc(pfg_context *ctx, const int **outer, const int **inner, double **values);
+
+/* Adjoint material term, 2E doubles [d/dlambda per element ; d/dmu per element]:
+ * term[e] = -sum_q da (lnJ F^-T):grad p, term[E+e] = -sum_q da (F - F^-T):grad p.
+ * Replaces ElasticForceDerivative::force_material_derivative
+ * (optimization/force_derivatives/ElasticForceDerivative.cpp:35-133). */
+int pfg_material_vjp(pfg_context *ctx, const double *u, const double *p, int mem, double *out);
+
+/* Adjoint shape term, 3*N_g doubles indexed by geometric node.  Replaces
+ * ElasticForceDerivative::force_shape_derivative
+ * (optimization/force_derivatives/ElasticForceDerivative.cpp:135-264). */
+int pfg_shape_vjp(pfg_context *ctx, const double *u, const double *p, int mem, int prec, double *out);
+
+/* Elements whose det(F) was <= 0 (or NaN) in the last energy/gradient call. */
+int pfg_inverted_count(pfg_context *ctx, long long *count);
+
+/* Waits for all work enqueued on the context's stream. */
+int pfg_synchronize(pfg_context *ctx);
+
+/* Human-readable detail of the last failing call on this context (never NULL). */
+const char *pfg_last_error(const pfg_context *ctx);
+const char *pfg_status_string(int status);
+
+/* Library version, e.g. 100 for 0.1.0. */
+int pfg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFGPU_H */

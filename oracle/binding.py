@@ -1,0 +1,193 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
+this module; the GPU product never does.  The oracle restates the reference's
+CPU algorithm (see oracle/pf_oracle.cpp for the file:line map).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.POINTER(ctypes.c_int)
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(_HERE, "pf_oracle.cpp")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE])
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _i, ctypes.c_int, _i, _d, _d, _d,
+                                 ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_energy.restype = ctypes.c_double
+        L.orc_energy.argtypes = [ctypes.c_void_p, _d]
+        L.orc_energy_per_element.argtypes = [ctypes.c_void_p, _d, _d]
+        L.orc_gradient.argtypes = [ctypes.c_void_p, _d, _d]
+        L.orc_hessian.restype = ctypes.c_longlong
+        L.orc_hessian.argtypes = [ctypes.c_void_p, _d]
+        L.orc_hessian_copy.argtypes = [ctypes.c_void_p, _i, _i, _d]
+        L.orc_slot.restype = ctypes.c_int
+        L.orc_slot.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.orc_material_vjp.argtypes = [ctypes.c_void_p, _d, _d, _d]
+        L.orc_shape_vjp.argtypes = [ctypes.c_void_p, _d, _d, _d]
+        L.orc_element.restype = ctypes.c_int
+        L.orc_element.argtypes = [ctypes.c_void_p, ctypes.c_int, _d, _d, _d, _d]
+        L.orc_tables.restype = ctypes.c_int
+        L.orc_tables.argtypes = [ctypes.c_int, _d, _d, _d, _d]
+        L.orc_smc_new.restype = ctypes.c_void_p
+        L.orc_smc_new.argtypes = [ctypes.c_int]
+        L.orc_smc_copy.restype = ctypes.c_void_p
+        L.orc_smc_copy.argtypes = [ctypes.c_void_p]
+        L.orc_smc_add.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        L.orc_smc_prune.argtypes = [ctypes.c_void_p]
+        L.orc_smc_get_matrix.restype = ctypes.c_longlong
+        L.orc_smc_get_matrix.argtypes = [ctypes.c_void_p]
+        L.orc_smc_coeff.restype = ctypes.c_double
+        L.orc_smc_coeff.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.orc_smc_free.argtypes = [ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(_d)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_i)
+
+
+class Oracle:
+    """CPU restatement of NLAssembler + ElasticForm + ElasticForceDerivative."""
+
+    def __init__(self, mesh, lam, mu, n_threads: int = 1, cache_size: int = 900000,
+                 fast_pattern: bool = False):
+        L = lib()
+        self.mesh = mesh
+        self._conn = np.ascontiguousarray(mesh.conn, dtype=np.int32)
+        self._gconn = np.ascontiguousarray(mesh.gconn, dtype=np.int32)
+        self._X = np.ascontiguousarray(mesh.X, dtype=np.float64)
+        self._lam = np.ascontiguousarray(lam, dtype=np.float64)
+        self._mu = np.ascontiguousarray(mu, dtype=np.float64)
+        self.h = L.orc_create(mesh.elem_type, mesh.n_elements, mesh.n_nodes, _ip(self._conn),
+                              mesh.n_geom_nodes, _ip(self._gconn), _dp(self._X), _dp(self._lam),
+                              _dp(self._mu), int(n_threads), int(cache_size), int(fast_pattern))
+        if not self.h:
+            raise RuntimeError("oracle creation failed")
+        self.n_dofs = mesh.n_dofs
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def set_threads(self, n: int):
+        lib().orc_set_threads(self.h, int(n))
+
+    def energy(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        return lib().orc_energy(self.h, _dp(u))
+
+    def energy_per_element(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        out = np.empty(self.mesh.n_elements)
+        lib().orc_energy_per_element(self.h, _dp(u), _dp(out))
+        return out
+
+    def gradient(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        g = np.empty(self.n_dofs)
+        lib().orc_gradient(self.h, _dp(u), _dp(g))
+        return g
+
+    def hessian(self, u):
+        """Returns (outer, inner, values) of the CSC Hessian."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        nnz = lib().orc_hessian(self.h, _dp(u))
+        if nnz < 0:
+            raise RuntimeError("oracle hessian failed")
+        outer = np.empty(self.n_dofs + 1, dtype=np.int32)
+        inner = np.empty(nnz, dtype=np.int32)
+        vals = np.empty(nnz)
+        lib().orc_hessian_copy(self.h, _ip(outer), _ip(inner), _dp(vals))
+        return outer, inner, vals
+
+    def slot(self, e: int, k: int) -> int:
+        return lib().orc_slot(self.h, int(e), int(k))
+
+    def material_vjp(self, u, p):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        out = np.empty(2 * self.mesh.n_elements)
+        lib().orc_material_vjp(self.h, _dp(u), _dp(p), _dp(out))
+        return out
+
+    def shape_vjp(self, u, p):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        out = np.empty(3 * self.mesh.n_geom_nodes)
+        lib().orc_shape_vjp(self.h, _dp(u), _dp(p), _dp(out))
+        return out
+
+    def element(self, e: int, u):
+        n = self.mesh.conn.shape[1]
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        en = np.zeros(1)
+        g = np.zeros(3 * n)
+        H = np.zeros((3 * n, 3 * n))
+        lib().orc_element(self.h, int(e), _dp(u), _dp(en), _dp(g), _dp(H))
+        return en[0], g, H
+
+
+def tables(elem_type: int):
+    n = {1: 4, 2: 10, 3: 8}[elem_type]
+    ng = {1: 4, 2: 4, 3: 8}[elem_type]
+    qp = np.zeros((8, 3))
+    qw = np.zeros(8)
+    gr = np.zeros((8, n, 3))
+    gg = np.zeros((8, ng, 3))
+    nq = lib().orc_tables(elem_type, _dp(qp), _dp(qw), _dp(gr), _dp(gg))
+    return qp[:nq], qw[:nq], gr[:nq], gg[:nq]
+
+
+class SparseMatrixCache:
+    """Bare restated SparseMatrixCache, for the reference's 'cache' known-answer test."""
+
+    def __init__(self, size: int = 0, other: "SparseMatrixCache | None" = None):
+        L = lib()
+        self.h = L.orc_smc_copy(other.h) if other is not None else L.orc_smc_new(int(size))
+
+    def add_value(self, e, i, j, v):
+        lib().orc_smc_add(self.h, int(e), int(i), int(j), float(v))
+
+    def prune(self):
+        lib().orc_smc_prune(self.h)
+
+    def get_matrix(self):
+        return lib().orc_smc_get_matrix(self.h)
+
+    def coeff(self, i, j):
+        return lib().orc_smc_coeff(self.h, int(i), int(j))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_smc_free(self.h)
+            self.h = None

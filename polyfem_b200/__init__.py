@@ -1,0 +1,10 @@
+"""B200-native NeoHookean assembly (energy, gradient, Hessian, adjoint VJPs) for PolyFEM.
+
+The compute path is the CUDA library ``libpfgpu.so`` (C ABI in include/pfgpu.h);
+this package is its host-side mirror of PolyFEM's NLAssembler / ElasticForm API.
+"""
+from . import mesh
+from ._lib import PfgError, build, lib
+from .assembler import ElasticForceDerivative, ElasticForm, NeoHookeanAssembler
+
+__all__ = ["mesh", "build", "lib", "PfgError", "NeoHookeanAssembler", "ElasticForm", "ElasticForceDerivative"]

@@ -1,0 +1,318 @@
+"""Host-side mirror of PolyFEM's NeoHookean assembly interface, backed by libpfgpu.
+
+``NeoHookeanAssembler`` plays the part of ``NLAssembler`` + ``NeoHookeanElasticity``
+(assembler/Assembler.hpp:238-299) together with the ``AssemblyValsCache`` and the
+``SparseMatrixCache`` that ``ElasticForm`` owns.  ``ElasticForm`` mirrors
+solver/forms/ElasticForm.cpp and solver/forms/Form.hpp (value, first_derivative,
+second_derivative with weight()/scale), and ``ElasticForceDerivative`` mirrors
+optimization/force_derivatives/ElasticForceDerivative.cpp.
+
+Vectors may be numpy arrays (host memory: the call copies to the device and back)
+or CUDA float64 torch tensors (device memory: the call enqueues on torch's current
+stream and returns device tensors).  Every computation runs in libpfgpu's CUDA
+kernels; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import PFG_FP32, PFG_FP64, PFG_MEM_DEVICE, PFG_MEM_HOST, PFG_SPLIT32, check, lib
+
+PRECISIONS = {"fp64": PFG_FP64, "fp32": PFG_FP32, "split32": PFG_SPLIT32}
+
+
+def _prec(p) -> int:
+    if isinstance(p, str):
+        if p not in PRECISIONS:
+            raise ValueError(f"unknown precision {p!r}; expected one of {sorted(PRECISIONS)}")
+        return PRECISIONS[p]
+    return int(p)
+
+
+def _is_device(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(x.is_cuda)
+
+
+class NeoHookeanAssembler:
+    """NeoHookean energy / gradient / Hessian / adjoint terms on one GPU.
+
+    Parameters mirror what NLAssembler reads from ElementBases and LameParameters:
+    ``conn`` (E x n FE node ids), ``gconn`` (E x n_g geometric node ids, or None
+    when isoparametric), ``X`` (N_g x 3 rest positions), per-element ``lam``/``mu``.
+    """
+
+    def __init__(self, elem_type: int, conn, X, lam, mu, n_nodes: int | None = None,
+                 gconn=None, device: int = 0):
+        L = lib()
+        self.elem_type = int(elem_type)
+        self._conn = np.ascontiguousarray(conn, dtype=np.int32)
+        self._gconn = None if gconn is None else np.ascontiguousarray(gconn, dtype=np.int32)
+        self._X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 3)
+        self.n_elements = int(self._conn.shape[0])
+        self.n_nodes = int(n_nodes if n_nodes is not None else (self._conn.max() + 1 if self._conn.size else 0))
+        self.n_geom_nodes = int(self._X.shape[0])
+        self.n_dofs = 3 * self.n_nodes
+        lam = np.ascontiguousarray(np.broadcast_to(np.asarray(lam, dtype=np.float64), (self.n_elements,)))
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (self.n_elements,)))
+        self.device = int(device)
+        desc = _lib.MeshDesc(
+            self.elem_type, self.n_elements, self.n_nodes, self.n_geom_nodes,
+            self._conn.ctypes.data, None if self._gconn is None else self._gconn.ctypes.data,
+            self._X.ctypes.data, lam.ctypes.data, mu.ctypes.data, self.device)
+        h = ctypes.c_void_p()
+        st = L.pfg_create(ctypes.byref(desc), ctypes.byref(h))
+        check(st, None, "pfg_create")
+        self._h = h
+        self._nnz = None
+
+    @classmethod
+    def from_mesh(cls, mesh, lam, mu, device: int = 0):
+        gconn = None if mesh.gconn is mesh.conn else mesh.gconn
+        return cls(mesh.elem_type, mesh.conn, mesh.X, lam, mu, n_nodes=mesh.n_nodes, gconn=gconn, device=device)
+
+    # -- lifecycle -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pfg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- helpers -------------------------------------------------------------
+    def _prepare(self, *xs):
+        dev = [_is_device(x) for x in xs if x is not None]
+        if any(dev) and not all(dev):
+            raise ValueError("mix of host and device arrays")
+        if dev and dev[0]:
+            import torch
+            for x in xs:
+                if x is not None and (x.dtype != torch.float64 or not x.is_contiguous()):
+                    raise ValueError("device inputs must be contiguous float64 CUDA tensors")
+            check(lib().pfg_set_stream(self._h, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)),
+                  self._h, "pfg_set_stream")
+            return PFG_MEM_DEVICE, [x if x is None else ctypes.c_void_p(x.data_ptr()) for x in xs], xs
+        check(lib().pfg_set_stream(self._h, None), self._h, "pfg_set_stream")
+        arrs = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in xs]
+        return PFG_MEM_HOST, [None if a is None else ctypes.c_void_p(a.ctypes.data) for a in arrs], arrs
+
+    def _alloc(self, mem, n):
+        if mem == PFG_MEM_DEVICE:
+            import torch
+            t = torch.empty(n, dtype=torch.float64, device=f"cuda:{self.device}")
+            return t, ctypes.c_void_p(t.data_ptr())
+        a = np.empty(n, dtype=np.float64)
+        return a, ctypes.c_void_p(a.ctypes.data)
+
+    def _check_len(self, x, n, name):
+        if x is not None and int(x.numel() if hasattr(x, "numel") else np.size(x)) != n:
+            raise ValueError(f"{name} must have {n} entries")
+
+    # -- material / geometry updates -------------------------------------------
+    def set_lame(self, lam, mu):
+        """LameParameters per-element override (lambda_mat_/mu_mat_)."""
+        mem, ptrs, keep = self._prepare(lam, mu)
+        self._check_len(lam, self.n_elements, "lambda")
+        self._check_len(mu, self.n_elements, "mu")
+        check(lib().pfg_set_lame(self._h, ptrs[0], ptrs[1], mem), self._h, "pfg_set_lame")
+
+    def set_rest_positions(self, X):
+        mem, ptrs, keep = self._prepare(X)
+        self._check_len(X, 3 * self.n_geom_nodes, "X")
+        check(lib().pfg_set_rest_positions(self._h, ptrs[0], mem), self._h, "pfg_set_rest_positions")
+
+    # -- NLAssembler interface ---------------------------------------------------
+    def assemble_energy(self, u, precision="fp64"):
+        """NLAssembler::assemble_energy (assembler/Assembler.cpp:495-531)."""
+        self._check_len(u, self.n_dofs, "u")
+        mem, ptrs, keep = self._prepare(u)
+        out, optr = self._alloc(mem, 1)
+        check(lib().pfg_energy(self._h, ptrs[0], mem, _prec(precision), optr), self._h, "pfg_energy")
+        return float(out[0]) if mem == PFG_MEM_HOST else out[0]
+
+    def assemble_energy_per_element(self, u, precision="fp64"):
+        """NLAssembler::assemble_energy_per_element (assembler/Assembler.cpp:533-572)."""
+        self._check_len(u, self.n_dofs, "u")
+        mem, ptrs, keep = self._prepare(u)
+        out, optr = self._alloc(mem, self.n_elements)
+        check(lib().pfg_energy_per_element(self._h, ptrs[0], mem, _prec(precision), optr), self._h,
+              "pfg_energy_per_element")
+        return out
+
+    def assemble_gradient(self, u, precision="fp64"):
+        """NLAssembler::assemble_gradient (assembler/Assembler.cpp:574-643)."""
+        self._check_len(u, self.n_dofs, "u")
+        mem, ptrs, keep = self._prepare(u)
+        out, optr = self._alloc(mem, self.n_dofs)
+        check(lib().pfg_gradient(self._h, ptrs[0], mem, _prec(precision), optr), self._h, "pfg_gradient")
+        return out
+
+    def hessian_nnz(self) -> int:
+        if self._nnz is None:
+            nnz = ctypes.c_longlong()
+            check(lib().pfg_hessian_pattern(self._h, ctypes.byref(nnz)), self._h, "pfg_hessian_pattern")
+            self._nnz = int(nnz.value)
+        return self._nnz
+
+    def hessian_pattern(self, device: bool = False):
+        """CSC (outer, inner) of the Hessian; int32, Eigen ColMajor layout."""
+        nnz = self.hessian_nnz()
+        if device:
+            import torch
+            outer = torch.empty(self.n_dofs + 1, dtype=torch.int32, device=f"cuda:{self.device}")
+            inner = torch.empty(nnz, dtype=torch.int32, device=f"cuda:{self.device}")
+            check(lib().pfg_set_stream(self._h, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)),
+                  self._h, "pfg_set_stream")
+            check(lib().pfg_hessian_pattern_copy(self._h, ctypes.c_void_p(outer.data_ptr()),
+                                                 ctypes.c_void_p(inner.data_ptr()), PFG_MEM_DEVICE),
+                  self._h, "pfg_hessian_pattern_copy")
+            return outer, inner
+        outer = np.empty(self.n_dofs + 1, dtype=np.int32)
+        inner = np.empty(nnz, dtype=np.int32)
+        check(lib().pfg_set_stream(self._h, None), self._h, "pfg_set_stream")
+        check(lib().pfg_hessian_pattern_copy(self._h, ctypes.c_void_p(outer.ctypes.data),
+                                             ctypes.c_void_p(inner.ctypes.data), PFG_MEM_HOST),
+              self._h, "pfg_hessian_pattern_copy")
+        return outer, inner
+
+    def assemble_hessian_values(self, u, precision="fp64", project_to_psd: bool = False):
+        """CSC values of the Hessian (numpy for host u, torch CUDA tensor for device u)."""
+        self._check_len(u, self.n_dofs, "u")
+        nnz = self.hessian_nnz()
+        mem, ptrs, keep = self._prepare(u)
+        out, optr = self._alloc(mem, nnz)
+        check(lib().pfg_hessian(self._h, ptrs[0], mem, _prec(precision), int(bool(project_to_psd)), optr),
+              self._h, "pfg_hessian")
+        return out
+
+    def assemble_hessian(self, u, precision="fp64", project_to_psd: bool = False):
+        """NLAssembler::assemble_hessian (assembler/Assembler.cpp:645-771).
+
+        Host input -> scipy.sparse.csc_matrix; device input -> torch sparse CSR
+        tensor of H^T (= H: the pattern is structurally symmetric).
+        """
+        vals = self.assemble_hessian_values(u, precision, project_to_psd)
+        if _is_device(vals):
+            import torch
+            outer, inner = self.hessian_pattern(device=True)
+            return torch.sparse_csr_tensor(outer.long(), inner.long(), vals, size=(self.n_dofs, self.n_dofs))
+        import scipy.sparse as sp
+        outer, inner = self.hessian_pattern()
+        return sp.csc_matrix((vals, inner, outer), shape=(self.n_dofs, self.n_dofs))
+
+    def inverted_count(self) -> int:
+        c = ctypes.c_longlong()
+        check(lib().pfg_inverted_count(self._h, ctypes.byref(c)), self._h, "pfg_inverted_count")
+        return int(c.value)
+
+    # -- adjoint terms (ElasticForceDerivative) ------------------------------------
+    def force_material_derivative(self, u, adjoint):
+        """term = [-sum da (lnJ F^-T):grad p ; -sum da (F - F^-T):grad p], 2E entries."""
+        self._check_len(u, self.n_dofs, "u")
+        self._check_len(adjoint, self.n_dofs, "adjoint")
+        mem, ptrs, keep = self._prepare(u, adjoint)
+        out, optr = self._alloc(mem, 2 * self.n_elements)
+        check(lib().pfg_material_vjp(self._h, ptrs[0], ptrs[1], mem, optr), self._h, "pfg_material_vjp")
+        return out
+
+    def force_shape_derivative(self, u, adjoint, precision="fp64"):
+        """Adjoint shape term indexed by geometric node (3 N_g entries)."""
+        self._check_len(u, self.n_dofs, "u")
+        self._check_len(adjoint, self.n_dofs, "adjoint")
+        mem, ptrs, keep = self._prepare(u, adjoint)
+        out, optr = self._alloc(mem, 3 * self.n_geom_nodes)
+        check(lib().pfg_shape_vjp(self._h, ptrs[0], ptrs[1], mem, _prec(precision), optr), self._h,
+              "pfg_shape_vjp")
+        return out
+
+    def synchronize(self):
+        check(lib().pfg_synchronize(self._h), self._h, "pfg_synchronize")
+
+
+class ElasticForm:
+    """Mirror of solver::ElasticForm (solver/forms/ElasticForm.cpp) over the GPU assembler.
+
+    Like Form (solver/forms/Form.hpp:26-56), the public derivatives are the
+    unweighted ones times ``weight() / scale``.
+    """
+
+    def __init__(self, assembler: NeoHookeanAssembler, precision: str = "fp64"):
+        self.assembler = assembler
+        self.precision = precision
+        self._weight = 1.0
+        self._scale = 1.0
+        self.project_to_psd = False
+        self.enabled = True
+
+    def name(self) -> str:
+        return "elastic"
+
+    def weight(self) -> float:
+        return self._weight
+
+    def set_weight(self, w: float):
+        self._weight = float(w)
+
+    def set_scale(self, s: float):
+        self._scale = float(s)
+
+    def set_project_to_psd(self, v: bool):
+        self.project_to_psd = bool(v)
+
+    # unweighted ------------------------------------------------------------
+    def value_unweighted(self, x):
+        return self.assembler.assemble_energy(x, self.precision)
+
+    def value_per_element_unweighted(self, x):
+        return self.assembler.assemble_energy_per_element(x, self.precision)
+
+    def first_derivative_unweighted(self, x):
+        return self.assembler.assemble_gradient(x, self.precision)
+
+    def second_derivative_unweighted(self, x):
+        return self.assembler.assemble_hessian(x, self.precision, self.project_to_psd)
+
+    # weighted (Form.hpp) -----------------------------------------------------
+    def value(self, x):
+        return (self.weight() / self._scale) * self.value_unweighted(x)
+
+    def value_per_element(self, x):
+        return (self.weight() / self._scale) * self.value_per_element_unweighted(x)
+
+    def first_derivative(self, x):
+        return self.first_derivative_unweighted(x) * (self.weight() / self._scale)
+
+    def second_derivative(self, x):
+        return self.second_derivative_unweighted(x) * (self.weight() / self._scale)
+
+    def is_step_valid(self, x0, x1) -> bool:
+        """ElasticForm::is_step_valid (ElasticForm.cpp:388-396): reject NaN gradients."""
+        g = self.first_derivative(x1)
+        if _is_device(g):
+            import torch
+            return not bool(torch.isnan(g).any())
+        return not bool(np.isnan(g).any())
+
+
+class ElasticForceDerivative:
+    """Static adjoint terms, as optimization/force_derivatives/ElasticForceDerivative.hpp:11-26."""
+
+    @staticmethod
+    def force_material_derivative(form: ElasticForm, t: float, x, x_prev, adjoint):
+        return form.assembler.force_material_derivative(x, adjoint)
+
+    @staticmethod
+    def force_shape_derivative(form: ElasticForm, t: float, n_verts: int, x, x_prev, adjoint):
+        if n_verts != form.assembler.n_geom_nodes:
+            raise ValueError("n_verts must equal the number of geometric nodes")
+        return form.assembler.force_shape_derivative(x, adjoint, "fp64")

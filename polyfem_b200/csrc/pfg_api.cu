@@ -1,0 +1,589 @@
+// Host side of the C ABI declared in include/pfgpu.h.
+//
+// Ownership and lifecycle mirror the reference: the context plays the role of
+// ElasticForm (solver/forms/ElasticForm.cpp) holding the AssemblyValsCache
+// inputs and the mutable SparseMatrixCache; the pattern and element->slot map
+// are built once (first pfg_hessian / pfg_hessian_pattern call) and then stay
+// on the device, like SparseMatrixCache's mapping_/second_cache_
+// (utils/MatrixCache.cpp:134-212).
+#include "../../include/pfgpu.h"
+#include "pfg_internal.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace pfg;
+
+struct pfg_context
+{
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	int n = 0, ng = 0; // nodes / geometric nodes per element
+	DevMesh m;
+	// owned device buffers
+	int *d_conn = nullptr, *d_gconn = nullptr;
+	double *d_X = nullptr;
+	double2 *d_lame = nullptr;
+	// pattern
+	bool has_pattern = false;
+	DevPattern pat;
+	int *d_outer = nullptr, *d_inner = nullptr, *d_slot = nullptr, *d_colstride = nullptr;
+	double *d_values = nullptr;
+	std::vector<int> h_conn; // row-major E x n copy for the host pattern build
+	// scratch and host-mode staging
+	Scratch sc;
+	double *d_result = nullptr;
+	double *d_u = nullptr, *d_p = nullptr, *d_out = nullptr;
+	size_t out_cap = 0;
+	std::string err;
+};
+
+static thread_local std::string g_create_error;
+
+namespace
+{
+int fail(pfg_context *c, int status, const std::string &msg)
+{
+	if (c)
+		c->err = msg;
+	else
+		g_create_error = msg;
+	return status;
+}
+
+int cuda_fail(pfg_context *c, cudaError_t e, const char *where)
+{
+	const int st = (e == cudaErrorMemoryAllocation) ? PFG_ERR_OOM : PFG_ERR_CUDA;
+	return fail(c, st, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define PFG_CUDA(c, call)                                   \
+	do                                                      \
+	{                                                       \
+		cudaError_t e_ = (call);                            \
+		if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+	} while (0)
+
+struct DeviceGuard
+{
+	int prev = -1;
+	explicit DeviceGuard(int dev)
+	{
+		cudaGetDevice(&prev);
+		if (prev != dev) cudaSetDevice(dev);
+	}
+	~DeviceGuard()
+	{
+		int cur = -1;
+		cudaGetDevice(&cur);
+		if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+	}
+};
+
+int nodes_per_element(int et) { return et == PFG_P1_TET ? 4 : et == PFG_P2_TET ? 10 : et == PFG_Q1_HEX ? 8 : 0; }
+int geom_nodes_per_element(int et) { return et == PFG_P1_TET ? 4 : et == PFG_P2_TET ? 4 : et == PFG_Q1_HEX ? 8 : 0; }
+
+template <class F>
+void parallel_ranges(long long n, F &&f)
+{
+	int nt = (int)std::min<long long>(std::max(1u, std::thread::hardware_concurrency()), 32);
+	if (n < 4096) nt = 1;
+	if (nt <= 1)
+	{
+		f(0LL, n, 0);
+		return;
+	}
+	std::vector<std::thread> th;
+	for (int t = 0; t < nt; ++t)
+		th.emplace_back([&, t] { f(n * t / nt, n * (t + 1) / nt, t); });
+	for (auto &x : th) x.join();
+}
+
+int check_mem(int mem) { return mem == PFG_MEM_HOST || mem == PFG_MEM_DEVICE; }
+int check_prec(int prec) { return prec == PFG_FP64 || prec == PFG_FP32 || prec == PFG_SPLIT32; }
+
+int ensure_staging(pfg_context *c, size_t out_doubles)
+{
+	const size_t ndof = 3 * (size_t)c->m.N;
+	if (!c->d_u)
+	{
+		PFG_CUDA(c, cudaMalloc(&c->d_u, std::max<size_t>(ndof, 1) * sizeof(double)));
+		PFG_CUDA(c, cudaMalloc(&c->d_p, std::max<size_t>(ndof, 1) * sizeof(double)));
+	}
+	if (out_doubles > c->out_cap)
+	{
+		if (c->d_out) cudaFree(c->d_out);
+		c->d_out = nullptr;
+		c->out_cap = 0;
+		PFG_CUDA(c, cudaMalloc(&c->d_out, out_doubles * sizeof(double)));
+		c->out_cap = out_doubles;
+	}
+	return PFG_OK;
+}
+
+// Stage a host input vector of 3N doubles into `dst`; device inputs are used in place.
+int stage_in(pfg_context *c, const double *src, int mem, double *dst, size_t n, const double **use)
+{
+	if (mem == PFG_MEM_DEVICE)
+	{
+		*use = src;
+		return PFG_OK;
+	}
+	if (n) PFG_CUDA(c, cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	*use = dst;
+	return PFG_OK;
+}
+
+int finish_host(pfg_context *c, double *host_dst, const double *dev_src, size_t n)
+{
+	if (n) PFG_CUDA(c, cudaMemcpyAsync(host_dst, dev_src, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+	PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	return PFG_OK;
+}
+
+// Host build of the CSC pattern (Eigen ColMajor semantics: per column the sorted
+// unique rows touched by any element) and the element node-pair slot map.
+int build_pattern(pfg_context *c)
+{
+	const int E = c->m.E, N = c->m.N, n = c->n;
+	const int *conn = c->h_conn.data();
+	// node -> element incidence
+	std::vector<long long> ioff(N + 1, 0);
+	for (long long i = 0; i < (long long)E * n; ++i) ioff[conn[i] + 1]++;
+	for (int i = 0; i < N; ++i) ioff[i + 1] += ioff[i];
+	std::vector<int> inc(ioff[N]);
+	{
+		std::vector<long long> pos(ioff.begin(), ioff.end() - 1);
+		for (int e = 0; e < E; ++e)
+			for (int a = 0; a < n; ++a) inc[pos[conn[(size_t)e * n + a]]++] = e;
+	}
+	// neighbours of every node, sorted and unique, built in parallel node ranges
+	std::vector<int> deg(N, 0);
+	const int nt_max = 64;
+	std::vector<std::vector<int>> part(nt_max);
+	std::vector<long long> part_begin(nt_max, 0), part_end(nt_max, 0);
+	int used_threads = 0;
+	parallel_ranges(N, [&](long long s, long long e, int t) {
+		std::vector<int> tmp;
+		auto &out = part[t];
+		part_begin[t] = s;
+		part_end[t] = e;
+		for (long long B = s; B < e; ++B)
+		{
+			tmp.clear();
+			for (long long k = ioff[B]; k < ioff[B + 1]; ++k)
+			{
+				const int el = inc[k];
+				for (int a = 0; a < n; ++a) tmp.push_back(conn[(size_t)el * n + a]);
+			}
+			std::sort(tmp.begin(), tmp.end());
+			tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+			deg[B] = (int)tmp.size();
+			out.insert(out.end(), tmp.begin(), tmp.end());
+		}
+	});
+	for (int t = 0; t < nt_max; ++t)
+		if (part_end[t] > part_begin[t]) used_threads = t + 1;
+	std::vector<long long> noff(N + 1, 0);
+	for (int i = 0; i < N; ++i) noff[i + 1] = noff[i] + deg[i];
+	std::vector<int> nbr(noff[N]);
+	for (int t = 0; t < used_threads; ++t)
+		if (!part[t].empty()) std::copy(part[t].begin(), part[t].end(), nbr.begin() + noff[part_begin[t]]);
+	part.clear();
+
+	const long long nnz = 9 * noff[N];
+	if (nnz > 0x7fffffffLL) return fail(c, PFG_ERR_UNSUPPORTED, "Hessian has more than 2^31-1 nonzeros (int32 CSC)");
+	const int ndof = 3 * N;
+	std::vector<int> outer(ndof + 1);
+	{
+		long long base = 0;
+		for (int B = 0; B < N; ++B)
+		{
+			for (int cc = 0; cc < 3; ++cc) outer[3 * B + cc] = (int)(base + (long long)cc * 3 * deg[B]);
+			base += 9LL * deg[B];
+		}
+		outer[ndof] = (int)base;
+	}
+	std::vector<int> inner(nnz);
+	parallel_ranges(N, [&](long long s, long long e, int) {
+		for (long long B = s; B < e; ++B)
+			for (int cc = 0; cc < 3; ++cc)
+			{
+				long long o = outer[3 * B + cc];
+				for (long long k = noff[B]; k < noff[B + 1]; ++k)
+					for (int m = 0; m < 3; ++m) inner[o++] = 3 * nbr[k] + m;
+			}
+	});
+	std::vector<int> slot((size_t)E * n * n);
+	parallel_ranges(E, [&](long long s, long long e, int) {
+		for (long long el = s; el < e; ++el)
+			for (int a = 0; a < n; ++a)
+				for (int b = 0; b < n; ++b)
+				{
+					const int A = conn[el * n + a], B = conn[el * n + b];
+					const int *lo = nbr.data() + noff[B], *hi = nbr.data() + noff[B + 1];
+					const int rank = (int)(std::lower_bound(lo, hi, A) - lo);
+					slot[(size_t)el * n * n + a * n + b] = outer[3 * B] + 3 * rank;
+				}
+	});
+	std::vector<int> colstride(N);
+	for (int B = 0; B < N; ++B) colstride[B] = 3 * deg[B];
+
+	PFG_CUDA(c, cudaMalloc(&c->d_outer, sizeof(int) * (ndof + 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_inner, sizeof(int) * std::max<long long>(nnz, 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_slot, sizeof(int) * std::max<size_t>(slot.size(), 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_colstride, sizeof(int) * std::max(N, 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_values, sizeof(double) * std::max<long long>(nnz, 1)));
+	PFG_CUDA(c, cudaMemcpy(c->d_outer, outer.data(), sizeof(int) * (ndof + 1), cudaMemcpyHostToDevice));
+	if (nnz) PFG_CUDA(c, cudaMemcpy(c->d_inner, inner.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice));
+	if (!slot.empty()) PFG_CUDA(c, cudaMemcpy(c->d_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice));
+	if (N) PFG_CUDA(c, cudaMemcpy(c->d_colstride, colstride.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+	c->pat.nnz = nnz;
+	c->pat.outer = c->d_outer;
+	c->pat.inner = c->d_inner;
+	c->pat.slot = c->d_slot;
+	c->pat.colstride = c->d_colstride;
+	c->pat.values = c->d_values;
+	c->has_pattern = true;
+	return PFG_OK;
+}
+
+void free_all(pfg_context *c)
+{
+	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_slot, c->d_colstride,
+					c->d_values, c->sc.partials, c->sc.ticket, c->sc.inverted, c->d_result, c->d_u, c->d_p, c->d_out};
+	for (void *p : ptrs)
+		if (p) cudaFree(p);
+}
+} // namespace
+
+extern "C" {
+
+int pfg_version(void) { return 100; }
+
+const char *pfg_status_string(int s)
+{
+	switch (s)
+	{
+	case PFG_OK: return "ok";
+	case PFG_ERR_INVALID: return "invalid argument";
+	case PFG_ERR_CUDA: return "CUDA error";
+	case PFG_ERR_OOM: return "out of memory";
+	case PFG_ERR_UNSUPPORTED: return "unsupported";
+	case PFG_ERR_STATE: return "invalid state";
+	}
+	return "unknown status";
+}
+
+const char *pfg_last_error(const pfg_context *c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+int pfg_create(const pfg_mesh_desc *d, pfg_context **out)
+{
+	if (!out) return fail(nullptr, PFG_ERR_INVALID, "out is NULL");
+	*out = nullptr;
+	if (!d) return fail(nullptr, PFG_ERR_INVALID, "desc is NULL");
+	const int n = nodes_per_element(d->elem_type), ng = geom_nodes_per_element(d->elem_type);
+	if (!n) return fail(nullptr, PFG_ERR_INVALID, "unknown elem_type");
+	if (d->n_elements < 0 || d->n_nodes < 0 || d->n_geom_nodes < 0) return fail(nullptr, PFG_ERR_INVALID, "negative size");
+	if ((long long)d->n_nodes * 3 > 0x7fffffffLL) return fail(nullptr, PFG_ERR_UNSUPPORTED, "too many nodes");
+	if (d->n_elements > 0 && (!d->conn || !d->X || !d->lambda || !d->mu))
+		return fail(nullptr, PFG_ERR_INVALID, "conn, X, lambda and mu are required");
+	const int *gconn = d->gconn ? d->gconn : d->conn;
+	if (!d->gconn && ng != n) return fail(nullptr, PFG_ERR_INVALID, "gconn is required for non-isoparametric elements");
+	const size_t E = (size_t)d->n_elements;
+	for (size_t i = 0; i < E * n; ++i)
+		if (d->conn[i] < 0 || d->conn[i] >= d->n_nodes)
+			return fail(nullptr, PFG_ERR_INVALID, "conn[" + std::to_string(i) + "] = " + std::to_string(d->conn[i]) + " out of range");
+	for (size_t i = 0; i < E * ng; ++i)
+		if (gconn[i] < 0 || gconn[i] >= d->n_geom_nodes)
+			return fail(nullptr, PFG_ERR_INVALID, "gconn[" + std::to_string(i) + "] out of range");
+	int ndev = 0;
+	cudaError_t ce = cudaGetDeviceCount(&ndev);
+	if (ce != cudaSuccess) return fail(nullptr, PFG_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(ce));
+	if (d->device < 0 || d->device >= ndev) return fail(nullptr, PFG_ERR_INVALID, "bad device ordinal");
+
+	DeviceGuard g(d->device);
+	auto *c = new pfg_context();
+	c->device = d->device;
+	c->n = n;
+	c->ng = ng;
+	c->m.et = d->elem_type;
+	c->m.E = d->n_elements;
+	c->m.N = d->n_nodes;
+	c->m.Ng = d->n_geom_nodes;
+	c->h_conn.assign(d->conn, d->conn + E * n);
+
+	auto bail = [&](int st) {
+		g_create_error = c->err;
+		free_all(c);
+		delete c;
+		return st;
+	};
+#define CREATE_CUDA(call)                                 \
+	do                                                    \
+	{                                                     \
+		cudaError_t e_ = (call);                          \
+		if (e_ != cudaSuccess) return bail(cuda_fail(c, e_, #call)); \
+	} while (0)
+
+	// structure-of-arrays connectivity
+	{
+		std::vector<int> soa(E * n);
+		for (size_t e = 0; e < E; ++e)
+			for (int a = 0; a < n; ++a) soa[(size_t)a * E + e] = d->conn[e * n + a];
+		CREATE_CUDA(cudaMalloc(&c->d_conn, sizeof(int) * std::max<size_t>(soa.size(), 1)));
+		if (!soa.empty()) CREATE_CUDA(cudaMemcpy(c->d_conn, soa.data(), sizeof(int) * soa.size(), cudaMemcpyHostToDevice));
+	}
+	if (d->gconn && (d->gconn != d->conn || ng != n))
+	{
+		std::vector<int> soa(E * ng);
+		for (size_t e = 0; e < E; ++e)
+			for (int a = 0; a < ng; ++a) soa[(size_t)a * E + e] = gconn[e * ng + a];
+		CREATE_CUDA(cudaMalloc(&c->d_gconn, sizeof(int) * std::max<size_t>(soa.size(), 1)));
+		if (!soa.empty()) CREATE_CUDA(cudaMemcpy(c->d_gconn, soa.data(), sizeof(int) * soa.size(), cudaMemcpyHostToDevice));
+	}
+	CREATE_CUDA(cudaMalloc(&c->d_X, sizeof(double) * 3 * std::max(d->n_geom_nodes, 1)));
+	if (d->n_geom_nodes)
+		CREATE_CUDA(cudaMemcpy(c->d_X, d->X, sizeof(double) * 3 * d->n_geom_nodes, cudaMemcpyHostToDevice));
+	{
+		std::vector<double2> lm(std::max<size_t>(E, 1));
+		for (size_t e = 0; e < E; ++e) lm[e] = make_double2(d->lambda[e], d->mu[e]);
+		CREATE_CUDA(cudaMalloc(&c->d_lame, sizeof(double2) * lm.size()));
+		CREATE_CUDA(cudaMemcpy(c->d_lame, lm.data(), sizeof(double2) * lm.size(), cudaMemcpyHostToDevice));
+	}
+	c->sc.max_blocks = (int)(E / 128 + 2);
+	CREATE_CUDA(cudaMalloc(&c->sc.partials, sizeof(double) * c->sc.max_blocks));
+	CREATE_CUDA(cudaMalloc(&c->sc.ticket, sizeof(unsigned int)));
+	CREATE_CUDA(cudaMemset(c->sc.ticket, 0, sizeof(unsigned int)));
+	CREATE_CUDA(cudaMalloc(&c->sc.inverted, sizeof(unsigned long long)));
+	CREATE_CUDA(cudaMemset(c->sc.inverted, 0, sizeof(unsigned long long)));
+	CREATE_CUDA(cudaMalloc(&c->d_result, sizeof(double)));
+	CREATE_CUDA(hessian_kernel_setup(c->device));
+#undef CREATE_CUDA
+	c->m.conn = c->d_conn;
+	c->m.gconn = c->d_gconn ? c->d_gconn : c->d_conn;
+	c->m.X = c->d_X;
+	c->m.lame = c->d_lame;
+	*out = c;
+	return PFG_OK;
+}
+
+int pfg_destroy(pfg_context *c)
+{
+	if (!c) return PFG_ERR_INVALID;
+	{
+		DeviceGuard g(c->device);
+		if (c->stream) cudaStreamSynchronize(c->stream);
+		free_all(c);
+	}
+	delete c;
+	return PFG_OK;
+}
+
+int pfg_set_stream(pfg_context *c, void *stream)
+{
+	if (!c) return PFG_ERR_INVALID;
+	c->stream = (cudaStream_t)stream;
+	return PFG_OK;
+}
+
+int pfg_set_lame(pfg_context *c, const double *lambda, const double *mu, int mem)
+{
+	if (!c || !check_mem(mem)) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (c->m.E && (!lambda || !mu)) return fail(c, PFG_ERR_INVALID, "lambda/mu NULL");
+	DeviceGuard g(c->device);
+	const size_t E = c->m.E;
+	if (!E) return PFG_OK;
+	if (mem == PFG_MEM_HOST)
+	{
+		std::vector<double2> lm(E);
+		for (size_t e = 0; e < E; ++e) lm[e] = make_double2(lambda[e], mu[e]);
+		PFG_CUDA(c, cudaMemcpyAsync(c->d_lame, lm.data(), sizeof(double2) * E, cudaMemcpyHostToDevice, c->stream));
+		PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	}
+	else
+	{
+		PFG_CUDA(c, cudaMemcpy2DAsync(c->d_lame, sizeof(double2), lambda, sizeof(double), sizeof(double), E,
+									  cudaMemcpyDeviceToDevice, c->stream));
+		PFG_CUDA(c, cudaMemcpy2DAsync((char *)c->d_lame + sizeof(double), sizeof(double2), mu, sizeof(double),
+									  sizeof(double), E, cudaMemcpyDeviceToDevice, c->stream));
+	}
+	return PFG_OK;
+}
+
+int pfg_set_rest_positions(pfg_context *c, const double *X, int mem)
+{
+	if (!c || !check_mem(mem)) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (c->m.Ng && !X) return fail(c, PFG_ERR_INVALID, "X NULL");
+	DeviceGuard g(c->device);
+	const size_t bytes = sizeof(double) * 3 * (size_t)c->m.Ng;
+	if (!bytes) return PFG_OK;
+	PFG_CUDA(c, cudaMemcpyAsync(c->d_X, X, bytes, mem == PFG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+								c->stream));
+	if (mem == PFG_MEM_HOST) PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	return PFG_OK;
+}
+
+int pfg_energy(pfg_context *c, const double *u, int mem, int prec, double *out)
+{
+	if (!c || !check_mem(mem) || !check_prec(prec) || !out) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (c->m.N && !u) return fail(c, PFG_ERR_INVALID, "u NULL");
+	DeviceGuard g(c->device);
+	int st = ensure_staging(c, 1);
+	if (st) return st;
+	const double *du;
+	if ((st = stage_in(c, u, mem, c->d_u, 3 * (size_t)c->m.N, &du))) return st;
+	PFG_CUDA(c, cudaMemsetAsync(c->sc.inverted, 0, sizeof(unsigned long long), c->stream));
+	double *dst = mem == PFG_MEM_DEVICE ? out : c->d_result;
+	PFG_CUDA(c, launch_energy(c->m, du, prec, false, dst, c->sc, c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, out, c->d_result, 1);
+	return PFG_OK;
+}
+
+int pfg_energy_per_element(pfg_context *c, const double *u, int mem, int prec, double *out)
+{
+	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.E && !out)) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (c->m.N && !u) return fail(c, PFG_ERR_INVALID, "u NULL");
+	DeviceGuard g(c->device);
+	int st = ensure_staging(c, std::max(c->m.E, 1));
+	if (st) return st;
+	const double *du;
+	if ((st = stage_in(c, u, mem, c->d_u, 3 * (size_t)c->m.N, &du))) return st;
+	PFG_CUDA(c, cudaMemsetAsync(c->sc.inverted, 0, sizeof(unsigned long long), c->stream));
+	double *dst = mem == PFG_MEM_DEVICE ? out : c->d_out;
+	PFG_CUDA(c, launch_energy(c->m, du, prec, true, dst, c->sc, c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, out, c->d_out, c->m.E);
+	return PFG_OK;
+}
+
+int pfg_gradient(pfg_context *c, const double *u, int mem, int prec, double *gout)
+{
+	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.N && (!gout || !u))) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	DeviceGuard g(c->device);
+	const size_t ndof = 3 * (size_t)c->m.N;
+	int st = ensure_staging(c, std::max<size_t>(ndof, 1));
+	if (st) return st;
+	const double *du;
+	if ((st = stage_in(c, u, mem, c->d_u, ndof, &du))) return st;
+	PFG_CUDA(c, cudaMemsetAsync(c->sc.inverted, 0, sizeof(unsigned long long), c->stream));
+	double *dst = mem == PFG_MEM_DEVICE ? gout : c->d_out;
+	PFG_CUDA(c, launch_gradient(c->m, du, prec, dst, c->sc, c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, gout, c->d_out, ndof);
+	return PFG_OK;
+}
+
+int pfg_hessian_pattern(pfg_context *c, long long *nnz)
+{
+	if (!c) return PFG_ERR_INVALID;
+	DeviceGuard g(c->device);
+	if (!c->has_pattern)
+	{
+		const int st = build_pattern(c);
+		if (st) return st;
+	}
+	if (nnz) *nnz = c->pat.nnz;
+	return PFG_OK;
+}
+
+int pfg_hessian_pattern_copy(pfg_context *c, int *outer, int *inner, int mem)
+{
+	if (!c || !check_mem(mem)) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (!c->has_pattern) return fail(c, PFG_ERR_STATE, "pattern not built");
+	DeviceGuard g(c->device);
+	const cudaMemcpyKind k = mem == PFG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+	if (outer) PFG_CUDA(c, cudaMemcpyAsync(outer, c->d_outer, sizeof(int) * (3 * (size_t)c->m.N + 1), k, c->stream));
+	if (inner && c->pat.nnz) PFG_CUDA(c, cudaMemcpyAsync(inner, c->d_inner, sizeof(int) * c->pat.nnz, k, c->stream));
+	if (mem == PFG_MEM_HOST) PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	return PFG_OK;
+}
+
+int pfg_hessian(pfg_context *c, const double *u, int mem, int prec, int project_psd, double *values)
+{
+	if (!c || !check_mem(mem) || !check_prec(prec)) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (c->m.N && !u) return fail(c, PFG_ERR_INVALID, "u NULL");
+	if (project_psd) return fail(c, PFG_ERR_UNSUPPORTED, "project_to_psd is not implemented");
+	DeviceGuard g(c->device);
+	int st;
+	if (!c->has_pattern && (st = build_pattern(c))) return st;
+	if ((st = ensure_staging(c, 1))) return st;
+	const double *du;
+	if ((st = stage_in(c, u, mem, c->d_u, 3 * (size_t)c->m.N, &du))) return st;
+	PFG_CUDA(c, launch_hessian(c->m, c->pat, du, prec, c->stream));
+	if (values)
+	{
+		if (mem == PFG_MEM_HOST) return finish_host(c, values, c->d_values, c->pat.nnz);
+		if (c->pat.nnz)
+			PFG_CUDA(c, cudaMemcpyAsync(values, c->d_values, sizeof(double) * c->pat.nnz, cudaMemcpyDeviceToDevice, c->stream));
+	}
+	else if (mem == PFG_MEM_HOST)
+		PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	return PFG_OK;
+}
+
+int pfg_hessian_device_csc(pfg_context *c, const int **outer, const int **inner, double **values)
+{
+	if (!c) return PFG_ERR_INVALID;
+	if (!c->has_pattern) return fail(c, PFG_ERR_STATE, "pattern not built");
+	if (outer) *outer = c->d_outer;
+	if (inner) *inner = c->d_inner;
+	if (values) *values = c->d_values;
+	return PFG_OK;
+}
+
+int pfg_material_vjp(pfg_context *c, const double *u, const double *p, int mem, double *out)
+{
+	if (!c || !check_mem(mem) || (c->m.E && !out) || (c->m.N && (!u || !p))) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	DeviceGuard g(c->device);
+	const size_t ndof = 3 * (size_t)c->m.N;
+	int st = ensure_staging(c, std::max<size_t>(2 * (size_t)c->m.E, 1));
+	if (st) return st;
+	const double *du, *dp;
+	if ((st = stage_in(c, u, mem, c->d_u, ndof, &du))) return st;
+	if ((st = stage_in(c, p, mem, c->d_p, ndof, &dp))) return st;
+	double *dst = mem == PFG_MEM_DEVICE ? out : c->d_out;
+	PFG_CUDA(c, launch_material_vjp(c->m, du, dp, dst, c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, out, c->d_out, 2 * (size_t)c->m.E);
+	return PFG_OK;
+}
+
+int pfg_shape_vjp(pfg_context *c, const double *u, const double *p, int mem, int prec, double *out)
+{
+	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.Ng && !out) || (c->m.N && (!u || !p)))
+		return fail(c, PFG_ERR_INVALID, "bad arguments");
+	DeviceGuard g(c->device);
+	const size_t ndof = 3 * (size_t)c->m.N;
+	int st = ensure_staging(c, std::max<size_t>(3 * (size_t)c->m.Ng, 1));
+	if (st) return st;
+	const double *du, *dp;
+	if ((st = stage_in(c, u, mem, c->d_u, ndof, &du))) return st;
+	if ((st = stage_in(c, p, mem, c->d_p, ndof, &dp))) return st;
+	double *dst = mem == PFG_MEM_DEVICE ? out : c->d_out;
+	PFG_CUDA(c, launch_shape_vjp(c->m, du, dp, prec, dst, c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, out, c->d_out, 3 * (size_t)c->m.Ng);
+	return PFG_OK;
+}
+
+int pfg_inverted_count(pfg_context *c, long long *count)
+{
+	if (!c || !count) return PFG_ERR_INVALID;
+	DeviceGuard g(c->device);
+	unsigned long long v = 0;
+	PFG_CUDA(c, cudaMemcpyAsync(&v, c->sc.inverted, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+	PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	*count = (long long)v;
+	return PFG_OK;
+}
+
+int pfg_synchronize(pfg_context *c)
+{
+	if (!c) return PFG_ERR_INVALID;
+	DeviceGuard g(c->device);
+	PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	return PFG_OK;
+}
+
+} // extern "C"
