@@ -155,6 +155,35 @@ const char *pfg_status_string(int status);
 /* Library version, e.g. 100 for 0.1.0. */
 int pfg_version(void);
 
+/* ---------------------------------------------------------------------------
+ * Allocation-free energy.  No counterpart in the reference: PolyFEM always
+ * owns its memory.  It exists for callers that must not allocate device
+ * memory at all (a host that pre-plans every byte, or runs inside a pool it
+ * does not own), for whom pfg_create is not an option because it allocates.
+ *
+ * Same result as pfg_energy for the same inputs.  Every pointer is device
+ * memory on the current device and is owned by the caller:
+ *   conn_soa  : [n][E] int32, local node a of element e at conn_soa[a*E + e]
+ *   gconn_soa : [n_g][E] int32 (required for P2; NULL = conn_soa otherwise)
+ *   X         : [N_g][3] float64 rest positions
+ *   lame      : [E][2] float64 (lambda, mu) per element
+ *   u         : [3N] float64 displacement, node-major
+ *   out       : 1 float64 (the energy)
+ * The call enqueues work on `stream` (cudaStream_t as void*, NULL = default
+ * stream) and returns without synchronising.  It allocates nothing: the
+ * reduction scratch is a fixed array inside the library's device image
+ * (512 KiB, held by every GPU that loads the library until exit), which
+ * limits n_elements to 256 * PFG_NOALLOC_MAX_BLOCKS; larger meshes return
+ * PFG_ERR_UNSUPPORTED with the limit in pfg_last_error(NULL).  All calls
+ * share that array, so calls that overlap on the GPU race.  The first call on
+ * a device looks up the array's address; make it before any stream capture.
+ * Errors are reported through pfg_last_error(NULL).
+ * ------------------------------------------------------------------------- */
+#define PFG_NOALLOC_MAX_BLOCKS 65536
+int pfg_energy_noalloc(int elem_type, int n_elements, int n_nodes, int n_geom_nodes, const int *conn_soa,
+                       const int *gconn_soa, const double *X, const double *lame, const double *u, int prec,
+                       double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB_PATH = os.path.join(HERE, "libpfgpu.so")
-SOURCES = ["pfg_api.cu", "pfg_kernels.cu", "pfg_tc.cu"]
+SOURCES = ["pfg_api.cu", "pfg_kernels.cu", "pfg_tc.cu", "pfg_noalloc.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 PFG_OK = 0
@@ -105,6 +105,8 @@ SIGNATURES = {
     "pfg_last_error": (ctypes.c_char_p, [_vp]),
     "pfg_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "pfg_version": (ctypes.c_int, []),
+    "pfg_energy_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                          _vp, ctypes.c_int, _vp, _vp]),
 }
 
 

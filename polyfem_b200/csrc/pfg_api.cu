@@ -44,6 +44,8 @@ struct pfg_context
 
 static thread_local std::string g_create_error;
 
+void pfg::set_global_error(const std::string &msg) { g_create_error = msg; }
+
 namespace
 {
 int fail(pfg_context *c, int status, const std::string &msg)

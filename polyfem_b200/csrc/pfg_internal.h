@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
 
 namespace pfg
 {
@@ -59,5 +60,8 @@ cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double 
 cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out,
 							 cudaStream_t s);
 cudaError_t hessian_kernel_setup(int device);
+
+// Sets the message pfg_last_error(NULL) returns on this host thread.
+void set_global_error(const std::string &msg);
 
 } // namespace pfg
