@@ -2,9 +2,10 @@
 //
 // Ownership and lifecycle mirror the reference: the context plays the role of
 // ElasticForm (solver/forms/ElasticForm.cpp) holding the AssemblyValsCache
-// inputs and the mutable SparseMatrixCache; the pattern and element->slot map
-// are built once (first pfg_hessian / pfg_hessian_pattern call) and then stay
-// on the device, like SparseMatrixCache's mapping_/second_cache_
+// inputs and the mutable SparseMatrixCache; the pattern and the assembly plan
+// (which element incidences feed which CSC column block, and at which row) are
+// built once (first pfg_hessian / pfg_hessian_pattern call) and then stay on
+// the device, like SparseMatrixCache's mapping_/second_cache_
 // (utils/MatrixCache.cpp:134-212).
 #include "../../include/pfgpu.h"
 #include "pfg_internal.h"
@@ -31,8 +32,17 @@ struct pfg_context
 	// pattern
 	bool has_pattern = false;
 	DevPattern pat;
-	int *d_outer = nullptr, *d_inner = nullptr, *d_slot = nullptr, *d_colstride = nullptr;
+	int *d_outer = nullptr, *d_inner = nullptr;
 	double *d_values = nullptr;
+	unsigned short *d_strip_rank = nullptr;
+	int *d_eb_inc = nullptr;
+	// node -> (element, local index) incidences, FE and geometric nodes
+	std::vector<long long> h_inc_off; // [N+1]
+	std::vector<int> h_inc_e;         // element of each incidence, grouped by node, ascending
+	int *d_inc_off = nullptr, *d_inc_eb = nullptr, *d_ginc_off = nullptr, *d_ginc_eb = nullptr;
+	// staging buffers (allocated on first use): element contributions / element Hessian blocks
+	double *d_vec_stage = nullptr;
+	void *d_hess_stage[2] = {nullptr, nullptr}; // [0] FP64, [1] FP32
 	std::vector<int> h_conn; // row-major E x n copy for the host pattern build
 	// scratch and host-mode staging
 	Scratch sc;
@@ -127,6 +137,32 @@ int ensure_staging(pfg_context *c, size_t out_doubles)
 	return PFG_OK;
 }
 
+// Element-contribution staging of the gradient / shape term (first use allocates).
+int ensure_vec_stage(pfg_context *c)
+{
+	if (!c->d_vec_stage)
+	{
+		const size_t n = (size_t)std::max(c->m.E, 1) * std::max(c->n, c->ng) * 3;
+		PFG_CUDA(c, cudaMalloc(&c->d_vec_stage, n * sizeof(double)));
+	}
+	c->sc.vec_stage = c->d_vec_stage;
+	return PFG_OK;
+}
+
+// Element-block staging of the Hessian for one precision (first use allocates).
+int ensure_hess_stage(pfg_context *c, int prec)
+{
+	const int k = prec == PFG_FP64 ? 0 : 1;
+	if (!c->d_hess_stage[k])
+	{
+		const size_t tsz = k == 0 ? sizeof(double) : sizeof(float);
+		const size_t rec = ((9 * c->n * tsz + 31) / 32) * 32; // padded record bytes
+		const size_t n = (size_t)std::max(c->m.E, 1) * c->n * rec;
+		PFG_CUDA(c, cudaMalloc(&c->d_hess_stage[k], n));
+	}
+	return PFG_OK;
+}
+
 // Stage a host input vector of 3N doubles into `dst`; device inputs are used in place.
 int stage_in(pfg_context *c, const double *src, int mem, double *dst, size_t n, const double **use)
 {
@@ -148,21 +184,13 @@ int finish_host(pfg_context *c, double *host_dst, const double *dev_src, size_t 
 }
 
 // Host build of the CSC pattern (Eigen ColMajor semantics: per column the sorted
-// unique rows touched by any element) and the element node-pair slot map.
+// unique rows touched by any element) and the node-owner assembly plans.
 int build_pattern(pfg_context *c)
 {
 	const int E = c->m.E, N = c->m.N, n = c->n;
 	const int *conn = c->h_conn.data();
-	// node -> element incidence
-	std::vector<long long> ioff(N + 1, 0);
-	for (long long i = 0; i < (long long)E * n; ++i) ioff[conn[i] + 1]++;
-	for (int i = 0; i < N; ++i) ioff[i + 1] += ioff[i];
-	std::vector<int> inc(ioff[N]);
-	{
-		std::vector<long long> pos(ioff.begin(), ioff.end() - 1);
-		for (int e = 0; e < E; ++e)
-			for (int a = 0; a < n; ++a) inc[pos[conn[(size_t)e * n + a]]++] = e;
-	}
+	const std::vector<long long> &ioff = c->h_inc_off;
+	const std::vector<int> &inc = c->h_inc_e;
 	// neighbours of every node, sorted and unique, built in parallel node ranges
 	std::vector<int> deg(N, 0);
 	const int nt_max = 64;
@@ -199,6 +227,9 @@ int build_pattern(pfg_context *c)
 
 	const long long nnz = 9 * noff[N];
 	if (nnz > 0x7fffffffLL) return fail(c, PFG_ERR_UNSUPPORTED, "Hessian has more than 2^31-1 nonzeros (int32 CSC)");
+	int max_deg = 0;
+	for (int B = 0; B < N; ++B) max_deg = std::max(max_deg, deg[B]);
+	if (max_deg > 65535) return fail(c, PFG_ERR_UNSUPPORTED, "a node has more than 65535 neighbours");
 	const int ndof = 3 * N;
 	std::vector<int> outer(ndof + 1);
 	{
@@ -220,44 +251,67 @@ int build_pattern(pfg_context *c)
 					for (int m = 0; m < 3; ++m) inner[o++] = 3 * nbr[k] + m;
 			}
 	});
-	std::vector<int> slot((size_t)E * n * n);
-	parallel_ranges(E, [&](long long s, long long e, int) {
-		for (long long el = s; el < e; ++el)
-			for (int a = 0; a < n; ++a)
-				for (int b = 0; b < n; ++b)
-				{
-					const int A = conn[el * n + a], B = conn[el * n + b];
-					const int *lo = nbr.data() + noff[B], *hi = nbr.data() + noff[B + 1];
-					const int rank = (int)(std::lower_bound(lo, hi, A) - lo);
-					slot[(size_t)el * n * n + a * n + b] = outer[3 * B] + 3 * rank;
-				}
+	// row rank of every (incidence, local row node)
+	const long long nstrip = ioff[N];
+	std::vector<unsigned short> strip_rank((size_t)nstrip * n);
+	parallel_ranges(N, [&](long long s0, long long s1, int) {
+		for (long long B = s0; B < s1; ++B)
+		{
+			const int *lo = nbr.data() + noff[B], *hi = nbr.data() + noff[B + 1];
+			for (long long k = ioff[B]; k < ioff[B + 1]; ++k)
+			{
+				const int *ce = conn + (size_t)inc[k] * n;
+				for (int a = 0; a < n; ++a)
+					strip_rank[(size_t)k * n + a] = (unsigned short)(std::lower_bound(lo, hi, ce[a]) - lo);
+			}
+		}
 	});
-	std::vector<int> colstride(N);
-	for (int B = 0; B < N; ++B) colstride[B] = 3 * deg[B];
 
 	PFG_CUDA(c, cudaMalloc(&c->d_outer, sizeof(int) * (ndof + 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_inner, sizeof(int) * std::max<long long>(nnz, 1)));
-	PFG_CUDA(c, cudaMalloc(&c->d_slot, sizeof(int) * std::max<size_t>(slot.size(), 1)));
-	PFG_CUDA(c, cudaMalloc(&c->d_colstride, sizeof(int) * std::max(N, 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_values, sizeof(double) * std::max<long long>(nnz, 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_strip_rank, sizeof(unsigned short) * std::max<size_t>(strip_rank.size(), 1)));
 	PFG_CUDA(c, cudaMemcpy(c->d_outer, outer.data(), sizeof(int) * (ndof + 1), cudaMemcpyHostToDevice));
 	if (nnz) PFG_CUDA(c, cudaMemcpy(c->d_inner, inner.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice));
-	if (!slot.empty()) PFG_CUDA(c, cudaMemcpy(c->d_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice));
-	if (N) PFG_CUDA(c, cudaMemcpy(c->d_colstride, colstride.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+	if (!strip_rank.empty())
+		PFG_CUDA(c, cudaMemcpy(c->d_strip_rank, strip_rank.data(), sizeof(unsigned short) * strip_rank.size(),
+							   cudaMemcpyHostToDevice));
+	if ((size_t)8 * 9 * max_deg * sizeof(double) > 200 * 1024)
+		return fail(c, PFG_ERR_UNSUPPORTED, "a node has too many neighbours for the shared-memory column assembly");
 	c->pat.nnz = nnz;
+	c->pat.max_deg = max_deg;
 	c->pat.outer = c->d_outer;
 	c->pat.inner = c->d_inner;
-	c->pat.slot = c->d_slot;
-	c->pat.colstride = c->d_colstride;
+	c->pat.strip_rank = c->d_strip_rank;
 	c->pat.values = c->d_values;
 	c->has_pattern = true;
 	return PFG_OK;
 }
 
+// node -> incidence lists (grouped by node, elements ascending) of a connectivity
+void build_incidence(const int *conn, int E, int n, int N, std::vector<long long> &off, std::vector<int> &elem,
+					 std::vector<int> &eb)
+{
+	off.assign(N + 1, 0);
+	for (long long i = 0; i < (long long)E * n; ++i) off[conn[i] + 1]++;
+	for (int i = 0; i < N; ++i) off[i + 1] += off[i];
+	elem.assign(off[N], 0);
+	eb.assign(off[N], 0);
+	std::vector<long long> pos(off.begin(), off.end() - 1);
+	for (int e = 0; e < E; ++e)
+		for (int a = 0; a < n; ++a)
+		{
+			const long long k = pos[conn[(size_t)e * n + a]]++;
+			elem[k] = e;
+			eb[k] = e * n + a;
+		}
+}
+
 void free_all(pfg_context *c)
 {
-	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_slot, c->d_colstride,
-					c->d_values, c->sc.partials, c->sc.ticket, c->sc.inverted, c->d_result, c->d_u, c->d_p, c->d_out};
+	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_strip_rank, c->d_eb_inc,
+					c->d_inc_off, c->d_inc_eb, c->d_ginc_off, c->d_ginc_eb, c->d_vec_stage, c->d_hess_stage[0],
+					c->d_hess_stage[1], c->sc.partials, c->sc.ticket, c->sc.inverted, c->d_result, c->d_u, c->d_p, c->d_out};
 	for (void *p : ptrs)
 		if (p) cudaFree(p);
 }
@@ -357,6 +411,32 @@ int pfg_create(const pfg_mesh_desc *d, pfg_context **out)
 		CREATE_CUDA(cudaMalloc(&c->d_lame, sizeof(double2) * lm.size()));
 		CREATE_CUDA(cudaMemcpy(c->d_lame, lm.data(), sizeof(double2) * lm.size(), cudaMemcpyHostToDevice));
 	}
+	// node -> incidence lists for the deterministic per-node sums
+	if ((long long)E * n > 0x7fffffffLL) return bail(fail(c, PFG_ERR_UNSUPPORTED, "E * n exceeds 2^31-1"));
+	{
+		std::vector<int> eb;
+		build_incidence(d->conn, (int)E, n, d->n_nodes, c->h_inc_off, c->h_inc_e, eb);
+		std::vector<int> off32(c->h_inc_off.begin(), c->h_inc_off.end());
+		CREATE_CUDA(cudaMalloc(&c->d_inc_off, sizeof(int) * off32.size()));
+		CREATE_CUDA(cudaMalloc(&c->d_inc_eb, sizeof(int) * std::max<size_t>(eb.size(), 1)));
+		CREATE_CUDA(cudaMemcpy(c->d_inc_off, off32.data(), sizeof(int) * off32.size(), cudaMemcpyHostToDevice));
+		if (!eb.empty()) CREATE_CUDA(cudaMemcpy(c->d_inc_eb, eb.data(), sizeof(int) * eb.size(), cudaMemcpyHostToDevice));
+		std::vector<int> inv(eb.size());
+		for (size_t k = 0; k < eb.size(); ++k) inv[eb[k]] = (int)k;
+		CREATE_CUDA(cudaMalloc(&c->d_eb_inc, sizeof(int) * std::max<size_t>(inv.size(), 1)));
+		if (!inv.empty()) CREATE_CUDA(cudaMemcpy(c->d_eb_inc, inv.data(), sizeof(int) * inv.size(), cudaMemcpyHostToDevice));
+		if (d->gconn && (d->gconn != d->conn || ng != n))
+		{
+			std::vector<long long> goff;
+			std::vector<int> gelem, geb;
+			build_incidence(gconn, (int)E, ng, d->n_geom_nodes, goff, gelem, geb);
+			std::vector<int> goff32(goff.begin(), goff.end());
+			CREATE_CUDA(cudaMalloc(&c->d_ginc_off, sizeof(int) * goff32.size()));
+			CREATE_CUDA(cudaMalloc(&c->d_ginc_eb, sizeof(int) * std::max<size_t>(geb.size(), 1)));
+			CREATE_CUDA(cudaMemcpy(c->d_ginc_off, goff32.data(), sizeof(int) * goff32.size(), cudaMemcpyHostToDevice));
+			if (!geb.empty()) CREATE_CUDA(cudaMemcpy(c->d_ginc_eb, geb.data(), sizeof(int) * geb.size(), cudaMemcpyHostToDevice));
+		}
+	}
 	c->sc.max_blocks = (int)(E / 128 + 2);
 	CREATE_CUDA(cudaMalloc(&c->sc.partials, sizeof(double) * c->sc.max_blocks));
 	CREATE_CUDA(cudaMalloc(&c->sc.ticket, sizeof(unsigned int)));
@@ -368,6 +448,11 @@ int pfg_create(const pfg_mesh_desc *d, pfg_context **out)
 #undef CREATE_CUDA
 	c->m.conn = c->d_conn;
 	c->m.gconn = c->d_gconn ? c->d_gconn : c->d_conn;
+	c->m.inc_off = c->d_inc_off;
+	c->m.inc_eb = c->d_inc_eb;
+	c->m.eb_inc = c->d_eb_inc;
+	c->m.ginc_off = c->d_ginc_off ? c->d_ginc_off : c->d_inc_off;
+	c->m.ginc_eb = c->d_ginc_eb ? c->d_ginc_eb : c->d_inc_eb;
 	c->m.X = c->d_X;
 	c->m.lame = c->d_lame;
 	*out = c;
@@ -473,6 +558,7 @@ int pfg_gradient(pfg_context *c, const double *u, int mem, int prec, double *gou
 	if ((st = stage_in(c, u, mem, c->d_u, ndof, &du))) return st;
 	PFG_CUDA(c, cudaMemsetAsync(c->sc.inverted, 0, sizeof(unsigned long long), c->stream));
 	double *dst = mem == PFG_MEM_DEVICE ? gout : c->d_out;
+	if ((st = ensure_vec_stage(c))) return st;
 	PFG_CUDA(c, launch_gradient(c->m, du, prec, dst, c->sc, c->stream));
 	if (mem == PFG_MEM_HOST) return finish_host(c, gout, c->d_out, ndof);
 	return PFG_OK;
@@ -514,7 +600,8 @@ int pfg_hessian(pfg_context *c, const double *u, int mem, int prec, int project_
 	if ((st = ensure_staging(c, 1))) return st;
 	const double *du;
 	if ((st = stage_in(c, u, mem, c->d_u, 3 * (size_t)c->m.N, &du))) return st;
-	PFG_CUDA(c, launch_hessian(c->m, c->pat, du, prec, c->stream));
+	if ((st = ensure_hess_stage(c, prec))) return st;
+	PFG_CUDA(c, launch_hessian(c->m, c->pat, du, prec, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
 	if (values)
 	{
 		if (mem == PFG_MEM_HOST) return finish_host(c, values, c->d_values, c->pat.nnz);
@@ -564,7 +651,8 @@ int pfg_shape_vjp(pfg_context *c, const double *u, const double *p, int mem, int
 	if ((st = stage_in(c, u, mem, c->d_u, ndof, &du))) return st;
 	if ((st = stage_in(c, p, mem, c->d_p, ndof, &dp))) return st;
 	double *dst = mem == PFG_MEM_DEVICE ? out : c->d_out;
-	PFG_CUDA(c, launch_shape_vjp(c->m, du, dp, prec, dst, c->stream));
+	if ((st = ensure_vec_stage(c))) return st;
+	PFG_CUDA(c, launch_shape_vjp(c->m, du, dp, prec, dst, c->sc, c->stream));
 	if (mem == PFG_MEM_HOST) return finish_host(c, out, c->d_out, 3 * (size_t)c->m.Ng);
 	return PFG_OK;
 }

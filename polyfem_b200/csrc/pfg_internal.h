@@ -9,10 +9,15 @@ namespace pfg
 {
 
 // Device-resident mesh in the layout the kernels read.
-//  conn  : [n][E] int32 (structure of arrays: local node a of all elements is contiguous)
-//  gconn : [n_g][E] int32 (aliases conn for isoparametric elements)
-//  X     : [N_g][3] float64 rest positions
-//  lame  : [E] (lambda, mu) float64 pairs
+//  conn     : [n][E] int32 (structure of arrays: local node a of all elements is contiguous)
+//  gconn    : [n_g][E] int32 (aliases conn for isoparametric elements)
+//  X        : [N_g][3] float64 rest positions
+//  lame     : [E] (lambda, mu) float64 pairs
+//  inc_off  : [N+1] offsets of each FE node's incidences ("strips") in inc_eb
+//  inc_eb   : [E*n] e*n + b for every incidence (element e holds the node at local b),
+//             grouped by node, elements ascending
+//  eb_inc   : [E*n] the incidence index of (e, b), i.e. the inverse permutation of inc_eb
+//  ginc_off / ginc_eb : the same for the geometric nodes (alias inc_* when isoparametric)
 struct DevMesh
 {
 	int et = 0, E = 0, N = 0, Ng = 0;
@@ -20,21 +25,26 @@ struct DevMesh
 	const int *gconn = nullptr;
 	const double *X = nullptr;
 	const double2 *lame = nullptr;
+	const int *inc_off = nullptr;
+	const int *inc_eb = nullptr;
+	const int *eb_inc = nullptr; // [E*n] inverse of inc_eb: incidence index of (e, b)
+	const int *ginc_off = nullptr;
+	const int *ginc_eb = nullptr;
 };
 
-// Device-resident Hessian pattern.
-//  outer/inner : CSC arrays (3N+1 / nnz)
-//  slot        : [E][n*n] int32, CSC index of entry (3A, 3B) for the node pair
-//                (A = conn[e][a], B = conn[e][b]); entry (3A+m, 3B+c) is at
-//                slot + c*colstride[B] + m
-//  colstride   : [N] int32, 3*deg(B) = length of each of node B's three columns
+// Device-resident Hessian pattern (Eigen ColMajor CSC, int32 indices) and the
+// row rank of every (incidence, local row node): entry (3A+r, 3B+c) of an element
+// holding B at local b and A at local a lives at
+//   outer[3B] + c*(outer[3B+1]-outer[3B]) + 3*strip_rank[s*n + a] + r,
+// s being the incidence's index in inc_eb.
 struct DevPattern
 {
 	long long nnz = 0;
+	int max_deg = 0; // largest number of neighbour nodes of a node
+
 	const int *outer = nullptr;
 	const int *inner = nullptr;
-	const int *slot = nullptr;
-	const int *colstride = nullptr;
+	const unsigned short *strip_rank = nullptr;
 	double *values = nullptr;
 };
 
@@ -44,6 +54,8 @@ struct Scratch
 	unsigned int *ticket = nullptr;   // last-block-done counter (returns to 0 after each launch)
 	unsigned long long *inverted = nullptr;
 	int max_blocks = 0;
+	double *vec_stage = nullptr;      // [E][max(n, n_g)][3] element gradient / shape contributions
+	void *hess_stage = nullptr;       // one padded record of 9n block values per incidence (FP64 or FP32)
 };
 
 constexpr int PREC_FP64 = 0;
@@ -55,10 +67,11 @@ cudaError_t launch_energy(const DevMesh &m, const double *u, int prec, bool per_
 						  const Scratch &sc, cudaStream_t s);
 cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double *g, const Scratch &sc,
 							cudaStream_t s);
-cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, cudaStream_t s);
+// vec_stage must hold E*max(n, n_g)*3 doubles
+cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, void *stage, cudaStream_t s);
 cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double *adj, double *out, cudaStream_t s);
 cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out,
-							 cudaStream_t s);
+							 const Scratch &sc, cudaStream_t s);
 cudaError_t hessian_kernel_setup(int device);
 
 // Sets the message pfg_last_error(NULL) returns on this host thread.

@@ -15,6 +15,7 @@
 #include "pfg_internal.h"
 
 #include <cstdio>
+#include <cstdlib>
 
 namespace pfg
 {
@@ -265,7 +266,7 @@ __global__ void __launch_bounds__(NT) k_energy_per_element(DevMesh m, const doub
 // gradient (NLAssembler::assemble_gradient)
 // ---------------------------------------------------------------------------
 template <class EL, class T, int NT>
-__global__ void __launch_bounds__(NT) k_gradient(DevMesh m, const double *__restrict__ u, double *__restrict__ g,
+__global__ void __launch_bounds__(NT) k_gradient(DevMesh m, const double *__restrict__ u, double *__restrict__ stage,
 												 unsigned long long *inverted)
 {
 	const int e = blockIdx.x * NT + threadIdx.x;
@@ -355,102 +356,201 @@ __global__ void __launch_bounds__(NT) k_gradient(DevMesh m, const double *__rest
 			}
 	}
 	if (bad) atomicAdd(inverted, 1ull);
+	// the element's contributions, contiguous: stage[e][a][d]
+	double *dst = stage + (size_t)e * EL::N * 3;
 #pragma unroll
 	for (int a = 0; a < EL::N; ++a)
 #pragma unroll
-		for (int d = 0; d < 3; ++d) atomicAdd(g + (size_t)nodes[a] * 3 + d, double(Gacc[a][d]));
+		for (int d = 0; d < 3; ++d) dst[a * 3 + d] = double(Gacc[a][d]);
+}
+
+// Per node: the sum of its incidences' contributions in incidence (element) order
+// (NLAssembler::assemble_gradient's scatter, Assembler.cpp:613-629), one thread per
+// node; loads are issued eight incidences at a time.  Deterministic.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_vec_gather(int n_nodes, const int *__restrict__ off, const int *__restrict__ eb,
+												   const double *__restrict__ stage, double *__restrict__ out)
+{
+	constexpr int BATCH = 8;
+	const int B = blockIdx.x * NT + threadIdx.x;
+	if (B >= n_nodes) return;
+	const int k0 = __ldg(off + B), k1 = __ldg(off + B + 1);
+	double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+	for (int kb = k0; kb < k1; kb += BATCH)
+	{
+		int idx[BATCH];
+#pragma unroll
+		for (int j = 0; j < BATCH; ++j) idx[j] = (kb + j < k1) ? __ldg(eb + kb + j) : -1;
+		double v[BATCH][3];
+#pragma unroll
+		for (int j = 0; j < BATCH; ++j)
+		{
+			if (idx[j] >= 0)
+			{
+				const double *p = stage + (size_t)idx[j] * 3;
+				v[j][0] = __ldg(p);
+				v[j][1] = __ldg(p + 1);
+				v[j][2] = __ldg(p + 2);
+			}
+		}
+#pragma unroll
+		for (int j = 0; j < BATCH; ++j)
+			if (idx[j] >= 0)
+			{
+				t0 += v[j][0];
+				t1 += v[j][1];
+				t2 += v[j][2];
+			}
+	}
+	out[(size_t)B * 3 + 0] = t0;
+	out[(size_t)B * 3 + 1] = t1;
+	out[(size_t)B * 3 + 2] = t2;
 }
 
 // ---------------------------------------------------------------------------
-// Hessian (NLAssembler::assemble_hessian + SparseMatrixCache slot adds)
+// Hessian (NLAssembler::assemble_hessian + SparseMatrixCache)
+//
+// Element block.  With g_a = grad(phi_a), d_a = F^-T g_a and the identity
+// F (g_a x g_b) = (cof F g_a) x (cof F g_b) / J (cof cof F = J F), the
+// reference's B^T C B (NeoHookeanElasticity.cpp:636-656) reduces exactly to
+//   H_ab = sum_q da [ mu (g_a.g_b) I + lambda d_a d_b^T + (mu - lambda ln J) d_b d_a^T ].
+//
+// Assembly in two passes, both without atomics:
+//  1. k_hessian_blocks: a tile of elements per CTA computes the symmetric node
+//     blocks once; for every incidence (e, b) the record of all blocks of column
+//     node b, [a][c][r] = H_e(3a+r, 3b+c), is written to the staging buffer at
+//     the incidence's position in node order (records padded to whole sectors).
+//  2. k_hessian_gather: one warp per column node B streams B's records -- one
+//     contiguous run, with their row ranks alongside -- adds them in incidence
+//     order into a shared-memory image of B's three CSC columns, and writes the
+//     columns once, coalesced.  Each CSC entry is summed in a fixed order: the
+//     result is deterministic.
 // ---------------------------------------------------------------------------
 template <class EL>
-struct HessTile
+struct OwnerKin
 {
-	static constexpr int TE = (EL::ET == 1) ? 32 : 8; // elements per tile
-	static constexpr int NT = 256;
-	static constexpr int N = EL::N, NQ = EL::NQ;
-	static constexpr int NP = N * (N + 1) / 2; // symmetric node pairs
-	static constexpr int NB = N * N;           // node blocks
+	// J^-T (9), F^-T (9), mu da, lambda da, (mu - lambda lnJ) da, then g_i (3), d_i (3) per local node
+	static constexpr int PER_Q = 21 + 6 * EL::N;
 };
 
+// reference gradient with run-time (q, a): evaluated from the compile-time table
 template <class EL, class T>
-struct HessSmem
+__device__ __forceinline__ T gtab_at(int q, int a, int r)
 {
-	using TL = HessTile<EL>;
-	T gphi[TL::TE][TL::NQ][TL::N][3]; // physical gradients
-	T cvec[TL::TE][TL::NQ][TL::N][3]; // cof(F) * gphi_a
-	T F[TL::TE][TL::NQ][9];
-	T sc[TL::TE][TL::NQ][3];          // mu*da, alpha*da, beta*da
-	T U[TL::TE][TL::N][3];
-	T H[TL::TE][TL::NB * 9];          // element Hessian, [a*N+b][c*3+m] = H_e(3a+m, 3b+c)
-	int slot[TL::TE][TL::NB];
-	int stride[TL::TE][TL::N];
-};
+	T out = T(0);
+#pragma unroll
+	for (int qq = 0; qq < EL::NQ; ++qq)
+#pragma unroll
+		for (int aa = 0; aa < EL::N; ++aa)
+#pragma unroll
+			for (int rr = 0; rr < 3; ++rr)
+				if (qq == q && aa == a && rr == r) out = T(gref<EL>(qq, aa, rr));
+	return out;
+}
+
+// Record of one incidence (e, b): the 9n values H_e(3a+r, 3b+c), [a][c][r], padded to
+// whole 32-byte sectors so that records written at scattered positions stay full-sector.
+template <class EL, class T>
+__host__ __device__ constexpr int rec_pad()
+{
+	return (((9 * EL::N * (int)sizeof(T)) + 31) / 32) * 32 / (int)sizeof(T);
+}
 
 template <class EL, class T>
-__global__ void __launch_bounds__(HessTile<EL>::NT) k_hessian(DevMesh m, DevPattern pat, const double *__restrict__ u)
+struct EcTile
 {
-	using TL = HessTile<EL>;
-	constexpr int TE = TL::TE, NT = TL::NT, N = TL::N, NQ = TL::NQ, NP = TL::NP, NB = TL::NB;
+	static constexpr int TE = (EL::ET == 1) ? 64 : (EL::ET == 2 ? 16 : 8);
+	static constexpr int NT = 128;
+	static constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ;
+	static constexpr int NP = N * (N + 1) / 2, NB = N * N, PQ = OwnerKin<EL>::PER_Q;
+};
+
+// K: arithmetic of the kinematics (J^-T, F^-T, g, d); T: arithmetic of the contraction and records
+template <class EL, class K, class T>
+struct EcSmem
+{
+	using TL = EcTile<EL, T>;
+	K U[TL::TE][TL::N][3];
+	K X[TL::TE][TL::NG][3];
+	K kin[TL::TE][TL::NQ][TL::PQ];
+	T rec[TL::NT / 32][TL::NB * 9]; // one element's blocks per warp, then copied out per incidence
+	int nodes[TL::TE][TL::N + TL::NG];
+	int sidx[TL::NT / 32][TL::N];   // incidence index of (e, b) for the warp's element
+};
+
+template <class EL, class K, class T>
+__global__ void __launch_bounds__(128, 4) k_hessian_blocks(DevMesh m, const double *__restrict__ u, T *__restrict__ stage)
+{
+	using TL = EcTile<EL, T>;
+	constexpr int TE = TL::TE, NT = TL::NT, N = TL::N, NG = TL::NG, NQ = TL::NQ, NP = TL::NP, NB = TL::NB;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
-	HessSmem<EL, T> &S = *reinterpret_cast<HessSmem<EL, T> *>(smem_raw);
+	EcSmem<EL, K, T> &S = *reinterpret_cast<EcSmem<EL, K, T> *>(smem_raw);
 	const int tid = threadIdx.x;
 	const int e0 = blockIdx.x * TE;
+	const int ne = min(TE, m.E - e0);
 
-	// phase 0: slots, column strides and nodal displacements of the tile
-	for (int i = tid; i < TE * NB; i += NT)
+	// phase 0: node ids (coalesced over the tile), then the gathers
+	for (int i = tid; i < TE * (N + NG); i += NT)
 	{
-		const int el = i / NB, e = e0 + el;
-		S.slot[el][i % NB] = (e < m.E) ? __ldg(pat.slot + (size_t)e0 * NB + i) : 0;
+		const int j = i / TE, el = i % TE, e = e0 + el;
+		int v = 0;
+		if (el < ne) v = (j < N) ? __ldg(m.conn + (size_t)j * m.E + e) : __ldg(m.gconn + (size_t)(j - N) * m.E + e);
+		S.nodes[el][j] = v;
 	}
+	__syncthreads();
 	for (int i = tid; i < TE * N * 3; i += NT)
 	{
-		const int el = i / (N * 3), r = i % (N * 3), a = r / 3, d = r % 3, e = e0 + el;
-		if (e < m.E)
-		{
-			const int node = __ldg(m.conn + (size_t)a * m.E + e);
-			S.U[el][a][d] = T(__ldg(u + (size_t)node * 3 + d));
-			if (d == 0) S.stride[el][a] = __ldg(pat.colstride + node);
-		}
-		else
-		{
-			S.U[el][a][d] = T(0);
-			if (d == 0) S.stride[el][a] = 0;
-		}
+		const int el = i / (N * 3), a = (i / 3) % N, d = i % 3;
+		S.U[el][a][d] = (el < ne) ? K(__ldg(u + (size_t)S.nodes[el][a] * 3 + d)) : K(0);
+	}
+	for (int i = tid; i < TE * NG * 3; i += NT)
+	{
+		const int el = i / (NG * 3), j = (i / 3) % NG, d = i % 3;
+		S.X[el][j][d] = (el < ne) ? K(__ldg(m.X + (size_t)S.nodes[el][N + j] * 3 + d)) : K(0);
 	}
 	__syncthreads();
 
-	// phase 1: per (element, quadrature point) kinematics
-	for (int i = tid; i < TE * NQ; i += NT)
+	// phase 1a: J^-T, F^-T and the weights of every (element, quadrature point)
+	for (int i = tid; i < ne * NQ; i += NT)
 	{
-		const int el = i / NQ, q = i % NQ, e = e0 + el;
-		if (e >= m.E) continue;
-		T Xg[EL::NG][3];
-		load_geom<EL, T>(m, e, Xg);
-		T Jit[3][3];
-		double detJ;
-		// the quadrature point index is a run-time value here; unrolled dispatch keeps tables constant
+		const int el = i / NQ, q = i % NQ;
+		const double2 lm = __ldg(m.lame + e0 + el);
+		K *Kq = S.kin[el][q];
 #pragma unroll
 		for (int qq = 0; qq < NQ; ++qq)
 		{
 			if (qq != q) continue;
-			geometry<EL, T>(qq, Xg, Jit, detJ);
-			T gphi[N][3];
-			phys_grads<EL, T>(qq, Jit, gphi);
-			T F[3][3];
-			{
-				T U[N][3];
+			K Xg[NG][3];
 #pragma unroll
-				for (int a = 0; a < N; ++a)
+			for (int j = 0; j < NG; ++j)
 #pragma unroll
-					for (int d = 0; d < 3; ++d) U[a][d] = S.U[el][a][d];
-				disp_grad<EL, T>(U, gphi, F);
-			}
+				for (int d = 0; d < 3; ++d) Xg[j][d] = S.X[el][j][d];
+			K Jit[3][3];
+			double detJ;
+			geometry<EL, K>(qq, Xg, Jit, detJ);
+			K Ar[3][3];
 #pragma unroll
-			for (int r = 0; r < 3; ++r) F[r][r] += T(1);
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+				{
+					K s_ = K(0);
+#pragma unroll
+					for (int a = 0; a < N; ++a)
+					{
+						const double gr = gref<EL>(qq, a, c);
+						if (gr != 0.0) s_ += S.U[el][a][r] * K(gr);
+					}
+					Ar[r][c] = s_;
+				}
+			K F[3][3];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+					F[r][c] = Ar[r][0] * Jit[0][c] + Ar[r][1] * Jit[1][c] + Ar[r][2] * Jit[2][c] + (r == c ? K(1) : K(0));
 			double J;
-			if constexpr (sizeof(T) == 8)
+			if constexpr (sizeof(K) == 8)
 				J = det3(F);
 			else
 			{
@@ -462,100 +562,208 @@ __global__ void __launch_bounds__(HessTile<EL>::NT) k_hessian(DevMesh m, DevPatt
 				J = det3(Fd);
 			}
 			const double lj = log(J);
-			const double2 lm = __ldg(m.lame + e);
-			const double lambda = lm.x, mu = lm.y;
 			const double da = detJ * qweight<EL>(qq);
-			T D[3][3];
-			cofactor3(F, D);
-			S.sc[el][qq][0] = T(mu * da);
-			S.sc[el][qq][1] = T((mu + lambda * (1 - lj)) / (J * J) * da);
-			S.sc[el][qq][2] = T((lambda * lj - mu) / J * da);
+			K FmT[3][3];
+			inv_transpose3(F, K(J), FmT);
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
 #pragma unroll
-				for (int c = 0; c < 3; ++c) S.F[el][qq][r * 3 + c] = F[r][c];
-#pragma unroll
-			for (int a = 0; a < N; ++a)
-#pragma unroll
 				for (int c = 0; c < 3; ++c)
 				{
-					S.gphi[el][qq][a][c] = gphi[a][c];
-					S.cvec[el][qq][a][c] = D[c][0] * gphi[a][0] + D[c][1] * gphi[a][1] + D[c][2] * gphi[a][2];
+					Kq[r * 3 + c] = Jit[r][c];
+					Kq[9 + r * 3 + c] = FmT[r][c];
 				}
+			Kq[18] = K(lm.y * da);
+			Kq[19] = K(lm.x * da);
+			Kq[20] = K((lm.y - lm.x * lj) * da);
 		}
 	}
 	__syncthreads();
-
-	// phase 2: symmetric node pairs
-	for (int i = tid; i < TE * NP; i += NT)
+	// phase 1b: g_i and d_i of every (element, point, node)
+	for (int i = tid; i < ne * NQ * N; i += NT)
 	{
-		const int el = i / NP;
-		int p = i % NP, a = 0;
-		while (p >= N - a)
-		{
-			p -= N - a;
-			++a;
-		}
-		const int b = a + p;
-		T h[3][3];
+		const int el = i / (NQ * N), q = (i / N) % NQ, a = i % N;
+		K *Kq = S.kin[el][q];
+		const K g0 = gtab_at<EL, K>(q, a, 0), g1 = gtab_at<EL, K>(q, a, 1), g2 = gtab_at<EL, K>(q, a, 2);
+		K g[3];
 #pragma unroll
-		for (int r = 0; r < 3; ++r) h[r][0] = h[r][1] = h[r][2] = T(0);
-		if (e0 + el < m.E)
+		for (int c = 0; c < 3; ++c) g[c] = g0 * Kq[c] + g1 * Kq[3 + c] + g2 * Kq[6 + c];
+		K *dst = Kq + 21 + 6 * a;
+		dst[0] = g[0];
+		dst[1] = g[1];
+		dst[2] = g[2];
+#pragma unroll
+		for (int r = 0; r < 3; ++r) dst[3 + r] = Kq[9 + r * 3] * g[0] + Kq[9 + r * 3 + 1] * g[1] + Kq[9 + r * 3 + 2] * g[2];
+	}
+	__syncthreads();
+
+	// phase 2: each warp takes whole elements: symmetric node pairs into the warp's
+	// record buffer (H_ba = H_ab^T alongside), then the element's n x n blocks are
+	// written out as one contiguous run, b-major: stage[e][b][a][c][r] = H_e(3a+r, 3b+c)
+	const int warp = tid >> 5, lane = tid & 31;
+	T *R = S.rec[warp];
+	for (int el = warp; el < ne; el += NT / 32)
+	{
+		for (int p0 = lane; p0 < NP; p0 += 32)
 		{
+			int p = p0, a = 0;
+			while (p >= N - a)
+			{
+				p -= N - a;
+				++a;
+			}
+			const int b = a + p;
+			T h[3][3];
+#pragma unroll
+			for (int r = 0; r < 3; ++r) h[r][0] = h[r][1] = h[r][2] = T(0);
 #pragma unroll
 			for (int q = 0; q < NQ; ++q)
 			{
-				const T *ga = S.gphi[el][q][a], *gb = S.gphi[el][q][b];
-				const T *ca = S.cvec[el][q][a], *cb = S.cvec[el][q][b];
-				const T *F = S.F[el][q];
-				const T smu = S.sc[el][q][0], sal = S.sc[el][q][1], sbe = S.sc[el][q][2];
-				const T dot = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
-				const T x0 = ga[1] * gb[2] - ga[2] * gb[1];
-				const T x1 = ga[2] * gb[0] - ga[0] * gb[2];
-				const T x2 = ga[0] * gb[1] - ga[1] * gb[0];
-				const T w0 = (F[0] * x0 + F[1] * x1 + F[2] * x2) * sbe;
-				const T w1 = (F[3] * x0 + F[4] * x1 + F[5] * x2) * sbe;
-				const T w2 = (F[6] * x0 + F[7] * x1 + F[8] * x2) * sbe;
-				const T md = smu * dot;
+				const K *Kq = S.kin[el][q];
+				const K *Ka = Kq + 21 + 6 * a, *Kb = Kq + 21 + 6 * b;
+				const T md = T(Kq[18]) * (T(Ka[0]) * T(Kb[0]) + T(Ka[1]) * T(Kb[1]) + T(Ka[2]) * T(Kb[2]));
+				const T sla = T(Kq[19]), sga = T(Kq[20]);
+				const T la[3] = {sla * T(Ka[3]), sla * T(Ka[4]), sla * T(Ka[5])};
+				const T gma[3] = {sga * T(Ka[3]), sga * T(Ka[4]), sga * T(Ka[5])};
+				const T db[3] = {T(Kb[3]), T(Kb[4]), T(Kb[5])};
 #pragma unroll
 				for (int r = 0; r < 3; ++r)
 #pragma unroll
-					for (int c = 0; c < 3; ++c) h[r][c] += sal * ca[r] * cb[c];
+					for (int c = 0; c < 3; ++c) h[r][c] += la[r] * db[c] + db[r] * gma[c];
 				h[0][0] += md;
 				h[1][1] += md;
 				h[2][2] += md;
-				// + beta * eps_{mnp} w_p
-				h[0][1] += w2;
-				h[1][0] -= w2;
-				h[1][2] += w0;
-				h[2][1] -= w0;
-				h[2][0] += w1;
-				h[0][2] -= w1;
+			}
+			T *Hab = R + (b * N + a) * 9; // block (a, b): record of column node b
+			T *Hba = R + (a * N + b) * 9; // block (b, a): record of column node a
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+				{
+					Hab[c * 3 + r] = h[r][c];
+					if (a != b) Hba[r * 3 + c] = h[r][c];
+				}
+		}
+		if (lane < N) S.sidx[warp][lane] = __ldg(m.eb_inc + (size_t)(e0 + el) * N + lane);
+		__syncwarp();
+		// record of (e, b) goes to the incidence's position in node order
+		constexpr int RP = rec_pad<EL, T>();
+		for (int i = lane; i < NB * 9; i += 32)
+		{
+			const int b = i / (9 * N), k = i % (9 * N);
+			stage[(size_t)S.sidx[warp][b] * RP + k] = R[i];
+		}
+		__syncwarp();
+	}
+}
+
+// One warp per column node B: stream B's records (contiguous in node order) into a
+// shared image of its three CSC columns, PF records in flight at a time.
+template <class EL, class T, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 3) k_hessian_gather(DevMesh m, DevPattern pat, const T *__restrict__ stage)
+{
+	constexpr int N = EL::N, REC = 9 * N, KPL = (REC + 31) / 32, PF = 4, RP = rec_pad<EL, T>();
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int B = blockIdx.x * WARPS + warp;
+	if (B >= m.N) return;
+	double *acc = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 9 * pat.max_deg;
+	const int o0 = __ldg(pat.outer + 3 * B);
+	const int stride = __ldg(pat.outer + 3 * B + 1) - o0; // 3 * deg(B)
+	const int len = 3 * stride;
+	for (int i = lane; i < len; i += 32) acc[i] = 0.0;
+	int slot[KPL];
+#pragma unroll
+	for (int k = 0; k < KPL; ++k)
+	{
+		const int idx = lane + 32 * k;
+		slot[k] = (idx < REC) ? ((idx % 9) / 3) * stride + idx % 3 : 0; // column c and row r of the entry
+	}
+	__syncwarp();
+	const int s0 = __ldg(m.inc_off + B), s1 = __ldg(m.inc_off + B + 1);
+	for (int sb = s0; sb < s1; sb += PF)
+	{
+		T v[PF][KPL];
+		int rk[PF][KPL];
+#pragma unroll
+		for (int j = 0; j < PF; ++j)
+		{
+			const int s = sb + j;
+			if (s < s1)
+			{
+				const T *rec = stage + (size_t)s * RP;
+#pragma unroll
+				for (int k = 0; k < KPL; ++k)
+				{
+					const int idx = lane + 32 * k;
+					if (idx < REC)
+					{
+						v[j][k] = __ldg(rec + idx);
+						rk[j][k] = __ldg(pat.strip_rank + (size_t)s * N + idx / 9);
+					}
+				}
 			}
 		}
-		T *Hab = S.H[el] + (a * N + b) * 9;
-		T *Hba = S.H[el] + (b * N + a) * 9;
 #pragma unroll
-		for (int r = 0; r < 3; ++r)
-#pragma unroll
-			for (int c = 0; c < 3; ++c)
+		for (int j = 0; j < PF; ++j)
+		{
+			if (sb + j < s1)
 			{
-				Hab[c * 3 + r] = h[r][c];
-				if (a != b) Hba[r * 3 + c] = h[r][c];
+#pragma unroll
+				for (int k = 0; k < KPL; ++k)
+					if (lane + 32 * k < REC) acc[slot[k] + 3 * rk[j][k]] += double(v[j][k]);
 			}
+			__syncwarp();
+		}
 	}
-	__syncthreads();
+	double *dst = pat.values + o0;
+	for (int i = lane; i < len; i += 32) dst[i] = acc[i];
+}
 
-	// phase 3: scatter through the slot map; consecutive threads hit consecutive rows
-	for (int i = tid; i < TE * NB * 9; i += NT)
+template <class EL, class K, class T>
+static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const double *u, void *stage_v, cudaStream_t s)
+{
+	using TL = EcTile<EL, T>;
+	T *stage = static_cast<T *>(stage_v);
+	const size_t bytes1 = sizeof(EcSmem<EL, K, T>);
+	cudaError_t e = cudaFuncSetAttribute(k_hessian_blocks<EL, K, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes1);
+	if (e != cudaSuccess) return e;
+	const int nb = (m.E + TL::TE - 1) / TL::TE;
+	if (nb > 0) k_hessian_blocks<EL, K, T><<<nb, TL::NT, bytes1, s>>>(m, u, stage);
+	constexpr int WARPS = 8;
+	const size_t bytes2 = (size_t)WARPS * 9 * p.max_deg * sizeof(double);
+	e = cudaFuncSetAttribute(k_hessian_gather<EL, T, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes2);
+	if (e != cudaSuccess) return e;
+	const int ng = (m.N + WARPS - 1) / WARPS;
+	if (ng > 0) k_hessian_gather<EL, T, WARPS><<<ng, WARPS * 32, bytes2, s>>>(m, p, stage);
+	return cudaGetLastError();
+}
+
+cudaError_t hessian_kernel_setup(int) { return cudaSuccess; }
+
+cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, void *stage, cudaStream_t s)
+{
+	if (p.nnz == 0) return cudaSuccess;
+	// FP64: everything in FP64.  FP32: everything in FP32 except det/log J.
+	// SPLIT32: kinematics (J^-T, F^-T, det/log J, g, d) in FP64, contraction and
+	// records in FP32, per-entry sums in FP64.
+	switch (m.et)
 	{
-		const int el = i / (NB * 9), r = i % (NB * 9);
-		if (e0 + el >= m.E) continue;
-		const int pair = r / 9, c = (r % 9) / 3, mrow = r % 3;
-		const int b = pair % N;
-		const long long idx = (long long)S.slot[el][pair] + (long long)c * S.stride[el][b] + mrow;
-		atomicAdd(pat.values + idx, double(S.H[el][r]));
+	case 1:
+		return prec == PREC_FP64 ? hessian_two_pass<P1Tet, double, double>(m, p, u, stage, s)
+			 : prec == PREC_FP32 ? hessian_two_pass<P1Tet, float, float>(m, p, u, stage, s)
+								 : hessian_two_pass<P1Tet, double, float>(m, p, u, stage, s);
+	case 2:
+		return prec == PREC_FP64 ? hessian_two_pass<P2Tet, double, double>(m, p, u, stage, s)
+			 : prec == PREC_FP32 ? hessian_two_pass<P2Tet, float, float>(m, p, u, stage, s)
+								 : hessian_two_pass<P2Tet, double, float>(m, p, u, stage, s);
+	case 3:
+		return prec == PREC_FP64 ? hessian_two_pass<Q1Hex, double, double>(m, p, u, stage, s)
+			 : prec == PREC_FP32 ? hessian_two_pass<Q1Hex, float, float>(m, p, u, stage, s)
+								 : hessian_two_pass<Q1Hex, double, float>(m, p, u, stage, s);
 	}
+	return cudaErrorInvalidValue;
 }
 
 // ---------------------------------------------------------------------------
@@ -619,7 +827,7 @@ __global__ void __launch_bounds__(NT) k_material_vjp(DevMesh m, const double *__
 // ---------------------------------------------------------------------------
 template <class EL, class T, int NT>
 __global__ void __launch_bounds__(NT) k_shape_vjp(DevMesh m, const double *__restrict__ u,
-												  const double *__restrict__ adj, double *__restrict__ out)
+												  const double *__restrict__ adj, double *__restrict__ stage)
 {
 	const int e = blockIdx.x * NT + threadIdx.x;
 	if (e >= m.E) return;
@@ -629,9 +837,6 @@ __global__ void __launch_bounds__(NT) k_shape_vjp(DevMesh m, const double *__res
 	load_geom<EL, T>(m, e, Xg);
 	load_nodal<EL, T>(m, e, u, U, nodes);
 	load_nodal<EL, T>(m, e, adj, Pn, nodes);
-	int gnodes[EL::NG];
-#pragma unroll
-	for (int j = 0; j < EL::NG; ++j) gnodes[j] = __ldg(m.gconn + (size_t)j * m.E + e);
 	const double2 lm = __ldg(m.lame + e);
 	const T lambda = T(lm.x), mu = T(lm.y);
 	T acc[EL::NG][3];
@@ -728,10 +933,11 @@ __global__ void __launch_bounds__(NT) k_shape_vjp(DevMesh m, const double *__res
 			}
 		}
 	}
+	double *dst = stage + (size_t)e * EL::NG * 3;
 #pragma unroll
 	for (int v = 0; v < EL::NG; ++v)
 #pragma unroll
-		for (int d = 0; d < 3; ++d) atomicAdd(out + (size_t)gnodes[v] * 3 + d, double(acc[v][d]));
+		for (int d = 0; d < 3; ++d) dst[v * 3 + d] = double(acc[v][d]);
 }
 
 // ---------------------------------------------------------------------------
@@ -767,65 +973,25 @@ cudaError_t launch_energy(const DevMesh &m, const double *u, int prec, bool per_
 }
 
 template <class EL, class T>
-static void gradient_t(const DevMesh &m, const double *u, double *g, const Scratch &sc, cudaStream_t s)
+static void gradient_t(const DevMesh &m, const double *u, const Scratch &sc, cudaStream_t s)
 {
 	constexpr int NT = 128;
-	k_gradient<EL, T, NT><<<blocks_for(m.E, NT), NT, 0, s>>>(m, u, g, sc.inverted);
+	k_gradient<EL, T, NT><<<blocks_for(m.E, NT), NT, 0, s>>>(m, u, sc.vec_stage, sc.inverted);
 }
 
 cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double *g, const Scratch &sc, cudaStream_t s)
 {
-	cudaError_t err = cudaMemsetAsync(g, 0, sizeof(double) * 3 * (size_t)m.N, s);
-	if (err != cudaSuccess || m.E == 0) return err;
+	if (m.E == 0) return cudaMemsetAsync(g, 0, sizeof(double) * 3 * (size_t)m.N, s);
 	const bool f32 = prec != PREC_FP64;
 	switch (m.et)
 	{
-	case 1: f32 ? gradient_t<P1Tet, float>(m, u, g, sc, s) : gradient_t<P1Tet, double>(m, u, g, sc, s); break;
-	case 2: f32 ? gradient_t<P2Tet, float>(m, u, g, sc, s) : gradient_t<P2Tet, double>(m, u, g, sc, s); break;
-	case 3: f32 ? gradient_t<Q1Hex, float>(m, u, g, sc, s) : gradient_t<Q1Hex, double>(m, u, g, sc, s); break;
+	case 1: f32 ? gradient_t<P1Tet, float>(m, u, sc, s) : gradient_t<P1Tet, double>(m, u, sc, s); break;
+	case 2: f32 ? gradient_t<P2Tet, float>(m, u, sc, s) : gradient_t<P2Tet, double>(m, u, sc, s); break;
+	case 3: f32 ? gradient_t<Q1Hex, float>(m, u, sc, s) : gradient_t<Q1Hex, double>(m, u, sc, s); break;
 	default: return cudaErrorInvalidValue;
 	}
-	return cudaGetLastError();
-}
-
-template <class EL, class T>
-static cudaError_t hess_attr()
-{
-	return cudaFuncSetAttribute(k_hessian<EL, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(HessSmem<EL, T>));
-}
-
-cudaError_t hessian_kernel_setup(int)
-{
-	cudaError_t e;
-	if ((e = hess_attr<P1Tet, double>()) != cudaSuccess) return e;
-	if ((e = hess_attr<P1Tet, float>()) != cudaSuccess) return e;
-	if ((e = hess_attr<P2Tet, double>()) != cudaSuccess) return e;
-	if ((e = hess_attr<P2Tet, float>()) != cudaSuccess) return e;
-	if ((e = hess_attr<Q1Hex, double>()) != cudaSuccess) return e;
-	if ((e = hess_attr<Q1Hex, float>()) != cudaSuccess) return e;
-	return cudaSuccess;
-}
-
-template <class EL, class T>
-static void hessian_t(const DevMesh &m, const DevPattern &p, const double *u, cudaStream_t s)
-{
-	using TL = HessTile<EL>;
-	const int nb = blocks_for(m.E, TL::TE);
-	k_hessian<EL, T><<<nb, TL::NT, sizeof(HessSmem<EL, T>), s>>>(m, p, u);
-}
-
-cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, cudaStream_t s)
-{
-	cudaError_t err = cudaMemsetAsync(p.values, 0, sizeof(double) * (size_t)p.nnz, s);
-	if (err != cudaSuccess || m.E == 0) return err;
-	const bool f32 = prec != PREC_FP64;
-	switch (m.et)
-	{
-	case 1: f32 ? hessian_t<P1Tet, float>(m, p, u, s) : hessian_t<P1Tet, double>(m, p, u, s); break;
-	case 2: f32 ? hessian_t<P2Tet, float>(m, p, u, s) : hessian_t<P2Tet, double>(m, p, u, s); break;
-	case 3: f32 ? hessian_t<Q1Hex, float>(m, p, u, s) : hessian_t<Q1Hex, double>(m, p, u, s); break;
-	default: return cudaErrorInvalidValue;
-	}
+	constexpr int NTG = 128;
+	if (m.N > 0) k_vec_gather<NTG><<<blocks_for(m.N, NTG), NTG, 0, s>>>(m.N, m.inc_off, m.inc_eb, sc.vec_stage, g);
 	return cudaGetLastError();
 }
 
@@ -844,20 +1010,23 @@ cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double 
 	return cudaGetLastError();
 }
 
-cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out, cudaStream_t s)
+cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out,
+							 const Scratch &sc, cudaStream_t s)
 {
-	cudaError_t err = cudaMemsetAsync(out, 0, sizeof(double) * 3 * (size_t)m.Ng, s);
-	if (err != cudaSuccess || m.E == 0) return err;
+	if (m.E == 0) return cudaMemsetAsync(out, 0, sizeof(double) * 3 * (size_t)m.Ng, s);
 	constexpr int NT = 128;
 	const int nb = blocks_for(m.E, NT);
 	const bool f32 = prec != PREC_FP64;
+	double *st = sc.vec_stage;
 	switch (m.et)
 	{
-	case 1: f32 ? k_shape_vjp<P1Tet, float, NT><<<nb, NT, 0, s>>>(m, u, adj, out) : k_shape_vjp<P1Tet, double, NT><<<nb, NT, 0, s>>>(m, u, adj, out); break;
-	case 2: f32 ? k_shape_vjp<P2Tet, float, NT><<<nb, NT, 0, s>>>(m, u, adj, out) : k_shape_vjp<P2Tet, double, NT><<<nb, NT, 0, s>>>(m, u, adj, out); break;
-	case 3: f32 ? k_shape_vjp<Q1Hex, float, NT><<<nb, NT, 0, s>>>(m, u, adj, out) : k_shape_vjp<Q1Hex, double, NT><<<nb, NT, 0, s>>>(m, u, adj, out); break;
+	case 1: f32 ? k_shape_vjp<P1Tet, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<P1Tet, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
+	case 2: f32 ? k_shape_vjp<P2Tet, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<P2Tet, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
+	case 3: f32 ? k_shape_vjp<Q1Hex, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<Q1Hex, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
 	default: return cudaErrorInvalidValue;
 	}
+	constexpr int NTG = 128;
+	if (m.Ng > 0) k_vec_gather<NTG><<<blocks_for(m.Ng, NTG), NTG, 0, s>>>(m.Ng, m.ginc_off, m.ginc_eb, st, out);
 	return cudaGetLastError();
 }
 
