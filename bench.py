@@ -5,7 +5,9 @@ Workload (the configuration the metric is quoted on): P2 tetrahedra on a 40^3 cu
 split 6 tets/hex (384,000 elements, 531,441 nodes, 1,594,323 dofs, 134,475,849
 CSC nonzeros), 4-point quadrature, per-element lognormal Lame parameters, seeded
 synthetic displacement u = 0.02 h N(0,1).  One step = one assembly of the global
-Hessian CSC values through the path's C ABI (pfg_hessian).
+Hessian CSC values through the path's C ABI (pfg_hessian), which launches two
+kernels: k_hessian_blocks (element blocks -> node-ordered records) and
+k_hessian_gather (records -> CSC columns).
 
   value     : split-precision Hessian assembly, inputs resident in HBM (elements/s)
   e2e       : the same call with host buffers (pinned u in, CSC values out) (elements/s)
@@ -14,6 +16,8 @@ Hessian CSC values through the path's C ABI (pfg_hessian).
               assembly (NLAssembler::assemble_hessian) on the host cores.
 
 Run:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+      python bench.py --grid G          (same line on a G^3 P2 cube: small profiling case)
+      python bench.py --suite           (per-operation timings on all five workloads)
 """
 from __future__ import annotations
 
@@ -31,11 +35,18 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-WORKLOAD = "P2 tet NeoHookean Hessian assembly, 40^3 cube x 6 tets (384,000 elements, 1,594,323 dofs)"
 METRIC = "NeoHookean elem Hessians/s on 1 B200: split-FP32 vs FP64, rel err vs FP64"
 UNIT = "elements/s"
-GRID = 40
 SEED_LAME, SEED_U = 5, 2
+PRECISION_NOTE = ("split32 = FP64 kinematics (J^-T, F, det/log J, F^-T, basis gradients) + FP32 "
+                  "block contraction and FP32 element records + FP64 per-entry sums and CSC values "
+                  "(CUDA cores)")
+
+
+def workload_name(grid: int) -> str:
+    E = 6 * grid ** 3
+    return (f"P2 tet NeoHookean Hessian assembly, {grid}^3 cube x 6 tets ({E:,} elements, "
+            f"{3 * (2 * grid + 1) ** 3:,} dofs), 4-pt quadrature, lognormal Lame")
 
 
 def _rank_info():
@@ -43,76 +54,128 @@ def _rank_info():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def _workload():
+def _workload(grid: int):
     from polyfem_b200 import mesh as M
-    mesh = M.structured_tet_mesh(GRID, 2)
+    mesh = M.structured_tet_mesh(grid, 2)
     lam, mu = M.lognormal_lame(mesh.n_elements, SEED_LAME)
     u = M.random_displacement(mesh, 0.02, SEED_U)
     return mesh, lam, mu, u
 
 
 def algorithmic_bytes(mesh, nnz: int) -> int:
-    """Bytes a Hessian assembly must move at least once (documented in DESIGN.md):
-    conn + gconn + Lame + X + u + slot map + column strides read, CSC values written."""
+    """Bytes a Hessian assembly must move at least once: conn + gconn + Lame + X + u
+    + node-block slot map (one int32 per element node pair) + column offsets read,
+    CSC values written."""
     E, n, ng = mesh.n_elements, mesh.conn.shape[1], mesh.gconn.shape[1]
     return (E * n * 4 + E * ng * 4 + E * 16 + mesh.n_geom_nodes * 24 + mesh.n_nodes * 24
             + E * n * n * 4 + mesh.n_nodes * 4 + nnz * 8)
 
 
+def staged_bytes(mesh, nnz: int, rec_bytes: int) -> int:
+    """HBM bytes the two-pass design moves when the records do not stay in L2:
+    algorithmic bytes + records written by pass 1 and read back by pass 2
+    (one padded record of 9n values per incidence) + the row ranks pass 2 reads."""
+    E, n = mesh.n_elements, mesh.conn.shape[1]
+    return algorithmic_bytes(mesh, nnz) + 2 * E * n * rec_bytes + E * n * n * 2
+
+
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
-    """Samples nvidia-smi during the timed region (clocks and throttle reasons)."""
+    """Samples SM clock and clock-event reasons through NVML every few ms while the
+    timed region runs (falls back to nvidia-smi at 100 ms when NVML is missing)."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event-reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_index: int, period_s: float = 0.005):
+        self.cuda_index = cuda_index
+        self.period = period_s
+        self.samples = []   # (sm_mhz, max_mhz, reasons bitmask)
+        self._stop = threading.Event()
+        self._thread = None
+        self._proc = None
+        self._lines = []
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            bus = torch.cuda.get_device_properties(self.cuda_index).pci_bus_id
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode() if isinstance(bus, str) else bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+            nv, hdl = self._nvml_handle()
+            reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            smax = nv.nvmlDeviceGetMaxClockInfo(hdl, nv.NVML_CLOCK_SM)
+
+            def loop():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append((nv.nvmlDeviceGetClockInfo(hdl, nv.NVML_CLOCK_SM), smax,
+                                             int(reasons_fn(hdl))))
+                    except Exception:
+                        pass
+                    time.sleep(self.period)
+
+            self.source = "nvml"
+            self._thread = threading.Thread(target=loop, daemon=True)
+            self._thread.start()
+            return
+        except Exception:
+            pass
+        try:
+            fields = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                      "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                      "clocks_event_reasons.sw_power_cap")
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.cuda_index}", f"--query-gpu={fields}",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
+            self._thread = threading.Thread(target=lambda: [self._lines.append(x.strip()) for x in self._proc.stdout],
+                                            daemon=True)
+            self._thread.start()
+            self.source = "nvidia-smi"
         except Exception:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.source = None
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 8:
-                continue
+        if self.source is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0}
+        self._stop.set()
+        if self._proc is not None:
+            time.sleep(0.2)
+            self._proc.terminate()
             try:
-                sm.append(float(parts[0]))
-                smax.append(float(parts[1]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[4:8]):
-                if val.lower() == "active":
-                    reasons.add(nm)
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+            bits = [0x8, 0x40, 0x20, 0x4]
+            for ln in self._lines:
+                p = [x.strip() for x in ln.split(",")]
+                if len(p) < 6:
+                    continue
+                try:
+                    mask = sum(b for b, v in zip(bits, p[2:6]) if v.lower() == "active")
+                    self.samples.append((float(p[0]), float(p[1]), mask))
+                except ValueError:
+                    continue
+        elif self._thread is not None:
+            self._thread.join(timeout=2)
+        sm = [s[0] for s in self.samples]
+        mask = 0
+        for s in self.samples:
+            mask |= s[2]
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "sm_max_mhz": max(s[1] for s in self.samples) if self.samples else None,
+                "reasons": sorted(name for bit, name in self.REASONS.items() if mask & bit),
+                "samples": len(sm), "source": self.source}
 
 
 # ----------------------------------------------------------------- CPU side
@@ -150,9 +213,8 @@ def run_reference(args):
     rank, world, _ = _rank_info()
     if rank != 0:
         return 0
-    mesh, lam, mu, u = _workload()
-    import psutil  # noqa: F401  (memory probe inside cpu_threads_for)
-    nnz = 134475849
+    mesh, lam, mu, u = _workload(args.grid)
+    nnz = _nnz_p2(args.grid)
     nt = cpu_threads_for(nnz)
     times, t_first = time_cpu_reference(mesh, lam, mu, u, nt, args.warmup + args.steps)
     timed = times[args.warmup:]
@@ -163,17 +225,65 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded mesh, lognormal Lame, u = 0.02 h N(0,1))",
-        "config": {"workload": WORKLOAD, "precision": "fp64",
-                   "implementation": "C++ restatement of NLAssembler::assemble_hessian + SparseMatrixCache (oracle/pf_oracle.cpp), std::thread"},
+        "config": {"workload": workload_name(args.grid), "precision": "fp64",
+                   "implementation": "C++ restatement of NLAssembler::assemble_hessian + SparseMatrixCache "
+                                     "(oracle/pf_oracle.cpp), std::thread element-parallel"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
-                         "sample": f"full 40^3 P2 Hessian per step (384,000 elements), steady-state calls; first call (pattern build) {t_first:.2f} s"},
+                         "sample": f"full {args.grid}^3 P2 Hessian per step ({mesh.n_elements:,} elements), "
+                                   f"steady-state calls; first call (pattern build) {t_first:.2f} s"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def _nnz_p2(grid: int) -> int:
+    """CSC nonzeros of the P2 Kuhn-split g^3 cube: exact at 40, scaled by volume
+    otherwise (only used to size the CPU port's per-thread buffers)."""
+    return int(134475849 * max(1.0, (grid / 40.0) ** 3)) if grid >= 40 else int(134475849 * (grid / 40.0) ** 3) + 1
+
+
 # ----------------------------------------------------------------- GPU arm
+def max_over_ranks_of(x: float, device="cpu") -> float:
+    """Slowest rank's time: every rank contributes x and receives the maximum
+    (identity outside an initialised process group)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
+def _events_ms(stream, fn, steps):
+    import torch
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    end.record(stream)
+    torch.cuda.synchronize()
+    return start.elapsed_time(end) / steps
+
+
+def _events_ms_flushed(stream, fn, steps, flush):
+    """Mean device time of fn over `steps` launches, each timed alone with CUDA
+    events after an L2 flush (a 256 MB write) on the same stream."""
+    import torch
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for i in range(steps):
+            flush.zero_()
+            starts[i].record(stream)
+            fn()
+            ends[i].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / steps
+
+
 def run_gpu(args):
     import torch
 
@@ -189,7 +299,7 @@ def run_gpu(args):
     from polyfem_b200 import NeoHookeanAssembler
     from polyfem_b200._lib import PFG_FP64, PFG_MEM_DEVICE, PFG_MEM_HOST, PFG_SPLIT32, check, lib
 
-    mesh, lam, mu, u = _workload()
+    mesh, lam, mu, u = _workload(args.grid)
     asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu, device=local)
     nnz = asm.hessian_nnz()
     E = mesh.n_elements
@@ -199,65 +309,59 @@ def run_gpu(args):
     check(L.pfg_set_stream(h, ctypes_ptr(stream.cuda_stream)), h, "pfg_set_stream")
     ud = torch.tensor(u, device=f"cuda:{local}", dtype=torch.float64)
     vals_dev = torch.empty(nnz, device=f"cuda:{local}", dtype=torch.float64)
+    uptr = ctypes_ptr(ud.data_ptr())
 
-    def call(prec, mem, uptr, vptr):
-        check(L.pfg_hessian(h, uptr, mem, prec, 0, vptr), h, "pfg_hessian")
+    def call(prec, mem, up, vptr):
+        check(L.pfg_hessian(h, up, mem, prec, 0, vptr), h, "pfg_hessian")
 
-    def timed_device(prec, steps, warmup):
-        for _ in range(warmup):
-            call(prec, PFG_MEM_DEVICE, ctypes_ptr(ud.data_ptr()), None)
+    def max_over_ranks(x):
+        return max_over_ranks_of(x, f"cuda:{local}")
+
+    def timed_device(prec, sampler=None):
+        for _ in range(args.warmup):
+            call(prec, PFG_MEM_DEVICE, uptr, None)
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
-        start = torch.cuda.Event(enable_timing=True)
-        end = torch.cuda.Event(enable_timing=True)
-        start.record(stream)
-        for _ in range(steps):
-            call(prec, PFG_MEM_DEVICE, ctypes_ptr(ud.data_ptr()), None)
-        end.record(stream)
         torch.cuda.synchronize()
-        ms = start.elapsed_time(end) / steps
+        if sampler is not None:
+            sampler.start()
+        ms = _events_ms(stream, lambda: call(prec, PFG_MEM_DEVICE, uptr, None), args.steps)
+        clocks = sampler.stop() if sampler is not None else None
         if dist is not None:
-            t = torch.tensor([ms], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t)
-        return ms
+            dist.barrier()
+        return max_over_ranks(ms), clocks
 
     # accuracy of the headline precision against the FP64 drop-in
-    call(PFG_FP64, PFG_MEM_DEVICE, ctypes_ptr(ud.data_ptr()), ctypes_ptr(vals_dev.data_ptr()))
+    call(PFG_FP64, PFG_MEM_DEVICE, uptr, ctypes_ptr(vals_dev.data_ptr()))
     torch.cuda.synchronize()
     v64 = vals_dev.clone()
-    call(PFG_SPLIT32, PFG_MEM_DEVICE, ctypes_ptr(ud.data_ptr()), ctypes_ptr(vals_dev.data_ptr()))
+    call(PFG_SPLIT32, PFG_MEM_DEVICE, uptr, ctypes_ptr(vals_dev.data_ptr()))
     torch.cuda.synchronize()
     rel_err = float(torch.linalg.vector_norm(vals_dev - v64) / torch.linalg.vector_norm(v64))
     del v64
 
-    ms64 = timed_device(PFG_FP64, args.steps, args.warmup)
-    sampler = ClockSampler(local)
-    sampler.start()
-    ms_split = timed_device(PFG_SPLIT32, args.steps, args.warmup)
-    clocks = sampler.stop()
+    ms64, _ = timed_device(PFG_FP64)
+    ms_split, clocks = timed_device(PFG_SPLIT32, ClockSampler(local))
 
-    # end to end through the C ABI with host buffers (pinned u in, pinned CSC values out)
+    # end to end through the C ABI with host buffers: pinned u in, CSC values out
+    # (the call copies u to the device, assembles, copies the values back and syncs)
     u_host = torch.tensor(u, dtype=torch.float64).pin_memory()
     v_host = torch.empty(nnz, dtype=torch.float64).pin_memory()
-    for _ in range(max(1, args.warmup)):
-        call(PFG_SPLIT32, PFG_MEM_HOST, ctypes_ptr(u_host.data_ptr()), ctypes_ptr(v_host.data_ptr()))
+    hptr_u, hptr_v = ctypes_ptr(u_host.data_ptr()), ctypes_ptr(v_host.data_ptr())
+    for _ in range(args.warmup):
+        call(PFG_SPLIT32, PFG_MEM_HOST, hptr_u, hptr_v)
     if dist is not None:
         dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        call(PFG_SPLIT32, PFG_MEM_HOST, ctypes_ptr(u_host.data_ptr()), ctypes_ptr(v_host.data_ptr()))
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t)
+    torch.cuda.synchronize()
+    e2e_ms = _events_ms(stream, lambda: call(PFG_SPLIT32, PFG_MEM_HOST, hptr_u, hptr_v), args.steps)
+    e2e_ms = max_over_ranks(e2e_ms)
 
+    rec_bytes = 32 * ((9 * 10 * 4 + 31) // 32)
     bytes_alg = algorithmic_bytes(mesh, nnz)
-    peaks = _peaks()
+    peak, peak_src = _peaks()
     achieved = bytes_alg / (ms_split * 1e-3) / 1e9
-    traffic = _profiled_traffic()
+    traffic = _profiled_traffic(args.grid)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -265,34 +369,123 @@ def run_gpu(args):
         times, t_first = time_cpu_reference(mesh, lam, mu, u, nt, 2)
         t = min(times)
         cpu = {"value": E / t, "unit": UNIT, "cores": nt, "kind": "port",
-               "sample": f"full 40^3 P2 Hessian (384,000 elements), best of 2 steady-state calls; pattern build {t_first:.1f} s"}
+               "sample": f"full {args.grid}^3 P2 Hessian ({E:,} elements), best of 2 steady-state calls "
+                         f"of the oracle's std::thread port; pattern build {t_first:.1f} s"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": world * E / (ms_split * 1e-3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_split, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (3xTF32 split) + f64 det/CSC",
-            "data": "synthetic (seeded 40^3 P2 mesh, lognormal Lame, u = 0.02 h N(0,1))",
-            "config": {"workload": WORKLOAD, "global_batch": world * E, "parallelism": f"replicas x{world}",
-                       "precision": "split32", "nnz": nnz, "l2": "inputs larger than L2 (1.08 GB CSC values)"},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 kinematics + f32 contraction, f64 CSC",
+            "data": f"synthetic (seeded {args.grid}^3 P2 mesh, lognormal Lame, u = 0.02 h N(0,1))",
+            "config": {"workload": workload_name(args.grid), "global_batch": world * E,
+                       "parallelism": f"replicas x{world}", "precision": "split32",
+                       "precision_detail": PRECISION_NOTE, "nnz": nnz,
+                       "l2": "no flush; every step writes the 1.08 GB CSC values and 1.4 GB of element "
+                             "records, both larger than the 126 MB L2"},
             "fp64": {"value": world * E / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64},
             "split_over_fp64": ms64 / ms_split,
             "rel_err_vs_fp64": rel_err,
-            "e2e": {"value": world * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": u_host.numel() * 8,
-                    "d2h_bytes_per_step": nnz * 8},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks[0], "unit": "GB/s",
-                         "frac": achieved / peaks[0], "traffic": traffic, "peak_source": peaks[1],
+            "e2e": {"value": world * E / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": u_host.numel() * 8, "d2h_bytes_per_step": nnz * 8},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "bytes_alg_per_launch": bytes_alg,
-                         "note": "pfg_hessian call (value zeroing + assembly kernel), CUDA events on its stream"},
+                         "staged_bytes_per_launch": staged_bytes(mesh, nnz, rec_bytes),
+                         "note": "one pfg_hessian call = k_hessian_blocks + k_hessian_gather, CUDA events "
+                                 "on the context's stream; frac of measured HBM copy bandwidth"},
             "cpu_baseline": cpu,
             "clocks": clocks,
-            "gpu_launches": args.steps * 1,
+            "gpu_launches": 2 * args.steps,
         }
         print(json.dumps(line), flush=True)
     asm.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+# ----------------------------------------------------------------- per-operation suite
+SUITE = {
+    # name: (element order or 'hex', grid, jitter, lognormal Lame, displacement kind)
+    "P1-20 (48,000 tets)": ("p1", 20, 0.0, False, "rand"),
+    "P1-48 (663,552 tets)": ("p1", 48, 0.0, True, "rand"),
+    "P2-40 (384,000 tets)": ("p2", 40, 0.0, True, "rand"),
+    "P2-32 jittered (196,608 tets)": ("p2", 32, 0.1, False, "rand"),
+    "Q1-96 jittered (884,736 hexes)": ("hex", 96, 0.1, True, "smooth"),
+}
+
+
+def run_suite(args):
+    """Per-operation device timings on every workload: inputs resident in HBM, L2
+    flushed before every timed launch, CUDA events around each launch."""
+    import ctypes
+
+    import torch
+
+    from polyfem_b200 import NeoHookeanAssembler
+    from polyfem_b200 import mesh as M
+    from polyfem_b200._lib import lib
+
+    L = lib()
+    vp = ctypes.c_void_p
+    stream = torch.cuda.Stream()
+    peak, _ = _peaks()
+    names = args.only.split(",") if args.only else list(SUITE)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    for name in names:
+        kind, g, jit, logn, disp = SUITE[name]
+        if kind == "hex":
+            mesh = M.structured_hex_mesh(g, jitter=jit, seed=3)
+        else:
+            mesh = M.structured_tet_mesh(g, 1 if kind == "p1" else 2, jitter=jit, seed=3)
+        E = mesh.n_elements
+        lam, mu = M.lognormal_lame(E, SEED_LAME) if logn else M.homogeneous_lame(E)
+        u = M.random_displacement(mesh, 0.02, SEED_U) if disp == "rand" else M.smooth_displacement(mesh, 0.05, 0.005, 4)
+        asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+        nnz = asm.hessian_nnz()
+        h = asm.handle
+        L.pfg_set_stream(h, vp(stream.cuda_stream))
+        ud = torch.tensor(u, dtype=torch.float64, device="cuda")
+        pd = torch.randn(mesh.n_dofs, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(7))
+        out = torch.empty(max(mesh.n_dofs, 2 * E, 3 * mesh.n_geom_nodes), dtype=torch.float64, device="cuda")
+        U, P, O = vp(ud.data_ptr()), vp(pd.data_ptr()), vp(out.data_ptr())
+        ops = {
+            "energy_fp64": lambda: L.pfg_energy(h, U, 1, 0, O),
+            "energy_fp32": lambda: L.pfg_energy(h, U, 1, 1, O),
+            "gradient_fp64": lambda: L.pfg_gradient(h, U, 1, 0, O),
+            "gradient_fp32": lambda: L.pfg_gradient(h, U, 1, 1, O),
+            "hessian_fp64": lambda: L.pfg_hessian(h, U, 1, 0, 0, None),
+            "hessian_fp32": lambda: L.pfg_hessian(h, U, 1, 1, 0, None),
+            "hessian_split32": lambda: L.pfg_hessian(h, U, 1, 2, 0, None),
+            "material_vjp": lambda: L.pfg_material_vjp(h, U, P, 1, O),
+            "shape_vjp_fp64": lambda: L.pfg_shape_vjp(h, U, P, 1, 0, O),
+            "shape_vjp_fp32": lambda: L.pfg_shape_vjp(h, U, P, 1, 1, O),
+        }
+        # algorithmic bytes of the HBM-bound operations
+        n, ng = mesh.conn.shape[1], mesh.gconn.shape[1]
+        ins = E * n * 4 + (E * ng * 4 if mesh.gconn is not mesh.conn else 0) + E * 16 + mesh.n_geom_nodes * 24 + mesh.n_nodes * 24
+        alg = {"energy_fp64": ins + 8, "energy_fp32": ins + 8,
+               "gradient_fp64": ins + mesh.n_dofs * 8, "gradient_fp32": ins + mesh.n_dofs * 8,
+               "material_vjp": ins + mesh.n_nodes * 24 + 2 * E * 8,
+               "hessian_fp64": algorithmic_bytes(mesh, nnz), "hessian_fp32": algorithmic_bytes(mesh, nnz),
+               "hessian_split32": algorithmic_bytes(mesh, nnz)}
+        res = {}
+        for op, fn in ops.items():
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            reps = 10 if op.startswith("hessian") else 50
+            ms = _events_ms_flushed(stream, fn, reps, flush)
+            r = {"us": round(ms * 1e3, 2), "elements_per_s": E / (ms * 1e-3)}
+            if op in alg:
+                gbs = alg[op] / (ms * 1e-3) / 1e9
+                r["alg_GBps"] = round(gbs, 1)
+                r["frac_hbm"] = round(gbs / peak, 4)
+            res[op] = r
+        print(json.dumps({"suite": name, "E": E, "N": mesh.n_nodes, "nnz": nnz, "ops": res}), flush=True)
+        asm.close()
     return 0
 
 
@@ -310,13 +503,18 @@ def _peaks():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def _profiled_traffic():
-    """DRAM bytes per launch of the Hessian assembly from the committed ncu summary."""
-    path = os.path.join(REPO, "profiles", "hessian_p2_40.txt")
+def _profiled_traffic(grid: int):
+    """DRAM bytes per pfg_hessian call (both kernels) from the committed ncu summary,
+    scaled from the profiled case to this workload by elements (traffic grows in
+    proportion to the elements processed)."""
+    path = os.path.join(REPO, "profiles", "hessian_p2_split32.txt")
     try:
+        per_elem = None
         for ln in open(path):
-            if ln.startswith("traffic_bytes_per_launch"):
-                return float(ln.split("=")[1].split()[0])
+            if ln.startswith("traffic_bytes_per_element"):
+                per_elem = float(ln.split("=")[1].split()[0])
+        if per_elem is not None:
+            return per_elem * 6 * grid ** 3
     except Exception:
         pass
     return None
@@ -328,10 +526,15 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=40, help="P2 cube cells per axis (40 = the benchmark workload)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--suite", action="store_true", help="per-operation timings on all workloads")
+    ap.add_argument("--only", default="", help="comma-separated suite workloads")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.suite:
+        return run_suite(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)

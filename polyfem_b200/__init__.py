@@ -2,6 +2,8 @@
 
 The compute path is the CUDA library ``libpfgpu.so`` (C ABI in include/pfgpu.h);
 this package is its host-side mirror of PolyFEM's NLAssembler / ElasticForm API.
+``polyfem_b200.autograd`` (imported on demand, it needs torch) wraps the gradient
+and the adjoint kernels as a torch.autograd.Function.
 """
 from . import mesh
 from ._lib import PfgError, build, lib
