@@ -22,6 +22,7 @@ Run:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import statistics
@@ -99,14 +100,19 @@ class ClockSampler:
         self.source = None
 
     def _nvml_handle(self):
+        """NVML handle of the CUDA device, matched by PCI domain/bus/device numbers
+        (CUDA and NVML may enumerate devices differently)."""
         import pynvml
+        import torch
         pynvml.nvmlInit()
-        try:
-            import torch
-            bus = torch.cuda.get_device_properties(self.cuda_index).pci_bus_id
-            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode() if isinstance(bus, str) else bus)
-        except Exception:
-            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
+        props = torch.cuda.get_device_properties(self.cuda_index)
+        want = tuple(int(getattr(props, k, -1)) for k in ("pci_domain_id", "pci_bus_id", "pci_device_id"))
+        for i in range(pynvml.nvmlDeviceGetCount()):
+            h = pynvml.nvmlDeviceGetHandleByIndex(i)
+            pi = pynvml.nvmlDeviceGetPciInfo(h)
+            if (int(pi.domain), int(pi.bus), int(pi.device)) == want:
+                return pynvml, h
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def start(self):
         try:
@@ -270,13 +276,18 @@ def _events_ms(stream, fn, steps):
 
 def _events_ms_flushed(stream, fn, steps, flush):
     """Mean device time of fn over `steps` launches, each timed alone with CUDA
-    events after an L2 flush (a 256 MB write) on the same stream."""
+    events after an L2 flush on the same stream: a 256 MB write (evicts the
+    operation's lines) followed by a 256 MB read (evicts the flush's own dirty
+    lines, so their write-back does not land inside the timed launch)."""
     import torch
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    half = flush.numel() // 2
+    sink = torch.empty((), dtype=flush.dtype, device=flush.device)
     with torch.cuda.stream(stream):
         for i in range(steps):
-            flush.zero_()
+            flush[:half].zero_()
+            torch.sum(flush[half:], out=sink)
             starts[i].record(stream)
             fn()
             ends[i].record(stream)
@@ -408,12 +419,12 @@ def run_gpu(args):
 
 # ----------------------------------------------------------------- per-operation suite
 SUITE = {
-    # name: (element order or 'hex', grid, jitter, lognormal Lame, displacement kind)
-    "P1-20 (48,000 tets)": ("p1", 20, 0.0, False, "rand"),
-    "P1-48 (663,552 tets)": ("p1", 48, 0.0, True, "rand"),
-    "P2-40 (384,000 tets)": ("p2", 40, 0.0, True, "rand"),
-    "P2-32 jittered (196,608 tets)": ("p2", 32, 0.1, False, "rand"),
-    "Q1-96 jittered (884,736 hexes)": ("hex", 96, 0.1, True, "smooth"),
+    # key: (element order or 'hex', grid, jitter, lognormal Lame, displacement kind, description)
+    "P1-20": ("p1", 20, 0.0, False, "rand", "P1 tets 20^3 x 6 (48,000), homogeneous E=1e5 nu=0.35"),
+    "P1-48": ("p1", 48, 0.0, True, "rand", "P1 tets 48^3 x 6 (663,552), lognormal Lame"),
+    "P2-40": ("p2", 40, 0.0, True, "rand", "P2 tets 40^3 x 6 (384,000), lognormal Lame"),
+    "P2-32j": ("p2", 32, 0.1, False, "rand", "P2 tets 32^3 x 6 (196,608), jittered rest positions, homogeneous"),
+    "Q1-96j": ("hex", 96, 0.1, True, "smooth", "Q1 hexes 96^3 (884,736), jittered, lognormal Lame, smooth u"),
 }
 
 
@@ -433,9 +444,9 @@ def run_suite(args):
     stream = torch.cuda.Stream()
     peak, _ = _peaks()
     names = args.only.split(",") if args.only else list(SUITE)
-    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    flush = torch.zeros(128 << 20, dtype=torch.float32, device="cuda")  # 2 x 256 MB, each > 126 MB L2
     for name in names:
-        kind, g, jit, logn, disp = SUITE[name]
+        kind, g, jit, logn, disp, desc = SUITE[name]
         if kind == "hex":
             mesh = M.structured_hex_mesh(g, jitter=jit, seed=3)
         else:
@@ -484,7 +495,7 @@ def run_suite(args):
                 r["alg_GBps"] = round(gbs, 1)
                 r["frac_hbm"] = round(gbs / peak, 4)
             res[op] = r
-        print(json.dumps({"suite": name, "E": E, "N": mesh.n_nodes, "nnz": nnz, "ops": res}), flush=True)
+        print(json.dumps({"suite": name, "workload": desc, "E": E, "N": mesh.n_nodes, "nnz": nnz, "ops": res}), flush=True)
         asm.close()
     return 0
 
@@ -521,6 +532,7 @@ def _profiled_traffic(grid: int):
 
 
 def main():
+    faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -529,7 +541,7 @@ def main():
     ap.add_argument("--grid", type=int, default=40, help="P2 cube cells per axis (40 = the benchmark workload)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--suite", action="store_true", help="per-operation timings on all workloads")
-    ap.add_argument("--only", default="", help="comma-separated suite workloads")
+    ap.add_argument("--only", default="", help="comma-separated suite workload keys (" + ",".join(SUITE) + ")")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -34,7 +34,7 @@ struct pfg_context
 	DevPattern pat;
 	int *d_outer = nullptr, *d_inner = nullptr;
 	double *d_values = nullptr;
-	unsigned short *d_strip_rank = nullptr;
+	unsigned short *d_contrib = nullptr, *d_blk_rel = nullptr;
 	int *d_eb_inc = nullptr;
 	// node -> (element, local index) incidences, FE and geometric nodes
 	std::vector<long long> h_inc_off; // [N+1]
@@ -187,7 +187,7 @@ int finish_host(pfg_context *c, double *host_dst, const double *dev_src, size_t 
 // unique rows touched by any element) and the node-owner assembly plans.
 int build_pattern(pfg_context *c)
 {
-	const int E = c->m.E, N = c->m.N, n = c->n;
+	const int N = c->m.N, n = c->n;
 	const int *conn = c->h_conn.data();
 	const std::vector<long long> &ioff = c->h_inc_off;
 	const std::vector<int> &inc = c->h_inc_e;
@@ -267,22 +267,57 @@ int build_pattern(pfg_context *c)
 		}
 	});
 
+	// Reduction plan of every column node B (the device form of SparseMatrixCache's
+	// second_cache_): its n * (#incidences) record blocks, grouped by the row rank
+	// they land on, incidences ascending inside a group.  contrib holds each block
+	// as (incidence - first incidence of B) * n + local row node, relative to B's
+	// first record; blk_rel[block] is where the block's group starts, relative to
+	// B's first contribution.  Both fit in 16 bits while a node has at most
+	// 65535 / n incidences.
+	long long max_tot = 0;
+	for (int B = 0; B < N; ++B) max_tot = std::max(max_tot, (ioff[B + 1] - ioff[B]) * n);
+	if (max_tot > 65535)
+		return fail(c, PFG_ERR_UNSUPPORTED,
+					"a node has more than 65535 incident (element, local node) pairs; the 16-bit reduction plan cannot hold it");
+	std::vector<unsigned short> contrib((size_t)nstrip * n);
+	std::vector<unsigned short> blk_rel((size_t)noff[N]);
+	parallel_ranges(N, [&](long long s0, long long s1, int) {
+		std::vector<int> pos;
+		for (long long B = s0; B < s1; ++B)
+		{
+			const int d = deg[B];
+			pos.assign(d + 1, 0);
+			const long long k0 = ioff[B], k1 = ioff[B + 1];
+			for (long long k = k0; k < k1; ++k)
+				for (int a = 0; a < n; ++a) pos[strip_rank[(size_t)k * n + a] + 1]++;
+			for (int r = 0; r < d; ++r) pos[r + 1] += pos[r];
+			for (int r = 0; r < d; ++r) blk_rel[noff[B] + r] = (unsigned short)pos[r];
+			unsigned short *cb = contrib.data() + (size_t)k0 * n;
+			for (long long k = k0; k < k1; ++k)
+				for (int a = 0; a < n; ++a)
+					cb[pos[strip_rank[(size_t)k * n + a]]++] = (unsigned short)((k - k0) * n + a);
+		}
+	});
+
 	PFG_CUDA(c, cudaMalloc(&c->d_outer, sizeof(int) * (ndof + 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_inner, sizeof(int) * std::max<long long>(nnz, 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_values, sizeof(double) * std::max<long long>(nnz, 1)));
-	PFG_CUDA(c, cudaMalloc(&c->d_strip_rank, sizeof(unsigned short) * std::max<size_t>(strip_rank.size(), 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_contrib, sizeof(unsigned short) * std::max<size_t>(contrib.size(), 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_blk_rel, sizeof(unsigned short) * std::max<size_t>(blk_rel.size(), 1)));
 	PFG_CUDA(c, cudaMemcpy(c->d_outer, outer.data(), sizeof(int) * (ndof + 1), cudaMemcpyHostToDevice));
 	if (nnz) PFG_CUDA(c, cudaMemcpy(c->d_inner, inner.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice));
-	if (!strip_rank.empty())
-		PFG_CUDA(c, cudaMemcpy(c->d_strip_rank, strip_rank.data(), sizeof(unsigned short) * strip_rank.size(),
+	if (!contrib.empty())
+		PFG_CUDA(c, cudaMemcpy(c->d_contrib, contrib.data(), sizeof(unsigned short) * contrib.size(),
 							   cudaMemcpyHostToDevice));
-	if ((size_t)8 * 9 * max_deg * sizeof(double) > 200 * 1024)
-		return fail(c, PFG_ERR_UNSUPPORTED, "a node has too many neighbours for the shared-memory column assembly");
+	if (!blk_rel.empty())
+		PFG_CUDA(c, cudaMemcpy(c->d_blk_rel, blk_rel.data(), sizeof(unsigned short) * blk_rel.size(),
+							   cudaMemcpyHostToDevice));
 	c->pat.nnz = nnz;
 	c->pat.max_deg = max_deg;
 	c->pat.outer = c->d_outer;
 	c->pat.inner = c->d_inner;
-	c->pat.strip_rank = c->d_strip_rank;
+	c->pat.contrib = c->d_contrib;
+	c->pat.blk_rel = c->d_blk_rel;
 	c->pat.values = c->d_values;
 	c->has_pattern = true;
 	return PFG_OK;
@@ -309,7 +344,7 @@ void build_incidence(const int *conn, int E, int n, int N, std::vector<long long
 
 void free_all(pfg_context *c)
 {
-	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_strip_rank, c->d_eb_inc,
+	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_contrib, c->d_blk_rel, c->d_eb_inc,
 					c->d_inc_off, c->d_inc_eb, c->d_ginc_off, c->d_ginc_eb, c->d_vec_stage, c->d_hess_stage[0],
 					c->d_hess_stage[1], c->sc.partials, c->sc.ticket, c->sc.inverted, c->d_result, c->d_u, c->d_p, c->d_out};
 	for (void *p : ptrs)

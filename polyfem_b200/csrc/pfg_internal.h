@@ -32,11 +32,15 @@ struct DevMesh
 	const int *ginc_eb = nullptr;
 };
 
-// Device-resident Hessian pattern (Eigen ColMajor CSC, int32 indices) and the
-// row rank of every (incidence, local row node): entry (3A+r, 3B+c) of an element
-// holding B at local b and A at local a lives at
-//   outer[3B] + c*(outer[3B+1]-outer[3B]) + 3*strip_rank[s*n + a] + r,
-// s being the incidence's index in inc_eb.
+// Device-resident Hessian pattern (Eigen ColMajor CSC, int32 indices) and its
+// reduction plan.  Node B's column block has deg(B) row nodes (rank 0..deg-1 in
+// ascending node order); entry (3A+r, 3B+c) lives at
+//   outer[3B] + c*3*deg(B) + 3*rank_B(A) + r,
+// and B's node blocks are numbered from outer[3B] / 9.  For node B with
+// incidences s0..s1-1 (inc_off):
+//   contrib[s0*n + k], k < (s1-s0)*n : record block (s - s0)*n + a, grouped by the
+//       rank of local node a, incidences ascending inside a group;
+//   blk_rel[outer[3B]/9 + rank]     : start of the rank's group, relative to s0*n.
 struct DevPattern
 {
 	long long nnz = 0;
@@ -44,7 +48,8 @@ struct DevPattern
 
 	const int *outer = nullptr;
 	const int *inner = nullptr;
-	const unsigned short *strip_rank = nullptr;
+	const unsigned short *contrib = nullptr;
+	const unsigned short *blk_rel = nullptr;
 	double *values = nullptr;
 };
 

@@ -420,33 +420,18 @@ __global__ void __launch_bounds__(NT) k_vec_gather(int n_nodes, const int *__res
 //     blocks once; for every incidence (e, b) the record of all blocks of column
 //     node b, [a][c][r] = H_e(3a+r, 3b+c), is written to the staging buffer at
 //     the incidence's position in node order (records padded to whole sectors).
-//  2. k_hessian_gather: one warp per column node B streams B's records -- one
-//     contiguous run, with their row ranks alongside -- adds them in incidence
-//     order into a shared-memory image of B's three CSC columns, and writes the
-//     columns once, coalesced.  Each CSC entry is summed in a fixed order: the
-//     result is deterministic.
+//  2. k_hessian_reduce: one warp per column node B reads B's records -- one
+//     contiguous run -- through the reduction plan built with the pattern (for
+//     each row rank, the record blocks that land on it), sums every CSC entry in
+//     registers in incidence order and writes B's three columns once.  Each CSC
+//     entry is summed in a fixed order: the result is deterministic.
 // ---------------------------------------------------------------------------
 template <class EL>
-struct OwnerKin
+struct BlockKin
 {
-	// J^-T (9), F^-T (9), mu da, lambda da, (mu - lambda lnJ) da, then g_i (3), d_i (3) per local node
-	static constexpr int PER_Q = 21 + 6 * EL::N;
+	// per (element, point): mu da, lambda da, (mu - lambda lnJ) da, then g_a (3), d_a (3) per local node
+	static constexpr int PER_Q = 3 + 6 * EL::N;
 };
-
-// reference gradient with run-time (q, a): evaluated from the compile-time table
-template <class EL, class T>
-__device__ __forceinline__ T gtab_at(int q, int a, int r)
-{
-	T out = T(0);
-#pragma unroll
-	for (int qq = 0; qq < EL::NQ; ++qq)
-#pragma unroll
-		for (int aa = 0; aa < EL::N; ++aa)
-#pragma unroll
-			for (int rr = 0; rr < 3; ++rr)
-				if (qq == q && aa == a && rr == r) out = T(gref<EL>(qq, aa, rr));
-	return out;
-}
 
 // Record of one incidence (e, b): the 9n values H_e(3a+r, 3b+c), [a][c][r], padded to
 // whole 32-byte sectors so that records written at scattered positions stay full-sector.
@@ -462,34 +447,60 @@ struct EcTile
 	static constexpr int TE = (EL::ET == 1) ? 64 : (EL::ET == 2 ? 16 : 8);
 	static constexpr int NT = 128;
 	static constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ;
-	static constexpr int NP = N * (N + 1) / 2, NB = N * N, PQ = OwnerKin<EL>::PER_Q;
+	static constexpr int NP = N * (N + 1) / 2, NB = N * N, PQ = BlockKin<EL>::PER_Q;
 };
 
-// K: arithmetic of the kinematics (J^-T, F^-T, g, d); T: arithmetic of the contraction and records
+// K: arithmetic of the kinematics (J^-T, F, F^-T, g, d); T: arithmetic of the
+// contraction and the records (g, d and the weights are stored rounded to T)
 template <class EL, class K, class T>
 struct EcSmem
 {
 	using TL = EcTile<EL, T>;
+	// one element's records per warp (record b padded to rec_pad values), then copied out in 16-byte vectors
+	__align__(16) T rec[TL::NT / 32][TL::N * rec_pad<EL, T>()];
 	K U[TL::TE][TL::N][3];
 	K X[TL::TE][TL::NG][3];
-	K kin[TL::TE][TL::NQ][TL::PQ];
-	T rec[TL::NT / 32][TL::NB * 9]; // one element's blocks per warp, then copied out per incidence
+	T kin[TL::TE][TL::NQ][TL::PQ];
 	int nodes[TL::TE][TL::N + TL::NG];
 	int sidx[TL::NT / 32][TL::N];   // incidence index of (e, b) for the warp's element
+	unsigned char pair_a[TL::NP], pair_b[TL::NP];
 };
 
+// CTAs per SM the shared-memory footprint allows; the register budget follows it
+#ifndef PFG_BLOCKS_CTAS_F32
+#define PFG_BLOCKS_CTAS_F32 5
+#endif
 template <class EL, class K, class T>
-__global__ void __launch_bounds__(128, 4) k_hessian_blocks(DevMesh m, const double *__restrict__ u, T *__restrict__ stage)
+constexpr int blocks_min_ctas()
+{
+	constexpr int by_smem = (int)((227 * 1024) / (sizeof(EcSmem<EL, K, T>) + 1024));
+	constexpr int cap = sizeof(T) == 8 ? 4 : PFG_BLOCKS_CTAS_F32;
+	return by_smem < 1 ? 1 : (by_smem < cap ? by_smem : cap);
+}
+
+template <class EL, class K, class T>
+__global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>()) k_hessian_blocks(DevMesh m, const double *__restrict__ u, T *__restrict__ stage)
 {
 	using TL = EcTile<EL, T>;
-	constexpr int TE = TL::TE, NT = TL::NT, N = TL::N, NG = TL::NG, NQ = TL::NQ, NP = TL::NP, NB = TL::NB;
+	constexpr int TE = TL::TE, NT = TL::NT, N = TL::N, NG = TL::NG, NQ = TL::NQ, NP = TL::NP;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	EcSmem<EL, K, T> &S = *reinterpret_cast<EcSmem<EL, K, T> *>(smem_raw);
 	const int tid = threadIdx.x;
 	const int e0 = blockIdx.x * TE;
 	const int ne = min(TE, m.E - e0);
 
-	// phase 0: node ids (coalesced over the tile), then the gathers
+	// phase 0: node-pair table, node ids (coalesced over the tile), then the gathers
+	for (int p = tid; p < NP; p += NT)
+	{
+		int a = 0, r = p;
+		while (r >= N - a)
+		{
+			r -= N - a;
+			++a;
+		}
+		S.pair_a[p] = (unsigned char)a;
+		S.pair_b[p] = (unsigned char)(a + r);
+	}
 	for (int i = tid; i < TE * (N + NG); i += NT)
 	{
 		const int j = i / TE, el = i % TE, e = e0 + el;
@@ -510,24 +521,21 @@ __global__ void __launch_bounds__(128, 4) k_hessian_blocks(DevMesh m, const doub
 	}
 	__syncthreads();
 
-	// phase 1a: J^-T, F^-T and the weights of every (element, quadrature point)
+	// phase 1: per (element, quadrature point): J^-T, F, det/log J and F^-T in K,
+	// then the weights and, for every local node, g_a = grad(phi_a) J^-T and
+	// d_a = F^-T g_a, stored rounded to T
 	for (int i = tid; i < ne * NQ; i += NT)
 	{
 		const int el = i / NQ, q = i % NQ;
 		const double2 lm = __ldg(m.lame + e0 + el);
-		K *Kq = S.kin[el][q];
+		T *Kq = S.kin[el][q];
 #pragma unroll
 		for (int qq = 0; qq < NQ; ++qq)
 		{
 			if (qq != q) continue;
-			K Xg[NG][3];
-#pragma unroll
-			for (int j = 0; j < NG; ++j)
-#pragma unroll
-				for (int d = 0; d < 3; ++d) Xg[j][d] = S.X[el][j][d];
 			K Jit[3][3];
 			double detJ;
-			geometry<EL, K>(qq, Xg, Jit, detJ);
+			geometry<EL, K>(qq, S.X[el], Jit, detJ);
 			K Ar[3][3];
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
@@ -565,77 +573,73 @@ __global__ void __launch_bounds__(128, 4) k_hessian_blocks(DevMesh m, const doub
 			const double da = detJ * qweight<EL>(qq);
 			K FmT[3][3];
 			inv_transpose3(F, K(J), FmT);
+			Kq[0] = T(lm.y * da);
+			Kq[1] = T(lm.x * da);
+			Kq[2] = T((lm.y - lm.x * lj) * da);
 #pragma unroll
-			for (int r = 0; r < 3; ++r)
+			for (int a = 0; a < N; ++a)
+			{
+				K g[3];
 #pragma unroll
 				for (int c = 0; c < 3; ++c)
 				{
-					Kq[r * 3 + c] = Jit[r][c];
-					Kq[9 + r * 3 + c] = FmT[r][c];
+					K s_ = K(0);
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+					{
+						const double gr = gref<EL>(qq, a, r);
+						if (gr != 0.0) s_ += K(gr) * Jit[r][c];
+					}
+					g[c] = s_;
 				}
-			Kq[18] = K(lm.y * da);
-			Kq[19] = K(lm.x * da);
-			Kq[20] = K((lm.y - lm.x * lj) * da);
+				T *dst = Kq + 3 + 6 * a;
+				dst[0] = T(g[0]);
+				dst[1] = T(g[1]);
+				dst[2] = T(g[2]);
+#pragma unroll
+				for (int r = 0; r < 3; ++r) dst[3 + r] = T(FmT[r][0] * g[0] + FmT[r][1] * g[1] + FmT[r][2] * g[2]);
+			}
 		}
-	}
-	__syncthreads();
-	// phase 1b: g_i and d_i of every (element, point, node)
-	for (int i = tid; i < ne * NQ * N; i += NT)
-	{
-		const int el = i / (NQ * N), q = (i / N) % NQ, a = i % N;
-		K *Kq = S.kin[el][q];
-		const K g0 = gtab_at<EL, K>(q, a, 0), g1 = gtab_at<EL, K>(q, a, 1), g2 = gtab_at<EL, K>(q, a, 2);
-		K g[3];
-#pragma unroll
-		for (int c = 0; c < 3; ++c) g[c] = g0 * Kq[c] + g1 * Kq[3 + c] + g2 * Kq[6 + c];
-		K *dst = Kq + 21 + 6 * a;
-		dst[0] = g[0];
-		dst[1] = g[1];
-		dst[2] = g[2];
-#pragma unroll
-		for (int r = 0; r < 3; ++r) dst[3 + r] = Kq[9 + r * 3] * g[0] + Kq[9 + r * 3 + 1] * g[1] + Kq[9 + r * 3 + 2] * g[2];
 	}
 	__syncthreads();
 
 	// phase 2: each warp takes whole elements: symmetric node pairs into the warp's
-	// record buffer (H_ba = H_ab^T alongside), then the element's n x n blocks are
-	// written out as one contiguous run, b-major: stage[e][b][a][c][r] = H_e(3a+r, 3b+c)
+	// record buffer (H_ba = H_ab^T alongside), then the element's n records are
+	// written out, record b = H_e(3a+r, 3b+c) as [a][c][r], to the incidence's
+	// position in node order, in 16-byte vectors (the padding travels along)
+	constexpr int RP = rec_pad<EL, T>();
+	constexpr int VW = 16 / (int)sizeof(T), RV = RP / VW;
+	static_assert(RP % VW == 0, "records must be whole 16-byte vectors");
 	const int warp = tid >> 5, lane = tid & 31;
 	T *R = S.rec[warp];
 	for (int el = warp; el < ne; el += NT / 32)
 	{
 		for (int p0 = lane; p0 < NP; p0 += 32)
 		{
-			int p = p0, a = 0;
-			while (p >= N - a)
-			{
-				p -= N - a;
-				++a;
-			}
-			const int b = a + p;
+			const int a = S.pair_a[p0], b = S.pair_b[p0];
 			T h[3][3];
 #pragma unroll
 			for (int r = 0; r < 3; ++r) h[r][0] = h[r][1] = h[r][2] = T(0);
 #pragma unroll
 			for (int q = 0; q < NQ; ++q)
 			{
-				const K *Kq = S.kin[el][q];
-				const K *Ka = Kq + 21 + 6 * a, *Kb = Kq + 21 + 6 * b;
-				const T md = T(Kq[18]) * (T(Ka[0]) * T(Kb[0]) + T(Ka[1]) * T(Kb[1]) + T(Ka[2]) * T(Kb[2]));
-				const T sla = T(Kq[19]), sga = T(Kq[20]);
-				const T la[3] = {sla * T(Ka[3]), sla * T(Ka[4]), sla * T(Ka[5])};
-				const T gma[3] = {sga * T(Ka[3]), sga * T(Ka[4]), sga * T(Ka[5])};
-				const T db[3] = {T(Kb[3]), T(Kb[4]), T(Kb[5])};
+				const T *Kq = S.kin[el][q];
+				const T *Ka = Kq + 3 + 6 * a, *Kb = Kq + 3 + 6 * b;
+				const T md = Kq[0] * (Ka[0] * Kb[0] + Ka[1] * Kb[1] + Ka[2] * Kb[2]);
+				const T sla = Kq[1], sga = Kq[2];
+				const T la[3] = {sla * Ka[3], sla * Ka[4], sla * Ka[5]};
+				const T gma[3] = {sga * Ka[3], sga * Ka[4], sga * Ka[5]};
+				const T db[3] = {Kb[3], Kb[4], Kb[5]};
 #pragma unroll
 				for (int r = 0; r < 3; ++r)
 #pragma unroll
-					for (int c = 0; c < 3; ++c) h[r][c] += la[r] * db[c] + db[r] * gma[c];
+					for (int c = 0; c < 3; ++c) h[r][c] = fma(db[r], gma[c], fma(la[r], db[c], h[r][c]));
 				h[0][0] += md;
 				h[1][1] += md;
 				h[2][2] += md;
 			}
-			T *Hab = R + (b * N + a) * 9; // block (a, b): record of column node b
-			T *Hba = R + (a * N + b) * 9; // block (b, a): record of column node a
+			T *Hab = R + b * RP + a * 9; // block (a, b): record of column node b
+			T *Hba = R + a * RP + b * 9; // block (b, a): record of column node a
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -647,78 +651,75 @@ __global__ void __launch_bounds__(128, 4) k_hessian_blocks(DevMesh m, const doub
 		}
 		if (lane < N) S.sidx[warp][lane] = __ldg(m.eb_inc + (size_t)(e0 + el) * N + lane);
 		__syncwarp();
-		// record of (e, b) goes to the incidence's position in node order
-		constexpr int RP = rec_pad<EL, T>();
-		for (int i = lane; i < NB * 9; i += 32)
+		for (int i = lane; i < N * RV; i += 32)
 		{
-			const int b = i / (9 * N), k = i % (9 * N);
-			stage[(size_t)S.sidx[warp][b] * RP + k] = R[i];
+			const int b = i / RV, k = i - b * RV;
+			const uint4 v = reinterpret_cast<const uint4 *>(R + b * RP)[k];
+			reinterpret_cast<uint4 *>(stage + (size_t)S.sidx[warp][b] * RP)[k] = v;
 		}
 		__syncwarp();
 	}
 }
 
-// One warp per column node B: stream B's records (contiguous in node order) into a
-// shared image of its three CSC columns, PF records in flight at a time.
+// One warp per column node B.  Node B's records are one contiguous run of the
+// staging buffer; the warp's 3*deg(B) work items are the (row rank, column c)
+// triples of B's column block, column-major so that consecutive lanes write
+// consecutive CSC rows.  Each item sums, in FP64 and in incidence order, the
+// three values (rows 3*rank .. 3*rank+2 of column 3B+c) of every record block
+// that lands on its rank, read through the reduction plan, and writes them once.
+// No shared memory, no atomics: the sum order of every entry is fixed.
 template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 3) k_hessian_gather(DevMesh m, DevPattern pat, const T *__restrict__ stage)
+__global__ void __launch_bounds__(WARPS * 32, 6) k_hessian_reduce(DevMesh m, DevPattern pat, const T *__restrict__ stage)
 {
-	constexpr int N = EL::N, REC = 9 * N, KPL = (REC + 31) / 32, PF = 4, RP = rec_pad<EL, T>();
-	extern __shared__ __align__(16) unsigned char smem_raw[];
+	constexpr int N = EL::N, RP = rec_pad<EL, T>();
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int B = blockIdx.x * WARPS + warp;
 	if (B >= m.N) return;
-	double *acc = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 9 * pat.max_deg;
 	const int o0 = __ldg(pat.outer + 3 * B);
 	const int stride = __ldg(pat.outer + 3 * B + 1) - o0; // 3 * deg(B)
-	const int len = 3 * stride;
-	for (int i = lane; i < len; i += 32) acc[i] = 0.0;
-	int slot[KPL];
-#pragma unroll
-	for (int k = 0; k < KPL; ++k)
-	{
-		const int idx = lane + 32 * k;
-		slot[k] = (idx < REC) ? ((idx % 9) / 3) * stride + idx % 3 : 0; // column c and row r of the entry
-	}
-	__syncwarp();
+	const int deg = stride / 3;
 	const int s0 = __ldg(m.inc_off + B), s1 = __ldg(m.inc_off + B + 1);
-	for (int sb = s0; sb < s1; sb += PF)
-	{
-		T v[PF][KPL];
-		int rk[PF][KPL];
-#pragma unroll
-		for (int j = 0; j < PF; ++j)
-		{
-			const int s = sb + j;
-			if (s < s1)
-			{
-				const T *rec = stage + (size_t)s * RP;
-#pragma unroll
-				for (int k = 0; k < KPL; ++k)
-				{
-					const int idx = lane + 32 * k;
-					if (idx < REC)
-					{
-						v[j][k] = __ldg(rec + idx);
-						rk[j][k] = __ldg(pat.strip_rank + (size_t)s * N + idx / 9);
-					}
-				}
-			}
-		}
-#pragma unroll
-		for (int j = 0; j < PF; ++j)
-		{
-			if (sb + j < s1)
-			{
-#pragma unroll
-				for (int k = 0; k < KPL; ++k)
-					if (lane + 32 * k < REC) acc[slot[k] + 3 * rk[j][k]] += double(v[j][k]);
-			}
-			__syncwarp();
-		}
-	}
+	const int tot = (s1 - s0) * N;
+	const T *rec = stage + (size_t)s0 * RP;
+	const unsigned short *cl = pat.contrib + (size_t)s0 * N;
+	const unsigned short *br = pat.blk_rel + o0 / 9;
 	double *dst = pat.values + o0;
-	for (int i = lane; i < len; i += 32) dst[i] = acc[i];
+	for (int it = lane; it < stride; it += 32)
+	{
+		const int c = it / deg, r = it - c * deg;
+		const int k0 = __ldg(br + r);
+		const int k1 = (r + 1 < deg) ? (int)__ldg(br + r + 1) : tot;
+		double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+		int k = k0;
+		for (; k + 1 < k1; k += 2)
+		{
+			const int q0 = __ldg(cl + k), q1 = __ldg(cl + k + 1);
+			const int sr0 = q0 / N, sr1 = q1 / N;
+			const T *p0 = rec + sr0 * RP + 9 * (q0 - sr0 * N) + 3 * c;
+			const T *p1 = rec + sr1 * RP + 9 * (q1 - sr1 * N) + 3 * c;
+			const T x0 = __ldg(p0), x1 = __ldg(p0 + 1), x2 = __ldg(p0 + 2);
+			const T y0 = __ldg(p1), y1 = __ldg(p1 + 1), y2 = __ldg(p1 + 2);
+			a0 += double(x0);
+			a1 += double(x1);
+			a2 += double(x2);
+			a0 += double(y0);
+			a1 += double(y1);
+			a2 += double(y2);
+		}
+		if (k < k1)
+		{
+			const int q0 = __ldg(cl + k);
+			const int sr0 = q0 / N;
+			const T *p0 = rec + sr0 * RP + 9 * (q0 - sr0 * N) + 3 * c;
+			a0 += double(__ldg(p0));
+			a1 += double(__ldg(p0 + 1));
+			a2 += double(__ldg(p0 + 2));
+		}
+		double *d = dst + c * stride + 3 * r;
+		d[0] = a0;
+		d[1] = a1;
+		d[2] = a2;
+	}
 }
 
 template <class EL, class K, class T>
@@ -732,11 +733,8 @@ static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const
 	const int nb = (m.E + TL::TE - 1) / TL::TE;
 	if (nb > 0) k_hessian_blocks<EL, K, T><<<nb, TL::NT, bytes1, s>>>(m, u, stage);
 	constexpr int WARPS = 8;
-	const size_t bytes2 = (size_t)WARPS * 9 * p.max_deg * sizeof(double);
-	e = cudaFuncSetAttribute(k_hessian_gather<EL, T, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes2);
-	if (e != cudaSuccess) return e;
 	const int ng = (m.N + WARPS - 1) / WARPS;
-	if (ng > 0) k_hessian_gather<EL, T, WARPS><<<ng, WARPS * 32, bytes2, s>>>(m, p, stage);
+	if (ng > 0) k_hessian_reduce<EL, T, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
 	return cudaGetLastError();
 }
 
