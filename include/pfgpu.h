@@ -122,8 +122,10 @@ int pfg_hessian_pattern(pfg_context *ctx, long long *nnz);
 /* Copies the CSC index arrays: outer (3N+1) and inner (nnz) int32. */
 int pfg_hessian_pattern_copy(pfg_context *ctx, int *outer, int *inner, int mem);
 
-/* Assembles the Hessian values (nnz doubles, CSC order) into `values`; with
- * values == NULL they stay in the context's device buffer (pfg_hessian_device_csc).
+/* Assembles the Hessian values (nnz doubles, CSC order) into `values` (device
+ * memory: written in place, no extra copy); with values == NULL they go to the
+ * context's device buffer (pfg_hessian_device_csc), which keeps the result of
+ * the last such call.
  * Builds the pattern on the first call.  Replaces NLAssembler::assemble_hessian
  * (assembler/Assembler.cpp:645-771) and the later-call branch of
  * SparseMatrixCache (utils/MatrixCache.cpp:88-113, 214-225).

@@ -636,15 +636,12 @@ int pfg_hessian(pfg_context *c, const double *u, int mem, int prec, int project_
 	const double *du;
 	if ((st = stage_in(c, u, mem, c->d_u, 3 * (size_t)c->m.N, &du))) return st;
 	if ((st = ensure_hess_stage(c, prec))) return st;
-	PFG_CUDA(c, launch_hessian(c->m, c->pat, du, prec, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
-	if (values)
-	{
-		if (mem == PFG_MEM_HOST) return finish_host(c, values, c->d_values, c->pat.nnz);
-		if (c->pat.nnz)
-			PFG_CUDA(c, cudaMemcpyAsync(values, c->d_values, sizeof(double) * c->pat.nnz, cudaMemcpyDeviceToDevice, c->stream));
-	}
-	else if (mem == PFG_MEM_HOST)
-		PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	// device output goes straight into the caller's array; otherwise into the context's
+	DevPattern p = c->pat;
+	if (values && mem == PFG_MEM_DEVICE) p.values = values;
+	PFG_CUDA(c, launch_hessian(c->m, p, du, prec, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
+	if (values && mem == PFG_MEM_HOST) return finish_host(c, values, c->d_values, c->pat.nnz);
+	if (mem == PFG_MEM_HOST) PFG_CUDA(c, cudaStreamSynchronize(c->stream));
 	return PFG_OK;
 }
 

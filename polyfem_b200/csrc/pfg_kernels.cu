@@ -426,12 +426,65 @@ __global__ void __launch_bounds__(NT) k_vec_gather(int n_nodes, const int *__res
 //     registers in incidence order and writes B's three columns once.  Each CSC
 //     entry is summed in a fixed order: the result is deterministic.
 // ---------------------------------------------------------------------------
-template <class EL>
+// Per (element, point) kinematics in the contraction type T, in 16-byte groups:
+// [mu da, lambda da, (mu - lambda lnJ) da, -], then for every local node a at
+// 4 + NS*a the vectors g_a and d_a: FP32 [g0 g1 g2 - | d0 d1 d2 -] (NS = 8,
+// two 16-byte loads), FP64 [g0 g1 | g2 d0 | d1 d2] (NS = 6, three).
+template <class EL, class T>
 struct BlockKin
 {
-	// per (element, point): mu da, lambda da, (mu - lambda lnJ) da, then g_a (3), d_a (3) per local node
-	static constexpr int PER_Q = 3 + 6 * EL::N;
+	static constexpr int NS = sizeof(T) == 8 ? 6 : 8;
+	static constexpr int PER_Q = 4 + NS * EL::N;
 };
+
+__device__ __forceinline__ void ld_w(const float *p, float w[3])
+{
+	const float4 x = *reinterpret_cast<const float4 *>(p);
+	w[0] = x.x;
+	w[1] = x.y;
+	w[2] = x.z;
+}
+__device__ __forceinline__ void ld_w(const double *p, double w[3])
+{
+	const double2 x = *reinterpret_cast<const double2 *>(p);
+	w[0] = x.x;
+	w[1] = x.y;
+	w[2] = p[2];
+}
+__device__ __forceinline__ void ld_gd(const float *p, float g[3], float d[3])
+{
+	const float4 x = *reinterpret_cast<const float4 *>(p);
+	const float4 y = *reinterpret_cast<const float4 *>(p + 4);
+	g[0] = x.x;
+	g[1] = x.y;
+	g[2] = x.z;
+	d[0] = y.x;
+	d[1] = y.y;
+	d[2] = y.z;
+}
+__device__ __forceinline__ void ld_gd(const double *p, double g[3], double d[3])
+{
+	const double2 x = *reinterpret_cast<const double2 *>(p);
+	const double2 y = *reinterpret_cast<const double2 *>(p + 2);
+	const double2 z = *reinterpret_cast<const double2 *>(p + 4);
+	g[0] = x.x;
+	g[1] = x.y;
+	g[2] = y.x;
+	d[0] = y.y;
+	d[1] = z.x;
+	d[2] = z.y;
+}
+__device__ __forceinline__ void st_gd(float *p, const float g[3], const float d[3])
+{
+	*reinterpret_cast<float4 *>(p) = make_float4(g[0], g[1], g[2], 0.f);
+	*reinterpret_cast<float4 *>(p + 4) = make_float4(d[0], d[1], d[2], 0.f);
+}
+__device__ __forceinline__ void st_gd(double *p, const double g[3], const double d[3])
+{
+	*reinterpret_cast<double2 *>(p) = make_double2(g[0], g[1]);
+	*reinterpret_cast<double2 *>(p + 2) = make_double2(g[2], d[0]);
+	*reinterpret_cast<double2 *>(p + 4) = make_double2(d[1], d[2]);
+}
 
 // Record of one incidence (e, b): the 9n values H_e(3a+r, 3b+c), [a][c][r], padded to
 // whole 32-byte sectors so that records written at scattered positions stay full-sector.
@@ -447,7 +500,7 @@ struct EcTile
 	static constexpr int TE = (EL::ET == 1) ? 64 : (EL::ET == 2 ? 16 : 8);
 	static constexpr int NT = 128;
 	static constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ;
-	static constexpr int NP = N * (N + 1) / 2, NB = N * N, PQ = BlockKin<EL>::PER_Q;
+	static constexpr int NP = N * (N + 1) / 2, NB = N * N, PQ = BlockKin<EL, T>::PER_Q, NS = BlockKin<EL, T>::NS;
 };
 
 // K: arithmetic of the kinematics (J^-T, F, F^-T, g, d); T: arithmetic of the
@@ -456,11 +509,19 @@ template <class EL, class K, class T>
 struct EcSmem
 {
 	using TL = EcTile<EL, T>;
-	// one element's records per warp (record b padded to rec_pad values), then copied out in 16-byte vectors
-	__align__(16) T rec[TL::NT / 32][TL::N * rec_pad<EL, T>()];
+	// one element's records per warp, record b at b * RS (rec_pad values + 16 bytes, so
+	// that blocks of one row node in different records fall in different banks),
+	// then copied out in 16-byte vectors
+	static constexpr int RS = rec_pad<EL, T>() + 16 / (int)sizeof(T);
+	__align__(16) T rec[TL::NT / 32][TL::N * RS];
+	__align__(16) T kin[TL::TE][TL::NQ][TL::PQ];
 	K U[TL::TE][TL::N][3];
 	K X[TL::TE][TL::NG][3];
-	T kin[TL::TE][TL::NQ][TL::PQ];
+	// reference gradients of the FE and geometric bases and the weights, indexed at
+	// run time so that lanes at different quadrature points share one code path
+	K gtab[TL::NQ][TL::N][3];
+	K ggtab[EL::AFFINE ? 1 : TL::NQ][TL::NG][3];
+	double wq[TL::NQ];
 	int nodes[TL::TE][TL::N + TL::NG];
 	int sidx[TL::NT / 32][TL::N];   // incidence index of (e, b) for the warp's element
 	unsigned char pair_a[TL::NP], pair_b[TL::NP];
@@ -479,17 +540,39 @@ constexpr int blocks_min_ctas()
 }
 
 template <class EL, class K, class T>
-__global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>()) k_hessian_blocks(DevMesh m, const double *__restrict__ u, T *__restrict__ stage)
+__global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
+	k_hessian_blocks(DevMesh m, const double *__restrict__ u, T *__restrict__ stage, int e_begin, int e_end)
 {
 	using TL = EcTile<EL, T>;
 	constexpr int TE = TL::TE, NT = TL::NT, N = TL::N, NG = TL::NG, NQ = TL::NQ, NP = TL::NP;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	EcSmem<EL, K, T> &S = *reinterpret_cast<EcSmem<EL, K, T> *>(smem_raw);
 	const int tid = threadIdx.x;
-	const int e0 = blockIdx.x * TE;
-	const int ne = min(TE, m.E - e0);
+	const int e0 = e_begin + blockIdx.x * TE;
+	const int ne = min(TE, e_end - e0);
 
-	// phase 0: node-pair table, node ids (coalesced over the tile), then the gathers
+	// phase 0: basis tables, node-pair table, node ids (coalesced over the tile), then the gathers
+	constexpr int GQ = EL::AFFINE ? 1 : NQ;
+	if (tid < NQ)
+	{
+#pragma unroll
+		for (int qq = 0; qq < NQ; ++qq)
+		{
+			if (qq != tid) continue;
+#pragma unroll
+			for (int a = 0; a < N; ++a)
+#pragma unroll
+				for (int r = 0; r < 3; ++r) S.gtab[qq][a][r] = K(gref<EL>(qq, a, r));
+			if (qq < GQ)
+			{
+#pragma unroll
+				for (int j = 0; j < NG; ++j)
+#pragma unroll
+					for (int r = 0; r < 3; ++r) S.ggtab[qq][j][r] = K(ggref<EL>(qq, j, r));
+			}
+			S.wq[qq] = qweight<EL>(qq);
+		}
+	}
 	for (int p = tid; p < NP; p += NT)
 	{
 		int a = 0, r = p;
@@ -529,76 +612,88 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>()) k_hessian_bl
 		const int el = i / NQ, q = i % NQ;
 		const double2 lm = __ldg(m.lame + e0 + el);
 		T *Kq = S.kin[el][q];
+		const K(*gq)[3] = S.gtab[q];
+		const K(*gg)[3] = S.ggtab[EL::AFFINE ? 0 : q];
+		// geometry: J = sum_j grad(psi_j) (x) X_j, rows d/dxi_r (ElementAssemblyValues.cpp:88-93)
+		K Jac[3][3];
 #pragma unroll
-		for (int qq = 0; qq < NQ; ++qq)
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+			{
+				K s_ = K(0);
+#pragma unroll
+				for (int j = 0; j < NG; ++j) s_ += gg[j][r] * S.X[el][j][c];
+				Jac[r][c] = s_;
+			}
+		K Jit[3][3];
+		double detJ;
+		if constexpr (sizeof(K) == 8)
 		{
-			if (qq != q) continue;
-			K Jit[3][3];
-			double detJ;
-			geometry<EL, K>(qq, S.X[el], Jit, detJ);
-			K Ar[3][3];
+			detJ = det3(Jac);
+			inv_transpose3(Jac, K(detJ), Jit);
+		}
+		else
+		{
+			double Jd[3][3];
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
 #pragma unroll
-				for (int c = 0; c < 3; ++c)
-				{
-					K s_ = K(0);
+				for (int c = 0; c < 3; ++c) Jd[r][c] = double(Jac[r][c]);
+			detJ = det3(Jd);
+			inv_transpose3(Jac, K(detJ), Jit);
+		}
+		K Ar[3][3];
 #pragma unroll
-					for (int a = 0; a < N; ++a)
-					{
-						const double gr = gref<EL>(qq, a, c);
-						if (gr != 0.0) s_ += S.U[el][a][r] * K(gr);
-					}
-					Ar[r][c] = s_;
-				}
-			K F[3][3];
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+			{
+				K s_ = K(0);
+#pragma unroll
+				for (int a = 0; a < N; ++a) s_ += S.U[el][a][r] * gq[a][c];
+				Ar[r][c] = s_;
+			}
+		K F[3][3];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+				F[r][c] = Ar[r][0] * Jit[0][c] + Ar[r][1] * Jit[1][c] + Ar[r][2] * Jit[2][c] + (r == c ? K(1) : K(0));
+		double J;
+		if constexpr (sizeof(K) == 8)
+			J = det3(F);
+		else
+		{
+			double Fd[3][3];
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
 #pragma unroll
-				for (int c = 0; c < 3; ++c)
-					F[r][c] = Ar[r][0] * Jit[0][c] + Ar[r][1] * Jit[1][c] + Ar[r][2] * Jit[2][c] + (r == c ? K(1) : K(0));
-			double J;
-			if constexpr (sizeof(K) == 8)
-				J = det3(F);
-			else
+				for (int c = 0; c < 3; ++c) Fd[r][c] = F[r][c];
+			J = det3(Fd);
+		}
+		const double lj = log(J);
+		const double da = detJ * S.wq[q];
+		K FmT[3][3];
+		inv_transpose3(F, K(J), FmT);
+		Kq[0] = T(lm.y * da);
+		Kq[1] = T(lm.x * da);
+		Kq[2] = T((lm.y - lm.x * lj) * da);
+		Kq[3] = T(0);
+#pragma unroll
+		for (int a = 0; a < N; ++a)
+		{
+			K g[3];
+#pragma unroll
+			for (int c = 0; c < 3; ++c) g[c] = gq[a][0] * Jit[0][c] + gq[a][1] * Jit[1][c] + gq[a][2] * Jit[2][c];
+			T gt[3], dt[3];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
 			{
-				double Fd[3][3];
-#pragma unroll
-				for (int r = 0; r < 3; ++r)
-#pragma unroll
-					for (int c = 0; c < 3; ++c) Fd[r][c] = F[r][c];
-				J = det3(Fd);
+				gt[r] = T(g[r]);
+				dt[r] = T(FmT[r][0] * g[0] + FmT[r][1] * g[1] + FmT[r][2] * g[2]);
 			}
-			const double lj = log(J);
-			const double da = detJ * qweight<EL>(qq);
-			K FmT[3][3];
-			inv_transpose3(F, K(J), FmT);
-			Kq[0] = T(lm.y * da);
-			Kq[1] = T(lm.x * da);
-			Kq[2] = T((lm.y - lm.x * lj) * da);
-#pragma unroll
-			for (int a = 0; a < N; ++a)
-			{
-				K g[3];
-#pragma unroll
-				for (int c = 0; c < 3; ++c)
-				{
-					K s_ = K(0);
-#pragma unroll
-					for (int r = 0; r < 3; ++r)
-					{
-						const double gr = gref<EL>(qq, a, r);
-						if (gr != 0.0) s_ += K(gr) * Jit[r][c];
-					}
-					g[c] = s_;
-				}
-				T *dst = Kq + 3 + 6 * a;
-				dst[0] = T(g[0]);
-				dst[1] = T(g[1]);
-				dst[2] = T(g[2]);
-#pragma unroll
-				for (int r = 0; r < 3; ++r) dst[3 + r] = T(FmT[r][0] * g[0] + FmT[r][1] * g[1] + FmT[r][2] * g[2]);
-			}
+			st_gd(Kq + 4 + TL::NS * a, gt, dt);
 		}
 	}
 	__syncthreads();
@@ -624,12 +719,13 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>()) k_hessian_bl
 			for (int q = 0; q < NQ; ++q)
 			{
 				const T *Kq = S.kin[el][q];
-				const T *Ka = Kq + 3 + 6 * a, *Kb = Kq + 3 + 6 * b;
-				const T md = Kq[0] * (Ka[0] * Kb[0] + Ka[1] * Kb[1] + Ka[2] * Kb[2]);
-				const T sla = Kq[1], sga = Kq[2];
-				const T la[3] = {sla * Ka[3], sla * Ka[4], sla * Ka[5]};
-				const T gma[3] = {sga * Ka[3], sga * Ka[4], sga * Ka[5]};
-				const T db[3] = {Kb[3], Kb[4], Kb[5]};
+				T w[3], ga[3], gb[3], da[3], db[3];
+				ld_w(Kq, w);
+				ld_gd(Kq + 4 + TL::NS * a, ga, da);
+				ld_gd(Kq + 4 + TL::NS * b, gb, db);
+				const T md = w[0] * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+				const T la[3] = {w[1] * da[0], w[1] * da[1], w[1] * da[2]};
+				const T gma[3] = {w[2] * da[0], w[2] * da[1], w[2] * da[2]};
 #pragma unroll
 				for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -638,8 +734,9 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>()) k_hessian_bl
 				h[1][1] += md;
 				h[2][2] += md;
 			}
-			T *Hab = R + b * RP + a * 9; // block (a, b): record of column node b
-			T *Hba = R + a * RP + b * 9; // block (b, a): record of column node a
+			constexpr int RS = EcSmem<EL, K, T>::RS;
+			T *Hab = R + b * RS + a * 9; // block (a, b): record of column node b
+			T *Hba = R + a * RS + b * 9; // block (b, a): record of column node a
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -654,7 +751,7 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>()) k_hessian_bl
 		for (int i = lane; i < N * RV; i += 32)
 		{
 			const int b = i / RV, k = i - b * RV;
-			const uint4 v = reinterpret_cast<const uint4 *>(R + b * RP)[k];
+			const uint4 v = reinterpret_cast<const uint4 *>(R + b * EcSmem<EL, K, T>::RS)[k];
 			reinterpret_cast<uint4 *>(stage + (size_t)S.sidx[warp][b] * RP)[k] = v;
 		}
 		__syncwarp();
@@ -663,13 +760,13 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>()) k_hessian_bl
 
 // One warp per column node B.  Node B's records are one contiguous run of the
 // staging buffer; the warp's 3*deg(B) work items are the (row rank, column c)
-// triples of B's column block, column-major so that consecutive lanes write
-// consecutive CSC rows.  Each item sums, in FP64 and in incidence order, the
+// pairs of B's column block.  Each item sums, in FP64 and in incidence order, the
 // three values (rows 3*rank .. 3*rank+2 of column 3B+c) of every record block
 // that lands on its rank, read through the reduction plan, and writes them once.
 // No shared memory, no atomics: the sum order of every entry is fixed.
 template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 6) k_hessian_reduce(DevMesh m, DevPattern pat, const T *__restrict__ stage)
+__global__ void __launch_bounds__(WARPS * 32, 6)
+	k_hessian_reduce(DevMesh m, DevPattern pat, const T *__restrict__ stage)
 {
 	constexpr int N = EL::N, RP = rec_pad<EL, T>();
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -686,34 +783,42 @@ __global__ void __launch_bounds__(WARPS * 32, 6) k_hessian_reduce(DevMesh m, Dev
 	double *dst = pat.values + o0;
 	for (int it = lane; it < stride; it += 32)
 	{
-		const int c = it / deg, r = it - c * deg;
+		// (rank, column) items rank-major: the three items of the diagonal block,
+		// which has the longest contribution list, share one pass of the warp
+		const int r = it / 3, c = it - 3 * r;
 		const int k0 = __ldg(br + r);
 		const int k1 = (r + 1 < deg) ? (int)__ldg(br + r + 1) : tot;
 		double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-		int k = k0;
-		for (; k + 1 < k1; k += 2)
+		// two contributions per step, the next step's plan entries loaded ahead;
+		// the sum order stays k ascending
+		int qa = k0 < k1 ? (int)__ldg(cl + k0) : 0;
+		int qb = k0 + 1 < k1 ? (int)__ldg(cl + k0 + 1) : 0;
+		for (int k = k0; k < k1; k += 2)
 		{
-			const int q0 = __ldg(cl + k), q1 = __ldg(cl + k + 1);
+			const int q0 = qa, q1 = qb;
+			const bool two = k + 1 < k1;
+			qa = k + 2 < k1 ? (int)__ldg(cl + k + 2) : 0;
+			qb = k + 3 < k1 ? (int)__ldg(cl + k + 3) : 0;
 			const int sr0 = q0 / N, sr1 = q1 / N;
 			const T *p0 = rec + sr0 * RP + 9 * (q0 - sr0 * N) + 3 * c;
 			const T *p1 = rec + sr1 * RP + 9 * (q1 - sr1 * N) + 3 * c;
 			const T x0 = __ldg(p0), x1 = __ldg(p0 + 1), x2 = __ldg(p0 + 2);
-			const T y0 = __ldg(p1), y1 = __ldg(p1 + 1), y2 = __ldg(p1 + 2);
+			T y0 = T(0), y1 = T(0), y2 = T(0);
+			if (two)
+			{
+				y0 = __ldg(p1);
+				y1 = __ldg(p1 + 1);
+				y2 = __ldg(p1 + 2);
+			}
 			a0 += double(x0);
 			a1 += double(x1);
 			a2 += double(x2);
-			a0 += double(y0);
-			a1 += double(y1);
-			a2 += double(y2);
-		}
-		if (k < k1)
-		{
-			const int q0 = __ldg(cl + k);
-			const int sr0 = q0 / N;
-			const T *p0 = rec + sr0 * RP + 9 * (q0 - sr0 * N) + 3 * c;
-			a0 += double(__ldg(p0));
-			a1 += double(__ldg(p0 + 1));
-			a2 += double(__ldg(p0 + 2));
+			if (two)
+			{
+				a0 += double(y0);
+				a1 += double(y1);
+				a2 += double(y2);
+			}
 		}
 		double *d = dst + c * stride + 3 * r;
 		d[0] = a0;
@@ -726,13 +831,13 @@ template <class EL, class K, class T>
 static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const double *u, void *stage_v, cudaStream_t s)
 {
 	using TL = EcTile<EL, T>;
+	constexpr int WARPS = 8;
 	T *stage = static_cast<T *>(stage_v);
 	const size_t bytes1 = sizeof(EcSmem<EL, K, T>);
 	cudaError_t e = cudaFuncSetAttribute(k_hessian_blocks<EL, K, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes1);
 	if (e != cudaSuccess) return e;
 	const int nb = (m.E + TL::TE - 1) / TL::TE;
-	if (nb > 0) k_hessian_blocks<EL, K, T><<<nb, TL::NT, bytes1, s>>>(m, u, stage);
-	constexpr int WARPS = 8;
+	if (nb > 0) k_hessian_blocks<EL, K, T><<<nb, TL::NT, bytes1, s>>>(m, u, stage, 0, m.E);
 	const int ng = (m.N + WARPS - 1) / WARPS;
 	if (ng > 0) k_hessian_reduce<EL, T, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
 	return cudaGetLastError();

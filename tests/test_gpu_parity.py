@@ -242,3 +242,23 @@ def test_full_size_hessian_properties(require_gpu, which):
     g = asm.assemble_gradient(ud)
     assert float(torch.abs(g.view(-1, 3).sum(0)).max()) <= 1e-9 * float(torch.abs(g).max())
     asm.close()
+
+
+@pytest.mark.parametrize("et,g", [(M.P1_TET, 26), (M.P2_TET, 16), (M.Q1_HEX, 32)], ids=["P1-26", "P2-16", "Q1-32"])
+def test_medium_mesh_hessian_against_oracle(require_gpu, et, g):
+    """Medium meshes (20k-105k elements, many CTAs and warps of both Hessian
+    passes): pattern bit-exact, FP64 and split32 values within their bounds, and
+    every call bitwise identical."""
+    mesh, lam, mu, u, _ = make_case(et, g, seed=31, jitter=0.1 if et != M.P1_TET else 0.0)
+    orc = Oracle(mesh, lam, mu, n_threads=8, fast_pattern=True)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    o, i, v = orc.hessian(u)
+    outer, inner = asm.hessian_pattern()
+    assert np.array_equal(outer, o) and np.array_equal(inner, i)
+    h64 = asm.assemble_hessian_values(u, "fp64")
+    assert rel_err(h64, v) <= TOL64
+    assert np.array_equal(h64, asm.assemble_hessian_values(u, "fp64"))
+    hs = asm.assemble_hessian_values(u, "split32")
+    assert rel_err(hs, v) <= 1e-6
+    assert np.array_equal(hs, asm.assemble_hessian_values(u, "split32"))
+    asm.close()
