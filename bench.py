@@ -6,8 +6,8 @@ split 6 tets/hex (384,000 elements, 531,441 nodes, 1,594,323 dofs, 134,475,849
 CSC nonzeros), 4-point quadrature, per-element lognormal Lame parameters, seeded
 synthetic displacement u = 0.02 h N(0,1).  One step = one assembly of the global
 Hessian CSC values through the path's C ABI (pfg_hessian), which launches two
-kernels: k_hessian_blocks (element blocks -> node-ordered records) and
-k_hessian_gather (records -> CSC columns).
+kernels: k_hessian_blocks (element blocks -> node-ordered records) and a
+reduction kernel (records -> CSC columns, summed per entry in a fixed order).
 
   value     : split-precision Hessian assembly, inputs resident in HBM (elements/s)
   e2e       : the same call with host buffers (pinned u in, CSC values out) (elements/s)
@@ -89,7 +89,7 @@ class ClockSampler:
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
                0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, cuda_index: int, period_s: float = 0.005):
+    def __init__(self, cuda_index: int, period_s: float = 0.001):
         self.cuda_index = cuda_index
         self.period = period_s
         self.samples = []   # (sm_mhz, max_mhz, reasons bitmask)
@@ -402,8 +402,9 @@ def run_gpu(args):
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "bytes_alg_per_launch": bytes_alg,
                          "staged_bytes_per_launch": staged_bytes(mesh, nnz, rec_bytes),
-                         "note": "one pfg_hessian call = k_hessian_blocks + k_hessian_gather, CUDA events "
-                                 "on the context's stream; frac of measured HBM copy bandwidth"},
+                         "note": "one pfg_hessian call = k_hessian_blocks + the reduction kernel, CUDA events "
+                                 "on the context's stream; frac of measured HBM copy bandwidth; traffic = ncu "
+                                 "DRAM bytes per element of the 24^3 capture x elements"},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": 2 * args.steps,

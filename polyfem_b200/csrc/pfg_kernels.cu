@@ -765,7 +765,7 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 // that lands on its rank, read through the reduction plan, and writes them once.
 // No shared memory, no atomics: the sum order of every entry is fixed.
 template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 6)
+__global__ void __launch_bounds__(WARPS * 32, 8)
 	k_hessian_reduce(DevMesh m, DevPattern pat, const T *__restrict__ stage)
 {
 	constexpr int N = EL::N, RP = rec_pad<EL, T>();
