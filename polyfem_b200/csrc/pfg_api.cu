@@ -142,7 +142,7 @@ int ensure_vec_stage(pfg_context *c)
 {
 	if (!c->d_vec_stage)
 	{
-		const size_t n = (size_t)std::max(c->m.E, 1) * std::max(c->n, c->ng) * 3;
+		const size_t n = (size_t)std::max(c->m.E, 1) * std::max(c->n, c->ng) * 4;
 		PFG_CUDA(c, cudaMalloc(&c->d_vec_stage, n * sizeof(double)));
 	}
 	c->sc.vec_stage = c->d_vec_stage;

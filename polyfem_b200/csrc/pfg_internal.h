@@ -59,7 +59,7 @@ struct Scratch
 	unsigned int *ticket = nullptr;   // last-block-done counter (returns to 0 after each launch)
 	unsigned long long *inverted = nullptr;
 	int max_blocks = 0;
-	double *vec_stage = nullptr;      // [E][max(n, n_g)][3] element gradient / shape contributions
+	double *vec_stage = nullptr;      // [E][max(n, n_g)][4] element gradient / shape contributions (32-byte slots)
 	void *hess_stage = nullptr;       // one padded record of 9n block values per incidence (FP64 or FP32)
 };
 
@@ -72,7 +72,7 @@ cudaError_t launch_energy(const DevMesh &m, const double *u, int prec, bool per_
 						  const Scratch &sc, cudaStream_t s);
 cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double *g, const Scratch &sc,
 							cudaStream_t s);
-// vec_stage must hold E*max(n, n_g)*3 doubles
+// vec_stage must hold E*max(n, n_g)*4 doubles
 cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, void *stage, cudaStream_t s);
 cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double *adj, double *out, cudaStream_t s);
 cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out,

@@ -112,6 +112,13 @@ __device__ __forceinline__ void disp_grad(const T U[EL::N][3], const T gphi[EL::
 		}
 }
 
+// one 32-byte staging slot (one DRAM sector): (x, y, z, 0) in two 16-byte stores
+__device__ __forceinline__ void st_slot(double *p, double x, double y, double z)
+{
+	reinterpret_cast<double2 *>(p)[0] = make_double2(x, y);
+	reinterpret_cast<double2 *>(p)[1] = make_double2(z, 0.0);
+}
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll
@@ -243,8 +250,15 @@ __device__ __forceinline__ double element_energy(const DevMesh &m, const double 
 	return en;
 }
 
+// P1 elements are small enough for four 256-thread CTAs per SM (64 registers)
+template <class EL>
+constexpr int elem_kernel_min_ctas()
+{
+	return EL::ET == 1 ? 4 : 1;
+}
+
 template <class EL, class T, int NT>
-__global__ void __launch_bounds__(NT) k_energy(DevMesh m, const double *__restrict__ u, double *__restrict__ partials,
+__global__ void __launch_bounds__(NT, elem_kernel_min_ctas<EL>()) k_energy(DevMesh m, const double *__restrict__ u, double *__restrict__ partials,
 											   double *__restrict__ result, unsigned int *ticket,
 											   unsigned long long *inverted)
 {
@@ -356,12 +370,10 @@ __global__ void __launch_bounds__(NT) k_gradient(DevMesh m, const double *__rest
 			}
 	}
 	if (bad) atomicAdd(inverted, 1ull);
-	// the element's contributions, contiguous: stage[e][a][d]
-	double *dst = stage + (size_t)e * EL::N * 3;
+	// the element's contributions, one 32-byte slot per (e, a): stage[e][a][0..2], [3] = 0
+	double *dst = stage + (size_t)e * EL::N * 4;
 #pragma unroll
-	for (int a = 0; a < EL::N; ++a)
-#pragma unroll
-		for (int d = 0; d < 3; ++d) dst[a * 3 + d] = double(Gacc[a][d]);
+	for (int a = 0; a < EL::N; ++a) st_slot(dst + a * 4, double(Gacc[a][0]), double(Gacc[a][1]), double(Gacc[a][2]));
 }
 
 // Per node: the sum of its incidences' contributions in incidence (element) order
@@ -387,10 +399,11 @@ __global__ void __launch_bounds__(NT) k_vec_gather(int n_nodes, const int *__res
 		{
 			if (idx[j] >= 0)
 			{
-				const double *p = stage + (size_t)idx[j] * 3;
-				v[j][0] = __ldg(p);
-				v[j][1] = __ldg(p + 1);
-				v[j][2] = __ldg(p + 2);
+				const double2 *p = reinterpret_cast<const double2 *>(stage + (size_t)idx[j] * 4);
+				const double2 x = __ldg(p), y = __ldg(p + 1);
+				v[j][0] = x.x;
+				v[j][1] = x.y;
+				v[j][2] = y.x;
 			}
 		}
 #pragma unroll
@@ -494,14 +507,116 @@ __host__ __device__ constexpr int rec_pad()
 	return (((9 * EL::N * (int)sizeof(T)) + 31) / 32) * 32 / (int)sizeof(T);
 }
 
+// elements per tile of k_hessian_blocks (four warps, each takes a quarter)
+#ifndef PFG_TE_P1
+#define PFG_TE_P1 64
+#endif
+#ifndef PFG_TE_P2
+#define PFG_TE_P2 16
+#endif
+#ifndef PFG_TE_Q1
+#define PFG_TE_Q1 8
+#endif
 template <class EL, class T>
 struct EcTile
 {
-	static constexpr int TE = (EL::ET == 1) ? 64 : (EL::ET == 2 ? 16 : 8);
+	static constexpr int TE = (EL::ET == 1) ? PFG_TE_P1 : (EL::ET == 2 ? PFG_TE_P2 : PFG_TE_Q1);
 	static constexpr int NT = 128;
 	static constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ;
 	static constexpr int NP = N * (N + 1) / 2, NB = N * N, PQ = BlockKin<EL, T>::PER_Q, NS = BlockKin<EL, T>::NS;
 };
+
+// g_a = grad(phi_a) J^-T and d_a = F^-T g_a in K, stored rounded to T at dst
+template <class EL, class K, class T>
+__device__ __forceinline__ void node_kin(const K gr[3], const K Jit[3][3], const K FmT[3][3], T *dst)
+{
+	K g[3];
+#pragma unroll
+	for (int c = 0; c < 3; ++c) g[c] = gr[0] * Jit[0][c] + gr[1] * Jit[1][c] + gr[2] * Jit[2][c];
+	T gt[3], dt[3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+	{
+		gt[r] = T(g[r]);
+		dt[r] = T(FmT[r][0] * g[0] + FmT[r][1] * g[1] + FmT[r][2] * g[2]);
+	}
+	st_gd(dst, gt, dt);
+}
+
+// Block of node pair (a, b) of one element from its per-point kinematics:
+//   h[r][c] = sum_q [ mu da (g_a.g_b) delta_rc + lambda da d_a[r] d_b[c] + (mu - lambda lnJ) da d_b[r] d_a[c] ]
+// In FP32 the row pairs (0,1) of every column and the column pair (0,1) of row
+// 2's partner are updated with packed FP32x2 FMAs; each entry sees the same
+// operations in the same order as the scalar form.
+template <class EL, class T>
+__device__ __forceinline__ void block_pair(const T (*kin)[BlockKin<EL, T>::PER_Q], int a, int b, T h[3][3])
+{
+	constexpr int NS = BlockKin<EL, T>::NS;
+#pragma unroll
+	for (int r = 0; r < 3; ++r) h[r][0] = h[r][1] = h[r][2] = T(0);
+	if constexpr (sizeof(T) == 4)
+	{
+		float2 h0 = make_float2(0.f, 0.f), h1 = h0, hc = h0; // (h00,h01) (h10,h11) (h02,h12)
+		float h20 = 0.f, h21 = 0.f, h22 = 0.f;
+#pragma unroll
+		for (int q = 0; q < EL::NQ; ++q)
+		{
+			const T *Kq = kin[q];
+			T w[3], ga[3], gb[3], da[3], db[3];
+			ld_w(Kq, w);
+			ld_gd(Kq + 4 + NS * a, ga, da);
+			ld_gd(Kq + 4 + NS * b, gb, db);
+			const float md = w[0] * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+			const float la0 = w[1] * da[0], la1 = w[1] * da[1], la2 = w[1] * da[2];
+			const float gm0 = w[2] * da[0], gm1 = w[2] * da[1], gm2 = w[2] * da[2];
+			const float2 db01 = make_float2(db[0], db[1]), gm01 = make_float2(gm0, gm1);
+			// rows 0 and 1, columns 0 and 1
+			h0 = __ffma2_rn(make_float2(db[0], db[0]), gm01, __ffma2_rn(make_float2(la0, la0), db01, h0));
+			h1 = __ffma2_rn(make_float2(db[1], db[1]), gm01, __ffma2_rn(make_float2(la1, la1), db01, h1));
+			// column 2 of rows 0 and 1
+			hc = __ffma2_rn(make_float2(db[0], db[1]), make_float2(gm2, gm2),
+							__ffma2_rn(make_float2(la0, la1), make_float2(db[2], db[2]), hc));
+			// row 2
+			h20 = fmaf(db[2], gm0, fmaf(la2, db[0], h20));
+			h21 = fmaf(db[2], gm1, fmaf(la2, db[1], h21));
+			h22 = fmaf(db[2], gm2, fmaf(la2, db[2], h22));
+			h0.x += md;
+			h1.y += md;
+			h22 += md;
+		}
+		h[0][0] = h0.x;
+		h[0][1] = h0.y;
+		h[1][0] = h1.x;
+		h[1][1] = h1.y;
+		h[0][2] = hc.x;
+		h[1][2] = hc.y;
+		h[2][0] = h20;
+		h[2][1] = h21;
+		h[2][2] = h22;
+	}
+	else
+	{
+#pragma unroll
+		for (int q = 0; q < EL::NQ; ++q)
+		{
+			const T *Kq = kin[q];
+			T w[3], ga[3], gb[3], da[3], db[3];
+			ld_w(Kq, w);
+			ld_gd(Kq + 4 + NS * a, ga, da);
+			ld_gd(Kq + 4 + NS * b, gb, db);
+			const T md = w[0] * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+			const T la[3] = {w[1] * da[0], w[1] * da[1], w[1] * da[2]};
+			const T gma[3] = {w[2] * da[0], w[2] * da[1], w[2] * da[2]};
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c) h[r][c] = fma(db[r], gma[c], fma(la[r], db[c], h[r][c]));
+			h[0][0] += md;
+			h[1][1] += md;
+			h[2][2] += md;
+		}
+	}
+}
 
 // K: arithmetic of the kinematics (J^-T, F, F^-T, g, d); T: arithmetic of the
 // contraction and the records (g, d and the weights are stored rounded to T)
@@ -551,7 +666,7 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 	const int e0 = e_begin + blockIdx.x * TE;
 	const int ne = min(TE, e_end - e0);
 
-	// phase 0: basis tables, node-pair table, node ids (coalesced over the tile), then the gathers
+	// basis tables and node-pair table, shared by the CTA's warps
 	constexpr int GQ = EL::AFFINE ? 1 : NQ;
 	if (tid < NQ)
 	{
@@ -584,32 +699,47 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 		S.pair_a[p] = (unsigned char)a;
 		S.pair_b[p] = (unsigned char)(a + r);
 	}
-	for (int i = tid; i < TE * (N + NG); i += NT)
-	{
-		const int j = i / TE, el = i % TE, e = e0 + el;
-		int v = 0;
-		if (el < ne) v = (j < N) ? __ldg(m.conn + (size_t)j * m.E + e) : __ldg(m.gconn + (size_t)(j - N) * m.E + e);
-		S.nodes[el][j] = v;
-	}
-	__syncthreads();
-	for (int i = tid; i < TE * N * 3; i += NT)
-	{
-		const int el = i / (N * 3), a = (i / 3) % N, d = i % 3;
-		S.U[el][a][d] = (el < ne) ? K(__ldg(u + (size_t)S.nodes[el][a] * 3 + d)) : K(0);
-	}
-	for (int i = tid; i < TE * NG * 3; i += NT)
-	{
-		const int el = i / (NG * 3), j = (i / 3) % NG, d = i % 3;
-		S.X[el][j][d] = (el < ne) ? K(__ldg(m.X + (size_t)S.nodes[el][N + j] * 3 + d)) : K(0);
-	}
 	__syncthreads();
 
-	// phase 1: per (element, quadrature point): J^-T, F, det/log J and F^-T in K,
-	// then the weights and, for every local node, g_a = grad(phi_a) J^-T and
-	// d_a = F^-T g_a, stored rounded to T
-	for (int i = tid; i < ne * NQ; i += NT)
+	// From here each warp runs its own WE elements of the tile end to end (gathers,
+	// kinematics, blocks, records) with warp-level synchronisation only, so the
+	// warps of a CTA overlap one another's memory waits.
+	constexpr int WPC = NT / 32, WE = TE / WPC;
+	static_assert(TE % WPC == 0, "tile must split evenly over the warps");
+	const int warp = tid >> 5, lane = tid & 31;
+	const int w0 = warp * WE;
+	const int wn = max(0, min(WE, ne - w0));
+	for (int i = lane; i < WE * (N + NG); i += 32)
 	{
-		const int el = i / NQ, q = i % NQ;
+		const int j = i / WE, el = w0 + i % WE, e = e0 + el;
+		int v = 0;
+		if (el - w0 < wn) v = (j < N) ? __ldg(m.conn + (size_t)j * m.E + e) : __ldg(m.gconn + (size_t)(j - N) * m.E + e);
+		S.nodes[el][j] = v;
+	}
+	__syncwarp();
+	for (int i = lane; i < WE * N * 3; i += 32)
+	{
+		const int el = w0 + i / (N * 3), a = (i / 3) % N, d = i % 3;
+		S.U[el][a][d] = (el - w0 < wn) ? K(__ldg(u + (size_t)S.nodes[el][a] * 3 + d)) : K(0);
+	}
+	for (int i = lane; i < WE * NG * 3; i += 32)
+	{
+		const int el = w0 + i / (NG * 3), j = (i / 3) % NG, d = i % 3;
+		S.X[el][j][d] = (el - w0 < wn) ? K(__ldg(m.X + (size_t)S.nodes[el][N + j] * 3 + d)) : K(0);
+	}
+	__syncwarp();
+
+	// per (element, quadrature point): J^-T, F, det/log J and F^-T in K, then the
+	// weights and, for every local node, g_a = grad(phi_a) J^-T and d_a = F^-T g_a,
+	// stored rounded to T.  When J^-T and F^-T of the warp's points fit in its
+	// (still unused) record buffer, the per-node vectors are a second step over
+	// (element, point, node) so that every lane has work.
+	constexpr bool SPLIT_KIN =
+		(size_t)WE * NQ * 18 * sizeof(K) <= (size_t)N * EcSmem<EL, K, T>::RS * sizeof(T);
+	K *JF = reinterpret_cast<K *>(S.rec[warp]); // [WE * NQ][18]: J^-T, then F^-T
+	for (int i = lane; i < wn * NQ; i += 32)
+	{
+		const int el = w0 + i / NQ, q = i % NQ;
 		const double2 lm = __ldg(m.lame + e0 + el);
 		T *Kq = S.kin[el][q];
 		const K(*gq)[3] = S.gtab[q];
@@ -680,60 +810,62 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 		Kq[1] = T(lm.x * da);
 		Kq[2] = T((lm.y - lm.x * lj) * da);
 		Kq[3] = T(0);
-#pragma unroll
-		for (int a = 0; a < N; ++a)
+		if constexpr (SPLIT_KIN)
 		{
-			K g[3];
-#pragma unroll
-			for (int c = 0; c < 3; ++c) g[c] = gq[a][0] * Jit[0][c] + gq[a][1] * Jit[1][c] + gq[a][2] * Jit[2][c];
-			T gt[3], dt[3];
+			K *jf = JF + i * 18;
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
-			{
-				gt[r] = T(g[r]);
-				dt[r] = T(FmT[r][0] * g[0] + FmT[r][1] * g[1] + FmT[r][2] * g[2]);
-			}
-			st_gd(Kq + 4 + TL::NS * a, gt, dt);
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+				{
+					jf[r * 3 + c] = Jit[r][c];
+					jf[9 + r * 3 + c] = FmT[r][c];
+				}
+		}
+		else
+		{
+#pragma unroll
+			for (int a = 0; a < N; ++a) node_kin<EL, K, T>(gq[a], Jit, FmT, Kq + 4 + TL::NS * a);
 		}
 	}
-	__syncthreads();
+	__syncwarp();
+	if constexpr (SPLIT_KIN)
+	{
+		// g_a and d_a of every (element, point, node) of the warp, all lanes busy
+		for (int t = lane; t < wn * NQ * N; t += 32)
+		{
+			const int iq = t / N, a = t - iq * N;
+			const int el = w0 + iq / NQ, q = iq % NQ;
+			const K *jf = JF + iq * 18;
+			K Jit[3][3], FmT[3][3];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+				{
+					Jit[r][c] = jf[r * 3 + c];
+					FmT[r][c] = jf[9 + r * 3 + c];
+				}
+			node_kin<EL, K, T>(S.gtab[q][a], Jit, FmT, S.kin[el][q] + 4 + TL::NS * a);
+		}
+		__syncwarp();
+	}
 
-	// phase 2: each warp takes whole elements: symmetric node pairs into the warp's
+	// blocks: the warp takes its elements one at a time: symmetric node pairs into the warp's
 	// record buffer (H_ba = H_ab^T alongside), then the element's n records are
 	// written out, record b = H_e(3a+r, 3b+c) as [a][c][r], to the incidence's
 	// position in node order, in 16-byte vectors (the padding travels along)
 	constexpr int RP = rec_pad<EL, T>();
 	constexpr int VW = 16 / (int)sizeof(T), RV = RP / VW;
 	static_assert(RP % VW == 0, "records must be whole 16-byte vectors");
-	const int warp = tid >> 5, lane = tid & 31;
 	T *R = S.rec[warp];
-	for (int el = warp; el < ne; el += NT / 32)
+	for (int el = w0; el < w0 + wn; ++el)
 	{
 		for (int p0 = lane; p0 < NP; p0 += 32)
 		{
 			const int a = S.pair_a[p0], b = S.pair_b[p0];
 			T h[3][3];
-#pragma unroll
-			for (int r = 0; r < 3; ++r) h[r][0] = h[r][1] = h[r][2] = T(0);
-#pragma unroll
-			for (int q = 0; q < NQ; ++q)
-			{
-				const T *Kq = S.kin[el][q];
-				T w[3], ga[3], gb[3], da[3], db[3];
-				ld_w(Kq, w);
-				ld_gd(Kq + 4 + TL::NS * a, ga, da);
-				ld_gd(Kq + 4 + TL::NS * b, gb, db);
-				const T md = w[0] * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
-				const T la[3] = {w[1] * da[0], w[1] * da[1], w[1] * da[2]};
-				const T gma[3] = {w[2] * da[0], w[2] * da[1], w[2] * da[2]};
-#pragma unroll
-				for (int r = 0; r < 3; ++r)
-#pragma unroll
-					for (int c = 0; c < 3; ++c) h[r][c] = fma(db[r], gma[c], fma(la[r], db[c], h[r][c]));
-				h[0][0] += md;
-				h[1][1] += md;
-				h[2][2] += md;
-			}
+			block_pair<EL, T>(S.kin[el], a, b, h);
 			constexpr int RS = EcSmem<EL, K, T>::RS;
 			T *Hab = R + b * RS + a * 9; // block (a, b): record of column node b
 			T *Hba = R + a * RS + b * 9; // block (b, a): record of column node a
@@ -1036,11 +1168,9 @@ __global__ void __launch_bounds__(NT) k_shape_vjp(DevMesh m, const double *__res
 			}
 		}
 	}
-	double *dst = stage + (size_t)e * EL::NG * 3;
+	double *dst = stage + (size_t)e * EL::NG * 4;
 #pragma unroll
-	for (int v = 0; v < EL::NG; ++v)
-#pragma unroll
-		for (int d = 0; d < 3; ++d) dst[v * 3 + d] = double(acc[v][d]);
+	for (int v = 0; v < EL::NG; ++v) st_slot(dst + v * 4, double(acc[v][0]), double(acc[v][1]), double(acc[v][2]));
 }
 
 // ---------------------------------------------------------------------------
