@@ -470,6 +470,8 @@ def run_suite(args):
             "hessian_fp64": lambda: L.pfg_hessian(h, U, 1, 0, 0, None),
             "hessian_fp32": lambda: L.pfg_hessian(h, U, 1, 1, 0, None),
             "hessian_split32": lambda: L.pfg_hessian(h, U, 1, 2, 0, None),
+            "hessian_psd_fp64": lambda: L.pfg_hessian(h, U, 1, 0, 1, None),
+            "hessian_psd_split32": lambda: L.pfg_hessian(h, U, 1, 2, 1, None),
             "material_vjp": lambda: L.pfg_material_vjp(h, U, P, 1, O),
             "shape_vjp_fp64": lambda: L.pfg_shape_vjp(h, U, P, 1, 0, O),
             "shape_vjp_fp32": lambda: L.pfg_shape_vjp(h, U, P, 1, 1, O),

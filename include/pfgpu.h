@@ -129,7 +129,10 @@ int pfg_hessian_pattern_copy(pfg_context *ctx, int *outer, int *inner, int mem);
  * Builds the pattern on the first call.  Replaces NLAssembler::assemble_hessian
  * (assembler/Assembler.cpp:645-771) and the later-call branch of
  * SparseMatrixCache (utils/MatrixCache.cpp:88-113, 214-225).
- * project_psd must be 0 (ipc::project_to_psd is not implemented). */
+ * project_psd != 0 projects every element matrix onto the PSD cone before the
+ * scatter, as ipc::project_to_psd (CLAMP) does at Assembler.cpp:693-694: an
+ * element whose smallest eigenvalue is > 0 is kept as it is, otherwise it
+ * becomes V max(l, 0) V^T (eigendecomposition in FP64 on the device). */
 int pfg_hessian(pfg_context *ctx, const double *u, int mem, int prec, int project_psd, double *values);
 
 /* Device pointers of the context-owned CSC arrays (valid until pfg_destroy). */

@@ -37,6 +37,8 @@ def lib():
                                  ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_destroy.argtypes = [ctypes.c_void_p]
         L.orc_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_set_project_psd.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_project_psd.argtypes = [_d, ctypes.c_int]
         L.orc_energy.restype = ctypes.c_double
         L.orc_energy.argtypes = [ctypes.c_void_p, _d]
         L.orc_energy_per_element.argtypes = [ctypes.c_void_p, _d, _d]
@@ -118,9 +120,12 @@ class Oracle:
         lib().orc_gradient(self.h, _dp(u), _dp(g))
         return g
 
-    def hessian(self, u):
-        """Returns (outer, inner, values) of the CSC Hessian."""
+    def hessian(self, u, project_psd: bool = False):
+        """Returns (outer, inner, values) of the CSC Hessian; with project_psd every
+        element matrix is projected onto the PSD cone before the scatter
+        (Assembler.cpp:693-694)."""
         u = np.ascontiguousarray(u, dtype=np.float64)
+        lib().orc_set_project_psd(self.h, int(bool(project_psd)))
         nnz = lib().orc_hessian(self.h, _dp(u))
         if nnz < 0:
             raise RuntimeError("oracle hessian failed")
@@ -155,6 +160,13 @@ class Oracle:
         H = np.zeros((3 * n, 3 * n))
         lib().orc_element(self.h, int(e), _dp(u), _dp(en), _dp(g), _dp(H))
         return en[0], g, H
+
+
+def project_psd(H):
+    """ipc::project_to_psd (CLAMP) of one symmetric matrix, restated in the oracle."""
+    A = np.array(H, dtype=np.float64, order="C", copy=True)
+    lib().orc_project_psd(_dp(A), A.shape[0])
+    return A
 
 
 def tables(elem_type: int):

@@ -707,6 +707,7 @@ struct Context
 	std::vector<ElementValues> cache; // AssemblyValsCache
 	SparseMatrixCache mat_cache;
 	bool fast_pattern = false; // build the first-call pattern by sorting instead of triplets
+	bool project_psd = false;  // NLAssembler::assemble_hessian(project_to_psd = true)
 	CSC last;                  // last assembled Hessian
 	std::string err;
 
@@ -810,6 +811,89 @@ static void build_pattern_fast(Context &c)
 	}
 }
 
+// ---------------------------------------------------------------------------
+// ipc::project_to_psd with the default PSDProjectionMethod::CLAMP, as called by
+// NLAssembler::assemble_hessian (Assembler.cpp:693-694).  The function lives in
+// ipc-toolkit (commit b40e9c0, cmake/recipes/ipc_toolkit.cmake:11), which is not
+// part of the reference tree; its published algorithm is: eigendecompose the
+// symmetric element matrix A = V diag(l) V^T (eigenvalues ascending); if the
+// smallest eigenvalue is > 0 return A unchanged, else clamp every eigenvalue
+// <= 0 to 0 and return V diag(l) V^T.  The projection onto the PSD cone is
+// unique, so the eigensolver (Eigen's SelfAdjointEigenSolver there, cyclic
+// Jacobi here) only changes rounding.
+// ---------------------------------------------------------------------------
+static void jacobi_eigen(std::vector<double> &A, int m, std::vector<double> &V, std::vector<double> &lam)
+{
+	V.assign((size_t)m * m, 0.0);
+	for (int i = 0; i < m; ++i) V[(size_t)i * m + i] = 1.0;
+	for (int sweep = 0; sweep < 60; ++sweep)
+	{
+		double off = 0.0, tot = 0.0;
+		for (int i = 0; i < m; ++i)
+			for (int j = 0; j < m; ++j)
+			{
+				const double a = A[(size_t)i * m + j];
+				tot += a * a;
+				if (i != j) off += a * a;
+			}
+		if (!(off > 1e-32 * tot)) break; // also stops on NaN
+		for (int p = 0; p < m - 1; ++p)
+			for (int q = p + 1; q < m; ++q)
+			{
+				const double apq = A[(size_t)p * m + q];
+				if (apq == 0.0) continue;
+				const double app = A[(size_t)p * m + p], aqq = A[(size_t)q * m + q];
+				const double theta = (aqq - app) / (2.0 * apq);
+				const double t = std::fabs(theta) > 1e100
+									 ? 0.5 / theta
+									 : (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+				const double cc = 1.0 / std::sqrt(t * t + 1.0), ss = t * cc;
+				// A <- J^T A J with J = I except J_pp = J_qq = c, J_pq = s, J_qp = -s
+				for (int k = 0; k < m; ++k)
+				{
+					const double akp = A[(size_t)k * m + p], akq = A[(size_t)k * m + q];
+					A[(size_t)k * m + p] = cc * akp - ss * akq;
+					A[(size_t)k * m + q] = ss * akp + cc * akq;
+				}
+				for (int k = 0; k < m; ++k)
+				{
+					const double apk = A[(size_t)p * m + k], aqk = A[(size_t)q * m + k];
+					A[(size_t)p * m + k] = cc * apk - ss * aqk;
+					A[(size_t)q * m + k] = ss * apk + cc * aqk;
+				}
+				A[(size_t)p * m + q] = A[(size_t)q * m + p] = 0.0;
+				for (int k = 0; k < m; ++k)
+				{
+					const double vkp = V[(size_t)k * m + p], vkq = V[(size_t)k * m + q];
+					V[(size_t)k * m + p] = cc * vkp - ss * vkq;
+					V[(size_t)k * m + q] = ss * vkp + cc * vkq;
+				}
+			}
+	}
+	lam.resize(m);
+	for (int i = 0; i < m; ++i) lam[i] = A[(size_t)i * m + i];
+}
+
+// In place on the row-major m x m symmetric matrix H.
+static void project_to_psd(double *H, int m)
+{
+	std::vector<double> A(H, H + (size_t)m * m), V, lam;
+	jacobi_eigen(A, m, V, lam);
+	double lmin = lam[0];
+	for (int i = 1; i < m; ++i) lmin = std::min(lmin, lam[i]);
+	if (lmin > 0.0) return;
+	if (std::isnan(lmin)) return; // NaN input propagates unchanged
+	for (int i = 0; i < m; ++i)
+		if (lam[i] <= 0.0) lam[i] = 0.0;
+	for (int i = 0; i < m; ++i)
+		for (int j = 0; j < m; ++j)
+		{
+			double s = 0.0;
+			for (int k = 0; k < m; ++k) s += V[(size_t)i * m + k] * lam[k] * V[(size_t)j * m + k];
+			H[(size_t)i * m + j] = s;
+		}
+}
+
 template <int N>
 static void hessian_impl(Context &c, const double *x)
 {
@@ -834,6 +918,7 @@ static void hessian_impl(Context &c, const double *x)
 		{
 			c.vals(el, v);
 			element_hessian<N>(v, x, c.lambda[el], c.mu[el], H.data());
+			if (c.project_psd) project_to_psd(H.data(), ND);
 			for (int i = 0; i < N; ++i)
 				for (int j = 0; j < N; ++j)
 					for (int nn = 0; nn < 3; ++nn)
@@ -1043,6 +1128,10 @@ extern "C"
 	void orc_destroy(void *h) { delete static_cast<Context *>(h); }
 
 	void orc_set_threads(void *h, int n) { static_cast<Context *>(h)->n_threads = std::max(1, n); }
+	// later orc_hessian calls project every element matrix onto the PSD cone
+	void orc_set_project_psd(void *h, int on) { static_cast<Context *>(h)->project_psd = on != 0; }
+	// ipc::project_to_psd (CLAMP) of one row-major m x m symmetric matrix, in place
+	void orc_project_psd(double *H, int m) { project_to_psd(H, m); }
 
 	double orc_energy(void *h, const double *x)
 	{

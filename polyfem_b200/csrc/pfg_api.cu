@@ -628,7 +628,6 @@ int pfg_hessian(pfg_context *c, const double *u, int mem, int prec, int project_
 {
 	if (!c || !check_mem(mem) || !check_prec(prec)) return fail(c, PFG_ERR_INVALID, "bad arguments");
 	if (c->m.N && !u) return fail(c, PFG_ERR_INVALID, "u NULL");
-	if (project_psd) return fail(c, PFG_ERR_UNSUPPORTED, "project_to_psd is not implemented");
 	DeviceGuard g(c->device);
 	int st;
 	if (!c->has_pattern && (st = build_pattern(c))) return st;
@@ -639,7 +638,7 @@ int pfg_hessian(pfg_context *c, const double *u, int mem, int prec, int project_
 	// device output goes straight into the caller's array; otherwise into the context's
 	DevPattern p = c->pat;
 	if (values && mem == PFG_MEM_DEVICE) p.values = values;
-	PFG_CUDA(c, launch_hessian(c->m, p, du, prec, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
+	PFG_CUDA(c, launch_hessian(c->m, p, du, prec, project_psd, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
 	if (values && mem == PFG_MEM_HOST) return finish_host(c, values, c->d_values, c->pat.nnz);
 	if (mem == PFG_MEM_HOST) PFG_CUDA(c, cudaStreamSynchronize(c->stream));
 	return PFG_OK;

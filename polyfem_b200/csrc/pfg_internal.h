@@ -73,7 +73,9 @@ cudaError_t launch_energy(const DevMesh &m, const double *u, int prec, bool per_
 cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double *g, const Scratch &sc,
 							cudaStream_t s);
 // vec_stage must hold E*max(n, n_g)*4 doubles
-cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, void *stage, cudaStream_t s);
+// project_psd != 0: every element matrix is projected onto the PSD cone (ipc::project_to_psd, CLAMP) before the scatter
+cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, int project_psd,
+						   void *stage, cudaStream_t s);
 cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double *adj, double *out, cudaStream_t s);
 cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out,
 							 const Scratch &sc, cudaStream_t s);

@@ -959,8 +959,220 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 	}
 }
 
+// ---------------------------------------------------------------------------
+// ipc::project_to_psd (PSDProjectionMethod::CLAMP), applied to every element
+// matrix before the scatter when NLAssembler::assemble_hessian is called with
+// project_to_psd (Assembler.cpp:693-694).  The element matrix is rebuilt from its
+// n records, A[3a+r][3b+c] = record_b[9a + 3c + r], in FP64; a warp diagonalises
+// it with cyclic Jacobi in round-robin order (M/2 disjoint rotations per round,
+// M - 1 rounds per sweep, at most PSD_MAX_SWEEPS sweeps, stopping when the
+// off-diagonal squares fall below 1e-32 of all squares).  If the smallest
+// eigenvalue is > 0 (or NaN) the records are left as they are; otherwise
+// V max(l, 0) V^T is written back, rounded to the record type.
+// ---------------------------------------------------------------------------
+constexpr int PSD_MAX_SWEEPS = 40;
+
+template <class EL>
+struct PsdWarp
+{
+	static constexpr int M = 3 * EL::N, H = M / 2, LD = M + 1;
+	double A[M][LD];
+	double V[M][LD];
+	double c[H], s[H], t[H];
+	int p[H], q[H];
+	double d[M];
+};
+
+__device__ __forceinline__ double warp_allsum(double v)
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+__device__ __forceinline__ double warp_allmin(double v)
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+	return v;
+}
+
+template <class EL, class T, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_project_psd(DevMesh m, T *__restrict__ stage)
+{
+	using W = PsdWarp<EL>;
+	constexpr int N = EL::N, M = W::M, H = W::H, RP = rec_pad<EL, T>();
+	constexpr int NBP = H * (H + 1) / 2, BPL = (NBP + 31) / 32;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	W &S = reinterpret_cast<W *>(smem_raw)[threadIdx.x >> 5];
+	unsigned char *bp_P = smem_raw + WARPS * sizeof(W), *bp_Q = bp_P + NBP;
+	for (int k = threadIdx.x; k < NBP; k += WARPS * 32)
+	{
+		int P = 0, r = k;
+		while (r >= H - P)
+		{
+			r -= H - P;
+			++P;
+		}
+		bp_P[k] = (unsigned char)P;
+		bp_Q[k] = (unsigned char)(P + r);
+	}
+	__syncthreads();
+	const int lane = threadIdx.x & 31;
+	const int e = blockIdx.x * WARPS + (threadIdx.x >> 5);
+	if (e >= m.E) return;
+	int sidx[N];
+#pragma unroll
+	for (int b = 0; b < N; ++b) sidx[b] = __ldg(m.eb_inc + (size_t)e * N + b);
+#pragma unroll
+	for (int b = 0; b < N; ++b)
+	{
+		const T *rec = stage + (size_t)sidx[b] * RP;
+		for (int k = lane; k < 9 * N; k += 32)
+		{
+			const int a = k / 9, cc = (k % 9) / 3, r = k % 3;
+			S.A[3 * a + r][3 * b + cc] = double(rec[k]);
+		}
+	}
+	for (int k = lane; k < M * M; k += 32) S.V[k / M][k % M] = (k / M == k % M) ? 1.0 : 0.0;
+	__syncwarp();
+
+	for (int sweep = 0; sweep < PSD_MAX_SWEEPS; ++sweep)
+	{
+		double off = 0.0, tot = 0.0;
+		for (int k = lane; k < M * M; k += 32)
+		{
+			const int i = k / M, j = k % M;
+			const double a = S.A[i][j];
+			tot += a * a;
+			if (i != j) off += a * a;
+		}
+		off = warp_allsum(off);
+		tot = warp_allsum(tot);
+		if (!(off > 1e-32 * tot)) break; // converged (or NaN): the same decision on every lane
+		for (int round = 0; round < M - 1; ++round)
+		{
+			if (lane < H)
+			{
+				// circle method: position 0 fixed, positions 1..M-1 rotate with the round
+				const int x = lane == 0 ? 0 : ((lane - 1 + round) % (M - 1)) + 1;
+				const int y = ((M - 2 - lane + round) % (M - 1)) + 1;
+				const int pp = min(x, y), qq = max(x, y);
+				const double apq = S.A[pp][qq], app = S.A[pp][pp], aqq = S.A[qq][qq];
+				double cc = 1.0, ss = 0.0, tt = 0.0;
+				if (apq != 0.0)
+				{
+					const double theta = (aqq - app) / (2.0 * apq);
+					// t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)), ~ 1 / (2 theta) once theta^2 overflows
+					tt = fabs(theta) > 1e100 ? 0.5 / theta
+											 : (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+					cc = 1.0 / sqrt(tt * tt + 1.0);
+					ss = tt * cc;
+				}
+				S.p[lane] = pp;
+				S.q[lane] = qq;
+				S.c[lane] = cc;
+				S.s[lane] = ss;
+				S.t[lane] = tt;
+			}
+			__syncwarp();
+			// A <- J^T A J, one 2x2 block of pair rows P and pair columns Q (P <= Q) per item
+			double nb[BPL][4];
+#pragma unroll
+			for (int j = 0; j < BPL; ++j)
+			{
+				const int bp = lane + 32 * j;
+				if (bp >= NBP) continue;
+				const int P = bp_P[bp], Q = bp_Q[bp];
+				const int pP = S.p[P], qP = S.q[P], pQ = S.p[Q], qQ = S.q[Q];
+				if (P == Q)
+				{
+					const double apq = S.A[pP][qP];
+					nb[j][0] = S.A[pP][pP] - S.t[P] * apq;
+					nb[j][3] = S.A[qP][qP] + S.t[P] * apq;
+					nb[j][1] = nb[j][2] = 0.0;
+				}
+				else
+				{
+					const double cP = S.c[P], sP = S.s[P], cQ = S.c[Q], sQ = S.s[Q];
+					const double b00 = S.A[pP][pQ], b01 = S.A[pP][qQ], b10 = S.A[qP][pQ], b11 = S.A[qP][qQ];
+					const double l0 = cP * b00 - sP * b10, l1 = cP * b01 - sP * b11;
+					const double l2 = sP * b00 + cP * b10, l3 = sP * b01 + cP * b11;
+					nb[j][0] = cQ * l0 - sQ * l1;
+					nb[j][1] = sQ * l0 + cQ * l1;
+					nb[j][2] = cQ * l2 - sQ * l3;
+					nb[j][3] = sQ * l2 + cQ * l3;
+				}
+			}
+			__syncwarp();
+#pragma unroll
+			for (int j = 0; j < BPL; ++j)
+			{
+				const int bp = lane + 32 * j;
+				if (bp >= NBP) continue;
+				const int P = bp_P[bp], Q = bp_Q[bp];
+				const int pP = S.p[P], qP = S.q[P], pQ = S.p[Q], qQ = S.q[Q];
+				S.A[pP][pQ] = nb[j][0];
+				S.A[pP][qQ] = nb[j][1];
+				S.A[qP][pQ] = nb[j][2];
+				S.A[qP][qQ] = nb[j][3];
+				S.A[pQ][pP] = nb[j][0];
+				S.A[qQ][pP] = nb[j][1];
+				S.A[pQ][qP] = nb[j][2];
+				S.A[qQ][qP] = nb[j][3];
+			}
+			// V <- V J, columns p and q of every pair
+			for (int k = lane; k < M * H; k += 32)
+			{
+				const int i = k / H, P = k % H;
+				const int pp = S.p[P], qq = S.q[P];
+				const double cc = S.c[P], ss = S.s[P];
+				const double vp = S.V[i][pp], vq = S.V[i][qq];
+				S.V[i][pp] = cc * vp - ss * vq;
+				S.V[i][qq] = ss * vp + cc * vq;
+			}
+			__syncwarp();
+		}
+	}
+	double lmin = INFINITY;
+	for (int i = lane; i < M; i += 32) lmin = fmin(lmin, S.A[i][i]);
+	lmin = warp_allmin(lmin);
+	bool has_nan = false;
+	for (int i = lane; i < M; i += 32) has_nan |= isnan(S.A[i][i]);
+	has_nan = __any_sync(0xffffffffu, has_nan);
+	if (has_nan || lmin > 0.0) return; // records stay as they are
+	for (int i = lane; i < M; i += 32) S.d[i] = S.A[i][i] > 0.0 ? S.A[i][i] : 0.0;
+	__syncwarp();
+	for (int k = lane; k < M * (M + 1) / 2; k += 32)
+	{
+		int i = 0, r = k;
+		while (r >= M - i)
+		{
+			r -= M - i;
+			++i;
+		}
+		const int j = i + r;
+		double acc = 0.0;
+#pragma unroll 6
+		for (int l = 0; l < M; ++l) acc += S.V[i][l] * S.d[l] * S.V[j][l];
+		S.A[i][j] = acc;
+		S.A[j][i] = acc;
+	}
+	__syncwarp();
+#pragma unroll
+	for (int b = 0; b < N; ++b)
+	{
+		T *rec = stage + (size_t)sidx[b] * RP;
+		for (int k = lane; k < 9 * N; k += 32)
+		{
+			const int a = k / 9, cc = (k % 9) / 3, r = k % 3;
+			rec[k] = T(S.A[3 * a + r][3 * b + cc]);
+		}
+	}
+}
+
 template <class EL, class K, class T>
-static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const double *u, void *stage_v, cudaStream_t s)
+static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const double *u, void *stage_v,
+									bool project_psd, cudaStream_t s)
 {
 	using TL = EcTile<EL, T>;
 	constexpr int WARPS = 8;
@@ -970,6 +1182,15 @@ static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const
 	if (e != cudaSuccess) return e;
 	const int nb = (m.E + TL::TE - 1) / TL::TE;
 	if (nb > 0) k_hessian_blocks<EL, K, T><<<nb, TL::NT, bytes1, s>>>(m, u, stage, 0, m.E);
+	if (project_psd && m.E > 0)
+	{
+		constexpr int PW = 4;
+		constexpr int NBP = (PsdWarp<EL>::H * (PsdWarp<EL>::H + 1)) / 2;
+		const size_t bytes_p = PW * sizeof(PsdWarp<EL>) + 2 * NBP;
+		e = cudaFuncSetAttribute(k_project_psd<EL, T, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
+		if (e != cudaSuccess) return e;
+		k_project_psd<EL, T, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
+	}
 	const int ng = (m.N + WARPS - 1) / WARPS;
 	if (ng > 0) k_hessian_reduce<EL, T, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
 	return cudaGetLastError();
@@ -977,8 +1198,10 @@ static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const
 
 cudaError_t hessian_kernel_setup(int) { return cudaSuccess; }
 
-cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, void *stage, cudaStream_t s)
+cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, int project_psd,
+						   void *stage, cudaStream_t s)
 {
+	const bool psd = project_psd != 0;
 	if (p.nnz == 0) return cudaSuccess;
 	// FP64: everything in FP64.  FP32: everything in FP32 except det/log J.
 	// SPLIT32: kinematics (J^-T, F^-T, det/log J, g, d) in FP64, contraction and
@@ -986,17 +1209,17 @@ cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *
 	switch (m.et)
 	{
 	case 1:
-		return prec == PREC_FP64 ? hessian_two_pass<P1Tet, double, double>(m, p, u, stage, s)
-			 : prec == PREC_FP32 ? hessian_two_pass<P1Tet, float, float>(m, p, u, stage, s)
-								 : hessian_two_pass<P1Tet, double, float>(m, p, u, stage, s);
+		return prec == PREC_FP64 ? hessian_two_pass<P1Tet, double, double>(m, p, u, stage, psd, s)
+			 : prec == PREC_FP32 ? hessian_two_pass<P1Tet, float, float>(m, p, u, stage, psd, s)
+								 : hessian_two_pass<P1Tet, double, float>(m, p, u, stage, psd, s);
 	case 2:
-		return prec == PREC_FP64 ? hessian_two_pass<P2Tet, double, double>(m, p, u, stage, s)
-			 : prec == PREC_FP32 ? hessian_two_pass<P2Tet, float, float>(m, p, u, stage, s)
-								 : hessian_two_pass<P2Tet, double, float>(m, p, u, stage, s);
+		return prec == PREC_FP64 ? hessian_two_pass<P2Tet, double, double>(m, p, u, stage, psd, s)
+			 : prec == PREC_FP32 ? hessian_two_pass<P2Tet, float, float>(m, p, u, stage, psd, s)
+								 : hessian_two_pass<P2Tet, double, float>(m, p, u, stage, psd, s);
 	case 3:
-		return prec == PREC_FP64 ? hessian_two_pass<Q1Hex, double, double>(m, p, u, stage, s)
-			 : prec == PREC_FP32 ? hessian_two_pass<Q1Hex, float, float>(m, p, u, stage, s)
-								 : hessian_two_pass<Q1Hex, double, float>(m, p, u, stage, s);
+		return prec == PREC_FP64 ? hessian_two_pass<Q1Hex, double, double>(m, p, u, stage, psd, s)
+			 : prec == PREC_FP32 ? hessian_two_pass<Q1Hex, float, float>(m, p, u, stage, psd, s)
+								 : hessian_two_pass<Q1Hex, double, float>(m, p, u, stage, psd, s);
 	}
 	return cudaErrorInvalidValue;
 }

@@ -309,3 +309,33 @@ def _moved(mesh, v, d, h):
     m2.X = mesh.X.copy()
     m2.X[v, d] += h
     return m2
+
+
+# ------------------------------------------------------ project_to_psd (CLAMP)
+def test_project_psd_restatement_against_numpy_eigh():
+    """ipc::project_to_psd (CLAMP) restated in the oracle == V max(l, 0) V^T from
+    numpy's eigh; PSD matrices come back unchanged (bitwise)."""
+    from oracle.binding import project_psd
+    rng = np.random.default_rng(0)
+    for m in (12, 24, 30):
+        B = rng.standard_normal((m, m))
+        A = B + B.T
+        w, V = np.linalg.eigh(A)
+        ref = (V * np.maximum(w, 0.0)) @ V.T
+        P = project_psd(A)
+        assert np.linalg.norm(P - ref) <= 1e-13 * np.linalg.norm(ref)
+        assert np.allclose(P, P.T, rtol=0, atol=1e-13 * np.abs(P).max())
+        C = B @ B.T + np.eye(m)
+        assert np.array_equal(project_psd(C), C)
+
+
+def test_projected_oracle_hessian_is_psd():
+    from oracle.binding import Oracle
+    mesh, lam, mu, _, _ = make_case(M.P1_TET, 2, seed=3)
+    rng = np.random.default_rng(4)
+    u = (-0.3 * mesh.node_pos + 0.02 * mesh.h * rng.standard_normal(mesh.node_pos.shape)).ravel()
+    o, i, v = Oracle(mesh, lam, mu).hessian(u, project_psd=True)
+    import scipy.sparse as sp
+    H = sp.csc_matrix((v, i, o), shape=(mesh.n_dofs, mesh.n_dofs)).toarray()
+    w = np.linalg.eigvalsh(0.5 * (H + H.T))
+    assert w.min() >= -1e-10 * np.abs(w).max()
