@@ -484,6 +484,12 @@ def run_suite(args):
                "material_vjp": ins + mesh.n_nodes * 24 + 2 * E * 8,
                "hessian_fp64": algorithmic_bytes(mesh, nnz), "hessian_fp32": algorithmic_bytes(mesh, nnz),
                "hessian_split32": algorithmic_bytes(mesh, nnz)}
+        # Dirichlet reduction: the dofs of the x = 0 face constrained
+        face = np.flatnonzero(mesh.node_pos[:, 0] <= 1e-12)
+        asm.set_dirichlet((3 * face[:, None] + np.arange(3)).ravel())
+        L.pfg_set_stream(h, vp(stream.cuda_stream))
+        ops["hessian_dirichlet_split32"] = lambda: L.pfg_hessian_reduced(h, U, 1, 2, 0, None)
+        ops["hessian_dirichlet_fp64"] = lambda: L.pfg_hessian_reduced(h, U, 1, 0, 0, None)
         res = {}
         for op, fn in ops.items():
             for _ in range(3):

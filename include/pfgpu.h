@@ -163,6 +163,41 @@ const char *pfg_status_string(int status);
 int pfg_version(void);
 
 /* ---------------------------------------------------------------------------
+ * Dirichlet reduction.  When the only constraint form of the nonlinear problem
+ * is the Dirichlet one (BCLagrangianForm::can_project), NLProblem reduces the
+ * full quantities by dropping the constrained dofs:
+ *   Hessian:  BCLagrangianForm::project_hessian (BCLagrangianForm.cpp:165-212),
+ *             called from NLProblem::full_hessian_to_reduced_hessian
+ *             (solver/NLProblem.cpp:735-740);
+ *   gradient: BCLagrangianForm::project_gradient (BCLagrangianForm.cpp:149-155),
+ *             called from NLProblem::gradient (NLProblem.cpp:596-611);
+ *   x:        NLProblem::reduced_to_full (NLProblem.cpp:713-735): free dofs from
+ *             the reduced vector, constrained dofs from the boundary values.
+ * Free dofs keep their order (old_to_new is increasing).  The reduced Hessian is
+ * assembled directly in its reduced CSC (the full matrix is never written).
+ * ------------------------------------------------------------------------- */
+
+/* Constrained dof indices (host memory, any order, duplicates ignored); builds the
+ * reduced pattern (and the full one if needed).  n = 0: no dof constrained. */
+int pfg_set_dirichlet(pfg_context *ctx, const int *dofs, int n);
+
+/* Number of free dofs and nonzeros of the reduced Hessian. */
+int pfg_reduced_pattern(pfg_context *ctx, int *n_free, long long *nnz);
+
+/* Reduced CSC index arrays: outer (n_free+1) and inner (nnz) int32. */
+int pfg_reduced_pattern_copy(pfg_context *ctx, int *outer, int *inner, int mem);
+
+/* Reduced Hessian values (nnz doubles) at the full displacement u (3N doubles);
+ * values == NULL keeps them in the context.  project_psd as in pfg_hessian. */
+int pfg_hessian_reduced(pfg_context *ctx, const double *u, int mem, int prec, int project_psd, double *values);
+
+/* Gradient at the full displacement u, restricted to the free dofs (n_free doubles). */
+int pfg_gradient_reduced(pfg_context *ctx, const double *u, int mem, int prec, double *g);
+
+/* x (3N) from y (n_free) and x_bc (3N, read at the constrained dofs; NULL = 0). */
+int pfg_reduced_to_full(pfg_context *ctx, const double *y, const double *x_bc, int mem, double *x);
+
+/* ---------------------------------------------------------------------------
  * Allocation-free energy.  No counterpart in the reference: PolyFEM always
  * owns its memory.  It exists for callers that must not allocate device
  * memory at all (a host that pre-plans every byte, or runs inside a pool it

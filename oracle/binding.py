@@ -203,3 +203,46 @@ class SparseMatrixCache:
         if getattr(self, "h", None):
             lib().orc_smc_free(self.h)
             self.h = None
+
+
+def free_dofs(ndof: int, constrained):
+    """not_constraints_ / old_to_new_ of BCLagrangianForm (BCLagrangianForm.cpp:122-137)."""
+    is_c = np.zeros(ndof, dtype=bool)
+    is_c[np.asarray(constrained, dtype=np.int64)] = True
+    free = np.flatnonzero(~is_c).astype(np.int64)
+    old_to_new = np.full(ndof, -1, dtype=np.int64)
+    old_to_new[free] = np.arange(free.size)
+    return free, old_to_new
+
+
+def project_hessian(outer, inner, values, constrained):
+    """BCLagrangianForm::project_hessian (BCLagrangianForm.cpp:165-212), restated:
+    drop the constrained rows and columns of a ColMajor CSC matrix in one scan,
+    renumbering the free dofs in ascending order.  Returns (outer, inner, values)."""
+    ndof = len(outer) - 1
+    free, old_to_new = free_dofs(ndof, constrained)
+    r_outer = [0]
+    r_inner, r_vals = [], []
+    for k in free:
+        rows = inner[outer[k]:outer[k + 1]]
+        keep = old_to_new[rows] >= 0
+        r_inner.append(old_to_new[rows[keep]])
+        r_vals.append(values[outer[k]:outer[k + 1]][keep])
+        r_outer.append(r_outer[-1] + int(keep.sum()))
+    cat = lambda xs, dt: np.concatenate(xs).astype(dt) if xs else np.zeros(0, dtype=dt)
+    return np.asarray(r_outer, dtype=np.int32), cat(r_inner, np.int32), cat(r_vals, np.float64)
+
+
+def project_gradient(grad, constrained):
+    """BCLagrangianForm::project_gradient (BCLagrangianForm.cpp:149-155)."""
+    free, _ = free_dofs(len(grad), constrained)
+    return np.asarray(grad)[free]
+
+
+def reduced_to_full(y, x_bc, constrained):
+    """NLProblem::reduced_to_full for the projecting Dirichlet form (NLProblem.cpp:713-735):
+    free dofs from y, constrained dofs from the boundary values."""
+    x = np.array(x_bc, dtype=np.float64, copy=True)
+    free, _ = free_dofs(len(x), constrained)
+    x[free] = y
+    return x

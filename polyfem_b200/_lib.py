@@ -107,6 +107,12 @@ SIGNATURES = {
     "pfg_version": (ctypes.c_int, []),
     "pfg_energy_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp,
                                           _vp, ctypes.c_int, _vp, _vp]),
+    "pfg_set_dirichlet": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    "pfg_reduced_pattern": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]),
+    "pfg_reduced_pattern_copy": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    "pfg_hessian_reduced": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "pfg_gradient_reduced": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "pfg_reduced_to_full": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
 }
 
 

@@ -235,6 +235,65 @@ class NeoHookeanAssembler:
               "pfg_shape_vjp")
         return out
 
+    # -- Dirichlet reduction (NLProblem + BCLagrangianForm projection) ---------------
+    def set_dirichlet(self, dofs):
+        """Constrained dofs (BCLagrangianForm boundary_nodes_); builds the reduced pattern."""
+        d = np.ascontiguousarray(np.asarray(dofs, dtype=np.int32).ravel())
+        check(lib().pfg_set_dirichlet(self._h, ctypes.c_void_p(d.ctypes.data) if d.size else None, int(d.size)),
+              self._h, "pfg_set_dirichlet")
+        n = ctypes.c_int()
+        nnz = ctypes.c_longlong()
+        check(lib().pfg_reduced_pattern(self._h, ctypes.byref(n), ctypes.byref(nnz)), self._h, "pfg_reduced_pattern")
+        self.n_free = int(n.value)
+        self._red_nnz = int(nnz.value)
+
+    def reduced_pattern(self):
+        """CSC (outer, inner) of the reduced Hessian (BCLagrangianForm::project_hessian)."""
+        outer = np.empty(self.n_free + 1, dtype=np.int32)
+        inner = np.empty(self._red_nnz, dtype=np.int32)
+        check(lib().pfg_set_stream(self._h, None), self._h, "pfg_set_stream")
+        check(lib().pfg_reduced_pattern_copy(self._h, ctypes.c_void_p(outer.ctypes.data),
+                                             ctypes.c_void_p(inner.ctypes.data), PFG_MEM_HOST),
+              self._h, "pfg_reduced_pattern_copy")
+        return outer, inner
+
+    def assemble_hessian_reduced_values(self, u, precision="fp64", project_to_psd: bool = False):
+        """Values of the reduced Hessian at the full displacement u."""
+        self._check_len(u, self.n_dofs, "u")
+        mem, ptrs, keep = self._prepare(u)
+        out, optr = self._alloc(mem, self._red_nnz)
+        check(lib().pfg_hessian_reduced(self._h, ptrs[0], mem, _prec(precision), int(bool(project_to_psd)), optr),
+              self._h, "pfg_hessian_reduced")
+        return out
+
+    def assemble_hessian_reduced(self, u, precision="fp64", project_to_psd: bool = False):
+        """NLProblem::hessian's reduction: scipy CSC (host u) of size n_free."""
+        import scipy.sparse as sp
+        vals = self.assemble_hessian_reduced_values(u, precision, project_to_psd)
+        outer, inner = self.reduced_pattern()
+        if _is_device(vals):
+            vals = vals.cpu().numpy()
+        return sp.csc_matrix((vals, inner, outer), shape=(self.n_free, self.n_free))
+
+    def assemble_gradient_reduced(self, u, precision="fp64"):
+        """Gradient at the full u restricted to the free dofs (project_gradient)."""
+        self._check_len(u, self.n_dofs, "u")
+        mem, ptrs, keep = self._prepare(u)
+        out, optr = self._alloc(mem, self.n_free)
+        check(lib().pfg_gradient_reduced(self._h, ptrs[0], mem, _prec(precision), optr), self._h,
+              "pfg_gradient_reduced")
+        return out
+
+    def reduced_to_full(self, y, x_bc=None):
+        """Full x from the free-dof vector y and the boundary values x_bc (full size)."""
+        self._check_len(y, self.n_free, "y")
+        if x_bc is not None:
+            self._check_len(x_bc, self.n_dofs, "x_bc")
+        mem, ptrs, keep = self._prepare(y, x_bc)
+        out, optr = self._alloc(mem, self.n_dofs)
+        check(lib().pfg_reduced_to_full(self._h, ptrs[0], ptrs[1], mem, optr), self._h, "pfg_reduced_to_full")
+        return out
+
     def synchronize(self):
         check(lib().pfg_synchronize(self._h), self._h, "pfg_synchronize")
 

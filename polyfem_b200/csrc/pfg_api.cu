@@ -35,6 +35,15 @@ struct pfg_context
 	int *d_outer = nullptr, *d_inner = nullptr;
 	double *d_values = nullptr;
 	unsigned short *d_contrib = nullptr, *d_blk_rel = nullptr;
+	// Dirichlet reduction (pfg_set_dirichlet)
+	bool has_dirichlet = false;
+	std::vector<int> h_constrained;      // sorted unique constrained dofs
+	int n_free = 0;
+	long long red_nnz = 0;
+	int *d_old_to_new = nullptr, *d_free = nullptr, *d_red_col_start = nullptr, *d_red_outer = nullptr,
+		*d_red_inner = nullptr;
+	unsigned short *d_red_row_off = nullptr;
+	double *d_red_values = nullptr, *d_full_tmp = nullptr;
 	int *d_eb_inc = nullptr;
 	// node -> (element, local index) incidences, FE and geometric nodes
 	std::vector<long long> h_inc_off; // [N+1]
@@ -342,12 +351,107 @@ void build_incidence(const int *conn, int E, int n, int N, std::vector<long long
 		}
 }
 
+void free_dirichlet(pfg_context *c)
+{
+	void *rptrs[] = {c->d_old_to_new, c->d_free, c->d_red_col_start, c->d_red_outer, c->d_red_inner, c->d_red_row_off,
+					 c->d_red_values};
+	for (void *p : rptrs)
+		if (p) cudaFree(p);
+	c->d_old_to_new = c->d_free = c->d_red_col_start = c->d_red_outer = c->d_red_inner = nullptr;
+	c->d_red_row_off = nullptr;
+	c->d_red_values = nullptr;
+	c->has_dirichlet = false;
+	c->n_free = 0;
+	c->red_nnz = 0;
+}
+
+// Reduced pattern of BCLagrangianForm::project_hessian (BCLagrangianForm.cpp:165-212):
+// constrained rows and columns dropped, free dofs renumbered in ascending order
+// (old_to_new), each column keeping its free rows in ascending order.  Because a
+// node's three columns share one row set, the position of a kept row inside its
+// column is one 16-bit offset per (node, row slot).
+int build_dirichlet(pfg_context *c)
+{
+	const int N = c->m.N, ndof = 3 * N;
+	std::vector<int> old_to_new(ndof, 0), freev;
+	for (int d : c->h_constrained) old_to_new[d] = -1;
+	freev.reserve(ndof);
+	for (int i = 0; i < ndof; ++i)
+		if (old_to_new[i] == 0)
+		{
+			old_to_new[i] = (int)freev.size();
+			freev.push_back(i);
+		}
+		else
+			old_to_new[i] = -1;
+	const int n_free = (int)freev.size();
+	std::vector<int> outer(ndof + 1), inner((size_t)c->pat.nnz);
+	PFG_CUDA(c, cudaMemcpy(outer.data(), c->d_outer, sizeof(int) * (ndof + 1), cudaMemcpyDeviceToHost));
+	if (c->pat.nnz) PFG_CUDA(c, cudaMemcpy(inner.data(), c->d_inner, sizeof(int) * c->pat.nnz, cudaMemcpyDeviceToHost));
+	// row offsets per (node, row slot) and kept rows per node
+	std::vector<unsigned short> row_off((size_t)c->pat.nnz / 3);
+	std::vector<int> kept(N, 0);
+	for (int B = 0; B < N; ++B)
+	{
+		const int o0 = outer[3 * B], len = outer[3 * B + 1] - o0; // 3 * deg rows
+		int k = 0;
+		for (int j = 0; j < len; ++j)
+			row_off[(size_t)o0 / 3 + j] = old_to_new[inner[(size_t)o0 + j]] >= 0 ? (unsigned short)k++ : (unsigned short)0xFFFF;
+		kept[B] = k;
+	}
+	std::vector<int> col_start(ndof, -1), red_outer(n_free + 1, 0);
+	long long pos = 0;
+	for (int i = 0; i < n_free; ++i)
+	{
+		const int col = freev[i];
+		if (pos > 0x7fffffffLL) return fail(c, PFG_ERR_UNSUPPORTED, "reduced Hessian has more than 2^31-1 nonzeros");
+		col_start[col] = (int)pos;
+		red_outer[i] = (int)pos;
+		pos += kept[col / 3];
+	}
+	red_outer[n_free] = (int)pos;
+	std::vector<int> red_inner((size_t)pos);
+	for (int i = 0; i < n_free; ++i)
+	{
+		const int col = freev[i], B = col / 3, o0 = outer[3 * B], len = outer[3 * B + 1] - o0;
+		long long q = red_outer[i];
+		for (int j = 0; j < len; ++j)
+		{
+			const int r = old_to_new[inner[(size_t)o0 + j]];
+			if (r >= 0) red_inner[(size_t)q++] = r;
+		}
+	}
+	free_dirichlet(c);
+	PFG_CUDA(c, cudaMalloc(&c->d_old_to_new, sizeof(int) * std::max(ndof, 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_free, sizeof(int) * std::max(n_free, 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_red_col_start, sizeof(int) * std::max(ndof, 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_red_outer, sizeof(int) * (n_free + 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_red_inner, sizeof(int) * std::max<long long>(pos, 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_red_row_off, sizeof(unsigned short) * std::max<size_t>(row_off.size(), 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_red_values, sizeof(double) * std::max<long long>(pos, 1)));
+	PFG_CUDA(c, cudaMemcpy(c->d_old_to_new, old_to_new.data(), sizeof(int) * ndof, cudaMemcpyHostToDevice));
+	if (n_free) PFG_CUDA(c, cudaMemcpy(c->d_free, freev.data(), sizeof(int) * n_free, cudaMemcpyHostToDevice));
+	PFG_CUDA(c, cudaMemcpy(c->d_red_col_start, col_start.data(), sizeof(int) * ndof, cudaMemcpyHostToDevice));
+	PFG_CUDA(c, cudaMemcpy(c->d_red_outer, red_outer.data(), sizeof(int) * (n_free + 1), cudaMemcpyHostToDevice));
+	if (pos) PFG_CUDA(c, cudaMemcpy(c->d_red_inner, red_inner.data(), sizeof(int) * pos, cudaMemcpyHostToDevice));
+	if (!row_off.empty())
+		PFG_CUDA(c, cudaMemcpy(c->d_red_row_off, row_off.data(), sizeof(unsigned short) * row_off.size(), cudaMemcpyHostToDevice));
+	c->n_free = n_free;
+	c->red_nnz = pos;
+	c->has_dirichlet = true;
+	return PFG_OK;
+}
+
 void free_all(pfg_context *c)
 {
 	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_contrib, c->d_blk_rel, c->d_eb_inc,
 					c->d_inc_off, c->d_inc_eb, c->d_ginc_off, c->d_ginc_eb, c->d_vec_stage, c->d_hess_stage[0],
 					c->d_hess_stage[1], c->sc.partials, c->sc.ticket, c->sc.inverted, c->d_result, c->d_u, c->d_p, c->d_out};
 	for (void *p : ptrs)
+		if (p) cudaFree(p);
+	void *rptrs[] = {c->d_old_to_new, c->d_free, c->d_red_col_start, c->d_red_outer, c->d_red_inner, c->d_red_row_off,
+					 c->d_red_values, c->d_full_tmp};
+	for (void *p : rptrs)
 		if (p) cudaFree(p);
 }
 } // namespace
@@ -704,6 +808,111 @@ int pfg_synchronize(pfg_context *c)
 	if (!c) return PFG_ERR_INVALID;
 	DeviceGuard g(c->device);
 	PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	return PFG_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * Dirichlet reduction (NLProblem with one BCLagrangianForm, which can project)
+ * ------------------------------------------------------------------------- */
+int pfg_set_dirichlet(pfg_context *c, const int *dofs, int n)
+{
+	if (!c || n < 0 || (n > 0 && !dofs)) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	const int ndof = 3 * c->m.N;
+	std::vector<int> d(dofs, dofs + n);
+	for (int v : d)
+		if (v < 0 || v >= ndof) return fail(c, PFG_ERR_INVALID, "constrained dof out of range");
+	std::sort(d.begin(), d.end());
+	d.erase(std::unique(d.begin(), d.end()), d.end());
+	DeviceGuard g(c->device);
+	if (c->stream) PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	int st;
+	if (!c->has_pattern && (st = build_pattern(c))) return st;
+	c->h_constrained = std::move(d);
+	return build_dirichlet(c);
+}
+
+int pfg_reduced_pattern(pfg_context *c, int *n_free, long long *nnz)
+{
+	if (!c) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (!c->has_dirichlet) return fail(c, PFG_ERR_STATE, "no Dirichlet set (pfg_set_dirichlet)");
+	if (n_free) *n_free = c->n_free;
+	if (nnz) *nnz = c->red_nnz;
+	return PFG_OK;
+}
+
+int pfg_reduced_pattern_copy(pfg_context *c, int *outer, int *inner, int mem)
+{
+	if (!c || !check_mem(mem)) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (!c->has_dirichlet) return fail(c, PFG_ERR_STATE, "no Dirichlet set (pfg_set_dirichlet)");
+	DeviceGuard g(c->device);
+	const cudaMemcpyKind k = mem == PFG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+	if (outer) PFG_CUDA(c, cudaMemcpyAsync(outer, c->d_red_outer, sizeof(int) * ((size_t)c->n_free + 1), k, c->stream));
+	if (inner && c->red_nnz) PFG_CUDA(c, cudaMemcpyAsync(inner, c->d_red_inner, sizeof(int) * c->red_nnz, k, c->stream));
+	if (mem == PFG_MEM_HOST) PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	return PFG_OK;
+}
+
+int pfg_hessian_reduced(pfg_context *c, const double *u, int mem, int prec, int project_psd, double *values)
+{
+	if (!c || !check_mem(mem) || !check_prec(prec)) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (c->m.N && !u) return fail(c, PFG_ERR_INVALID, "u NULL");
+	if (!c->has_dirichlet) return fail(c, PFG_ERR_STATE, "no Dirichlet set (pfg_set_dirichlet)");
+	DeviceGuard g(c->device);
+	int st;
+	if ((st = ensure_staging(c, 1))) return st;
+	const double *du;
+	if ((st = stage_in(c, u, mem, c->d_u, 3 * (size_t)c->m.N, &du))) return st;
+	if ((st = ensure_hess_stage(c, prec))) return st;
+	DevPattern p = c->pat;
+	p.values = (values && mem == PFG_MEM_DEVICE) ? values : c->d_red_values;
+	p.red_col_start = c->d_red_col_start;
+	p.red_row_off = c->d_red_row_off;
+	PFG_CUDA(c, launch_hessian(c->m, p, du, prec, project_psd, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
+	if (values && mem == PFG_MEM_HOST) return finish_host(c, values, c->d_red_values, c->red_nnz);
+	if (mem == PFG_MEM_HOST) PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	return PFG_OK;
+}
+
+int pfg_gradient_reduced(pfg_context *c, const double *u, int mem, int prec, double *g_out)
+{
+	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.N && (!g_out || !u))) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (!c->has_dirichlet) return fail(c, PFG_ERR_STATE, "no Dirichlet set (pfg_set_dirichlet)");
+	DeviceGuard g(c->device);
+	const size_t ndof = 3 * (size_t)c->m.N;
+	int st = ensure_staging(c, std::max<size_t>(ndof, 1));
+	if (st) return st;
+	if (!c->d_full_tmp) PFG_CUDA(c, cudaMalloc(&c->d_full_tmp, sizeof(double) * std::max<size_t>(ndof, 1)));
+	const double *du;
+	if ((st = stage_in(c, u, mem, c->d_u, ndof, &du))) return st;
+	PFG_CUDA(c, cudaMemsetAsync(c->sc.inverted, 0, sizeof(unsigned long long), c->stream));
+	if ((st = ensure_vec_stage(c))) return st;
+	PFG_CUDA(c, launch_gradient(c->m, du, prec, c->d_full_tmp, c->sc, c->stream));
+	double *dst = mem == PFG_MEM_DEVICE ? g_out : c->d_out;
+	PFG_CUDA(c, launch_gather_free(c->d_full_tmp, c->d_free, c->n_free, dst, c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, g_out, c->d_out, c->n_free);
+	return PFG_OK;
+}
+
+int pfg_reduced_to_full(pfg_context *c, const double *y, const double *x_bc, int mem, double *x)
+{
+	if (!c || !check_mem(mem) || (c->m.N && (!x || (c->n_free && !y)))) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (!c->has_dirichlet) return fail(c, PFG_ERR_STATE, "no Dirichlet set (pfg_set_dirichlet)");
+	DeviceGuard g(c->device);
+	const size_t ndof = 3 * (size_t)c->m.N;
+	int st = ensure_staging(c, std::max<size_t>(ndof, 1));
+	if (st) return st;
+	const double *dy = y, *dbc = x_bc;
+	if (mem == PFG_MEM_HOST)
+	{
+		// y -> d_p (n_free <= ndof doubles), x_bc -> d_u
+		if (c->n_free) PFG_CUDA(c, cudaMemcpyAsync(c->d_p, y, sizeof(double) * c->n_free, cudaMemcpyHostToDevice, c->stream));
+		if (x_bc) PFG_CUDA(c, cudaMemcpyAsync(c->d_u, x_bc, sizeof(double) * ndof, cudaMemcpyHostToDevice, c->stream));
+		dy = c->d_p;
+		dbc = x_bc ? c->d_u : nullptr;
+	}
+	double *dst = mem == PFG_MEM_DEVICE ? x : c->d_out;
+	PFG_CUDA(c, launch_reduced_to_full(dy, dbc, c->d_old_to_new, (int)ndof, dst, c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, x, c->d_out, ndof);
 	return PFG_OK;
 }
 

@@ -51,6 +51,12 @@ struct DevPattern
 	const unsigned short *contrib = nullptr;
 	const unsigned short *blk_rel = nullptr;
 	double *values = nullptr;
+	// Dirichlet-reduced output (BCLagrangianForm::project_hessian): when red_col_start
+	// is set the reduction writes only entries whose row and column are free, at
+	//   values[red_col_start[col] + red_row_off[outer[3B]/3 + 3*rank + r]]
+	// (red_col_start < 0: constrained column; red_row_off == 0xFFFF: constrained row)
+	const int *red_col_start = nullptr;
+	const unsigned short *red_row_off = nullptr;
 };
 
 struct Scratch
@@ -76,6 +82,11 @@ cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double 
 // project_psd != 0: every element matrix is projected onto the PSD cone (ipc::project_to_psd, CLAMP) before the scatter
 cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, int project_psd,
 						   void *stage, cudaStream_t s);
+// Dirichlet reduction helpers: dof maps of the free dofs (old_to_new[dof] = index
+// among the free dofs or -1, free[i] = dof of the i-th free dof)
+cudaError_t launch_gather_free(const double *full, const int *free, int n_free, double *out, cudaStream_t s);
+cudaError_t launch_reduced_to_full(const double *y, const double *x_bc, const int *old_to_new, int ndof, double *x,
+								   cudaStream_t s);
 cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double *adj, double *out, cudaStream_t s);
 cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out,
 							 const Scratch &sc, cudaStream_t s);

@@ -952,10 +952,26 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 				a2 += double(y2);
 			}
 		}
-		double *d = dst + c * stride + 3 * r;
-		d[0] = a0;
-		d[1] = a1;
-		d[2] = a2;
+		if (pat.red_col_start == nullptr)
+		{
+			double *d = dst + c * stride + 3 * r;
+			d[0] = a0;
+			d[1] = a1;
+			d[2] = a2;
+		}
+		else
+		{
+			// Dirichlet-reduced output: free rows of free columns only
+			const int cs = __ldg(pat.red_col_start + 3 * B + c);
+			if (cs >= 0)
+			{
+				const unsigned short *ro = pat.red_row_off + o0 / 3 + 3 * r;
+				const unsigned short r0 = __ldg(ro), r1 = __ldg(ro + 1), r2 = __ldg(ro + 2);
+				if (r0 != 0xFFFF) pat.values[cs + r0] = a0;
+				if (r1 != 0xFFFF) pat.values[cs + r1] = a1;
+				if (r2 != 0xFFFF) pat.values[cs + r2] = a2;
+			}
+		}
 	}
 }
 
@@ -1483,6 +1499,39 @@ cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *ad
 	}
 	constexpr int NTG = 128;
 	if (m.Ng > 0) k_vec_gather<NTG><<<blocks_for(m.Ng, NTG), NTG, 0, s>>>(m.Ng, m.ginc_off, m.ginc_eb, st, out);
+	return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Dirichlet reduction of vectors (BCLagrangianForm::project_gradient,
+// BCLagrangianForm.cpp:149-155; NLProblem::reduced_to_full, NLProblem.cpp:713-735)
+// ---------------------------------------------------------------------------
+__global__ void k_gather_free(const double *__restrict__ full, const int *__restrict__ free, int n_free,
+							  double *__restrict__ out)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n_free) out[i] = __ldg(full + __ldg(free + i));
+}
+
+__global__ void k_reduced_to_full(const double *__restrict__ y, const double *__restrict__ x_bc,
+								  const int *__restrict__ old_to_new, int ndof, double *__restrict__ x)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= ndof) return;
+	const int k = __ldg(old_to_new + i);
+	x[i] = k >= 0 ? __ldg(y + k) : (x_bc ? __ldg(x_bc + i) : 0.0);
+}
+
+cudaError_t launch_gather_free(const double *full, const int *free, int n_free, double *out, cudaStream_t s)
+{
+	if (n_free > 0) k_gather_free<<<(n_free + 255) / 256, 256, 0, s>>>(full, free, n_free, out);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_reduced_to_full(const double *y, const double *x_bc, const int *old_to_new, int ndof, double *x,
+								   cudaStream_t s)
+{
+	if (ndof > 0) k_reduced_to_full<<<(ndof + 255) / 256, 256, 0, s>>>(y, x_bc, old_to_new, ndof, x);
 	return cudaGetLastError();
 }
 

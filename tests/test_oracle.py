@@ -339,3 +339,20 @@ def test_projected_oracle_hessian_is_psd():
     H = sp.csc_matrix((v, i, o), shape=(mesh.n_dofs, mesh.n_dofs)).toarray()
     w = np.linalg.eigvalsh(0.5 * (H + H.T))
     assert w.min() >= -1e-10 * np.abs(w).max()
+
+
+# ------------------------------------------------------ Dirichlet reduction
+def test_project_hessian_known_answer():
+    """BCLagrangianForm::project_hessian on a 4x4 matrix with dof 1 constrained."""
+    from oracle.binding import project_gradient, project_hessian, reduced_to_full
+    A = np.array([[4.0, 1.0, 0.0, 2.0],
+                  [1.0, 5.0, 3.0, 0.0],
+                  [0.0, 3.0, 6.0, 7.0],
+                  [2.0, 0.0, 7.0, 8.0]])
+    C = sp.csc_matrix(A)
+    o, i, v = project_hessian(C.indptr, C.indices, C.data, [1])
+    R = sp.csc_matrix((v, i, o), shape=(3, 3)).toarray()
+    assert np.array_equal(R, A[np.ix_([0, 2, 3], [0, 2, 3])])
+    assert list(o) == [0, 2, 4, 7] and list(i) == [0, 2, 1, 2, 0, 1, 2]
+    assert np.array_equal(project_gradient(np.arange(4.0), [1]), [0.0, 2.0, 3.0])
+    assert np.array_equal(reduced_to_full([10.0, 20.0, 30.0], [-1.0, -2.0, -3.0, -4.0], [1]), [10.0, -2.0, 20.0, 30.0])
