@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(NT) k_energy_per_element(DevMesh m, const doub
 // gradient (NLAssembler::assemble_gradient)
 // ---------------------------------------------------------------------------
 template <class EL, class T, int NT>
-__global__ void __launch_bounds__(NT) k_gradient(DevMesh m, const double *__restrict__ u, double *__restrict__ stage,
+__global__ void __launch_bounds__(NT, EL::ET == 1 ? 8 : 1) k_gradient(DevMesh m, const double *__restrict__ u, double *__restrict__ stage,
 												 unsigned long long *inverted)
 {
 	const int e = blockIdx.x * NT + threadIdx.x;

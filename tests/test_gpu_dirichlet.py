@@ -73,3 +73,35 @@ def test_reduced_device_mode_and_empty_set(require_gpu):
     gd = asm.assemble_gradient_reduced(ud)
     assert np.array_equal(gd.cpu().numpy(), asm.assemble_gradient_reduced(u))
     asm.close()
+
+
+def test_reduction_argument_checks(require_gpu):
+    import ctypes
+
+    from polyfem_b200 import _lib
+    L = _lib.lib()
+    mesh, lam, mu, u, _ = make_case(M.P1_TET, 2, seed=14)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    h = asm.handle
+    n = ctypes.c_int()
+    nnz = ctypes.c_longlong()
+    # before any Dirichlet set: state errors
+    assert L.pfg_reduced_pattern(h, ctypes.byref(n), ctypes.byref(nnz)) == 5
+    ub = np.ascontiguousarray(u)
+    out = np.empty(mesh.n_dofs)
+    assert L.pfg_hessian_reduced(h, ctypes.c_void_p(ub.ctypes.data), 0, 0, 0, None) == 5
+    assert L.pfg_gradient_reduced(h, ctypes.c_void_p(ub.ctypes.data), 0, 0, ctypes.c_void_p(out.ctypes.data)) == 5
+    # out-of-range and negative dofs are rejected
+    bad = np.array([0, mesh.n_dofs], dtype=np.int32)
+    assert L.pfg_set_dirichlet(h, ctypes.c_void_p(bad.ctypes.data), 2) == 1
+    bad = np.array([-1], dtype=np.int32)
+    assert L.pfg_set_dirichlet(h, ctypes.c_void_p(bad.ctypes.data), 1) == 1
+    assert L.pfg_set_dirichlet(h, None, 3) == 1
+    assert L.pfg_set_dirichlet(None, None, 0) == 1
+    # all dofs constrained: empty reduced system
+    asm.set_dirichlet(np.arange(mesh.n_dofs))
+    assert asm.n_free == 0
+    outer, inner = asm.reduced_pattern()
+    assert list(outer) == [0] and inner.size == 0
+    assert asm.assemble_hessian_reduced_values(u).size == 0
+    asm.close()

@@ -73,3 +73,20 @@ def test_elastic_form_project_to_psd_flag(require_gpu):
     _, _, v_psd = Oracle(mesh, lam, mu).hessian(u, project_psd=True)
     assert rel_err(H.data, v_psd) <= 1e-11
     asm.close()
+
+
+def test_projection_keeps_nan_of_inverted_elements(require_gpu):
+    """An inverted element (J <= 0) has NaN entries (log J); the projection leaves
+    them alone, so the NaN still reaches the assembled matrix as in the reference."""
+    mesh, lam, mu, u, _ = make_case(M.P1_TET, 2, seed=15)
+    u = u.copy()
+    # collapse element 0 through its first node
+    n0 = mesh.conn[0, 0]
+    c = mesh.node_pos[mesh.conn[0]].mean(axis=0)
+    u[3 * n0:3 * n0 + 3] = 2.5 * (c - mesh.node_pos[n0])
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    plain = asm.assemble_hessian_values(u, "fp64")
+    proj = asm.assemble_hessian_values(u, "fp64", project_to_psd=True)
+    assert np.isnan(plain).any()
+    assert np.array_equal(np.isnan(plain), np.isnan(proj))
+    asm.close()
