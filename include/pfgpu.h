@@ -215,7 +215,8 @@ int pfg_reduced_to_full(pfg_context *ctx, const double *y, const double *x_bc, i
  * stream) and returns without synchronising.  It allocates nothing: the
  * reduction scratch is a fixed array inside the library's device image
  * (512 KiB, held by every GPU that loads the library until exit), which
- * limits n_elements to 256 * PFG_NOALLOC_MAX_BLOCKS; larger meshes return
+ * limits n_elements to 256 * PFG_NOALLOC_MAX_BLOCKS = 16,777,216 (the energy
+ * kernel takes 256 elements per block); larger meshes return
  * PFG_ERR_UNSUPPORTED with the limit in pfg_last_error(NULL).  All calls
  * share that array, so calls that overlap on the GPU race.  The first call on
  * a device looks up the array's address; make it before any stream capture.

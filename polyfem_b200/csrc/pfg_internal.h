@@ -73,6 +73,10 @@ constexpr int PREC_FP64 = 0;
 constexpr int PREC_FP32 = 1;
 constexpr int PREC_SPLIT32 = 2;
 
+// Elements per thread block of the total-energy kernel for an element type (the
+// number of per-block partial sums is ceil(E / this)).
+int energy_elems_per_block(int et);
+
 // All launchers return cudaGetLastError() after enqueueing on `s`.
 cudaError_t launch_energy(const DevMesh &m, const double *u, int prec, bool per_element, double *out,
 						  const Scratch &sc, cudaStream_t s);

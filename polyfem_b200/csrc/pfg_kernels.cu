@@ -1428,6 +1428,8 @@ static void energy_t(const DevMesh &m, const double *u, bool per_element, double
 		k_energy<EL, T, NT><<<nb, NT, 0, s>>>(m, u, sc.partials, out, sc.ticket, sc.inverted);
 }
 
+int energy_elems_per_block(int) { return 256; }
+
 cudaError_t launch_energy(const DevMesh &m, const double *u, int prec, bool per_element, double *out,
 						  const Scratch &sc, cudaStream_t s)
 {

@@ -10,8 +10,9 @@
 // allocates nothing: no cudaMalloc, no cudaFree, no allocating library routine.
 //
 // Limits and rules (also in include/pfgpu.h):
-//  * at most PFG_NOALLOC_MAX_BLOCKS thread blocks of 256 elements, i.e.
-//    n_elements <= 256 * PFG_NOALLOC_MAX_BLOCKS; larger meshes are rejected;
+//  * at most PFG_NOALLOC_MAX_BLOCKS thread blocks of the energy kernel
+//    (energy_elems_per_block: 256 elements), i.e. n_elements <= 256 *
+//    PFG_NOALLOC_MAX_BLOCKS; larger meshes are rejected;
 //  * the scratch array (512 KiB of partial sums plus two counters) is held by
 //    every GPU that loads the library until the process exits;
 //  * all calls share that one array: calls that overlap on the GPU (different
@@ -27,7 +28,6 @@
 
 namespace
 {
-constexpr int kNoallocThreads = 256; // threads per block of the energy kernel
 
 // file-scope device scratch: per-block partial sums, the last-block ticket and
 // the inverted-element counter
@@ -86,11 +86,12 @@ extern "C" int pfg_energy_noalloc(int elem_type, int n_elements, int n_nodes, in
 	if (n_elements > 0 && (!conn_soa || !X || !lame || !u)) return noalloc_fail(PFG_ERR_INVALID, "NULL input array");
 	if (elem_type == PFG_P2_TET && n_elements > 0 && !gconn_soa)
 		return noalloc_fail(PFG_ERR_INVALID, "gconn_soa is required for P2 elements");
-	const long long blocks = ((long long)n_elements + kNoallocThreads - 1) / kNoallocThreads;
+	const long long per_block = pfg::energy_elems_per_block(elem_type);
+	const long long blocks = ((long long)n_elements + per_block - 1) / per_block;
 	if (blocks > PFG_NOALLOC_MAX_BLOCKS)
 		return noalloc_fail(PFG_ERR_UNSUPPORTED, "n_elements = " + std::to_string(n_elements) + " exceeds the limit of " +
-													 std::to_string((long long)PFG_NOALLOC_MAX_BLOCKS * kNoallocThreads) +
-													 " elements of pfg_energy_noalloc");
+													 std::to_string((long long)PFG_NOALLOC_MAX_BLOCKS * per_block) +
+													 " elements of pfg_energy_noalloc for this element type");
 	int device = -1;
 	cudaError_t ce = cudaGetDevice(&device);
 	if (ce != cudaSuccess || device < 0 || device >= kMaxDevices)

@@ -57,3 +57,13 @@ def test_noalloc_rejects_oversized_mesh(require_gpu):
                               ctypes.c_void_p(16), ctypes.c_void_p(16), 0, ctypes.c_void_p(16), None)
     assert st == 4
     assert b"exceeds the limit" in L.pfg_last_error(None)
+
+
+@pytest.mark.parametrize("et,per_block", [(M.P2_TET, 256), (M.Q1_HEX, 256)])
+def test_noalloc_limit_follows_the_energy_kernel_blocks(require_gpu, et, per_block):
+    L = _lib.lib()
+    too_many = per_block * 65536 + 1
+    st = L.pfg_energy_noalloc(et, too_many, 10, 10, ctypes.c_void_p(16), ctypes.c_void_p(16), ctypes.c_void_p(16),
+                              ctypes.c_void_p(16), ctypes.c_void_p(16), 0, ctypes.c_void_p(16), None)
+    assert st == 4
+    assert b"exceeds the limit" in L.pfg_last_error(None)
