@@ -44,7 +44,7 @@ struct pfg_context
 		*d_red_inner = nullptr;
 	unsigned short *d_red_row_off = nullptr;
 	double *d_red_values = nullptr, *d_full_tmp = nullptr;
-	int *d_eb_inc = nullptr;
+	int *d_eb_inc = nullptr, *d_g_eb_inc = nullptr;
 	// node -> (element, local index) incidences, FE and geometric nodes
 	std::vector<long long> h_inc_off; // [N+1]
 	std::vector<int> h_inc_e;         // element of each incidence, grouped by node, ascending
@@ -444,7 +444,7 @@ int build_dirichlet(pfg_context *c)
 
 void free_all(pfg_context *c)
 {
-	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_contrib, c->d_blk_rel, c->d_eb_inc,
+	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_contrib, c->d_blk_rel, c->d_eb_inc, c->d_g_eb_inc,
 					c->d_inc_off, c->d_inc_eb, c->d_ginc_off, c->d_ginc_eb, c->d_vec_stage, c->d_hess_stage[0],
 					c->d_hess_stage[1], c->sc.partials, c->sc.ticket, c->sc.inverted, c->d_result, c->d_u, c->d_p, c->d_out};
 	for (void *p : ptrs)
@@ -574,6 +574,11 @@ int pfg_create(const pfg_mesh_desc *d, pfg_context **out)
 			CREATE_CUDA(cudaMalloc(&c->d_ginc_eb, sizeof(int) * std::max<size_t>(geb.size(), 1)));
 			CREATE_CUDA(cudaMemcpy(c->d_ginc_off, goff32.data(), sizeof(int) * goff32.size(), cudaMemcpyHostToDevice));
 			if (!geb.empty()) CREATE_CUDA(cudaMemcpy(c->d_ginc_eb, geb.data(), sizeof(int) * geb.size(), cudaMemcpyHostToDevice));
+			std::vector<int> ginv(geb.size());
+			for (size_t k = 0; k < geb.size(); ++k) ginv[geb[k]] = (int)k;
+			CREATE_CUDA(cudaMalloc(&c->d_g_eb_inc, sizeof(int) * std::max<size_t>(ginv.size(), 1)));
+			if (!ginv.empty())
+				CREATE_CUDA(cudaMemcpy(c->d_g_eb_inc, ginv.data(), sizeof(int) * ginv.size(), cudaMemcpyHostToDevice));
 		}
 	}
 	c->sc.max_blocks = (int)(E / 128 + 2);
@@ -592,6 +597,7 @@ int pfg_create(const pfg_mesh_desc *d, pfg_context **out)
 	c->m.eb_inc = c->d_eb_inc;
 	c->m.ginc_off = c->d_ginc_off ? c->d_ginc_off : c->d_inc_off;
 	c->m.ginc_eb = c->d_ginc_eb ? c->d_ginc_eb : c->d_inc_eb;
+	c->m.g_eb_inc = c->d_g_eb_inc ? c->d_g_eb_inc : c->d_eb_inc;
 	c->m.X = c->d_X;
 	c->m.lame = c->d_lame;
 	*out = c;

@@ -30,6 +30,7 @@ struct DevMesh
 	const int *eb_inc = nullptr; // [E*n] inverse of inc_eb: incidence index of (e, b)
 	const int *ginc_off = nullptr;
 	const int *ginc_eb = nullptr;
+	const int *g_eb_inc = nullptr; // [E*n_g] inverse of ginc_eb (aliases eb_inc when isoparametric)
 };
 
 // Device-resident Hessian pattern (Eigen ColMajor CSC, int32 indices) and its
@@ -65,7 +66,7 @@ struct Scratch
 	unsigned int *ticket = nullptr;   // last-block-done counter (returns to 0 after each launch)
 	unsigned long long *inverted = nullptr;
 	int max_blocks = 0;
-	double *vec_stage = nullptr;      // [E][max(n, n_g)][4] element gradient / shape contributions (32-byte slots)
+	double *vec_stage = nullptr;      // one 32-byte slot per incidence, in incidence (node) order: element gradient / shape contributions
 	void *hess_stage = nullptr;       // one padded record of 9n block values per incidence (FP64 or FP32)
 };
 

@@ -370,49 +370,47 @@ __global__ void __launch_bounds__(NT, EL::ET == 1 ? 8 : 1) k_gradient(DevMesh m,
 			}
 	}
 	if (bad) atomicAdd(inverted, 1ull);
-	// the element's contributions, one 32-byte slot per (e, a): stage[e][a][0..2], [3] = 0
-	double *dst = stage + (size_t)e * EL::N * 4;
+	// the element's contributions, one 32-byte slot per incidence (e, a) at the
+	// incidence's position in node order: (G0, G1, G2, 0)
 #pragma unroll
-	for (int a = 0; a < EL::N; ++a) st_slot(dst + a * 4, double(Gacc[a][0]), double(Gacc[a][1]), double(Gacc[a][2]));
+	for (int a = 0; a < EL::N; ++a)
+	{
+		const int k = __ldg(m.eb_inc + (size_t)e * EL::N + a);
+		st_slot(stage + (size_t)k * 4, double(Gacc[a][0]), double(Gacc[a][1]), double(Gacc[a][2]));
+	}
 }
 
 // Per node: the sum of its incidences' contributions in incidence (element) order
 // (NLAssembler::assemble_gradient's scatter, Assembler.cpp:613-629), one thread per
-// node; loads are issued eight incidences at a time.  Deterministic.
+// node.  The slots are in node order, so a node's incidences are one contiguous
+// run; loads are issued eight slots at a time.  Deterministic.
 template <int NT>
-__global__ void __launch_bounds__(NT) k_vec_gather(int n_nodes, const int *__restrict__ off, const int *__restrict__ eb,
+__global__ void __launch_bounds__(NT) k_vec_gather(int n_nodes, const int *__restrict__ off,
 												   const double *__restrict__ stage, double *__restrict__ out)
 {
 	constexpr int BATCH = 8;
 	const int B = blockIdx.x * NT + threadIdx.x;
 	if (B >= n_nodes) return;
 	const int k0 = __ldg(off + B), k1 = __ldg(off + B + 1);
+	const double2 *slots = reinterpret_cast<const double2 *>(stage);
 	double t0 = 0.0, t1 = 0.0, t2 = 0.0;
 	for (int kb = k0; kb < k1; kb += BATCH)
 	{
-		int idx[BATCH];
-#pragma unroll
-		for (int j = 0; j < BATCH; ++j) idx[j] = (kb + j < k1) ? __ldg(eb + kb + j) : -1;
-		double v[BATCH][3];
+		double2 x[BATCH], y[BATCH];
 #pragma unroll
 		for (int j = 0; j < BATCH; ++j)
-		{
-			if (idx[j] >= 0)
+			if (kb + j < k1)
 			{
-				const double2 *p = reinterpret_cast<const double2 *>(stage + (size_t)idx[j] * 4);
-				const double2 x = __ldg(p), y = __ldg(p + 1);
-				v[j][0] = x.x;
-				v[j][1] = x.y;
-				v[j][2] = y.x;
+				x[j] = __ldg(slots + 2 * (size_t)(kb + j));
+				y[j] = __ldg(slots + 2 * (size_t)(kb + j) + 1);
 			}
-		}
 #pragma unroll
 		for (int j = 0; j < BATCH; ++j)
-			if (idx[j] >= 0)
+			if (kb + j < k1)
 			{
-				t0 += v[j][0];
-				t1 += v[j][1];
-				t2 += v[j][2];
+				t0 += x[j].x;
+				t1 += x[j].y;
+				t2 += y[j].x;
 			}
 	}
 	out[(size_t)B * 3 + 0] = t0;
@@ -1407,9 +1405,12 @@ __global__ void __launch_bounds__(NT) k_shape_vjp(DevMesh m, const double *__res
 			}
 		}
 	}
-	double *dst = stage + (size_t)e * EL::NG * 4;
 #pragma unroll
-	for (int v = 0; v < EL::NG; ++v) st_slot(dst + v * 4, double(acc[v][0]), double(acc[v][1]), double(acc[v][2]));
+	for (int v = 0; v < EL::NG; ++v)
+	{
+		const int k = __ldg(m.g_eb_inc + (size_t)e * EL::NG + v);
+		st_slot(stage + (size_t)k * 4, double(acc[v][0]), double(acc[v][1]), double(acc[v][2]));
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -1465,7 +1466,7 @@ cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double 
 	default: return cudaErrorInvalidValue;
 	}
 	constexpr int NTG = 128;
-	if (m.N > 0) k_vec_gather<NTG><<<blocks_for(m.N, NTG), NTG, 0, s>>>(m.N, m.inc_off, m.inc_eb, sc.vec_stage, g);
+	if (m.N > 0) k_vec_gather<NTG><<<blocks_for(m.N, NTG), NTG, 0, s>>>(m.N, m.inc_off, sc.vec_stage, g);
 	return cudaGetLastError();
 }
 
@@ -1500,7 +1501,7 @@ cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *ad
 	default: return cudaErrorInvalidValue;
 	}
 	constexpr int NTG = 128;
-	if (m.Ng > 0) k_vec_gather<NTG><<<blocks_for(m.Ng, NTG), NTG, 0, s>>>(m.Ng, m.ginc_off, m.ginc_eb, st, out);
+	if (m.Ng > 0) k_vec_gather<NTG><<<blocks_for(m.Ng, NTG), NTG, 0, s>>>(m.Ng, m.ginc_off, st, out);
 	return cudaGetLastError();
 }
 
