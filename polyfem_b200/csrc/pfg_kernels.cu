@@ -977,24 +977,26 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 // ipc::project_to_psd (PSDProjectionMethod::CLAMP), applied to every element
 // matrix before the scatter when NLAssembler::assemble_hessian is called with
 // project_to_psd (Assembler.cpp:693-694).  The element matrix is rebuilt from its
-// n records, A[3a+r][3b+c] = record_b[9a + 3c + r], in FP64; a warp diagonalises
-// it with cyclic Jacobi in round-robin order (M/2 disjoint rotations per round,
-// M - 1 rounds per sweep, at most PSD_MAX_SWEEPS sweeps, stopping when the
-// off-diagonal squares fall below 1e-32 of all squares).  If the smallest
-// eigenvalue is > 0 (or NaN) the records are left as they are; otherwise
-// V max(l, 0) V^T is written back, rounded to the record type.
+// n records, A[3a+r][3b+c] = record_b[9a + 3c + r], in FP64.  A warp (lane i
+// owning row/column i) diagonalises it with the classical symmetric eigensolver:
+// Householder reduction to tridiagonal form with the orthogonal factor
+// accumulated (EISPACK tred2), then the QL algorithm with implicit shifts on the
+// tridiagonal matrix, rotating the accumulated factor (EISPACK tql2; the scalar
+// recurrence is evaluated identically on every lane, each lane rotates its own
+// row).  If the smallest eigenvalue is > 0, or the matrix holds NaN, or QL does
+// not converge in PSD_MAX_QL_ITER iterations for an eigenvalue, the records are
+// left as they are; otherwise Z max(l, 0) Z^T is written back, rounded to the
+// record type.
 // ---------------------------------------------------------------------------
-constexpr int PSD_MAX_SWEEPS = 40;
+constexpr int PSD_MAX_QL_ITER = 60;
 
 template <class EL>
 struct PsdWarp
 {
-	static constexpr int M = 3 * EL::N, H = M / 2, LD = M + 1;
-	double A[M][LD];
-	double V[M][LD];
-	double c[H], s[H], t[H];
-	int p[H], q[H];
-	double d[M];
+	static constexpr int M = 3 * EL::N, LD = M + 1;
+	double A[M][LD]; // the element matrix, then the orthogonal factor Z
+	double R[M][LD]; // the projected matrix
+	double d[M], e[M];
 };
 
 __device__ __forceinline__ double warp_allsum(double v)
@@ -1014,26 +1016,15 @@ template <class EL, class T, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_project_psd(DevMesh m, T *__restrict__ stage)
 {
 	using W = PsdWarp<EL>;
-	constexpr int N = EL::N, M = W::M, H = W::H, RP = rec_pad<EL, T>();
-	constexpr int NBP = H * (H + 1) / 2, BPL = (NBP + 31) / 32;
+	constexpr int N = EL::N, M = W::M, RP = rec_pad<EL, T>();
+	static_assert(M <= 32, "one lane per row");
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	W &S = reinterpret_cast<W *>(smem_raw)[threadIdx.x >> 5];
-	unsigned char *bp_P = smem_raw + WARPS * sizeof(W), *bp_Q = bp_P + NBP;
-	for (int k = threadIdx.x; k < NBP; k += WARPS * 32)
-	{
-		int P = 0, r = k;
-		while (r >= H - P)
-		{
-			r -= H - P;
-			++P;
-		}
-		bp_P[k] = (unsigned char)P;
-		bp_Q[k] = (unsigned char)(P + r);
-	}
-	__syncthreads();
 	const int lane = threadIdx.x & 31;
 	const int e = blockIdx.x * WARPS + (threadIdx.x >> 5);
 	if (e >= m.E) return;
+	double(*a)[W::LD] = S.A;
+	double *d = S.d, *ev = S.e;
 	int sidx[N];
 #pragma unroll
 	for (int b = 0; b < N; ++b) sidx[b] = __ldg(m.eb_inc + (size_t)e * N + b);
@@ -1043,133 +1034,208 @@ __global__ void __launch_bounds__(WARPS * 32) k_project_psd(DevMesh m, T *__rest
 		const T *rec = stage + (size_t)sidx[b] * RP;
 		for (int k = lane; k < 9 * N; k += 32)
 		{
-			const int a = k / 9, cc = (k % 9) / 3, r = k % 3;
-			S.A[3 * a + r][3 * b + cc] = double(rec[k]);
+			const int aa = k / 9, cc = (k % 9) / 3, r = k % 3;
+			a[3 * aa + r][3 * b + cc] = double(rec[k]);
 		}
 	}
-	for (int k = lane; k < M * M; k += 32) S.V[k / M][k % M] = (k / M == k % M) ? 1.0 : 0.0;
 	__syncwarp();
+	bool nan_in = false;
+	if (lane < M)
+		for (int k = 0; k < M; ++k) nan_in |= isnan(a[lane][k]);
+	if (__any_sync(0xffffffffu, nan_in)) return; // NaN propagates unchanged
 
-	for (int sweep = 0; sweep < PSD_MAX_SWEEPS; ++sweep)
+	// --- Householder reduction to tridiagonal form (tred2) -------------------
+	for (int i = M - 1; i > 0; --i)
 	{
-		double off = 0.0, tot = 0.0;
-		for (int k = lane; k < M * M; k += 32)
+		const int l = i - 1;
+		double h = 0.0;
+		if (l > 0)
 		{
-			const int i = k / M, j = k % M;
-			const double a = S.A[i][j];
-			tot += a * a;
-			if (i != j) off += a * a;
+			const double scale = warp_allsum(lane <= l ? fabs(a[i][lane]) : 0.0);
+			if (scale == 0.0)
+			{
+				if (lane == 0) ev[i] = a[i][l];
+			}
+			else
+			{
+				if (lane <= l) a[i][lane] /= scale;
+				__syncwarp();
+				h = warp_allsum(lane <= l ? a[i][lane] * a[i][lane] : 0.0);
+				const double f = a[i][l];
+				const double g = f >= 0.0 ? -sqrt(h) : sqrt(h);
+				h -= f * g;
+				__syncwarp();
+				if (lane == 0)
+				{
+					ev[i] = scale * g;
+					a[i][l] = f - g;
+				}
+				__syncwarp();
+				double ej = 0.0;
+				if (lane <= l)
+				{
+					const int j = lane;
+					a[j][i] = a[i][j] / h;
+					double gg = 0.0;
+					for (int k = 0; k <= j; ++k) gg += a[j][k] * a[i][k];
+					for (int k = j + 1; k <= l; ++k) gg += a[k][j] * a[i][k];
+					ej = gg / h;
+				}
+				const double ff = warp_allsum(lane <= l ? ej * a[i][lane] : 0.0);
+				const double hh = ff / (h + h);
+				if (lane <= l) ev[lane] = ej - hh * a[i][lane];
+				__syncwarp();
+				if (lane <= l)
+				{
+					const int j = lane;
+					const double fj = a[i][j], gj = ev[j];
+					for (int k = 0; k <= j; ++k) a[j][k] -= (fj * ev[k] + gj * a[i][k]);
+				}
+				__syncwarp();
+			}
 		}
-		off = warp_allsum(off);
-		tot = warp_allsum(tot);
-		if (!(off > 1e-32 * tot)) break; // converged (or NaN): the same decision on every lane
-		for (int round = 0; round < M - 1; ++round)
-		{
-			if (lane < H)
-			{
-				// circle method: position 0 fixed, positions 1..M-1 rotate with the round
-				const int x = lane == 0 ? 0 : ((lane - 1 + round) % (M - 1)) + 1;
-				const int y = ((M - 2 - lane + round) % (M - 1)) + 1;
-				const int pp = min(x, y), qq = max(x, y);
-				const double apq = S.A[pp][qq], app = S.A[pp][pp], aqq = S.A[qq][qq];
-				double cc = 1.0, ss = 0.0, tt = 0.0;
-				if (apq != 0.0)
-				{
-					const double theta = (aqq - app) / (2.0 * apq);
-					// t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)), ~ 1 / (2 theta) once theta^2 overflows
-					tt = fabs(theta) > 1e100 ? 0.5 / theta
-											 : (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-					cc = 1.0 / sqrt(tt * tt + 1.0);
-					ss = tt * cc;
-				}
-				S.p[lane] = pp;
-				S.q[lane] = qq;
-				S.c[lane] = cc;
-				S.s[lane] = ss;
-				S.t[lane] = tt;
-			}
-			__syncwarp();
-			// A <- J^T A J, one 2x2 block of pair rows P and pair columns Q (P <= Q) per item
-			double nb[BPL][4];
-#pragma unroll
-			for (int j = 0; j < BPL; ++j)
-			{
-				const int bp = lane + 32 * j;
-				if (bp >= NBP) continue;
-				const int P = bp_P[bp], Q = bp_Q[bp];
-				const int pP = S.p[P], qP = S.q[P], pQ = S.p[Q], qQ = S.q[Q];
-				if (P == Q)
-				{
-					const double apq = S.A[pP][qP];
-					nb[j][0] = S.A[pP][pP] - S.t[P] * apq;
-					nb[j][3] = S.A[qP][qP] + S.t[P] * apq;
-					nb[j][1] = nb[j][2] = 0.0;
-				}
-				else
-				{
-					const double cP = S.c[P], sP = S.s[P], cQ = S.c[Q], sQ = S.s[Q];
-					const double b00 = S.A[pP][pQ], b01 = S.A[pP][qQ], b10 = S.A[qP][pQ], b11 = S.A[qP][qQ];
-					const double l0 = cP * b00 - sP * b10, l1 = cP * b01 - sP * b11;
-					const double l2 = sP * b00 + cP * b10, l3 = sP * b01 + cP * b11;
-					nb[j][0] = cQ * l0 - sQ * l1;
-					nb[j][1] = sQ * l0 + cQ * l1;
-					nb[j][2] = cQ * l2 - sQ * l3;
-					nb[j][3] = sQ * l2 + cQ * l3;
-				}
-			}
-			__syncwarp();
-#pragma unroll
-			for (int j = 0; j < BPL; ++j)
-			{
-				const int bp = lane + 32 * j;
-				if (bp >= NBP) continue;
-				const int P = bp_P[bp], Q = bp_Q[bp];
-				const int pP = S.p[P], qP = S.q[P], pQ = S.p[Q], qQ = S.q[Q];
-				S.A[pP][pQ] = nb[j][0];
-				S.A[pP][qQ] = nb[j][1];
-				S.A[qP][pQ] = nb[j][2];
-				S.A[qP][qQ] = nb[j][3];
-				S.A[pQ][pP] = nb[j][0];
-				S.A[qQ][pP] = nb[j][1];
-				S.A[pQ][qP] = nb[j][2];
-				S.A[qQ][qP] = nb[j][3];
-			}
-			// V <- V J, columns p and q of every pair
-			for (int k = lane; k < M * H; k += 32)
-			{
-				const int i = k / H, P = k % H;
-				const int pp = S.p[P], qq = S.q[P];
-				const double cc = S.c[P], ss = S.s[P];
-				const double vp = S.V[i][pp], vq = S.V[i][qq];
-				S.V[i][pp] = cc * vp - ss * vq;
-				S.V[i][qq] = ss * vp + cc * vq;
-			}
-			__syncwarp();
-		}
+		else if (lane == 0)
+			ev[i] = a[i][l];
+		if (lane == 0) d[i] = h;
+		__syncwarp();
 	}
-	double lmin = INFINITY;
-	for (int i = lane; i < M; i += 32) lmin = fmin(lmin, S.A[i][i]);
-	lmin = warp_allmin(lmin);
-	bool has_nan = false;
-	for (int i = lane; i < M; i += 32) has_nan |= isnan(S.A[i][i]);
-	has_nan = __any_sync(0xffffffffu, has_nan);
-	if (has_nan || lmin > 0.0) return; // records stay as they are
-	for (int i = lane; i < M; i += 32) S.d[i] = S.A[i][i] > 0.0 ? S.A[i][i] : 0.0;
-	__syncwarp();
-	for (int k = lane; k < M * (M + 1) / 2; k += 32)
+	if (lane == 0)
 	{
-		int i = 0, r = k;
-		while (r >= M - i)
+		d[0] = 0.0;
+		ev[0] = 0.0;
+	}
+	__syncwarp();
+	// accumulate the orthogonal factor in place
+	for (int i = 0; i < M; ++i)
+	{
+		const int l = i - 1;
+		if (d[i] != 0.0)
 		{
-			r -= M - i;
-			++i;
+			if (lane <= l)
+			{
+				const int j = lane;
+				double g = 0.0;
+				for (int k = 0; k <= l; ++k) g += a[i][k] * a[k][j];
+				for (int k = 0; k <= l; ++k) a[k][j] -= g * a[k][i];
+			}
 		}
-		const int j = i + r;
-		double acc = 0.0;
-#pragma unroll 6
-		for (int l = 0; l < M; ++l) acc += S.V[i][l] * S.d[l] * S.V[j][l];
-		S.A[i][j] = acc;
-		S.A[j][i] = acc;
+		__syncwarp();
+		const double dii = a[i][i];
+		__syncwarp();
+		if (lane == 0)
+		{
+			d[i] = dii;
+			a[i][i] = 1.0;
+		}
+		if (lane <= l)
+		{
+			a[lane][i] = 0.0;
+			a[i][lane] = 0.0;
+		}
+		__syncwarp();
+	}
+
+	// --- QL with implicit shifts (tql2) ----------------------------------------
+	// d, e are read by every lane and written by lane 0 only; every lane evaluates
+	// the same scalar recurrence, lane k rotates row k of Z.
+	if (lane == 0)
+	{
+		for (int i = 1; i < M; ++i) ev[i - 1] = ev[i];
+		ev[M - 1] = 0.0;
+	}
+	__syncwarp();
+	bool converged = true;
+	for (int l = 0; l < M && converged; ++l)
+	{
+		int iter = 0;
+		int mm;
+		do
+		{
+			for (mm = l; mm < M - 1; ++mm)
+			{
+				const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
+				if (fabs(ev[mm]) <= 2.220446049250313e-16 * dd) break;
+			}
+			if (mm != l)
+			{
+				if (iter++ == PSD_MAX_QL_ITER)
+				{
+					converged = false;
+					break;
+				}
+				double g = (d[l + 1] - d[l]) / (2.0 * ev[l]);
+				double r = hypot(g, 1.0);
+				g = d[mm] - d[l] + ev[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
+				double s = 1.0, c = 1.0, p = 0.0;
+				int i;
+				bool zero_r = false;
+				for (i = mm - 1; i >= l; --i)
+				{
+					const double f = s * ev[i], b = c * ev[i];
+					r = hypot(f, g);
+					__syncwarp();
+					if (lane == 0) ev[i + 1] = r;
+					if (r == 0.0)
+					{
+						const double di1 = d[i + 1];
+						__syncwarp();
+						if (lane == 0)
+						{
+							d[i + 1] = di1 - p;
+							ev[mm] = 0.0;
+						}
+						__syncwarp();
+						zero_r = true;
+						break;
+					}
+					s = f / r;
+					c = g / r;
+					g = d[i + 1] - p;
+					r = (d[i] - g) * s + 2.0 * c * b;
+					p = s * r;
+					__syncwarp();
+					if (lane == 0) d[i + 1] = g + p;
+					g = c * r - b;
+					if (lane < M)
+					{
+						const double zf = a[lane][i + 1], zi = a[lane][i];
+						a[lane][i + 1] = s * zi + c * zf;
+						a[lane][i] = c * zi - s * zf;
+					}
+				}
+				if (zero_r && i >= l) continue;
+				const double dl = d[l];
+				__syncwarp();
+				if (lane == 0)
+				{
+					d[l] = dl - p;
+					ev[l] = g;
+					ev[mm] = 0.0;
+				}
+				__syncwarp();
+			}
+		} while (mm != l);
+	}
+	__syncwarp();
+	if (!converged) return;
+
+	double lmin = INFINITY;
+	if (lane < M) lmin = d[lane];
+	lmin = warp_allmin(lmin);
+	if (!(lmin <= 0.0)) return; // all eigenvalues > 0: A stays as it is
+	// R = Z max(l, 0) Z^T, lane i computes row i
+	if (lane < M)
+	{
+		double zi[M];
+#pragma unroll
+		for (int k = 0; k < M; ++k) zi[k] = a[lane][k] * (d[k] > 0.0 ? d[k] : 0.0);
+		for (int j = 0; j < M; ++j)
+		{
+			double acc = 0.0;
+#pragma unroll
+			for (int k = 0; k < M; ++k) acc += zi[k] * a[j][k];
+			S.R[lane][j] = acc;
+		}
 	}
 	__syncwarp();
 #pragma unroll
@@ -1178,8 +1244,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_project_psd(DevMesh m, T *__rest
 		T *rec = stage + (size_t)sidx[b] * RP;
 		for (int k = lane; k < 9 * N; k += 32)
 		{
-			const int a = k / 9, cc = (k % 9) / 3, r = k % 3;
-			rec[k] = T(S.A[3 * a + r][3 * b + cc]);
+			const int aa = k / 9, cc = (k % 9) / 3, r = k % 3;
+			rec[k] = T(S.R[3 * aa + r][3 * b + cc]);
 		}
 	}
 }
@@ -1199,8 +1265,7 @@ static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const
 	if (project_psd && m.E > 0)
 	{
 		constexpr int PW = 4;
-		constexpr int NBP = (PsdWarp<EL>::H * (PsdWarp<EL>::H + 1)) / 2;
-		const size_t bytes_p = PW * sizeof(PsdWarp<EL>) + 2 * NBP;
+		const size_t bytes_p = PW * sizeof(PsdWarp<EL>);
 		e = cudaFuncSetAttribute(k_project_psd<EL, T, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
 		if (e != cudaSuccess) return e;
 		k_project_psd<EL, T, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
