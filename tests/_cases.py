@@ -28,3 +28,31 @@ def rel_err(a, b):
     b = np.asarray(b, dtype=np.float64)
     den = np.linalg.norm(b.ravel())
     return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))
+
+
+def permuted(mesh, u, seed=0):
+    """The same mesh with elements, FE nodes and geometric nodes renumbered at
+    random (no locality left).  Returns (mesh', u', node_perm, elem_perm): FE node
+    i becomes node_perm[i], element elem_perm[k] becomes element k, and
+    u'[3*node_perm[i] + d] = u[3*i + d]."""
+    import copy
+    rng = np.random.default_rng(seed)
+    m2 = copy.copy(mesh)
+    pe = rng.permutation(mesh.n_elements)
+    pn = rng.permutation(mesh.n_nodes)
+    m2.conn = np.ascontiguousarray(pn[mesh.conn[pe]].astype(np.int32))
+    node_pos = np.empty_like(mesh.node_pos)
+    node_pos[pn] = mesh.node_pos
+    m2.node_pos = node_pos
+    X = np.empty_like(mesh.X)
+    if mesh.gconn is mesh.conn:
+        m2.gconn = m2.conn
+        X[pn] = mesh.X
+    else:
+        pg = rng.permutation(mesh.n_geom_nodes)
+        m2.gconn = np.ascontiguousarray(pg[mesh.gconn[pe]].astype(np.int32))
+        X[pg] = mesh.X
+    m2.X = X
+    u2 = np.empty_like(u)
+    u2.reshape(-1, 3)[pn] = u.reshape(-1, 3)
+    return m2, u2, pn, pe
