@@ -1172,7 +1172,20 @@ __global__ void __launch_bounds__(WARPS * 32) k_project_psd(DevMesh m, T *__rest
 				for (i = mm - 1; i >= l; --i)
 				{
 					const double f = s * ev[i], b = c * ev[i];
-					r = hypot(f, g);
+					// r = |(f, g)| and 1/r from one reciprocal square root; hypot and two
+					// divisions only where f^2 + g^2 would leave the normal range
+					const double rr = f * f + g * g;
+					double ri;
+					if (rr > 1e-300 && rr < 1e300)
+					{
+						ri = rsqrt(rr);
+						r = rr * ri;
+					}
+					else
+					{
+						r = hypot(f, g);
+						ri = 1.0 / r;
+					}
 					__syncwarp();
 					if (lane == 0) ev[i + 1] = r;
 					if (r == 0.0)
@@ -1188,8 +1201,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_project_psd(DevMesh m, T *__rest
 						zero_r = true;
 						break;
 					}
-					s = f / r;
-					c = g / r;
+					s = f * ri;
+					c = g * ri;
 					g = d[i + 1] - p;
 					r = (d[i] - g) * s + 2.0 * c * b;
 					p = s * r;
