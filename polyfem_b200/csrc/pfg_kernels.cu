@@ -976,27 +976,56 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 // ---------------------------------------------------------------------------
 // ipc::project_to_psd (PSDProjectionMethod::CLAMP), applied to every element
 // matrix before the scatter when NLAssembler::assemble_hessian is called with
-// project_to_psd (Assembler.cpp:693-694).  The element matrix is rebuilt from its
-// n records, A[3a+r][3b+c] = record_b[9a + 3c + r], in FP64.  A warp (lane i
-// owning row/column i) diagonalises it with the classical symmetric eigensolver:
-// Householder reduction to tridiagonal form with the orthogonal factor
-// accumulated (EISPACK tred2), then the QL algorithm with implicit shifts on the
-// tridiagonal matrix, rotating the accumulated factor (EISPACK tql2; the scalar
-// recurrence is evaluated identically on every lane, each lane rotates its own
-// row).  If the smallest eigenvalue is > 0, or the matrix holds NaN, or QL does
-// not converge in PSD_MAX_QL_ITER iterations for an eigenvalue, the records are
-// left as they are; otherwise Z max(l, 0) Z^T is written back, rounded to the
-// record type.
+// project_to_psd (Assembler.cpp:693-694): A = Z diag(l) Z^T is replaced by
+// Z diag(max(l, 0)) Z^T when its smallest eigenvalue is <= 0.  Equivalently
+// A+ = A + sum_{l_j < 0} |l_j| z_j z_j^T, which needs only the eigenpairs with
+// l_j < 0; this kernel computes those and nothing else.  One warp per element,
+// all in FP64, the element matrix A[3a+r][3b+c] = record_b[9a + 3c + r]:
+//   1. Householder reduction to tridiagonal T = Q^T A Q (EISPACK tred2 without
+//      the accumulation of Q), lane j holding row j of A in registers and
+//      applying the symmetric rank-2 update to its own row; the reflectors
+//      u_i (with 1/h_i) stay in shared memory.
+//   2. T is scaled by its Gershgorin bound ||T|| (so |l| <= 1) and the number k
+//      of eigenvalues below -tau is one Sturm count (LDL^T sign count).
+//      k == 0: the matrix counts as PSD and the records stay as they are.
+//   3. The k eigenvalues by multisection: 32 / k lanes per eigenvalue each
+//      evaluate a Sturm count at an interior point of the eigenvalue's interval,
+//      a ballot picks the sub-interval, until the width is <= 1e-15 ||T||.
+//   4. Lane j (< k) computes eigenvector j of T by inverse iteration with that
+//      shift (tridiagonal LU without pivoting, tiny pivots replaced by
+//      +-eps ||T||), PSD_INV_ITERS steps, each followed by modified
+//      Gram-Schmidt across the k lanes (clustered eigenvalues).
+//   5. x_j = Q y_j through the stored reflectors, w_j = sqrt(|l_j|) x_j, and
+//      every record entry becomes A + sum_j w_j w_j^T (rounded to the record
+//      type).
+// Eigenvalues in (-tau ||T||, 0] are left in place where the reference clamps
+// them to zero; tau sits above the rounding noise of the record type: 1e-12 for
+// FP64 records (the rigid-motion null space of an element matrix is computed at
+// +-1e-15 ||A||), 1e-6 for FP32 records (rounding A to FP32 moves those null
+// eigenvalues by up to ~3e-7 ||A||).  The difference is below tau ||A|| per
+// element.
+// A matrix holding NaN, or whose inverse iteration overflows, is left as it is.
+// The reciprocals of the inverse iteration's LU pivots use the hardware
+// approximation (rcp.approx.ftz.f64) refined by two Newton-Raphson steps.
 // ---------------------------------------------------------------------------
-constexpr int PSD_MAX_QL_ITER = 60;
+template <class T>
+__host__ __device__ constexpr double psd_tau() { return sizeof(T) == 8 ? 1e-12 : 1e-6; } // relative to ||T||
+constexpr double PSD_PIVMIN = 1e-280;  // pivot given to a zero Sturm minor (scaled T)
+constexpr double PSD_WIDTH = 1e-15;    // bisection stops at this interval width
+constexpr int PSD_MAX_BISECT = 80;     // 53 halvings reach PSD_WIDTH from width 1
+constexpr int PSD_INV_ITERS = 2;
 
 template <class EL>
 struct PsdWarp
 {
-	static constexpr int M = 3 * EL::N, LD = M + 1;
-	double A[M][LD]; // the element matrix, then the orthogonal factor Z
-	double R[M][LD]; // the projected matrix
-	double d[M], e[M];
+	static constexpr int M = 3 * EL::N;
+	static_assert(M % 2 == 0, "rows are read as double2");
+	double V[M * M]; // reflector i in row i (zero beyond column i-1); later w_j in row j
+	double2 de2[M];  // scaled diagonal of T and squared off-diagonal (T[i-1][i]^2)
+	double en[M];    // off-diagonal T[i-1][i] (raw, then scaled); en[0] = 0
+	double hinv[M];  // 1/h_i of reflector i, 0 where step i has none
+	double row[M];   // row i of A during tridiagonalisation step i
+	double buf[M];   // q of a tridiagonalisation step; a Gram-Schmidt vector
 };
 
 __device__ __forceinline__ double warp_allsum(double v)
@@ -1005,261 +1034,384 @@ __device__ __forceinline__ double warp_allsum(double v)
 	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
 	return v;
 }
-__device__ __forceinline__ double warp_allmin(double v)
+__device__ __forceinline__ double warp_allmax(double v)
 {
 #pragma unroll
-	for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+	for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
 	return v;
 }
 
+// 1/q: hardware approximation refined by two Newton-Raphson steps r += r (1 - q r)
+__device__ __forceinline__ double rcp_nr(double q)
+{
+	double r;
+	asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
+	double e = fma(-q, r, 1.0);
+	r = fma(r, e, r);
+	e = fma(-q, r, 1.0);
+	return fma(r, e, r);
+}
+
+// Number of eigenvalues of the scaled T below x: the sign changes of the leading
+// principal minors p_i = det(T_i - x I) = (d_i - x) p_{i-1} - e_i^2 p_{i-2}
+// (Sturm sequence), i.e. the negative pivots q_i = p_i / p_{i-1} of the LDL^T
+// factorisation of T - x I, without a division.  A zero minor becomes
+// -PSD_PIVMIN p_{i-1} (a pivot of -PSD_PIVMIN, as the LDL^T count does); the pair
+// (p_i, p_{i-1}) is rescaled by 2^500 every fourth step once |p_i| < 2^-500, so
+// no minor underflows (|d_i - x| <= 2.001 and e_i^2 <= 1 bound the growth by
+// (1 + sqrt 2)^30 < 2^40 between rescalings).
+template <int M>
+__device__ __forceinline__ int sturm_count(const double2 *__restrict__ de2, double x)
+{
+	double pm = 1.0, p = de2[0].x - x;
+	if (p == 0.0) p = -PSD_PIVMIN;
+	int c = p < 0.0;
+#pragma unroll
+	for (int i = 1; i < M; ++i)
+	{
+		const double2 v = de2[i];
+		double pn = fma(v.x - x, p, -(v.y * pm));
+		if (pn == 0.0) pn = -PSD_PIVMIN * p;
+		c += (pn < 0.0) != (p < 0.0);
+		if ((i & 3) == 0)
+		{
+			const double sc = fabs(pn) < 0x1p-500 ? 0x1p500 : 1.0;
+			pn *= sc;
+			p *= sc;
+		}
+		pm = p;
+		p = pn;
+	}
+	return c;
+}
+
+// 3 CTAs of 4 warps per SM: at most 168 registers a thread (a few spill for P2)
 template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_project_psd(DevMesh m, T *__restrict__ stage)
+__global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__restrict__ stage)
 {
 	using W = PsdWarp<EL>;
 	constexpr int N = EL::N, M = W::M, RP = rec_pad<EL, T>();
+	constexpr unsigned FULL = 0xffffffffu;
 	static_assert(M <= 32, "one lane per row");
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	W &S = reinterpret_cast<W *>(smem_raw)[threadIdx.x >> 5];
 	const int lane = threadIdx.x & 31;
 	const int e = blockIdx.x * WARPS + (threadIdx.x >> 5);
 	if (e >= m.E) return;
-	double(*a)[W::LD] = S.A;
-	double *d = S.d, *ev = S.e;
 	int sidx[N];
 #pragma unroll
 	for (int b = 0; b < N; ++b) sidx[b] = __ldg(m.eb_inc + (size_t)e * N + b);
+	// lane i < M owns row i: A[i][3b+c] = record_b[9 (i/3) + 3c + i%3]
+	const int off = 9 * (lane / 3) + lane % 3;
+
+	double a[M];
 #pragma unroll
 	for (int b = 0; b < N; ++b)
-	{
-		const T *rec = stage + (size_t)sidx[b] * RP;
-		for (int k = lane; k < 9 * N; k += 32)
+#pragma unroll
+		for (int c = 0; c < 3; ++c)
 		{
-			const int aa = k / 9, cc = (k % 9) / 3, r = k % 3;
-			a[3 * aa + r][3 * b + cc] = double(rec[k]);
+			a[3 * b + c] = 0.0;
+			if (lane < M) a[3 * b + c] = double(stage[(size_t)sidx[b] * RP + off + 3 * c]);
 		}
-	}
-	__syncwarp();
 	bool nan_in = false;
-	if (lane < M)
-		for (int k = 0; k < M; ++k) nan_in |= isnan(a[lane][k]);
-	if (__any_sync(0xffffffffu, nan_in)) return; // NaN propagates unchanged
+#pragma unroll
+	for (int t = 0; t < M; ++t) nan_in |= isnan(a[t]);
+	if (__any_sync(FULL, nan_in)) return; // NaN propagates unchanged
 
-	// --- Householder reduction to tridiagonal form (tred2) -------------------
-	for (int i = M - 1; i > 0; --i)
+	// --- 1. tridiagonalisation ------------------------------------------------
+	// Step i (l = i - 1) annihilates row/column i left of the subdiagonal.  Row i is
+	// broadcast through S.row by lane i; the reflector u (zero beyond l) goes to
+	// V[i][*]; rows j <= l apply A -= u q^T + q u^T to themselves, the other lanes
+	// hold u_j = q_j = 0 and leave their rows unchanged.
+	double *V = S.V;
+	const double2 *row2 = reinterpret_cast<const double2 *>(S.row);
+	const double2 *q2 = reinterpret_cast<const double2 *>(S.buf);
+	if (lane < M)
+	{
+		V[lane] = 0.0;     // rows 0 and 1 hold no reflector
+		V[M + lane] = 0.0;
+	}
+#pragma unroll 1
+	for (int i = M - 1; i >= 2; --i)
 	{
 		const int l = i - 1;
-		double h = 0.0;
-		if (l > 0)
+		const bool mine = lane <= l;
+		if (lane == i)
 		{
-			const double scale = warp_allsum(lane <= l ? fabs(a[i][lane]) : 0.0);
-			if (scale == 0.0)
-			{
-				if (lane == 0) ev[i] = a[i][l];
-			}
-			else
-			{
-				if (lane <= l) a[i][lane] /= scale;
-				__syncwarp();
-				h = warp_allsum(lane <= l ? a[i][lane] * a[i][lane] : 0.0);
-				const double f = a[i][l];
-				const double g = f >= 0.0 ? -sqrt(h) : sqrt(h);
-				h -= f * g;
-				__syncwarp();
-				if (lane == 0)
-				{
-					ev[i] = scale * g;
-					a[i][l] = f - g;
-				}
-				__syncwarp();
-				double ej = 0.0;
-				if (lane <= l)
-				{
-					const int j = lane;
-					a[j][i] = a[i][j] / h;
-					double gg = 0.0;
-					for (int k = 0; k <= j; ++k) gg += a[j][k] * a[i][k];
-					for (int k = j + 1; k <= l; ++k) gg += a[k][j] * a[i][k];
-					ej = gg / h;
-				}
-				const double ff = warp_allsum(lane <= l ? ej * a[i][lane] : 0.0);
-				const double hh = ff / (h + h);
-				if (lane <= l) ev[lane] = ej - hh * a[i][lane];
-				__syncwarp();
-				if (lane <= l)
-				{
-					const int j = lane;
-					const double fj = a[i][j], gj = ev[j];
-					for (int k = 0; k <= j; ++k) a[j][k] -= (fj * ev[k] + gj * a[i][k]);
-				}
-				__syncwarp();
-			}
-		}
-		else if (lane == 0)
-			ev[i] = a[i][l];
-		if (lane == 0) d[i] = h;
-		__syncwarp();
-	}
-	if (lane == 0)
-	{
-		d[0] = 0.0;
-		ev[0] = 0.0;
-	}
-	__syncwarp();
-	// accumulate the orthogonal factor in place
-	for (int i = 0; i < M; ++i)
-	{
-		const int l = i - 1;
-		if (d[i] != 0.0)
-		{
-			if (lane <= l)
-			{
-				const int j = lane;
-				double g = 0.0;
-				for (int k = 0; k <= l; ++k) g += a[i][k] * a[k][j];
-				for (int k = 0; k <= l; ++k) a[k][j] -= g * a[k][i];
-			}
+			double2 *w2 = reinterpret_cast<double2 *>(S.row);
+#pragma unroll
+			for (int t = 0; t < M; t += 2) w2[t / 2] = make_double2(a[t], a[t + 1]);
 		}
 		__syncwarp();
-		const double dii = a[i][i];
-		__syncwarp();
+		double x = mine ? S.row[lane] : 0.0; // A[i][lane]
+		const double scale = warp_allsum(fabs(x));
+		double u = 0.0, q = 0.0, g = 0.0, ih = 0.0;
+		if (scale != 0.0)
+		{
+			x *= 1.0 / scale;
+			const double sig = warp_allsum(x * x);
+			const double f = __shfl_sync(FULL, x, l);
+			g = f >= 0.0 ? -sqrt(sig) : sqrt(sig);
+			ih = 1.0 / (sig - f * g);
+			u = lane == l ? f - g : x;
+		}
+		else
+			g = 0.0;
+		if (lane < M) V[i * M + lane] = u;
 		if (lane == 0)
 		{
-			d[i] = dii;
-			a[i][i] = 1.0;
+			S.en[i] = scale * g;
+			S.hinv[i] = ih;
 		}
-		if (lane <= l)
+		__syncwarp();
+		if (scale != 0.0)
 		{
-			a[lane][i] = 0.0;
-			a[i][lane] = 0.0;
+			const double2 *u2 = reinterpret_cast<const double2 *>(V + i * M);
+			double p0 = 0.0, p1 = 0.0;
+#pragma unroll
+			for (int t = 0; t < M; t += 2)
+			{
+				const double2 uu = u2[t / 2];
+				p0 = fma(a[t], uu.x, p0);
+				p1 = fma(a[t + 1], uu.y, p1);
+			}
+			const double p = (p0 + p1) * ih;
+			const double kk = warp_allsum(mine ? p * u : 0.0) * (0.5 * ih);
+			q = mine ? p - kk * u : 0.0;
+			if (lane < M) S.buf[lane] = q;
+			__syncwarp();
+#pragma unroll
+			for (int t = 0; t < M; t += 2)
+			{
+				const double2 uu = u2[t / 2], qq = q2[t / 2];
+				a[t] = fma(-u, qq.x, fma(-q, uu.x, a[t]));
+				a[t + 1] = fma(-u, qq.y, fma(-q, uu.y, a[t + 1]));
+			}
 		}
 		__syncwarp();
 	}
-
-	// --- QL with implicit shifts (tql2) ----------------------------------------
-	// d, e are read by every lane and written by lane 0 only; every lane evaluates
-	// the same scalar recurrence, lane k rotates row k of Z.
+	double dj = 0.0;
+#pragma unroll
+	for (int t = 0; t < M; ++t)
+		if (t == lane) dj = a[t];
+	if (lane == 1) S.en[1] = a[0]; // A[1][0]
 	if (lane == 0)
 	{
-		for (int i = 1; i < M; ++i) ev[i - 1] = ev[i];
-		ev[M - 1] = 0.0;
+		S.en[0] = 0.0;
+		S.hinv[0] = 0.0;
+		S.hinv[1] = 0.0;
 	}
 	__syncwarp();
-	bool converged = true;
-	for (int l = 0; l < M && converged; ++l)
-	{
-		int iter = 0;
-		int mm;
-		do
-		{
-			for (mm = l; mm < M - 1; ++mm)
-			{
-				const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
-				if (fabs(ev[mm]) <= 2.220446049250313e-16 * dd) break;
-			}
-			if (mm != l)
-			{
-				if (iter++ == PSD_MAX_QL_ITER)
-				{
-					converged = false;
-					break;
-				}
-				double g = (d[l + 1] - d[l]) / (2.0 * ev[l]);
-				double r = hypot(g, 1.0);
-				g = d[mm] - d[l] + ev[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
-				double s = 1.0, c = 1.0, p = 0.0;
-				int i;
-				bool zero_r = false;
-				for (i = mm - 1; i >= l; --i)
-				{
-					const double f = s * ev[i], b = c * ev[i];
-					// r = |(f, g)| and 1/r from one reciprocal square root; hypot and two
-					// divisions only where f^2 + g^2 would leave the normal range
-					const double rr = f * f + g * g;
-					double ri;
-					if (rr > 1e-300 && rr < 1e300)
-					{
-						ri = rsqrt(rr);
-						r = rr * ri;
-					}
-					else
-					{
-						r = hypot(f, g);
-						ri = 1.0 / r;
-					}
-					__syncwarp();
-					if (lane == 0) ev[i + 1] = r;
-					if (r == 0.0)
-					{
-						const double di1 = d[i + 1];
-						__syncwarp();
-						if (lane == 0)
-						{
-							d[i + 1] = di1 - p;
-							ev[mm] = 0.0;
-						}
-						__syncwarp();
-						zero_r = true;
-						break;
-					}
-					s = f * ri;
-					c = g * ri;
-					g = d[i + 1] - p;
-					r = (d[i] - g) * s + 2.0 * c * b;
-					p = s * r;
-					__syncwarp();
-					if (lane == 0) d[i + 1] = g + p;
-					g = c * r - b;
-					if (lane < M)
-					{
-						const double zf = a[lane][i + 1], zi = a[lane][i];
-						a[lane][i + 1] = s * zi + c * zf;
-						a[lane][i] = c * zi - s * zf;
-					}
-				}
-				if (zero_r && i >= l) continue;
-				const double dl = d[l];
-				__syncwarp();
-				if (lane == 0)
-				{
-					d[l] = dl - p;
-					ev[l] = g;
-					ev[mm] = 0.0;
-				}
-				__syncwarp();
-			}
-		} while (mm != l);
-	}
-	__syncwarp();
-	if (!converged) return;
 
-	double lmin = INFINITY;
-	if (lane < M) lmin = d[lane];
-	lmin = warp_allmin(lmin);
-	if (!(lmin <= 0.0)) return; // all eigenvalues > 0: A stays as it is
-	// R = Z max(l, 0) Z^T, lane i computes row i
+	// --- 2./3. scale; count below -tau, then multisection ------------------------
+	const double ej = lane < M ? S.en[lane] : 0.0;
+	const double ej1 = lane + 1 < M ? S.en[lane + 1] : 0.0;
+	const double nrm = warp_allmax(lane < M ? fabs(dj) + fabs(ej) + fabs(ej1) : 0.0);
+	if (!(nrm > 0.0 && nrm <= 1.7976931348623157e308)) return; // zero, Inf or NaN
+	const double inv = 1.0 / nrm;
+	__syncwarp();
 	if (lane < M)
 	{
-		double zi[M];
-#pragma unroll
-		for (int k = 0; k < M; ++k) zi[k] = a[lane][k] * (d[k] > 0.0 ? d[k] : 0.0);
-		for (int j = 0; j < M; ++j)
+		const double en = ej * inv;
+		S.de2[lane] = make_double2(dj * inv, en * en);
+		S.en[lane] = en;
+	}
+	__syncwarp();
+	// iteration -1 counts the eigenvalues below -tau on every lane; later
+	// iterations: 32 / k lanes per eigenvalue j < k, each at an interior point of
+	// the eigenvalue's interval [lo, hi) (count(lo) <= j < count(hi))
+	int k = 0, G = 1, jg = 0;
+	bool act = false;
+	unsigned gmask = 0u;
+	double frac = 0.0, lo = -1.0 - 1e-3, hi = -psd_tau<T>(), x = hi;
+#pragma unroll 1
+	for (int it = -1; it < PSD_MAX_BISECT; ++it)
+	{
+		bool done = true;
+		if (it >= 0)
 		{
-			double acc = 0.0;
+			done = !act || hi - lo <= PSD_WIDTH;
+			if (__all_sync(FULL, done)) break;
+			x = fma(hi - lo, frac, lo);
+		}
+		const int c = sturm_count<M>(S.de2, x);
+		if (it < 0)
+		{
+			k = c;
+			if (k == 0) return; // PSD: the records stay as they are
+			G = 32 / k;
+			jg = lane / G;
+			act = jg < k;
+			gmask = G == 32 ? FULL : ((1u << G) - 1u);
+			frac = double(lane - jg * G + 1) / double(G + 1);
+			continue;
+		}
+		const unsigned bal = __ballot_sync(FULL, c <= jg);
+		const unsigned mg = act ? (bal >> (jg * G)) & gmask : 0u;
+		// first point of the group with more than jg eigenvalues below it
+		const int tf = mg == gmask ? G : __ffs(~mg) - 1;
+		const double xlo = __shfl_sync(FULL, x, (jg * G + tf - 1) & 31);
+		const double xhi = __shfl_sync(FULL, x, (jg * G + tf) & 31);
+		if (!done)
+		{
+			if (tf > 0) lo = xlo;
+			if (tf < G) hi = xhi;
+		}
+	}
+	const bool vec = lane < k;
+	const double sig = __shfl_sync(FULL, 0.5 * (lo + hi), (lane * G) & 31);
+
+	// --- 4. inverse iteration, lane j -> eigenvector j ---------------------------
+	double y[M];
 #pragma unroll
-			for (int k = 0; k < M; ++k) acc += zi[k] * a[j][k];
-			S.R[lane][j] = acc;
+	for (int i = 0; i < M; ++i)
+	{
+		const unsigned hsh = (unsigned)(i * 7919 + lane * 104729 + 12345) * 2654435761u;
+		y[i] = 1.0 + 0.5 * (double)(hsh >> 8) * (1.0 / 16777216.0);
+	}
+	bool bad = false;
+	constexpr double PMIN = 2.220446049250313e-16;
+	double2 *b2 = reinterpret_cast<double2 *>(S.buf);
+#pragma unroll 1
+	for (int it = 0; it < PSD_INV_ITERS; ++it)
+	{
+		// T is re-read from shared memory in every pass (an opaque pointer keeps the
+		// compiler from holding all of it in registers across the passes)
+		const double2 *de2 = S.de2;
+		const double *enp = S.en;
+		asm volatile("" : "+l"(de2), "+l"(enp));
+		double rp[M];
+		{
+			double pv = de2[0].x - sig;
+			if (fabs(pv) < PMIN) pv = pv >= 0.0 ? PMIN : -PMIN;
+			rp[0] = rcp_nr(pv);
+		}
+#pragma unroll
+		for (int i = 1; i < M; ++i)
+		{
+			const double eni = enp[i];
+			const double mi = eni * rp[i - 1];
+			double pv = (de2[i].x - sig) - mi * eni;
+			if (fabs(pv) < PMIN) pv = pv >= 0.0 ? PMIN : -PMIN;
+			rp[i] = rcp_nr(pv);
+			y[i] = fma(-mi, y[i - 1], y[i]);
+		}
+		y[M - 1] *= rp[M - 1];
+#pragma unroll
+		for (int i = M - 2; i >= 0; --i) y[i] = fma(-enp[i + 1], y[i + 1], y[i]) * rp[i];
+		double ym = 0.0;
+#pragma unroll
+		for (int i = 0; i < M; ++i) ym = fmax(ym, fabs(y[i]));
+		bad |= vec && !(ym > 0.0 && ym <= 1.7976931348623157e308);
+		const double iy = 1.0 / ym;
+#pragma unroll
+		for (int i = 0; i < M; ++i) y[i] *= iy;
+		// modified Gram-Schmidt over lanes 0..k-1
+#pragma unroll 1
+		for (int j = 0; j < k; ++j)
+		{
+			if (lane == j)
+			{
+				double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+				for (int i = 0; i < M; i += 2)
+				{
+					s0 = fma(y[i], y[i], s0);
+					s1 = fma(y[i + 1], y[i + 1], s1);
+				}
+				const double s = s0 + s1;
+				bad |= !(s > 0.0 && s <= 1.7976931348623157e308); // NaN, overflow or a lost vector
+				const double r = rsqrt(s);
+#pragma unroll
+				for (int i = 0; i < M; i += 2)
+				{
+					y[i] *= r;
+					y[i + 1] *= r;
+					b2[i / 2] = make_double2(y[i], y[i + 1]);
+				}
+			}
+			__syncwarp();
+			if (lane > j && vec)
+			{
+				double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+				for (int i = 0; i < M; i += 2)
+				{
+					const double2 bb = b2[i / 2];
+					d0 = fma(y[i], bb.x, d0);
+					d1 = fma(y[i + 1], bb.y, d1);
+				}
+				const double dot = d0 + d1;
+#pragma unroll
+				for (int i = 0; i < M; i += 2)
+				{
+					const double2 bb = b2[i / 2];
+					y[i] = fma(-dot, bb.x, y[i]);
+					y[i + 1] = fma(-dot, bb.y, y[i + 1]);
+				}
+			}
+			__syncwarp();
+		}
+	}
+	if (__any_sync(FULL, bad)) return;
+
+	// --- 5. back-transform x = P_2 ... P_{M-1} y (reflector 2 first), w = sqrt|l| x
+#pragma unroll 1
+	for (int i = 2; i < M; ++i)
+	{
+		const double2 *u2 = reinterpret_cast<const double2 *>(V + i * M);
+		double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+		for (int t = 0; t < M; t += 2)
+		{
+			const double2 uu = u2[t / 2];
+			s0 = fma(uu.x, y[t], s0);
+			s1 = fma(uu.y, y[t + 1], s1);
+		}
+		const double s = (s0 + s1) * S.hinv[i];
+#pragma unroll
+		for (int t = 0; t < M; t += 2)
+		{
+			const double2 uu = u2[t / 2];
+			y[t] = fma(-s, uu.x, y[t]);
+			y[t + 1] = fma(-s, uu.y, y[t + 1]);
 		}
 	}
 	__syncwarp();
-#pragma unroll
-	for (int b = 0; b < N; ++b)
+	if (vec)
 	{
-		T *rec = stage + (size_t)sidx[b] * RP;
-		for (int k = lane; k < 9 * N; k += 32)
+		const double sw = sqrt(-sig * nrm);
+		double2 *w2 = reinterpret_cast<double2 *>(V + lane * M);
+#pragma unroll
+		for (int t = 0; t < M; t += 2) w2[t / 2] = make_double2(sw * y[t], sw * y[t + 1]);
+	}
+	__syncwarp();
+
+	// --- 6. row i of A + sum_j w_j w_j^T back into the records -------------------
+	if (lane < M)
+	{
+		double r[M];
+#pragma unroll
+		for (int b = 0; b < N; ++b)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) r[3 * b + c] = double(stage[(size_t)sidx[b] * RP + off + 3 * c]);
+#pragma unroll 1
+		for (int j = 0; j < k; ++j)
 		{
-			const int aa = k / 9, cc = (k % 9) / 3, r = k % 3;
-			rec[k] = T(S.R[3 * aa + r][3 * b + cc]);
+			const double wi = V[j * M + lane];
+			const double2 *w2 = reinterpret_cast<const double2 *>(V + j * M);
+#pragma unroll
+			for (int t = 0; t < M; t += 2)
+			{
+				const double2 ww = w2[t / 2];
+				r[t] = fma(wi, ww.x, r[t]);
+				r[t + 1] = fma(wi, ww.y, r[t + 1]);
+			}
 		}
+#pragma unroll
+		for (int b = 0; b < N; ++b)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) stage[(size_t)sidx[b] * RP + off + 3 * c] = T(r[3 * b + c]);
 	}
 }
 
