@@ -1085,6 +1085,112 @@ __device__ __forceinline__ int sturm_count(const double2 *__restrict__ de2, doub
 	return c;
 }
 
+// Householder step i (l = i - 1) of the tridiagonalisation (EISPACK tred2 without
+// the accumulation of Q), on the lanes' register rows a (lane j < M owns row j):
+// row i is broadcast through S.row by lane i; the reflector u = x - g e_l with
+// x = A[i][0..l], g = -sign(x_l) |x|, h = |x|^2 - x_l g, goes to V[i][*] (zero
+// beyond l); rows j <= l apply A -= u q^T + q u^T with p = A u / h,
+// q = p - (u.p / 2h) u, the other lanes hold u_j = q_j = 0.  Columns >= W are
+// untouched (W > l).  |x|^2 is formed unscaled when it lies in [1e-250, 1e250],
+// else from x / sum|x_k| as tred2 does.
+template <int M, int W, class PW>
+__device__ __forceinline__ void psd_tred2_step(PW &S, double (&a)[M], int i, int lane)
+{
+	constexpr unsigned FULL = 0xffffffffu;
+	const int l = i - 1;
+	const bool mine = lane <= l;
+	if (lane == i)
+	{
+		double2 *w2 = reinterpret_cast<double2 *>(S.row);
+#pragma unroll
+		for (int t = 0; t < W; t += 2) w2[t / 2] = make_double2(a[t], a[t + 1]);
+	}
+	__syncwarp();
+	double x = mine ? S.row[lane] : 0.0; // A[i][lane]
+	double sig = warp_allsum(x * x), scale = 1.0;
+	if (!(sig >= 1e-250 && sig <= 1e250))
+	{
+		scale = warp_allsum(fabs(x));
+		if (scale != 0.0)
+		{
+			x *= 1.0 / scale;
+			sig = warp_allsum(x * x);
+		}
+	}
+	double u = 0.0, g = 0.0, ih = 0.0;
+	if (sig != 0.0)
+	{
+		const double f = __shfl_sync(FULL, x, l);
+		g = f >= 0.0 ? -sqrt(sig) : sqrt(sig);
+		ih = rcp_nr(sig - f * g);
+		u = lane == l ? f - g : x;
+	}
+	double *V = S.V;
+	if (lane < M) V[i * M + lane] = u;
+	if (lane == 0)
+	{
+		S.en[i] = scale * g;
+		S.hinv[i] = ih;
+	}
+	__syncwarp();
+	if (ih != 0.0)
+	{
+		const double2 *u2 = reinterpret_cast<const double2 *>(V + i * M);
+		const double2 *q2 = reinterpret_cast<const double2 *>(S.buf);
+		double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+#pragma unroll
+		for (int t = 0; t < W; t += 4)
+		{
+			const double2 u01 = u2[t / 2];
+			p0 = fma(a[t], u01.x, p0);
+			p1 = fma(a[t + 1], u01.y, p1);
+			if (t + 2 < W)
+			{
+				const double2 u23 = u2[t / 2 + 1];
+				p2 = fma(a[t + 2], u23.x, p2);
+				p3 = fma(a[t + 3], u23.y, p3);
+			}
+		}
+		const double p = ((p0 + p1) + (p2 + p3)) * ih;
+		const double kk = warp_allsum(mine ? p * u : 0.0) * (0.5 * ih);
+		const double q = mine ? p - kk * u : 0.0;
+		if (lane < M) S.buf[lane] = q;
+		__syncwarp();
+#pragma unroll
+		for (int t = 0; t < W; t += 2)
+		{
+			const double2 uu = u2[t / 2], qq = q2[t / 2];
+			a[t] = fma(-u, qq.x, fma(-q, uu.x, a[t]));
+			a[t + 1] = fma(-u, qq.y, fma(-q, uu.y, a[t + 1]));
+		}
+	}
+	__syncwarp();
+}
+
+// y -= (u_i . y / h_i) u_i for the reflector u_i in V[i][*] (zero from column i on,
+// so columns >= W > i - 1 are untouched)
+template <int M, int W, class PW>
+__device__ __forceinline__ void psd_reflect(const PW &S, double (&y)[M], int i)
+{
+	const double2 *u2 = reinterpret_cast<const double2 *>(S.V + i * M);
+	double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+	for (int t = 0; t < W; t += 2)
+	{
+		const double2 uu = u2[t / 2];
+		s0 = fma(uu.x, y[t], s0);
+		s1 = fma(uu.y, y[t + 1], s1);
+	}
+	const double s = (s0 + s1) * S.hinv[i];
+#pragma unroll
+	for (int t = 0; t < W; t += 2)
+	{
+		const double2 uu = u2[t / 2];
+		y[t] = fma(-s, uu.x, y[t]);
+		y[t + 1] = fma(-s, uu.y, y[t + 1]);
+	}
+}
+
 // 3 CTAs of 4 warps per SM: at most 168 registers a thread (a few spill for P2)
 template <class EL, class T, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__restrict__ stage)
@@ -1119,77 +1225,13 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__r
 	if (__any_sync(FULL, nan_in)) return; // NaN propagates unchanged
 
 	// --- 1. tridiagonalisation ------------------------------------------------
-	// Step i (l = i - 1) annihilates row/column i left of the subdiagonal.  Row i is
-	// broadcast through S.row by lane i; the reflector u (zero beyond l) goes to
-	// V[i][*]; rows j <= l apply A -= u q^T + q u^T to themselves, the other lanes
-	// hold u_j = q_j = 0 and leave their rows unchanged.
-	double *V = S.V;
-	const double2 *row2 = reinterpret_cast<const double2 *>(S.row);
-	const double2 *q2 = reinterpret_cast<const double2 *>(S.buf);
-	if (lane < M)
-	{
-		V[lane] = 0.0;     // rows 0 and 1 hold no reflector
-		V[M + lane] = 0.0;
-	}
+	// steps M-1 .. H+1 touch all columns, steps H .. 2 only columns < H
+	constexpr int H = ((M / 2) + 1) & ~1;
 #pragma unroll 1
-	for (int i = M - 1; i >= 2; --i)
-	{
-		const int l = i - 1;
-		const bool mine = lane <= l;
-		if (lane == i)
-		{
-			double2 *w2 = reinterpret_cast<double2 *>(S.row);
-#pragma unroll
-			for (int t = 0; t < M; t += 2) w2[t / 2] = make_double2(a[t], a[t + 1]);
-		}
-		__syncwarp();
-		double x = mine ? S.row[lane] : 0.0; // A[i][lane]
-		const double scale = warp_allsum(fabs(x));
-		double u = 0.0, q = 0.0, g = 0.0, ih = 0.0;
-		if (scale != 0.0)
-		{
-			x *= 1.0 / scale;
-			const double sig = warp_allsum(x * x);
-			const double f = __shfl_sync(FULL, x, l);
-			g = f >= 0.0 ? -sqrt(sig) : sqrt(sig);
-			ih = 1.0 / (sig - f * g);
-			u = lane == l ? f - g : x;
-		}
-		else
-			g = 0.0;
-		if (lane < M) V[i * M + lane] = u;
-		if (lane == 0)
-		{
-			S.en[i] = scale * g;
-			S.hinv[i] = ih;
-		}
-		__syncwarp();
-		if (scale != 0.0)
-		{
-			const double2 *u2 = reinterpret_cast<const double2 *>(V + i * M);
-			double p0 = 0.0, p1 = 0.0;
-#pragma unroll
-			for (int t = 0; t < M; t += 2)
-			{
-				const double2 uu = u2[t / 2];
-				p0 = fma(a[t], uu.x, p0);
-				p1 = fma(a[t + 1], uu.y, p1);
-			}
-			const double p = (p0 + p1) * ih;
-			const double kk = warp_allsum(mine ? p * u : 0.0) * (0.5 * ih);
-			q = mine ? p - kk * u : 0.0;
-			if (lane < M) S.buf[lane] = q;
-			__syncwarp();
-#pragma unroll
-			for (int t = 0; t < M; t += 2)
-			{
-				const double2 uu = u2[t / 2], qq = q2[t / 2];
-				a[t] = fma(-u, qq.x, fma(-q, uu.x, a[t]));
-				a[t + 1] = fma(-u, qq.y, fma(-q, uu.y, a[t + 1]));
-			}
-		}
-		__syncwarp();
-	}
+	for (int i = M - 1; i > H; --i) psd_tred2_step<M, M>(S, a, i, lane);
+#pragma unroll 1
+	for (int i = H; i >= 2; --i) psd_tred2_step<M, H>(S, a, i, lane);
+	double *V = S.V;
 	double dj = 0.0;
 #pragma unroll
 	for (int t = 0; t < M; ++t)
@@ -1357,26 +1399,9 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__r
 
 	// --- 5. back-transform x = P_2 ... P_{M-1} y (reflector 2 first), w = sqrt|l| x
 #pragma unroll 1
-	for (int i = 2; i < M; ++i)
-	{
-		const double2 *u2 = reinterpret_cast<const double2 *>(V + i * M);
-		double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-		for (int t = 0; t < M; t += 2)
-		{
-			const double2 uu = u2[t / 2];
-			s0 = fma(uu.x, y[t], s0);
-			s1 = fma(uu.y, y[t + 1], s1);
-		}
-		const double s = (s0 + s1) * S.hinv[i];
-#pragma unroll
-		for (int t = 0; t < M; t += 2)
-		{
-			const double2 uu = u2[t / 2];
-			y[t] = fma(-s, uu.x, y[t]);
-			y[t + 1] = fma(-s, uu.y, y[t + 1]);
-		}
-	}
+	for (int i = 2; i <= H; ++i) psd_reflect<M, H>(S, y, i);
+#pragma unroll 1
+	for (int i = H + 1; i < M; ++i) psd_reflect<M, M>(S, y, i);
 	__syncwarp();
 	if (vec)
 	{
