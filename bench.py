@@ -6,8 +6,8 @@ split 6 tets/hex (384,000 elements, 531,441 nodes, 1,594,323 dofs, 134,475,849
 CSC nonzeros), 4-point quadrature, per-element lognormal Lame parameters, seeded
 synthetic displacement u = 0.02 h N(0,1).  One step = one assembly of the global
 Hessian CSC values through the path's C ABI (pfg_hessian), which launches two
-kernels: k_hessian_blocks (element blocks -> node-ordered records) and a
-reduction kernel (records -> CSC columns, summed per entry in a fixed order).
+kernels: k_hessian_blocks (element blocks -> one packed block triangle per element)
+and a reduction kernel (blocks -> CSC columns, summed per entry in a fixed order).
 
   value     : split-precision Hessian assembly, inputs resident in HBM (elements/s)
   e2e       : the same call with host buffers (pinned u in, CSC values out) (elements/s)
@@ -40,7 +40,7 @@ METRIC = "NeoHookean elem Hessians/s on 1 B200: split-FP32 vs FP64, rel err vs F
 UNIT = "elements/s"
 SEED_LAME, SEED_U = 5, 2
 PRECISION_NOTE = ("split32 = FP64 kinematics (J^-T, F, det/log J, F^-T, basis gradients) + FP32 "
-                  "block contraction and FP32 element records + FP64 per-entry sums and CSC values "
+                  "block contraction and FP32 staged element blocks + FP64 per-entry sums and CSC values "
                   "(CUDA cores)")
 
 
@@ -72,12 +72,14 @@ def algorithmic_bytes(mesh, nnz: int) -> int:
             + E * n * n * 4 + mesh.n_nodes * 4 + nnz * 8)
 
 
-def staged_bytes(mesh, nnz: int, rec_bytes: int) -> int:
-    """HBM bytes the two-pass design moves when the records do not stay in L2:
-    algorithmic bytes + records written by pass 1 and read back by pass 2
-    (one padded record of 9n values per incidence) + the row ranks pass 2 reads."""
+def staged_bytes(mesh, nnz: int, tri_bytes: int) -> int:
+    """HBM bytes the two-pass design moves when the staged blocks do not stay in L2:
+    algorithmic bytes + the block triangles written by pass 1 and read once by
+    pass 2 (one padded triangle of 9 n(n+1)/2 values per element; the second read
+    of an off-diagonal block comes from L2).  The 32-bit reduction plan is the
+    algorithmic slot map's 4 bytes per node pair."""
     E, n = mesh.n_elements, mesh.conn.shape[1]
-    return algorithmic_bytes(mesh, nnz) + 2 * E * n * rec_bytes + E * n * n * 2
+    return algorithmic_bytes(mesh, nnz) + 2 * E * tri_bytes
 
 
 # ----------------------------------------------------------------- clocks
@@ -367,7 +369,7 @@ def run_gpu(args):
     e2e_ms = _events_ms(stream, lambda: call(PFG_SPLIT32, PFG_MEM_HOST, hptr_u, hptr_v), args.steps)
     e2e_ms = max_over_ranks(e2e_ms)
 
-    rec_bytes = 32 * ((9 * 10 * 4 + 31) // 32)
+    tri_bytes = 4 * 8 * ((9 * 55 + 7) // 8)  # P2 block triangle in FP32
     bytes_alg = algorithmic_bytes(mesh, nnz)
     peak, peak_src = _peaks()
     achieved = bytes_alg / (ms_split * 1e-3) / 1e9
@@ -391,8 +393,8 @@ def run_gpu(args):
             "config": {"workload": workload_name(args.grid), "global_batch": world * E,
                        "parallelism": f"replicas x{world}", "precision": "split32",
                        "precision_detail": PRECISION_NOTE, "nnz": nnz,
-                       "l2": "no flush; every step writes the 1.08 GB CSC values and 1.4 GB of element "
-                             "records, both larger than the 126 MB L2"},
+                       "l2": "no flush; every step writes the 1.08 GB CSC values and 0.76 GB of element "
+                             "block triangles, both larger than the 126 MB L2"},
             "fp64": {"value": world * E / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64},
             "split_over_fp64": ms64 / ms_split,
             "rel_err_vs_fp64": rel_err,
@@ -401,7 +403,7 @@ def run_gpu(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "bytes_alg_per_launch": bytes_alg,
-                         "staged_bytes_per_launch": staged_bytes(mesh, nnz, rec_bytes),
+                         "staged_bytes_per_launch": staged_bytes(mesh, nnz, tri_bytes),
                          "note": "one pfg_hessian call = k_hessian_blocks + the reduction kernel, CUDA events "
                                  "on the context's stream; frac of measured HBM copy bandwidth; traffic = ncu "
                                  "DRAM bytes per element of the 24^3 capture x elements"},

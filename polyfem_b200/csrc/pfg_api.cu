@@ -34,7 +34,8 @@ struct pfg_context
 	DevPattern pat;
 	int *d_outer = nullptr, *d_inner = nullptr;
 	double *d_values = nullptr;
-	unsigned short *d_contrib = nullptr, *d_blk_rel = nullptr;
+	unsigned int *d_contrib = nullptr;
+	unsigned short *d_blk_rel = nullptr;
 	// Dirichlet reduction (pfg_set_dirichlet)
 	bool has_dirichlet = false;
 	std::vector<int> h_constrained;      // sorted unique constrained dofs
@@ -165,8 +166,7 @@ int ensure_hess_stage(pfg_context *c, int prec)
 	if (!c->d_hess_stage[k])
 	{
 		const size_t tsz = k == 0 ? sizeof(double) : sizeof(float);
-		const size_t rec = ((9 * c->n * tsz + 31) / 32) * 32; // padded record bytes
-		const size_t n = (size_t)std::max(c->m.E, 1) * c->n * rec;
+		const size_t n = (size_t)std::max(c->m.E, 1) * tri_pad(c->n) * tsz; // one block triangle per element
 		PFG_CUDA(c, cudaMalloc(&c->d_hess_stage[k], n));
 	}
 	return PFG_OK;
@@ -277,18 +277,20 @@ int build_pattern(pfg_context *c)
 	});
 
 	// Reduction plan of every column node B (the device form of SparseMatrixCache's
-	// second_cache_): its n * (#incidences) record blocks, grouped by the row rank
+	// second_cache_): its n * (#incidences) element blocks, grouped by the row rank
 	// they land on, incidences ascending inside a group.  contrib holds each block
-	// as (incidence - first incidence of B) * n + local row node, relative to B's
-	// first record; blk_rel[block] is where the block's group starts, relative to
-	// B's first contribution.  Both fit in 16 bits while a node has at most
-	// 65535 / n incidences.
+	// as its offset in the staged block triangles (transposed flag for a > b);
+	// blk_rel[block] is where the block's group starts, relative to B's first
+	// contribution, in 16 bits while a node has at most 65535 / n incidences.
 	long long max_tot = 0;
 	for (int B = 0; B < N; ++B) max_tot = std::max(max_tot, (ioff[B + 1] - ioff[B]) * n);
 	if (max_tot > 65535)
 		return fail(c, PFG_ERR_UNSUPPORTED,
 					"a node has more than 65535 incident (element, local node) pairs; the 16-bit reduction plan cannot hold it");
-	std::vector<unsigned short> contrib((size_t)nstrip * n);
+	const long long tp = tri_pad(n);
+	if ((long long)c->m.E * tp > 0x7fffffffLL)
+		return fail(c, PFG_ERR_UNSUPPORTED, "E * (9 n(n+1)/2, padded) staged block values exceed 2^31-1 (31-bit plan offsets)");
+	std::vector<unsigned int> contrib((size_t)nstrip * n);
 	std::vector<unsigned short> blk_rel((size_t)noff[N]);
 	parallel_ranges(N, [&](long long s0, long long s1, int) {
 		std::vector<int> pos;
@@ -301,22 +303,31 @@ int build_pattern(pfg_context *c)
 				for (int a = 0; a < n; ++a) pos[strip_rank[(size_t)k * n + a] + 1]++;
 			for (int r = 0; r < d; ++r) pos[r + 1] += pos[r];
 			for (int r = 0; r < d; ++r) blk_rel[noff[B] + r] = (unsigned short)pos[r];
-			unsigned short *cb = contrib.data() + (size_t)k0 * n;
+			unsigned int *cb = contrib.data() + (size_t)k0 * n;
 			for (long long k = k0; k < k1; ++k)
+			{
+				const int el = inc[k];
+				const int *ce = conn + (size_t)el * n;
+				int b = 0;
+				while (ce[b] != B) ++b;
 				for (int a = 0; a < n; ++a)
-					cb[pos[strip_rank[(size_t)k * n + a]]++] = (unsigned short)((k - k0) * n + a);
+				{
+					const unsigned blk = (unsigned)(el * tp + 9 * tri_index(n, std::min(a, b), std::max(a, b)));
+					cb[pos[strip_rank[(size_t)k * n + a]]++] = a > b ? (blk | TRI_TRANSPOSED) : blk;
+				}
+			}
 		}
 	});
 
 	PFG_CUDA(c, cudaMalloc(&c->d_outer, sizeof(int) * (ndof + 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_inner, sizeof(int) * std::max<long long>(nnz, 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_values, sizeof(double) * std::max<long long>(nnz, 1)));
-	PFG_CUDA(c, cudaMalloc(&c->d_contrib, sizeof(unsigned short) * std::max<size_t>(contrib.size(), 1)));
+	PFG_CUDA(c, cudaMalloc(&c->d_contrib, sizeof(unsigned int) * std::max<size_t>(contrib.size(), 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_blk_rel, sizeof(unsigned short) * std::max<size_t>(blk_rel.size(), 1)));
 	PFG_CUDA(c, cudaMemcpy(c->d_outer, outer.data(), sizeof(int) * (ndof + 1), cudaMemcpyHostToDevice));
 	if (nnz) PFG_CUDA(c, cudaMemcpy(c->d_inner, inner.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice));
 	if (!contrib.empty())
-		PFG_CUDA(c, cudaMemcpy(c->d_contrib, contrib.data(), sizeof(unsigned short) * contrib.size(),
+		PFG_CUDA(c, cudaMemcpy(c->d_contrib, contrib.data(), sizeof(unsigned int) * contrib.size(),
 							   cudaMemcpyHostToDevice));
 	if (!blk_rel.empty())
 		PFG_CUDA(c, cudaMemcpy(c->d_blk_rel, blk_rel.data(), sizeof(unsigned short) * blk_rel.size(),

@@ -33,14 +33,25 @@ struct DevMesh
 	const int *g_eb_inc = nullptr; // [E*n_g] inverse of ginc_eb (aliases eb_inc when isoparametric)
 };
 
+// Element Hessian staging: element e's symmetric node blocks (a, b), a <= b, as one
+// packed upper triangle of n(n+1)/2 blocks at stage[e * tri_pad(n)], block (a, b)
+// at 9 * tri_index(n, a, b) holding H_e(3a+r, 3b+c) at [c][r]; tri_pad rounds the
+// 9 n(n+1)/2 values up to a multiple of 8 so that a triangle is whole 32-byte
+// sectors in FP32 and FP64 alike.
+__host__ __device__ constexpr int tri_index(int n, int a, int b) { return a * n - a * (a - 1) / 2 + (b - a); }
+__host__ __device__ constexpr int tri_pad(int n) { return ((9 * (n * (n + 1) / 2) + 7) / 8) * 8; }
+constexpr unsigned TRI_TRANSPOSED = 0x80000000u;
+
 // Device-resident Hessian pattern (Eigen ColMajor CSC, int32 indices) and its
 // reduction plan.  Node B's column block has deg(B) row nodes (rank 0..deg-1 in
 // ascending node order); entry (3A+r, 3B+c) lives at
 //   outer[3B] + c*3*deg(B) + 3*rank_B(A) + r,
 // and B's node blocks are numbered from outer[3B] / 9.  For node B with
-// incidences s0..s1-1 (inc_off):
-//   contrib[s0*n + k], k < (s1-s0)*n : record block (s - s0)*n + a, grouped by the
-//       rank of local node a, incidences ascending inside a group;
+// incidences s0..s1-1 (inc_off), element e holding B at local b:
+//   contrib[s0*n + k], k < (s1-s0)*n : the staged block that gives column node B
+//       its rows of local row node a, grouped by the rank of a, incidences
+//       ascending inside a group: e * tri_pad(n) + 9 * tri_index(n, min(a,b), max(a,b)),
+//       with TRI_TRANSPOSED set when a > b (the block is (b, a), read transposed);
 //   blk_rel[outer[3B]/9 + rank]     : start of the rank's group, relative to s0*n.
 struct DevPattern
 {
@@ -49,7 +60,7 @@ struct DevPattern
 
 	const int *outer = nullptr;
 	const int *inner = nullptr;
-	const unsigned short *contrib = nullptr;
+	const unsigned int *contrib = nullptr;
 	const unsigned short *blk_rel = nullptr;
 	double *values = nullptr;
 	// Dirichlet-reduced output (BCLagrangianForm::project_hessian): when red_col_start
@@ -67,7 +78,7 @@ struct Scratch
 	unsigned long long *inverted = nullptr;
 	int max_blocks = 0;
 	double *vec_stage = nullptr;      // one 32-byte slot per incidence, in incidence (node) order: element gradient / shape contributions
-	void *hess_stage = nullptr;       // one padded record of 9n block values per incidence (FP64 or FP32)
+	void *hess_stage = nullptr;       // one packed block triangle per element (tri_pad values, FP64 or FP32)
 };
 
 constexpr int PREC_FP64 = 0;

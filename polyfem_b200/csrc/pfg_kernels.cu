@@ -428,14 +428,16 @@ __global__ void __launch_bounds__(NT) k_vec_gather(int n_nodes, const int *__res
 //
 // Assembly in two passes, both without atomics:
 //  1. k_hessian_blocks: a tile of elements per CTA computes the symmetric node
-//     blocks once; for every incidence (e, b) the record of all blocks of column
-//     node b, [a][c][r] = H_e(3a+r, 3b+c), is written to the staging buffer at
-//     the incidence's position in node order (records padded to whole sectors).
-//  2. k_hessian_reduce: one warp per column node B reads B's records -- one
-//     contiguous run -- through the reduction plan built with the pattern (for
-//     each row rank, the record blocks that land on it), sums every CSC entry in
-//     registers in incidence order and writes B's three columns once.  Each CSC
-//     entry is summed in a fixed order: the result is deterministic.
+//     blocks (a, b), a <= b, once each and writes every element's blocks as one
+//     packed upper triangle (tri_index order, [c][r] = H_e(3a+r, 3b+c)), a
+//     contiguous run of whole sectors per element.
+//  2. k_hessian_reduce: one warp per column node B reads, through the reduction
+//     plan built with the pattern (for each row rank, the staged blocks that land
+//     on it; block (b, a) read transposed for a > b), the blocks of B's
+//     incidences, sums every CSC entry in registers in incidence order and writes
+//     B's three columns once.  Each CSC entry is summed in a fixed order: the
+//     result is deterministic.  An off-diagonal block is read by the warps of both
+//     its nodes, the second time mostly from L2.
 // ---------------------------------------------------------------------------
 // Per (element, point) kinematics in the contraction type T, in 16-byte groups:
 // [mu da, lambda da, (mu - lambda lnJ) da, -], then for every local node a at
@@ -497,13 +499,6 @@ __device__ __forceinline__ void st_gd(double *p, const double g[3], const double
 	*reinterpret_cast<double2 *>(p + 4) = make_double2(d[1], d[2]);
 }
 
-// Record of one incidence (e, b): the 9n values H_e(3a+r, 3b+c), [a][c][r], padded to
-// whole 32-byte sectors so that records written at scattered positions stay full-sector.
-template <class EL, class T>
-__host__ __device__ constexpr int rec_pad()
-{
-	return (((9 * EL::N * (int)sizeof(T)) + 31) / 32) * 32 / (int)sizeof(T);
-}
 
 // elements per tile of k_hessian_blocks (four warps, each takes a quarter)
 #ifndef PFG_TE_P1
@@ -622,11 +617,12 @@ template <class EL, class K, class T>
 struct EcSmem
 {
 	using TL = EcTile<EL, T>;
-	// one element's records per warp, record b at b * RS (rec_pad values + 16 bytes, so
-	// that blocks of one row node in different records fall in different banks),
-	// then copied out in 16-byte vectors
-	static constexpr int RS = rec_pad<EL, T>() + 16 / (int)sizeof(T);
-	__align__(16) T rec[TL::NT / 32][TL::N * RS];
+	// one element's block triangle per warp (tri_pad values, copied out in 16-byte
+	// vectors); before the blocks it holds the warp's J^-T and F^-T in K
+	static constexpr int TP = tri_pad(TL::N), VW = 16 / (int)sizeof(T);
+	static constexpr int JF_T = (int)(((TL::TE / (TL::NT / 32)) * TL::NQ * 18 * sizeof(K) + sizeof(T) - 1) / sizeof(T));
+	static constexpr int TB = ((TP > JF_T ? TP : JF_T) + VW - 1) / VW * VW;
+	__align__(16) T rec[TL::NT / 32][TB];
 	__align__(16) T kin[TL::TE][TL::NQ][TL::PQ];
 	K U[TL::TE][TL::N][3];
 	K X[TL::TE][TL::NG][3];
@@ -636,7 +632,6 @@ struct EcSmem
 	K ggtab[EL::AFFINE ? 1 : TL::NQ][TL::NG][3];
 	double wq[TL::NQ];
 	int nodes[TL::TE][TL::N + TL::NG];
-	int sidx[TL::NT / 32][TL::N];   // incidence index of (e, b) for the warp's element
 	unsigned char pair_a[TL::NP], pair_b[TL::NP];
 };
 
@@ -732,8 +727,7 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 	// stored rounded to T.  When J^-T and F^-T of the warp's points fit in its
 	// (still unused) record buffer, the per-node vectors are a second step over
 	// (element, point, node) so that every lane has work.
-	constexpr bool SPLIT_KIN =
-		(size_t)WE * NQ * 18 * sizeof(K) <= (size_t)N * EcSmem<EL, K, T>::RS * sizeof(T);
+	constexpr bool SPLIT_KIN = true; // the warp's buffer is sized for J^-T and F^-T
 	K *JF = reinterpret_cast<K *>(S.rec[warp]); // [WE * NQ][18]: J^-T, then F^-T
 	for (int i = lane; i < wn * NQ; i += 32)
 	{
@@ -849,13 +843,12 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 		__syncwarp();
 	}
 
-	// blocks: the warp takes its elements one at a time: symmetric node pairs into the warp's
-	// record buffer (H_ba = H_ab^T alongside), then the element's n records are
-	// written out, record b = H_e(3a+r, 3b+c) as [a][c][r], to the incidence's
-	// position in node order, in 16-byte vectors (the padding travels along)
-	constexpr int RP = rec_pad<EL, T>();
-	constexpr int VW = 16 / (int)sizeof(T), RV = RP / VW;
-	static_assert(RP % VW == 0, "records must be whole 16-byte vectors");
+	// blocks: the warp takes its elements one at a time: the symmetric node pairs
+	// into the warp's triangle buffer, block (a, b) at 9 * tri_index(a, b) as
+	// [c][r] (lanes write blocks 9 values apart: no bank conflicts), then the
+	// triangle is copied to stage[e * TP] in 16-byte vectors (padding included)
+	constexpr int TP = EcSmem<EL, K, T>::TP, VW = EcSmem<EL, K, T>::VW;
+	static_assert(TP % VW == 0, "triangles must be whole 16-byte vectors");
 	T *R = S.rec[warp];
 	for (int el = w0; el < w0 + wn; ++el)
 	{
@@ -864,41 +857,32 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 			const int a = S.pair_a[p0], b = S.pair_b[p0];
 			T h[3][3];
 			block_pair<EL, T>(S.kin[el], a, b, h);
-			constexpr int RS = EcSmem<EL, K, T>::RS;
-			T *Hab = R + b * RS + a * 9; // block (a, b): record of column node b
-			T *Hba = R + a * RS + b * 9; // block (b, a): record of column node a
+			T *Hab = R + 9 * p0; // pair table order is tri_index order
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
 #pragma unroll
-				for (int c = 0; c < 3; ++c)
-				{
-					Hab[c * 3 + r] = h[r][c];
-					if (a != b) Hba[r * 3 + c] = h[r][c];
-				}
+				for (int c = 0; c < 3; ++c) Hab[c * 3 + r] = h[r][c];
 		}
-		if (lane < N) S.sidx[warp][lane] = __ldg(m.eb_inc + (size_t)(e0 + el) * N + lane);
 		__syncwarp();
-		for (int i = lane; i < N * RV; i += 32)
-		{
-			const int b = i / RV, k = i - b * RV;
-			const uint4 v = reinterpret_cast<const uint4 *>(R + b * EcSmem<EL, K, T>::RS)[k];
-			reinterpret_cast<uint4 *>(stage + (size_t)S.sidx[warp][b] * RP)[k] = v;
-		}
+		uint4 *dst = reinterpret_cast<uint4 *>(stage + (size_t)(e0 + el) * TP);
+		const uint4 *src = reinterpret_cast<const uint4 *>(R);
+		for (int i = lane; i < TP / VW; i += 32) dst[i] = src[i];
 		__syncwarp();
 	}
 }
 
-// One warp per column node B.  Node B's records are one contiguous run of the
-// staging buffer; the warp's 3*deg(B) work items are the (row rank, column c)
-// pairs of B's column block.  Each item sums, in FP64 and in incidence order, the
-// three values (rows 3*rank .. 3*rank+2 of column 3B+c) of every record block
-// that lands on its rank, read through the reduction plan, and writes them once.
-// No shared memory, no atomics: the sum order of every entry is fixed.
+// One warp per column node B; the warp's 3*deg(B) work items are the (row rank,
+// column c) pairs of B's column block.  Each item sums, in FP64 and in incidence
+// order, the three values (rows 3*rank .. 3*rank+2 of column 3B+c) of every
+// staged block that lands on its rank, read through the reduction plan
+// (consecutive values of block (a, b); for a flagged transposed block (b, a), the
+// values c, c+3, c+6), and writes them once.  No shared memory, no atomics: the
+// sum order of every entry is fixed.
 template <class EL, class T, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 8)
 	k_hessian_reduce(DevMesh m, DevPattern pat, const T *__restrict__ stage)
 {
-	constexpr int N = EL::N, RP = rec_pad<EL, T>();
+	constexpr int N = EL::N;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int B = blockIdx.x * WARPS + warp;
 	if (B >= m.N) return;
@@ -907,8 +891,7 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 	const int deg = stride / 3;
 	const int s0 = __ldg(m.inc_off + B), s1 = __ldg(m.inc_off + B + 1);
 	const int tot = (s1 - s0) * N;
-	const T *rec = stage + (size_t)s0 * RP;
-	const unsigned short *cl = pat.contrib + (size_t)s0 * N;
+	const unsigned *cl = pat.contrib + (size_t)s0 * N;
 	const unsigned short *br = pat.blk_rel + o0 / 9;
 	double *dst = pat.values + o0;
 	for (int it = lane; it < stride; it += 32)
@@ -921,24 +904,26 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 		double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 		// two contributions per step, the next step's plan entries loaded ahead;
 		// the sum order stays k ascending
-		int qa = k0 < k1 ? (int)__ldg(cl + k0) : 0;
-		int qb = k0 + 1 < k1 ? (int)__ldg(cl + k0 + 1) : 0;
+		unsigned qa = k0 < k1 ? __ldg(cl + k0) : 0u;
+		unsigned qb = k0 + 1 < k1 ? __ldg(cl + k0 + 1) : 0u;
 		for (int k = k0; k < k1; k += 2)
 		{
-			const int q0 = qa, q1 = qb;
+			const unsigned q0 = qa, q1 = qb;
 			const bool two = k + 1 < k1;
-			qa = k + 2 < k1 ? (int)__ldg(cl + k + 2) : 0;
-			qb = k + 3 < k1 ? (int)__ldg(cl + k + 3) : 0;
-			const int sr0 = q0 / N, sr1 = q1 / N;
-			const T *p0 = rec + sr0 * RP + 9 * (q0 - sr0 * N) + 3 * c;
-			const T *p1 = rec + sr1 * RP + 9 * (q1 - sr1 * N) + 3 * c;
-			const T x0 = __ldg(p0), x1 = __ldg(p0 + 1), x2 = __ldg(p0 + 2);
+			qa = k + 2 < k1 ? __ldg(cl + k + 2) : 0u;
+			qb = k + 3 < k1 ? __ldg(cl + k + 3) : 0u;
+			// (a, b): values 3c, 3c+1, 3c+2 of the block; transposed (b, a): c, c+3, c+6
+			const bool t0 = q0 & TRI_TRANSPOSED, t1 = q1 & TRI_TRANSPOSED;
+			const T *p0 = stage + (q0 & ~TRI_TRANSPOSED) + (t0 ? c : 3 * c);
+			const T *p1 = stage + (q1 & ~TRI_TRANSPOSED) + (t1 ? c : 3 * c);
+			const int s0_ = t0 ? 3 : 1, s1_ = t1 ? 3 : 1;
+			const T x0 = __ldg(p0), x1 = __ldg(p0 + s0_), x2 = __ldg(p0 + 2 * s0_);
 			T y0 = T(0), y1 = T(0), y2 = T(0);
 			if (two)
 			{
 				y0 = __ldg(p1);
-				y1 = __ldg(p1 + 1);
-				y2 = __ldg(p1 + 2);
+				y1 = __ldg(p1 + s1_);
+				y2 = __ldg(p1 + 2 * s1_);
 			}
 			a0 += double(x0);
 			a1 += double(x1);
@@ -980,14 +965,14 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 // Z diag(max(l, 0)) Z^T when its smallest eigenvalue is <= 0.  Equivalently
 // A+ = A + sum_{l_j < 0} |l_j| z_j z_j^T, which needs only the eigenpairs with
 // l_j < 0; this kernel computes those and nothing else.  One warp per element,
-// all in FP64, the element matrix A[3a+r][3b+c] = record_b[9a + 3c + r]:
+// all in FP64, on the element matrix rebuilt from its staged block triangle:
 //   1. Householder reduction to tridiagonal T = Q^T A Q (EISPACK tred2 without
 //      the accumulation of Q), lane j holding row j of A in registers and
 //      applying the symmetric rank-2 update to its own row; the reflectors
 //      u_i (with 1/h_i) stay in shared memory.
 //   2. T is scaled by its Gershgorin bound ||T|| (so |l| <= 1) and the number k
 //      of eigenvalues below -tau is one Sturm count (LDL^T sign count).
-//      k == 0: the matrix counts as PSD and the records stay as they are.
+//      k == 0: the matrix counts as PSD and the staged blocks stay as they are.
 //   3. The k eigenvalues by multisection: 32 / k lanes per eigenvalue each
 //      evaluate a Sturm count at an interior point of the eigenvalue's interval,
 //      a ballot picks the sub-interval, until the width is <= 1e-15 ||T||.
@@ -996,12 +981,12 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 //      +-eps ||T||), PSD_INV_ITERS steps, each followed by modified
 //      Gram-Schmidt across the k lanes (clustered eigenvalues).
 //   5. x_j = Q y_j through the stored reflectors, w_j = sqrt(|l_j|) x_j, and
-//      every record entry becomes A + sum_j w_j w_j^T (rounded to the record
+//      every staged value becomes A + sum_j w_j w_j^T (rounded to the staging
 //      type).
 // Eigenvalues in (-tau ||T||, 0] are left in place where the reference clamps
-// them to zero; tau sits above the rounding noise of the record type: 1e-12 for
-// FP64 records (the rigid-motion null space of an element matrix is computed at
-// +-1e-15 ||A||), 1e-6 for FP32 records (rounding A to FP32 moves those null
+// them to zero; tau sits above the rounding noise of the staging type: 1e-12 for
+// FP64 blocks (the rigid-motion null space of an element matrix is computed at
+// +-1e-15 ||A||), 1e-6 for FP32 blocks (rounding A to FP32 moves those null
 // eigenvalues by up to ~3e-7 ||A||).  The difference is below tau ||A|| per
 // element.
 // A matrix holding NaN, or whose inverse iteration overflows, is left as it is.
@@ -1196,7 +1181,7 @@ template <class EL, class T, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__restrict__ stage)
 {
 	using W = PsdWarp<EL>;
-	constexpr int N = EL::N, M = W::M, RP = rec_pad<EL, T>();
+	constexpr int N = EL::N, M = W::M;
 	constexpr unsigned FULL = 0xffffffffu;
 	static_assert(M <= 32, "one lane per row");
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1204,11 +1189,13 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__r
 	const int lane = threadIdx.x & 31;
 	const int e = blockIdx.x * WARPS + (threadIdx.x >> 5);
 	if (e >= m.E) return;
-	int sidx[N];
-#pragma unroll
-	for (int b = 0; b < N; ++b) sidx[b] = __ldg(m.eb_inc + (size_t)e * N + b);
-	// lane i < M owns row i: A[i][3b+c] = record_b[9 (i/3) + 3c + i%3]
-	const int off = 9 * (lane / 3) + lane % 3;
+	// lane i = 3a + r < M owns row i of the element matrix: A[3a+r][3b+c] is value
+	// 3c + r of staged block (a, b) for a <= b, value 3r + c of block (b, a) for a > b
+	T *tri = stage + (size_t)e * tri_pad(N);
+	const int ra = lane / 3, rr = lane % 3;
+	const auto at = [&](int b, int c) {
+		return ra <= b ? 9 * tri_index(N, ra, b) + 3 * c + rr : 9 * tri_index(N, b, ra) + 3 * rr + c;
+	};
 
 	double a[M];
 #pragma unroll
@@ -1217,7 +1204,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__r
 		for (int c = 0; c < 3; ++c)
 		{
 			a[3 * b + c] = 0.0;
-			if (lane < M) a[3 * b + c] = double(stage[(size_t)sidx[b] * RP + off + 3 * c]);
+			if (lane < M) a[3 * b + c] = double(tri[at(b, c)]);
 		}
 	bool nan_in = false;
 #pragma unroll
@@ -1280,7 +1267,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__r
 		if (it < 0)
 		{
 			k = c;
-			if (k == 0) return; // PSD: the records stay as they are
+			if (k == 0) return; // PSD: the staged blocks stay as they are
 			G = 32 / k;
 			jg = lane / G;
 			act = jg < k;
@@ -1412,14 +1399,14 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__r
 	}
 	__syncwarp();
 
-	// --- 6. row i of A + sum_j w_j w_j^T back into the records -------------------
+	// --- 6. row i of A + sum_j w_j w_j^T, blocks (a, b >= a), back into the triangle
 	if (lane < M)
 	{
 		double r[M];
 #pragma unroll
 		for (int b = 0; b < N; ++b)
 #pragma unroll
-			for (int c = 0; c < 3; ++c) r[3 * b + c] = double(stage[(size_t)sidx[b] * RP + off + 3 * c]);
+			for (int c = 0; c < 3; ++c) r[3 * b + c] = double(tri[at(b, c)]);
 #pragma unroll 1
 		for (int j = 0; j < k; ++j)
 		{
@@ -1436,7 +1423,8 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__r
 #pragma unroll
 		for (int b = 0; b < N; ++b)
 #pragma unroll
-			for (int c = 0; c < 3; ++c) stage[(size_t)sidx[b] * RP + off + 3 * c] = T(r[3 * b + c]);
+			for (int c = 0; c < 3; ++c)
+				if (b >= ra) tri[at(b, c)] = T(r[3 * b + c]); // each stored value once
 	}
 }
 
