@@ -637,13 +637,16 @@ struct EcSmem
 
 // CTAs per SM the shared-memory footprint allows; the register budget follows it
 #ifndef PFG_BLOCKS_CTAS_F32
-#define PFG_BLOCKS_CTAS_F32 5
+#define PFG_BLOCKS_CTAS_F32 6
+#endif
+#ifndef PFG_BLOCKS_CTAS_F64
+#define PFG_BLOCKS_CTAS_F64 5
 #endif
 template <class EL, class K, class T>
 constexpr int blocks_min_ctas()
 {
 	constexpr int by_smem = (int)((227 * 1024) / (sizeof(EcSmem<EL, K, T>) + 1024));
-	constexpr int cap = sizeof(T) == 8 ? 4 : PFG_BLOCKS_CTAS_F32;
+	constexpr int cap = sizeof(T) == 8 ? PFG_BLOCKS_CTAS_F64 : PFG_BLOCKS_CTAS_F32;
 	return by_smem < 1 ? 1 : (by_smem < cap ? by_smem : cap);
 }
 
