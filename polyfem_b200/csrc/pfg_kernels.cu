@@ -517,6 +517,11 @@ struct EcTile
 	static constexpr int NT = 128;
 	static constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ;
 	static constexpr int NP = N * (N + 1) / 2, NB = N * N, PQ = BlockKin<EL, T>::PER_Q, NS = BlockKin<EL, T>::NS;
+	// A lane computes a group of NPB pairs (a, b), (a, b + 1), .. of one row node a:
+	// two for Q1 (its 36 pairs in one round of 20 lanes, the row node's vectors loaded
+	// once for both), one for P1 and P2 (measured: no gain for P2, a loss for P1).
+	static constexpr int NPB = EL::ET == 3 ? 2 : 1;
+	static constexpr int NPG = []() { int s = 0; for (int a = 0; a < N; ++a) s += (N - a + NPB - 1) / NPB; return s; }();
 };
 
 // g_a = grad(phi_a) J^-T and d_a = F^-T g_a in K, stored rounded to T at dst
@@ -541,72 +546,99 @@ __device__ __forceinline__ void node_kin(const K gr[3], const K Jit[3][3], const
 // In FP32 the row pairs (0,1) of every column and the column pair (0,1) of row
 // 2's partner are updated with packed FP32x2 FMAs; each entry sees the same
 // operations in the same order as the scalar form.
-template <class EL, class T>
-__device__ __forceinline__ void block_pair(const T (*kin)[BlockKin<EL, T>::PER_Q], int a, int b, T h[3][3])
+// The blocks (a, b[j]), j < NPB, of one row node a: the weights, g_a, d_a and the
+// products lambda da d_a, (mu - lambda lnJ) da d_a are loaded or formed once per
+// point for all NPB partners.
+template <class EL, class T, int NPB>
+__device__ __forceinline__ void block_pairs(const T (*kin)[BlockKin<EL, T>::PER_Q], int a, const int (&b)[NPB],
+											T (&h)[NPB][3][3])
 {
 	constexpr int NS = BlockKin<EL, T>::NS;
-#pragma unroll
-	for (int r = 0; r < 3; ++r) h[r][0] = h[r][1] = h[r][2] = T(0);
 	if constexpr (sizeof(T) == 4)
 	{
-		float2 h0 = make_float2(0.f, 0.f), h1 = h0, hc = h0; // (h00,h01) (h10,h11) (h02,h12)
-		float h20 = 0.f, h21 = 0.f, h22 = 0.f;
+		float2 h0[NPB], h1[NPB], hc[NPB]; // (h00,h01) (h10,h11) (h02,h12)
+		float h20[NPB], h21[NPB], h22[NPB];
+#pragma unroll
+		for (int j = 0; j < NPB; ++j)
+		{
+			h0[j] = h1[j] = hc[j] = make_float2(0.f, 0.f);
+			h20[j] = h21[j] = h22[j] = 0.f;
+		}
 #pragma unroll
 		for (int q = 0; q < EL::NQ; ++q)
 		{
 			const T *Kq = kin[q];
-			T w[3], ga[3], gb[3], da[3], db[3];
+			T w[3], ga[3], da[3];
 			ld_w(Kq, w);
 			ld_gd(Kq + 4 + NS * a, ga, da);
-			ld_gd(Kq + 4 + NS * b, gb, db);
-			const float md = w[0] * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
 			const float la0 = w[1] * da[0], la1 = w[1] * da[1], la2 = w[1] * da[2];
 			const float gm0 = w[2] * da[0], gm1 = w[2] * da[1], gm2 = w[2] * da[2];
-			const float2 db01 = make_float2(db[0], db[1]), gm01 = make_float2(gm0, gm1);
-			// rows 0 and 1, columns 0 and 1
-			h0 = __ffma2_rn(make_float2(db[0], db[0]), gm01, __ffma2_rn(make_float2(la0, la0), db01, h0));
-			h1 = __ffma2_rn(make_float2(db[1], db[1]), gm01, __ffma2_rn(make_float2(la1, la1), db01, h1));
-			// column 2 of rows 0 and 1
-			hc = __ffma2_rn(make_float2(db[0], db[1]), make_float2(gm2, gm2),
-							__ffma2_rn(make_float2(la0, la1), make_float2(db[2], db[2]), hc));
-			// row 2
-			h20 = fmaf(db[2], gm0, fmaf(la2, db[0], h20));
-			h21 = fmaf(db[2], gm1, fmaf(la2, db[1], h21));
-			h22 = fmaf(db[2], gm2, fmaf(la2, db[2], h22));
-			h0.x += md;
-			h1.y += md;
-			h22 += md;
+			const float2 gm01 = make_float2(gm0, gm1);
+#pragma unroll
+			for (int j = 0; j < NPB; ++j)
+			{
+				T gb[3], db[3];
+				ld_gd(Kq + 4 + NS * b[j], gb, db);
+				const float md = w[0] * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+				const float2 db01 = make_float2(db[0], db[1]);
+				// rows 0 and 1, columns 0 and 1
+				h0[j] = __ffma2_rn(make_float2(db[0], db[0]), gm01, __ffma2_rn(make_float2(la0, la0), db01, h0[j]));
+				h1[j] = __ffma2_rn(make_float2(db[1], db[1]), gm01, __ffma2_rn(make_float2(la1, la1), db01, h1[j]));
+				// column 2 of rows 0 and 1
+				hc[j] = __ffma2_rn(make_float2(db[0], db[1]), make_float2(gm2, gm2),
+								   __ffma2_rn(make_float2(la0, la1), make_float2(db[2], db[2]), hc[j]));
+				// row 2
+				h20[j] = fmaf(db[2], gm0, fmaf(la2, db[0], h20[j]));
+				h21[j] = fmaf(db[2], gm1, fmaf(la2, db[1], h21[j]));
+				h22[j] = fmaf(db[2], gm2, fmaf(la2, db[2], h22[j]));
+				h0[j].x += md;
+				h1[j].y += md;
+				h22[j] += md;
+			}
 		}
-		h[0][0] = h0.x;
-		h[0][1] = h0.y;
-		h[1][0] = h1.x;
-		h[1][1] = h1.y;
-		h[0][2] = hc.x;
-		h[1][2] = hc.y;
-		h[2][0] = h20;
-		h[2][1] = h21;
-		h[2][2] = h22;
+#pragma unroll
+		for (int j = 0; j < NPB; ++j)
+		{
+			h[j][0][0] = h0[j].x;
+			h[j][0][1] = h0[j].y;
+			h[j][1][0] = h1[j].x;
+			h[j][1][1] = h1[j].y;
+			h[j][0][2] = hc[j].x;
+			h[j][1][2] = hc[j].y;
+			h[j][2][0] = h20[j];
+			h[j][2][1] = h21[j];
+			h[j][2][2] = h22[j];
+		}
 	}
 	else
 	{
 #pragma unroll
+		for (int j = 0; j < NPB; ++j)
+#pragma unroll
+			for (int r = 0; r < 3; ++r) h[j][r][0] = h[j][r][1] = h[j][r][2] = T(0);
+#pragma unroll
 		for (int q = 0; q < EL::NQ; ++q)
 		{
 			const T *Kq = kin[q];
-			T w[3], ga[3], gb[3], da[3], db[3];
+			T w[3], ga[3], da[3];
 			ld_w(Kq, w);
 			ld_gd(Kq + 4 + NS * a, ga, da);
-			ld_gd(Kq + 4 + NS * b, gb, db);
-			const T md = w[0] * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
 			const T la[3] = {w[1] * da[0], w[1] * da[1], w[1] * da[2]};
 			const T gma[3] = {w[2] * da[0], w[2] * da[1], w[2] * da[2]};
 #pragma unroll
-			for (int r = 0; r < 3; ++r)
+			for (int j = 0; j < NPB; ++j)
+			{
+				T gb[3], db[3];
+				ld_gd(Kq + 4 + NS * b[j], gb, db);
+				const T md = w[0] * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
 #pragma unroll
-				for (int c = 0; c < 3; ++c) h[r][c] = fma(db[r], gma[c], fma(la[r], db[c], h[r][c]));
-			h[0][0] += md;
-			h[1][1] += md;
-			h[2][2] += md;
+				for (int r = 0; r < 3; ++r)
+#pragma unroll
+					for (int c = 0; c < 3; ++c) h[j][r][c] = fma(db[r], gma[c], fma(la[r], db[c], h[j][r][c]));
+				h[j][0][0] += md;
+				h[j][1][1] += md;
+				h[j][2][2] += md;
+			}
 		}
 	}
 }
@@ -632,7 +664,7 @@ struct EcSmem
 	K ggtab[EL::AFFINE ? 1 : TL::NQ][TL::NG][3];
 	double wq[TL::NQ];
 	int nodes[TL::TE][TL::N + TL::NG];
-	unsigned char pair_a[TL::NP], pair_b[TL::NP];
+	unsigned char grp_a[TL::NPG], grp_b[TL::NPG]; // pair group: row node, first column node
 };
 
 // CTAs per SM the shared-memory footprint allows; the register budget follows it
@@ -684,16 +716,16 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 			S.wq[qq] = qweight<EL>(qq);
 		}
 	}
-	for (int p = tid; p < NP; p += NT)
+	for (int g = tid; g < TL::NPG; g += NT)
 	{
-		int a = 0, r = p;
-		while (r >= N - a)
+		int a = 0, r = g;
+		while (r >= (N - a + TL::NPB - 1) / TL::NPB)
 		{
-			r -= N - a;
+			r -= (N - a + TL::NPB - 1) / TL::NPB;
 			++a;
 		}
-		S.pair_a[p] = (unsigned char)a;
-		S.pair_b[p] = (unsigned char)(a + r);
+		S.grp_a[g] = (unsigned char)a;
+		S.grp_b[g] = (unsigned char)(a + TL::NPB * r);
 	}
 	__syncthreads();
 
@@ -846,25 +878,33 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 		__syncwarp();
 	}
 
-	// blocks: the warp takes its elements one at a time: the symmetric node pairs
-	// into the warp's triangle buffer, block (a, b) at 9 * tri_index(a, b) as
-	// [c][r] (lanes write blocks 9 values apart: no bank conflicts), then the
-	// triangle is copied to stage[e * TP] in 16-byte vectors (padding included)
-	constexpr int TP = EcSmem<EL, K, T>::TP, VW = EcSmem<EL, K, T>::VW;
+	// blocks: the warp takes its elements one at a time; every lane computes the
+	// blocks of its pair group and writes them to the warp's triangle buffer, block
+	// (a, b) at 9 * tri_index(a, b) as [c][r]; the triangle then goes to
+	// stage[e * TP] in 16-byte vectors (padding included)
+	constexpr int TP = EcSmem<EL, K, T>::TP, VW = EcSmem<EL, K, T>::VW, NPB = TL::NPB, NPG = TL::NPG;
 	static_assert(TP % VW == 0, "triangles must be whole 16-byte vectors");
 	T *R = S.rec[warp];
 	for (int el = w0; el < w0 + wn; ++el)
 	{
-		for (int p0 = lane; p0 < NP; p0 += 32)
+		for (int g = lane; g < NPG; g += 32)
 		{
-			const int a = S.pair_a[p0], b = S.pair_b[p0];
-			T h[3][3];
-			block_pair<EL, T>(S.kin[el], a, b, h);
-			T *Hab = R + 9 * p0; // pair table order is tri_index order
+			const int a = S.grp_a[g], b0 = S.grp_b[g];
+			int bb[NPB];
 #pragma unroll
-			for (int r = 0; r < 3; ++r)
+			for (int j = 0; j < NPB; ++j) bb[j] = b0 + j < N ? b0 + j : b0; // past a row's end: recomputed, not stored
+			T h[NPB][3][3];
+			block_pairs<EL, T, NPB>(S.kin[el], a, bb, h);
+			T *Hab = R + 9 * tri_index(N, a, b0); // the group's blocks are tri_index neighbours
 #pragma unroll
-				for (int c = 0; c < 3; ++c) Hab[c * 3 + r] = h[r][c];
+			for (int j = 0; j < NPB; ++j)
+				if (b0 + j < N)
+				{
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+#pragma unroll
+						for (int c = 0; c < 3; ++c) Hab[9 * j + c * 3 + r] = h[j][r][c];
+				}
 		}
 		__syncwarp();
 		uint4 *dst = reinterpret_cast<uint4 *>(stage + (size_t)(e0 + el) * TP);
