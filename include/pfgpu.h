@@ -40,7 +40,7 @@ enum pfg_status
 	PFG_ERR_INVALID = 1,     /* bad argument (null pointer, index out of range, bad enum) */
 	PFG_ERR_CUDA = 2,        /* a CUDA runtime call failed; see pfg_last_error */
 	PFG_ERR_OOM = 3,         /* device or host allocation failed */
-	PFG_ERR_UNSUPPORTED = 4, /* combination not implemented (e.g. project_to_psd) */
+	PFG_ERR_UNSUPPORTED = 4, /* beyond an implementation limit (e.g. the 32-bit reduction plan) */
 	PFG_ERR_STATE = 5        /* call made in the wrong state (e.g. pattern not built) */
 };
 
@@ -57,7 +57,7 @@ enum pfg_precision
 	PFG_FP32 = 1,    /* FP32 arithmetic; det(F)/log J and reductions in FP64 */
 	PFG_SPLIT32 = 2  /* Hessian: kinematics (J^-T, F, det/log J, F^-T, basis
 	                    gradients) in FP64, the per-block contraction and the
-	                    element records in FP32, every CSC entry summed in FP64.
+	                    staged element blocks in FP32, every CSC entry summed in FP64.
 	                    Relative Frobenius error vs PFG_FP64 <= 1e-6.
 	                    Energy/gradient/shape VJP treat it as PFG_FP32. */
 };
@@ -196,6 +196,36 @@ int pfg_gradient_reduced(pfg_context *ctx, const double *u, int mem, int prec, d
 
 /* x (3N) from y (n_free) and x_bc (3N, read at the constrained dofs; NULL = 0). */
 int pfg_reduced_to_full(pfg_context *ctx, const double *y, const double *x_bc, int mem, double *x);
+
+/* ---------------------------------------------------------------------------
+ * Linear solve on the device.  After every assembly NewtonMethod hands the
+ * Hessian to its linear solver through polysolve's linear::Solver
+ * (analyze_pattern, factorize, solve; called from solver/NLProblem.cpp:261-262,
+ * 419-420).  pfg_cg_solve is that hand-off without a host round trip: the
+ * conjugate gradient of Eigen's ConjugateGradient<..., Lower|Upper,
+ * DiagonalPreconditioner>, the "Eigen::ConjugateGradient" choice of polysolve,
+ * run on the context's assembled Hessian:
+ *   system = PFG_SYS_FULL   : the 3N x 3N Hessian of the last pfg_hessian call
+ *                             that wrote into the context (values == NULL there);
+ *   system = PFG_SYS_REDUCED: the n_free x n_free Hessian of the last
+ *                             pfg_hessian_reduced call into the context.
+ * `values` (device memory, nnz doubles of that pattern) replaces the context's
+ * values when not NULL.  b and x have the system's size; x is the starting guess
+ * when `guess` is non-zero, else the iteration starts at x = 0.  The iteration
+ * stops when |b - H x| < tol |b| or after max_iter iterations; *iters and
+ * *rel_res (host pointers, NULL allowed) receive the iteration count and
+ * |b - H x| / |b| as Eigen's iterations() and error() report them.  Reaching
+ * max_iter is not an error (Eigen reports it through info()): check *rel_res.
+ * H must be symmetric positive definite for the iteration to converge (the
+ * Dirichlet-reduced Hessian with project_psd, for instance).  The result is
+ * bitwise deterministic. */
+enum pfg_system
+{
+	PFG_SYS_FULL = 0,
+	PFG_SYS_REDUCED = 1
+};
+int pfg_cg_solve(pfg_context *ctx, int system, const double *values, const double *b, int mem, double tol,
+                 int max_iter, int guess, double *x, int *iters, double *rel_res);
 
 /* ---------------------------------------------------------------------------
  * Allocation-free energy.  No counterpart in the reference: PolyFEM always

@@ -246,3 +246,50 @@ def reduced_to_full(y, x_bc, constrained):
     free, _ = free_dofs(len(x), constrained)
     x[free] = y
     return x
+
+
+def conjugate_gradient(outer, inner, values, b, tol, max_iter, x0=None):
+    """Eigen 3.4's ConjugateGradient<SparseMatrix, Lower|Upper, DiagonalPreconditioner>
+    (the "Eigen::ConjugateGradient" choice of polysolve's linear::Solver, which
+    NewtonMethod calls after every assembly, solver/NLProblem.cpp:261-262,419-420),
+    restated on a ColMajor CSC matrix.  Eigen is a dependency absent from the
+    reference tree (cmake/recipes/eigen.cmake pins 3.4.0); its published iteration:
+    r = b - A x, stop when |r|^2 < max(tol^2 |b|^2, smallest normal double),
+    p = D^-1 r, then per iteration q = A p, alpha = r.z / p.q, x += alpha p,
+    r -= alpha q, check, z = D^-1 r, beta = r.z' / r.z, p = z + beta p.
+    D^-1 = 1 / diag(A) where the diagonal entry is non-zero, else 1.
+    Returns (x, iterations, relative residual) as Eigen's solve / iterations() /
+    error() report them."""
+    import scipy.sparse as sp
+
+    n = len(outer) - 1
+    A = sp.csc_matrix((np.asarray(values, dtype=np.float64), inner, outer), shape=(n, n))
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+    d = A.diagonal()
+    invd = np.where(d != 0.0, 1.0 / np.where(d != 0.0, d, 1.0), 1.0)
+    rhs2 = float(b @ b)
+    if rhs2 == 0.0:
+        return np.zeros(n), 0, 0.0
+    r = b - A @ x
+    thr = max(tol * tol * rhs2, np.finfo(np.float64).tiny)
+    rr = float(r @ r)
+    if rr < thr:
+        return x, 0, float(np.sqrt(rr / rhs2))
+    p = invd * r
+    rz = float(r @ p)
+    i = 0
+    while i < max_iter:
+        q = A @ p
+        alpha = rz / float(p @ q)
+        x += alpha * p
+        r -= alpha * q
+        rr = float(r @ r)
+        if rr < thr:
+            break
+        z = invd * r
+        rz_new = float(r @ z)
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+        i += 1
+    return x, i, float(np.sqrt(rr / rhs2))

@@ -11,6 +11,8 @@
 #include "pfg_internal.h"
 
 #include <algorithm>
+#include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -59,6 +61,11 @@ struct pfg_context
 	double *d_result = nullptr;
 	double *d_u = nullptr, *d_p = nullptr, *d_out = nullptr;
 	size_t out_cap = 0;
+	// conjugate gradient (pfg_cg_solve): r, z, p, q, invd, b, x (cg_n doubles each),
+	// the per-block partials and the scalars; a pinned host copy of the scalars
+	double *d_cg = nullptr;
+	size_t cg_n = 0;
+	double *h_cg_sc = nullptr;
 	std::string err;
 };
 
@@ -464,6 +471,8 @@ void free_all(pfg_context *c)
 					 c->d_red_values, c->d_full_tmp};
 	for (void *p : rptrs)
 		if (p) cudaFree(p);
+	if (c->d_cg) cudaFree(c->d_cg);
+	if (c->h_cg_sc) cudaFreeHost(c->h_cg_sc);
 }
 } // namespace
 
@@ -907,6 +916,101 @@ int pfg_gradient_reduced(pfg_context *c, const double *u, int mem, int prec, dou
 	double *dst = mem == PFG_MEM_DEVICE ? g_out : c->d_out;
 	PFG_CUDA(c, launch_gather_free(c->d_full_tmp, c->d_free, c->n_free, dst, c->stream));
 	if (mem == PFG_MEM_HOST) return finish_host(c, g_out, c->d_out, c->n_free);
+	return PFG_OK;
+}
+
+int pfg_cg_solve(pfg_context *c, int system, const double *values, const double *b, int mem, double tol, int max_iter,
+				 int guess, double *x, int *iters, double *rel_res)
+{
+	if (!c || !check_mem(mem) || (system != PFG_SYS_FULL && system != PFG_SYS_REDUCED) || !(tol >= 0.0) || max_iter < 0)
+		return fail(c, PFG_ERR_INVALID, "bad arguments");
+	const int *outer, *inner;
+	const double *vals;
+	int n;
+	if (system == PFG_SYS_FULL)
+	{
+		if (!c->has_pattern) return fail(c, PFG_ERR_STATE, "no Hessian assembled (pfg_hessian)");
+		outer = c->d_outer;
+		inner = c->d_inner;
+		vals = values ? values : c->d_values;
+		n = 3 * c->m.N;
+	}
+	else
+	{
+		if (!c->has_dirichlet) return fail(c, PFG_ERR_STATE, "no Dirichlet set (pfg_set_dirichlet)");
+		outer = c->d_red_outer;
+		inner = c->d_red_inner;
+		vals = values ? values : c->d_red_values;
+		n = c->n_free;
+	}
+	if (n > 0 && (!b || !x)) return fail(c, PFG_ERR_INVALID, "b or x NULL");
+	DeviceGuard g(c->device);
+	const size_t nn = std::max<size_t>(n, 1);
+	if (c->cg_n < nn)
+	{
+		if (c->d_cg) cudaFree(c->d_cg);
+		c->d_cg = nullptr;
+		c->cg_n = 0;
+		PFG_CUDA(c, cudaMalloc(&c->d_cg, sizeof(double) * (7 * nn + cg_partials_doubles() + CG_NSC)));
+		c->cg_n = nn;
+	}
+	if (!c->h_cg_sc) PFG_CUDA(c, cudaMallocHost(&c->h_cg_sc, sizeof(double) * CG_NSC));
+	CgWork w;
+	const size_t cn = c->cg_n;
+	w.r = c->d_cg;
+	w.z = w.r + cn;
+	w.p = w.z + cn;
+	w.q = w.p + cn;
+	w.invd = w.q + cn;
+	double *db = w.invd + cn, *dx = db + cn;
+	w.part = dx + cn;
+	w.sc = w.part + cg_partials_doubles();
+	if (mem == PFG_MEM_HOST)
+	{
+		if (n) PFG_CUDA(c, cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+		if (n && guess) PFG_CUDA(c, cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+	}
+	else
+	{
+		db = const_cast<double *>(b);
+		dx = x;
+	}
+	int it = 0;
+	double res = 0.0;
+	if (n > 0)
+	{
+		const auto read_scalars = [&]() -> int {
+			PFG_CUDA(c, cudaMemcpyAsync(c->h_cg_sc, w.sc, sizeof(double) * CG_NSC, cudaMemcpyDeviceToHost, c->stream));
+			PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+			return PFG_OK;
+		};
+		int st;
+		PFG_CUDA(c, launch_cg_diag_inv(n, outer, inner, vals, w.invd, c->stream));
+		PFG_CUDA(c, launch_cg_start(n, outer, inner, vals, db, guess != 0, dx, w, c->stream));
+		if ((st = read_scalars())) return st;
+		const double rhs2 = c->h_cg_sc[CG_RHS2];
+		double rr = c->h_cg_sc[CG_RR];
+		if (rhs2 == 0.0)
+			PFG_CUDA(c, cudaMemsetAsync(dx, 0, sizeof(double) * n, c->stream)); // Eigen: x = 0, no iteration
+		else
+		{
+			const double thr = std::max(tol * tol * rhs2, std::numeric_limits<double>::min());
+			if (!(rr < thr))
+				while (it < max_iter)
+				{
+					PFG_CUDA(c, launch_cg_iteration(n, outer, inner, vals, dx, w, c->stream));
+					if ((st = read_scalars())) return st;
+					rr = c->h_cg_sc[CG_RR];
+					if (rr < thr) break;
+					PFG_CUDA(c, launch_cg_direction(n, w, c->stream));
+					++it;
+				}
+			res = std::sqrt(rr / rhs2);
+		}
+	}
+	if (iters) *iters = it;
+	if (rel_res) *rel_res = res;
+	if (mem == PFG_MEM_HOST) return finish_host(c, x, dx, n);
 	return PFG_OK;
 }
 

@@ -108,6 +108,34 @@ cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *ad
 							 const Scratch &sc, cudaStream_t s);
 cudaError_t hessian_kernel_setup(int device);
 
+// Device conjugate gradient (pfg_solve.cu).  Work vectors of n doubles (r, z, p, q,
+// invd), cg_partials_doubles() per-block partial sums and the scalars sc[CG_NSC].
+enum
+{
+	CG_RZ = 0,    // r.z of the current iterate
+	CG_ALPHA = 1, // step length of the last iteration
+	CG_BETA = 2,  // direction update factor of the last iteration
+	CG_RR = 3,    // |r|^2 of the current iterate
+	CG_RHS2 = 4,  // |b|^2
+	CG_NSC = 8
+};
+struct CgWork
+{
+	double *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *invd = nullptr, *part = nullptr, *sc = nullptr;
+};
+size_t cg_partials_doubles();
+// invd[j] = 1 / H(j, j), or 1 where the diagonal is zero or structurally absent
+cudaError_t launch_cg_diag_inv(int n, const int *outer, const int *inner, const double *vals, double *invd,
+							   cudaStream_t s);
+// r = b - H x (x = 0 unless guess), p = D^-1 r; sc: r.z, |r|^2, |b|^2
+cudaError_t launch_cg_start(int n, const int *outer, const int *inner, const double *vals, const double *b,
+							bool guess, double *x, const CgWork &w, cudaStream_t s);
+// q = H p, alpha, x += alpha p, r -= alpha q, z = D^-1 r; sc: |r|^2, beta, r.z
+cudaError_t launch_cg_iteration(int n, const int *outer, const int *inner, const double *vals, double *x,
+								const CgWork &w, cudaStream_t s);
+// p = z + beta p
+cudaError_t launch_cg_direction(int n, const CgWork &w, cudaStream_t s);
+
 // Sets the message pfg_last_error(NULL) returns on this host thread.
 void set_global_error(const std::string &msg);
 

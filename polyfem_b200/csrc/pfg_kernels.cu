@@ -687,7 +687,7 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 	k_hessian_blocks(DevMesh m, const double *__restrict__ u, T *__restrict__ stage, int e_begin, int e_end)
 {
 	using TL = EcTile<EL, T>;
-	constexpr int TE = TL::TE, NT = TL::NT, N = TL::N, NG = TL::NG, NQ = TL::NQ, NP = TL::NP;
+	constexpr int TE = TL::TE, NT = TL::NT, N = TL::N, NG = TL::NG, NQ = TL::NQ;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	EcSmem<EL, K, T> &S = *reinterpret_cast<EcSmem<EL, K, T> *>(smem_raw);
 	const int tid = threadIdx.x;

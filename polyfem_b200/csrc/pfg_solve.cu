@@ -1,0 +1,266 @@
+// Linear solve on the device: conjugate gradient with the diagonal (Jacobi)
+// preconditioner on the context's assembled Hessian (full or Dirichlet-reduced
+// CSC), the hand-off NewtonMethod makes to its linear solver after every
+// assembly (polysolve's linear::Solver: analyze_pattern / factorize / solve, as
+// called from solver/NLProblem.cpp:261-262,419-420).
+//
+// The iteration is Eigen's ConjugateGradient with DiagonalPreconditioner (Eigen
+// 3.4, the version the reference pins in cmake/recipes/eigen.cmake), restated:
+//   r = b - H x, rhs2 = |b|^2;  rhs2 == 0: x = 0, done
+//   threshold = max(tol^2 rhs2, smallest normal double)
+//   |r|^2 < threshold: done after 0 iterations
+//   p = D^-1 r, rz = r.p, i = 0
+//   while i < max_iter:
+//     q = H p;  alpha = rz / p.q;  x += alpha p;  r -= alpha q
+//     |r|^2 < threshold: stop
+//     z = D^-1 r;  rz' = r.z;  beta = rz' / rz;  rz = rz';  p = z + beta p;  i += 1
+//   iterations = i, relative residual = sqrt(|r|^2 / rhs2)
+// with D^-1 = 1 / diag(H) where the diagonal is non-zero, else 1.
+//
+// H is structurally and numerically symmetric (the reduction sums both triangles of
+// every block in the same element order), so column j of the CSC is row j and
+// q = H p is a gather: one warp per column, no atomics.  Every dot product is a
+// fixed-order reduction (warp butterfly, warps in order, blocks in order), so the
+// iterates are bitwise deterministic.
+#include "pfg_internal.h"
+
+#include <algorithm>
+
+namespace pfg
+{
+
+namespace
+{
+
+constexpr int CG_NT = 256;      // threads per block of every kernel here
+constexpr int CG_MAX_GRID = 1184; // 148 SMs x 8: blocks of the grid-stride kernels
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+// sum over the block's threads in a fixed order; the result is valid in thread 0
+__device__ __forceinline__ double block_sum(double v)
+{
+	__shared__ double ws[CG_NT / 32];
+	v = warp_sum(v);
+	if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+	__syncthreads();
+	double s = 0.0;
+	if (threadIdx.x == 0)
+#pragma unroll
+		for (int w = 0; w < CG_NT / 32; ++w) s += ws[w];
+	__syncthreads();
+	return s;
+}
+
+__global__ void __launch_bounds__(CG_NT) k_diag_inv(int n, const int *__restrict__ outer, const int *__restrict__ inner,
+													const double *__restrict__ vals, double *__restrict__ invd)
+{
+	for (int j = blockIdx.x * CG_NT + threadIdx.x; j < n; j += gridDim.x * CG_NT)
+	{
+		// rows of a column are sorted: binary search for the diagonal entry
+		int lo = __ldg(outer + j), hi = __ldg(outer + j + 1);
+		double d = 0.0;
+		while (lo < hi)
+		{
+			const int mid = (lo + hi) >> 1;
+			const int r = __ldg(inner + mid);
+			if (r == j)
+			{
+				d = __ldg(vals + mid);
+				break;
+			}
+			if (r < j)
+				lo = mid + 1;
+			else
+				hi = mid;
+		}
+		invd[j] = d != 0.0 ? 1.0 / d : 1.0;
+	}
+}
+
+// q = H p (column j gathered by one warp); part[block] = sum over the block's
+// columns of p_j q_j when part != nullptr
+__global__ void __launch_bounds__(CG_NT) k_spmv(int n, const int *__restrict__ outer, const int *__restrict__ inner,
+												const double *__restrict__ vals, const double *__restrict__ p,
+												double *__restrict__ q, double *__restrict__ part)
+{
+	const int lane = threadIdx.x & 31;
+	const int wpb = CG_NT / 32;
+	double pq = 0.0;
+	for (int j = blockIdx.x * wpb + (threadIdx.x >> 5); j < n; j += gridDim.x * wpb)
+	{
+		const int k0 = __ldg(outer + j), k1 = __ldg(outer + j + 1);
+		double s = 0.0;
+		for (int k = k0 + lane; k < k1; k += 32) s = fma(__ldg(vals + k), __ldg(p + __ldg(inner + k)), s);
+		s = warp_sum(s);
+		if (lane == 0)
+		{
+			q[j] = s;
+			pq = fma(p[j], s, pq);
+		}
+	}
+	if (part)
+	{
+		const double t = block_sum(pq);
+		if (threadIdx.x == 0) part[blockIdx.x] = t;
+	}
+}
+
+// r = b - q
+__global__ void __launch_bounds__(CG_NT) k_resid(int n, const double *__restrict__ b, const double *__restrict__ q,
+												 double *__restrict__ r)
+{
+	for (int j = blockIdx.x * CG_NT + threadIdx.x; j < n; j += gridDim.x * CG_NT) r[j] = b[j] - q[j];
+}
+
+// z = D^-1 r, p = z; part = (r.z, r.r, b.b) per block
+__global__ void __launch_bounds__(CG_NT) k_cg_start(int n, const double *__restrict__ invd, const double *__restrict__ b,
+													const double *__restrict__ r, double *__restrict__ p,
+													double *__restrict__ part)
+{
+	double rz = 0.0, rr = 0.0, bb = 0.0;
+	for (int j = blockIdx.x * CG_NT + threadIdx.x; j < n; j += gridDim.x * CG_NT)
+	{
+		const double rj = r[j], zj = invd[j] * rj, bj = b[j];
+		p[j] = zj;
+		rz = fma(rj, zj, rz);
+		rr = fma(rj, rj, rr);
+		bb = fma(bj, bj, bb);
+	}
+	const double s0 = block_sum(rz), s1 = block_sum(rr), s2 = block_sum(bb);
+	if (threadIdx.x == 0)
+	{
+		part[blockIdx.x] = s0;
+		part[gridDim.x + blockIdx.x] = s1;
+		part[2 * gridDim.x + blockIdx.x] = s2;
+	}
+}
+
+// x += alpha p, r -= alpha q, z = D^-1 r; part = (r.r, r.z) per block
+__global__ void __launch_bounds__(CG_NT) k_cg_step(int n, const double *__restrict__ sc, const double *__restrict__ p,
+												   const double *__restrict__ q, double *__restrict__ x,
+												   double *__restrict__ r, const double *__restrict__ invd,
+												   double *__restrict__ z, double *__restrict__ part)
+{
+	const double alpha = sc[CG_ALPHA];
+	double rr = 0.0, rz = 0.0;
+	for (int j = blockIdx.x * CG_NT + threadIdx.x; j < n; j += gridDim.x * CG_NT)
+	{
+		x[j] = fma(alpha, p[j], x[j]);
+		const double rj = fma(-alpha, q[j], r[j]);
+		r[j] = rj;
+		const double zj = invd[j] * rj;
+		z[j] = zj;
+		rr = fma(rj, rj, rr);
+		rz = fma(rj, zj, rz);
+	}
+	const double s0 = block_sum(rr), s1 = block_sum(rz);
+	if (threadIdx.x == 0)
+	{
+		part[blockIdx.x] = s0;
+		part[gridDim.x + blockIdx.x] = s1;
+	}
+}
+
+// p = z + beta p
+__global__ void __launch_bounds__(CG_NT) k_cg_dir(int n, const double *__restrict__ sc, const double *__restrict__ z,
+												  double *__restrict__ p)
+{
+	const double beta = sc[CG_BETA];
+	for (int j = blockIdx.x * CG_NT + threadIdx.x; j < n; j += gridDim.x * CG_NT) p[j] = fma(beta, p[j], z[j]);
+}
+
+enum
+{
+	RED_START = 0, // (r.z, r.r, b.b) -> rz, rr, rhs2
+	RED_ALPHA = 1, // p.q -> alpha = rz / p.q
+	RED_BETA = 2   // (r.r, r.z') -> rr, beta = rz' / rz, rz = rz'
+};
+
+// one block: the per-block partials summed in block order, then the scalars
+__global__ void __launch_bounds__(CG_NT) k_cg_reduce(const double *__restrict__ part, int count, int mode,
+													 double *__restrict__ sc)
+{
+	const int ncomp = mode == RED_START ? 3 : (mode == RED_ALPHA ? 1 : 2);
+	double s[3] = {0.0, 0.0, 0.0};
+	for (int c = 0; c < ncomp; ++c)
+	{
+		double v = 0.0;
+		for (int i = threadIdx.x; i < count; i += CG_NT) v += part[c * count + i];
+		s[c] = block_sum(v);
+	}
+	if (threadIdx.x != 0) return;
+	if (mode == RED_START)
+	{
+		sc[CG_RZ] = s[0];
+		sc[CG_RR] = s[1];
+		sc[CG_RHS2] = s[2];
+	}
+	else if (mode == RED_ALPHA)
+		sc[CG_ALPHA] = sc[CG_RZ] / s[0];
+	else
+	{
+		sc[CG_RR] = s[0];
+		sc[CG_BETA] = s[1] / sc[CG_RZ];
+		sc[CG_RZ] = s[1];
+	}
+}
+
+int grid_vec(int n) { return n <= 0 ? 1 : (int)std::min<long long>(CG_MAX_GRID, ((long long)n + CG_NT - 1) / CG_NT); }
+int grid_spmv(int n) { return n <= 0 ? 1 : (int)std::min<long long>(CG_MAX_GRID, ((long long)n + 7) / 8); }
+
+} // namespace
+
+size_t cg_partials_doubles() { return 3 * (size_t)CG_MAX_GRID; }
+
+cudaError_t launch_cg_diag_inv(int n, const int *outer, const int *inner, const double *vals, double *invd,
+							   cudaStream_t s)
+{
+	if (n > 0) k_diag_inv<<<grid_vec(n), CG_NT, 0, s>>>(n, outer, inner, vals, invd);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_cg_start(int n, const int *outer, const int *inner, const double *vals, const double *b,
+							bool guess, double *x, const CgWork &w, cudaStream_t s)
+{
+	const int gv = grid_vec(n);
+	if (guess)
+	{
+		k_spmv<<<grid_spmv(n), CG_NT, 0, s>>>(n, outer, inner, vals, x, w.q, nullptr);
+		k_resid<<<gv, CG_NT, 0, s>>>(n, b, w.q, w.r);
+	}
+	else
+	{
+		cudaError_t e = cudaMemsetAsync(x, 0, sizeof(double) * (size_t)n, s);
+		if (e != cudaSuccess) return e;
+		e = cudaMemcpyAsync(w.r, b, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s);
+		if (e != cudaSuccess) return e;
+	}
+	k_cg_start<<<gv, CG_NT, 0, s>>>(n, w.invd, b, w.r, w.p, w.part);
+	k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gv, RED_START, w.sc);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_cg_iteration(int n, const int *outer, const int *inner, const double *vals, double *x,
+								const CgWork &w, cudaStream_t s)
+{
+	const int gs = grid_spmv(n), gv = grid_vec(n);
+	k_spmv<<<gs, CG_NT, 0, s>>>(n, outer, inner, vals, w.p, w.q, w.part);
+	k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gs, RED_ALPHA, w.sc);
+	k_cg_step<<<gv, CG_NT, 0, s>>>(n, w.sc, w.p, w.q, x, w.r, w.invd, w.z, w.part);
+	k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gv, RED_BETA, w.sc);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_cg_direction(int n, const CgWork &w, cudaStream_t s)
+{
+	k_cg_dir<<<grid_vec(n), CG_NT, 0, s>>>(n, w.sc, w.z, w.p);
+	return cudaGetLastError();
+}
+
+} // namespace pfg
