@@ -439,7 +439,7 @@ def run_suite(args):
 
     from polyfem_b200 import NeoHookeanAssembler
     from polyfem_b200 import mesh as M
-    from polyfem_b200._lib import lib
+    from polyfem_b200._lib import check, lib
 
     L = lib()
     vp = ctypes.c_void_p
@@ -505,6 +505,26 @@ def run_suite(args):
                 r["alg_GBps"] = round(gbs, 1)
                 r["frac_hbm"] = round(gbs / peak, 4)
             res[op] = r
+        # device conjugate gradient on the reduced, PSD-projected FP64 Hessian: 50
+        # iterations (tolerance 0), one |r|^2 read-back per iteration included
+        check(L.pfg_hessian_reduced(h, U, 1, 0, 1, None), h, "pfg_hessian_reduced")
+        nf, rnnz = asm.n_free, asm._red_nnz
+        bd = torch.randn(nf, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(9))
+        xd = torch.empty(nf, dtype=torch.float64, device="cuda")
+        it, rr = ctypes.c_int(), ctypes.c_double()
+        cg = lambda: L.pfg_cg_solve(h, 1, None, vp(bd.data_ptr()), 1, 0.0, 50, 0, vp(xd.data_ptr()),
+                                    ctypes.byref(it), ctypes.byref(rr))
+        cg()
+        ms = _events_ms_flushed(stream, cg, 3, flush)
+        # per iteration: values + rows of the SpMV (12 B per nonzero), its column
+        # offsets, gathered p and q (4 + 8 + 8 B per dof), then x, r, z, p, q, D^-1
+        # read and x, r, z, p written by the update kernels (88 B per dof)
+        it_bytes = 12 * rnnz + 108 * nf
+        per_it = ms / max(it.value, 1)
+        gbs = it_bytes / (per_it * 1e-3) / 1e9
+        res["cg_reduced_psd"] = {"us": round(ms * 1e3, 2), "iterations": it.value,
+                                 "us_per_iteration": round(per_it * 1e3, 2), "alg_GBps": round(gbs, 1),
+                                 "frac_hbm": round(gbs / peak, 4), "n": nf, "nnz": rnnz}
         print(json.dumps({"suite": name, "workload": desc, "E": E, "N": mesh.n_nodes, "nnz": nnz, "ops": res}), flush=True)
         asm.close()
     return 0

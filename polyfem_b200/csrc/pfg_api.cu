@@ -47,6 +47,8 @@ struct pfg_context
 		*d_red_inner = nullptr;
 	unsigned short *d_red_row_off = nullptr;
 	double *d_red_values = nullptr, *d_full_tmp = nullptr;
+	int *d_red_groups = nullptr; // per node with free dofs: first reduced column * 4 + their count
+	int n_red_groups = 0;
 	int *d_eb_inc = nullptr, *d_g_eb_inc = nullptr;
 	// node -> (element, local index) incidences, FE and geometric nodes
 	std::vector<long long> h_inc_off; // [N+1]
@@ -372,12 +374,14 @@ void build_incidence(const int *conn, int E, int n, int N, std::vector<long long
 void free_dirichlet(pfg_context *c)
 {
 	void *rptrs[] = {c->d_old_to_new, c->d_free, c->d_red_col_start, c->d_red_outer, c->d_red_inner, c->d_red_row_off,
-					 c->d_red_values};
+					 c->d_red_values, c->d_red_groups};
 	for (void *p : rptrs)
 		if (p) cudaFree(p);
 	c->d_old_to_new = c->d_free = c->d_red_col_start = c->d_red_outer = c->d_red_inner = nullptr;
 	c->d_red_row_off = nullptr;
 	c->d_red_values = nullptr;
+	c->d_red_groups = nullptr;
+	c->n_red_groups = 0;
 	c->has_dirichlet = false;
 	c->n_free = 0;
 	c->red_nnz = 0;
@@ -439,7 +443,25 @@ int build_dirichlet(pfg_context *c)
 			if (r >= 0) red_inner[(size_t)q++] = r;
 		}
 	}
+	// column groups of the conjugate gradient's SpMV: the free dofs of a node are
+	// consecutive reduced columns with the same rows
+	std::vector<int> groups;
+	for (int B = 0; B < N; ++B)
+	{
+		int m = 0, c0 = -1;
+		for (int d = 0; d < 3; ++d)
+			if (old_to_new[3 * B + d] >= 0)
+			{
+				if (c0 < 0) c0 = old_to_new[3 * B + d];
+				++m;
+			}
+		if (m) groups.push_back(c0 * 4 + m);
+	}
 	free_dirichlet(c);
+	PFG_CUDA(c, cudaMalloc(&c->d_red_groups, sizeof(int) * std::max<size_t>(groups.size(), 1)));
+	if (!groups.empty())
+		PFG_CUDA(c, cudaMemcpy(c->d_red_groups, groups.data(), sizeof(int) * groups.size(), cudaMemcpyHostToDevice));
+	c->n_red_groups = (int)groups.size();
 	PFG_CUDA(c, cudaMalloc(&c->d_old_to_new, sizeof(int) * std::max(ndof, 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_free, sizeof(int) * std::max(n_free, 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_red_col_start, sizeof(int) * std::max(ndof, 1)));
@@ -468,7 +490,7 @@ void free_all(pfg_context *c)
 	for (void *p : ptrs)
 		if (p) cudaFree(p);
 	void *rptrs[] = {c->d_old_to_new, c->d_free, c->d_red_col_start, c->d_red_outer, c->d_red_inner, c->d_red_row_off,
-					 c->d_red_values, c->d_full_tmp};
+					 c->d_red_values, c->d_full_tmp, c->d_red_groups};
 	for (void *p : rptrs)
 		if (p) cudaFree(p);
 	if (c->d_cg) cudaFree(c->d_cg);
@@ -924,9 +946,9 @@ int pfg_cg_solve(pfg_context *c, int system, const double *values, const double 
 {
 	if (!c || !check_mem(mem) || (system != PFG_SYS_FULL && system != PFG_SYS_REDUCED) || !(tol >= 0.0) || max_iter < 0)
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
-	const int *outer, *inner;
+	const int *outer, *inner, *groups;
 	const double *vals;
-	int n;
+	int n, ngroups;
 	if (system == PFG_SYS_FULL)
 	{
 		if (!c->has_pattern) return fail(c, PFG_ERR_STATE, "no Hessian assembled (pfg_hessian)");
@@ -934,6 +956,8 @@ int pfg_cg_solve(pfg_context *c, int system, const double *values, const double 
 		inner = c->d_inner;
 		vals = values ? values : c->d_values;
 		n = 3 * c->m.N;
+		groups = nullptr; // node B: columns 3B .. 3B+2
+		ngroups = c->m.N;
 	}
 	else
 	{
@@ -942,6 +966,8 @@ int pfg_cg_solve(pfg_context *c, int system, const double *values, const double 
 		inner = c->d_red_inner;
 		vals = values ? values : c->d_red_values;
 		n = c->n_free;
+		groups = c->d_red_groups;
+		ngroups = c->n_red_groups;
 	}
 	if (n > 0 && (!b || !x)) return fail(c, PFG_ERR_INVALID, "b or x NULL");
 	DeviceGuard g(c->device);
@@ -986,27 +1012,24 @@ int pfg_cg_solve(pfg_context *c, int system, const double *values, const double 
 		};
 		int st;
 		PFG_CUDA(c, launch_cg_diag_inv(n, outer, inner, vals, w.invd, c->stream));
-		PFG_CUDA(c, launch_cg_start(n, outer, inner, vals, db, guess != 0, dx, w, c->stream));
-		if ((st = read_scalars())) return st;
+		PFG_CUDA(c, launch_cg_start(n, ngroups, groups, outer, inner, vals, db, guess != 0, tol, dx, w, c->stream));
+		// iterations in batches of CG_BATCH; the device stops them at convergence
+		constexpr int CG_BATCH = 8;
+		int queued = 0;
+		for (;;)
+		{
+			if ((st = read_scalars())) return st;
+			if (c->h_cg_sc[CG_DONE] != 0.0 || queued >= max_iter) break;
+			const int k = std::min(CG_BATCH, max_iter - queued);
+			PFG_CUDA(c, launch_cg_iterations(n, k, ngroups, groups, outer, inner, vals, dx, w, c->stream));
+			queued += k;
+		}
 		const double rhs2 = c->h_cg_sc[CG_RHS2];
-		double rr = c->h_cg_sc[CG_RR];
+		it = (int)c->h_cg_sc[CG_ITER];
 		if (rhs2 == 0.0)
 			PFG_CUDA(c, cudaMemsetAsync(dx, 0, sizeof(double) * n, c->stream)); // Eigen: x = 0, no iteration
 		else
-		{
-			const double thr = std::max(tol * tol * rhs2, std::numeric_limits<double>::min());
-			if (!(rr < thr))
-				while (it < max_iter)
-				{
-					PFG_CUDA(c, launch_cg_iteration(n, outer, inner, vals, dx, w, c->stream));
-					if ((st = read_scalars())) return st;
-					rr = c->h_cg_sc[CG_RR];
-					if (rr < thr) break;
-					PFG_CUDA(c, launch_cg_direction(n, w, c->stream));
-					++it;
-				}
-			res = std::sqrt(rr / rhs2);
-		}
+			res = std::sqrt(c->h_cg_sc[CG_RR] / rhs2);
 	}
 	if (iters) *iters = it;
 	if (rel_res) *rel_res = res;

@@ -117,6 +117,9 @@ enum
 	CG_BETA = 2,  // direction update factor of the last iteration
 	CG_RR = 3,    // |r|^2 of the current iterate
 	CG_RHS2 = 4,  // |b|^2
+	CG_THR = 5,   // stopping threshold on |r|^2
+	CG_DONE = 6,  // 1 once |r|^2 < threshold: every later kernel of the iteration returns at once
+	CG_ITER = 7,  // iterations counted as Eigen counts them (not the one that stopped)
 	CG_NSC = 8
 };
 struct CgWork
@@ -127,14 +130,18 @@ size_t cg_partials_doubles();
 // invd[j] = 1 / H(j, j), or 1 where the diagonal is zero or structurally absent
 cudaError_t launch_cg_diag_inv(int n, const int *outer, const int *inner, const double *vals, double *invd,
 							   cudaStream_t s);
-// r = b - H x (x = 0 unless guess), p = D^-1 r; sc: r.z, |r|^2, |b|^2
-cudaError_t launch_cg_start(int n, const int *outer, const int *inner, const double *vals, const double *b,
-							bool guess, double *x, const CgWork &w, cudaStream_t s);
-// q = H p, alpha, x += alpha p, r -= alpha q, z = D^-1 r; sc: |r|^2, beta, r.z
-cudaError_t launch_cg_iteration(int n, const int *outer, const int *inner, const double *vals, double *x,
-								const CgWork &w, cudaStream_t s);
-// p = z + beta p
-cudaError_t launch_cg_direction(int n, const CgWork &w, cudaStream_t s);
+// The SpMV takes the columns in groups of m <= 3 consecutive columns with the same
+// rows (a node's dofs): groups[g] = first column * 4 + m, or, with groups == NULL,
+// group g = columns 3g .. 3g+2.
+// r = b - H x (x = 0 unless guess), p = D^-1 r; sc: r.z, |r|^2, |b|^2, the threshold
+// max(tol^2 |b|^2, smallest normal), done (|b| = 0 or |r|^2 below it), 0 iterations
+cudaError_t launch_cg_start(int n, int ngroups, const int *groups, const int *outer, const int *inner,
+							const double *vals, const double *b, bool guess, double tol, double *x, const CgWork &w,
+							cudaStream_t s);
+// `count` iterations unless done: q = H p, alpha, x += alpha p, r -= alpha q, stop
+// test, z = D^-1 r, beta, p = z + beta p, iteration count + 1
+cudaError_t launch_cg_iterations(int n, int count, int ngroups, const int *groups, const int *outer,
+								 const int *inner, const double *vals, double *x, const CgWork &w, cudaStream_t s);
 
 // Sets the message pfg_last_error(NULL) returns on this host thread.
 void set_global_error(const std::string &msg);

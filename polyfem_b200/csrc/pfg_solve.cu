@@ -16,10 +16,13 @@
 //     z = D^-1 r;  rz' = r.z;  beta = rz' / rz;  rz = rz';  p = z + beta p;  i += 1
 //   iterations = i, relative residual = sqrt(|r|^2 / rhs2)
 // with D^-1 = 1 / diag(H) where the diagonal is non-zero, else 1.
+// The stop test runs on the device: the reduction that forms |r|^2 sets a done flag
+// that makes every later kernel return at once, so the host enqueues iterations in
+// batches and reads the flag and the count once per batch.
 //
 // H is structurally and numerically symmetric (the reduction sums both triangles of
 // every block in the same element order), so column j of the CSC is row j and
-// q = H p is a gather: one warp per column, no atomics.  Every dot product is a
+// q = H p is a gather: one warp per node's columns, no atomics.  Every dot product is a
 // fixed-order reduction (warp butterfly, warps in order, blocks in order), so the
 // iterates are bitwise deterministic.
 #include "pfg_internal.h"
@@ -83,25 +86,55 @@ __global__ void __launch_bounds__(CG_NT) k_diag_inv(int n, const int *__restrict
 	}
 }
 
-// q = H p (column j gathered by one warp); part[block] = sum over the block's
-// columns of p_j q_j when part != nullptr
-__global__ void __launch_bounds__(CG_NT) k_spmv(int n, const int *__restrict__ outer, const int *__restrict__ inner,
+// q = H p, one warp per column group (m <= 3 consecutive columns with the same rows,
+// a node's dofs): each row index is loaded and p gathered once for the m columns.
+// part[block] = sum over the block's columns of p_j q_j when part != nullptr.
+__global__ void __launch_bounds__(CG_NT) k_spmv(int ngroups, const int *__restrict__ groups,
+												const int *__restrict__ outer, const int *__restrict__ inner,
 												const double *__restrict__ vals, const double *__restrict__ p,
-												double *__restrict__ q, double *__restrict__ part)
+												double *__restrict__ q, double *__restrict__ part,
+												const double *__restrict__ sc)
 {
+	if (part && sc[CG_DONE] != 0.0) return; // an iteration after the stopping one
 	const int lane = threadIdx.x & 31;
 	const int wpb = CG_NT / 32;
 	double pq = 0.0;
-	for (int j = blockIdx.x * wpb + (threadIdx.x >> 5); j < n; j += gridDim.x * wpb)
+	for (int g = blockIdx.x * wpb + (threadIdx.x >> 5); g < ngroups; g += gridDim.x * wpb)
 	{
-		const int k0 = __ldg(outer + j), k1 = __ldg(outer + j + 1);
-		double s = 0.0;
-		for (int k = k0 + lane; k < k1; k += 32) s = fma(__ldg(vals + k), __ldg(p + __ldg(inner + k)), s);
-		s = warp_sum(s);
+		int c0 = 3 * g, m = 3;
+		if (groups)
+		{
+			const int code = __ldg(groups + g);
+			c0 = code >> 2;
+			m = code & 3;
+		}
+		const int k0 = __ldg(outer + c0), len = __ldg(outer + c0 + 1) - k0;
+		const int o1 = m > 1 ? __ldg(outer + c0 + 1) : k0, o2 = m > 2 ? __ldg(outer + c0 + 2) : k0;
+		double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+		for (int t = lane; t < len; t += 32)
+		{
+			const double pv = __ldg(p + __ldg(inner + k0 + t));
+			s0 = fma(__ldg(vals + k0 + t), pv, s0);
+			if (m > 1) s1 = fma(__ldg(vals + o1 + t), pv, s1);
+			if (m > 2) s2 = fma(__ldg(vals + o2 + t), pv, s2);
+		}
+		s0 = warp_sum(s0);
+		if (m > 1) s1 = warp_sum(s1);
+		if (m > 2) s2 = warp_sum(s2);
 		if (lane == 0)
 		{
-			q[j] = s;
-			pq = fma(p[j], s, pq);
+			q[c0] = s0;
+			pq = fma(p[c0], s0, pq);
+			if (m > 1)
+			{
+				q[c0 + 1] = s1;
+				pq = fma(p[c0 + 1], s1, pq);
+			}
+			if (m > 2)
+			{
+				q[c0 + 2] = s2;
+				pq = fma(p[c0 + 2], s2, pq);
+			}
 		}
 	}
 	if (part)
@@ -147,6 +180,7 @@ __global__ void __launch_bounds__(CG_NT) k_cg_step(int n, const double *__restri
 												   double *__restrict__ r, const double *__restrict__ invd,
 												   double *__restrict__ z, double *__restrict__ part)
 {
+	if (sc[CG_DONE] != 0.0) return;
 	const double alpha = sc[CG_ALPHA];
 	double rr = 0.0, rz = 0.0;
 	for (int j = blockIdx.x * CG_NT + threadIdx.x; j < n; j += gridDim.x * CG_NT)
@@ -171,6 +205,7 @@ __global__ void __launch_bounds__(CG_NT) k_cg_step(int n, const double *__restri
 __global__ void __launch_bounds__(CG_NT) k_cg_dir(int n, const double *__restrict__ sc, const double *__restrict__ z,
 												  double *__restrict__ p)
 {
+	if (sc[CG_DONE] != 0.0) return;
 	const double beta = sc[CG_BETA];
 	for (int j = blockIdx.x * CG_NT + threadIdx.x; j < n; j += gridDim.x * CG_NT) p[j] = fma(beta, p[j], z[j]);
 }
@@ -183,9 +218,10 @@ enum
 };
 
 // one block: the per-block partials summed in block order, then the scalars
-__global__ void __launch_bounds__(CG_NT) k_cg_reduce(const double *__restrict__ part, int count, int mode,
+__global__ void __launch_bounds__(CG_NT) k_cg_reduce(const double *__restrict__ part, int count, int mode, double tol,
 													 double *__restrict__ sc)
 {
+	if (mode != RED_START && sc[CG_DONE] != 0.0) return;
 	const int ncomp = mode == RED_START ? 3 : (mode == RED_ALPHA ? 1 : 2);
 	double s[3] = {0.0, 0.0, 0.0};
 	for (int c = 0; c < ncomp; ++c)
@@ -200,19 +236,29 @@ __global__ void __launch_bounds__(CG_NT) k_cg_reduce(const double *__restrict__ 
 		sc[CG_RZ] = s[0];
 		sc[CG_RR] = s[1];
 		sc[CG_RHS2] = s[2];
+		const double thr = fmax(tol * tol * s[2], 2.2250738585072014e-308);
+		sc[CG_THR] = thr;
+		sc[CG_DONE] = (s[2] == 0.0 || s[1] < thr) ? 1.0 : 0.0;
+		sc[CG_ITER] = 0.0;
 	}
 	else if (mode == RED_ALPHA)
 		sc[CG_ALPHA] = sc[CG_RZ] / s[0];
 	else
 	{
 		sc[CG_RR] = s[0];
-		sc[CG_BETA] = s[1] / sc[CG_RZ];
-		sc[CG_RZ] = s[1];
+		if (s[0] < sc[CG_THR])
+			sc[CG_DONE] = 1.0; // converged: x and r stay as they are, the count is not advanced
+		else
+		{
+			sc[CG_BETA] = s[1] / sc[CG_RZ];
+			sc[CG_RZ] = s[1];
+			sc[CG_ITER] += 1.0;
+		}
 	}
 }
 
 int grid_vec(int n) { return n <= 0 ? 1 : (int)std::min<long long>(CG_MAX_GRID, ((long long)n + CG_NT - 1) / CG_NT); }
-int grid_spmv(int n) { return n <= 0 ? 1 : (int)std::min<long long>(CG_MAX_GRID, ((long long)n + 7) / 8); }
+int grid_spmv(int ngroups) { return ngroups <= 0 ? 1 : (int)std::min<long long>(CG_MAX_GRID, ((long long)ngroups + 7) / 8); }
 
 } // namespace
 
@@ -225,13 +271,14 @@ cudaError_t launch_cg_diag_inv(int n, const int *outer, const int *inner, const 
 	return cudaGetLastError();
 }
 
-cudaError_t launch_cg_start(int n, const int *outer, const int *inner, const double *vals, const double *b,
-							bool guess, double *x, const CgWork &w, cudaStream_t s)
+cudaError_t launch_cg_start(int n, int ngroups, const int *groups, const int *outer, const int *inner,
+							const double *vals, const double *b, bool guess, double tol, double *x, const CgWork &w,
+							cudaStream_t s)
 {
 	const int gv = grid_vec(n);
 	if (guess)
 	{
-		k_spmv<<<grid_spmv(n), CG_NT, 0, s>>>(n, outer, inner, vals, x, w.q, nullptr);
+		k_spmv<<<grid_spmv(ngroups), CG_NT, 0, s>>>(ngroups, groups, outer, inner, vals, x, w.q, nullptr, w.sc);
 		k_resid<<<gv, CG_NT, 0, s>>>(n, b, w.q, w.r);
 	}
 	else
@@ -242,24 +289,22 @@ cudaError_t launch_cg_start(int n, const int *outer, const int *inner, const dou
 		if (e != cudaSuccess) return e;
 	}
 	k_cg_start<<<gv, CG_NT, 0, s>>>(n, w.invd, b, w.r, w.p, w.part);
-	k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gv, RED_START, w.sc);
+	k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gv, RED_START, tol, w.sc);
 	return cudaGetLastError();
 }
 
-cudaError_t launch_cg_iteration(int n, const int *outer, const int *inner, const double *vals, double *x,
-								const CgWork &w, cudaStream_t s)
+cudaError_t launch_cg_iterations(int n, int count, int ngroups, const int *groups, const int *outer,
+								 const int *inner, const double *vals, double *x, const CgWork &w, cudaStream_t s)
 {
-	const int gs = grid_spmv(n), gv = grid_vec(n);
-	k_spmv<<<gs, CG_NT, 0, s>>>(n, outer, inner, vals, w.p, w.q, w.part);
-	k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gs, RED_ALPHA, w.sc);
-	k_cg_step<<<gv, CG_NT, 0, s>>>(n, w.sc, w.p, w.q, x, w.r, w.invd, w.z, w.part);
-	k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gv, RED_BETA, w.sc);
-	return cudaGetLastError();
-}
-
-cudaError_t launch_cg_direction(int n, const CgWork &w, cudaStream_t s)
-{
-	k_cg_dir<<<grid_vec(n), CG_NT, 0, s>>>(n, w.sc, w.z, w.p);
+	const int gs = grid_spmv(ngroups), gv = grid_vec(n);
+	for (int i = 0; i < count; ++i)
+	{
+		k_spmv<<<gs, CG_NT, 0, s>>>(ngroups, groups, outer, inner, vals, w.p, w.q, w.part, w.sc);
+		k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gs, RED_ALPHA, 0.0, w.sc);
+		k_cg_step<<<gv, CG_NT, 0, s>>>(n, w.sc, w.p, w.q, x, w.r, w.invd, w.z, w.part);
+		k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gv, RED_BETA, 0.0, w.sc);
+		k_cg_dir<<<gv, CG_NT, 0, s>>>(n, w.sc, w.z, w.p);
+	}
 	return cudaGetLastError();
 }
 
