@@ -37,6 +37,9 @@ namespace
 
 constexpr int CG_NT = 256;      // threads per block of every kernel here
 constexpr int CG_MAX_GRID = 1184; // 148 SMs x 8: blocks of the grid-stride kernels
+#ifndef PFG_SPMV_MINB
+#define PFG_SPMV_MINB 8 // 64 warps per SM at 32 registers (a few spill): measured best
+#endif
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -88,8 +91,9 @@ __global__ void __launch_bounds__(CG_NT) k_diag_inv(int n, const int *__restrict
 
 // q = H p, one warp per column group (m <= 3 consecutive columns with the same rows,
 // a node's dofs): each row index is loaded and p gathered once for the m columns.
-// part[block] = sum over the block's columns of p_j q_j when part != nullptr.
-__global__ void __launch_bounds__(CG_NT) k_spmv(int ngroups, const int *__restrict__ groups,
+// part[warp] = sum over the warp's columns of p_j q_j when part != nullptr (one
+// partial per warp: no block barrier behind the slowest warp).
+__global__ void __launch_bounds__(CG_NT, PFG_SPMV_MINB) k_spmv(int ngroups, const int *__restrict__ groups,
 												const int *__restrict__ outer, const int *__restrict__ inner,
 												const double *__restrict__ vals, const double *__restrict__ p,
 												double *__restrict__ q, double *__restrict__ part,
@@ -137,11 +141,7 @@ __global__ void __launch_bounds__(CG_NT) k_spmv(int ngroups, const int *__restri
 			}
 		}
 	}
-	if (part)
-	{
-		const double t = block_sum(pq);
-		if (threadIdx.x == 0) part[blockIdx.x] = t;
-	}
+	if (part && lane == 0) part[blockIdx.x * wpb + (threadIdx.x >> 5)] = pq;
 }
 
 // r = b - q
@@ -262,7 +262,7 @@ int grid_spmv(int ngroups) { return ngroups <= 0 ? 1 : (int)std::min<long long>(
 
 } // namespace
 
-size_t cg_partials_doubles() { return 3 * (size_t)CG_MAX_GRID; }
+size_t cg_partials_doubles() { return (size_t)(CG_NT / 32) * CG_MAX_GRID; } // one per SpMV warp, >= 3 per vector block
 
 cudaError_t launch_cg_diag_inv(int n, const int *outer, const int *inner, const double *vals, double *invd,
 							   cudaStream_t s)
@@ -300,7 +300,7 @@ cudaError_t launch_cg_iterations(int n, int count, int ngroups, const int *group
 	for (int i = 0; i < count; ++i)
 	{
 		k_spmv<<<gs, CG_NT, 0, s>>>(ngroups, groups, outer, inner, vals, w.p, w.q, w.part, w.sc);
-		k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gs, RED_ALPHA, 0.0, w.sc);
+		k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gs * (CG_NT / 32), RED_ALPHA, 0.0, w.sc);
 		k_cg_step<<<gv, CG_NT, 0, s>>>(n, w.sc, w.p, w.q, x, w.r, w.invd, w.z, w.part);
 		k_cg_reduce<<<1, CG_NT, 0, s>>>(w.part, gv, RED_BETA, 0.0, w.sc);
 		k_cg_dir<<<gv, CG_NT, 0, s>>>(n, w.sc, w.z, w.p);
