@@ -163,6 +163,30 @@ const char *pfg_status_string(int status);
 int pfg_version(void);
 
 /* ---------------------------------------------------------------------------
+ * Other materials.  AssemblerUtils::make_assembler picks the elastic formulation by
+ * name (assembler/AssemblerUtils.cpp:69-93); NeoHookean is this library's default
+ * and its fully tuned path.  pfg_set_material switches a context to
+ *   PFG_MAT_ISOCHORIC_NEOHOOKEAN: IsochoricNeoHookean (IsochoricNeoHookean.hpp:19-33),
+ *                                 psi = mu/2 (tr(F^T F) / J^(2/3) - 3);
+ *   PFG_MAT_SAINT_VENANT        : SaintVenantElasticity (SaintVenantElasticity.cpp:
+ *                                 209-267) with the isotropic elasticity tensor of
+ *                                 (lambda, mu) (ElasticityTensor::set_from_lambda_mu),
+ *                                 psi = lambda/2 tr(E)^2 + mu |E|^2, E = (F^T F - I)/2;
+ * both with the per-element (lambda, mu) of pfg_set_lame.  Energy, gradient and
+ * Hessian (with project_psd and the Dirichlet reduction) then follow the chosen
+ * material in PFG_FP64 (other precisions return PFG_ERR_UNSUPPORTED); the adjoint
+ * terms (pfg_material_vjp, pfg_shape_vjp) remain NeoHookean-only.  Takes effect for
+ * the calls that follow; the pattern is unchanged.
+ * ------------------------------------------------------------------------- */
+enum pfg_material
+{
+	PFG_MAT_NEOHOOKEAN = 0,
+	PFG_MAT_ISOCHORIC_NEOHOOKEAN = 1,
+	PFG_MAT_SAINT_VENANT = 2
+};
+int pfg_set_material(pfg_context *ctx, int material);
+
+/* ---------------------------------------------------------------------------
  * Dirichlet reduction.  When the only constraint form of the nonlinear problem
  * is the Dirichlet one (BCLagrangianForm::can_project), NLProblem reduces the
  * full quantities by dropping the constrained dofs:

@@ -38,6 +38,7 @@ def lib():
         L.orc_destroy.argtypes = [ctypes.c_void_p]
         L.orc_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_project_psd.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_set_material.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_project_psd.argtypes = [_d, ctypes.c_int]
         L.orc_energy.restype = ctypes.c_double
         L.orc_energy.argtypes = [ctypes.c_void_p, _d]
@@ -80,8 +81,10 @@ def _ip(a):
 class Oracle:
     """CPU restatement of NLAssembler + ElasticForm + ElasticForceDerivative."""
 
+    MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2}
+
     def __init__(self, mesh, lam, mu, n_threads: int = 1, cache_size: int = 900000,
-                 fast_pattern: bool = False):
+                 fast_pattern: bool = False, material: str = "NeoHookean"):
         L = lib()
         self.mesh = mesh
         self._conn = np.ascontiguousarray(mesh.conn, dtype=np.int32)
@@ -95,6 +98,7 @@ class Oracle:
         if not self.h:
             raise RuntimeError("oracle creation failed")
         self.n_dofs = mesh.n_dofs
+        L.orc_set_material(self.h, self.MATERIALS[material])
 
     def __del__(self):
         if getattr(self, "h", None):

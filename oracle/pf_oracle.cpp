@@ -463,6 +463,211 @@ static void element_hessian(const ElementValues &v, const double *x, double lamb
 // ---------------------------------------------------------------------------
 // SparseMatrixCache restatement (utils/MatrixCache.cpp:8-228, 289-322)
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Other materials of the GenericElastic family (assembler/GenericElastic.hpp:93-130):
+// energy = sum_q psi(F_q) da_q with F = I + grad u (real_def_grad, the default);
+// gradient and Hessian with AutodiffType::STRESS (GenericElastic.hpp:70): dpsi/dF
+// and d2psi/dF2 by second-order forward-mode dual numbers over the 9 entries of F
+// (the reference's DScalar2 over def_grad, GenericElastic.cpp:502-511), contracted
+// with the physical basis gradients.
+//   MAT_ISO_NEOHOOKEAN: IsochoricNeoHookean::elastic_energy (IsochoricNeoHookean.hpp:19-33)
+//   MAT_SAINT_VENANT  : SaintVenantElasticity::compute_energy_aux (SaintVenantElasticity.cpp:
+//                       209-267) with the isotropic tensor of ElasticityTensor::set_from_lambda_mu
+//                       (MatParams.cpp:211-260); per element (lambda, mu) here.
+// ---------------------------------------------------------------------------
+enum
+{
+	MAT_NEOHOOKEAN = 0,
+	MAT_ISO_NEOHOOKEAN = 1,
+	MAT_SAINT_VENANT = 2
+};
+
+// value, gradient and Hessian with respect to the 9 entries F(r, c) (index 3r + c)
+struct D2
+{
+	double v = 0, g[9] = {}, h[9][9] = {};
+	D2() = default;
+	D2(double x) : v(x) {}
+	static D2 var(double x, int k)
+	{
+		D2 d(x);
+		d.g[k] = 1.0;
+		return d;
+	}
+};
+static D2 operator+(const D2 &a, const D2 &b)
+{
+	D2 r(a.v + b.v);
+	for (int i = 0; i < 9; ++i)
+	{
+		r.g[i] = a.g[i] + b.g[i];
+		for (int j = 0; j < 9; ++j) r.h[i][j] = a.h[i][j] + b.h[i][j];
+	}
+	return r;
+}
+static D2 operator*(double s, const D2 &a)
+{
+	D2 r(s * a.v);
+	for (int i = 0; i < 9; ++i)
+	{
+		r.g[i] = s * a.g[i];
+		for (int j = 0; j < 9; ++j) r.h[i][j] = s * a.h[i][j];
+	}
+	return r;
+}
+static D2 operator-(const D2 &a, const D2 &b) { return a + (-1.0) * b; }
+static D2 operator*(const D2 &a, const D2 &b)
+{
+	D2 r(a.v * b.v);
+	for (int i = 0; i < 9; ++i)
+	{
+		r.g[i] = a.g[i] * b.v + a.v * b.g[i];
+		for (int j = 0; j < 9; ++j)
+			r.h[i][j] = a.h[i][j] * b.v + a.v * b.h[i][j] + a.g[i] * b.g[j] + b.g[i] * a.g[j];
+	}
+	return r;
+}
+// f(a) for a scalar function with f' = d1, f'' = d2 at a.v
+static D2 chain(const D2 &a, double f, double d1, double d2)
+{
+	D2 r(f);
+	for (int i = 0; i < 9; ++i)
+	{
+		r.g[i] = d1 * a.g[i];
+		for (int j = 0; j < 9; ++j) r.h[i][j] = d1 * a.h[i][j] + d2 * a.g[i] * a.g[j];
+	}
+	return r;
+}
+static D2 dpow(const D2 &a, double p)
+{
+	return chain(a, std::pow(a.v, p), p * std::pow(a.v, p - 1), p * (p - 1) * std::pow(a.v, p - 2));
+}
+static D2 operator/(const D2 &a, const D2 &b) { return a * dpow(b, -1.0); }
+static double dpow(double a, double p) { return std::pow(a, p); }
+
+template <class S>
+static S det3s(const S (&F)[3][3])
+{
+	return F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) - F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+		   F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+}
+
+// IsochoricNeoHookean: Cbar = F^T F / J^(2/3), psi = mu/2 (tr Cbar - 3)
+template <class S>
+static S psi_iso_neohookean(const S (&F)[3][3], double, double mu)
+{
+	const S J = det3s(F);
+	const S jp = dpow(J, 2.0 / 3.0);
+	S tr = S(0.0);
+	for (int k = 0; k < 3; ++k)
+		for (int i = 0; i < 3; ++i) tr = tr + F[i][k] * F[i][k] / jp; // (F^T F)(k,k) / J^(2/3)
+	return (mu / 2.0) * (tr - S(3.0));
+}
+
+// SaintVenant: strain from the displacement gradient, Voigt strain with doubled
+// shears, stress = C eps with C = [2mu+lambda, lambda, lambda; ...; mu, mu, mu],
+// psi = 1/2 tr(stress * strain)
+template <class S>
+static S psi_saint_venant(const S (&F)[3][3], double lambda, double mu)
+{
+	S G[3][3], E[3][3];
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c) G[r][c] = F[r][c] - S(r == c ? 1.0 : 0.0);
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c)
+		{
+			S gtg = S(0.0);
+			for (int k = 0; k < 3; ++k) gtg = gtg + G[k][r] * G[k][c];
+			E[r][c] = 0.5 * (gtg + G[r][c] + G[c][r]);
+		}
+	const S eps[6] = {E[0][0], E[1][1], E[2][2], 2.0 * E[1][2], 2.0 * E[0][2], 2.0 * E[0][1]};
+	const double C[6][6] = {{2 * mu + lambda, lambda, lambda, 0, 0, 0}, {lambda, 2 * mu + lambda, lambda, 0, 0, 0},
+							{lambda, lambda, 2 * mu + lambda, 0, 0, 0}, {0, 0, 0, mu, 0, 0},
+							{0, 0, 0, 0, mu, 0},                       {0, 0, 0, 0, 0, mu}};
+	S st[6];
+	for (int j = 0; j < 6; ++j)
+	{
+		st[j] = C[j][0] * eps[0];
+		for (int k = 1; k < 6; ++k) st[j] = st[j] + C[j][k] * eps[k];
+	}
+	const S sig[3][3] = {{st[0], st[5], st[4]}, {st[5], st[1], st[3]}, {st[4], st[3], st[2]}};
+	S tr = S(0.0);
+	for (int r = 0; r < 3; ++r)
+		for (int k = 0; k < 3; ++k) tr = tr + sig[r][k] * E[k][r];
+	return 0.5 * tr;
+}
+
+template <class S>
+static S psi_material(int mat, const S (&F)[3][3], double lambda, double mu)
+{
+	return mat == MAT_ISO_NEOHOOKEAN ? psi_iso_neohookean(F, lambda, mu) : psi_saint_venant(F, lambda, mu);
+}
+
+template <int N>
+static void def_grad_plain(const ElementValues &v, const double *x, int p, double (&F)[3][3])
+{
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c)
+		{
+			double s = 0;
+			for (int i = 0; i < N; ++i) s += x[(size_t)v.global[i] * 3 + r] * v.grad_t_m[p][i][c];
+			F[r][c] = s + (r == c ? 1.0 : 0.0);
+		}
+}
+
+template <int N>
+static double gen_element_energy(int mat, const ElementValues &v, const double *x, double lambda, double mu)
+{
+	double energy = 0;
+	for (int p = 0; p < v.nq; ++p)
+	{
+		double F[3][3];
+		def_grad_plain<N>(v, x, p, F);
+		energy += psi_material(mat, F, lambda, mu) * (v.det[p] * v.w[p]);
+	}
+	return energy;
+}
+
+// gradient (grad != nullptr, 3N) and Hessian (hess != nullptr, 3N x 3N row-major)
+template <int N>
+static void gen_element_derivatives(int mat, const ElementValues &v, const double *x, double lambda, double mu,
+									double *grad, double *hess)
+{
+	constexpr int ND = 3 * N;
+	if (grad) std::fill(grad, grad + ND, 0.0);
+	if (hess) std::fill(hess, hess + ND * ND, 0.0);
+	for (int p = 0; p < v.nq; ++p)
+	{
+		double Fv[3][3];
+		def_grad_plain<N>(v, x, p, Fv);
+		D2 F[3][3];
+		for (int r = 0; r < 3; ++r)
+			for (int c = 0; c < 3; ++c) F[r][c] = D2::var(Fv[r][c], 3 * r + c);
+		const D2 psi = psi_material(mat, F, lambda, mu);
+		const double da = v.det[p] * v.w[p];
+		const double(*g)[3] = v.grad_t_m[p];
+		for (int i = 0; i < N; ++i)
+			for (int r = 0; r < 3; ++r)
+			{
+				if (grad)
+				{
+					double s = 0;
+					for (int c = 0; c < 3; ++c) s += psi.g[3 * r + c] * g[i][c];
+					grad[i * 3 + r] += s * da;
+				}
+				if (hess)
+					for (int j = 0; j < N; ++j)
+						for (int t = 0; t < 3; ++t)
+						{
+							double s = 0;
+							for (int c = 0; c < 3; ++c)
+								for (int d = 0; d < 3; ++d) s += g[i][c] * psi.h[3 * r + c][3 * t + d] * g[j][d];
+							hess[(i * 3 + r) * ND + j * 3 + t] += s * da;
+						}
+			}
+	}
+}
+
 struct Triplet
 {
 	int r, c;
@@ -708,6 +913,7 @@ struct Context
 	SparseMatrixCache mat_cache;
 	bool fast_pattern = false; // build the first-call pattern by sorting instead of triplets
 	bool project_psd = false;  // NLAssembler::assemble_hessian(project_to_psd = true)
+	int material = 0;          // MAT_*: the assembler's formulation
 	CSC last;                  // last assembled Hessian
 	std::string err;
 
@@ -730,7 +936,8 @@ static double energy_impl(Context &c, const double *x, double *per_elem)
 		for (int el = s; el < e; ++el)
 		{
 			c.vals(el, v);
-			const double val = element_energy<N>(v, x, c.lambda[el], c.mu[el]);
+			const double val = c.material ? gen_element_energy<N>(c.material, v, x, c.lambda[el], c.mu[el])
+										  : element_energy<N>(v, x, c.lambda[el], c.mu[el]);
 			if (per_elem) per_elem[el] = val;
 			acc += val;
 		}
@@ -753,7 +960,10 @@ static void gradient_impl(Context &c, const double *x, double *g)
 		for (int el = s; el < e; ++el)
 		{
 			c.vals(el, v);
-			element_gradient<N>(v, x, c.lambda[el], c.mu[el], val);
+			if (c.material)
+				gen_element_derivatives<N>(c.material, v, x, c.lambda[el], c.mu[el], val, nullptr);
+			else
+				element_gradient<N>(v, x, c.lambda[el], c.mu[el], val);
 			for (int j = 0; j < N; ++j)
 				for (int m = 0; m < 3; ++m) local[tid][(size_t)v.global[j] * 3 + m] += val[j * 3 + m];
 		}
@@ -917,7 +1127,10 @@ static void hessian_impl(Context &c, const double *x)
 		for (int el = s; el < e; ++el)
 		{
 			c.vals(el, v);
-			element_hessian<N>(v, x, c.lambda[el], c.mu[el], H.data());
+			if (c.material)
+				gen_element_derivatives<N>(c.material, v, x, c.lambda[el], c.mu[el], nullptr, H.data());
+			else
+				element_hessian<N>(v, x, c.lambda[el], c.mu[el], H.data());
 			if (c.project_psd) project_to_psd(H.data(), ND);
 			for (int i = 0; i < N; ++i)
 				for (int j = 0; j < N; ++j)
@@ -1130,6 +1343,8 @@ extern "C"
 	void orc_set_threads(void *h, int n) { static_cast<Context *>(h)->n_threads = std::max(1, n); }
 	// later orc_hessian calls project every element matrix onto the PSD cone
 	void orc_set_project_psd(void *h, int on) { static_cast<Context *>(h)->project_psd = on != 0; }
+	// later calls use another material of the GenericElastic family (MAT_*); 0 = NeoHookean
+	void orc_set_material(void *h, int mat) { static_cast<Context *>(h)->material = mat; }
 	// ipc::project_to_psd (CLAMP) of one row-major m x m symmetric matrix, in place
 	void orc_project_psd(double *H, int m) { project_to_psd(H, m); }
 
@@ -1205,6 +1420,12 @@ extern "C"
 		c.vals(e, v);
 		return dispatch(c.t.n, [&](auto N) {
 			constexpr int n = decltype(N)::value;
+			if (c.material)
+			{
+				if (energy) *energy = gen_element_energy<n>(c.material, v, x, c.lambda[e], c.mu[e]);
+				if (grad || hess) gen_element_derivatives<n>(c.material, v, x, c.lambda[e], c.mu[e], grad, hess);
+				return 0;
+			}
 			if (energy) *energy = element_energy<n>(v, x, c.lambda[e], c.mu[e]);
 			if (grad) element_gradient<n>(v, x, c.lambda[e], c.mu[e], grad);
 			if (hess) element_hessian<n>(v, x, c.lambda[e], c.mu[e], hess);

@@ -55,6 +55,7 @@ class NeoHookeanAssembler:
         self.n_nodes = int(n_nodes if n_nodes is not None else (self._conn.max() + 1 if self._conn.size else 0))
         self.n_geom_nodes = int(self._X.shape[0])
         self.n_dofs = 3 * self.n_nodes
+        self.material = "NeoHookean"
         lam = np.ascontiguousarray(np.broadcast_to(np.asarray(lam, dtype=np.float64), (self.n_elements,)))
         mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (self.n_elements,)))
         self.device = int(device)
@@ -234,6 +235,18 @@ class NeoHookeanAssembler:
         check(lib().pfg_shape_vjp(self._h, ptrs[0], ptrs[1], mem, _prec(precision), optr), self._h,
               "pfg_shape_vjp")
         return out
+
+    # -- material (AssemblerUtils::make_assembler's formulation name) ------------------
+    MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2}
+
+    def set_material(self, formulation: str):
+        """Switch the elastic formulation: "NeoHookean" (default), "IsochoricNeoHookean"
+        or "SaintVenant" (isotropic, per-element lambda/mu).  The two others are
+        assembled in FP64; the adjoint terms stay NeoHookean-only."""
+        if formulation not in self.MATERIALS:
+            raise ValueError(f"unknown formulation {formulation!r}; one of {sorted(self.MATERIALS)}")
+        check(lib().pfg_set_material(self._h, self.MATERIALS[formulation]), self._h, "pfg_set_material")
+        self.material = formulation
 
     # -- Dirichlet reduction (NLProblem + BCLagrangianForm projection) ---------------
     def set_dirichlet(self, dofs):

@@ -135,6 +135,13 @@ void parallel_ranges(long long n, F &&f)
 }
 
 int check_mem(int mem) { return mem == PFG_MEM_HOST || mem == PFG_MEM_DEVICE; }
+// The other materials (pfg_set_material) are assembled in FP64 only.
+int check_material_prec(pfg_context *c, int prec)
+{
+	if (c->m.mat != PFG_MAT_NEOHOOKEAN && prec != PFG_FP64)
+		return fail(c, PFG_ERR_UNSUPPORTED, "only PFG_FP64 is implemented for materials other than NeoHookean");
+	return PFG_OK;
+}
 int check_prec(int prec) { return prec == PFG_FP64 || prec == PFG_FP32 || prec == PFG_SPLIT32; }
 
 int ensure_staging(pfg_context *c, size_t out_doubles)
@@ -665,6 +672,14 @@ int pfg_set_stream(pfg_context *c, void *stream)
 	return PFG_OK;
 }
 
+int pfg_set_material(pfg_context *c, int material)
+{
+	if (!c || (material != PFG_MAT_NEOHOOKEAN && material != PFG_MAT_ISOCHORIC_NEOHOOKEAN && material != PFG_MAT_SAINT_VENANT))
+		return fail(c, PFG_ERR_INVALID, "bad arguments");
+	c->m.mat = material;
+	return PFG_OK;
+}
+
 int pfg_set_lame(pfg_context *c, const double *lambda, const double *mu, int mem)
 {
 	if (!c || !check_mem(mem)) return fail(c, PFG_ERR_INVALID, "bad arguments");
@@ -706,6 +721,7 @@ int pfg_energy(pfg_context *c, const double *u, int mem, int prec, double *out)
 {
 	if (!c || !check_mem(mem) || !check_prec(prec) || !out) return fail(c, PFG_ERR_INVALID, "bad arguments");
 	if (c->m.N && !u) return fail(c, PFG_ERR_INVALID, "u NULL");
+	if (int st_m = check_material_prec(c, prec)) return st_m;
 	DeviceGuard g(c->device);
 	int st = ensure_staging(c, 1);
 	if (st) return st;
@@ -722,6 +738,7 @@ int pfg_energy_per_element(pfg_context *c, const double *u, int mem, int prec, d
 {
 	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.E && !out)) return fail(c, PFG_ERR_INVALID, "bad arguments");
 	if (c->m.N && !u) return fail(c, PFG_ERR_INVALID, "u NULL");
+	if (int st_m = check_material_prec(c, prec)) return st_m;
 	DeviceGuard g(c->device);
 	int st = ensure_staging(c, std::max(c->m.E, 1));
 	if (st) return st;
@@ -737,6 +754,7 @@ int pfg_energy_per_element(pfg_context *c, const double *u, int mem, int prec, d
 int pfg_gradient(pfg_context *c, const double *u, int mem, int prec, double *gout)
 {
 	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.N && (!gout || !u))) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (int st_m = check_material_prec(c, prec)) return st_m;
 	DeviceGuard g(c->device);
 	const size_t ndof = 3 * (size_t)c->m.N;
 	int st = ensure_staging(c, std::max<size_t>(ndof, 1));
@@ -780,6 +798,7 @@ int pfg_hessian(pfg_context *c, const double *u, int mem, int prec, int project_
 {
 	if (!c || !check_mem(mem) || !check_prec(prec)) return fail(c, PFG_ERR_INVALID, "bad arguments");
 	if (c->m.N && !u) return fail(c, PFG_ERR_INVALID, "u NULL");
+	if (int st_m = check_material_prec(c, prec)) return st_m;
 	DeviceGuard g(c->device);
 	int st;
 	if (!c->has_pattern && (st = build_pattern(c))) return st;
@@ -809,6 +828,8 @@ int pfg_hessian_device_csc(pfg_context *c, const int **outer, const int **inner,
 int pfg_material_vjp(pfg_context *c, const double *u, const double *p, int mem, double *out)
 {
 	if (!c || !check_mem(mem) || (c->m.E && !out) || (c->m.N && (!u || !p))) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (c->m.mat != PFG_MAT_NEOHOOKEAN)
+		return fail(c, PFG_ERR_UNSUPPORTED, "the adjoint terms are implemented for NeoHookean only");
 	DeviceGuard g(c->device);
 	const size_t ndof = 3 * (size_t)c->m.N;
 	int st = ensure_staging(c, std::max<size_t>(2 * (size_t)c->m.E, 1));
@@ -826,6 +847,8 @@ int pfg_shape_vjp(pfg_context *c, const double *u, const double *p, int mem, int
 {
 	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.Ng && !out) || (c->m.N && (!u || !p)))
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (c->m.mat != PFG_MAT_NEOHOOKEAN)
+		return fail(c, PFG_ERR_UNSUPPORTED, "the adjoint terms are implemented for NeoHookean only");
 	DeviceGuard g(c->device);
 	const size_t ndof = 3 * (size_t)c->m.N;
 	int st = ensure_staging(c, std::max<size_t>(3 * (size_t)c->m.Ng, 1));
@@ -905,6 +928,7 @@ int pfg_hessian_reduced(pfg_context *c, const double *u, int mem, int prec, int 
 	if (!c || !check_mem(mem) || !check_prec(prec)) return fail(c, PFG_ERR_INVALID, "bad arguments");
 	if (c->m.N && !u) return fail(c, PFG_ERR_INVALID, "u NULL");
 	if (!c->has_dirichlet) return fail(c, PFG_ERR_STATE, "no Dirichlet set (pfg_set_dirichlet)");
+	if (int st_m = check_material_prec(c, prec)) return st_m;
 	DeviceGuard g(c->device);
 	int st;
 	if ((st = ensure_staging(c, 1))) return st;
@@ -925,6 +949,7 @@ int pfg_gradient_reduced(pfg_context *c, const double *u, int mem, int prec, dou
 {
 	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.N && (!g_out || !u))) return fail(c, PFG_ERR_INVALID, "bad arguments");
 	if (!c->has_dirichlet) return fail(c, PFG_ERR_STATE, "no Dirichlet set (pfg_set_dirichlet)");
+	if (int st_m = check_material_prec(c, prec)) return st_m;
 	DeviceGuard g(c->device);
 	const size_t ndof = 3 * (size_t)c->m.N;
 	int st = ensure_staging(c, std::max<size_t>(ndof, 1));

@@ -21,6 +21,7 @@ namespace pfg
 struct DevMesh
 {
 	int et = 0, E = 0, N = 0, Ng = 0;
+	int mat = 0; // 0 NeoHookean, 1 IsochoricNeoHookean, 2 SaintVenant (pfg_set_material)
 	const int *conn = nullptr;
 	const int *gconn = nullptr;
 	const double *X = nullptr;

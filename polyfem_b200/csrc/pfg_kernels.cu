@@ -1471,6 +1471,404 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__r
 	}
 }
 
+// ---------------------------------------------------------------------------
+// Other materials of the GenericElastic family, FP64: energy, gradient and the
+// element blocks of the Hessian (the scatter, the PSD projection and the Dirichlet
+// reduction are the NeoHookean path's).  The reference differentiates psi(F) with
+// dual numbers (GenericElastic.cpp, AutodiffType::STRESS); here the first Piola
+// stress P = dpsi/dF and the blocks H_ab = sum_q da sum_jl g_a[j] dP_ij/dF_kl g_b[l]
+// are written out analytically with the per-node vectors g_a (physical basis
+// gradient), f_a = F g_a and d_a = F^-T g_a:
+//  IsochoricNeoHookean (IsochoricNeoHookean.hpp:19-33), psi = mu/2 (|F|^2 J^-2/3 - 3):
+//    P = mu J^-2/3 (F - |F|^2/3 F^-T)
+//    H_ab = mu J^-2/3 da [ (g_a.g_b) I - 2/3 (f_a d_b^T + d_a f_b^T)
+//                          + 2/9 |F|^2 d_a d_b^T + |F|^2/3 d_b d_a^T ]
+//  SaintVenant, isotropic (SaintVenantElasticity.cpp:209-267 with the tensor of
+//  ElasticityTensor::set_from_lambda_mu, MatParams.cpp:211-260),
+//  psi = lambda/2 tr(E)^2 + mu |E|^2, E = (F^T F - I)/2, S = lambda tr(E) I + 2 mu E:
+//    P = F S
+//    H_ab = da [ (g_a^T S g_b) I + lambda f_a f_b^T + mu (g_a.g_b) F F^T + mu f_b f_a^T ]
+// ---------------------------------------------------------------------------
+constexpr int MAT_ISO_NEOHOOKEAN = 1, MAT_SAINT_VENANT = 2;
+
+// Green strain from the displacement gradient G = F - I: E = (G^T G + G + G^T) / 2
+__device__ __forceinline__ void green_strain(const double F[3][3], double E[3][3])
+{
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c)
+		{
+			double gtg = 0.0;
+#pragma unroll
+			for (int k = 0; k < 3; ++k) gtg += (F[k][r] - (k == r)) * (F[k][c] - (k == c));
+			E[r][c] = 0.5 * (gtg + (F[r][c] - (r == c)) + (F[c][r] - (r == c)));
+		}
+}
+
+template <int MAT>
+__device__ __forceinline__ double mat_psi(const double F[3][3], double lambda, double mu)
+{
+	if constexpr (MAT == MAT_ISO_NEOHOOKEAN)
+	{
+		double I1 = 0.0;
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) I1 += F[r][c] * F[r][c];
+		return mu / 2 * (I1 * pow(det3(F), -2.0 / 3.0) - 3.0);
+	}
+	else
+	{
+		double E[3][3];
+		green_strain(F, E);
+		const double tr = E[0][0] + E[1][1] + E[2][2];
+		double e2 = 0.0;
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) e2 += E[r][c] * E[r][c];
+		return lambda / 2 * tr * tr + mu * e2;
+	}
+}
+
+template <int MAT>
+__device__ __forceinline__ void mat_piola(const double F[3][3], double lambda, double mu, double P[3][3])
+{
+	if constexpr (MAT == MAT_ISO_NEOHOOKEAN)
+	{
+		double I1 = 0.0;
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) I1 += F[r][c] * F[r][c];
+		const double J = det3(F);
+		double G[3][3];
+		inv_transpose3(F, J, G);
+		const double cj = mu * pow(J, -2.0 / 3.0);
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) P[r][c] = cj * (F[r][c] - I1 / 3 * G[r][c]);
+	}
+	else
+	{
+		double E[3][3];
+		green_strain(F, E);
+		const double tr = E[0][0] + E[1][1] + E[2][2];
+		double S[3][3];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) S[r][c] = 2 * mu * E[r][c] + (r == c ? lambda * tr : 0.0);
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) P[r][c] = F[r][0] * S[0][c] + F[r][1] * S[1][c] + F[r][2] * S[2][c];
+	}
+}
+
+// F = I + (U^T gref_q) J^-T at quadrature point q
+template <class EL>
+__device__ __forceinline__ void gen_def_grad(int q, const double U[EL::N][3], const double Jit[3][3], double F[3][3])
+{
+	double A[3][3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c)
+		{
+			double s_ = 0.0;
+#pragma unroll
+			for (int a = 0; a < EL::N; ++a) s_ += U[a][r] * gref<EL>(q, a, c);
+			A[r][c] = s_;
+		}
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) F[r][c] = A[r][0] * Jit[0][c] + A[r][1] * Jit[1][c] + A[r][2] * Jit[2][c] + (r == c);
+}
+
+template <class EL, int MAT>
+__device__ __forceinline__ double gen_element_energy(const DevMesh &m, const double *__restrict__ u, int e,
+													 unsigned long long *inverted)
+{
+	double Xg[EL::NG][3], U[EL::N][3];
+	int nodes[EL::N];
+	load_geom<EL, double>(m, e, Xg);
+	load_nodal<EL, double>(m, e, u, U, nodes);
+	const double2 lm = __ldg(m.lame + e);
+	double en = 0.0;
+	bool bad = false;
+#pragma unroll
+	for (int q = 0; q < EL::NQ; ++q)
+	{
+		double Jit[3][3], detJ, F[3][3];
+		geometry<EL, double>(q, Xg, Jit, detJ);
+		gen_def_grad<EL>(q, U, Jit, F);
+		bad |= !(det3(F) > 0.0);
+		en += mat_psi<MAT>(F, lm.x, lm.y) * (detJ * qweight<EL>(q));
+	}
+	if (bad) atomicAdd(inverted, 1ull);
+	return en;
+}
+
+template <class EL, int MAT, int NT>
+__global__ void __launch_bounds__(NT) k_gen_energy(DevMesh m, const double *__restrict__ u, double *__restrict__ partials,
+												   double *__restrict__ result, unsigned int *ticket,
+												   unsigned long long *inverted)
+{
+	const int e = blockIdx.x * NT + threadIdx.x;
+	double en = 0.0;
+	if (e < m.E) en = gen_element_energy<EL, MAT>(m, u, e, inverted);
+	reduce_to_result<NT>(en, partials, result, ticket);
+}
+
+template <class EL, int MAT, int NT>
+__global__ void __launch_bounds__(NT) k_gen_energy_per_element(DevMesh m, const double *__restrict__ u,
+															   double *__restrict__ out, unsigned long long *inverted)
+{
+	const int e = blockIdx.x * NT + threadIdx.x;
+	if (e < m.E) out[e] = gen_element_energy<EL, MAT>(m, u, e, inverted);
+}
+
+// element gradient G[a][d] = sum_q da (P J^-1)[d][r] gref(q, a, r), staged per
+// incidence like the NeoHookean gradient
+template <class EL, int MAT, int NT>
+__global__ void __launch_bounds__(NT) k_gen_gradient(DevMesh m, const double *__restrict__ u, double *__restrict__ stage,
+													 unsigned long long *inverted)
+{
+	const int e = blockIdx.x * NT + threadIdx.x;
+	if (e >= m.E) return;
+	double Xg[EL::NG][3], U[EL::N][3], Gacc[EL::N][3];
+	int nodes[EL::N];
+	load_geom<EL, double>(m, e, Xg);
+	load_nodal<EL, double>(m, e, u, U, nodes);
+	const double2 lm = __ldg(m.lame + e);
+#pragma unroll
+	for (int a = 0; a < EL::N; ++a) Gacc[a][0] = Gacc[a][1] = Gacc[a][2] = 0.0;
+	bool bad = false;
+#pragma unroll
+	for (int q = 0; q < EL::NQ; ++q)
+	{
+		double Jit[3][3], detJ, F[3][3], P[3][3];
+		geometry<EL, double>(q, Xg, Jit, detJ);
+		gen_def_grad<EL>(q, U, Jit, F);
+		bad |= !(det3(F) > 0.0);
+		mat_piola<MAT>(F, lm.x, lm.y, P);
+		const double da = detJ * qweight<EL>(q);
+		double Q[3][3]; // da P J^-1 = da P Jit^T
+#pragma unroll
+		for (int d = 0; d < 3; ++d)
+#pragma unroll
+			for (int r = 0; r < 3; ++r) Q[d][r] = da * (P[d][0] * Jit[r][0] + P[d][1] * Jit[r][1] + P[d][2] * Jit[r][2]);
+#pragma unroll
+		for (int a = 0; a < EL::N; ++a)
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+			{
+				const double gr = gref<EL>(q, a, r);
+				if (gr != 0.0)
+				{
+#pragma unroll
+					for (int d = 0; d < 3; ++d) Gacc[a][d] += gr * Q[d][r];
+				}
+			}
+	}
+	if (bad) atomicAdd(inverted, 1ull);
+#pragma unroll
+	for (int a = 0; a < EL::N; ++a)
+	{
+		const int k = __ldg(m.eb_inc + (size_t)e * EL::N + a);
+		st_slot(stage + (size_t)k * 4, Gacc[a][0], Gacc[a][1], Gacc[a][2]);
+	}
+}
+
+// Element blocks for the other materials, one warp per element: per point (lanes
+// q < NQ) J^-T, F, F^-T and the material's coefficients; per (point, node) the
+// vectors g, f = F g, d = F^-T g; per node pair (a <= b, tri_index order) the block,
+// written as the packed block triangle of the element (as k_hessian_blocks does).
+template <class EL>
+struct GenWarp
+{
+	static constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ, TP = tri_pad(EL::N);
+	double U[N][3], X[NG][3];
+	double F[NQ][9], G[NQ][9], Jit[NQ][9];
+	double c[NQ][16]; // IsochoricNeoHookean: mu J^-2/3 da, |F|^2; SaintVenant: da, lambda, mu, S (row-major 9)
+	double nv[NQ][N][9];
+	alignas(16) double tri[TP]; // copied out as double2 (the members above can end on an odd double)
+};
+
+template <class EL, int MAT, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_gen_blocks(DevMesh m, const double *__restrict__ u, double *__restrict__ stage)
+{
+	using W = GenWarp<EL>;
+	constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ, NP = N * (N + 1) / 2, TP = W::TP;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	W &S = reinterpret_cast<W *>(smem_raw)[threadIdx.x >> 5];
+	const int lane = threadIdx.x & 31;
+	for (int e = blockIdx.x * WPB + (threadIdx.x >> 5); e < m.E; e += gridDim.x * WPB)
+	{
+		for (int i = lane; i < N * 3; i += 32)
+			S.U[i / 3][i % 3] = __ldg(u + (size_t)__ldg(m.conn + (size_t)(i / 3) * m.E + e) * 3 + i % 3);
+		for (int i = lane; i < NG * 3; i += 32)
+			S.X[i / 3][i % 3] = __ldg(m.X + (size_t)__ldg(m.gconn + (size_t)(i / 3) * m.E + e) * 3 + i % 3);
+		__syncwarp();
+		if (lane < NQ)
+		{
+			const int q = lane;
+			const double2 lm = __ldg(m.lame + e);
+			double Jit[3][3], detJ, F[3][3];
+			geometry<EL, double>(q, S.X, Jit, detJ);
+			gen_def_grad<EL>(q, S.U, Jit, F);
+			const double da = detJ * qweight<EL>(q);
+			const double J = det3(F);
+			double G[3][3];
+			inv_transpose3(F, J, G);
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+				{
+					S.F[q][3 * r + c] = F[r][c];
+					S.G[q][3 * r + c] = G[r][c];
+					S.Jit[q][3 * r + c] = Jit[r][c];
+				}
+			if constexpr (MAT == MAT_ISO_NEOHOOKEAN)
+			{
+				double I1 = 0.0;
+#pragma unroll
+				for (int r = 0; r < 3; ++r)
+#pragma unroll
+					for (int c = 0; c < 3; ++c) I1 += F[r][c] * F[r][c];
+				S.c[q][0] = lm.y * pow(J, -2.0 / 3.0) * da;
+				S.c[q][1] = I1;
+			}
+			else
+			{
+				// c = [da, lambda, mu, S (row-major 9), -] and F F^T in S.G (F^-T unused)
+				double E[3][3];
+				green_strain(F, E);
+				const double tr = E[0][0] + E[1][1] + E[2][2];
+				S.c[q][0] = da;
+				S.c[q][1] = lm.x;
+				S.c[q][2] = lm.y;
+#pragma unroll
+				for (int r = 0; r < 3; ++r)
+#pragma unroll
+					for (int c = 0; c < 3; ++c)
+					{
+						S.c[q][3 + 3 * r + c] = 2 * lm.y * E[r][c] + (r == c ? lm.x * tr : 0.0);
+						S.G[q][3 * r + c] = F[r][0] * F[c][0] + F[r][1] * F[c][1] + F[r][2] * F[c][2];
+					}
+			}
+		}
+		__syncwarp();
+		for (int i = lane; i < NQ * N; i += 32)
+		{
+			const int q = i / N, a = i - q * N;
+			double g[3];
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+				g[c] = gref<EL>(q, a, 0) * S.Jit[q][c] + gref<EL>(q, a, 1) * S.Jit[q][3 + c] + gref<EL>(q, a, 2) * S.Jit[q][6 + c];
+			double *v = S.nv[q][a];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+			{
+				v[r] = g[r];
+				v[3 + r] = S.F[q][3 * r] * g[0] + S.F[q][3 * r + 1] * g[1] + S.F[q][3 * r + 2] * g[2];
+				v[6 + r] = MAT == MAT_ISO_NEOHOOKEAN ? S.G[q][3 * r] * g[0] + S.G[q][3 * r + 1] * g[1] + S.G[q][3 * r + 2] * g[2] : 0.0;
+			}
+		}
+		__syncwarp();
+		for (int p = lane; p < NP; p += 32)
+		{
+			int a = 0, b = p;
+			while (b >= N - a)
+			{
+				b -= N - a;
+				++a;
+			}
+			b += a;
+			double h[3][3] = {};
+			for (int q = 0; q < NQ; ++q)
+			{
+				const double *va = S.nv[q][a], *vb = S.nv[q][b];
+				const double gab = va[0] * vb[0] + va[1] * vb[1] + va[2] * vb[2];
+				if constexpr (MAT == MAT_ISO_NEOHOOKEAN)
+				{
+					const double c0 = S.c[q][0], I1 = S.c[q][1];
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+#pragma unroll
+						for (int k = 0; k < 3; ++k)
+							h[r][k] += c0 * ((r == k ? gab : 0.0) - 2.0 / 3.0 * (va[3 + r] * vb[6 + k] + va[6 + r] * vb[3 + k]) +
+											 2.0 / 9.0 * I1 * va[6 + r] * vb[6 + k] + I1 / 3.0 * vb[6 + r] * va[6 + k]);
+				}
+				else
+				{
+					const double da = S.c[q][0], lam = S.c[q][1], mu = S.c[q][2];
+					const double *Sm = S.c[q] + 3, *B = S.G[q];
+					double sab = 0.0;
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+#pragma unroll
+						for (int k = 0; k < 3; ++k) sab += va[r] * Sm[3 * r + k] * vb[k];
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+#pragma unroll
+						for (int k = 0; k < 3; ++k)
+							h[r][k] += da * ((r == k ? sab : 0.0) + lam * va[3 + r] * vb[3 + k] + mu * gab * B[3 * r + k] +
+											 mu * vb[3 + r] * va[3 + k]);
+				}
+			}
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int k = 0; k < 3; ++k) S.tri[9 * p + 3 * k + r] = h[r][k];
+		}
+		__syncwarp();
+		double2 *dst = reinterpret_cast<double2 *>(stage + (size_t)e * TP);
+		const double2 *src = reinterpret_cast<const double2 *>(S.tri);
+		for (int i = lane; i < TP / 2; i += 32) dst[i] = src[i];
+		__syncwarp();
+	}
+}
+
+template <class EL, int MAT>
+static cudaError_t gen_hessian(const DevMesh &m, const DevPattern &p, const double *u, double *stage, bool project_psd,
+							   cudaStream_t s)
+{
+	constexpr int WPB = 4, WARPS = 8;
+	const size_t bytes = WPB * sizeof(GenWarp<EL>);
+	cudaError_t e = cudaFuncSetAttribute(k_gen_blocks<EL, MAT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+	if (e != cudaSuccess) return e;
+	if (m.E > 0)
+	{
+		const int nb = std::min((m.E + WPB - 1) / WPB, 148 * 32);
+		k_gen_blocks<EL, MAT, WPB><<<nb, WPB * 32, bytes, s>>>(m, u, stage);
+	}
+	if (project_psd && m.E > 0)
+	{
+		constexpr int PW = 4;
+		const size_t bytes_p = PW * sizeof(PsdWarp<EL>);
+		e = cudaFuncSetAttribute(k_project_psd<EL, double, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
+		if (e != cudaSuccess) return e;
+		k_project_psd<EL, double, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
+	}
+	const int ng = (m.N + WARPS - 1) / WARPS;
+	if (ng > 0) k_hessian_reduce<EL, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+	return cudaGetLastError();
+}
+
+template <class EL>
+static cudaError_t gen_hessian_mat(const DevMesh &m, const DevPattern &p, const double *u, double *stage,
+								   bool project_psd, cudaStream_t s)
+{
+	return m.mat == MAT_ISO_NEOHOOKEAN ? gen_hessian<EL, MAT_ISO_NEOHOOKEAN>(m, p, u, stage, project_psd, s)
+									   : gen_hessian<EL, MAT_SAINT_VENANT>(m, p, u, stage, project_psd, s);
+}
+
 template <class EL, class K, class T>
 static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const double *u, void *stage_v,
 									bool project_psd, cudaStream_t s)
@@ -1503,6 +1901,17 @@ cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *
 {
 	const bool psd = project_psd != 0;
 	if (p.nnz == 0) return cudaSuccess;
+	if (m.mat != 0) // other materials: FP64 blocks (the caller admits PREC_FP64 only)
+	{
+		double *st = static_cast<double *>(stage);
+		switch (m.et)
+		{
+		case 1: return gen_hessian_mat<P1Tet>(m, p, u, st, psd, s);
+		case 2: return gen_hessian_mat<P2Tet>(m, p, u, st, psd, s);
+		case 3: return gen_hessian_mat<Q1Hex>(m, p, u, st, psd, s);
+		}
+		return cudaErrorInvalidValue;
+	}
 	// FP64: everything in FP64.  FP32: everything in FP32 except det/log J.
 	// SPLIT32: kinematics (J^-T, F^-T, det/log J, g, d) in FP64, contraction and
 	// records in FP32, per-entry sums in FP64.
@@ -1715,6 +2124,37 @@ static void energy_t(const DevMesh &m, const double *u, bool per_element, double
 		k_energy<EL, T, NT><<<nb, NT, 0, s>>>(m, u, sc.partials, out, sc.ticket, sc.inverted);
 }
 
+template <class EL, int MAT>
+static void gen_energy_t(const DevMesh &m, const double *u, bool per_element, double *out, const Scratch &sc, cudaStream_t s)
+{
+	constexpr int NT = 256;
+	const int nb = blocks_for(m.E, NT);
+	if (per_element)
+		k_gen_energy_per_element<EL, MAT, NT><<<nb, NT, 0, s>>>(m, u, out, sc.inverted);
+	else
+		k_gen_energy<EL, MAT, NT><<<nb, NT, 0, s>>>(m, u, sc.partials, out, sc.ticket, sc.inverted);
+}
+
+template <class EL>
+static void gen_energy_mat(const DevMesh &m, const double *u, bool per_element, double *out, const Scratch &sc,
+						   cudaStream_t s)
+{
+	if (m.mat == MAT_ISO_NEOHOOKEAN)
+		gen_energy_t<EL, MAT_ISO_NEOHOOKEAN>(m, u, per_element, out, sc, s);
+	else
+		gen_energy_t<EL, MAT_SAINT_VENANT>(m, u, per_element, out, sc, s);
+}
+
+template <class EL>
+static void gen_gradient_mat(const DevMesh &m, const double *u, const Scratch &sc, cudaStream_t s)
+{
+	constexpr int NT = 128;
+	if (m.mat == MAT_ISO_NEOHOOKEAN)
+		k_gen_gradient<EL, MAT_ISO_NEOHOOKEAN, NT><<<blocks_for(m.E, NT), NT, 0, s>>>(m, u, sc.vec_stage, sc.inverted);
+	else
+		k_gen_gradient<EL, MAT_SAINT_VENANT, NT><<<blocks_for(m.E, NT), NT, 0, s>>>(m, u, sc.vec_stage, sc.inverted);
+}
+
 int energy_elems_per_block(int) { return 256; }
 
 cudaError_t launch_energy(const DevMesh &m, const double *u, int prec, bool per_element, double *out,
@@ -1722,6 +2162,17 @@ cudaError_t launch_energy(const DevMesh &m, const double *u, int prec, bool per_
 {
 	if (m.E == 0)
 		return per_element ? cudaSuccess : cudaMemsetAsync(out, 0, sizeof(double), s);
+	if (m.mat != 0) // other materials: FP64 (the caller admits PREC_FP64 only)
+	{
+		switch (m.et)
+		{
+		case 1: gen_energy_mat<P1Tet>(m, u, per_element, out, sc, s); break;
+		case 2: gen_energy_mat<P2Tet>(m, u, per_element, out, sc, s); break;
+		case 3: gen_energy_mat<Q1Hex>(m, u, per_element, out, sc, s); break;
+		default: return cudaErrorInvalidValue;
+		}
+		return cudaGetLastError();
+	}
 	const bool f32 = prec != PREC_FP64;
 	switch (m.et)
 	{
@@ -1744,13 +2195,22 @@ cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double 
 {
 	if (m.E == 0) return cudaMemsetAsync(g, 0, sizeof(double) * 3 * (size_t)m.N, s);
 	const bool f32 = prec != PREC_FP64;
-	switch (m.et)
-	{
-	case 1: f32 ? gradient_t<P1Tet, float>(m, u, sc, s) : gradient_t<P1Tet, double>(m, u, sc, s); break;
-	case 2: f32 ? gradient_t<P2Tet, float>(m, u, sc, s) : gradient_t<P2Tet, double>(m, u, sc, s); break;
-	case 3: f32 ? gradient_t<Q1Hex, float>(m, u, sc, s) : gradient_t<Q1Hex, double>(m, u, sc, s); break;
-	default: return cudaErrorInvalidValue;
-	}
+	if (m.mat != 0) // other materials: FP64 (the caller admits PREC_FP64 only)
+		switch (m.et)
+		{
+		case 1: gen_gradient_mat<P1Tet>(m, u, sc, s); break;
+		case 2: gen_gradient_mat<P2Tet>(m, u, sc, s); break;
+		case 3: gen_gradient_mat<Q1Hex>(m, u, sc, s); break;
+		default: return cudaErrorInvalidValue;
+		}
+	else
+		switch (m.et)
+		{
+		case 1: f32 ? gradient_t<P1Tet, float>(m, u, sc, s) : gradient_t<P1Tet, double>(m, u, sc, s); break;
+		case 2: f32 ? gradient_t<P2Tet, float>(m, u, sc, s) : gradient_t<P2Tet, double>(m, u, sc, s); break;
+		case 3: f32 ? gradient_t<Q1Hex, float>(m, u, sc, s) : gradient_t<Q1Hex, double>(m, u, sc, s); break;
+		default: return cudaErrorInvalidValue;
+		}
 	constexpr int NTG = 128;
 	if (m.N > 0) k_vec_gather<NTG><<<blocks_for(m.N, NTG), NTG, 0, s>>>(m.N, m.inc_off, sc.vec_stage, g);
 	return cudaGetLastError();
