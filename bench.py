@@ -525,6 +525,19 @@ def run_suite(args):
         res["cg_reduced_psd"] = {"us": round(ms * 1e3, 2), "iterations": it.value,
                                  "us_per_iteration": round(per_it * 1e3, 2), "alg_GBps": round(gbs, 1),
                                  "frac_hbm": round(gbs / peak, 4), "n": nf, "nnz": rnnz}
+        # the other materials (FP64): energy, gradient and the Hessian
+        for mname, mid in (("iso_neohookean", 1), ("saint_venant", 2)):
+            check(L.pfg_set_material(h, mid), h, "pfg_set_material")
+            mops = {f"energy_{mname}": lambda: L.pfg_energy(h, U, 1, 0, O),
+                    f"gradient_{mname}": lambda: L.pfg_gradient(h, U, 1, 0, O),
+                    f"hessian_{mname}": lambda: L.pfg_hessian(h, U, 1, 0, 0, None)}
+            for op, fn in mops.items():
+                for _ in range(3):
+                    fn()
+                torch.cuda.synchronize()
+                ms = _events_ms_flushed(stream, fn, 10 if op.startswith("hessian") else 50, flush)
+                res[op] = {"us": round(ms * 1e3, 2), "elements_per_s": E / (ms * 1e-3)}
+        check(L.pfg_set_material(h, 0), h, "pfg_set_material")
         print(json.dumps({"suite": name, "workload": desc, "E": E, "N": mesh.n_nodes, "nnz": nnz, "ops": res}), flush=True)
         asm.close()
     return 0
