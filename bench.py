@@ -464,6 +464,8 @@ def run_suite(args):
         pd = torch.randn(mesh.n_dofs, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(7))
         out = torch.empty(max(mesh.n_dofs, 2 * E, 3 * mesh.n_geom_nodes), dtype=torch.float64, device="cuda")
         U, P, O = vp(ud.data_ptr()), vp(pd.data_ptr()), vp(out.data_ptr())
+        mvals = torch.empty(nnz, dtype=torch.float64, device="cuda")
+        MV = vp(mvals.data_ptr())
         ops = {
             "energy_fp64": lambda: L.pfg_energy(h, U, 1, 0, O),
             "energy_fp32": lambda: L.pfg_energy(h, U, 1, 1, O),
@@ -477,6 +479,7 @@ def run_suite(args):
             "material_vjp": lambda: L.pfg_material_vjp(h, U, P, 1, O),
             "shape_vjp_fp64": lambda: L.pfg_shape_vjp(h, U, P, 1, 0, O),
             "shape_vjp_fp32": lambda: L.pfg_shape_vjp(h, U, P, 1, 1, O),
+            "mass_matrix": lambda: L.pfg_mass_matrix(h, None, 1, MV),
         }
         # algorithmic bytes of the HBM-bound operations
         n, ng = mesh.conn.shape[1], mesh.gconn.shape[1]

@@ -222,6 +222,18 @@ int pfg_gradient_reduced(pfg_context *ctx, const double *u, int mem, int prec, d
 int pfg_reduced_to_full(pfg_context *ctx, const double *y, const double *x_bc, int mem, double *x);
 
 /* ---------------------------------------------------------------------------
+ * Mass matrix: MassMatrixAssembler's M = sum_e rho_e int phi_a phi_b I dV
+ * (LinearAssembler::assemble with the Mass term, assembler/Assembler.cpp:157-260,
+ * assembler/Mass.cpp:5-24), in the Hessian's CSC pattern (the linear assembler adds
+ * all nine entries of every node block: the off-diagonal ones are stored zeros).
+ * rho: per-element density (E doubles in `mem`) or NULL for 1.  values: nnz
+ * doubles in `mem` (required).  Quadrature of order 2p as the reference's mass
+ * quadrature (AssemblerUtils::quadrature_order("Mass")): the exact integral on the
+ * affine tets, the 2x2x2 Gauss rule on Q1.  FP64; the context's Hessian values are
+ * not touched. */
+int pfg_mass_matrix(pfg_context *ctx, const double *rho, int mem, double *values);
+
+/* ---------------------------------------------------------------------------
  * Linear solve on the device.  After every assembly NewtonMethod hands the
  * Hessian to its linear solver through polysolve's linear::Solver
  * (analyze_pattern, factorize, solve; called from solver/NLProblem.cpp:261-262,

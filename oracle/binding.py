@@ -39,6 +39,11 @@ def lib():
         L.orc_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_project_psd.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_material.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_basis_value.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.orc_basis_value.restype = ctypes.c_double
+        L.orc_mass.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_mass.restype = ctypes.c_longlong
+        L.orc_mass_copy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.orc_project_psd.argtypes = [_d, ctypes.c_int]
         L.orc_energy.restype = ctypes.c_double
         L.orc_energy.argtypes = [ctypes.c_void_p, _d]
@@ -104,6 +109,17 @@ class Oracle:
         if getattr(self, "h", None):
             lib().orc_destroy(self.h)
             self.h = None
+
+    def mass_matrix(self, rho=None):
+        """MassMatrixAssembler's CSC (outer, inner, values); rho per element or None for 1."""
+        r = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64)
+        nnz = lib().orc_mass(self.h, None if r is None else ctypes.c_void_p(r.ctypes.data))
+        outer = np.empty(self.n_dofs + 1, dtype=np.int32)
+        inner = np.empty(nnz, dtype=np.int32)
+        vals = np.empty(nnz)
+        lib().orc_mass_copy(self.h, ctypes.c_void_p(outer.ctypes.data), ctypes.c_void_p(inner.ctypes.data),
+                            ctypes.c_void_p(vals.ctypes.data))
+        return outer, inner, vals
 
     def set_threads(self, n: int):
         lib().orc_set_threads(self.h, int(n))

@@ -29,6 +29,7 @@
 // reproduced, so agreement with the reference is expected to ~1e-15 relative,
 // not bit-for-bit.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -915,6 +916,7 @@ struct Context
 	bool project_psd = false;  // NLAssembler::assemble_hessian(project_to_psd = true)
 	int material = 0;          // MAT_*: the assembler's formulation
 	CSC last;                  // last assembled Hessian
+	CSC mass;                  // last assembled mass matrix
 	std::string err;
 
 	void vals(int e, ElementValues &v) const
@@ -1288,6 +1290,131 @@ static void shape_vjp_impl(Context &c, const double *x, const double *adj, doubl
 			for (size_t i = 0; i < nout; ++i) term[i] += l[i];
 }
 
+// ---------------------------------------------------------------------------
+// MassMatrixAssembler: LinearAssembler::assemble with the Mass term
+// (assembler/Assembler.cpp:157-260, assembler/Mass.cpp:5-24).  For every local pair
+// j <= i the block rho int phi_i phi_j dV * I is added with all nine entries (zeros
+// included), and its transpose for j < i; triplets summed into CSC.  The mass
+// quadrature has order 2p (AssemblerUtils::quadrature_order, AssemblerUtils.cpp:
+// 201-211): Q1 uses the 2x2x2 Gauss rule as the reference does; on the affine tets any
+// rule exact to degree 2p gives the integral, here a conical-product Gauss rule
+// (Gauss-Legendre nodes by Newton iteration on the Legendre recurrence, collapsed
+// to the tetrahedron) instead of the reference's tabulated rules.
+// ---------------------------------------------------------------------------
+static void gauss_legendre01(int n, std::vector<double> &x, std::vector<double> &w)
+{
+	x.resize(n);
+	w.resize(n);
+	for (int i = 0; i < n; ++i)
+	{
+		double t = std::cos(3.14159265358979323846 * (i + 0.75) / (n + 0.5)), dp = 0;
+		for (int it = 0; it < 100; ++it)
+		{
+			double p0 = 1, p1 = t;
+			for (int k = 2; k <= n; ++k)
+			{
+				const double p2 = ((2 * k - 1) * t * p1 - (k - 1) * p0) / k;
+				p0 = p1;
+				p1 = p2;
+			}
+			const double pn = n == 1 ? t : p1, pm = n == 1 ? 1.0 : p0;
+			dp = n * (t * pn - pm) / (t * t - 1);
+			const double dt = pn / dp;
+			t -= dt;
+			if (std::fabs(dt) < 1e-16) break;
+		}
+		x[i] = 0.5 * (1 - t);
+		w[i] = 1.0 / ((1 - t * t) * dp * dp); // 2 / ((1 - t^2) P_n'(t)^2), halved for [0, 1]
+	}
+}
+
+// points (x, y, z) and weights on the unit tetrahedron exact to degree `deg`
+static void tet_rule(int deg, std::vector<std::array<double, 3>> &pts, std::vector<double> &wts)
+{
+	std::vector<double> xu, wu, xv, wv, xw, ww;
+	// an n-point Gauss-Legendre rule is exact to degree 2n - 1
+	gauss_legendre01(deg / 2 + 2, xu, wu); // with the weight (1-u)^2: degree deg + 2
+	gauss_legendre01(deg / 2 + 1, xv, wv); // with the weight (1-v): degree deg + 1
+	gauss_legendre01(deg / 2 + 1, xw, ww); // degree deg
+	pts.clear();
+	wts.clear();
+	for (size_t i = 0; i < xu.size(); ++i)
+		for (size_t j = 0; j < xv.size(); ++j)
+			for (size_t k = 0; k < xw.size(); ++k)
+			{
+				const double u = xu[i], v = xv[j], t = xw[k];
+				pts.push_back({u, v * (1 - u), t * (1 - u) * (1 - v)});
+				wts.push_back(wu[i] * wv[j] * ww[k] * (1 - u) * (1 - u) * (1 - v));
+			}
+}
+
+// FE basis values: P1 barycentric; P2 vertices lambda(2 lambda - 1), edges 4 lambda_i
+// lambda_j (01, 12, 20, 03, 13, 23); Q1 trilinear (corners 000 100 110 010 001 101 111 011)
+static double basis_value(int type, int i, double x, double y, double z)
+{
+	const double l[4] = {1 - x - y - z, x, y, z};
+	if (type == P1_TET) return l[i];
+	if (type == P2_TET)
+	{
+		static const int e[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+		return i < 4 ? l[i] * (2 * l[i] - 1) : 4 * l[e[i - 4][0]] * l[e[i - 4][1]];
+	}
+	static const int c[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+	return (c[i][0] ? x : 1 - x) * (c[i][1] ? y : 1 - y) * (c[i][2] ? z : 1 - z);
+}
+
+static void mass_impl(Context &c, const double *rho)
+{
+	const Tables &t = c.t;
+	std::vector<std::array<double, 3>> pts;
+	std::vector<double> wts;
+	if (t.type == Q1_HEX)
+		for (int q = 0; q < t.nq; ++q)
+		{
+			pts.push_back({t.qp[q][0], t.qp[q][1], t.qp[q][2]});
+			wts.push_back(t.qw[q]);
+		}
+	else
+		tet_rule(t.type == P1_TET ? 2 : 4, pts, wts);
+	void (*const ge)(int, double, double, double, double *) = t.type == Q1_HEX ? q1_grad : p1_grad;
+	std::vector<Triplet> trip;
+	for (int e = 0; e < c.E; ++e)
+	{
+		const double r = rho ? rho[e] : 1.0;
+		std::vector<double> m((size_t)t.n * t.n, 0.0);
+		for (size_t q = 0; q < pts.size(); ++q)
+		{
+			// geometry Jacobian at the point from the geometric basis
+			M3 J;
+			std::memset(&J, 0, sizeof(J));
+			for (int j = 0; j < t.ng; ++j)
+			{
+				double g[3];
+				ge(j, pts[q][0], pts[q][1], pts[q][2], g);
+				const double *node = c.X.data() + (size_t)c.gconn[(size_t)e * t.ng + j] * 3;
+				for (int rr = 0; rr < 3; ++rr)
+					for (int cc = 0; cc < 3; ++cc) J.a[rr][cc] += g[rr] * node[cc];
+			}
+			const double da = det3(J) * wts[q];
+			for (int a = 0; a < t.n; ++a)
+				for (int b = 0; b < t.n; ++b)
+					m[(size_t)a * t.n + b] += r * basis_value(t.type, a, pts[q][0], pts[q][1], pts[q][2]) *
+											  basis_value(t.type, b, pts[q][0], pts[q][1], pts[q][2]) * da;
+		}
+		for (int i = 0; i < t.n; ++i)
+			for (int j = 0; j <= i; ++j)
+				for (int n = 0; n < 3; ++n)
+					for (int mm = 0; mm < 3; ++mm)
+					{
+						const double v = n == mm ? m[(size_t)i * t.n + j] : 0.0;
+						const int gi = c.conn[(size_t)e * t.n + i] * 3 + mm, gj = c.conn[(size_t)e * t.n + j] * 3 + n;
+						trip.push_back({gi, gj, v});
+						if (j < i) trip.push_back({gj, gi, v});
+					}
+	}
+	c.mass = csc_from_triplets(c.N * 3, c.N * 3, trip);
+}
+
 template <typename Fn>
 static auto dispatch(int n, Fn &&fn)
 {
@@ -1339,6 +1466,22 @@ extern "C"
 	}
 
 	void orc_destroy(void *h) { delete static_cast<Context *>(h); }
+	// FE basis value (for the check of the values against the gradient tables)
+	double orc_basis_value(int type, int i, double x, double y, double z) { return basis_value(type, i, x, y, z); }
+	// MassMatrixAssembler (rho per element or NULL for 1); returns nnz, then orc_mass_copy
+	long long orc_mass(void *h, const double *rho)
+	{
+		Context &c = *static_cast<Context *>(h);
+		mass_impl(c, rho);
+		return (long long)c.mass.inner.size();
+	}
+	void orc_mass_copy(void *h, int *outer, int *inner, double *values)
+	{
+		const CSC &m = static_cast<Context *>(h)->mass;
+		std::copy(m.outer.begin(), m.outer.end(), outer);
+		std::copy(m.inner.begin(), m.inner.end(), inner);
+		std::copy(m.values.begin(), m.values.end(), values);
+	}
 
 	void orc_set_threads(void *h, int n) { static_cast<Context *>(h)->n_threads = std::max(1, n); }
 	// later orc_hessian calls project every element matrix onto the PSD cone

@@ -236,6 +236,25 @@ class NeoHookeanAssembler:
               "pfg_shape_vjp")
         return out
 
+    def assemble_mass_matrix_values(self, rho=None):
+        """MassMatrixAssembler's mass matrix values (nnz doubles, the Hessian pattern):
+        sum_e rho_e int phi_a phi_b I; rho per element, None for 1.  Host arrays in,
+        numpy out; a CUDA tensor rho gives a CUDA tensor."""
+        mem, ptrs, keep = self._prepare(rho) if rho is not None else self._prepare()
+        if rho is not None:
+            self._check_len(rho, self.n_elements, "rho")
+        out, optr = self._alloc(mem, self.hessian_nnz())
+        check(lib().pfg_mass_matrix(self._h, ptrs[0] if rho is not None else None, mem, optr), self._h,
+              "pfg_mass_matrix")
+        return out
+
+    def assemble_mass_matrix(self, rho=None):
+        """The mass matrix as scipy CSC (host)."""
+        import scipy.sparse as sp
+        vals = self.assemble_mass_matrix_values(None if rho is None else np.asarray(rho, dtype=np.float64))
+        outer, inner = self.hessian_pattern()
+        return sp.csc_matrix((vals, inner, outer), shape=(self.n_dofs, self.n_dofs))
+
     # -- material (AssemblerUtils::make_assembler's formulation name) ------------------
     MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2}
 

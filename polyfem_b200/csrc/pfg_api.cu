@@ -67,6 +67,8 @@ struct pfg_context
 	// the per-block partials and the scalars; a pinned host copy of the scalars
 	double *d_cg = nullptr;
 	size_t cg_n = 0;
+	// mass matrix (pfg_mass_matrix): values for host-mode calls, staged densities
+	double *d_mass = nullptr, *d_rho = nullptr;
 	double *h_cg_sc = nullptr;
 	std::string err;
 };
@@ -502,6 +504,8 @@ void free_all(pfg_context *c)
 		if (p) cudaFree(p);
 	if (c->d_cg) cudaFree(c->d_cg);
 	if (c->h_cg_sc) cudaFreeHost(c->h_cg_sc);
+	if (c->d_mass) cudaFree(c->d_mass);
+	if (c->d_rho) cudaFree(c->d_rho);
 }
 } // namespace
 
@@ -963,6 +967,33 @@ int pfg_gradient_reduced(pfg_context *c, const double *u, int mem, int prec, dou
 	double *dst = mem == PFG_MEM_DEVICE ? g_out : c->d_out;
 	PFG_CUDA(c, launch_gather_free(c->d_full_tmp, c->d_free, c->n_free, dst, c->stream));
 	if (mem == PFG_MEM_HOST) return finish_host(c, g_out, c->d_out, c->n_free);
+	return PFG_OK;
+}
+
+int pfg_mass_matrix(pfg_context *c, const double *rho, int mem, double *values)
+{
+	if (!c || !check_mem(mem) || !values) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	DeviceGuard g(c->device);
+	int st;
+	if (!c->has_pattern && (st = build_pattern(c))) return st;
+	if ((st = ensure_hess_stage(c, PFG_FP64))) return st;
+	const double *drho = rho;
+	if (rho && mem == PFG_MEM_HOST)
+	{
+		if (!c->d_rho) PFG_CUDA(c, cudaMalloc(&c->d_rho, sizeof(double) * std::max(c->m.E, 1)));
+		if (c->m.E) PFG_CUDA(c, cudaMemcpyAsync(c->d_rho, rho, sizeof(double) * c->m.E, cudaMemcpyHostToDevice, c->stream));
+		drho = c->d_rho;
+	}
+	DevPattern p = c->pat;
+	if (mem == PFG_MEM_HOST)
+	{
+		if (!c->d_mass) PFG_CUDA(c, cudaMalloc(&c->d_mass, sizeof(double) * std::max<long long>(c->pat.nnz, 1)));
+		p.values = c->d_mass;
+	}
+	else
+		p.values = values;
+	PFG_CUDA(c, launch_mass(c->m, p, drho, c->d_hess_stage[0], c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, values, c->d_mass, c->pat.nnz);
 	return PFG_OK;
 }
 

@@ -99,6 +99,9 @@ cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double 
 // project_psd != 0: every element matrix is projected onto the PSD cone (ipc::project_to_psd, CLAMP) before the scatter
 cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, int project_psd,
 						   void *stage, cudaStream_t s);
+// Mass matrix values (nnz of the Hessian pattern) into p.values; rho = per-element
+// density (device, E doubles) or NULL for 1; stage as for the FP64 Hessian
+cudaError_t launch_mass(const DevMesh &m, const DevPattern &p, const double *rho, void *stage, cudaStream_t s);
 // Dirichlet reduction helpers: dof maps of the free dofs (old_to_new[dof] = index
 // among the free dofs or -1, free[i] = dof of the i-th free dof)
 cudaError_t launch_gather_free(const double *full, const int *free, int n_free, double *out, cudaStream_t s);

@@ -1869,6 +1869,111 @@ static cudaError_t gen_hessian_mat(const DevMesh &m, const DevPattern &p, const 
 									   : gen_hessian<EL, MAT_SAINT_VENANT>(m, p, u, stage, project_psd, s);
 }
 
+// ---------------------------------------------------------------------------
+// Mass matrix (MassMatrixAssembler: LinearAssembler::assemble with the Mass term,
+// assembler/Assembler.cpp:157-260, assembler/Mass.cpp:5-24): node block (a, b) =
+// rho_e int phi_a phi_b dV * I.  The mass quadrature has order 2p
+// (AssemblerUtils::quadrature_order("Mass"), AssemblerUtils.cpp:201-211), exact for
+// phi_a phi_b on the affine tets, where the integral is taken in closed form from
+// int lambda^alpha = |T| 3! alpha! / (|alpha| + 3)!:
+//   P1: |T| (1 + delta_ab) / 20;   P2: |T| mass_p2(a, b) / 420
+// (P2 nodes: vertices lambda_i (2 lambda_i - 1), edges 4 lambda_i lambda_j in the order
+// 01, 12, 20, 03, 13, 23); Q1 uses its 2x2x2 Gauss points, as the reference does.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int mass_p2(int a, int b)
+{
+	constexpr int T[10][10] = {{6, 1, 1, 1, -4, -6, -4, -4, -6, -6},   {1, 6, 1, 1, -4, -4, -6, -6, -4, -6},
+							   {1, 1, 6, 1, -6, -4, -4, -6, -6, -4},   {1, 1, 1, 6, -6, -6, -6, -4, -4, -4},
+							   {-4, -4, -6, -6, 32, 16, 16, 16, 16, 8}, {-6, -4, -4, -6, 16, 32, 16, 8, 16, 16},
+							   {-4, -6, -4, -6, 16, 16, 32, 16, 8, 16}, {-4, -6, -6, -4, 16, 8, 16, 32, 16, 16},
+							   {-6, -4, -6, -4, 16, 16, 8, 16, 32, 16}, {-6, -6, -4, -4, 8, 16, 16, 16, 16, 32}};
+	return T[a][b];
+}
+
+// trilinear Q1 basis value of node i at (x, y, z): corners 000 100 110 010 001 101 111 011
+__host__ __device__ constexpr double q1_value(int i, double x, double y, double z)
+{
+	const int cx = (i == 1 || i == 2 || i == 5 || i == 6), cy = (i == 2 || i == 3 || i == 6 || i == 7), cz = i >= 4;
+	return (cx ? x : 1 - x) * (cy ? y : 1 - y) * (cz ? z : 1 - z);
+}
+
+template <class EL, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_mass_blocks(DevMesh m, const double *__restrict__ rho, double *__restrict__ stage)
+{
+	constexpr int N = EL::N, NQ = EL::NQ, NP = N * (N + 1) / 2, TP = tri_pad(EL::N);
+	__shared__ double wdet[WPB][NQ];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	for (int e = blockIdx.x * WPB + w; e < m.E; e += gridDim.x * WPB)
+	{
+		const double r_e = rho ? __ldg(rho + e) : 1.0;
+		if (lane < NQ)
+		{
+			double Xg[EL::NG][3], Jit[3][3], detJ;
+			load_geom<EL, double>(m, e, Xg);
+			geometry<EL, double>(lane, Xg, Jit, detJ);
+			wdet[w][lane] = detJ * qweight<EL>(lane);
+		}
+		__syncwarp();
+		double *tri = stage + (size_t)e * TP;
+		for (int p = lane; p < NP; p += 32)
+		{
+			int a = 0, b = p;
+			while (b >= N - a)
+			{
+				b -= N - a;
+				++a;
+			}
+			b += a;
+			double v;
+			if constexpr (EL::ET == 3)
+			{
+				v = 0.0;
+				for (int q = 0; q < NQ; ++q)
+					v += q1_value(a, qpoint<EL>(q, 0), qpoint<EL>(q, 1), qpoint<EL>(q, 2)) *
+						 q1_value(b, qpoint<EL>(q, 0), qpoint<EL>(q, 1), qpoint<EL>(q, 2)) * wdet[w][q];
+			}
+			else
+			{
+				// |T| = sum_q detJ w_q (the stiffness rule's weights sum to 1/6)
+				double vol = 0.0;
+				for (int q = 0; q < NQ; ++q) vol += wdet[w][q];
+				v = EL::ET == 1 ? vol * (a == b ? 2.0 : 1.0) / 20.0 : vol * mass_p2(a, b) / 420.0;
+			}
+			v *= r_e;
+			double *blk = tri + 9 * p;
+#pragma unroll
+			for (int k = 0; k < 9; ++k) blk[k] = (k == 0 || k == 4 || k == 8) ? v : 0.0;
+		}
+		__syncwarp();
+	}
+}
+
+cudaError_t launch_mass(const DevMesh &m, const DevPattern &p, const double *rho, void *stage_v, cudaStream_t s)
+{
+	if (p.nnz == 0) return cudaSuccess;
+	double *stage = static_cast<double *>(stage_v);
+	constexpr int WPB = 4, WARPS = 8;
+	const int nb = m.E > 0 ? std::min((m.E + WPB - 1) / WPB, 148 * 32) : 0;
+	const int ng = (m.N + WARPS - 1) / WARPS;
+	switch (m.et)
+	{
+	case 1:
+		if (nb) k_mass_blocks<P1Tet, WPB><<<nb, WPB * 32, 0, s>>>(m, rho, stage);
+		if (ng) k_hessian_reduce<P1Tet, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+		break;
+	case 2:
+		if (nb) k_mass_blocks<P2Tet, WPB><<<nb, WPB * 32, 0, s>>>(m, rho, stage);
+		if (ng) k_hessian_reduce<P2Tet, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+		break;
+	case 3:
+		if (nb) k_mass_blocks<Q1Hex, WPB><<<nb, WPB * 32, 0, s>>>(m, rho, stage);
+		if (ng) k_hessian_reduce<Q1Hex, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+		break;
+	default: return cudaErrorInvalidValue;
+	}
+	return cudaGetLastError();
+}
+
 template <class EL, class K, class T>
 static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const double *u, void *stage_v,
 									bool project_psd, cudaStream_t s)

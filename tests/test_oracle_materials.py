@@ -54,3 +54,51 @@ def test_material_known_answers(mat):
         lam_v, mu_v = np.asarray(lam), np.asarray(mu)
         vol = o.energy_per_element(us) / (lam_v / 2 * 9 * e * e + mu_v * 3 * e * e)
         assert np.isclose(vol.sum(), 1.0, rtol=1e-12)
+
+
+@pytest.mark.parametrize("et", [M.P1_TET, M.P2_TET, M.Q1_HEX], ids=["P1", "P2", "Q1"])
+def test_oracle_mass_matrix_known_answers(et):
+    """The oracle's mass matrix: symmetric, in the Hessian's pattern, total mass
+    rho * volume; its basis values are the antiderivatives of the gradient tables the
+    stiffness uses (same node order)."""
+    mesh, lam, mu, u, _ = make_case(et, 2, seed=13, jitter=0.1 if et != M.P1_TET else 0.0)
+    o = Oracle(mesh, lam, mu)
+    outer, inner, vals = o.mass_matrix(np.full(mesh.n_elements, 2.5))
+    Mm = sp.csc_matrix((vals, inner, outer), shape=(mesh.n_dofs, mesh.n_dofs))
+    assert abs(Mm - Mm.T).max() == 0.0
+    ho, hi, _ = o.hessian(u)
+    assert np.array_equal(ho, outer) and np.array_equal(hi, inner)
+    ex = np.zeros(mesh.n_dofs)
+    ex[1::3] = 1.0
+    assert abs(ex @ (Mm @ ex) - 2.5) <= 1e-12
+    from oracle.binding import lib as olib, tables
+    L = olib()
+    qp, qw, gr, _ = tables(et)
+    nq, n = gr.shape[0], gr.shape[1]
+    h = 1e-6
+    for q in range(nq):
+        for i in range(n):
+            for d in range(3):
+                xp, xm = qp[q].copy(), qp[q].copy()
+                xp[d] += h
+                xm[d] -= h
+                fd = (L.orc_basis_value(et, i, *xp) - L.orc_basis_value(et, i, *xm)) / (2 * h)
+                assert abs(fd - gr[q, i, d]) <= 1e-8
+    vals_q = [sum(L.orc_basis_value(et, i, *qp[q]) for i in range(n)) for q in range(nq)]
+    assert np.allclose(vals_q, 1.0, atol=1e-14)  # partition of unity
+
+
+def test_oracle_p1_mass_closed_form():
+    """On an affine P1 tet, int lambda_a lambda_b dV = |T| (1 + delta_ab) / 20: the
+    oracle's quadrature (its own conical-product Gauss rule) must reproduce it."""
+    mesh, lam, mu, _, _ = make_case(M.P1_TET, 1, seed=3)
+    o = Oracle(mesh, lam, mu)
+    rho = np.arange(1, mesh.n_elements + 1, dtype=float)
+    outer, inner, vals = o.mass_matrix(rho)
+    Mx = sp.csc_matrix((vals, inner, outer), shape=(mesh.n_dofs, mesh.n_dofs)).toarray()[0::3, 0::3]
+    ref = np.zeros((mesh.n_nodes, mesh.n_nodes))
+    for e in range(mesh.n_elements):
+        Xe = mesh.X[mesh.gconn[e]]
+        vol = np.linalg.det(np.stack([Xe[1] - Xe[0], Xe[2] - Xe[0], Xe[3] - Xe[0]], 1)) / 6
+        ref[np.ix_(mesh.conn[e], mesh.conn[e])] += rho[e] * vol * (np.ones((4, 4)) + np.eye(4)) / 20
+    assert np.abs(Mx - ref).max() <= 1e-14 * np.abs(ref).max()
