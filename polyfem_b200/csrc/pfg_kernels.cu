@@ -1876,19 +1876,15 @@ static cudaError_t gen_hessian_mat(const DevMesh &m, const DevPattern &p, const 
 // (AssemblerUtils::quadrature_order("Mass"), AssemblerUtils.cpp:201-211), exact for
 // phi_a phi_b on the affine tets, where the integral is taken in closed form from
 // int lambda^alpha = |T| 3! alpha! / (|alpha| + 3)!:
-//   P1: |T| (1 + delta_ab) / 20;   P2: |T| mass_p2(a, b) / 420
+//   P1: |T| (1 + delta_ab) / 20;   P2: |T| c_mass_p2[a][b] / 420
 // (P2 nodes: vertices lambda_i (2 lambda_i - 1), edges 4 lambda_i lambda_j in the order
 // 01, 12, 20, 03, 13, 23); Q1 uses its 2x2x2 Gauss points, as the reference does.
 // ---------------------------------------------------------------------------
-__host__ __device__ constexpr int mass_p2(int a, int b)
-{
-	constexpr int T[10][10] = {{6, 1, 1, 1, -4, -6, -4, -4, -6, -6},   {1, 6, 1, 1, -4, -4, -6, -6, -4, -6},
-							   {1, 1, 6, 1, -6, -4, -4, -6, -6, -4},   {1, 1, 1, 6, -6, -6, -6, -4, -4, -4},
-							   {-4, -4, -6, -6, 32, 16, 16, 16, 16, 8}, {-6, -4, -4, -6, 16, 32, 16, 8, 16, 16},
-							   {-4, -6, -4, -6, 16, 16, 32, 16, 8, 16}, {-4, -6, -6, -4, 16, 8, 16, 32, 16, 16},
-							   {-6, -4, -6, -4, 16, 16, 8, 16, 32, 16}, {-6, -6, -4, -4, 8, 16, 16, 16, 16, 32}};
-	return T[a][b];
-}
+__constant__ int c_mass_p2[10][10] = {{6, 1, 1, 1, -4, -6, -4, -4, -6, -6},   {1, 6, 1, 1, -4, -4, -6, -6, -4, -6},
+									   {1, 1, 6, 1, -6, -4, -4, -6, -6, -4},   {1, 1, 1, 6, -6, -6, -6, -4, -4, -4},
+									   {-4, -4, -6, -6, 32, 16, 16, 16, 16, 8}, {-6, -4, -4, -6, 16, 32, 16, 8, 16, 16},
+									   {-4, -6, -4, -6, 16, 16, 32, 16, 8, 16}, {-4, -6, -6, -4, 16, 8, 16, 32, 16, 16},
+									   {-6, -4, -6, -4, 16, 16, 8, 16, 32, 16}, {-6, -6, -4, -4, 8, 16, 16, 16, 16, 32}};
 
 // trilinear Q1 basis value of node i at (x, y, z): corners 000 100 110 010 001 101 111 011
 __host__ __device__ constexpr double q1_value(int i, double x, double y, double z)
@@ -1902,6 +1898,7 @@ __global__ void __launch_bounds__(WPB * 32) k_mass_blocks(DevMesh m, const doubl
 {
 	constexpr int N = EL::N, NQ = EL::NQ, NP = N * (N + 1) / 2, TP = tri_pad(EL::N);
 	__shared__ double wdet[WPB][NQ];
+	__shared__ double vpair[WPB][NP];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	for (int e = blockIdx.x * WPB + w; e < m.E; e += gridDim.x * WPB)
 	{
@@ -1914,7 +1911,7 @@ __global__ void __launch_bounds__(WPB * 32) k_mass_blocks(DevMesh m, const doubl
 			wdet[w][lane] = detJ * qweight<EL>(lane);
 		}
 		__syncwarp();
-		double *tri = stage + (size_t)e * TP;
+		// the pairs' values, then the whole triangle in consecutive stores
 		for (int p = lane; p < NP; p += 32)
 		{
 			int a = 0, b = p;
@@ -1937,12 +1934,16 @@ __global__ void __launch_bounds__(WPB * 32) k_mass_blocks(DevMesh m, const doubl
 				// |T| = sum_q detJ w_q (the stiffness rule's weights sum to 1/6)
 				double vol = 0.0;
 				for (int q = 0; q < NQ; ++q) vol += wdet[w][q];
-				v = EL::ET == 1 ? vol * (a == b ? 2.0 : 1.0) / 20.0 : vol * mass_p2(a, b) / 420.0;
+				v = EL::ET == 1 ? vol * (a == b ? 2.0 : 1.0) / 20.0 : vol * c_mass_p2[a][b] / 420.0;
 			}
-			v *= r_e;
-			double *blk = tri + 9 * p;
-#pragma unroll
-			for (int k = 0; k < 9; ++k) blk[k] = (k == 0 || k == 4 || k == 8) ? v : 0.0;
+			vpair[w][p] = v * r_e;
+		}
+		__syncwarp();
+		double *tri = stage + (size_t)e * TP;
+		for (int i = lane; i < TP; i += 32)
+		{
+			const int p = i / 9, k = i - 9 * p;
+			tri[i] = (p < NP && (k == 0 || k == 4 || k == 8)) ? vpair[w][p] : 0.0;
 		}
 		__syncwarp();
 	}
