@@ -1491,6 +1491,27 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__r
 // ---------------------------------------------------------------------------
 constexpr int MAT_ISO_NEOHOOKEAN = 1, MAT_SAINT_VENANT = 2;
 
+// node pairs (a <= b) in tri_index order for n = 4, 10, 8 nodes (P1, P2, Q1), in
+// constant memory: lanes at different pairs read them without a decoding loop
+struct PairTable
+{
+	unsigned char a[55], b[55];
+};
+constexpr PairTable make_pairs(int n)
+{
+	PairTable t{};
+	int p = 0;
+	for (int a = 0; a < n; ++a)
+		for (int b = a; b < n; ++b)
+		{
+			t.a[p] = (unsigned char)a;
+			t.b[p] = (unsigned char)b;
+			++p;
+		}
+	return t;
+}
+__constant__ PairTable c_pairs[3] = {make_pairs(4), make_pairs(10), make_pairs(8)};
+
 // Green strain from the displacement gradient G = F - I: E = (G^T G + G + G^T) / 2
 __device__ __forceinline__ void green_strain(const double F[3][3], double E[3][3])
 {
@@ -1695,12 +1716,21 @@ struct GenWarp
 	double U[N][3], X[NG][3];
 	double F[NQ][9], G[NQ][9], Jit[NQ][9];
 	double c[NQ][16]; // IsochoricNeoHookean: mu J^-2/3 da, |F|^2; SaintVenant: da, lambda, mu, S (row-major 9)
-	double nv[NQ][N][9];
+	alignas(16) double nv[NQ][N][10]; // g, f, d, pad: five 16-byte loads
 	alignas(16) double tri[TP]; // copied out as double2 (the members above can end on an odd double)
 };
 
+// 128-thread CTAs per SM the register budget allows: P2 five (at most 102 registers),
+// Q1 three (IsochoricNeoHookean) or four, P1 five or seven
+template <class EL, int MAT>
+constexpr int gen_blocks_min_ctas()
+{
+	return EL::ET == 2 ? 5 : EL::ET == 3 ? (MAT == MAT_ISO_NEOHOOKEAN ? 3 : 4) : (MAT == MAT_ISO_NEOHOOKEAN ? 5 : 7);
+}
+
 template <class EL, int MAT, int WPB>
-__global__ void __launch_bounds__(WPB * 32) k_gen_blocks(DevMesh m, const double *__restrict__ u, double *__restrict__ stage)
+__global__ void __launch_bounds__(WPB * 32, gen_blocks_min_ctas<EL, MAT>())
+	k_gen_blocks(DevMesh m, const double *__restrict__ u, double *__restrict__ stage)
 {
 	using W = GenWarp<EL>;
 	constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ, NP = N * (N + 1) / 2, TP = W::TP;
@@ -1779,21 +1809,26 @@ __global__ void __launch_bounds__(WPB * 32) k_gen_blocks(DevMesh m, const double
 				v[3 + r] = S.F[q][3 * r] * g[0] + S.F[q][3 * r + 1] * g[1] + S.F[q][3 * r + 2] * g[2];
 				v[6 + r] = MAT == MAT_ISO_NEOHOOKEAN ? S.G[q][3 * r] * g[0] + S.G[q][3 * r + 1] * g[1] + S.G[q][3 * r + 2] * g[2] : 0.0;
 			}
+			v[9] = 0.0;
 		}
 		__syncwarp();
 		for (int p = lane; p < NP; p += 32)
 		{
-			int a = 0, b = p;
-			while (b >= N - a)
-			{
-				b -= N - a;
-				++a;
-			}
-			b += a;
+			const int a = c_pairs[EL::ET - 1].a[p], b = c_pairs[EL::ET - 1].b[p];
 			double h[3][3] = {};
 			for (int q = 0; q < NQ; ++q)
 			{
-				const double *va = S.nv[q][a], *vb = S.nv[q][b];
+				double va[10], vb[10];
+				const double2 *pa = reinterpret_cast<const double2 *>(S.nv[q][a]), *pb = reinterpret_cast<const double2 *>(S.nv[q][b]);
+#pragma unroll
+				for (int t = 0; t < 5; ++t)
+				{
+					const double2 x = pa[t], y = pb[t];
+					va[2 * t] = x.x;
+					va[2 * t + 1] = x.y;
+					vb[2 * t] = y.x;
+					vb[2 * t + 1] = y.y;
+				}
 				const double gab = va[0] * vb[0] + va[1] * vb[1] + va[2] * vb[2];
 				if constexpr (MAT == MAT_ISO_NEOHOOKEAN)
 				{
