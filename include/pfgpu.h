@@ -172,19 +172,42 @@ int pfg_version(void);
  *                                 209-267) with the isotropic elasticity tensor of
  *                                 (lambda, mu) (ElasticityTensor::set_from_lambda_mu),
  *                                 psi = lambda/2 tr(E)^2 + mu |E|^2, E = (F^T F - I)/2;
- * both with the per-element (lambda, mu) of pfg_set_lame.  Energy, gradient and
- * Hessian (with project_psd and the Dirichlet reduction) then follow the chosen
- * material in PFG_FP64 (other precisions return PFG_ERR_UNSUPPORTED); the adjoint
- * terms (pfg_material_vjp, pfg_shape_vjp) remain NeoHookean-only.  Takes effect for
- * the calls that follow; the pattern is unchanged.
+ * both with the per-element (lambda, mu) of pfg_set_lame, and the formulations
+ * defined by their energy density alone, differentiated automatically as the
+ * reference does (GenericElastic AutodiffType::STRESS, GenericElastic.cpp:493-611):
+ *   PFG_MAT_LINEAR_ELASTICITY   : LinearElasticity (LinearElasticity.cpp:113-139),
+ *                                 psi = mu eps:eps + lambda/2 tr(eps)^2,
+ *                                 eps = (grad u + grad u^T)/2; (lambda, mu) of pfg_set_lame;
+ *   PFG_MAT_MOONEY_RIVLIN       : MooneyRivlinElasticity (MooneyRivlinElasticity.hpp:25-46),
+ *                                 parameters (c1, c2, k);
+ *   PFG_MAT_MOONEY_RIVLIN_3PARAM: MooneyRivlin3ParamElasticity
+ *                                 (MooneyRivlin3ParamElasticity.hpp:26-49), (c1, c2, c3, d1);
+ *   PFG_MAT_VOLUME_PENALTY      : VolumePenalty (VolumePenalty.hpp:20-34), (k).
+ * Energy, gradient and Hessian (with project_psd and the Dirichlet reduction) then
+ * follow the chosen material in PFG_FP64 (other precisions return
+ * PFG_ERR_UNSUPPORTED); the adjoint terms (pfg_material_vjp, pfg_shape_vjp) remain
+ * NeoHookean-only.  Takes effect for the calls that follow; the pattern is unchanged.
  * ------------------------------------------------------------------------- */
 enum pfg_material
 {
 	PFG_MAT_NEOHOOKEAN = 0,
 	PFG_MAT_ISOCHORIC_NEOHOOKEAN = 1,
-	PFG_MAT_SAINT_VENANT = 2
+	PFG_MAT_SAINT_VENANT = 2,
+	PFG_MAT_LINEAR_ELASTICITY = 3,
+	PFG_MAT_MOONEY_RIVLIN = 4,
+	PFG_MAT_MOONEY_RIVLIN_3PARAM = 5,
+	PFG_MAT_VOLUME_PENALTY = 6
 };
 int pfg_set_material(pfg_context *ctx, int material);
+
+/* Per-element parameters of PFG_MAT_MOONEY_RIVLIN (n_params 3: c1, c2, k),
+ * PFG_MAT_MOONEY_RIVLIN_3PARAM (4: c1, c2, c3, d1) and PFG_MAT_VOLUME_PENALTY
+ * (1: k): the reference's GenericMatParam values (MatParams.cpp), one per element,
+ * parameter-major: params[k * n_elements + e] is parameter k of element e.
+ * 1 <= n_params <= 4.  The energy, gradient and Hessian calls of these materials
+ * return PFG_ERR_STATE until parameters of the material's count are set; the
+ * parameters stay with the context when the material changes. */
+int pfg_set_material_params(pfg_context *ctx, const double *params, int n_params, int mem);
 
 /* ---------------------------------------------------------------------------
  * Dirichlet reduction.  When the only constraint form of the nonlinear problem

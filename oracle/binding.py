@@ -39,6 +39,7 @@ def lib():
         L.orc_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_project_psd.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_material.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_set_material_params.argtypes = [ctypes.c_void_p, _d, ctypes.c_int]
         L.orc_basis_value.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.orc_basis_value.restype = ctypes.c_double
         L.orc_mass.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
@@ -86,10 +87,15 @@ def _ip(a):
 class Oracle:
     """CPU restatement of NLAssembler + ElasticForm + ElasticForceDerivative."""
 
-    MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2}
+    MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2, "LinearElasticity": 3,
+                 "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6}
+    MATERIAL_PARAMS = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
+                       "VolumePenalty": ("k",)}
 
     def __init__(self, mesh, lam, mu, n_threads: int = 1, cache_size: int = 900000,
-                 fast_pattern: bool = False, material: str = "NeoHookean"):
+                 fast_pattern: bool = False, material: str = "NeoHookean", params=None):
+        """params: the GenericMatParam values of a parameterised material, a dict of
+        name -> scalar or per-element array (MATERIAL_PARAMS names)."""
         L = lib()
         self.mesh = mesh
         self._conn = np.ascontiguousarray(mesh.conn, dtype=np.int32)
@@ -103,6 +109,14 @@ class Oracle:
         if not self.h:
             raise RuntimeError("oracle creation failed")
         self.n_dofs = mesh.n_dofs
+        names = self.MATERIAL_PARAMS.get(material, ())
+        if set(params or {}) != set(names):
+            raise ValueError(f"{material} takes the parameters {list(names)}")
+        if names:
+            E = mesh.n_elements
+            self._mparams = np.ascontiguousarray(
+                np.stack([np.broadcast_to(np.asarray(params[n], dtype=np.float64), (E,)) for n in names]))
+            L.orc_set_material_params(self.h, _dp(self._mparams), len(names))
         L.orc_set_material(self.h, self.MATERIALS[material])
 
     def __del__(self):

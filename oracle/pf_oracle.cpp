@@ -475,12 +475,26 @@ static void element_hessian(const ElementValues &v, const double *x, double lamb
 //   MAT_SAINT_VENANT  : SaintVenantElasticity::compute_energy_aux (SaintVenantElasticity.cpp:
 //                       209-267) with the isotropic tensor of ElasticityTensor::set_from_lambda_mu
 //                       (MatParams.cpp:211-260); per element (lambda, mu) here.
+//   MAT_LINEAR_ELASTICITY: LinearElasticity::compute_energy_aux (LinearElasticity.cpp:113-139),
+//                       differentiated over the nodal values there (gradient_from_energy /
+//                       hessian_from_energy), over F here: the same derivatives, since F is
+//                       linear in the nodal values.
+//   MAT_MOONEY_RIVLIN : MooneyRivlinElasticity::elastic_energy (MooneyRivlinElasticity.hpp:25-46)
+//   MAT_MOONEY_RIVLIN_3PARAM: MooneyRivlin3ParamElasticity::elastic_energy
+//                       (MooneyRivlin3ParamElasticity.hpp:26-49)
+//   MAT_VOLUME_PENALTY: VolumePenalty::elastic_energy (VolumePenalty.hpp:20-34)
+// The material parameters of an element are prm[0..3]: (lambda, mu) for the first
+// four, the GenericMatParam values for the others (orc_set_material_params).
 // ---------------------------------------------------------------------------
 enum
 {
 	MAT_NEOHOOKEAN = 0,
 	MAT_ISO_NEOHOOKEAN = 1,
-	MAT_SAINT_VENANT = 2
+	MAT_SAINT_VENANT = 2,
+	MAT_LINEAR_ELASTICITY = 3,
+	MAT_MOONEY_RIVLIN = 4,
+	MAT_MOONEY_RIVLIN_3PARAM = 5,
+	MAT_VOLUME_PENALTY = 6
 };
 
 // value, gradient and Hessian with respect to the 9 entries F(r, c) (index 3r + c)
@@ -545,6 +559,8 @@ static D2 dpow(const D2 &a, double p)
 }
 static D2 operator/(const D2 &a, const D2 &b) { return a * dpow(b, -1.0); }
 static double dpow(double a, double p) { return std::pow(a, p); }
+static D2 dlog(const D2 &a) { return chain(a, std::log(a.v), 1.0 / a.v, -1.0 / (a.v * a.v)); }
+static double dlog(double a) { return std::log(a); }
 
 template <class S>
 static S det3s(const S (&F)[3][3])
@@ -598,10 +614,100 @@ static S psi_saint_venant(const S (&F)[3][3], double lambda, double mu)
 	return 0.5 * tr;
 }
 
+// LinearElasticity: strain = (G + G^T) / 2 of the displacement gradient G = F - I,
+// psi = mu tr(strain^T strain) + lambda/2 tr(strain)^2
 template <class S>
-static S psi_material(int mat, const S (&F)[3][3], double lambda, double mu)
+static S psi_linear_elasticity(const S (&F)[3][3], double lambda, double mu)
 {
-	return mat == MAT_ISO_NEOHOOKEAN ? psi_iso_neohookean(F, lambda, mu) : psi_saint_venant(F, lambda, mu);
+	S eps[3][3];
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c)
+			eps[r][c] = 0.5 * ((F[r][c] - S(r == c ? 1.0 : 0.0)) + (F[c][r] - S(r == c ? 1.0 : 0.0)));
+	S ee = S(0.0), tr = S(0.0);
+	for (int r = 0; r < 3; ++r)
+	{
+		tr = tr + eps[r][r];
+		for (int k = 0; k < 3; ++k) ee = ee + eps[k][r] * eps[k][r]; // (strain^T strain)(r, r)
+	}
+	return mu * ee + (lambda / 2.0) * (tr * tr);
+}
+
+// tr(A) and (tr(A)^2 - tr(A A)) / 2 of a 3 x 3 matrix (first_invariant and
+// second_invariant of utils/ElasticityUtils.hpp:140-149)
+template <class S>
+static void invariants12(const S (&A)[3][3], S &i1, S &i2)
+{
+	i1 = A[0][0] + A[1][1] + A[2][2];
+	S trAA = S(0.0);
+	for (int r = 0; r < 3; ++r)
+		for (int k = 0; k < 3; ++k) trAA = trAA + A[r][k] * A[k][r];
+	i2 = 0.5 * (i1 * i1 - trAA);
+}
+
+// MooneyRivlin: F~ = F / J^(1/3), C~ = F~ F~^T,
+// psi = c1 (tr C~ - 3) + c2 (I2(C~) - 3) + k/2 ln^2 J
+template <class S>
+static S psi_mooney_rivlin(const S (&F)[3][3], double c1, double c2, double k)
+{
+	const S J = det3s(F);
+	const S lj = dlog(J);
+	const S s = dpow(J, -1.0 / 3.0);
+	S Ft[3][3], Ct[3][3];
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c) Ft[r][c] = F[r][c] * s;
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c)
+		{
+			Ct[r][c] = S(0.0);
+			for (int m = 0; m < 3; ++m) Ct[r][c] = Ct[r][c] + Ft[r][m] * Ft[c][m];
+		}
+	S i1, i2;
+	invariants12(Ct, i1, i2);
+	return c1 * (i1 - S(3.0)) + c2 * (i2 - S(3.0)) + (k / 2.0) * (lj * lj);
+}
+
+// MooneyRivlin3Param: B = F F^T, I1~ = J^(-2/3) tr B - 3, I2~ = J^(-4/3) I2(B) - 3,
+// psi = c1 I1~ + (c2 + c3 I1~) I2~ + d1 (J - 1)^2
+template <class S>
+static S psi_mooney_rivlin_3param(const S (&F)[3][3], double c1, double c2, double c3, double d1)
+{
+	const S J = det3s(F);
+	S B[3][3];
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c)
+		{
+			B[r][c] = S(0.0);
+			for (int m = 0; m < 3; ++m) B[r][c] = B[r][c] + F[r][m] * F[c][m];
+		}
+	const S pj = dpow(J, -2.0 / 3.0);
+	S trB, i2;
+	invariants12(B, trB, i2);
+	const S I1t = pj * trB - S(3.0);
+	const S I2t = (pj * pj) * i2 - S(3.0);
+	const S jm = J - S(1.0);
+	return c1 * I1t + (S(c2) + c3 * I1t) * I2t + d1 * (jm * jm);
+}
+
+// VolumePenalty: psi = k/2 ((J^2 - 1)/2 - ln J)
+template <class S>
+static S psi_volume_penalty(const S (&F)[3][3], double k)
+{
+	const S J = det3s(F);
+	return (k / 2.0) * (0.5 * (J * J - S(1.0)) - dlog(J));
+}
+
+template <class S>
+static S psi_material(int mat, const S (&F)[3][3], const double *prm)
+{
+	switch (mat)
+	{
+	case MAT_ISO_NEOHOOKEAN: return psi_iso_neohookean(F, prm[0], prm[1]);
+	case MAT_SAINT_VENANT: return psi_saint_venant(F, prm[0], prm[1]);
+	case MAT_LINEAR_ELASTICITY: return psi_linear_elasticity(F, prm[0], prm[1]);
+	case MAT_MOONEY_RIVLIN: return psi_mooney_rivlin(F, prm[0], prm[1], prm[2]);
+	case MAT_MOONEY_RIVLIN_3PARAM: return psi_mooney_rivlin_3param(F, prm[0], prm[1], prm[2], prm[3]);
+	default: return psi_volume_penalty(F, prm[0]);
+	}
 }
 
 template <int N>
@@ -617,22 +723,22 @@ static void def_grad_plain(const ElementValues &v, const double *x, int p, doubl
 }
 
 template <int N>
-static double gen_element_energy(int mat, const ElementValues &v, const double *x, double lambda, double mu)
+static double gen_element_energy(int mat, const ElementValues &v, const double *x, const double *prm)
 {
 	double energy = 0;
 	for (int p = 0; p < v.nq; ++p)
 	{
 		double F[3][3];
 		def_grad_plain<N>(v, x, p, F);
-		energy += psi_material(mat, F, lambda, mu) * (v.det[p] * v.w[p]);
+		energy += psi_material(mat, F, prm) * (v.det[p] * v.w[p]);
 	}
 	return energy;
 }
 
 // gradient (grad != nullptr, 3N) and Hessian (hess != nullptr, 3N x 3N row-major)
 template <int N>
-static void gen_element_derivatives(int mat, const ElementValues &v, const double *x, double lambda, double mu,
-									double *grad, double *hess)
+static void gen_element_derivatives(int mat, const ElementValues &v, const double *x, const double *prm, double *grad,
+									double *hess)
 {
 	constexpr int ND = 3 * N;
 	if (grad) std::fill(grad, grad + ND, 0.0);
@@ -644,7 +750,7 @@ static void gen_element_derivatives(int mat, const ElementValues &v, const doubl
 		D2 F[3][3];
 		for (int r = 0; r < 3; ++r)
 			for (int c = 0; c < 3; ++c) F[r][c] = D2::var(Fv[r][c], 3 * r + c);
-		const D2 psi = psi_material(mat, F, lambda, mu);
+		const D2 psi = psi_material(mat, F, prm);
 		const double da = v.det[p] * v.w[p];
 		const double(*g)[3] = v.grad_t_m[p];
 		for (int i = 0; i < N; ++i)
@@ -915,6 +1021,18 @@ struct Context
 	bool fast_pattern = false; // build the first-call pattern by sorting instead of triplets
 	bool project_psd = false;  // NLAssembler::assemble_hessian(project_to_psd = true)
 	int material = 0;          // MAT_*: the assembler's formulation
+	std::vector<double> mparams; // per-element parameters of the GenericMatParam materials, parameter-major
+	int n_mparams = 0;
+
+	// the element's material parameters (lambda, mu) or GenericMatParam values
+	void params(int e, double (&prm)[4]) const
+	{
+		prm[0] = lambda[e];
+		prm[1] = mu[e];
+		prm[2] = prm[3] = 0.0;
+		if (material >= MAT_MOONEY_RIVLIN)
+			for (int k = 0; k < 4; ++k) prm[k] = k < n_mparams ? mparams[(size_t)k * E + e] : 0.0;
+	}
 	CSC last;                  // last assembled Hessian
 	CSC mass;                  // last assembled mass matrix
 	std::string err;
@@ -938,7 +1056,9 @@ static double energy_impl(Context &c, const double *x, double *per_elem)
 		for (int el = s; el < e; ++el)
 		{
 			c.vals(el, v);
-			const double val = c.material ? gen_element_energy<N>(c.material, v, x, c.lambda[el], c.mu[el])
+			double prm[4];
+			c.params(el, prm);
+			const double val = c.material ? gen_element_energy<N>(c.material, v, x, prm)
 										  : element_energy<N>(v, x, c.lambda[el], c.mu[el]);
 			if (per_elem) per_elem[el] = val;
 			acc += val;
@@ -963,7 +1083,11 @@ static void gradient_impl(Context &c, const double *x, double *g)
 		{
 			c.vals(el, v);
 			if (c.material)
-				gen_element_derivatives<N>(c.material, v, x, c.lambda[el], c.mu[el], val, nullptr);
+			{
+				double prm[4];
+				c.params(el, prm);
+				gen_element_derivatives<N>(c.material, v, x, prm, val, nullptr);
+			}
 			else
 				element_gradient<N>(v, x, c.lambda[el], c.mu[el], val);
 			for (int j = 0; j < N; ++j)
@@ -1130,7 +1254,11 @@ static void hessian_impl(Context &c, const double *x)
 		{
 			c.vals(el, v);
 			if (c.material)
-				gen_element_derivatives<N>(c.material, v, x, c.lambda[el], c.mu[el], nullptr, H.data());
+			{
+				double prm[4];
+				c.params(el, prm);
+				gen_element_derivatives<N>(c.material, v, x, prm, nullptr, H.data());
+			}
 			else
 				element_hessian<N>(v, x, c.lambda[el], c.mu[el], H.data());
 			if (c.project_psd) project_to_psd(H.data(), ND);
@@ -1488,6 +1616,13 @@ extern "C"
 	void orc_set_project_psd(void *h, int on) { static_cast<Context *>(h)->project_psd = on != 0; }
 	// later calls use another material of the GenericElastic family (MAT_*); 0 = NeoHookean
 	void orc_set_material(void *h, int mat) { static_cast<Context *>(h)->material = mat; }
+	// per-element GenericMatParam values, parameter-major (params[k * E + e]), 1..4 of them
+	void orc_set_material_params(void *h, const double *params, int n_params)
+	{
+		Context &c = *static_cast<Context *>(h);
+		c.n_mparams = n_params;
+		c.mparams.assign(params, params + (size_t)n_params * c.E);
+	}
 	// ipc::project_to_psd (CLAMP) of one row-major m x m symmetric matrix, in place
 	void orc_project_psd(double *H, int m) { project_to_psd(H, m); }
 
@@ -1565,8 +1700,10 @@ extern "C"
 			constexpr int n = decltype(N)::value;
 			if (c.material)
 			{
-				if (energy) *energy = gen_element_energy<n>(c.material, v, x, c.lambda[e], c.mu[e]);
-				if (grad || hess) gen_element_derivatives<n>(c.material, v, x, c.lambda[e], c.mu[e], grad, hess);
+				double prm[4];
+				c.params(e, prm);
+				if (energy) *energy = gen_element_energy<n>(c.material, v, x, prm);
+				if (grad || hess) gen_element_derivatives<n>(c.material, v, x, prm, grad, hess);
 				return 0;
 			}
 			if (energy) *energy = element_energy<n>(v, x, c.lambda[e], c.mu[e]);

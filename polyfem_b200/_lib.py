@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB_PATH = os.path.join(HERE, "libpfgpu.so")
-SOURCES = ["pfg_api.cu", "pfg_kernels.cu", "pfg_solve.cu", "pfg_noalloc.cu"]
+SOURCES = ["pfg_api.cu", "pfg_kernels.cu", "pfg_materials.cu", "pfg_solve.cu", "pfg_noalloc.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 PFG_OK = 0
@@ -114,6 +114,7 @@ SIGNATURES = {
     "pfg_gradient_reduced": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "pfg_reduced_to_full": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     "pfg_set_material": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pfg_set_material_params": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int]),
     "pfg_mass_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
     "pfg_cg_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),

@@ -256,16 +256,47 @@ class NeoHookeanAssembler:
         return sp.csc_matrix((vals, inner, outer), shape=(self.n_dofs, self.n_dofs))
 
     # -- material (AssemblerUtils::make_assembler's formulation name) ------------------
-    MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2}
+    MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2, "LinearElasticity": 3,
+                 "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6}
+    # the GenericMatParam names of the parameterised formulations, in pfg_set_material_params order
+    MATERIAL_PARAMS = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
+                       "VolumePenalty": ("k",)}
 
-    def set_material(self, formulation: str):
-        """Switch the elastic formulation: "NeoHookean" (default), "IsochoricNeoHookean"
-        or "SaintVenant" (isotropic, per-element lambda/mu).  The two others are
-        assembled in FP64; the adjoint terms stay NeoHookean-only."""
+    def set_material(self, formulation: str, **params):
+        """Switch the elastic formulation (AssemblerUtils::make_assembler's name).
+
+        "NeoHookean" (default), "IsochoricNeoHookean", "SaintVenant" (isotropic) and
+        "LinearElasticity" use the per-element lambda/mu.  "MooneyRivlin" (c1, c2, k),
+        "MooneyRivlin3Param" (c1, c2, c3, d1) and "VolumePenalty" (k) take their
+        parameters as keywords, each a scalar or one value per element (host arrays
+        or CUDA tensors).  Every formulation but NeoHookean is assembled in FP64; the
+        adjoint terms stay NeoHookean-only."""
         if formulation not in self.MATERIALS:
             raise ValueError(f"unknown formulation {formulation!r}; one of {sorted(self.MATERIALS)}")
+        names = self.MATERIAL_PARAMS.get(formulation, ())
+        if set(params) != set(names):
+            raise ValueError(f"{formulation} takes the parameters {list(names)}, got {sorted(params)}")
+        if names:
+            self.set_material_params(*(params[n] for n in names))
         check(lib().pfg_set_material(self._h, self.MATERIALS[formulation]), self._h, "pfg_set_material")
         self.material = formulation
+
+    def set_material_params(self, *params):
+        """Per-element parameters of the current or next parameterised formulation, in
+        MATERIAL_PARAMS order (pfg_set_material_params)."""
+        E = self.n_elements
+        if not 1 <= len(params) <= 4:
+            raise ValueError("1 to 4 parameters")
+        if any(_is_device(p) for p in params):
+            import torch
+            cols = [p if _is_device(p) else torch.tensor(p, dtype=torch.float64) for p in params]
+            packed = torch.stack([torch.broadcast_to(c.to(device=f"cuda:{self.device}", dtype=torch.float64), (E,))
+                                  for c in cols]).contiguous()
+        else:
+            packed = np.ascontiguousarray(
+                np.stack([np.broadcast_to(np.asarray(p, dtype=np.float64), (E,)) for p in params]))
+        mem, ptrs, keep = self._prepare(packed)
+        check(lib().pfg_set_material_params(self._h, ptrs[0], len(params), mem), self._h, "pfg_set_material_params")
 
     # -- Dirichlet reduction (NLProblem + BCLagrangianForm projection) ---------------
     def set_dirichlet(self, dofs):

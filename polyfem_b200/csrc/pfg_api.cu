@@ -69,6 +69,10 @@ struct pfg_context
 	size_t cg_n = 0;
 	// mass matrix (pfg_mass_matrix): values for host-mode calls, staged densities
 	double *d_mass = nullptr, *d_rho = nullptr;
+	// parameters of the automatically differentiated materials (pfg_set_material_params):
+	// one zero-padded double4 per element; n_mpar = the count last set (0: none)
+	double4 *d_mpar = nullptr;
+	int n_mpar = 0;
 	double *h_cg_sc = nullptr;
 	std::string err;
 };
@@ -137,11 +141,26 @@ void parallel_ranges(long long n, F &&f)
 }
 
 int check_mem(int mem) { return mem == PFG_MEM_HOST || mem == PFG_MEM_DEVICE; }
-// The other materials (pfg_set_material) are assembled in FP64 only.
+// number of pfg_set_material_params parameters a material takes (0: none, or Lame)
+int material_param_count(int mat)
+{
+	switch (mat)
+	{
+	case PFG_MAT_MOONEY_RIVLIN: return 3;
+	case PFG_MAT_MOONEY_RIVLIN_3PARAM: return 4;
+	case PFG_MAT_VOLUME_PENALTY: return 1;
+	default: return 0;
+	}
+}
+// The other materials (pfg_set_material) are assembled in FP64 only, and the
+// parameterised ones need their parameters.
 int check_material_prec(pfg_context *c, int prec)
 {
 	if (c->m.mat != PFG_MAT_NEOHOOKEAN && prec != PFG_FP64)
 		return fail(c, PFG_ERR_UNSUPPORTED, "only PFG_FP64 is implemented for materials other than NeoHookean");
+	const int np = material_param_count(c->m.mat);
+	if (np && c->m.E && c->n_mpar != np)
+		return fail(c, PFG_ERR_STATE, "the material's parameters are not set (pfg_set_material_params)");
 	return PFG_OK;
 }
 int check_prec(int prec) { return prec == PFG_FP64 || prec == PFG_FP32 || prec == PFG_SPLIT32; }
@@ -506,6 +525,7 @@ void free_all(pfg_context *c)
 	if (c->h_cg_sc) cudaFreeHost(c->h_cg_sc);
 	if (c->d_mass) cudaFree(c->d_mass);
 	if (c->d_rho) cudaFree(c->d_rho);
+	if (c->d_mpar) cudaFree(c->d_mpar);
 }
 } // namespace
 
@@ -678,9 +698,45 @@ int pfg_set_stream(pfg_context *c, void *stream)
 
 int pfg_set_material(pfg_context *c, int material)
 {
-	if (!c || (material != PFG_MAT_NEOHOOKEAN && material != PFG_MAT_ISOCHORIC_NEOHOOKEAN && material != PFG_MAT_SAINT_VENANT))
+	if (!c || material < PFG_MAT_NEOHOOKEAN || material > PFG_MAT_VOLUME_PENALTY)
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
 	c->m.mat = material;
+	return PFG_OK;
+}
+
+int pfg_set_material_params(pfg_context *c, const double *params, int n_params, int mem)
+{
+	if (!c || !check_mem(mem) || n_params < 1 || n_params > 4) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (c->m.E && !params) return fail(c, PFG_ERR_INVALID, "params NULL");
+	DeviceGuard g(c->device);
+	const size_t E = c->m.E;
+	if (E)
+	{
+		if (!c->d_mpar)
+		{
+			PFG_CUDA(c, cudaMalloc(&c->d_mpar, sizeof(double4) * E));
+			c->m.mpar = c->d_mpar;
+		}
+		if (mem == PFG_MEM_HOST)
+		{
+			std::vector<double4> pv(E, make_double4(0.0, 0.0, 0.0, 0.0));
+			for (size_t e = 0; e < E; ++e)
+			{
+				double *d = &pv[e].x;
+				for (int k = 0; k < n_params; ++k) d[k] = params[(size_t)k * E + e];
+			}
+			PFG_CUDA(c, cudaMemcpyAsync(c->d_mpar, pv.data(), sizeof(double4) * E, cudaMemcpyHostToDevice, c->stream));
+			PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+		}
+		else
+		{
+			PFG_CUDA(c, cudaMemsetAsync(c->d_mpar, 0, sizeof(double4) * E, c->stream));
+			for (int k = 0; k < n_params; ++k)
+				PFG_CUDA(c, cudaMemcpy2DAsync((char *)c->d_mpar + k * sizeof(double), sizeof(double4), params + (size_t)k * E,
+											  sizeof(double), sizeof(double), E, cudaMemcpyDeviceToDevice, c->stream));
+		}
+	}
+	c->n_mpar = n_params;
 	return PFG_OK;
 }
 

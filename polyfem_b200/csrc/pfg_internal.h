@@ -21,11 +21,13 @@ namespace pfg
 struct DevMesh
 {
 	int et = 0, E = 0, N = 0, Ng = 0;
-	int mat = 0; // 0 NeoHookean, 1 IsochoricNeoHookean, 2 SaintVenant (pfg_set_material)
+	int mat = 0; // pfg_material: 0 NeoHookean, 1 IsochoricNeoHookean, 2 SaintVenant, 3 LinearElasticity,
+	             // 4 MooneyRivlin, 5 MooneyRivlin3Param, 6 VolumePenalty (pfg_set_material)
 	const int *conn = nullptr;
 	const int *gconn = nullptr;
 	const double *X = nullptr;
 	const double2 *lame = nullptr;
+	const double4 *mpar = nullptr; // per-element parameters of materials 4..6 (pfg_set_material_params), zero-padded
 	const int *inc_off = nullptr;
 	const int *inc_eb = nullptr;
 	const int *eb_inc = nullptr; // [E*n] inverse of inc_eb: incidence index of (e, b)
@@ -107,6 +109,14 @@ cudaError_t launch_mass(const DevMesh &m, const DevPattern &p, const double *rho
 cudaError_t launch_gather_free(const double *full, const int *free, int n_free, double *out, cudaStream_t s);
 cudaError_t launch_reduced_to_full(const double *y, const double *x_bc, const int *old_to_new, int ndof, double *x,
 								   cudaStream_t s);
+// Materials from MAT_FIRST_AD on are differentiated automatically (pfg_materials.cu):
+// the energy, the element gradients into sc.vec_stage (one slot per incidence, as
+// the other gradient kernels), and the FP64 element block triangles into stage.
+constexpr int MAT_FIRST_AD = 3;
+cudaError_t launch_ad_energy(const DevMesh &m, const double *u, bool per_element, double *out, const Scratch &sc,
+							 cudaStream_t s);
+cudaError_t launch_ad_gradient_stage(const DevMesh &m, const double *u, const Scratch &sc, cudaStream_t s);
+cudaError_t launch_ad_blocks(const DevMesh &m, const double *u, double *stage, cudaStream_t s);
 cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double *adj, double *out, cudaStream_t s);
 cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out,
 							 const Scratch &sc, cudaStream_t s);

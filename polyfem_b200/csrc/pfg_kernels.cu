@@ -11,157 +11,13 @@
 // beta = (lambda ln J - mu)/J and eps(w)[m][n] = sum_p eps_mnp w_p.  This is
 // exactly B^T C B of the reference (d2J/dF_mk dF_nl = eps_mnp eps_klq F_pq),
 // evaluated without the zeros of B.
-#include "pfg_elem.cuh"
-#include "pfg_internal.h"
+#include "pfg_device.cuh"
 
 #include <cstdio>
 #include <cstdlib>
 
 namespace pfg
 {
-
-// ---------------------------------------------------------------------------
-// shared element helpers
-// ---------------------------------------------------------------------------
-template <class EL, class T>
-__device__ __forceinline__ void load_geom(const DevMesh &m, int e, T Xg[EL::NG][3])
-{
-#pragma unroll
-	for (int j = 0; j < EL::NG; ++j)
-	{
-		const int g = __ldg(m.gconn + (size_t)j * m.E + e);
-		const double *x = m.X + (size_t)g * 3;
-		Xg[j][0] = T(__ldg(x + 0));
-		Xg[j][1] = T(__ldg(x + 1));
-		Xg[j][2] = T(__ldg(x + 2));
-	}
-}
-
-template <class EL, class T>
-__device__ __forceinline__ void load_nodal(const DevMesh &m, int e, const double *__restrict__ f, T U[EL::N][3], int nodes[EL::N])
-{
-#pragma unroll
-	for (int a = 0; a < EL::N; ++a)
-	{
-		const int n = __ldg(m.conn + (size_t)a * m.E + e);
-		nodes[a] = n;
-		const double *p = f + (size_t)n * 3;
-		U[a][0] = T(__ldg(p + 0));
-		U[a][1] = T(__ldg(p + 1));
-		U[a][2] = T(__ldg(p + 2));
-	}
-}
-
-// Geometry at quadrature point q: J^-T and det J (ElementAssemblyValues.cpp:76-104).
-// The determinant is always FP64; J^-T is kept in T.
-template <class EL, class T>
-__device__ __forceinline__ void geometry(int q, const T Xg[EL::NG][3], T Jit[3][3], double &detJ)
-{
-	T Jac[3][3];
-	geom_jacobian<EL, T>(q, Xg, Jac);
-	if constexpr (sizeof(T) == 8)
-	{
-		detJ = det3(Jac);
-		inv_transpose3(Jac, T(detJ), Jit);
-	}
-	else
-	{
-		double Jd[3][3];
-#pragma unroll
-		for (int r = 0; r < 3; ++r)
-#pragma unroll
-			for (int c = 0; c < 3; ++c) Jd[r][c] = double(Jac[r][c]);
-		detJ = det3(Jd);
-		inv_transpose3(Jac, T(detJ), Jit);
-	}
-}
-
-// physical gradients gphi[a][c] = sum_r gref(q,a,r) Jit[r][c]  (grad_t_m)
-template <class EL, class T>
-__device__ __forceinline__ void phys_grads(int q, const T Jit[3][3], T gphi[EL::N][3])
-{
-#pragma unroll
-	for (int a = 0; a < EL::N; ++a)
-#pragma unroll
-		for (int c = 0; c < 3; ++c)
-		{
-			T s = T(0);
-#pragma unroll
-			for (int r = 0; r < 3; ++r)
-			{
-				const double gr = gref<EL>(q, a, r);
-				if (gr != 0.0) s += T(gr) * Jit[r][c];
-			}
-			gphi[a][c] = s;
-		}
-}
-
-// displacement gradient G[r][c] = sum_a U[a][r] gphi[a][c]
-template <class EL, class T>
-__device__ __forceinline__ void disp_grad(const T U[EL::N][3], const T gphi[EL::N][3], T G[3][3])
-{
-#pragma unroll
-	for (int r = 0; r < 3; ++r)
-#pragma unroll
-		for (int c = 0; c < 3; ++c)
-		{
-			T s = T(0);
-#pragma unroll
-			for (int a = 0; a < EL::N; ++a) s += U[a][r] * gphi[a][c];
-			G[r][c] = s;
-		}
-}
-
-// one 32-byte staging slot (one DRAM sector): (x, y, z, 0) in two 16-byte stores
-__device__ __forceinline__ void st_slot(double *p, double x, double y, double z)
-{
-	reinterpret_cast<double2 *>(p)[0] = make_double2(x, y);
-	reinterpret_cast<double2 *>(p)[1] = make_double2(z, 0.0);
-}
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-	return v;
-}
-
-// Deterministic two-level reduction: fixed tree inside each block, then the
-// last block to finish sums the per-block partials in block order.
-template <int NT>
-__device__ void reduce_to_result(double v, double *partials, double *result, unsigned int *ticket)
-{
-	__shared__ double s_w[NT / 32];
-	__shared__ bool s_last;
-	v = warp_sum(v);
-	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-	if (lane == 0) s_w[wid] = v;
-	__syncthreads();
-	if (threadIdx.x == 0)
-	{
-		double b = 0.0;
-		for (int i = 0; i < NT / 32; ++i) b += s_w[i];
-		partials[blockIdx.x] = b;
-		__threadfence();
-		const unsigned int t = atomicAdd(ticket, 1u);
-		s_last = (t == gridDim.x - 1);
-	}
-	__syncthreads();
-	if (!s_last) return;
-	__threadfence();
-	double acc = 0.0;
-	for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) acc += *((volatile double *)partials + i);
-	acc = warp_sum(acc);
-	if (lane == 0) s_w[wid] = acc;
-	__syncthreads();
-	if (threadIdx.x == 0)
-	{
-		double b = 0.0;
-		for (int i = 0; i < NT / 32; ++i) b += s_w[i];
-		*result = b;
-		*ticket = 0u;
-	}
-}
 
 // ---------------------------------------------------------------------------
 // energy (NLAssembler::assemble_energy / assemble_energy_per_element)
@@ -1493,23 +1349,6 @@ constexpr int MAT_ISO_NEOHOOKEAN = 1, MAT_SAINT_VENANT = 2;
 
 // node pairs (a <= b) in tri_index order for n = 4, 10, 8 nodes (P1, P2, Q1), in
 // constant memory: lanes at different pairs read them without a decoding loop
-struct PairTable
-{
-	unsigned char a[55], b[55];
-};
-constexpr PairTable make_pairs(int n)
-{
-	PairTable t{};
-	int p = 0;
-	for (int a = 0; a < n; ++a)
-		for (int b = a; b < n; ++b)
-		{
-			t.a[p] = (unsigned char)a;
-			t.b[p] = (unsigned char)b;
-			++p;
-		}
-	return t;
-}
 __constant__ PairTable c_pairs[3] = {make_pairs(4), make_pairs(10), make_pairs(8)};
 
 // Green strain from the displacement gradient G = F - I: E = (G^T G + G + G^T) / 2
@@ -1589,26 +1428,6 @@ __device__ __forceinline__ void mat_piola(const double F[3][3], double lambda, d
 	}
 }
 
-// F = I + (U^T gref_q) J^-T at quadrature point q
-template <class EL>
-__device__ __forceinline__ void gen_def_grad(int q, const double U[EL::N][3], const double Jit[3][3], double F[3][3])
-{
-	double A[3][3];
-#pragma unroll
-	for (int r = 0; r < 3; ++r)
-#pragma unroll
-		for (int c = 0; c < 3; ++c)
-		{
-			double s_ = 0.0;
-#pragma unroll
-			for (int a = 0; a < EL::N; ++a) s_ += U[a][r] * gref<EL>(q, a, c);
-			A[r][c] = s_;
-		}
-#pragma unroll
-	for (int r = 0; r < 3; ++r)
-#pragma unroll
-		for (int c = 0; c < 3; ++c) F[r][c] = A[r][0] * Jit[0][c] + A[r][1] * Jit[1][c] + A[r][2] * Jit[2][c] + (r == c);
-}
 
 template <class EL, int MAT>
 __device__ __forceinline__ double gen_element_energy(const DevMesh &m, const double *__restrict__ u, int e,
@@ -1870,11 +1689,31 @@ __global__ void __launch_bounds__(WPB * 32, gen_blocks_min_ctas<EL, MAT>())
 	}
 }
 
+// FP64 staged element triangles -> (PSD projection) -> CSC values: the tail of the
+// Hessian for every material other than NeoHookean
+template <class EL>
+static cudaError_t finish_fp64_hessian(const DevMesh &m, const DevPattern &p, double *stage, bool project_psd,
+									   cudaStream_t s)
+{
+	constexpr int WARPS = 8;
+	if (project_psd && m.E > 0)
+	{
+		constexpr int PW = 4;
+		const size_t bytes_p = PW * sizeof(PsdWarp<EL>);
+		cudaError_t e = cudaFuncSetAttribute(k_project_psd<EL, double, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
+		if (e != cudaSuccess) return e;
+		k_project_psd<EL, double, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
+	}
+	const int ng = (m.N + WARPS - 1) / WARPS;
+	if (ng > 0) k_hessian_reduce<EL, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+	return cudaGetLastError();
+}
+
 template <class EL, int MAT>
 static cudaError_t gen_hessian(const DevMesh &m, const DevPattern &p, const double *u, double *stage, bool project_psd,
 							   cudaStream_t s)
 {
-	constexpr int WPB = 4, WARPS = 8;
+	constexpr int WPB = 4;
 	const size_t bytes = WPB * sizeof(GenWarp<EL>);
 	cudaError_t e = cudaFuncSetAttribute(k_gen_blocks<EL, MAT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 	if (e != cudaSuccess) return e;
@@ -1883,17 +1722,7 @@ static cudaError_t gen_hessian(const DevMesh &m, const DevPattern &p, const doub
 		const int nb = std::min((m.E + WPB - 1) / WPB, 148 * 32);
 		k_gen_blocks<EL, MAT, WPB><<<nb, WPB * 32, bytes, s>>>(m, u, stage);
 	}
-	if (project_psd && m.E > 0)
-	{
-		constexpr int PW = 4;
-		const size_t bytes_p = PW * sizeof(PsdWarp<EL>);
-		e = cudaFuncSetAttribute(k_project_psd<EL, double, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
-		if (e != cudaSuccess) return e;
-		k_project_psd<EL, double, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
-	}
-	const int ng = (m.N + WARPS - 1) / WARPS;
-	if (ng > 0) k_hessian_reduce<EL, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
-	return cudaGetLastError();
+	return finish_fp64_hessian<EL>(m, p, stage, project_psd, s);
 }
 
 template <class EL>
@@ -2042,6 +1871,19 @@ cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *
 {
 	const bool psd = project_psd != 0;
 	if (p.nnz == 0) return cudaSuccess;
+	if (m.mat >= MAT_FIRST_AD) // automatically differentiated materials: FP64 blocks
+	{
+		double *st = static_cast<double *>(stage);
+		cudaError_t e = launch_ad_blocks(m, u, st, s);
+		if (e != cudaSuccess) return e;
+		switch (m.et)
+		{
+		case 1: return finish_fp64_hessian<P1Tet>(m, p, st, psd, s);
+		case 2: return finish_fp64_hessian<P2Tet>(m, p, st, psd, s);
+		case 3: return finish_fp64_hessian<Q1Hex>(m, p, st, psd, s);
+		}
+		return cudaErrorInvalidValue;
+	}
 	if (m.mat != 0) // other materials: FP64 blocks (the caller admits PREC_FP64 only)
 	{
 		double *st = static_cast<double *>(stage);
@@ -2303,6 +2145,7 @@ cudaError_t launch_energy(const DevMesh &m, const double *u, int prec, bool per_
 {
 	if (m.E == 0)
 		return per_element ? cudaSuccess : cudaMemsetAsync(out, 0, sizeof(double), s);
+	if (m.mat >= MAT_FIRST_AD) return launch_ad_energy(m, u, per_element, out, sc, s);
 	if (m.mat != 0) // other materials: FP64 (the caller admits PREC_FP64 only)
 	{
 		switch (m.et)
@@ -2336,7 +2179,12 @@ cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double 
 {
 	if (m.E == 0) return cudaMemsetAsync(g, 0, sizeof(double) * 3 * (size_t)m.N, s);
 	const bool f32 = prec != PREC_FP64;
-	if (m.mat != 0) // other materials: FP64 (the caller admits PREC_FP64 only)
+	if (m.mat >= MAT_FIRST_AD)
+	{
+		cudaError_t e = launch_ad_gradient_stage(m, u, sc, s);
+		if (e != cudaSuccess) return e;
+	}
+	else if (m.mat != 0) // other materials: FP64 (the caller admits PREC_FP64 only)
 		switch (m.et)
 		{
 		case 1: gen_gradient_mat<P1Tet>(m, u, sc, s); break;

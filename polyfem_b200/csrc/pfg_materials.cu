@@ -1,0 +1,465 @@
+// Energy-defined materials, differentiated automatically on the device (FP64).
+//
+// The reference assembles these formulations from an energy density psi(F) alone:
+// GenericElastic (assembler/GenericElastic.cpp:493-611, AutodiffType::STRESS) takes
+// dpsi/dF and d2psi/dF2 by forward-mode autodiff over the 9 entries of F and
+// contracts them with the physical basis gradients; LinearElasticity
+// (LinearElasticity.cpp:65-139) differentiates its strain energy over the nodal
+// values.  Both give, per quadrature point q and node pair (a, b),
+//   gradient  G[a][r]      = sum_q da_q sum_c P[r][c] g_a[c]
+//   Hessian   H_ab[r][k]   = sum_q da_q sum_{c,d} g_a[c] C[(r,c),(k,d)] g_b[d]
+// with P = dpsi/dF and C = d2psi/dF2.  Here psi is written once, generic in its
+// number type, and evaluated as
+//   double  : the energy;
+//   Dual1   : first-order dual numbers, one direction per evaluation: P[i];
+//   HDual   : hyper-dual numbers (Fike and Alonso, "The development of hyper-dual
+//             numbers for exact second-derivative calculations", AIAA 2011-886),
+//             two directions per evaluation: C[i][j] exactly, without truncation.
+// The 45 entries i <= j of C at every point are spread over the lanes of the
+// element's warp; the blocks are then written as the packed block triangle of the
+// element, which the PSD projection and the scatter of pfg_kernels.cu consume.
+//
+// Materials (per-element parameters, pfg_set_material_params / pfg_set_lame):
+//   3 LinearElasticity    (lambda, mu)   psi = mu eps:eps + lambda/2 tr(eps)^2,  eps = (G + G^T)/2, G = F - I
+//                                        (LinearElasticity.cpp:113-139)
+//   4 MooneyRivlin        (c1, c2, k)    psi = c1 (I1~ - 3) + c2 (I2~ - 3) + k/2 ln^2 J
+//                                        (MooneyRivlinElasticity.hpp:25-46)
+//   5 MooneyRivlin3Param  (c1, c2, c3, d1) psi = c1 I1~ + (c2 + c3 I1~) I2~ + d1 (J - 1)^2, with
+//                                        I1~ = J^-2/3 tr B - 3, I2~ = J^-4/3 (tr^2 B - tr B^2)/2 - 3
+//                                        (MooneyRivlin3ParamElasticity.hpp:26-49)
+//   6 VolumePenalty       (k)            psi = k/2 ((J^2 - 1)/2 - ln J)   (VolumePenalty.hpp:20-34)
+// with B = F F^T, I1~ = J^-2/3 tr B and I2~ = J^-4/3 (tr^2 B - tr B^2)/2 (the
+// invariants of F~ F~^T, F~ = J^-1/3 F).
+#include "pfg_device.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace pfg
+{
+
+constexpr int MAT_LINEAR_ELASTICITY = 3, MAT_MOONEY_RIVLIN = 4, MAT_MOONEY_RIVLIN_3PARAM = 5, MAT_VOLUME_PENALTY = 6;
+
+// ---------------------------------------------------------------------------
+// forward-mode numbers
+// ---------------------------------------------------------------------------
+struct Dual1
+{
+	double v, d; // value, derivative along one direction
+};
+struct HDual
+{
+	double v, a, b, ab; // value, d/de1, d/de2, d2/de1de2
+};
+
+__device__ __forceinline__ Dual1 operator+(Dual1 x, Dual1 y) { return {x.v + y.v, x.d + y.d}; }
+__device__ __forceinline__ Dual1 operator-(Dual1 x, Dual1 y) { return {x.v - y.v, x.d - y.d}; }
+__device__ __forceinline__ Dual1 operator*(Dual1 x, Dual1 y) { return {x.v * y.v, x.v * y.d + x.d * y.v}; }
+__device__ __forceinline__ Dual1 operator*(double s, Dual1 x) { return {s * x.v, s * x.d}; }
+__device__ __forceinline__ Dual1 operator-(Dual1 x, double s) { return {x.v - s, x.d}; }
+__device__ __forceinline__ Dual1 operator+(Dual1 x, double s) { return {x.v + s, x.d}; }
+// f(x) with f'(x.v) = f1
+__device__ __forceinline__ Dual1 chain(Dual1 x, double f0, double f1, double) { return {f0, f1 * x.d}; }
+
+__device__ __forceinline__ HDual operator+(HDual x, HDual y) { return {x.v + y.v, x.a + y.a, x.b + y.b, x.ab + y.ab}; }
+__device__ __forceinline__ HDual operator-(HDual x, HDual y) { return {x.v - y.v, x.a - y.a, x.b - y.b, x.ab - y.ab}; }
+__device__ __forceinline__ HDual operator*(HDual x, HDual y)
+{
+	return {x.v * y.v, x.v * y.a + x.a * y.v, x.v * y.b + x.b * y.v, x.v * y.ab + x.a * y.b + x.b * y.a + x.ab * y.v};
+}
+__device__ __forceinline__ HDual operator*(double s, HDual x) { return {s * x.v, s * x.a, s * x.b, s * x.ab}; }
+__device__ __forceinline__ HDual operator-(HDual x, double s) { return {x.v - s, x.a, x.b, x.ab}; }
+__device__ __forceinline__ HDual operator+(HDual x, double s) { return {x.v + s, x.a, x.b, x.ab}; }
+// f(x) with f'(x.v) = f1, f''(x.v) = f2
+__device__ __forceinline__ HDual chain(HDual x, double f0, double f1, double f2)
+{
+	return {f0, f1 * x.a, f1 * x.b, f1 * x.ab + f2 * x.a * x.b};
+}
+
+__device__ __forceinline__ double ad_log(double x) { return log(x); }
+__device__ __forceinline__ double ad_pow(double x, double p) { return pow(x, p); }
+template <class S>
+__device__ __forceinline__ S ad_log(S x)
+{
+	const double r = 1.0 / x.v;
+	return chain(x, log(x.v), r, -r * r);
+}
+// x^p: f' = p x^(p-1) = p f / x, f'' = (p - 1) f' / x
+template <class S>
+__device__ __forceinline__ S ad_pow(S x, double p)
+{
+	const double f = pow(x.v, p), r = 1.0 / x.v, f1 = p * f * r;
+	return chain(x, f, f1, (p - 1.0) * f1 * r);
+}
+
+template <class S>
+__device__ __forceinline__ S sq(S x) { return x * x; }
+
+// ---------------------------------------------------------------------------
+// energy densities, generic in the number type
+// ---------------------------------------------------------------------------
+template <int MAT, class S>
+__device__ __forceinline__ S ad_psi(const S F[3][3], const double4 &p)
+{
+	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
+	{
+		// eps:eps = sum_r G_rr^2 + 1/2 sum_{r<c} (G_rc + G_cr)^2
+		const S g0 = F[0][0] - 1.0, g1 = F[1][1] - 1.0, g2 = F[2][2] - 1.0;
+		const S tr = g0 + g1 + g2;
+		const S ee = sq(g0) + sq(g1) + sq(g2) + 0.5 * (sq(F[0][1] + F[1][0]) + sq(F[0][2] + F[2][0]) + sq(F[1][2] + F[2][1]));
+		return p.y * ee + (0.5 * p.x) * sq(tr);
+	}
+	else
+	{
+		const S J = det3(F);
+		if constexpr (MAT == MAT_VOLUME_PENALTY)
+			return (0.5 * p.x) * (0.5 * (sq(J) - 1.0) - ad_log(J));
+		else
+		{
+			S B[3][3]; // B = F F^T (symmetric)
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = r; c < 3; ++c) B[r][c] = F[r][0] * F[c][0] + F[r][1] * F[c][1] + F[r][2] * F[c][2];
+			const S trB = B[0][0] + B[1][1] + B[2][2];
+			const S trB2 = sq(B[0][0]) + sq(B[1][1]) + sq(B[2][2]) + 2.0 * (sq(B[0][1]) + sq(B[0][2]) + sq(B[1][2]));
+			const S i2 = 0.5 * (sq(trB) - trB2);
+			const S j23 = ad_pow(J, -2.0 / 3.0);
+			if constexpr (MAT == MAT_MOONEY_RIVLIN)
+			{
+				const S lj = ad_log(J);
+				return p.x * (j23 * trB - 3.0) + p.y * (sq(j23) * i2 - 3.0) + (0.5 * p.z) * sq(lj);
+			}
+			else // MAT_MOONEY_RIVLIN_3PARAM
+			{
+				const S I1t = j23 * trB - 3.0, I2t = sq(j23) * i2 - 3.0, jm1 = J - 1.0;
+				return p.x * I1t + (p.z * I1t + p.y) * I2t + p.w * sq(jm1);
+			}
+		}
+	}
+}
+
+template <int MAT>
+__device__ __forceinline__ double4 ad_params(const DevMesh &m, int e)
+{
+	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
+	{
+		const double2 lm = __ldg(m.lame + e);
+		return make_double4(lm.x, lm.y, 0.0, 0.0);
+	}
+	else
+	{
+		const double2 *q = reinterpret_cast<const double2 *>(m.mpar + e);
+		const double2 x = __ldg(q), y = __ldg(q + 1);
+		return make_double4(x.x, x.y, y.x, y.y);
+	}
+}
+
+// P[i] = dpsi/dF_i (i = 3r + c), one dual evaluation per entry
+template <int MAT>
+__device__ __forceinline__ void ad_piola(const double F[3][3], const double4 &p, double P[9])
+{
+#pragma unroll 1
+	for (int i = 0; i < 9; ++i)
+	{
+		Dual1 Fd[3][3];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) Fd[r][c] = {F[r][c], 3 * r + c == i ? 1.0 : 0.0};
+		P[i] = ad_psi<MAT, Dual1>(Fd, p).d;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// energy and gradient: thread per element
+// ---------------------------------------------------------------------------
+template <class EL, int MAT>
+__device__ __forceinline__ double ad_element_energy(const DevMesh &m, const double *__restrict__ u, int e,
+													unsigned long long *inverted)
+{
+	double Xg[EL::NG][3], U[EL::N][3];
+	int nodes[EL::N];
+	load_geom<EL, double>(m, e, Xg);
+	load_nodal<EL, double>(m, e, u, U, nodes);
+	const double4 prm = ad_params<MAT>(m, e);
+	double en = 0.0;
+	bool bad = false;
+#pragma unroll
+	for (int q = 0; q < EL::NQ; ++q)
+	{
+		double Jit[3][3], detJ, F[3][3];
+		geometry<EL, double>(q, Xg, Jit, detJ);
+		gen_def_grad<EL>(q, U, Jit, F);
+		bad |= !(det3(F) > 0.0);
+		en += ad_psi<MAT, double>(F, prm) * (detJ * qweight<EL>(q));
+	}
+	if (bad) atomicAdd(inverted, 1ull);
+	return en;
+}
+
+template <class EL, int MAT, int NT>
+__global__ void __launch_bounds__(NT) k_ad_energy(DevMesh m, const double *__restrict__ u, double *__restrict__ partials,
+												  double *__restrict__ result, unsigned int *ticket,
+												  unsigned long long *inverted)
+{
+	const int e = blockIdx.x * NT + threadIdx.x;
+	double en = 0.0;
+	if (e < m.E) en = ad_element_energy<EL, MAT>(m, u, e, inverted);
+	reduce_to_result<NT>(en, partials, result, ticket);
+}
+
+template <class EL, int MAT, int NT>
+__global__ void __launch_bounds__(NT) k_ad_energy_per_element(DevMesh m, const double *__restrict__ u,
+															  double *__restrict__ out, unsigned long long *inverted)
+{
+	const int e = blockIdx.x * NT + threadIdx.x;
+	if (e < m.E) out[e] = ad_element_energy<EL, MAT>(m, u, e, inverted);
+}
+
+// element gradient G[a][d] = sum_q da sum_c P[d][c] g_a[c], g_a = J^-T gref_a, one
+// slot per incidence as the other gradient kernels stage it
+template <class EL, int MAT, int NT>
+__global__ void __launch_bounds__(NT) k_ad_gradient(DevMesh m, const double *__restrict__ u, double *__restrict__ stage,
+													unsigned long long *inverted)
+{
+	const int e = blockIdx.x * NT + threadIdx.x;
+	if (e >= m.E) return;
+	double Xg[EL::NG][3], U[EL::N][3], Gacc[EL::N][3];
+	int nodes[EL::N];
+	load_geom<EL, double>(m, e, Xg);
+	load_nodal<EL, double>(m, e, u, U, nodes);
+	const double4 prm = ad_params<MAT>(m, e);
+#pragma unroll
+	for (int a = 0; a < EL::N; ++a) Gacc[a][0] = Gacc[a][1] = Gacc[a][2] = 0.0;
+	bool bad = false;
+#pragma unroll 1
+	for (int q = 0; q < EL::NQ; ++q)
+	{
+		double Jit[3][3], detJ, F[3][3], P[9];
+		geometry<EL, double>(q, Xg, Jit, detJ);
+		gen_def_grad<EL>(q, U, Jit, F);
+		bad |= !(det3(F) > 0.0);
+		ad_piola<MAT>(F, prm, P);
+		const double da = detJ * qweight<EL>(q);
+		double Q[3][3]; // da P J^-1 = da P Jit^T: G[a][d] = sum_r gref(q, a, r) Q[d][r]
+#pragma unroll
+		for (int d = 0; d < 3; ++d)
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+				Q[d][r] = da * (P[3 * d] * Jit[r][0] + P[3 * d + 1] * Jit[r][1] + P[3 * d + 2] * Jit[r][2]);
+#pragma unroll
+		for (int a = 0; a < EL::N; ++a)
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+			{
+				const double gr = gref<EL>(q, a, r);
+				if (gr != 0.0)
+				{
+#pragma unroll
+					for (int d = 0; d < 3; ++d) Gacc[a][d] += gr * Q[d][r];
+				}
+			}
+	}
+	if (bad) atomicAdd(inverted, 1ull);
+#pragma unroll
+	for (int a = 0; a < EL::N; ++a)
+	{
+		const int k = __ldg(m.eb_inc + (size_t)e * EL::N + a);
+		st_slot(stage + (size_t)k * 4, Gacc[a][0], Gacc[a][1], Gacc[a][2]);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// element blocks: one warp per element
+// ---------------------------------------------------------------------------
+// (i, j), i <= j, of the 9 x 9 table C in tri_index(9, i, j) order; and the node
+// pairs of the element block triangle (P1, P2, Q1)
+__constant__ PairTable c_ad_c9 = make_pairs(9);
+__constant__ PairTable c_ad_pairs[3] = {make_pairs(4), make_pairs(10), make_pairs(8)};
+
+template <class EL>
+struct AdWarp
+{
+	static constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ, TP = tri_pad(EL::N);
+	double U[N][3], X[NG][3];
+	double F[NQ][9], Jit[NQ][9], da[NQ];
+	double C[NQ][45];               // da d2psi/dF2 at point q, entry (i <= j) at tri_index(9, i, j)
+	alignas(16) double g[NQ][N][4]; // physical basis gradients (x, y, z, 0): two 16-byte loads
+	alignas(16) double tri[TP];     // the element's packed block triangle, copied out as double2
+};
+
+__host__ __device__ constexpr int c9(int i, int j) { return i <= j ? tri_index(9, i, j) : tri_index(9, j, i); }
+
+template <class EL, int MAT, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double *__restrict__ u, double *__restrict__ stage)
+{
+	using W = AdWarp<EL>;
+	constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ, NP = N * (N + 1) / 2, TP = W::TP;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	W &S = reinterpret_cast<W *>(smem_raw)[threadIdx.x >> 5];
+	const int lane = threadIdx.x & 31;
+	for (int e = blockIdx.x * WPB + (threadIdx.x >> 5); e < m.E; e += gridDim.x * WPB)
+	{
+		for (int i = lane; i < N * 3; i += 32)
+			S.U[i / 3][i % 3] = __ldg(u + (size_t)__ldg(m.conn + (size_t)(i / 3) * m.E + e) * 3 + i % 3);
+		for (int i = lane; i < NG * 3; i += 32)
+			S.X[i / 3][i % 3] = __ldg(m.X + (size_t)__ldg(m.gconn + (size_t)(i / 3) * m.E + e) * 3 + i % 3);
+		__syncwarp();
+		if (lane < NQ)
+		{
+			const int q = lane;
+			double Jit[3][3], detJ, F[3][3];
+			geometry<EL, double>(q, S.X, Jit, detJ);
+			gen_def_grad<EL>(q, S.U, Jit, F);
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+				{
+					S.F[q][3 * r + c] = F[r][c];
+					S.Jit[q][3 * r + c] = Jit[r][c];
+				}
+			S.da[q] = detJ * qweight<EL>(q);
+		}
+		__syncwarp();
+		const double4 prm = ad_params<MAT>(m, e);
+		// lanes over (point, node): g = J^-T gref
+		for (int t = lane; t < NQ * N; t += 32)
+		{
+			const int q = t / N, a = t - q * N;
+			double *g = S.g[q][a];
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+				g[c] = gref<EL>(q, a, 0) * S.Jit[q][c] + gref<EL>(q, a, 1) * S.Jit[q][3 + c] + gref<EL>(q, a, 2) * S.Jit[q][6 + c];
+			g[3] = 0.0;
+		}
+		// lanes over (point, entry i <= j of C): one hyper-dual evaluation each
+		for (int t = lane; t < NQ * 45; t += 32)
+		{
+			const int q = t / 45, k = t - q * 45;
+			const int i = c_ad_c9.a[k], j = c_ad_c9.b[k];
+			HDual Fh[3][3];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+				{
+					const int x = 3 * r + c;
+					Fh[r][c] = {S.F[q][x], x == i ? 1.0 : 0.0, x == j ? 1.0 : 0.0, 0.0};
+				}
+			S.C[q][k] = S.da[q] * ad_psi<MAT, HDual>(Fh, prm).ab;
+		}
+		__syncwarp();
+		// lanes over node pairs (a <= b): H_ab[r][k] = sum_q sum_{c,d} g_a[c] C[(r,c),(k,d)] g_b[d]
+		for (int p = lane; p < NP; p += 32)
+		{
+			const int a = c_ad_pairs[EL::ET - 1].a[p], b = c_ad_pairs[EL::ET - 1].b[p];
+			double h[3][3] = {};
+			for (int q = 0; q < NQ; ++q)
+			{
+				const double2 a01 = reinterpret_cast<const double2 *>(S.g[q][a])[0], a2 = reinterpret_cast<const double2 *>(S.g[q][a])[1];
+				const double2 b01 = reinterpret_cast<const double2 *>(S.g[q][b])[0], b2 = reinterpret_cast<const double2 *>(S.g[q][b])[1];
+				const double ga[3] = {a01.x, a01.y, a2.x}, gb[3] = {b01.x, b01.y, b2.x};
+				const double *Cq = S.C[q];
+#pragma unroll
+				for (int r = 0; r < 3; ++r)
+#pragma unroll
+					for (int k = 0; k < 3; ++k)
+					{
+						double s_ = 0.0;
+#pragma unroll
+						for (int c = 0; c < 3; ++c)
+						{
+							const double w = Cq[c9(3 * r + c, 3 * k)] * gb[0] + Cq[c9(3 * r + c, 3 * k + 1)] * gb[1] +
+											 Cq[c9(3 * r + c, 3 * k + 2)] * gb[2];
+							s_ += ga[c] * w;
+						}
+						h[r][k] += s_;
+					}
+			}
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int k = 0; k < 3; ++k) S.tri[9 * p + 3 * k + r] = h[r][k];
+		}
+		__syncwarp();
+		double2 *dst = reinterpret_cast<double2 *>(stage + (size_t)e * TP);
+		const double2 *src = reinterpret_cast<const double2 *>(S.tri);
+		for (int i = lane; i < TP / 2; i += 32) dst[i] = src[i];
+		__syncwarp();
+	}
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static inline int ad_blocks_for(int n, int nt) { return (n + nt - 1) / nt; }
+
+// f(element type, material) for the context's element type and material
+template <class Fn>
+static cudaError_t with_ad_material(const DevMesh &m, Fn &&f)
+{
+	auto by_mat = [&](auto el) -> cudaError_t {
+		using EL = decltype(el);
+		switch (m.mat)
+		{
+		case MAT_LINEAR_ELASTICITY: f(EL{}, std::integral_constant<int, MAT_LINEAR_ELASTICITY>{}); break;
+		case MAT_MOONEY_RIVLIN: f(EL{}, std::integral_constant<int, MAT_MOONEY_RIVLIN>{}); break;
+		case MAT_MOONEY_RIVLIN_3PARAM: f(EL{}, std::integral_constant<int, MAT_MOONEY_RIVLIN_3PARAM>{}); break;
+		case MAT_VOLUME_PENALTY: f(EL{}, std::integral_constant<int, MAT_VOLUME_PENALTY>{}); break;
+		default: return cudaErrorInvalidValue;
+		}
+		return cudaGetLastError();
+	};
+	switch (m.et)
+	{
+	case 1: return by_mat(P1Tet{});
+	case 2: return by_mat(P2Tet{});
+	case 3: return by_mat(Q1Hex{});
+	}
+	return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_ad_energy(const DevMesh &m, const double *u, bool per_element, double *out, const Scratch &sc,
+							 cudaStream_t s)
+{
+	if (m.E == 0) return per_element ? cudaSuccess : cudaMemsetAsync(out, 0, sizeof(double), s);
+	return with_ad_material(m, [&](auto el, auto mat) {
+		using EL = decltype(el);
+		constexpr int MAT = decltype(mat)::value, NT = 256;
+		const int nb = ad_blocks_for(m.E, NT);
+		if (per_element)
+			k_ad_energy_per_element<EL, MAT, NT><<<nb, NT, 0, s>>>(m, u, out, sc.inverted);
+		else
+			k_ad_energy<EL, MAT, NT><<<nb, NT, 0, s>>>(m, u, sc.partials, out, sc.ticket, sc.inverted);
+	});
+}
+
+cudaError_t launch_ad_gradient_stage(const DevMesh &m, const double *u, const Scratch &sc, cudaStream_t s)
+{
+	if (m.E == 0) return cudaSuccess;
+	return with_ad_material(m, [&](auto el, auto mat) {
+		using EL = decltype(el);
+		constexpr int MAT = decltype(mat)::value, NT = 128;
+		k_ad_gradient<EL, MAT, NT><<<ad_blocks_for(m.E, NT), NT, 0, s>>>(m, u, sc.vec_stage, sc.inverted);
+	});
+}
+
+cudaError_t launch_ad_blocks(const DevMesh &m, const double *u, double *stage, cudaStream_t s)
+{
+	if (m.E == 0) return cudaSuccess;
+	cudaError_t err = cudaSuccess;
+	cudaError_t st = with_ad_material(m, [&](auto el, auto mat) {
+		using EL = decltype(el);
+		constexpr int MAT = decltype(mat)::value, WPB = 4;
+		const size_t bytes = WPB * sizeof(AdWarp<EL>);
+		err = cudaFuncSetAttribute(k_ad_blocks<EL, MAT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+		if (err != cudaSuccess) return;
+		const int nb = std::min((m.E + WPB - 1) / WPB, 148 * 32);
+		k_ad_blocks<EL, MAT, WPB><<<nb, WPB * 32, bytes, s>>>(m, u, stage);
+	});
+	return err != cudaSuccess ? err : st;
+}
+
+} // namespace pfg

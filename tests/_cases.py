@@ -56,3 +56,15 @@ def permuted(mesh, u, seed=0):
     u2 = np.empty_like(u)
     u2.reshape(-1, 3)[pn] = u.reshape(-1, 3)
     return m2, u2, pn, pe
+
+
+# GenericMatParam names of the parameterised formulations (MooneyRivlinElasticity.hpp,
+# MooneyRivlin3ParamElasticity.hpp, VolumePenalty.hpp)
+MATERIAL_PARAM_NAMES = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
+                        "VolumePenalty": ("k",)}
+
+
+def material_params(mat, n_elements, seed=0):
+    """Per-element parameter values of a parameterised material (stress scale ~1e5)."""
+    rng = np.random.default_rng(seed)
+    return {n: 1e5 * rng.uniform(0.5, 1.5, n_elements) for n in MATERIAL_PARAM_NAMES.get(mat, ())}

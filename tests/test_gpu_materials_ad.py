@@ -1,0 +1,109 @@
+"""Energy-defined formulations on the GPU (pfg_materials.cu): LinearElasticity,
+MooneyRivlin, MooneyRivlin3Param and VolumePenalty, differentiated on the device by
+dual and hyper-dual numbers.  FP64 energy, gradient and Hessian (with
+project_to_psd and the Dirichlet reduction) against the oracle, which
+differentiates the same energies with second-order dual numbers over F as the
+reference's GenericElastic does (AutodiffType::STRESS)."""
+import numpy as np
+import pytest
+
+from oracle.binding import Oracle, project_hessian
+from polyfem_b200 import NeoHookeanAssembler, PfgError
+from polyfem_b200 import mesh as M
+from polyfem_b200._lib import lib
+
+from _cases import make_case, material_params, rel_err
+
+pytestmark = pytest.mark.gpu
+
+MATS = ["LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty"]
+ELEMS = [(M.P1_TET, 3), (M.P2_TET, 2), (M.Q1_HEX, 3)]
+
+
+def setup(et, g, mat, seed=3, disp=0.05):
+    mesh, lam, mu, u, p = make_case(et, g, seed=seed, jitter=0.1 if et != M.P1_TET else 0.0, disp_scale=disp)
+    prm = material_params(mat, mesh.n_elements, seed=seed)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    asm.set_material(mat, **prm)
+    return mesh, asm, Oracle(mesh, lam, mu, material=mat, params=prm), u, p
+
+
+@pytest.mark.parametrize("mat", MATS)
+@pytest.mark.parametrize("et,g", ELEMS, ids=["P1", "P2", "Q1"])
+def test_energy_gradient_hessian_match_oracle(require_gpu, mat, et, g):
+    mesh, asm, orc, u, _ = setup(et, g, mat)
+    e_o = orc.energy(u)
+    assert abs(asm.assemble_energy(u) - e_o) <= 1e-12 * abs(e_o)
+    assert rel_err(asm.assemble_energy_per_element(u), orc.energy_per_element(u)) <= 1e-12
+    assert rel_err(asm.assemble_gradient(u), orc.gradient(u)) <= 1e-12
+    outer, inner, vals = orc.hessian(u)
+    o2, i2 = asm.hessian_pattern()
+    assert np.array_equal(o2, outer) and np.array_equal(i2, inner)
+    v = asm.assemble_hessian_values(u, "fp64")
+    assert rel_err(v, vals) <= 1e-12
+    assert np.array_equal(v, asm.assemble_hessian_values(u, "fp64"))  # deterministic
+    asm.close()
+
+
+@pytest.mark.parametrize("mat", ["MooneyRivlin", "MooneyRivlin3Param"])
+def test_projected_and_reduced_hessian(require_gpu, mat):
+    mesh, asm, orc, _, _ = setup(M.P2_TET, 2, mat, seed=5)
+    rng = np.random.default_rng(6)
+    u = (-0.25 * mesh.node_pos + 0.02 * mesh.h * rng.standard_normal(mesh.node_pos.shape)).ravel()
+    outer, inner, v_psd = orc.hessian(u, project_psd=True)
+    _, _, v_raw = orc.hessian(u)
+    assert rel_err(v_psd, v_raw) > 1e-6  # the projection changes this matrix
+    assert rel_err(asm.assemble_hessian_values(u, "fp64", project_to_psd=True), v_psd) <= 1e-11
+    face = np.flatnonzero(mesh.node_pos[:, 0] <= 1e-12)
+    dofs = (3 * face[:, None] + np.arange(3)).ravel()
+    asm.set_dirichlet(dofs)
+    ro, ri, rv = project_hessian(outer, inner, v_raw, dofs)
+    go, gi = asm.reduced_pattern()
+    assert np.array_equal(go, ro) and np.array_equal(gi, ri)
+    assert rel_err(asm.assemble_hessian_reduced_values(u, "fp64"), rv) <= 1e-12
+    assert rel_err(asm.assemble_gradient_reduced(u, "fp64"), np.delete(orc.gradient(u), np.unique(dofs))) <= 1e-12
+    asm.close()
+
+
+def test_linear_elasticity_hessian_constant_on_device(require_gpu):
+    mesh, asm, orc, u, _ = setup(M.Q1_HEX, 2, "LinearElasticity", seed=8)
+    v0 = asm.assemble_hessian_values(np.zeros(mesh.n_dofs), "fp64")
+    v1 = asm.assemble_hessian_values(u, "fp64")
+    assert rel_err(v1, v0) <= 1e-12
+    asm.close()
+
+
+def test_device_parameters_and_state_errors(require_gpu):
+    import torch
+    mesh, lam, mu, u, _ = make_case(M.P2_TET, 2, seed=9)
+    E = mesh.n_elements
+    prm = material_params("MooneyRivlin3Param", E, seed=9)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    # the material before its parameters: PFG_ERR_STATE
+    assert lib().pfg_set_material(asm.handle, 5) == 0
+    with pytest.raises(PfgError) as ei:
+        asm.assemble_energy(u)
+    assert ei.value.status == 5
+    # parameters as CUDA tensors give the host-array results bit for bit
+    asm.set_material("MooneyRivlin3Param", **{k: torch.tensor(v, device="cuda") for k, v in prm.items()})
+    e_dev, g_dev = asm.assemble_energy(u), asm.assemble_gradient(u)
+    asm.set_material("MooneyRivlin3Param", **prm)
+    assert asm.assemble_energy(u) == e_dev and np.array_equal(asm.assemble_gradient(u), g_dev)
+    # scalars broadcast to every element
+    asm.set_material("VolumePenalty", k=2.5e5)
+    orc = Oracle(mesh, lam, mu, material="VolumePenalty", params={"k": 2.5e5})
+    assert abs(asm.assemble_energy(u) - orc.energy(u)) <= 1e-12 * abs(orc.energy(u))
+    # a parameter count that does not match the material: PFG_ERR_STATE
+    assert lib().pfg_set_material(asm.handle, 4) == 0
+    with pytest.raises(PfgError) as ei:
+        asm.assemble_hessian_values(u, "fp64")
+    assert ei.value.status == 5
+    # FP32 paths stay NeoHookean-only; bad counts and names are rejected
+    asm.set_material("MooneyRivlin", **material_params("MooneyRivlin", E))
+    with pytest.raises(PfgError) as ei:
+        asm.assemble_gradient(u, "fp32")
+    assert ei.value.status == 4
+    assert lib().pfg_set_material_params(asm.handle, None, 5, 0) == 1
+    with pytest.raises(ValueError):
+        asm.set_material("MooneyRivlin", c1=1.0)
+    asm.close()

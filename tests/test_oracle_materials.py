@@ -1,6 +1,7 @@
-"""The oracle's restatement of the GenericElastic materials (IsochoricNeoHookean,
-SaintVenant): derivatives by central finite differences, as the reference checks its
-forms (tests/test_form_derivatives.cpp:166-226), and closed-form known answers."""
+"""The oracle's restatement of the other elastic formulations (IsochoricNeoHookean,
+SaintVenant, LinearElasticity, MooneyRivlin, MooneyRivlin3Param, VolumePenalty):
+derivatives by central finite differences, as the reference checks its forms
+(tests/test_form_derivatives.cpp:166-226), and closed-form known answers."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -8,9 +9,10 @@ import scipy.sparse as sp
 from oracle.binding import Oracle
 from polyfem_b200 import mesh as M
 
-from _cases import make_case
+from _cases import make_case, material_params
 
-MATS = ["IsochoricNeoHookean", "SaintVenant"]
+MATS = ["IsochoricNeoHookean", "SaintVenant", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param",
+        "VolumePenalty"]
 ELEMS = [(M.P1_TET, "P1"), (M.P2_TET, "P2"), (M.Q1_HEX, "Q1")]
 
 
@@ -18,7 +20,7 @@ ELEMS = [(M.P1_TET, "P1"), (M.P2_TET, "P2"), (M.Q1_HEX, "Q1")]
 @pytest.mark.parametrize("et,name", ELEMS, ids=[n for _, n in ELEMS])
 def test_material_derivatives_finite_differences(mat, et, name):
     mesh, lam, mu, u, p = make_case(et, 2, seed=3, jitter=0.1 if et != M.P1_TET else 0.0, disp_scale=0.05)
-    o = Oracle(mesh, lam, mu, material=mat)
+    o = Oracle(mesh, lam, mu, material=mat, params=material_params(mat, mesh.n_elements))
     g = o.gradient(u)
     h = 1e-6 * np.abs(u).max() / np.abs(p).max()
     fd = (o.energy(u + h * p) - o.energy(u - h * p)) / (2 * h)
@@ -31,7 +33,7 @@ def test_material_derivatives_finite_differences(mat, et, name):
     assert np.isclose(o.energy_per_element(u).sum(), o.energy(u), rtol=1e-13)
 
 
-@pytest.mark.parametrize("mat", MATS)
+@pytest.mark.parametrize("mat", MATS[:2])
 def test_material_known_answers(mat):
     mesh, lam, mu, _, _ = make_case(M.P2_TET, 2, seed=4)
     o = Oracle(mesh, lam, mu, material=mat)
@@ -54,6 +56,59 @@ def test_material_known_answers(mat):
         lam_v, mu_v = np.asarray(lam), np.asarray(mu)
         vol = o.energy_per_element(us) / (lam_v / 2 * 9 * e * e + mu_v * 3 * e * e)
         assert np.isclose(vol.sum(), 1.0, rtol=1e-12)
+
+
+
+def _uniform(mesh, F):
+    """Displacement of the homogeneous deformation x -> F x."""
+    return (mesh.node_pos @ (np.asarray(F) - np.eye(3)).T).ravel()
+
+
+def test_energy_defined_materials_known_answers():
+    """Homogeneous deformations of the unit cube, where psi is known in closed form:
+    the energy is psi times the volume (1) for every element type."""
+    for et in (M.P1_TET, M.P2_TET, M.Q1_HEX):
+        mesh, lam, mu, _, _ = make_case(et, 2, seed=4)
+        E = mesh.n_elements
+        lam1, mu1 = 2.0e5, 0.7e5
+        lam = np.full(E, lam1)
+        mu = np.full(E, mu1)
+        c1, c2, c3, d1, k = 1.1e5, 0.4e5, 0.3e5, 2.0e5, 3.0e5
+        s_, th, g_, a_ = 1.2, 0.6, 0.3, 1.25
+        dil = np.eye(3) * s_
+        rot = np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1]])
+        shear = np.eye(3) + g_ * np.outer([1, 0, 0], [0, 1, 0])
+        iso = np.diag([a_, a_ ** -0.5, a_ ** -0.5])  # J = 1
+        I1, I2 = a_ ** 2 + 2 / a_, 2 * a_ + 1 / a_ ** 2  # invariants of F F^T for iso
+        cases = {
+            "LinearElasticity": ({}, [(dil, mu1 * 3 * (s_ - 1) ** 2 + lam1 / 2 * 9 * (s_ - 1) ** 2),
+                                      (rot, mu1 * 2 * (np.cos(th) - 1) ** 2 + lam1 / 2 * 4 * (np.cos(th) - 1) ** 2),
+                                      (shear, mu1 * g_ ** 2 / 2)]),
+            "MooneyRivlin": ({"c1": c1, "c2": c2, "k": k}, [(dil, k / 2 * (3 * np.log(s_)) ** 2), (rot, 0.0),
+                                                            (iso, c1 * (I1 - 3) + c2 * (I2 - 3))]),
+            "MooneyRivlin3Param": ({"c1": c1, "c2": c2, "c3": c3, "d1": d1},
+                                   [(dil, d1 * (s_ ** 3 - 1) ** 2), (rot, 0.0),
+                                    (iso, c1 * (I1 - 3) + (c2 + c3 * (I1 - 3)) * (I2 - 3))]),
+            "VolumePenalty": ({"k": k}, [(dil, k / 2 * ((s_ ** 6 - 1) / 2 - 3 * np.log(s_))), (rot, 0.0), (iso, 0.0)]),
+        }
+        for mat, (prm, checks) in cases.items():
+            o = Oracle(mesh, lam, mu, material=mat, params=prm)
+            assert abs(o.energy(np.zeros(mesh.n_dofs))) <= 1e-12 * c1
+            assert np.abs(o.gradient(np.zeros(mesh.n_dofs))).max() <= 1e-9 * c1
+            for F, psi in checks:
+                assert abs(o.energy(_uniform(mesh, F)) - psi) <= 1e-11 * max(abs(psi), c1), (mat, et, psi)
+
+
+def test_linear_elasticity_hessian_is_constant():
+    """LinearElasticity is quadratic in u: the Hessian does not depend on u and the
+    energy is 1/2 u^T H u."""
+    mesh, lam, mu, u, _ = make_case(M.P2_TET, 2, seed=6, jitter=0.1)
+    o = Oracle(mesh, lam, mu, material="LinearElasticity")
+    outer, inner, v0 = o.hessian(np.zeros(mesh.n_dofs))
+    _, _, v1 = o.hessian(u)
+    assert np.abs(v1 - v0).max() <= 1e-9 * np.abs(v0).max()
+    H = sp.csc_matrix((v0, inner, outer), shape=(mesh.n_dofs, mesh.n_dofs))
+    assert np.isclose(0.5 * u @ (H @ u), o.energy(u), rtol=1e-12)
 
 
 @pytest.mark.parametrize("et", [M.P1_TET, M.P2_TET, M.Q1_HEX], ids=["P1", "P2", "Q1"])
