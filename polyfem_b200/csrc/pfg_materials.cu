@@ -1,35 +1,45 @@
-// Energy-defined materials, differentiated automatically on the device (FP64).
+// Energy-defined materials on the device (FP64).
 //
-// The reference assembles these formulations from an energy density psi(F) alone:
+// The reference assembles these formulations from an energy density alone:
 // GenericElastic (assembler/GenericElastic.cpp:493-611, AutodiffType::STRESS) takes
 // dpsi/dF and d2psi/dF2 by forward-mode autodiff over the 9 entries of F and
 // contracts them with the physical basis gradients; LinearElasticity
 // (LinearElasticity.cpp:65-139) differentiates its strain energy over the nodal
 // values.  Both give, per quadrature point q and node pair (a, b),
-//   gradient  G[a][r]      = sum_q da_q sum_c P[r][c] g_a[c]
-//   Hessian   H_ab[r][k]   = sum_q da_q sum_{c,d} g_a[c] C[(r,c),(k,d)] g_b[d]
-// with P = dpsi/dF and C = d2psi/dF2.  Here psi is written once, generic in its
-// number type, and evaluated as
-//   double  : the energy;
-//   Dual1   : first-order dual numbers, one direction per evaluation: P[i];
-//   HDual   : hyper-dual numbers (Fike and Alonso, "The development of hyper-dual
-//             numbers for exact second-derivative calculations", AIAA 2011-886),
-//             two directions per evaluation: C[i][j] exactly, without truncation.
-// The 45 entries i <= j of C at every point are spread over the lanes of the
-// element's warp; the blocks are then written as the packed block triangle of the
-// element, which the PSD projection and the scatter of pfg_kernels.cu consume.
+//   gradient  G[a][r]    = sum_q da_q sum_c P[r][c] g_a[c]
+//   Hessian   H_ab[r][k] = sum_q da_q sum_{c,d} g_a[c] C[(r,c),(k,d)] g_b[d]
+// with P = dpsi/dF and C = d2psi/dF2 (index 3r + c for F(r, c)).
+//
+// MooneyRivlin, MooneyRivlin3Param and VolumePenalty are functions of the three
+// invariants x = (I1, I2, J) of F, I1 = tr B, I2 = (tr^2 B - tr B^2)/2, J = det F,
+// B = F F^T; their density psi(I1, I2, J) is written once, generic in its number
+// type, and its derivatives psi_x, psi_xy come from hyper-dual numbers over the
+// three scalars (Fike and Alonso, "The development of hyper-dual numbers for exact
+// second-derivative calculations", AIAA 2011-886): six evaluations per point give
+// all of them exactly.  The chain rule through the invariants then gives
+//   P = sum_x psi_x dx/dF,
+//   C = sum_x psi_x d2x/dF2 + sum_{x,y} psi_xy dx/dF (x) dy/dF,
+// with, for i = (a, A), j = (b, B):
+//   dI1/dF = 2F,  dI2/dF = 2 I1 F - 2 B F,  dJ/dF = cof F,
+//   d2I1 = 2 delta_ij,
+//   d2I2 = 4 F_aA F_bB + 2 I1 delta_ab delta_AB - 2 delta_ab (F^T F)_AB - 2 F_aB F_bA - 2 delta_AB B_ab,
+//   d2J  = eps_abc eps_ABC F_cC.
+// LinearElasticity is quadratic: P = 2 mu eps + lambda tr(eps) I and the constant
+// C = mu (delta_ab delta_AB + delta_aB delta_Ab) + lambda delta_aA delta_bB.
+// In the blocks kernel the 45 entries i <= j of C at every point are spread over
+// the lanes of the element's warp; the blocks are written as the packed block
+// triangle of the element, which the PSD projection and the scatter of
+// pfg_kernels.cu consume.
 //
 // Materials (per-element parameters, pfg_set_material_params / pfg_set_lame):
-//   3 LinearElasticity    (lambda, mu)   psi = mu eps:eps + lambda/2 tr(eps)^2,  eps = (G + G^T)/2, G = F - I
-//                                        (LinearElasticity.cpp:113-139)
-//   4 MooneyRivlin        (c1, c2, k)    psi = c1 (I1~ - 3) + c2 (I2~ - 3) + k/2 ln^2 J
-//                                        (MooneyRivlinElasticity.hpp:25-46)
-//   5 MooneyRivlin3Param  (c1, c2, c3, d1) psi = c1 I1~ + (c2 + c3 I1~) I2~ + d1 (J - 1)^2, with
-//                                        I1~ = J^-2/3 tr B - 3, I2~ = J^-4/3 (tr^2 B - tr B^2)/2 - 3
-//                                        (MooneyRivlin3ParamElasticity.hpp:26-49)
-//   6 VolumePenalty       (k)            psi = k/2 ((J^2 - 1)/2 - ln J)   (VolumePenalty.hpp:20-34)
-// with B = F F^T, I1~ = J^-2/3 tr B and I2~ = J^-4/3 (tr^2 B - tr B^2)/2 (the
-// invariants of F~ F~^T, F~ = J^-1/3 F).
+//   3 LinearElasticity    (lambda, mu)     psi = mu eps:eps + lambda/2 tr(eps)^2, eps = (G + G^T)/2, G = F - I
+//                                          (LinearElasticity.cpp:113-139)
+//   4 MooneyRivlin        (c1, c2, k)      psi = c1 (I1~ - 3) + c2 (I2~ - 3) + k/2 ln^2 J
+//                                          (MooneyRivlinElasticity.hpp:25-46)
+//   5 MooneyRivlin3Param  (c1, c2, c3, d1) psi = c1 (I1~ - 3) + (c2 + c3 (I1~ - 3)) (I2~ - 3) + d1 (J - 1)^2
+//                                          (MooneyRivlin3ParamElasticity.hpp:26-49)
+//   6 VolumePenalty       (k)              psi = k/2 ((J^2 - 1)/2 - ln J)   (VolumePenalty.hpp:20-34)
+// with I1~ = J^-2/3 I1 and I2~ = J^-4/3 I2 (the invariants of F~ F~^T, F~ = J^-1/3 F).
 #include "pfg_device.cuh"
 
 #include <algorithm>
@@ -96,47 +106,69 @@ template <class S>
 __device__ __forceinline__ S sq(S x) { return x * x; }
 
 // ---------------------------------------------------------------------------
-// energy densities, generic in the number type
+// energy densities of the invariant materials, generic in the number type
 // ---------------------------------------------------------------------------
 template <int MAT, class S>
-__device__ __forceinline__ S ad_psi(const S F[3][3], const double4 &p)
+__device__ __forceinline__ S inv_psi(S I1, S I2, S J, const double4 &p)
 {
-	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
-	{
-		// eps:eps = sum_r G_rr^2 + 1/2 sum_{r<c} (G_rc + G_cr)^2
-		const S g0 = F[0][0] - 1.0, g1 = F[1][1] - 1.0, g2 = F[2][2] - 1.0;
-		const S tr = g0 + g1 + g2;
-		const S ee = sq(g0) + sq(g1) + sq(g2) + 0.5 * (sq(F[0][1] + F[1][0]) + sq(F[0][2] + F[2][0]) + sq(F[1][2] + F[2][1]));
-		return p.y * ee + (0.5 * p.x) * sq(tr);
-	}
+	if constexpr (MAT == MAT_VOLUME_PENALTY)
+		return (0.5 * p.x) * (0.5 * (sq(J) - 1.0) - ad_log(J));
 	else
 	{
-		const S J = det3(F);
-		if constexpr (MAT == MAT_VOLUME_PENALTY)
-			return (0.5 * p.x) * (0.5 * (sq(J) - 1.0) - ad_log(J));
-		else
-		{
-			S B[3][3]; // B = F F^T (symmetric)
-#pragma unroll
-			for (int r = 0; r < 3; ++r)
-#pragma unroll
-				for (int c = r; c < 3; ++c) B[r][c] = F[r][0] * F[c][0] + F[r][1] * F[c][1] + F[r][2] * F[c][2];
-			const S trB = B[0][0] + B[1][1] + B[2][2];
-			const S trB2 = sq(B[0][0]) + sq(B[1][1]) + sq(B[2][2]) + 2.0 * (sq(B[0][1]) + sq(B[0][2]) + sq(B[1][2]));
-			const S i2 = 0.5 * (sq(trB) - trB2);
-			const S j23 = ad_pow(J, -2.0 / 3.0);
-			if constexpr (MAT == MAT_MOONEY_RIVLIN)
-			{
-				const S lj = ad_log(J);
-				return p.x * (j23 * trB - 3.0) + p.y * (sq(j23) * i2 - 3.0) + (0.5 * p.z) * sq(lj);
-			}
-			else // MAT_MOONEY_RIVLIN_3PARAM
-			{
-				const S I1t = j23 * trB - 3.0, I2t = sq(j23) * i2 - 3.0, jm1 = J - 1.0;
-				return p.x * I1t + (p.z * I1t + p.y) * I2t + p.w * sq(jm1);
-			}
-		}
+		const S j23 = ad_pow(J, -2.0 / 3.0);
+		const S I1t = j23 * I1 - 3.0, I2t = sq(j23) * I2 - 3.0;
+		if constexpr (MAT == MAT_MOONEY_RIVLIN)
+			return p.x * I1t + p.y * I2t + (0.5 * p.z) * sq(ad_log(J));
+		else // MAT_MOONEY_RIVLIN_3PARAM
+			return p.x * I1t + (p.z * I1t + p.y) * I2t + p.w * sq(J - 1.0);
 	}
+}
+
+// invariants of F and their derivatives: dx[x][3a + A] = dx/dF(a, A) for x = I1, I2, J;
+// B = F F^T and Cr = F^T F (row-major 9)
+struct Invariants
+{
+	double I1, I2, J;
+	double B[9], Cr[9], dx[3][9];
+};
+
+__device__ __forceinline__ void invariants(const double F[3][3], Invariants &v)
+{
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c)
+		{
+			v.B[3 * r + c] = F[r][0] * F[c][0] + F[r][1] * F[c][1] + F[r][2] * F[c][2];
+			v.Cr[3 * r + c] = F[0][r] * F[0][c] + F[1][r] * F[1][c] + F[2][r] * F[2][c];
+		}
+	v.I1 = v.B[0] + v.B[4] + v.B[8];
+	double trB2 = 0.0;
+#pragma unroll
+	for (int i = 0; i < 9; ++i) trB2 += v.B[i] * v.B[i];
+	v.I2 = 0.5 * (v.I1 * v.I1 - trB2);
+	v.J = det3(F);
+	double cof[3][3];
+	cofactor3(F, cof);
+#pragma unroll
+	for (int a = 0; a < 3; ++a)
+#pragma unroll
+		for (int A = 0; A < 3; ++A)
+		{
+			const double BF = v.B[3 * a] * F[0][A] + v.B[3 * a + 1] * F[1][A] + v.B[3 * a + 2] * F[2][A];
+			v.dx[0][3 * a + A] = 2.0 * F[a][A];
+			v.dx[1][3 * a + A] = 2.0 * (v.I1 * F[a][A] - BF);
+			v.dx[2][3 * a + A] = cof[a][A];
+		}
+}
+
+// psi_x (x = I1, I2, J) by three dual evaluations
+template <int MAT>
+__device__ __forceinline__ void inv_psi_first(const Invariants &v, const double4 &p, double d[3])
+{
+#pragma unroll 1
+	for (int x = 0; x < 3; ++x)
+		d[x] = inv_psi<MAT, Dual1>({v.I1, x == 0 ? 1.0 : 0.0}, {v.I2, x == 1 ? 1.0 : 0.0}, {v.J, x == 2 ? 1.0 : 0.0}, p).d;
 }
 
 template <int MAT>
@@ -155,19 +187,46 @@ __device__ __forceinline__ double4 ad_params(const DevMesh &m, int e)
 	}
 }
 
-// P[i] = dpsi/dF_i (i = 3r + c), one dual evaluation per entry
 template <int MAT>
-__device__ __forceinline__ void ad_piola(const double F[3][3], const double4 &p, double P[9])
+__device__ __forceinline__ double mat_energy(const double F[3][3], const double4 &p)
 {
-#pragma unroll 1
-	for (int i = 0; i < 9; ++i)
+	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
 	{
-		Dual1 Fd[3][3];
+		// eps:eps = sum_r G_rr^2 + 1/2 sum_{r<c} (G_rc + G_cr)^2
+		const double g0 = F[0][0] - 1.0, g1 = F[1][1] - 1.0, g2 = F[2][2] - 1.0, tr = g0 + g1 + g2;
+		const double ee = g0 * g0 + g1 * g1 + g2 * g2 +
+						  0.5 * (sq(F[0][1] + F[1][0]) + sq(F[0][2] + F[2][0]) + sq(F[1][2] + F[2][1]));
+		return p.y * ee + 0.5 * p.x * tr * tr;
+	}
+	else
+	{
+		Invariants v;
+		invariants(F, v);
+		return inv_psi<MAT, double>(v.I1, v.I2, v.J, p);
+	}
+}
+
+// P = dpsi/dF (row-major 9)
+template <int MAT>
+__device__ __forceinline__ void mat_stress(const double F[3][3], const double4 &p, double P[9])
+{
+	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
+	{
+		const double tr = F[0][0] + F[1][1] + F[2][2] - 3.0;
 #pragma unroll
 		for (int r = 0; r < 3; ++r)
 #pragma unroll
-			for (int c = 0; c < 3; ++c) Fd[r][c] = {F[r][c], 3 * r + c == i ? 1.0 : 0.0};
-		P[i] = ad_psi<MAT, Dual1>(Fd, p).d;
+			for (int c = 0; c < 3; ++c)
+				P[3 * r + c] = p.y * ((F[r][c] - (r == c)) + (F[c][r] - (r == c))) + (r == c ? p.x * tr : 0.0);
+	}
+	else
+	{
+		Invariants v;
+		invariants(F, v);
+		double d[3];
+		inv_psi_first<MAT>(v, p, d);
+#pragma unroll
+		for (int i = 0; i < 9; ++i) P[i] = d[0] * v.dx[0][i] + d[1] * v.dx[1][i] + d[2] * v.dx[2][i];
 	}
 }
 
@@ -192,7 +251,7 @@ __device__ __forceinline__ double ad_element_energy(const DevMesh &m, const doub
 		geometry<EL, double>(q, Xg, Jit, detJ);
 		gen_def_grad<EL>(q, U, Jit, F);
 		bad |= !(det3(F) > 0.0);
-		en += ad_psi<MAT, double>(F, prm) * (detJ * qweight<EL>(q));
+		en += mat_energy<MAT>(F, prm) * (detJ * qweight<EL>(q));
 	}
 	if (bad) atomicAdd(inverted, 1ull);
 	return en;
@@ -233,14 +292,14 @@ __global__ void __launch_bounds__(NT) k_ad_gradient(DevMesh m, const double *__r
 #pragma unroll
 	for (int a = 0; a < EL::N; ++a) Gacc[a][0] = Gacc[a][1] = Gacc[a][2] = 0.0;
 	bool bad = false;
-#pragma unroll 1
+#pragma unroll
 	for (int q = 0; q < EL::NQ; ++q)
 	{
 		double Jit[3][3], detJ, F[3][3], P[9];
 		geometry<EL, double>(q, Xg, Jit, detJ);
 		gen_def_grad<EL>(q, U, Jit, F);
 		bad |= !(det3(F) > 0.0);
-		ad_piola<MAT>(F, prm, P);
+		mat_stress<MAT>(F, prm, P);
 		const double da = detJ * qweight<EL>(q);
 		double Q[3][3]; // da P J^-1 = da P Jit^T: G[a][d] = sum_r gref(q, a, r) Q[d][r]
 #pragma unroll
@@ -273,9 +332,12 @@ __global__ void __launch_bounds__(NT) k_ad_gradient(DevMesh m, const double *__r
 // ---------------------------------------------------------------------------
 // element blocks: one warp per element
 // ---------------------------------------------------------------------------
-// (i, j), i <= j, of the 9 x 9 table C in tri_index(9, i, j) order; and the node
-// pairs of the element block triangle (P1, P2, Q1)
+// (i, j), i <= j, of the 9 x 9 table C in tri_index(9, i, j) order; the pairs
+// (x, y), x <= y, of the three invariants; the node pairs of the element block
+// triangle (P1, P2, Q1)
 __constant__ PairTable c_ad_c9 = make_pairs(9);
+__constant__ PairTable c_ad_x3 = make_pairs(3);
+
 __constant__ PairTable c_ad_pairs[3] = {make_pairs(4), make_pairs(10), make_pairs(8)};
 
 template <class EL>
@@ -283,13 +345,41 @@ struct AdWarp
 {
 	static constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ, TP = tri_pad(EL::N);
 	double U[N][3], X[NG][3];
-	double F[NQ][9], Jit[NQ][9], da[NQ];
+	double Jit[NQ][9], da[NQ];
+	Invariants inv[NQ];
+	double psi[NQ][9];              // psi_x (x = I1, I2, J), then psi_xy (x <= y) in tri_index(3, x, y) order
 	double C[NQ][45];               // da d2psi/dF2 at point q, entry (i <= j) at tri_index(9, i, j)
 	alignas(16) double g[NQ][N][4]; // physical basis gradients (x, y, z, 0): two 16-byte loads
 	alignas(16) double tri[TP];     // the element's packed block triangle, copied out as double2
 };
 
 __host__ __device__ constexpr int c9(int i, int j) { return i <= j ? tri_index(9, i, j) : tri_index(9, j, i); }
+
+// d2psi/dF_i dF_j from the invariants' derivatives (i = 3a + A, j = 3b + B)
+__device__ __forceinline__ double inv_hessian_entry(const Invariants &v, const double *psi, int i, int j)
+{
+	const int a = i / 3, A = i - 3 * a, b = j / 3, B = j - 3 * b;
+	const double *dx0 = v.dx[0], *dx1 = v.dx[1], *dx2 = v.dx[2];
+	// F from dI1/dF = 2F
+	const double FaA = 0.5 * dx0[i], FbB = 0.5 * dx0[j], FaB = 0.5 * dx0[3 * a + B], FbA = 0.5 * dx0[3 * b + A];
+	double d2I2 = 4.0 * FaA * FbB - 2.0 * FaB * FbA;
+	if (a == b) d2I2 += 2.0 * ((A == B ? v.I1 : 0.0) - v.Cr[3 * A + B]);
+	if (A == B) d2I2 -= 2.0 * v.B[3 * a + b];
+	double d2J = 0.0;
+	if (a != b && A != B)
+	{
+		const int c = 3 - a - b, C = 3 - A - B;
+		const double s = ((b - a + 3) % 3 == 1) == ((B - A + 3) % 3 == 1) ? 1.0 : -1.0; // eps_abc eps_ABC
+		d2J = s * 0.5 * dx0[3 * c + C];
+	}
+	const double xi[3] = {dx0[i], dx1[i], dx2[i]}, xj[3] = {dx0[j], dx1[j], dx2[j]};
+	double h = psi[0] * (i == j ? 2.0 : 0.0) + psi[1] * d2I2 + psi[2] * d2J;
+#pragma unroll
+	for (int x = 0; x < 3; ++x)
+#pragma unroll
+		for (int y = 0; y < 3; ++y) h += psi[3 + (x <= y ? tri_index(3, x, y) : tri_index(3, y, x))] * xi[x] * xj[y];
+	return h;
+}
 
 template <class EL, int MAT, int WPB>
 __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double *__restrict__ u, double *__restrict__ stage)
@@ -306,6 +396,7 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 		for (int i = lane; i < NG * 3; i += 32)
 			S.X[i / 3][i % 3] = __ldg(m.X + (size_t)__ldg(m.gconn + (size_t)(i / 3) * m.E + e) * 3 + i % 3);
 		__syncwarp();
+		const double4 prm = ad_params<MAT>(m, e);
 		if (lane < NQ)
 		{
 			const int q = lane;
@@ -315,15 +406,11 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
 #pragma unroll
-				for (int c = 0; c < 3; ++c)
-				{
-					S.F[q][3 * r + c] = F[r][c];
-					S.Jit[q][3 * r + c] = Jit[r][c];
-				}
+				for (int c = 0; c < 3; ++c) S.Jit[q][3 * r + c] = Jit[r][c];
 			S.da[q] = detJ * qweight<EL>(q);
+			if constexpr (MAT != MAT_LINEAR_ELASTICITY) invariants(F, S.inv[q]);
 		}
 		__syncwarp();
-		const double4 prm = ad_params<MAT>(m, e);
 		// lanes over (point, node): g = J^-T gref
 		for (int t = lane; t < NQ * N; t += 32)
 		{
@@ -334,21 +421,35 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 				g[c] = gref<EL>(q, a, 0) * S.Jit[q][c] + gref<EL>(q, a, 1) * S.Jit[q][3 + c] + gref<EL>(q, a, 2) * S.Jit[q][6 + c];
 			g[3] = 0.0;
 		}
-		// lanes over (point, entry i <= j of C): one hyper-dual evaluation each
+		if constexpr (MAT != MAT_LINEAR_ELASTICITY)
+		{
+			// lanes over (point, invariant pair x <= y): one hyper-dual evaluation each
+			for (int t = lane; t < NQ * 6; t += 32)
+			{
+				const int q = t / 6, k = t - q * 6, x = c_ad_x3.a[k], y = c_ad_x3.b[k];
+				const Invariants &v = S.inv[q];
+				const HDual h = inv_psi<MAT, HDual>({v.I1, x == 0 ? 1.0 : 0.0, y == 0 ? 1.0 : 0.0, 0.0},
+													{v.I2, x == 1 ? 1.0 : 0.0, y == 1 ? 1.0 : 0.0, 0.0},
+													{v.J, x == 2 ? 1.0 : 0.0, y == 2 ? 1.0 : 0.0, 0.0}, prm);
+				S.psi[q][3 + k] = h.ab;
+				if (x == y) S.psi[q][x] = h.a;
+			}
+			__syncwarp();
+		}
+		// lanes over (point, entry i <= j of C)
 		for (int t = lane; t < NQ * 45; t += 32)
 		{
-			const int q = t / 45, k = t - q * 45;
-			const int i = c_ad_c9.a[k], j = c_ad_c9.b[k];
-			HDual Fh[3][3];
-#pragma unroll
-			for (int r = 0; r < 3; ++r)
-#pragma unroll
-				for (int c = 0; c < 3; ++c)
-				{
-					const int x = 3 * r + c;
-					Fh[r][c] = {S.F[q][x], x == i ? 1.0 : 0.0, x == j ? 1.0 : 0.0, 0.0};
-				}
-			S.C[q][k] = S.da[q] * ad_psi<MAT, HDual>(Fh, prm).ab;
+			const int q = t / 45, k = t - q * 45, i = c_ad_c9.a[k], j = c_ad_c9.b[k];
+			double h;
+			if constexpr (MAT == MAT_LINEAR_ELASTICITY)
+			{
+				const int a = i / 3, A = i - 3 * a, b = j / 3, B = j - 3 * b;
+				h = prm.y * ((a == b && A == B ? 1.0 : 0.0) + (a == B && A == b ? 1.0 : 0.0)) +
+					(a == A && b == B ? prm.x : 0.0);
+			}
+			else
+				h = inv_hessian_entry(S.inv[q], S.psi[q], i, j);
+			S.C[q][k] = S.da[q] * h;
 		}
 		__syncwarp();
 		// lanes over node pairs (a <= b): H_ab[r][k] = sum_q sum_{c,d} g_a[c] C[(r,c),(k,d)] g_b[d]
