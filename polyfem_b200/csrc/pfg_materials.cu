@@ -332,12 +332,56 @@ __global__ void __launch_bounds__(NT) k_ad_gradient(DevMesh m, const double *__r
 // ---------------------------------------------------------------------------
 // element blocks: one warp per element
 // ---------------------------------------------------------------------------
-// (i, j), i <= j, of the 9 x 9 table C in tri_index(9, i, j) order; the pairs
-// (x, y), x <= y, of the three invariants; the node pairs of the element block
-// triangle (P1, P2, Q1)
-__constant__ PairTable c_ad_c9 = make_pairs(9);
+// Entry k (i <= j, tri_index(9, i, j) order) of the 9 x 9 table C, with i = 3a + A,
+// j = 3b + B: the flat indices and 0/1 factors of its terms, so that the lanes of a
+// warp, each at its own entry, form it without branches:
+//   aB = 3a + B, bA = 3b + A, AB = 3A + B, ab = 3a + b (indices into F, F^T F, F F^T),
+//   cC = 3c + C and sJ = eps_abc eps_ABC for the one nonzero term of d2J (a != b, A != B),
+//   the deltas ab, AB and ij, and the two index patterns of the LinearElasticity tangent.
+struct alignas(4) CEntry
+{
+	unsigned char i, j, aB, bA, AB, ab, cC, dab, dAB, dij, le_aBbA, le_aAbB;
+	signed char sJ;
+	unsigned char pad[3];
+};
+struct CEntryTable
+{
+	CEntry e[45];
+};
+constexpr CEntryTable make_centries()
+{
+	CEntryTable t{};
+	int k = 0;
+	for (int i = 0; i < 9; ++i)
+		for (int j = i; j < 9; ++j)
+		{
+			const int a = i / 3, A = i % 3, b = j / 3, B = j % 3;
+			CEntry &c = t.e[k++];
+			c.i = (unsigned char)i;
+			c.j = (unsigned char)j;
+			c.aB = (unsigned char)(3 * a + B);
+			c.bA = (unsigned char)(3 * b + A);
+			c.AB = (unsigned char)(3 * A + B);
+			c.ab = (unsigned char)(3 * a + b);
+			c.dab = a == b;
+			c.dAB = A == B;
+			c.dij = i == j;
+			c.le_aBbA = a == B && A == b;
+			c.le_aAbB = a == A && b == B;
+			if (a != b && A != B)
+			{
+				const int cc = 3 - a - b, CC = 3 - A - B;
+				const bool p1 = (b - a + 3) % 3 == 1, p2 = (B - A + 3) % 3 == 1; // cyclic (a, b, c), (A, B, C)
+				c.cC = (unsigned char)(3 * cc + CC);
+				c.sJ = p1 == p2 ? 1 : -1;
+			}
+		}
+	return t;
+}
+__constant__ CEntryTable c_ad_centries = make_centries();
+// the pairs (x, y), x <= y, of the three invariants; the node pairs of the element
+// block triangle (P1, P2, Q1)
 __constant__ PairTable c_ad_x3 = make_pairs(3);
-
 __constant__ PairTable c_ad_pairs[3] = {make_pairs(4), make_pairs(10), make_pairs(8)};
 
 template <class EL>
@@ -355,25 +399,18 @@ struct AdWarp
 
 __host__ __device__ constexpr int c9(int i, int j) { return i <= j ? tri_index(9, i, j) : tri_index(9, j, i); }
 
-// d2psi/dF_i dF_j from the invariants' derivatives (i = 3a + A, j = 3b + B)
-__device__ __forceinline__ double inv_hessian_entry(const Invariants &v, const double *psi, int i, int j)
+// d2psi/dF_i dF_j from the invariants' derivatives, entry ce of C
+__device__ __forceinline__ double inv_hessian_entry(const Invariants &v, const double *psi, const CEntry &ce)
 {
-	const int a = i / 3, A = i - 3 * a, b = j / 3, B = j - 3 * b;
 	const double *dx0 = v.dx[0], *dx1 = v.dx[1], *dx2 = v.dx[2];
-	// F from dI1/dF = 2F
-	const double FaA = 0.5 * dx0[i], FbB = 0.5 * dx0[j], FaB = 0.5 * dx0[3 * a + B], FbA = 0.5 * dx0[3 * b + A];
-	double d2I2 = 4.0 * FaA * FbB - 2.0 * FaB * FbA;
-	if (a == b) d2I2 += 2.0 * ((A == B ? v.I1 : 0.0) - v.Cr[3 * A + B]);
-	if (A == B) d2I2 -= 2.0 * v.B[3 * a + b];
-	double d2J = 0.0;
-	if (a != b && A != B)
-	{
-		const int c = 3 - a - b, C = 3 - A - B;
-		const double s = ((b - a + 3) % 3 == 1) == ((B - A + 3) % 3 == 1) ? 1.0 : -1.0; // eps_abc eps_ABC
-		d2J = s * 0.5 * dx0[3 * c + C];
-	}
+	const int i = ce.i, j = ce.j;
+	// F = dI1/dF / 2
+	const double FaA = 0.5 * dx0[i], FbB = 0.5 * dx0[j], FaB = 0.5 * dx0[ce.aB], FbA = 0.5 * dx0[ce.bA];
+	const double d2I2 = 4.0 * FaA * FbB - 2.0 * FaB * FbA + 2.0 * ce.dab * (ce.dAB * v.I1 - v.Cr[ce.AB]) -
+						2.0 * ce.dAB * v.B[ce.ab];
+	const double d2J = ce.sJ * 0.5 * dx0[ce.cC];
 	const double xi[3] = {dx0[i], dx1[i], dx2[i]}, xj[3] = {dx0[j], dx1[j], dx2[j]};
-	double h = psi[0] * (i == j ? 2.0 : 0.0) + psi[1] * d2I2 + psi[2] * d2J;
+	double h = psi[0] * (2.0 * ce.dij) + psi[1] * d2I2 + psi[2] * d2J;
 #pragma unroll
 	for (int x = 0; x < 3; ++x)
 #pragma unroll
@@ -389,6 +426,22 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	W &S = reinterpret_cast<W *>(smem_raw)[threadIdx.x >> 5];
 	const int lane = threadIdx.x & 31;
+	// the lookup tables in shared memory: lanes at different entries read them without
+	// the serialisation of divergent constant-memory reads
+	__shared__ CEntry s_ce[45];
+	__shared__ unsigned char s_pa[NP], s_pb[NP], s_xa[6], s_xb[6];
+	for (int t = threadIdx.x; t < 45; t += WPB * 32) s_ce[t] = c_ad_centries.e[t];
+	for (int t = threadIdx.x; t < NP; t += WPB * 32)
+	{
+		s_pa[t] = c_ad_pairs[EL::ET - 1].a[t];
+		s_pb[t] = c_ad_pairs[EL::ET - 1].b[t];
+	}
+	for (int t = threadIdx.x; t < 6; t += WPB * 32)
+	{
+		s_xa[t] = c_ad_x3.a[t];
+		s_xb[t] = c_ad_x3.b[t];
+	}
+	__syncthreads();
 	for (int e = blockIdx.x * WPB + (threadIdx.x >> 5); e < m.E; e += gridDim.x * WPB)
 	{
 		for (int i = lane; i < N * 3; i += 32)
@@ -426,7 +479,7 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 			// lanes over (point, invariant pair x <= y): one hyper-dual evaluation each
 			for (int t = lane; t < NQ * 6; t += 32)
 			{
-				const int q = t / 6, k = t - q * 6, x = c_ad_x3.a[k], y = c_ad_x3.b[k];
+				const int q = t / 6, k = t - q * 6, x = s_xa[k], y = s_xb[k];
 				const Invariants &v = S.inv[q];
 				const HDual h = inv_psi<MAT, HDual>({v.I1, x == 0 ? 1.0 : 0.0, y == 0 ? 1.0 : 0.0, 0.0},
 													{v.I2, x == 1 ? 1.0 : 0.0, y == 1 ? 1.0 : 0.0, 0.0},
@@ -439,23 +492,20 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 		// lanes over (point, entry i <= j of C)
 		for (int t = lane; t < NQ * 45; t += 32)
 		{
-			const int q = t / 45, k = t - q * 45, i = c_ad_c9.a[k], j = c_ad_c9.b[k];
+			const int q = t / 45, k = t - q * 45;
+			const CEntry ce = s_ce[k];
 			double h;
 			if constexpr (MAT == MAT_LINEAR_ELASTICITY)
-			{
-				const int a = i / 3, A = i - 3 * a, b = j / 3, B = j - 3 * b;
-				h = prm.y * ((a == b && A == B ? 1.0 : 0.0) + (a == B && A == b ? 1.0 : 0.0)) +
-					(a == A && b == B ? prm.x : 0.0);
-			}
+				h = prm.y * (ce.dab * ce.dAB + ce.le_aBbA) + prm.x * ce.le_aAbB;
 			else
-				h = inv_hessian_entry(S.inv[q], S.psi[q], i, j);
+				h = inv_hessian_entry(S.inv[q], S.psi[q], ce);
 			S.C[q][k] = S.da[q] * h;
 		}
 		__syncwarp();
 		// lanes over node pairs (a <= b): H_ab[r][k] = sum_q sum_{c,d} g_a[c] C[(r,c),(k,d)] g_b[d]
 		for (int p = lane; p < NP; p += 32)
 		{
-			const int a = c_ad_pairs[EL::ET - 1].a[p], b = c_ad_pairs[EL::ET - 1].b[p];
+			const int a = s_pa[p], b = s_pb[p];
 			double h[3][3] = {};
 			for (int q = 0; q < NQ; ++q)
 			{
