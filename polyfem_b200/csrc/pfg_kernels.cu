@@ -1556,6 +1556,15 @@ __global__ void __launch_bounds__(WPB * 32, gen_blocks_min_ctas<EL, MAT>())
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	W &S = reinterpret_cast<W *>(smem_raw)[threadIdx.x >> 5];
 	const int lane = threadIdx.x & 31;
+	// the node pairs in shared memory: lanes at different pairs read them without the
+	// serialisation of divergent constant-memory reads
+	__shared__ unsigned char s_pa[NP], s_pb[NP];
+	for (int t = threadIdx.x; t < NP; t += WPB * 32)
+	{
+		s_pa[t] = c_pairs[EL::ET - 1].a[t];
+		s_pb[t] = c_pairs[EL::ET - 1].b[t];
+	}
+	__syncthreads();
 	for (int e = blockIdx.x * WPB + (threadIdx.x >> 5); e < m.E; e += gridDim.x * WPB)
 	{
 		for (int i = lane; i < N * 3; i += 32)
@@ -1633,7 +1642,7 @@ __global__ void __launch_bounds__(WPB * 32, gen_blocks_min_ctas<EL, MAT>())
 		__syncwarp();
 		for (int p = lane; p < NP; p += 32)
 		{
-			const int a = c_pairs[EL::ET - 1].a[p], b = c_pairs[EL::ET - 1].b[p];
+			const int a = s_pa[p], b = s_pb[p];
 			double h[3][3] = {};
 			for (int q = 0; q < NQ; ++q)
 			{
@@ -1763,6 +1772,24 @@ __global__ void __launch_bounds__(WPB * 32) k_mass_blocks(DevMesh m, const doubl
 	constexpr int N = EL::N, NQ = EL::NQ, NP = N * (N + 1) / 2, TP = tri_pad(EL::N);
 	__shared__ double wdet[WPB][NQ];
 	__shared__ double vpair[WPB][NP];
+	// per pair (tri_index order): its nodes, and on the affine tets the closed-form
+	// factor of |T| (P1 (1 + delta_ab) / 20, P2 c_mass_p2[a][b] / 420)
+	__shared__ unsigned char s_pa[NP], s_pb[NP];
+	__shared__ double s_coef[NP];
+	for (int p = threadIdx.x; p < NP; p += WPB * 32)
+	{
+		int a = 0, b = p;
+		while (b >= N - a)
+		{
+			b -= N - a;
+			++a;
+		}
+		b += a;
+		s_pa[p] = (unsigned char)a;
+		s_pb[p] = (unsigned char)b;
+		s_coef[p] = EL::ET == 1 ? (a == b ? 2.0 : 1.0) / 20.0 : EL::ET == 2 ? c_mass_p2[a][b] / 420.0 : 0.0;
+	}
+	__syncthreads();
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	for (int e = blockIdx.x * WPB + w; e < m.E; e += gridDim.x * WPB)
 	{
@@ -1778,13 +1805,7 @@ __global__ void __launch_bounds__(WPB * 32) k_mass_blocks(DevMesh m, const doubl
 		// the pairs' values, then the whole triangle in consecutive stores
 		for (int p = lane; p < NP; p += 32)
 		{
-			int a = 0, b = p;
-			while (b >= N - a)
-			{
-				b -= N - a;
-				++a;
-			}
-			b += a;
+			const int a = s_pa[p], b = s_pb[p];
 			double v;
 			if constexpr (EL::ET == 3)
 			{
@@ -1798,7 +1819,7 @@ __global__ void __launch_bounds__(WPB * 32) k_mass_blocks(DevMesh m, const doubl
 				// |T| = sum_q detJ w_q (the stiffness rule's weights sum to 1/6)
 				double vol = 0.0;
 				for (int q = 0; q < NQ; ++q) vol += wdet[w][q];
-				v = EL::ET == 1 ? vol * (a == b ? 2.0 : 1.0) / 20.0 : vol * c_mass_p2[a][b] / 420.0;
+				v = vol * s_coef[p];
 			}
 			vpair[w][p] = v * r_e;
 		}
