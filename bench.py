@@ -426,6 +426,7 @@ SUITE = {
     "P1-48": ("p1", 48, 0.0, True, "rand", "P1 tets 48^3 x 6 (663,552), lognormal Lame"),
     "P2-40": ("p2", 40, 0.0, True, "rand", "P2 tets 40^3 x 6 (384,000), lognormal Lame"),
     "P2-32j": ("p2", 32, 0.1, False, "rand", "P2 tets 32^3 x 6 (196,608), jittered rest positions, homogeneous"),
+    "P2-24": ("p2", 24, 0.0, True, "rand", "P2 tets 24^3 x 6 (82,944), lognormal Lame: the small case of the ncu captures"),
     "Q1-96j": ("hex", 96, 0.1, True, "smooth", "Q1 hexes 96^3 (884,736), jittered, lognormal Lame, smooth u"),
 }
 
@@ -528,8 +529,17 @@ def run_suite(args):
         res["cg_reduced_psd"] = {"us": round(ms * 1e3, 2), "iterations": it.value,
                                  "us_per_iteration": round(per_it * 1e3, 2), "alg_GBps": round(gbs, 1),
                                  "frac_hbm": round(gbs / peak, 4), "n": nf, "nnz": rnnz}
-        # the other materials (FP64): energy, gradient and the Hessian
-        for mname, mid in (("iso_neohookean", 1), ("saint_venant", 2)):
+        # the other materials (FP64): energy, gradient and the Hessian; the
+        # parameterised ones with (c1, c2, k), (c1, c2, c3, d1), (k) of stress scale mu
+        mu_s = float(np.median(mu))
+        mpar = {4: [mu_s, 0.5 * mu_s, 10 * mu_s], 5: [mu_s, 0.5 * mu_s, 0.2 * mu_s, 10 * mu_s], 6: [10 * mu_s]}
+        for mname, mid in (("iso_neohookean", 1), ("saint_venant", 2), ("linear_elasticity", 3),
+                           ("mooney_rivlin", 4), ("mooney_rivlin_3param", 5), ("volume_penalty", 6)):
+            if mid in mpar:
+                pv = np.ascontiguousarray(np.repeat(np.asarray(mpar[mid], dtype=np.float64)[:, None], E, axis=1))
+                check(L.pfg_set_material_params(h, vp(pv.ctypes.data), len(mpar[mid]), 0), h,
+                      "pfg_set_material_params")
+                L.pfg_set_stream(h, vp(stream.cuda_stream))
             check(L.pfg_set_material(h, mid), h, "pfg_set_material")
             mops = {f"energy_{mname}": lambda: L.pfg_energy(h, U, 1, 0, O),
                     f"gradient_{mname}": lambda: L.pfg_gradient(h, U, 1, 0, O),
