@@ -107,3 +107,30 @@ def test_device_parameters_and_state_errors(require_gpu):
     with pytest.raises(ValueError):
         asm.set_material("MooneyRivlin", c1=1.0)
     asm.close()
+
+
+@pytest.mark.parametrize("mat", MATS)
+def test_inverted_element(require_gpu, mat):
+    """An element turned inside out: ln J and J^(-2/3) of a negative J give NaN, which
+    propagates as in the reference (no clamp); LinearElasticity stays finite.  The
+    per-element energies, the gradient's NaN pattern and the inverted count follow the
+    oracle."""
+    mesh, lam, mu, _, _ = make_case(M.P1_TET, 2, seed=17)
+    bad = np.zeros(mesh.n_dofs)
+    c = mesh.conn[0]
+    X = mesh.node_pos
+    bad.reshape(-1, 3)[c[3]] = 2.0 * (X[c[:3]].mean(axis=0) - X[c[3]])  # vertex 3 through the opposite face
+    prm = material_params(mat, mesh.n_elements, seed=17)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    asm.set_material(mat, **prm)
+    orc = Oracle(mesh, lam, mu, material=mat, params=prm)
+    pe, pe_o = asm.assemble_energy_per_element(bad), orc.energy_per_element(bad)
+    assert np.array_equal(np.isnan(pe), np.isnan(pe_o))
+    assert np.isnan(pe[0]) == (mat != "LinearElasticity")
+    ok = ~np.isnan(pe_o)
+    assert rel_err(pe[ok], pe_o[ok]) <= 1e-12
+    g, g_o = asm.assemble_gradient(bad), orc.gradient(bad)
+    assert np.array_equal(np.isnan(g), np.isnan(g_o))
+    assert rel_err(g[~np.isnan(g_o)], g_o[~np.isnan(g_o)]) <= 1e-12
+    assert asm.inverted_count() >= 1
+    asm.close()
