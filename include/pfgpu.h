@@ -185,8 +185,14 @@ int pfg_version(void);
  *   PFG_MAT_VOLUME_PENALTY      : VolumePenalty (VolumePenalty.hpp:20-34), (k).
  * Energy, gradient and Hessian (with project_psd and the Dirichlet reduction) then
  * follow the chosen material in PFG_FP64 (other precisions return
- * PFG_ERR_UNSUPPORTED); the adjoint terms (pfg_material_vjp, pfg_shape_vjp) remain
- * NeoHookean-only.  Takes effect for the calls that follow; the pattern is unchanged.
+ * PFG_ERR_UNSUPPORTED).  The adjoint terms follow the reference's assemblers:
+ * pfg_material_vjp (compute_dstress_dmu_dlambda) exists for NeoHookean and
+ * LinearElasticity (dP/dmu = grad u + grad u^T, dP/dlambda = tr(grad u) I,
+ * LinearElasticity.cpp:290-299); pfg_shape_vjp (compute_stress_grad_multiply_mat)
+ * for every formulation here but SaintVenant, in PFG_FP64 for all but NeoHookean;
+ * the others return PFG_ERR_UNSUPPORTED, where the reference throws "Not
+ * implemented" (Assembler.hpp:147-156).  Takes effect for the calls that follow;
+ * the pattern is unchanged.
  * ------------------------------------------------------------------------- */
 enum pfg_material
 {

@@ -1314,6 +1314,21 @@ static void material_vjp_impl(Context &c, const double *x, const double *adj, do
 			for (int q = 0; q < v.nq; ++q)
 			{
 				const double da = v.det[q] * v.w[q];
+				if (c.material == MAT_LINEAR_ELASTICITY)
+				{
+					// LinearElasticity::compute_dstress_dmu_dlambda (LinearElasticity.cpp:290-299):
+					// dP/dmu = grad u + grad u^T, dP/dlambda = tr(grad u) I
+					double imu = 0, tru = 0, trp = 0;
+					for (int i = 0; i < 3; ++i)
+					{
+						tru += gu[q][i][i];
+						trp += gp[q][i][i];
+						for (int j = 0; j < 3; ++j) imu += (gu[q][i][j] + gu[q][j][i]) * gp[q][i][j];
+					}
+					local[tid][el + E] += -imu * da;
+					local[tid][el] += -(tru * trp) * da;
+					continue;
+				}
 				M3 F;
 				for (int i = 0; i < 3; ++i)
 					for (int j = 0; j < 3; ++j) F.a[i][j] = (i == j ? 1.0 : 0.0) + gu[q][i][j];
@@ -1352,12 +1367,50 @@ static void shape_vjp_impl(Context &c, const double *x, const double *adj, doubl
 			interp_grad<N>(v, x, gu);
 			interp_grad<N>(v, adj, gp);
 			const double lambda = c.lambda[el], mu = c.mu[el];
+			double prm[4];
+			c.params(el, prm);
 			for (int q = 0; q < v.nq; ++q)
 			{
 				const double da = v.det[q] * v.w[q];
 				M3 F;
 				for (int i = 0; i < 3; ++i)
 					for (int j = 0; j < 3; ++j) F.a[i][j] = (i == j ? 1.0 : 0.0) + gu[q][i][j];
+				if (c.material)
+				{
+					// the other formulations: P = dpsi/dF and C = d2psi/dF2 by dual numbers over F,
+					// then compute_stress_grad_multiply_mat's C : (grad u V), as GenericElastic
+					// evaluates it (GenericElastic.cpp:613-690)
+					D2 Fd[3][3];
+					for (int r = 0; r < 3; ++r)
+						for (int cc = 0; cc < 3; ++cc) Fd[r][cc] = D2::var(F.a[r][cc], 3 * r + cc);
+					const D2 psi = psi_material(c.material, Fd, prm);
+					for (int vi = 0; vi < v.ng; ++vi)
+						for (int d = 0; d < 3; ++d)
+						{
+							double V[3][3] = {}, Mm[3][3];
+							for (int k = 0; k < 3; ++k) V[d][k] = v.ggrad_t_m[q][vi][k];
+							for (int i = 0; i < 3; ++i)
+								for (int j = 0; j < 3; ++j)
+								{
+									double s2 = 0;
+									for (int k = 0; k < 3; ++k) s2 += gu[q][i][k] * V[k][j];
+									Mm[i][j] = s2;
+								}
+							const double tr = V[0][0] + V[1][1] + V[2][2];
+							double ip = 0;
+							for (int i = 0; i < 3; ++i)
+								for (int j = 0; j < 3; ++j)
+								{
+									double R = 0, PVt = 0;
+									for (int k = 0; k < 3; ++k)
+										for (int l = 0; l < 3; ++l) R += psi.h[3 * i + j][3 * k + l] * Mm[k][l];
+									for (int k = 0; k < 3; ++k) PVt += psi.g[3 * i + k] * V[j][k];
+									ip += (R + PVt - tr * psi.g[3 * i + j]) * gp[q][i][j];
+								}
+							local[tid][(size_t)v.gglobal[vi] * 3 + d] -= ip * da;
+						}
+					continue;
+				}
 				const M3 FmT = transpose(inv3(F));
 				const double lj = std::log(det3(F));
 				M3 P;

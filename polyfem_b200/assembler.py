@@ -269,8 +269,9 @@ class NeoHookeanAssembler:
         "LinearElasticity" use the per-element lambda/mu.  "MooneyRivlin" (c1, c2, k),
         "MooneyRivlin3Param" (c1, c2, c3, d1) and "VolumePenalty" (k) take their
         parameters as keywords, each a scalar or one value per element (host arrays
-        or CUDA tensors).  Every formulation but NeoHookean is assembled in FP64; the
-        adjoint terms stay NeoHookean-only."""
+        or CUDA tensors).  Every formulation but NeoHookean is assembled in FP64.  The
+        material derivative exists for NeoHookean and LinearElasticity, the shape
+        derivative for all but SaintVenant (as in the reference's assemblers)."""
         if formulation not in self.MATERIALS:
             raise ValueError(f"unknown formulation {formulation!r}; one of {sorted(self.MATERIALS)}")
         names = self.MATERIAL_PARAMS.get(formulation, ())

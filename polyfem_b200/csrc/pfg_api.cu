@@ -888,8 +888,10 @@ int pfg_hessian_device_csc(pfg_context *c, const int **outer, const int **inner,
 int pfg_material_vjp(pfg_context *c, const double *u, const double *p, int mem, double *out)
 {
 	if (!c || !check_mem(mem) || (c->m.E && !out) || (c->m.N && (!u || !p))) return fail(c, PFG_ERR_INVALID, "bad arguments");
-	if (c->m.mat != PFG_MAT_NEOHOOKEAN)
-		return fail(c, PFG_ERR_UNSUPPORTED, "the adjoint terms are implemented for NeoHookean only");
+	// compute_dstress_dmu_dlambda exists for NeoHookean and LinearElasticity (and
+	// FixedCorotational, not built); the reference throws for the others
+	if (c->m.mat != PFG_MAT_NEOHOOKEAN && c->m.mat != PFG_MAT_LINEAR_ELASTICITY)
+		return fail(c, PFG_ERR_UNSUPPORTED, "the material derivative exists for NeoHookean and LinearElasticity only");
 	DeviceGuard g(c->device);
 	const size_t ndof = 3 * (size_t)c->m.N;
 	int st = ensure_staging(c, std::max<size_t>(2 * (size_t)c->m.E, 1));
@@ -907,8 +909,11 @@ int pfg_shape_vjp(pfg_context *c, const double *u, const double *p, int mem, int
 {
 	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.Ng && !out) || (c->m.N && (!u || !p)))
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
-	if (c->m.mat != PFG_MAT_NEOHOOKEAN)
-		return fail(c, PFG_ERR_UNSUPPORTED, "the adjoint terms are implemented for NeoHookean only");
+	// compute_stress_grad_multiply_mat exists for every formulation built here but
+	// SaintVenant, whose reference assembler throws
+	if (c->m.mat == PFG_MAT_SAINT_VENANT)
+		return fail(c, PFG_ERR_UNSUPPORTED, "the shape derivative does not exist for SaintVenant");
+	if (int st_m = check_material_prec(c, prec)) return st_m;
 	DeviceGuard g(c->device);
 	const size_t ndof = 3 * (size_t)c->m.N;
 	int st = ensure_staging(c, std::max<size_t>(3 * (size_t)c->m.Ng, 1));

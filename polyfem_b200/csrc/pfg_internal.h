@@ -117,6 +117,12 @@ cudaError_t launch_ad_energy(const DevMesh &m, const double *u, bool per_element
 							 cudaStream_t s);
 cudaError_t launch_ad_gradient_stage(const DevMesh &m, const double *u, const Scratch &sc, cudaStream_t s);
 cudaError_t launch_ad_blocks(const DevMesh &m, const double *u, double *stage, cudaStream_t s);
+// adjoint terms of the other materials: LinearElasticity's material derivative, and the
+// shape derivative's element contributions (one slot per geometric incidence) of
+// IsochoricNeoHookean and materials MAT_FIRST_AD.. (SaintVenant has none in the reference)
+cudaError_t launch_ad_material_vjp(const DevMesh &m, const double *u, const double *adj, double *out, cudaStream_t s);
+cudaError_t launch_ad_shape_vjp_stage(const DevMesh &m, const double *u, const double *adj, const Scratch &sc,
+									  cudaStream_t s);
 cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double *adj, double *out, cudaStream_t s);
 cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out,
 							 const Scratch &sc, cudaStream_t s);

@@ -2229,6 +2229,7 @@ cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double 
 cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double *adj, double *out, cudaStream_t s)
 {
 	if (m.E == 0) return cudaSuccess;
+	if (m.mat != 0) return launch_ad_material_vjp(m, u, adj, out, s);
 	constexpr int NT = 128;
 	const int nb = blocks_for(m.E, NT);
 	switch (m.et)
@@ -2249,13 +2250,19 @@ cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *ad
 	const int nb = blocks_for(m.E, NT);
 	const bool f32 = prec != PREC_FP64;
 	double *st = sc.vec_stage;
-	switch (m.et)
+	if (m.mat != 0)
 	{
-	case 1: f32 ? k_shape_vjp<P1Tet, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<P1Tet, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
-	case 2: f32 ? k_shape_vjp<P2Tet, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<P2Tet, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
-	case 3: f32 ? k_shape_vjp<Q1Hex, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<Q1Hex, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
-	default: return cudaErrorInvalidValue;
+		cudaError_t e = launch_ad_shape_vjp_stage(m, u, adj, sc, s);
+		if (e != cudaSuccess) return e;
 	}
+	else
+		switch (m.et)
+		{
+		case 1: f32 ? k_shape_vjp<P1Tet, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<P1Tet, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
+		case 2: f32 ? k_shape_vjp<P2Tet, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<P2Tet, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
+		case 3: f32 ? k_shape_vjp<Q1Hex, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<Q1Hex, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
+		default: return cudaErrorInvalidValue;
+		}
 	constexpr int NTG = 128;
 	if (m.Ng > 0) k_vec_gather<NTG><<<blocks_for(m.Ng, NTG), NTG, 0, s>>>(m.Ng, m.ginc_off, st, out);
 	return cudaGetLastError();

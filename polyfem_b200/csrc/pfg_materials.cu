@@ -49,6 +49,9 @@ namespace pfg
 {
 
 constexpr int MAT_LINEAR_ELASTICITY = 3, MAT_MOONEY_RIVLIN = 4, MAT_MOONEY_RIVLIN_3PARAM = 5, MAT_VOLUME_PENALTY = 6;
+// IsochoricNeoHookean (hand-derived tangent in pfg_kernels.cu) is also an invariant
+// density; its shape derivative is taken here
+constexpr int MAT_ISO_NEOHOOKEAN = 1;
 
 // ---------------------------------------------------------------------------
 // forward-mode numbers
@@ -111,7 +114,9 @@ __device__ __forceinline__ S sq(S x) { return x * x; }
 template <int MAT, class S>
 __device__ __forceinline__ S inv_psi(S I1, S I2, S J, const double4 &p)
 {
-	if constexpr (MAT == MAT_VOLUME_PENALTY)
+	if constexpr (MAT == MAT_ISO_NEOHOOKEAN) // psi = mu/2 (J^-2/3 I1 - 3), IsochoricNeoHookean.hpp:19-33
+		return (0.5 * p.y) * (ad_pow(J, -2.0 / 3.0) * I1 - 3.0);
+	else if constexpr (MAT == MAT_VOLUME_PENALTY)
 		return (0.5 * p.x) * (0.5 * (sq(J) - 1.0) - ad_log(J));
 	else
 	{
@@ -174,7 +179,7 @@ __device__ __forceinline__ void inv_psi_first(const Invariants &v, const double4
 template <int MAT>
 __device__ __forceinline__ double4 ad_params(const DevMesh &m, int e)
 {
-	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
+	if constexpr (MAT == MAT_LINEAR_ELASTICITY || MAT == MAT_ISO_NEOHOOKEAN)
 	{
 		const double2 lm = __ldg(m.lame + e);
 		return make_double4(lm.x, lm.y, 0.0, 0.0);
@@ -543,6 +548,186 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 }
 
 // ---------------------------------------------------------------------------
+// adjoint terms (ElasticForceDerivative.cpp:35-132, 134-260)
+// ---------------------------------------------------------------------------
+// The invariants and dx/dF of F, generic in the number type: with F + eps W in
+// first-order dual numbers they carry their directional derivatives along W.
+template <class S>
+__device__ __forceinline__ void stress_invariants(const S F[3][3], S &I1, S &I2, S &J, S dx[3][9])
+{
+	S B[3][3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) B[r][c] = F[r][0] * F[c][0] + F[r][1] * F[c][1] + F[r][2] * F[c][2];
+	I1 = B[0][0] + B[1][1] + B[2][2];
+	const S trB2 = sq(B[0][0]) + sq(B[1][1]) + sq(B[2][2]) + 2.0 * (sq(B[0][1]) + sq(B[0][2]) + sq(B[1][2]));
+	I2 = 0.5 * (sq(I1) - trB2);
+	J = det3(F);
+	S cof[3][3];
+	cofactor3(F, cof);
+#pragma unroll
+	for (int a = 0; a < 3; ++a)
+#pragma unroll
+		for (int A = 0; A < 3; ++A)
+		{
+			dx[0][3 * a + A] = 2.0 * F[a][A];
+			dx[1][3 * a + A] = 2.0 * (I1 * F[a][A] - (B[a][0] * F[0][A] + B[a][1] * F[1][A] + B[a][2] * F[2][A]));
+			dx[2][3 * a + A] = cof[a][A];
+		}
+}
+
+// P = dpsi/dF and Q = C : W = dP/dF[W], the stress's directional derivative along W
+// (compute_stress_grad_multiply_mat with mat = W): P = sum_x psi_x dx/dF and
+// Q = sum_x (psi_x' dx/dF + psi_x (dx/dF)'), with ' the derivative along W; psi_x and
+// psi_x' = sum_y psi_xy y' come from one hyper-dual evaluation per invariant x.
+template <int MAT>
+__device__ __forceinline__ void stress_and_directional(const double F[3][3], const double W[3][3], const double4 &p,
+													   double P[9], double Q[9])
+{
+	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
+	{
+		const double trG = F[0][0] + F[1][1] + F[2][2] - 3.0, trW = W[0][0] + W[1][1] + W[2][2];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+			{
+				P[3 * r + c] = p.y * ((F[r][c] - (r == c)) + (F[c][r] - (r == c))) + (r == c ? p.x * trG : 0.0);
+				Q[3 * r + c] = p.y * (W[r][c] + W[c][r]) + (r == c ? p.x * trW : 0.0);
+			}
+	}
+	else
+	{
+		Dual1 Fd[3][3], I1, I2, J, dx[3][9];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) Fd[r][c] = {F[r][c], W[r][c]};
+		stress_invariants(Fd, I1, I2, J, dx);
+#pragma unroll
+		for (int i = 0; i < 9; ++i) P[i] = Q[i] = 0.0;
+#pragma unroll
+		for (int x = 0; x < 3; ++x)
+		{
+			const HDual h = inv_psi<MAT, HDual>({I1.v, x == 0 ? 1.0 : 0.0, I1.d, 0.0}, {I2.v, x == 1 ? 1.0 : 0.0, I2.d, 0.0},
+												{J.v, x == 2 ? 1.0 : 0.0, J.d, 0.0}, p);
+#pragma unroll
+			for (int i = 0; i < 9; ++i)
+			{
+				P[i] += h.a * dx[x][i].v;
+				Q[i] += h.ab * dx[x][i].v + h.a * dx[x][i].d;
+			}
+		}
+	}
+}
+
+// LinearElasticity's material derivative: dP/dmu = grad u + grad u^T, dP/dlambda =
+// tr(grad u) I (LinearElasticity.cpp:290-299); out = [lambda block; mu block], each
+// -sum_q da dP:grad p
+template <class EL, int NT>
+__global__ void __launch_bounds__(NT) k_le_material_vjp(DevMesh m, const double *__restrict__ u,
+														const double *__restrict__ adj, double *__restrict__ out)
+{
+	const int e = blockIdx.x * NT + threadIdx.x;
+	if (e >= m.E) return;
+	double Xg[EL::NG][3], U[EL::N][3], Pn[EL::N][3];
+	int nodes[EL::N];
+	load_geom<EL, double>(m, e, Xg);
+	load_nodal<EL, double>(m, e, u, U, nodes);
+	load_nodal<EL, double>(m, e, adj, Pn, nodes);
+	double tl = 0.0, tm = 0.0;
+#pragma unroll
+	for (int q = 0; q < EL::NQ; ++q)
+	{
+		double Jit[3][3], detJ, gphi[EL::N][3], Gu[3][3], Gp[3][3];
+		geometry<EL, double>(q, Xg, Jit, detJ);
+		phys_grads<EL, double>(q, Jit, gphi);
+		disp_grad<EL, double>(U, gphi, Gu);
+		disp_grad<EL, double>(Pn, gphi, Gp);
+		double imu = 0.0;
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) imu += (Gu[r][c] + Gu[c][r]) * Gp[r][c];
+		const double da = detJ * qweight<EL>(q);
+		tl -= (Gu[0][0] + Gu[1][1] + Gu[2][2]) * (Gp[0][0] + Gp[1][1] + Gp[2][2]) * da;
+		tm -= imu * da;
+	}
+	out[e] = tl;
+	out[(size_t)m.E + e] = tm;
+}
+
+// Shape derivative (ElasticForceDerivative.cpp:207-260): for the rank-one V = e_d (x) g,
+// g the physical gradient of geometric basis function v, and M = grad u V,
+//   (C:M + P V^T - tr(V) P) : grad p = a.(Q g) + (P g).grad p[:, d] - g_d (P : grad p),
+// with a = grad u[:, d] and Q = C : grad p (C is symmetric in its index pairs).
+// Element contributions into one slot per geometric incidence.
+template <class EL, int MAT, int NT>
+__global__ void __launch_bounds__(NT) k_ad_shape_vjp(DevMesh m, const double *__restrict__ u,
+													 const double *__restrict__ adj, double *__restrict__ stage)
+{
+	const int e = blockIdx.x * NT + threadIdx.x;
+	if (e >= m.E) return;
+	double Xg[EL::NG][3], U[EL::N][3], Pn[EL::N][3], acc[EL::NG][3];
+	int nodes[EL::N];
+	load_geom<EL, double>(m, e, Xg);
+	load_nodal<EL, double>(m, e, u, U, nodes);
+	load_nodal<EL, double>(m, e, adj, Pn, nodes);
+	const double4 prm = ad_params<MAT>(m, e);
+#pragma unroll
+	for (int j = 0; j < EL::NG; ++j) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
+#pragma unroll 1
+	for (int q = 0; q < EL::NQ; ++q)
+	{
+		double Jit[3][3], detJ, gphi[EL::N][3], Gu[3][3], Gp[3][3], F[3][3], P[9], Q[9];
+		geometry<EL, double>(q, Xg, Jit, detJ);
+		phys_grads<EL, double>(q, Jit, gphi);
+		disp_grad<EL, double>(U, gphi, Gu);
+		disp_grad<EL, double>(Pn, gphi, Gp);
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) F[r][c] = Gu[r][c] + (r == c ? 1.0 : 0.0);
+		stress_and_directional<MAT>(F, Gp, prm, P, Q);
+		double PGp = 0.0;
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) PGp += P[3 * r + c] * Gp[r][c];
+		const double da = detJ * qweight<EL>(q);
+#pragma unroll
+		for (int v = 0; v < EL::NG; ++v)
+		{
+			double g[3];
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+				g[c] = ggref<EL>(q, v, 0) * Jit[0][c] + ggref<EL>(q, v, 1) * Jit[1][c] + ggref<EL>(q, v, 2) * Jit[2][c];
+			double Qg[3], Pg[3];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+			{
+				Qg[r] = Q[3 * r] * g[0] + Q[3 * r + 1] * g[1] + Q[3 * r + 2] * g[2];
+				Pg[r] = P[3 * r] * g[0] + P[3 * r + 1] * g[1] + P[3 * r + 2] * g[2];
+			}
+#pragma unroll
+			for (int d = 0; d < 3; ++d)
+			{
+				const double t = Gu[0][d] * Qg[0] + Gu[1][d] * Qg[1] + Gu[2][d] * Qg[2] + Pg[0] * Gp[0][d] +
+								 Pg[1] * Gp[1][d] + Pg[2] * Gp[2][d] - g[d] * PGp;
+				acc[v][d] -= t * da;
+			}
+		}
+	}
+#pragma unroll
+	for (int v = 0; v < EL::NG; ++v)
+	{
+		const int k = __ldg(m.g_eb_inc + (size_t)e * EL::NG + v);
+		st_slot(stage + (size_t)k * 4, acc[v][0], acc[v][1], acc[v][2]);
+	}
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 static inline int ad_blocks_for(int n, int nt) { return (n + nt - 1) / nt; }
@@ -611,6 +796,54 @@ cudaError_t launch_ad_blocks(const DevMesh &m, const double *u, double *stage, c
 		k_ad_blocks<EL, MAT, WPB><<<nb, WPB * 32, bytes, s>>>(m, u, stage);
 	});
 	return err != cudaSuccess ? err : st;
+}
+
+
+cudaError_t launch_ad_material_vjp(const DevMesh &m, const double *u, const double *adj, double *out, cudaStream_t s)
+{
+	if (m.E == 0) return cudaSuccess;
+	if (m.mat != MAT_LINEAR_ELASTICITY) return cudaErrorInvalidValue;
+	constexpr int NT = 128;
+	const int nb = ad_blocks_for(m.E, NT);
+	switch (m.et)
+	{
+	case 1: k_le_material_vjp<P1Tet, NT><<<nb, NT, 0, s>>>(m, u, adj, out); break;
+	case 2: k_le_material_vjp<P2Tet, NT><<<nb, NT, 0, s>>>(m, u, adj, out); break;
+	case 3: k_le_material_vjp<Q1Hex, NT><<<nb, NT, 0, s>>>(m, u, adj, out); break;
+	default: return cudaErrorInvalidValue;
+	}
+	return cudaGetLastError();
+}
+
+cudaError_t launch_ad_shape_vjp_stage(const DevMesh &m, const double *u, const double *adj, const Scratch &sc,
+									  cudaStream_t s)
+{
+	if (m.E == 0) return cudaSuccess;
+	constexpr int NT = 128;
+	const int nb = ad_blocks_for(m.E, NT);
+	auto launch = [&](auto el, auto mat) {
+		using EL = decltype(el);
+		k_ad_shape_vjp<EL, decltype(mat)::value, NT><<<nb, NT, 0, s>>>(m, u, adj, sc.vec_stage);
+	};
+	auto by_el = [&](auto mat) -> cudaError_t {
+		switch (m.et)
+		{
+		case 1: launch(P1Tet{}, mat); break;
+		case 2: launch(P2Tet{}, mat); break;
+		case 3: launch(Q1Hex{}, mat); break;
+		default: return cudaErrorInvalidValue;
+		}
+		return cudaGetLastError();
+	};
+	switch (m.mat)
+	{
+	case MAT_ISO_NEOHOOKEAN: return by_el(std::integral_constant<int, MAT_ISO_NEOHOOKEAN>{});
+	case MAT_LINEAR_ELASTICITY: return by_el(std::integral_constant<int, MAT_LINEAR_ELASTICITY>{});
+	case MAT_MOONEY_RIVLIN: return by_el(std::integral_constant<int, MAT_MOONEY_RIVLIN>{});
+	case MAT_MOONEY_RIVLIN_3PARAM: return by_el(std::integral_constant<int, MAT_MOONEY_RIVLIN_3PARAM>{});
+	case MAT_VOLUME_PENALTY: return by_el(std::integral_constant<int, MAT_VOLUME_PENALTY>{});
+	}
+	return cudaErrorInvalidValue;
 }
 
 } // namespace pfg

@@ -134,3 +134,55 @@ def test_inverted_element(require_gpu, mat):
     assert rel_err(g[~np.isnan(g_o)], g_o[~np.isnan(g_o)]) <= 1e-12
     assert asm.inverted_count() >= 1
     asm.close()
+
+
+SHAPE_MATS = ["IsochoricNeoHookean", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty"]
+
+
+@pytest.mark.parametrize("mat", SHAPE_MATS)
+@pytest.mark.parametrize("et,g", ELEMS, ids=["P1", "P2", "Q1"])
+def test_shape_vjp_matches_oracle(require_gpu, mat, et, g):
+    """force_shape_derivative for the formulations whose reference assembler has
+    compute_stress_grad_multiply_mat: the stress and its directional derivative along
+    grad p from hyper-dual numbers over the invariants (closed form for LinearElasticity)."""
+    mesh, lam, mu, u, p = make_case(et, g, seed=11, jitter=0.1 if et != M.P1_TET else 0.0, disp_scale=0.05)
+    prm = material_params(mat, mesh.n_elements, seed=11)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    asm.set_material(mat, **prm)
+    orc = Oracle(mesh, lam, mu, material=mat, params=prm)
+    t = asm.force_shape_derivative(u, p)
+    assert rel_err(t, orc.shape_vjp(u, p)) <= 1e-11
+    assert np.array_equal(t, asm.force_shape_derivative(u, p))  # deterministic
+    asm.close()
+
+
+@pytest.mark.parametrize("et,g", ELEMS, ids=["P1", "P2", "Q1"])
+def test_linear_elasticity_material_vjp_matches_oracle(require_gpu, et, g):
+    mesh, lam, mu, u, p = make_case(et, g, seed=12, jitter=0.1 if et != M.P1_TET else 0.0)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    asm.set_material("LinearElasticity")
+    orc = Oracle(mesh, lam, mu, material="LinearElasticity")
+    assert rel_err(asm.force_material_derivative(u, p), orc.material_vjp(u, p)) <= 1e-12
+    asm.close()
+
+
+def test_adjoint_terms_the_reference_lacks(require_gpu):
+    """The reference throws for the material derivative of the GenericElastic materials
+    and for SaintVenant's shape derivative: PFG_ERR_UNSUPPORTED here; FP32 shape terms
+    stay NeoHookean-only."""
+    mesh, lam, mu, u, p = make_case(M.P1_TET, 2, seed=13)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    for mat in ("IsochoricNeoHookean", "SaintVenant", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty"):
+        asm.set_material(mat, **material_params(mat, mesh.n_elements))
+        with pytest.raises(PfgError) as ei:
+            asm.force_material_derivative(u, p)
+        assert ei.value.status == 4
+    asm.set_material("SaintVenant")
+    with pytest.raises(PfgError) as ei:
+        asm.force_shape_derivative(u, p)
+    assert ei.value.status == 4
+    asm.set_material("LinearElasticity")
+    with pytest.raises(PfgError) as ei:
+        asm.force_shape_derivative(u, p, "fp32")
+    assert ei.value.status == 4
+    asm.close()

@@ -157,3 +157,54 @@ def test_oracle_p1_mass_closed_form():
         vol = np.linalg.det(np.stack([Xe[1] - Xe[0], Xe[2] - Xe[0], Xe[3] - Xe[0]], 1)) / 6
         ref[np.ix_(mesh.conn[e], mesh.conn[e])] += rho[e] * vol * (np.ones((4, 4)) + np.eye(4)) / 20
     assert np.abs(Mx - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+# ----------------------------------------------------------- adjoint terms
+SHAPE_MATS = ["IsochoricNeoHookean", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty"]
+
+
+def _moved(mesh, v, d, h):
+    import copy
+    m2 = copy.copy(mesh)
+    m2.X = mesh.X.copy()
+    m2.X[v, d] += h
+    return m2
+
+
+@pytest.mark.parametrize("mat", SHAPE_MATS)
+@pytest.mark.parametrize("et,name", [(M.P2_TET, "P2"), (M.Q1_HEX, "Q1")], ids=["P2", "Q1"])
+def test_shape_vjp_finite_differences_other_materials(mat, et, name):
+    """term[3v+d] = p . df/dX_{v,d}, with P and C:(grad u V) from the material's dual
+    numbers (GenericElastic / LinearElasticity compute_stress_grad_multiply_mat)."""
+    mesh, lam, mu, u, p = make_case(et, 2, seed=10, jitter=0.1, disp_scale=0.05)
+    prm = material_params(mat, mesh.n_elements, seed=10)
+    orc = Oracle(mesh, lam, mu, material=mat, params=prm)
+    term = orc.shape_vjp(u, p)
+    rng = np.random.default_rng(1)
+    for v in rng.choice(mesh.n_geom_nodes, 4, replace=False):
+        for d in range(3):
+            h = 1e-5 * mesh.h  # between the O(h^2) truncation (8e-6 at 1e-4 h) and rounding (3e-6 at 1e-6 h)
+            fp = Oracle(_moved(mesh, v, d, h), lam, mu, material=mat, params=prm).gradient(u) @ p
+            fm = Oracle(_moved(mesh, v, d, -h), lam, mu, material=mat, params=prm).gradient(u) @ p
+            fd = (fp - fm) / (2 * h)
+            assert abs(term[3 * v + d] - fd) <= 1e-6 * max(abs(fd), 1.0), (mat, v, d, term[3 * v + d], fd)
+
+
+def test_linear_elasticity_material_vjp_finite_differences():
+    """LinearElasticity's term[e] = -p . df/dlambda_e, term[E+e] = -p . df/dmu_e."""
+    mesh, lam, mu, u, p = make_case(M.P2_TET, 2, seed=8)
+    orc = Oracle(mesh, lam, mu, material="LinearElasticity")
+    term = orc.material_vjp(u, p)
+    E = mesh.n_elements
+    for e in (0, E // 2, E - 1):
+        for which, arr in ((0, lam), (1, mu)):
+            h = 1e-6 * arr[e]
+            ap, am = arr.copy(), arr.copy()
+            ap[e] += h
+            am[e] -= h
+            lp, mp = (ap, mu) if which == 0 else (lam, ap)
+            lm, mm = (am, mu) if which == 0 else (lam, am)
+            fp = Oracle(mesh, lp, mp, material="LinearElasticity").gradient(u) @ p
+            fm = Oracle(mesh, lm, mm, material="LinearElasticity").gradient(u) @ p
+            fd = (fp - fm) / (2 * h)
+            assert abs(-term[e + which * E] - fd) <= 1e-6 * max(abs(fd), 1e-12) + 1e-9
