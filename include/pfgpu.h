@@ -263,6 +263,19 @@ int pfg_reduced_to_full(pfg_context *ctx, const double *y, const double *x_bc, i
 int pfg_mass_matrix(pfg_context *ctx, const double *rho, int mem, double *values);
 
 /* ---------------------------------------------------------------------------
+ * Row-sum lumping: polyfem::utils::lump_matrix (utils/MatrixUtils.cpp:84-101),
+ * which BCLagrangianForm applies to the mass matrix (solver/forms/lagrangian/
+ * BCLagrangianForm.cpp:68) and State to the mass matrix when
+ * solver.advanced.lump_mass_matrix is set (State.cpp:1542-1544).
+ * diag[r] = sum_k M(r, k), summed in ascending column order as the reference's
+ * setFromTriplets sums the duplicates of (r, r): the diagonal of the lumped
+ * matrix (every row has an entry, so the diagonal is dense).
+ * values: nnz doubles in the Hessian pattern (e.g. pfg_mass_matrix output) in
+ * `mem`; diag: 3N doubles in `mem`.  FP64.  Host-mode calls stage the values
+ * in the buffer host-mode pfg_mass_matrix calls use. */
+int pfg_lump_matrix(pfg_context *ctx, const double *values, int mem, double *diag);
+
+/* ---------------------------------------------------------------------------
  * Linear solve on the device.  After every assembly NewtonMethod hands the
  * Hessian to its linear solver through polysolve's linear::Solver
  * (analyze_pattern, factorize, solve; called from solver/NLProblem.cpp:261-262,

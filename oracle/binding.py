@@ -282,6 +282,26 @@ def reduced_to_full(y, x_bc, constrained):
     return x
 
 
+def lump_matrix(outer, inner, values):
+    """polyfem::utils::lump_matrix (utils/MatrixUtils.cpp:84-101), restated: every
+    stored (row, value) of the ColMajor CSC matrix, column by column, becomes the
+    triplet (row, row, value), and Eigen's setFromTriplets sums the duplicates of
+    one (row, row) in insertion order starting from the first value (ascending
+    column).  Returns the diagonal (0 where a row has no entry)."""
+    outer = np.asarray(outer, dtype=np.int64)
+    inner = np.asarray(inner, dtype=np.int64)
+    values = np.asarray(values, dtype=np.float64)
+    n = len(outer) - 1
+    diag = np.zeros(n, dtype=np.float64)
+    seen = np.zeros(n, dtype=bool)
+    for k in range(n):
+        rows = inner[outer[k]:outer[k + 1]]  # unique within a column
+        v = values[outer[k]:outer[k + 1]]
+        diag[rows] = np.where(seen[rows], diag[rows] + v, v)
+        seen[rows] = True
+    return diag
+
+
 def conjugate_gradient(outer, inner, values, b, tol, max_iter, x0=None):
     """Eigen 3.4's ConjugateGradient<SparseMatrix, Lower|Upper, DiagonalPreconditioner>
     (the "Eigen::ConjugateGradient" choice of polysolve's linear::Solver, which

@@ -248,6 +248,22 @@ class NeoHookeanAssembler:
               "pfg_mass_matrix")
         return out
 
+    def lump_matrix(self, values):
+        """utils::lump_matrix (utils/MatrixUtils.cpp:84-101) of a matrix in the Hessian
+        pattern: the dense diagonal of its row sums (3N doubles), each summed in
+        ascending column order.  numpy in, numpy out; a CUDA tensor gives a CUDA tensor."""
+        self._check_len(values, self.hessian_nnz(), "values")
+        mem, ptrs, keep = self._prepare(values)
+        out, optr = self._alloc(mem, self.n_dofs)
+        check(lib().pfg_lump_matrix(self._h, ptrs[0], mem, optr), self._h, "pfg_lump_matrix")
+        return out
+
+    def assemble_lumped_mass(self, rho=None):
+        """The lumped mass matrix's diagonal, lump_matrix(mass), as BCLagrangianForm
+        builds it (BCLagrangianForm.cpp:68) and State does for
+        solver.advanced.lump_mass_matrix (State.cpp:1542-1544)."""
+        return self.lump_matrix(self.assemble_mass_matrix_values(rho))
+
     def assemble_mass_matrix(self, rho=None):
         """The mass matrix as scipy CSC (host)."""
         import scipy.sparse as sp

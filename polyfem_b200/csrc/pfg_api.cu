@@ -69,6 +69,8 @@ struct pfg_context
 	size_t cg_n = 0;
 	// mass matrix (pfg_mass_matrix): values for host-mode calls, staged densities
 	double *d_mass = nullptr, *d_rho = nullptr;
+	// lumped diagonal for host-mode pfg_lump_matrix calls (3N doubles)
+	double *d_lump = nullptr;
 	// parameters of the automatically differentiated materials (pfg_set_material_params):
 	// one zero-padded double4 per element; n_mpar = the count last set (0: none)
 	double4 *d_mpar = nullptr;
@@ -524,6 +526,7 @@ void free_all(pfg_context *c)
 	if (c->d_cg) cudaFree(c->d_cg);
 	if (c->h_cg_sc) cudaFreeHost(c->h_cg_sc);
 	if (c->d_mass) cudaFree(c->d_mass);
+	if (c->d_lump) cudaFree(c->d_lump);
 	if (c->d_rho) cudaFree(c->d_rho);
 	if (c->d_mpar) cudaFree(c->d_mpar);
 }
@@ -1055,6 +1058,30 @@ int pfg_mass_matrix(pfg_context *c, const double *rho, int mem, double *values)
 		p.values = values;
 	PFG_CUDA(c, launch_mass(c->m, p, drho, c->d_hess_stage[0], c->stream));
 	if (mem == PFG_MEM_HOST) return finish_host(c, values, c->d_mass, c->pat.nnz);
+	return PFG_OK;
+}
+
+int pfg_lump_matrix(pfg_context *c, const double *values, int mem, double *diag)
+{
+	if (!c || !check_mem(mem) || !values || !diag) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	DeviceGuard g(c->device);
+	int st;
+	if (!c->has_pattern && (st = build_pattern(c))) return st;
+	const long long nnz = c->pat.nnz;
+	const int ndof = 3 * c->m.N;
+	const double *dv = values;
+	double *dd = diag;
+	if (mem == PFG_MEM_HOST)
+	{
+		// host values go through the mass matrix's host staging buffer (nnz doubles)
+		if (!c->d_mass) PFG_CUDA(c, cudaMalloc(&c->d_mass, sizeof(double) * std::max<long long>(nnz, 1)));
+		if (!c->d_lump) PFG_CUDA(c, cudaMalloc(&c->d_lump, sizeof(double) * std::max(ndof, 1)));
+		if (nnz) PFG_CUDA(c, cudaMemcpyAsync(c->d_mass, values, sizeof(double) * nnz, cudaMemcpyHostToDevice, c->stream));
+		dv = c->d_mass;
+		dd = c->d_lump;
+	}
+	PFG_CUDA(c, launch_lump_rows(c->m.N, c->d_outer, c->d_inner, dv, dd, c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, diag, c->d_lump, ndof);
 	return PFG_OK;
 }
 

@@ -104,6 +104,10 @@ cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *
 // Mass matrix values (nnz of the Hessian pattern) into p.values; rho = per-element
 // density (device, E doubles) or NULL for 1; stage as for the FP64 Hessian
 cudaError_t launch_mass(const DevMesh &m, const DevPattern &p, const double *rho, void *stage, cudaStream_t s);
+// utils::lump_matrix: diag (3 * n_nodes) = row sums of the values in the Hessian
+// pattern (outer, inner), each summed in ascending column order
+cudaError_t launch_lump_rows(int n_nodes, const int *outer, const int *inner, const double *vals, double *diag,
+							 cudaStream_t s);
 // Dirichlet reduction helpers: dof maps of the free dofs (old_to_new[dof] = index
 // among the free dofs or -1, free[i] = dof of the i-th free dof)
 cudaError_t launch_gather_free(const double *full, const int *free, int n_free, double *out, cudaStream_t s);

@@ -2288,6 +2288,59 @@ __global__ void k_reduced_to_full(const double *__restrict__ y, const double *__
 	x[i] = k >= 0 ? __ldg(y + k) : (x_bc ? __ldg(x_bc + i) : 0.0);
 }
 
+// ---------------------------------------------------------------------------
+// utils::lump_matrix (utils/MatrixUtils.cpp:84-101): diag[r] = sum_k M(r, k).  The
+// reference walks the CSC column by column and hands every (row, value) to
+// setFromTriplets as a diagonal triplet, which sums the duplicates of row r in
+// insertion order starting from the first value: ascending column k.  One thread
+// per row r = 3A + m reads row r across the columns 3B + c of every neighbour node
+// B of A, ascending, through the node-block pattern: in column 3B + c, row r sits
+// at outer[3B + c] + 3 rank_B(A) + m, rank_B(A) found by binary search in B's
+// neighbour list (rows 3 * rank of column 3B).  The pattern is structurally
+// symmetric, so A is always in B's list.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_lump_rows(int n_nodes, const int *__restrict__ outer,
+												   const int *__restrict__ inner, const double *__restrict__ vals,
+												   double *__restrict__ diag)
+{
+	const int r = blockIdx.x * blockDim.x + threadIdx.x;
+	if (r >= 3 * n_nodes) return;
+	const int A = r / 3, m = r - 3 * A;
+	const int oA = __ldg(outer + 3 * A), degA = (__ldg(outer + 3 * A + 1) - oA) / 3;
+	double s = 0.0;
+	bool first = true;
+	for (int i = 0; i < degA; ++i)
+	{
+		const int B = __ldg(inner + oA + 3 * i) / 3;
+		const int oB = __ldg(outer + 3 * B), degB = (__ldg(outer + 3 * B + 1) - oB) / 3;
+		int lo = 0, hi = degB - 1;
+		while (lo < hi)
+		{
+			const int mid = (lo + hi) >> 1;
+			if (__ldg(inner + oB + 3 * mid) / 3 < A)
+				lo = mid + 1;
+			else
+				hi = mid;
+		}
+#pragma unroll
+		for (int c = 0; c < 3; ++c)
+		{
+			const double v = __ldg(vals + __ldg(outer + 3 * B + c) + 3 * lo + m);
+			s = first ? v : s + v;
+			first = false;
+		}
+	}
+	diag[r] = s;
+}
+
+cudaError_t launch_lump_rows(int n_nodes, const int *outer, const int *inner, const double *vals, double *diag,
+							 cudaStream_t s)
+{
+	const int n = 3 * n_nodes;
+	if (n > 0) k_lump_rows<<<(n + 255) / 256, 256, 0, s>>>(n_nodes, outer, inner, vals, diag);
+	return cudaGetLastError();
+}
+
 cudaError_t launch_gather_free(const double *full, const int *free, int n_free, double *out, cudaStream_t s)
 {
 	if (n_free > 0) k_gather_free<<<(n_free + 255) / 256, 256, 0, s>>>(full, free, n_free, out);

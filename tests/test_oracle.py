@@ -52,6 +52,26 @@ def test_sparse_matrix_cache_known_answer():
     assert [cache2.coeff(0, 0), cache2.coeff(0, 1), cache2.coeff(9, 4), cache2.coeff(9, 9)] == [1, 2, 6, 4]
 
 
+def test_lump_matrix_known_answer():
+    """utils::lump_matrix (utils/MatrixUtils.cpp:84-101) restated: row sums in
+    ascending column order, starting from the first value (setFromTriplets)."""
+    from oracle.binding import lump_matrix
+    # row 0 holds 1e16, 1, -1e16 in columns 0, 1, 2: (1e16 + 1) - 1e16 == 0 in FP64,
+    # while the column-2-first order would give 1
+    A = sp.csc_matrix(np.array([[1e16, 1.0, -1e16, 0.0],
+                                [2.0, 3.0, 0.0, 0.0],
+                                [0.0, 0.0, 0.0, 0.0],
+                                [-0.0, 0.0, 0.0, 5.0]]))
+    A.eliminate_zeros()
+    d = lump_matrix(A.indptr, A.indices, A.data)
+    assert d.tolist() == [0.0, 5.0, 0.0, 5.0]
+    # structurally present zeros are summed like any value
+    d = lump_matrix(np.array([0, 1, 2]), np.array([0, 0]), np.array([-0.0, 2.5]))
+    assert d.tolist() == [2.5, 0.0]
+    B = sp.random(40, 40, density=0.2, random_state=4, format="csc")
+    assert np.allclose(lump_matrix(B.indptr, B.indices, B.data), np.asarray(B.sum(axis=1)).ravel(), rtol=1e-14)
+
+
 # ------------------------------------------------------------------ tables
 def _indep_tables(et):
     """Second, independent reading of the reference tables."""
