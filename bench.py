@@ -533,8 +533,19 @@ def run_suite(args):
         # parameterised ones with (c1, c2, k), (c1, c2, c3, d1), (k) of stress scale mu
         mu_s = float(np.median(mu))
         mpar = {4: [mu_s, 0.5 * mu_s, 10 * mu_s], 5: [mu_s, 0.5 * mu_s, 0.2 * mu_s, 10 * mu_s], 6: [10 * mu_s]}
+        # HookeLinearElasticity and the anisotropic SaintVenant: the isotropic tensor of
+        # (2.333 mu, mu) (nu = 0.35) plus a seeded symmetric positive semi-definite part
+        Ct = np.zeros((6, 6))
+        Ct[:3, :3] = 2.333 * mu_s
+        Ct[[0, 1, 2], [0, 1, 2]] += 2 * mu_s
+        Ct[[3, 4, 5], [3, 4, 5]] = mu_s
+        Rt = np.random.default_rng(7).standard_normal((6, 6))
+        Ct += 0.25 * mu_s * (Rt @ Rt.T) / 6
+        c21 = np.ascontiguousarray(Ct[np.triu_indices(6)])
+        check(L.pfg_set_elasticity_tensor(h, vp(c21.ctypes.data)), h, "pfg_set_elasticity_tensor")
         for mname, mid in (("iso_neohookean", 1), ("saint_venant", 2), ("linear_elasticity", 3),
-                           ("mooney_rivlin", 4), ("mooney_rivlin_3param", 5), ("volume_penalty", 6)):
+                           ("mooney_rivlin", 4), ("mooney_rivlin_3param", 5), ("volume_penalty", 6),
+                           ("hooke", 7), ("saint_venant_tensor", 8)):
             if mid in mpar:
                 pv = np.ascontiguousarray(np.repeat(np.asarray(mpar[mid], dtype=np.float64)[:, None], E, axis=1))
                 check(L.pfg_set_material_params(h, vp(pv.ctypes.data), len(mpar[mid]), 0), h,

@@ -182,14 +182,22 @@ int pfg_version(void);
  *                                 parameters (c1, c2, k);
  *   PFG_MAT_MOONEY_RIVLIN_3PARAM: MooneyRivlin3ParamElasticity
  *                                 (MooneyRivlin3ParamElasticity.hpp:26-49), (c1, c2, c3, d1);
- *   PFG_MAT_VOLUME_PENALTY      : VolumePenalty (VolumePenalty.hpp:20-34), (k).
+ *   PFG_MAT_VOLUME_PENALTY      : VolumePenalty (VolumePenalty.hpp:20-34), (k);
+ *   PFG_MAT_HOOKE               : HookeLinearElasticity (HookeLinearElasticity.cpp:
+ *                                 332-423), psi = 1/2 sigma:eps with the Voigt stress
+ *                                 sigma = C eps of one anisotropic elasticity tensor C
+ *                                 (pfg_set_elasticity_tensor), eps the small strain;
+ *   PFG_MAT_SAINT_VENANT_TENSOR : SaintVenantElasticity with that anisotropic tensor
+ *                                 (SaintVenantElasticity.cpp:209-267), psi = 1/2 S:E,
+ *                                 S = C E in Voigt form, E = (F^T F - I)/2.
  * Energy, gradient and Hessian (with project_psd and the Dirichlet reduction) then
  * follow the chosen material in PFG_FP64 (other precisions return
  * PFG_ERR_UNSUPPORTED).  The adjoint terms follow the reference's assemblers:
  * pfg_material_vjp (compute_dstress_dmu_dlambda) exists for NeoHookean and
  * LinearElasticity (dP/dmu = grad u + grad u^T, dP/dlambda = tr(grad u) I,
  * LinearElasticity.cpp:290-299); pfg_shape_vjp (compute_stress_grad_multiply_mat)
- * for every formulation here but SaintVenant, in PFG_FP64 for all but NeoHookean;
+ * for every formulation here but the two SaintVenant ones and HookeLinearElasticity,
+ * in PFG_FP64 for all but NeoHookean;
  * the others return PFG_ERR_UNSUPPORTED, where the reference throws "Not
  * implemented" (Assembler.hpp:147-156).  Takes effect for the calls that follow;
  * the pattern is unchanged.
@@ -202,9 +210,20 @@ enum pfg_material
 	PFG_MAT_LINEAR_ELASTICITY = 3,
 	PFG_MAT_MOONEY_RIVLIN = 4,
 	PFG_MAT_MOONEY_RIVLIN_3PARAM = 5,
-	PFG_MAT_VOLUME_PENALTY = 6
+	PFG_MAT_VOLUME_PENALTY = 6,
+	PFG_MAT_HOOKE = 7,
+	PFG_MAT_SAINT_VENANT_TENSOR = 8
 };
 int pfg_set_material(pfg_context *ctx, int material);
+
+/* The elasticity tensor of PFG_MAT_HOOKE and PFG_MAT_SAINT_VENANT_TENSOR: ElasticityTensor (assembler/MatParams.cpp:
+ * 91-123, 336-344), a symmetric 6 x 6 matrix over the Voigt strain
+ * (e00, e11, e22, 2 e12, 2 e02, 2 e01), given as its 21 entries C(i, j), i <= j,
+ * row by row: C00 C01 .. C05 C11 .. C15 .. C55 (the order of
+ * ElasticityTensor::set_from_entries with 21 entries).  Host memory; one tensor
+ * per context, as the reference's assembler holds one.  The calls of these two
+ * materials return PFG_ERR_STATE until it is set. */
+int pfg_set_elasticity_tensor(pfg_context *ctx, const double *c21);
 
 /* Per-element parameters of PFG_MAT_MOONEY_RIVLIN (n_params 3: c1, c2, k),
  * PFG_MAT_MOONEY_RIVLIN_3PARAM (4: c1, c2, c3, d1) and PFG_MAT_VOLUME_PENALTY

@@ -40,6 +40,7 @@ def lib():
         L.orc_set_project_psd.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_material.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_material_params.argtypes = [ctypes.c_void_p, _d, ctypes.c_int]
+        L.orc_set_elasticity_tensor.argtypes = [ctypes.c_void_p, _d]
         L.orc_basis_value.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.orc_basis_value.restype = ctypes.c_double
         L.orc_mass.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
@@ -88,7 +89,8 @@ class Oracle:
     """CPU restatement of NLAssembler + ElasticForm + ElasticForceDerivative."""
 
     MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2, "LinearElasticity": 3,
-                 "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6}
+                 "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6, "HookeLinearElasticity": 7,
+                 "SaintVenantTensor": 8}
     MATERIAL_PARAMS = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
                        "VolumePenalty": ("k",)}
 
@@ -109,6 +111,14 @@ class Oracle:
         if not self.h:
             raise RuntimeError("oracle creation failed")
         self.n_dofs = mesh.n_dofs
+        if material in ("HookeLinearElasticity", "SaintVenantTensor"):
+            if set(params or {}) != {"elasticity_tensor"}:
+                raise ValueError(f"{material} takes the parameter elasticity_tensor (21 entries)")
+            self._hooke = np.ascontiguousarray(np.asarray(params["elasticity_tensor"], dtype=np.float64).ravel())
+            if self._hooke.size != 21:
+                raise ValueError("the elasticity tensor takes 21 entries")
+            L.orc_set_elasticity_tensor(self.h, _dp(self._hooke))
+            params = None
         names = self.MATERIAL_PARAMS.get(material, ())
         if set(params or {}) != set(names):
             raise ValueError(f"{material} takes the parameters {list(names)}")

@@ -483,6 +483,9 @@ static void element_hessian(const ElementValues &v, const double *x, double lamb
 //   MAT_MOONEY_RIVLIN_3PARAM: MooneyRivlin3ParamElasticity::elastic_energy
 //                       (MooneyRivlin3ParamElasticity.hpp:26-49)
 //   MAT_VOLUME_PENALTY: VolumePenalty::elastic_energy (VolumePenalty.hpp:20-34)
+//   MAT_HOOKE         : HookeLinearElasticity::compute_energy_aux (HookeLinearElasticity.cpp:
+//                       372-421), one anisotropic tensor (orc_set_elasticity_tensor)
+//   MAT_SAINT_VENANT_TENSOR: SaintVenantElasticity::compute_energy_aux with that tensor
 // The material parameters of an element are prm[0..3]: (lambda, mu) for the first
 // four, the GenericMatParam values for the others (orc_set_material_params).
 // ---------------------------------------------------------------------------
@@ -494,8 +497,12 @@ enum
 	MAT_LINEAR_ELASTICITY = 3,
 	MAT_MOONEY_RIVLIN = 4,
 	MAT_MOONEY_RIVLIN_3PARAM = 5,
-	MAT_VOLUME_PENALTY = 6
+	MAT_VOLUME_PENALTY = 6,
+	MAT_HOOKE = 7,
+	MAT_SAINT_VENANT_TENSOR = 8
 };
+constexpr int PRM_MAX = 21; // material parameters of an element: 21 tensor entries for MAT_HOOKE and
+                            // MAT_SAINT_VENANT_TENSOR
 
 // value, gradient and Hessian with respect to the 9 entries F(r, c) (index 3r + c)
 struct D2
@@ -585,7 +592,21 @@ static S psi_iso_neohookean(const S (&F)[3][3], double, double mu)
 // shears, stress = C eps with C = [2mu+lambda, lambda, lambda; ...; mu, mu, mu],
 // psi = 1/2 tr(stress * strain)
 template <class S>
+static S psi_saint_venant_tensor(const S (&F)[3][3], const double (&C)[6][6]);
+
+template <class S>
 static S psi_saint_venant(const S (&F)[3][3], double lambda, double mu)
+{
+	const double C[6][6] = {{2 * mu + lambda, lambda, lambda, 0, 0, 0}, {lambda, 2 * mu + lambda, lambda, 0, 0, 0},
+							{lambda, lambda, 2 * mu + lambda, 0, 0, 0}, {0, 0, 0, mu, 0, 0},
+							{0, 0, 0, 0, mu, 0},                       {0, 0, 0, 0, 0, mu}};
+	return psi_saint_venant_tensor(F, C);
+}
+
+// SaintVenant with any elasticity tensor C (ElasticityTensor::set_from_entries):
+// the Green strain of the displacement gradient, its Voigt form, stress = C eps
+template <class S>
+static S psi_saint_venant_tensor(const S (&F)[3][3], const double (&C)[6][6])
 {
 	S G[3][3], E[3][3];
 	for (int r = 0; r < 3; ++r)
@@ -598,9 +619,6 @@ static S psi_saint_venant(const S (&F)[3][3], double lambda, double mu)
 			E[r][c] = 0.5 * (gtg + G[r][c] + G[c][r]);
 		}
 	const S eps[6] = {E[0][0], E[1][1], E[2][2], 2.0 * E[1][2], 2.0 * E[0][2], 2.0 * E[0][1]};
-	const double C[6][6] = {{2 * mu + lambda, lambda, lambda, 0, 0, 0}, {lambda, 2 * mu + lambda, lambda, 0, 0, 0},
-							{lambda, lambda, 2 * mu + lambda, 0, 0, 0}, {0, 0, 0, mu, 0, 0},
-							{0, 0, 0, 0, mu, 0},                       {0, 0, 0, 0, 0, mu}};
 	S st[6];
 	for (int j = 0; j < 6; ++j)
 	{
@@ -696,11 +714,48 @@ static S psi_volume_penalty(const S (&F)[3][3], double k)
 	return (k / 2.0) * (0.5 * (J * J - S(1.0)) - dlog(J));
 }
 
+// HookeLinearElasticity::compute_energy_aux (HookeLinearElasticity.cpp:372-421): the
+// small strain of the displacement gradient G = F - I, its Voigt form with doubled
+// shears, stress(j) = sum_k C(j, k) eps[k] (ElasticityTensor::compute_stress,
+// MatParams.cpp:336-344, C(j, k) = C(k, j) read from the upper triangle), and
+// psi = 1/2 tr(stress_tensor * strain).  c21: C(i, j), i <= j, row by row.
+template <class S>
+static S psi_hooke(const S (&F)[3][3], const double *c21)
+{
+	double C[6][6];
+	for (int i = 0, k = 0; i < 6; ++i)
+		for (int j = i; j < 6; ++j, ++k) C[i][j] = C[j][i] = c21[k];
+	S E[3][3];
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c)
+			E[r][c] = 0.5 * ((F[r][c] - S(r == c ? 1.0 : 0.0)) + (F[c][r] - S(c == r ? 1.0 : 0.0)));
+	const S eps[6] = {E[0][0], E[1][1], E[2][2], 2.0 * E[1][2], 2.0 * E[0][2], 2.0 * E[0][1]};
+	S st[6];
+	for (int j = 0; j < 6; ++j)
+	{
+		st[j] = S(0.0);
+		for (int k = 0; k < 6; ++k) st[j] = st[j] + C[j][k] * eps[k];
+	}
+	const S sig[3][3] = {{st[0], st[5], st[4]}, {st[5], st[1], st[3]}, {st[4], st[3], st[2]}};
+	S tr = S(0.0);
+	for (int r = 0; r < 3; ++r)
+		for (int k = 0; k < 3; ++k) tr = tr + sig[r][k] * E[k][r];
+	return 0.5 * tr;
+}
+
 template <class S>
 static S psi_material(int mat, const S (&F)[3][3], const double *prm)
 {
 	switch (mat)
 	{
+	case MAT_HOOKE: return psi_hooke(F, prm);
+	case MAT_SAINT_VENANT_TENSOR:
+	{
+		double C[6][6];
+		for (int i = 0, k = 0; i < 6; ++i)
+			for (int j = i; j < 6; ++j, ++k) C[i][j] = C[j][i] = prm[k];
+		return psi_saint_venant_tensor(F, C);
+	}
 	case MAT_ISO_NEOHOOKEAN: return psi_iso_neohookean(F, prm[0], prm[1]);
 	case MAT_SAINT_VENANT: return psi_saint_venant(F, prm[0], prm[1]);
 	case MAT_LINEAR_ELASTICITY: return psi_linear_elasticity(F, prm[0], prm[1]);
@@ -1022,15 +1077,18 @@ struct Context
 	bool project_psd = false;  // NLAssembler::assemble_hessian(project_to_psd = true)
 	int material = 0;          // MAT_*: the assembler's formulation
 	std::vector<double> mparams; // per-element parameters of the GenericMatParam materials, parameter-major
+	double hooke[PRM_MAX] = {};  // MAT_HOOKE's elasticity tensor, 21 entries C(i, j), i <= j, row by row
 	int n_mparams = 0;
 
 	// the element's material parameters (lambda, mu) or GenericMatParam values
-	void params(int e, double (&prm)[4]) const
+	void params(int e, double (&prm)[PRM_MAX]) const
 	{
+		for (int k = 0; k < PRM_MAX; ++k) prm[k] = 0.0;
 		prm[0] = lambda[e];
 		prm[1] = mu[e];
-		prm[2] = prm[3] = 0.0;
-		if (material >= MAT_MOONEY_RIVLIN)
+		if (material == MAT_HOOKE || material == MAT_SAINT_VENANT_TENSOR)
+			for (int k = 0; k < PRM_MAX; ++k) prm[k] = hooke[k];
+		else if (material >= MAT_MOONEY_RIVLIN)
 			for (int k = 0; k < 4; ++k) prm[k] = k < n_mparams ? mparams[(size_t)k * E + e] : 0.0;
 	}
 	CSC last;                  // last assembled Hessian
@@ -1056,7 +1114,7 @@ static double energy_impl(Context &c, const double *x, double *per_elem)
 		for (int el = s; el < e; ++el)
 		{
 			c.vals(el, v);
-			double prm[4];
+			double prm[PRM_MAX];
 			c.params(el, prm);
 			const double val = c.material ? gen_element_energy<N>(c.material, v, x, prm)
 										  : element_energy<N>(v, x, c.lambda[el], c.mu[el]);
@@ -1084,7 +1142,7 @@ static void gradient_impl(Context &c, const double *x, double *g)
 			c.vals(el, v);
 			if (c.material)
 			{
-				double prm[4];
+				double prm[PRM_MAX];
 				c.params(el, prm);
 				gen_element_derivatives<N>(c.material, v, x, prm, val, nullptr);
 			}
@@ -1255,7 +1313,7 @@ static void hessian_impl(Context &c, const double *x)
 			c.vals(el, v);
 			if (c.material)
 			{
-				double prm[4];
+				double prm[PRM_MAX];
 				c.params(el, prm);
 				gen_element_derivatives<N>(c.material, v, x, prm, nullptr, H.data());
 			}
@@ -1367,7 +1425,7 @@ static void shape_vjp_impl(Context &c, const double *x, const double *adj, doubl
 			interp_grad<N>(v, x, gu);
 			interp_grad<N>(v, adj, gp);
 			const double lambda = c.lambda[el], mu = c.mu[el];
-			double prm[4];
+			double prm[PRM_MAX];
 			c.params(el, prm);
 			for (int q = 0; q < v.nq; ++q)
 			{
@@ -1676,6 +1734,13 @@ extern "C"
 		c.n_mparams = n_params;
 		c.mparams.assign(params, params + (size_t)n_params * c.E);
 	}
+	// HookeLinearElasticity's tensor: 21 entries C(i, j), i <= j, row by row
+	// (ElasticityTensor::set_from_entries, MatParams.cpp:180-205)
+	void orc_set_elasticity_tensor(void *h, const double *c21)
+	{
+		Context &c = *static_cast<Context *>(h);
+		for (int k = 0; k < PRM_MAX; ++k) c.hooke[k] = c21[k];
+	}
 	// ipc::project_to_psd (CLAMP) of one row-major m x m symmetric matrix, in place
 	void orc_project_psd(double *H, int m) { project_to_psd(H, m); }
 
@@ -1753,7 +1818,7 @@ extern "C"
 			constexpr int n = decltype(N)::value;
 			if (c.material)
 			{
-				double prm[4];
+				double prm[PRM_MAX];
 				c.params(e, prm);
 				if (energy) *energy = gen_element_energy<n>(c.material, v, x, prm);
 				if (grad || hess) gen_element_derivatives<n>(c.material, v, x, prm, grad, hess);

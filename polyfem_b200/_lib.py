@@ -115,6 +115,7 @@ SIGNATURES = {
     "pfg_reduced_to_full": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     "pfg_set_material": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pfg_set_material_params": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int]),
+    "pfg_set_elasticity_tensor": (ctypes.c_int, [_vp, _vp]),
     "pfg_mass_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
     "pfg_lump_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
     "pfg_cg_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,

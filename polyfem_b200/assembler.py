@@ -273,7 +273,8 @@ class NeoHookeanAssembler:
 
     # -- material (AssemblerUtils::make_assembler's formulation name) ------------------
     MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2, "LinearElasticity": 3,
-                 "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6}
+                 "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6, "HookeLinearElasticity": 7}
+    SAINT_VENANT_TENSOR = 8  # "SaintVenant" with an elasticity_tensor
     # the GenericMatParam names of the parameterised formulations, in pfg_set_material_params order
     MATERIAL_PARAMS = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
                        "VolumePenalty": ("k",)}
@@ -285,18 +286,49 @@ class NeoHookeanAssembler:
         "LinearElasticity" use the per-element lambda/mu.  "MooneyRivlin" (c1, c2, k),
         "MooneyRivlin3Param" (c1, c2, c3, d1) and "VolumePenalty" (k) take their
         parameters as keywords, each a scalar or one value per element (host arrays
-        or CUDA tensors).  Every formulation but NeoHookean is assembled in FP64.  The
-        material derivative exists for NeoHookean and LinearElasticity, the shape
-        derivative for all but SaintVenant (as in the reference's assemblers)."""
+        or CUDA tensors).  "HookeLinearElasticity" takes ``elasticity_tensor``: the 21
+        entries C(i, j), i <= j, of its 6 x 6 Voigt tensor, row by row (the reference's
+        material key; ``isotropic_elasticity_tensor`` gives the lambda/mu one); so does
+        "SaintVenant" given ``elasticity_tensor``, which is then anisotropic.  Every
+        formulation but NeoHookean is assembled in FP64.  The material derivative exists
+        for NeoHookean and LinearElasticity, the shape derivative for all but SaintVenant
+        and HookeLinearElasticity (as in the reference's assemblers)."""
         if formulation not in self.MATERIALS:
             raise ValueError(f"unknown formulation {formulation!r}; one of {sorted(self.MATERIALS)}")
+        mat_id = self.MATERIALS[formulation]
+        if formulation == "HookeLinearElasticity" or (formulation == "SaintVenant" and params):
+            # SaintVenant with elasticity_tensor: the anisotropic form (PFG_MAT_SAINT_VENANT_TENSOR)
+            if set(params) != {"elasticity_tensor"}:
+                raise ValueError(f"{formulation} takes the parameter elasticity_tensor, got {sorted(params)}")
+            self.set_elasticity_tensor(params["elasticity_tensor"])
+            params = {}
+            if formulation == "SaintVenant":
+                mat_id = self.SAINT_VENANT_TENSOR
         names = self.MATERIAL_PARAMS.get(formulation, ())
         if set(params) != set(names):
             raise ValueError(f"{formulation} takes the parameters {list(names)}, got {sorted(params)}")
         if names:
             self.set_material_params(*(params[n] for n in names))
-        check(lib().pfg_set_material(self._h, self.MATERIALS[formulation]), self._h, "pfg_set_material")
+        check(lib().pfg_set_material(self._h, mat_id), self._h, "pfg_set_material")
         self.material = formulation
+
+    def set_elasticity_tensor(self, c21):
+        """ElasticityTensor::set_from_entries with 21 entries (MatParams.cpp:180-205):
+        C(i, j), i <= j, row by row, over the Voigt strain (e00, e11, e22, 2e12, 2e02, 2e01)."""
+        c = np.ascontiguousarray(np.asarray(c21, dtype=np.float64).ravel())
+        if c.size != 21:
+            raise ValueError("the elasticity tensor takes 21 entries")
+        check(lib().pfg_set_elasticity_tensor(self._h, ctypes.c_void_p(c.ctypes.data)), self._h,
+              "pfg_set_elasticity_tensor")
+
+    @staticmethod
+    def isotropic_elasticity_tensor(lam: float, mu: float):
+        """The 21 entries ElasticityTensor::set_from_lambda_mu sets (MatParams.cpp:211-260)."""
+        C = np.zeros((6, 6))
+        C[:3, :3] = lam
+        C[[0, 1, 2], [0, 1, 2]] = 2 * mu + lam
+        C[[3, 4, 5], [3, 4, 5]] = mu
+        return C[np.triu_indices(6)]
 
     def set_material_params(self, *params):
         """Per-element parameters of the current or next parameterised formulation, in

@@ -75,6 +75,9 @@ struct pfg_context
 	// one zero-padded double4 per element; n_mpar = the count last set (0: none)
 	double4 *d_mpar = nullptr;
 	int n_mpar = 0;
+	// elasticity tensor of HookeLinearElasticity and the anisotropic SaintVenant
+	// (pfg_set_elasticity_tensor): 36 doubles
+	double *d_hooke = nullptr;
 	double *h_cg_sc = nullptr;
 	std::string err;
 };
@@ -163,6 +166,8 @@ int check_material_prec(pfg_context *c, int prec)
 	const int np = material_param_count(c->m.mat);
 	if (np && c->m.E && c->n_mpar != np)
 		return fail(c, PFG_ERR_STATE, "the material's parameters are not set (pfg_set_material_params)");
+	if ((c->m.mat == PFG_MAT_HOOKE || c->m.mat == PFG_MAT_SAINT_VENANT_TENSOR) && !c->d_hooke)
+		return fail(c, PFG_ERR_STATE, "the elasticity tensor is not set (pfg_set_elasticity_tensor)");
 	return PFG_OK;
 }
 int check_prec(int prec) { return prec == PFG_FP64 || prec == PFG_FP32 || prec == PFG_SPLIT32; }
@@ -527,6 +532,7 @@ void free_all(pfg_context *c)
 	if (c->h_cg_sc) cudaFreeHost(c->h_cg_sc);
 	if (c->d_mass) cudaFree(c->d_mass);
 	if (c->d_lump) cudaFree(c->d_lump);
+	if (c->d_hooke) cudaFree(c->d_hooke);
 	if (c->d_rho) cudaFree(c->d_rho);
 	if (c->d_mpar) cudaFree(c->d_mpar);
 }
@@ -701,9 +707,25 @@ int pfg_set_stream(pfg_context *c, void *stream)
 
 int pfg_set_material(pfg_context *c, int material)
 {
-	if (!c || material < PFG_MAT_NEOHOOKEAN || material > PFG_MAT_VOLUME_PENALTY)
+	if (!c || material < PFG_MAT_NEOHOOKEAN || material > PFG_MAT_SAINT_VENANT_TENSOR)
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
 	c->m.mat = material;
+	return PFG_OK;
+}
+
+int pfg_set_elasticity_tensor(pfg_context *c, const double *c21)
+{
+	if (!c || !c21) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	// ElasticityTensor::set_from_entries (MatParams.cpp:180-205): C(i, j), i <= j, row by
+	// row; operator() reads C(j, i) for j < i (MatParams.cpp:103-112)
+	double full[36];
+	for (int i = 0, k = 0; i < 6; ++i)
+		for (int j = i; j < 6; ++j, ++k) full[6 * i + j] = full[6 * j + i] = c21[k];
+	DeviceGuard g(c->device);
+	if (!c->d_hooke) PFG_CUDA(c, cudaMalloc(&c->d_hooke, sizeof(full)));
+	PFG_CUDA(c, cudaMemcpyAsync(c->d_hooke, full, sizeof(full), cudaMemcpyHostToDevice, c->stream));
+	PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	c->m.hooke = c->d_hooke;
 	return PFG_OK;
 }
 
@@ -913,9 +935,9 @@ int pfg_shape_vjp(pfg_context *c, const double *u, const double *p, int mem, int
 	if (!c || !check_mem(mem) || !check_prec(prec) || (c->m.Ng && !out) || (c->m.N && (!u || !p)))
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
 	// compute_stress_grad_multiply_mat exists for every formulation built here but
-	// SaintVenant, whose reference assembler throws
-	if (c->m.mat == PFG_MAT_SAINT_VENANT)
-		return fail(c, PFG_ERR_UNSUPPORTED, "the shape derivative does not exist for SaintVenant");
+	// SaintVenant and HookeLinearElasticity, whose reference assemblers throw
+	if (c->m.mat == PFG_MAT_SAINT_VENANT || c->m.mat == PFG_MAT_SAINT_VENANT_TENSOR || c->m.mat == PFG_MAT_HOOKE)
+		return fail(c, PFG_ERR_UNSUPPORTED, "the shape derivative does not exist for SaintVenant and HookeLinearElasticity");
 	if (int st_m = check_material_prec(c, prec)) return st_m;
 	DeviceGuard g(c->device);
 	const size_t ndof = 3 * (size_t)c->m.N;

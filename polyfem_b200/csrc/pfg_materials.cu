@@ -26,6 +26,13 @@
 //   d2J  = eps_abc eps_ABC F_cC.
 // LinearElasticity is quadratic: P = 2 mu eps + lambda tr(eps) I and the constant
 // C = mu (delta_ab delta_AB + delta_aB delta_Ab) + lambda delta_aA delta_bB.
+// HookeLinearElasticity is quadratic too: with the Voigt strain v(G) = (G00, G11,
+// G22, G12 + G21, G02 + G20, G01 + G10) of G = F - I and the 6 x 6 tensor T,
+// psi = 1/2 v.T v, P(r, c) = (T v)[voigt(r, c)] and C = T[voigt(a, A)][voigt(b, B)].
+// SaintVenant with that tensor takes the Green strain E = (F^T F - I)/2 in the same
+// Voigt form e = (E00, E11, E22, 2E12, 2E02, 2E01): psi = 1/2 e.T e, the second
+// Piola-Kirchhoff stress S(A, B) = (T e)[voigt(A, B)], P = F S and
+//   C[(a,A),(b,B)] = delta_ab S(A, B) + sum_{I,J} F(a, I) F(b, J) T[voigt(I, A)][voigt(J, B)].
 // In the blocks kernel the 45 entries i <= j of C at every point are spread over
 // the lanes of the element's warp; the blocks are written as the packed block
 // triangle of the element, which the PSD projection and the scatter of
@@ -39,6 +46,10 @@
 //   5 MooneyRivlin3Param  (c1, c2, c3, d1) psi = c1 (I1~ - 3) + (c2 + c3 (I1~ - 3)) (I2~ - 3) + d1 (J - 1)^2
 //                                          (MooneyRivlin3ParamElasticity.hpp:26-49)
 //   6 VolumePenalty       (k)              psi = k/2 ((J^2 - 1)/2 - ln J)   (VolumePenalty.hpp:20-34)
+//   7 HookeLinearElasticity (one tensor)  psi = 1/2 sigma:eps, sigma = T eps in Voigt form
+//                                          (HookeLinearElasticity.cpp:372-421)
+//   8 SaintVenant         (one tensor)     psi = 1/2 S:E, S = T E in Voigt form, E the Green strain
+//                                          (SaintVenantElasticity.cpp:209-267)
 // with I1~ = J^-2/3 I1 and I2~ = J^-4/3 I2 (the invariants of F~ F~^T, F~ = J^-1/3 F).
 #include "pfg_device.cuh"
 
@@ -48,7 +59,16 @@
 namespace pfg
 {
 
-constexpr int MAT_LINEAR_ELASTICITY = 3, MAT_MOONEY_RIVLIN = 4, MAT_MOONEY_RIVLIN_3PARAM = 5, MAT_VOLUME_PENALTY = 6;
+constexpr int MAT_LINEAR_ELASTICITY = 3, MAT_MOONEY_RIVLIN = 4, MAT_MOONEY_RIVLIN_3PARAM = 5, MAT_VOLUME_PENALTY = 6,
+			  MAT_HOOKE = 7, MAT_SAINT_VENANT_TENSOR = 8;
+// the quadratic densities: constant tangent, no invariants
+template <int MAT>
+__host__ __device__ constexpr bool quadratic_mat() { return MAT == MAT_LINEAR_ELASTICITY || MAT == MAT_HOOKE; }
+// the densities of (I1, I2, J), differentiated by hyper-dual numbers
+template <int MAT>
+__host__ __device__ constexpr bool invariant_mat() { return !quadratic_mat<MAT>() && MAT != MAT_SAINT_VENANT_TENSOR; }
+// Voigt index of F(r, c) in HookeLinearElasticity's strain (e00, e11, e22, 2e12, 2e02, 2e01)
+__host__ __device__ constexpr int voigt(int r, int c) { return r == c ? r : 6 - r - c; }
 // IsochoricNeoHookean (hand-derived tangent in pfg_kernels.cu) is also an invariant
 // density; its shape derivative is taken here
 constexpr int MAT_ISO_NEOHOOKEAN = 1;
@@ -179,7 +199,9 @@ __device__ __forceinline__ void inv_psi_first(const Invariants &v, const double4
 template <int MAT>
 __device__ __forceinline__ double4 ad_params(const DevMesh &m, int e)
 {
-	if constexpr (MAT == MAT_LINEAR_ELASTICITY || MAT == MAT_ISO_NEOHOOKEAN)
+	if constexpr (MAT == MAT_HOOKE || MAT == MAT_SAINT_VENANT_TENSOR) // their one tensor is m.hooke
+		return make_double4(0.0, 0.0, 0.0, 0.0);
+	else if constexpr (MAT == MAT_LINEAR_ELASTICITY || MAT == MAT_ISO_NEOHOOKEAN)
 	{
 		const double2 lm = __ldg(m.lame + e);
 		return make_double4(lm.x, lm.y, 0.0, 0.0);
@@ -192,10 +214,71 @@ __device__ __forceinline__ double4 ad_params(const DevMesh &m, int e)
 	}
 }
 
-template <int MAT>
-__device__ __forceinline__ double mat_energy(const double F[3][3], const double4 &p)
+// HookeLinearElasticity: the Voigt strain v and the Voigt stress T v
+__device__ __forceinline__ void hooke_strain_stress(const double F[3][3], const double *__restrict__ T, double v[6],
+													double sv[6])
 {
-	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
+	v[0] = F[0][0] - 1.0;
+	v[1] = F[1][1] - 1.0;
+	v[2] = F[2][2] - 1.0;
+	v[3] = F[1][2] + F[2][1];
+	v[4] = F[0][2] + F[2][0];
+	v[5] = F[0][1] + F[1][0];
+#pragma unroll
+	for (int j = 0; j < 6; ++j)
+	{
+		double s_ = 0.0;
+#pragma unroll
+		for (int k = 0; k < 6; ++k) s_ += __ldg(T + 6 * j + k) * v[k];
+		sv[j] = s_;
+	}
+}
+
+// SaintVenant with a tensor: the Voigt Green strain from F^T F and the Voigt stress T e
+__device__ __forceinline__ void green_voigt_stress(const double Cr[9], const double *__restrict__ T, double e[6],
+												   double sv[6])
+{
+	e[0] = 0.5 * (Cr[0] - 1.0);
+	e[1] = 0.5 * (Cr[4] - 1.0);
+	e[2] = 0.5 * (Cr[8] - 1.0);
+	e[3] = Cr[5];
+	e[4] = Cr[2];
+	e[5] = Cr[1];
+#pragma unroll
+	for (int j = 0; j < 6; ++j)
+	{
+		double s_ = 0.0;
+#pragma unroll
+		for (int k = 0; k < 6; ++k) s_ += __ldg(T + 6 * j + k) * e[k];
+		sv[j] = s_;
+	}
+}
+
+__device__ __forceinline__ void right_cauchy_green(const double F[3][3], double Cr[9])
+{
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) Cr[3 * r + c] = F[0][r] * F[0][c] + F[1][r] * F[1][c] + F[2][r] * F[2][c];
+}
+
+template <int MAT>
+__device__ __forceinline__ double mat_energy(const double F[3][3], const double4 &p, const double *T)
+{
+	if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
+	{
+		double Cr[9], e[6], sv[6];
+		right_cauchy_green(F, Cr);
+		green_voigt_stress(Cr, T, e, sv);
+		return 0.5 * (sv[0] * e[0] + sv[1] * e[1] + sv[2] * e[2] + sv[3] * e[3] + sv[4] * e[4] + sv[5] * e[5]);
+	}
+	else if constexpr (MAT == MAT_HOOKE)
+	{
+		double v[6], sv[6];
+		hooke_strain_stress(F, T, v, sv);
+		return 0.5 * (sv[0] * v[0] + sv[1] * v[1] + sv[2] * v[2] + sv[3] * v[3] + sv[4] * v[4] + sv[5] * v[5]);
+	}
+	else if constexpr (MAT == MAT_LINEAR_ELASTICITY)
 	{
 		// eps:eps = sum_r G_rr^2 + 1/2 sum_{r<c} (G_rc + G_cr)^2
 		const double g0 = F[0][0] - 1.0, g1 = F[1][1] - 1.0, g2 = F[2][2] - 1.0, tr = g0 + g1 + g2;
@@ -213,9 +296,29 @@ __device__ __forceinline__ double mat_energy(const double F[3][3], const double4
 
 // P = dpsi/dF (row-major 9)
 template <int MAT>
-__device__ __forceinline__ void mat_stress(const double F[3][3], const double4 &p, double P[9])
+__device__ __forceinline__ void mat_stress(const double F[3][3], const double4 &p, const double *T, double P[9])
 {
-	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
+	if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
+	{
+		double Cr[9], e[6], sv[6];
+		right_cauchy_green(F, Cr);
+		green_voigt_stress(Cr, T, e, sv);
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+				P[3 * r + c] = F[r][0] * sv[voigt(0, c)] + F[r][1] * sv[voigt(1, c)] + F[r][2] * sv[voigt(2, c)];
+	}
+	else if constexpr (MAT == MAT_HOOKE)
+	{
+		double v[6], sv[6];
+		hooke_strain_stress(F, T, v, sv);
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) P[3 * r + c] = sv[voigt(r, c)];
+	}
+	else if constexpr (MAT == MAT_LINEAR_ELASTICITY)
 	{
 		const double tr = F[0][0] + F[1][1] + F[2][2] - 3.0;
 #pragma unroll
@@ -256,7 +359,7 @@ __device__ __forceinline__ double ad_element_energy(const DevMesh &m, const doub
 		geometry<EL, double>(q, Xg, Jit, detJ);
 		gen_def_grad<EL>(q, U, Jit, F);
 		bad |= !(det3(F) > 0.0);
-		en += mat_energy<MAT>(F, prm) * (detJ * qweight<EL>(q));
+		en += mat_energy<MAT>(F, prm, m.hooke) * (detJ * qweight<EL>(q));
 	}
 	if (bad) atomicAdd(inverted, 1ull);
 	return en;
@@ -304,7 +407,7 @@ __global__ void __launch_bounds__(NT) k_ad_gradient(DevMesh m, const double *__r
 		geometry<EL, double>(q, Xg, Jit, detJ);
 		gen_def_grad<EL>(q, U, Jit, F);
 		bad |= !(det3(F) > 0.0);
-		mat_stress<MAT>(F, prm, P);
+		mat_stress<MAT>(F, prm, m.hooke, P);
 		const double da = detJ * qweight<EL>(q);
 		double Q[3][3]; // da P J^-1 = da P Jit^T: G[a][d] = sum_r gref(q, a, r) Q[d][r]
 #pragma unroll
@@ -404,6 +507,23 @@ struct AdWarp
 
 __host__ __device__ constexpr int c9(int i, int j) { return i <= j ? tri_index(9, i, j) : tri_index(9, j, i); }
 
+// SaintVenant with a tensor, entry ce = ((a, A), (b, B)) of C:
+//   delta_ab S(A, B) + sum_{I,J} F(a, I) F(b, J) T[voigt(I, A)][voigt(J, B)]
+__device__ __forceinline__ double svt_hessian_entry(const Invariants &v, const double *__restrict__ T, const CEntry &ce)
+{
+	const int a = ce.i / 3, A = ce.i % 3, b = ce.j / 3, B = ce.j % 3;
+	const double *F = v.dx[0]; // dI1/dF = 2F
+	double e[6], sv[6];
+	green_voigt_stress(v.Cr, T, e, sv);
+	double h = ce.dab ? sv[voigt(A, B)] : 0.0;
+#pragma unroll
+	for (int I = 0; I < 3; ++I)
+#pragma unroll
+		for (int J = 0; J < 3; ++J)
+			h += (0.25 * F[3 * a + I] * F[3 * b + J]) * __ldg(T + 6 * voigt(I, A) + voigt(J, B));
+	return h;
+}
+
 // d2psi/dF_i dF_j from the invariants' derivatives, entry ce of C
 __device__ __forceinline__ double inv_hessian_entry(const Invariants &v, const double *psi, const CEntry &ce)
 {
@@ -466,7 +586,7 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 #pragma unroll
 				for (int c = 0; c < 3; ++c) S.Jit[q][3 * r + c] = Jit[r][c];
 			S.da[q] = detJ * qweight<EL>(q);
-			if constexpr (MAT != MAT_LINEAR_ELASTICITY) invariants(F, S.inv[q]);
+			if constexpr (!quadratic_mat<MAT>()) invariants(F, S.inv[q]);
 		}
 		__syncwarp();
 		// lanes over (point, node): g = J^-T gref
@@ -479,7 +599,7 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 				g[c] = gref<EL>(q, a, 0) * S.Jit[q][c] + gref<EL>(q, a, 1) * S.Jit[q][3 + c] + gref<EL>(q, a, 2) * S.Jit[q][6 + c];
 			g[3] = 0.0;
 		}
-		if constexpr (MAT != MAT_LINEAR_ELASTICITY)
+		if constexpr (invariant_mat<MAT>())
 		{
 			// lanes over (point, invariant pair x <= y): one hyper-dual evaluation each
 			for (int t = lane; t < NQ * 6; t += 32)
@@ -500,7 +620,11 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 			const int q = t / 45, k = t - q * 45;
 			const CEntry ce = s_ce[k];
 			double h;
-			if constexpr (MAT == MAT_LINEAR_ELASTICITY)
+			if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
+				h = svt_hessian_entry(S.inv[q], m.hooke, ce);
+			else if constexpr (MAT == MAT_HOOKE)
+				h = __ldg(m.hooke + 6 * voigt(ce.i / 3, ce.i % 3) + voigt(ce.j / 3, ce.j % 3));
+			else if constexpr (MAT == MAT_LINEAR_ELASTICITY)
 				h = prm.y * (ce.dab * ce.dAB + ce.le_aBbA) + prm.x * ce.le_aAbB;
 			else
 				h = inv_hessian_entry(S.inv[q], S.psi[q], ce);
@@ -744,6 +868,8 @@ static cudaError_t with_ad_material(const DevMesh &m, Fn &&f)
 		case MAT_MOONEY_RIVLIN: f(EL{}, std::integral_constant<int, MAT_MOONEY_RIVLIN>{}); break;
 		case MAT_MOONEY_RIVLIN_3PARAM: f(EL{}, std::integral_constant<int, MAT_MOONEY_RIVLIN_3PARAM>{}); break;
 		case MAT_VOLUME_PENALTY: f(EL{}, std::integral_constant<int, MAT_VOLUME_PENALTY>{}); break;
+		case MAT_HOOKE: f(EL{}, std::integral_constant<int, MAT_HOOKE>{}); break;
+		case MAT_SAINT_VENANT_TENSOR: f(EL{}, std::integral_constant<int, MAT_SAINT_VENANT_TENSOR>{}); break;
 		default: return cudaErrorInvalidValue;
 		}
 		return cudaGetLastError();

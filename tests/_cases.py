@@ -64,7 +64,25 @@ MATERIAL_PARAM_NAMES = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param":
                         "VolumePenalty": ("k",)}
 
 
+def hooke_tensor(seed=0, lam=86419.75, mu=37037.04):
+    """21 entries (i <= j, row by row) of a seeded anisotropic elasticity tensor: the
+    isotropic (lam, mu) tensor plus a random symmetric positive semi-definite part
+    that couples every pair of Voigt components."""
+    rng = np.random.default_rng(seed)
+    C = np.zeros((6, 6))
+    C[:3, :3] = lam
+    C[[0, 1, 2], [0, 1, 2]] = 2 * mu + lam
+    C[[3, 4, 5], [3, 4, 5]] = mu
+    R = rng.standard_normal((6, 6))
+    C += 1e4 * (R @ R.T) / 6
+    return C[np.triu_indices(6)]
+
+
 def material_params(mat, n_elements, seed=0):
-    """Per-element parameter values of a parameterised material (stress scale ~1e5)."""
+    """Per-element parameter values of a parameterised material (stress scale ~1e5);
+    the one elasticity tensor of HookeLinearElasticity and of the anisotropic
+    SaintVenant (the oracle's "SaintVenantTensor")."""
+    if mat in ("HookeLinearElasticity", "SaintVenantTensor"):
+        return {"elasticity_tensor": hooke_tensor(seed)}
     rng = np.random.default_rng(seed)
     return {n: 1e5 * rng.uniform(0.5, 1.5, n_elements) for n in MATERIAL_PARAM_NAMES.get(mat, ())}

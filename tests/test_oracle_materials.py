@@ -1,5 +1,6 @@
 """The oracle's restatement of the other elastic formulations (IsochoricNeoHookean,
-SaintVenant, LinearElasticity, MooneyRivlin, MooneyRivlin3Param, VolumePenalty):
+SaintVenant, LinearElasticity, MooneyRivlin, MooneyRivlin3Param, VolumePenalty,
+HookeLinearElasticity):
 derivatives by central finite differences, as the reference checks its forms
 (tests/test_form_derivatives.cpp:166-226), and closed-form known answers."""
 import numpy as np
@@ -12,7 +13,7 @@ from polyfem_b200 import mesh as M
 from _cases import make_case, material_params
 
 MATS = ["IsochoricNeoHookean", "SaintVenant", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param",
-        "VolumePenalty"]
+        "VolumePenalty", "HookeLinearElasticity", "SaintVenantTensor"]
 ELEMS = [(M.P1_TET, "P1"), (M.P2_TET, "P2"), (M.Q1_HEX, "Q1")]
 
 
@@ -108,6 +109,68 @@ def test_linear_elasticity_hessian_is_constant():
     _, _, v1 = o.hessian(u)
     assert np.abs(v1 - v0).max() <= 1e-9 * np.abs(v0).max()
     H = sp.csc_matrix((v0, inner, outer), shape=(mesh.n_dofs, mesh.n_dofs))
+    assert np.isclose(0.5 * u @ (H @ u), o.energy(u), rtol=1e-12)
+
+
+def test_saint_venant_tensor_known_answers():
+    """SaintVenant with the isotropic tensor of (lambda, mu) given as 21 entries is the
+    lambda/mu SaintVenant; with an anisotropic tensor and a homogeneous deformation
+    F the energy is |domain| 1/2 e.C e, e the Voigt Green strain with doubled shears."""
+    from polyfem_b200 import NeoHookeanAssembler
+    from _cases import hooke_tensor
+    mesh, lam, mu, u, _ = make_case(M.Q1_HEX, 2, seed=26, jitter=0.1, disp_scale=0.05)
+    lam0, mu0 = 7.5e4, 3.2e4
+    E = mesh.n_elements
+    iso = NeoHookeanAssembler.isotropic_elasticity_tensor(lam0, mu0)
+    o_t = Oracle(mesh, np.full(E, lam0), np.full(E, mu0), material="SaintVenantTensor",
+                 params={"elasticity_tensor": iso})
+    o_s = Oracle(mesh, np.full(E, lam0), np.full(E, mu0), material="SaintVenant")
+    assert np.isclose(o_t.energy(u), o_s.energy(u), rtol=1e-13)
+    gs = o_s.gradient(u)
+    assert np.abs(o_t.gradient(u) - gs).max() <= 1e-13 * np.abs(gs).max()
+    c21 = hooke_tensor(27)
+    C = np.zeros((6, 6))
+    C[np.triu_indices(6)] = c21
+    C = C + np.triu(C, 1).T
+    G = np.random.default_rng(28).normal(scale=5e-2, size=(3, 3))
+    uh = (mesh.node_pos @ G.T).ravel()
+    F = np.eye(3) + G
+    Eg = 0.5 * (F.T @ F - np.eye(3))
+    e = np.array([Eg[0, 0], Eg[1, 1], Eg[2, 2], 2 * Eg[1, 2], 2 * Eg[0, 2], 2 * Eg[0, 1]])
+    o = Oracle(mesh, lam, mu, material="SaintVenantTensor", params={"elasticity_tensor": c21})
+    assert np.isclose(o.energy(uh), 0.5 * e @ C @ e, rtol=1e-12)  # unit cube
+
+
+def test_hooke_known_answers():
+    """HookeLinearElasticity: with the isotropic tensor of (lambda, mu)
+    (ElasticityTensor::set_from_lambda_mu) it is LinearElasticity; with an
+    anisotropic tensor and a homogeneous strain u = G x the energy is
+    |domain| 1/2 v.C v (v the Voigt strain with doubled shears), the Hessian is
+    constant and the energy is 1/2 u^T H u."""
+    from polyfem_b200 import NeoHookeanAssembler
+    from _cases import hooke_tensor
+    mesh, lam, mu, u, _ = make_case(M.P2_TET, 2, seed=21, jitter=0.1, disp_scale=0.05)
+    lam0, mu0 = 7.5e4, 3.2e4
+    iso = NeoHookeanAssembler.isotropic_elasticity_tensor(lam0, mu0)
+    E = mesh.n_elements
+    o_h = Oracle(mesh, np.full(E, lam0), np.full(E, mu0), material="HookeLinearElasticity",
+                 params={"elasticity_tensor": iso})
+    o_l = Oracle(mesh, np.full(E, lam0), np.full(E, mu0), material="LinearElasticity")
+    assert np.isclose(o_h.energy(u), o_l.energy(u), rtol=1e-13)
+    assert np.allclose(o_h.gradient(u), o_l.gradient(u), rtol=0, atol=1e-13 * np.abs(o_l.gradient(u)).max())
+    c21 = hooke_tensor(22)
+    C = np.zeros((6, 6))
+    C[np.triu_indices(6)] = c21
+    C = C + np.triu(C, 1).T
+    G = np.random.default_rng(23).normal(scale=1e-2, size=(3, 3))
+    uh = (mesh.node_pos @ G.T).ravel()
+    v = np.array([G[0, 0], G[1, 1], G[2, 2], G[1, 2] + G[2, 1], G[0, 2] + G[2, 0], G[0, 1] + G[1, 0]])
+    o = Oracle(mesh, lam, mu, material="HookeLinearElasticity", params={"elasticity_tensor": c21})
+    assert np.isclose(o.energy(uh), 0.5 * v @ C @ v, rtol=1e-12)  # unit cube
+    outer, inner, h0 = o.hessian(np.zeros(mesh.n_dofs))
+    _, _, h1 = o.hessian(u)
+    assert np.abs(h1 - h0).max() <= 1e-9 * np.abs(h0).max()
+    H = sp.csc_matrix((h0, inner, outer), shape=(mesh.n_dofs, mesh.n_dofs))
     assert np.isclose(0.5 * u @ (H @ u), o.energy(u), rtol=1e-12)
 
 
