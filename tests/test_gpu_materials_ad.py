@@ -1,5 +1,5 @@
 """Energy-defined formulations on the GPU (pfg_materials.cu): LinearElasticity,
-MooneyRivlin, MooneyRivlin3Param, VolumePenalty and HookeLinearElasticity, differentiated on the device by
+MooneyRivlin, MooneyRivlin3Param and VolumePenalty, differentiated on the device by
 dual and hyper-dual numbers.  FP64 energy, gradient and Hessian (with
 project_to_psd and the Dirichlet reduction) against the oracle, which
 differentiates the same energies with second-order dual numbers over F as the
@@ -16,7 +16,7 @@ from _cases import make_case, material_params, rel_err
 
 pytestmark = pytest.mark.gpu
 
-MATS = ["LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty", "HookeLinearElasticity"]
+MATS = ["LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty"]
 ELEMS = [(M.P1_TET, 3), (M.P2_TET, 2), (M.Q1_HEX, 3)]
 
 
@@ -70,74 +70,6 @@ def test_linear_elasticity_hessian_constant_on_device(require_gpu):
     v0 = asm.assemble_hessian_values(np.zeros(mesh.n_dofs), "fp64")
     v1 = asm.assemble_hessian_values(u, "fp64")
     assert rel_err(v1, v0) <= 1e-12
-    asm.close()
-
-
-def test_hooke_linear_elasticity(require_gpu):
-    """HookeLinearElasticity: with the isotropic tensor it gives LinearElasticity's
-    results; with an anisotropic tensor its Hessian is constant; the tensor must be
-    set before use; it has no adjoint terms (the reference's assembler throws)."""
-    from _cases import hooke_tensor
-    mesh, lam, mu, u, p = make_case(M.Q1_HEX, 3, seed=24, jitter=0.1, disp_scale=0.05)
-    E = mesh.n_elements
-    lam0, mu0 = 7.5e4, 3.2e4
-    asm = NeoHookeanAssembler.from_mesh(mesh, np.full(E, lam0), np.full(E, mu0))
-    assert lib().pfg_set_material(asm.handle, 7) == 0
-    with pytest.raises(PfgError) as ei:
-        asm.assemble_energy(u)
-    assert ei.value.status == 5  # no tensor yet
-    asm.set_material("LinearElasticity")
-    e_l, g_l, h_l = asm.assemble_energy(u), asm.assemble_gradient(u), asm.assemble_hessian_values(u, "fp64")
-    asm.set_material("HookeLinearElasticity",
-                     elasticity_tensor=NeoHookeanAssembler.isotropic_elasticity_tensor(lam0, mu0))
-    assert abs(asm.assemble_energy(u) - e_l) <= 1e-12 * abs(e_l)
-    assert rel_err(asm.assemble_gradient(u), g_l) <= 1e-12
-    assert rel_err(asm.assemble_hessian_values(u, "fp64"), h_l) <= 1e-12
-    asm.set_material("HookeLinearElasticity", elasticity_tensor=hooke_tensor(25))
-    v0 = asm.assemble_hessian_values(np.zeros(mesh.n_dofs), "fp64")
-    assert rel_err(asm.assemble_hessian_values(u, "fp64"), v0) <= 1e-12
-    with pytest.raises(PfgError) as ei:
-        asm.force_shape_derivative(u, p)
-    assert ei.value.status == 4
-    with pytest.raises(PfgError) as ei:
-        asm.force_material_derivative(u, p)
-    assert ei.value.status == 4
-    with pytest.raises(ValueError):
-        asm.set_material("HookeLinearElasticity", elasticity_tensor=np.ones(20))
-    asm.close()
-
-
-@pytest.mark.parametrize("et,g", ELEMS, ids=["P1", "P2", "Q1"])
-def test_saint_venant_tensor(require_gpu, et, g):
-    """SaintVenant with an anisotropic elasticity tensor (PFG_MAT_SAINT_VENANT_TENSOR)
-    against the oracle; with the isotropic tensor it gives the lambda/mu SaintVenant;
-    like the reference it has no shape derivative."""
-    from _cases import hooke_tensor
-    mesh, lam, mu, u, p = make_case(et, g, seed=29, jitter=0.1 if et != M.P1_TET else 0.0, disp_scale=0.05)
-    c21 = hooke_tensor(30)
-    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
-    asm.set_material("SaintVenant", elasticity_tensor=c21)
-    orc = Oracle(mesh, lam, mu, material="SaintVenantTensor", params={"elasticity_tensor": c21})
-    e_o = orc.energy(u)
-    assert abs(asm.assemble_energy(u) - e_o) <= 1e-12 * abs(e_o)
-    assert rel_err(asm.assemble_energy_per_element(u), orc.energy_per_element(u)) <= 1e-12
-    assert rel_err(asm.assemble_gradient(u), orc.gradient(u)) <= 1e-12
-    outer, inner, vals = orc.hessian(u)
-    assert rel_err(asm.assemble_hessian_values(u, "fp64"), vals) <= 1e-12
-    _, _, v_psd = orc.hessian(u, project_psd=True)
-    assert rel_err(asm.assemble_hessian_values(u, "fp64", project_to_psd=True), v_psd) <= 1e-11
-    with pytest.raises(PfgError) as ei:
-        asm.force_shape_derivative(u, p)
-    assert ei.value.status == 4
-    E = mesh.n_elements
-    lam0, mu0 = 7.5e4, 3.2e4
-    asm.set_lame(np.full(E, lam0), np.full(E, mu0))
-    asm.set_material("SaintVenant")
-    e_s, g_s, h_s = asm.assemble_energy(u), asm.assemble_gradient(u), asm.assemble_hessian_values(u, "fp64")
-    asm.set_material("SaintVenant", elasticity_tensor=NeoHookeanAssembler.isotropic_elasticity_tensor(lam0, mu0))
-    assert abs(asm.assemble_energy(u) - e_s) <= 1e-12 * abs(e_s)
-    assert rel_err(asm.assemble_gradient(u), g_s) <= 1e-12
-    assert rel_err(asm.assemble_hessian_values(u, "fp64"), h_s) <= 1e-12
     asm.close()
 
 
