@@ -507,14 +507,14 @@ struct AdWarp
 
 __host__ __device__ constexpr int c9(int i, int j) { return i <= j ? tri_index(9, i, j) : tri_index(9, j, i); }
 
-// SaintVenant with a tensor, entry ce = ((a, A), (b, B)) of C:
+// SaintVenant with a tensor, entry ce = ((a, A), (b, B)) of C, with sv the point's
+// Voigt stress:
 //   delta_ab S(A, B) + sum_{I,J} F(a, I) F(b, J) T[voigt(I, A)][voigt(J, B)]
-__device__ __forceinline__ double svt_hessian_entry(const Invariants &v, const double *__restrict__ T, const CEntry &ce)
+__device__ __forceinline__ double svt_hessian_entry(const Invariants &v, const double *sv, const double *__restrict__ T,
+													const CEntry &ce)
 {
 	const int a = ce.i / 3, A = ce.i % 3, b = ce.j / 3, B = ce.j % 3;
 	const double *F = v.dx[0]; // dI1/dF = 2F
-	double e[6], sv[6];
-	green_voigt_stress(v.Cr, T, e, sv);
 	double h = ce.dab ? sv[voigt(A, B)] : 0.0;
 #pragma unroll
 	for (int I = 0; I < 3; ++I)
@@ -587,6 +587,12 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 				for (int c = 0; c < 3; ++c) S.Jit[q][3 * r + c] = Jit[r][c];
 			S.da[q] = detJ * qweight<EL>(q);
 			if constexpr (!quadratic_mat<MAT>()) invariants(F, S.inv[q]);
+			if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
+			{
+				// the point's Voigt stress, shared by its 45 tangent entries (psi is unused here)
+				double e[6];
+				green_voigt_stress(S.inv[q].Cr, m.hooke, e, S.psi[q]);
+			}
 		}
 		__syncwarp();
 		// lanes over (point, node): g = J^-T gref
@@ -621,7 +627,7 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 			const CEntry ce = s_ce[k];
 			double h;
 			if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
-				h = svt_hessian_entry(S.inv[q], m.hooke, ce);
+				h = svt_hessian_entry(S.inv[q], S.psi[q], m.hooke, ce);
 			else if constexpr (MAT == MAT_HOOKE)
 				h = __ldg(m.hooke + 6 * voigt(ce.i / 3, ce.i % 3) + voigt(ce.j / 3, ce.j % 3));
 			else if constexpr (MAT == MAT_LINEAR_ELASTICITY)
