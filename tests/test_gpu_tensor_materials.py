@@ -103,3 +103,41 @@ def test_saint_venant_tensor(require_gpu, et, g):
     assert rel_err(asm.assemble_gradient(u), g_s) <= 1e-12
     assert rel_err(asm.assemble_hessian_values(u, "fp64"), h_s) <= 1e-12
     asm.close()
+
+
+def test_hooke_inverted_element_and_reduced_saint_venant(require_gpu):
+    """An element turned inside out: HookeLinearElasticity has no ln J and stays finite,
+    the per-element energies follow the oracle and the inverted count sees it.  The
+    anisotropic SaintVenant through the Dirichlet reduction: reduced pattern and values
+    against the oracle's restatement of BCLagrangianForm::project_hessian."""
+    from oracle.binding import project_hessian
+    mesh, lam, mu, _, _ = make_case(M.P1_TET, 2, seed=17)
+    bad = np.zeros(mesh.n_dofs)
+    c = mesh.conn[0]
+    X = mesh.node_pos
+    bad.reshape(-1, 3)[c[3]] = 2.0 * (X[c[:3]].mean(axis=0) - X[c[3]])  # vertex 3 through the opposite face
+    c21 = hooke_tensor(31)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    asm.set_material("HookeLinearElasticity", elasticity_tensor=c21)
+    orc = Oracle(mesh, lam, mu, material="HookeLinearElasticity", params={"elasticity_tensor": c21})
+    pe = asm.assemble_energy_per_element(bad)
+    assert np.all(np.isfinite(pe))
+    assert rel_err(pe, orc.energy_per_element(bad)) <= 1e-12
+    assert rel_err(asm.assemble_gradient(bad), orc.gradient(bad)) <= 1e-12
+    assert asm.inverted_count() >= 1
+    asm.close()
+
+    mesh, lam, mu, u, _ = make_case(M.P2_TET, 2, seed=32, jitter=0.1, disp_scale=0.05)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    asm.set_material("SaintVenant", elasticity_tensor=c21)
+    orc = Oracle(mesh, lam, mu, material="SaintVenantTensor", params={"elasticity_tensor": c21})
+    outer, inner, vals = orc.hessian(u)
+    face = np.flatnonzero(mesh.node_pos[:, 0] <= 1e-12)
+    dofs = (3 * face[:, None] + np.arange(3)).ravel()
+    asm.set_dirichlet(dofs)
+    ro, ri, rv = project_hessian(outer, inner, vals, dofs)
+    go, gi = asm.reduced_pattern()
+    assert np.array_equal(go, ro) and np.array_equal(gi, ri)
+    assert rel_err(asm.assemble_hessian_reduced_values(u, "fp64"), rv) <= 1e-12
+    assert rel_err(asm.assemble_gradient_reduced(u, "fp64"), np.delete(orc.gradient(u), np.unique(dofs))) <= 1e-12
+    asm.close()
