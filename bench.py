@@ -481,6 +481,8 @@ def run_suite(args):
             "shape_vjp_fp64": lambda: L.pfg_shape_vjp(h, U, P, 1, 0, O),
             "shape_vjp_fp32": lambda: L.pfg_shape_vjp(h, U, P, 1, 1, O),
             "mass_matrix": lambda: L.pfg_mass_matrix(h, None, 1, MV),
+            # row-sum lumping of the mass values just assembled (utils::lump_matrix)
+            "lump_matrix": lambda: L.pfg_lump_matrix(h, MV, 1, O),
         }
         # algorithmic bytes of the HBM-bound operations
         n, ng = mesh.conn.shape[1], mesh.gconn.shape[1]
@@ -489,7 +491,9 @@ def run_suite(args):
                "gradient_fp64": ins + mesh.n_dofs * 8, "gradient_fp32": ins + mesh.n_dofs * 8,
                "material_vjp": ins + mesh.n_nodes * 24 + 2 * E * 8,
                "hessian_fp64": algorithmic_bytes(mesh, nnz), "hessian_fp32": algorithmic_bytes(mesh, nnz),
-               "hessian_split32": algorithmic_bytes(mesh, nnz)}
+               "hessian_split32": algorithmic_bytes(mesh, nnz),
+               # every value read once, the diagonal written, the column starts read
+               "lump_matrix": nnz * 8 + mesh.n_dofs * 8 + (mesh.n_dofs + 1) * 4}
         # Dirichlet reduction: the dofs of the x = 0 face constrained
         face = np.flatnonzero(mesh.node_pos[:, 0] <= 1e-12)
         asm.set_dirichlet((3 * face[:, None] + np.arange(3)).ravel())
