@@ -309,7 +309,7 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     from polyfem_b200 import NeoHookeanAssembler
-    from polyfem_b200._lib import PFG_FP64, PFG_MEM_DEVICE, PFG_MEM_HOST, PFG_SPLIT32, check, lib
+    from polyfem_b200._lib import PFG_FP64, PFG_MEM_DEVICE, PFG_MEM_HOST, PFG_SPLIT32, PFG_SPLIT32_SIMT, check, lib
 
     mesh, lam, mu, u = _workload(args.grid)
     asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu, device=local)
@@ -354,6 +354,7 @@ def run_gpu(args):
     del v64
 
     ms64, _ = timed_device(PFG_FP64)
+    ms_simt, _ = timed_device(PFG_SPLIT32_SIMT)
     ms_split, clocks = timed_device(PFG_SPLIT32, ClockSampler(local))
 
     # end to end through the C ABI with host buffers: pinned u in, CSC values out
@@ -396,6 +397,8 @@ def run_gpu(args):
                        "l2": "no flush; every step writes the 1.08 GB CSC values and 0.76 GB of element "
                              "block triangles, both larger than the 126 MB L2"},
             "fp64": {"value": world * E / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64},
+            "split32_simt": {"value": world * E / (ms_simt * 1e-3), "unit": UNIT, "ms_per_step": ms_simt,
+                             "note": "the same split with the element contraction on CUDA cores"},
             "split_over_fp64": ms64 / ms_split,
             "rel_err_vs_fp64": rel_err,
             "e2e": {"value": world * E / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,

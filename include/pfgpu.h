@@ -55,11 +55,16 @@ enum pfg_precision
 {
 	PFG_FP64 = 0,    /* all arithmetic in FP64 (the drop-in) */
 	PFG_FP32 = 1,    /* FP32 arithmetic; det(F)/log J and reductions in FP64 */
-	PFG_SPLIT32 = 2  /* Hessian: kinematics (J^-T, F, det/log J, F^-T, basis
-	                    gradients) in FP64, the per-block contraction and the
-	                    staged element blocks in FP32, every CSC entry summed in FP64.
+	PFG_SPLIT32 = 2, /* Hessian: kinematics (J^-T, F, det/log J, F^-T, basis
+	                    gradients) in FP64; for P2 and Q1 the element contraction
+	                    on the tensor cores (tcgen05, each FP32 operand split into
+	                    two TF32 halves, 3 products, FP32 accumulation), for P1 on
+	                    CUDA cores in FP32; staged element blocks in FP32, every
+	                    CSC entry summed in FP64.
 	                    Relative Frobenius error vs PFG_FP64 <= 1e-6.
 	                    Energy/gradient/shape VJP treat it as PFG_FP32. */
+	PFG_SPLIT32_SIMT = 3 /* PFG_SPLIT32 with the contraction on CUDA cores (FP32
+	                        FMA) for every element type; same bound. */
 };
 
 enum pfg_mem
@@ -134,6 +139,16 @@ int pfg_hessian_pattern_copy(pfg_context *ctx, int *outer, int *inner, int mem);
  * element whose smallest eigenvalue is > 0 is kept as it is, otherwise it
  * becomes V max(l, 0) V^T (eigendecomposition in FP64 on the device). */
 int pfg_hessian(pfg_context *ctx, const double *u, int mem, int prec, int project_psd, double *values);
+
+/* q = H p (3N doubles each, in `mem`) with the Hessian in the full pattern:
+ * `values` (device memory, nnz doubles) or, when NULL, the values of the last
+ * pfg_hessian call that wrote into the context.  H is symmetric, so this is also
+ * H^T p, the product the reference's adjoint terms form with Eigen's sparse
+ * matrix-vector product (e.g. `term = -hessian.transpose() * adjoint_zeroed`,
+ * optimization/force_derivatives/PressureForceDerivative.cpp:24).  One warp per
+ * node, each entry summed in a fixed order: bitwise deterministic.  Requires the
+ * pattern (any pfg_hessian or pfg_hessian_pattern call builds it). */
+int pfg_hessian_apply(pfg_context *ctx, const double *values, const double *p, int mem, double *q);
 
 /* Device pointers of the context-owned CSC arrays (valid until pfg_destroy). */
 int pfg_hessian_device_csc(pfg_context *ctx, const int **outer, const int **inner, double **values);
@@ -335,9 +350,17 @@ int pfg_cg_solve(pfg_context *ctx, int system, const double *values, const doubl
  *   conn_soa  : [n][E] int32, local node a of element e at conn_soa[a*E + e]
  *   gconn_soa : [n_g][E] int32 (required for P2; NULL = conn_soa otherwise)
  *   X         : [N_g][3] float64 rest positions
- *   lame      : [E][2] float64 (lambda, mu) per element
+ *   lame      : [E][2] float64 (lambda, mu) per element, 16-byte aligned (each
+ *               pair is read as one 16-byte load; a misaligned pointer is
+ *               refused with PFG_ERR_INVALID before anything is launched)
  *   u         : [3N] float64 displacement, node-major
  *   out       : 1 float64 (the energy)
+ * The connectivity is trusted: every conn_soa entry must lie in [0, n_nodes)
+ * and every gconn_soa entry in [0, n_geom_nodes).  pfg_create checks each index
+ * on the host; this call cannot, because the tables are already on the device
+ * and reading them back would need a host buffer, so an index out of range
+ * reads out of bounds on the device.  The sizes are checked as pfg_create
+ * checks them (3 n_nodes and E n below 2^31).
  * The call enqueues work on `stream` (cudaStream_t as void*, NULL = default
  * stream) and returns without synchronising.  It allocates nothing: the
  * reduction scratch is a fixed array inside the library's device image

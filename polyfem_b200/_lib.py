@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB_PATH = os.path.join(HERE, "libpfgpu.so")
-SOURCES = ["pfg_api.cu", "pfg_kernels.cu", "pfg_materials.cu", "pfg_solve.cu", "pfg_noalloc.cu"]
+SOURCES = ["pfg_api.cu", "pfg_kernels.cu", "pfg_materials.cu", "pfg_solve.cu", "pfg_noalloc.cu", "pfg_tc.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 PFG_OK = 0
@@ -22,6 +22,7 @@ PFG_MEM_DEVICE = 1
 PFG_FP64 = 0
 PFG_FP32 = 1
 PFG_SPLIT32 = 2
+PFG_SPLIT32_SIMT = 3
 
 _lib = None
 
@@ -44,17 +45,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB_PATH
     nvcc = os.environ.get("NVCC", "nvcc")
-    objs = []
     build_dir = os.path.join(HERE, "_build")
     os.makedirs(build_dir, exist_ok=True)
+    cmds, objs = [], []
     for src in _sources():
         obj = os.path.join(build_dir, os.path.basename(src) + ".o")
         cmd = [nvcc, *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
                "-I", os.path.join(REPO, "include"), "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        subprocess.check_call(cmd)
+        cmds.append(cmd)
         objs.append(obj)
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(subprocess.check_call, c) for c in cmds]:
+            f.result()
     tmp = LIB_PATH + ".tmp"
     cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", tmp, *objs, "-lpthread"]
     if verbose:
@@ -97,6 +103,7 @@ SIGNATURES = {
     "pfg_hessian_pattern": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "pfg_hessian_pattern_copy": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     "pfg_hessian": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "pfg_hessian_apply": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     "pfg_hessian_device_csc": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "pfg_material_vjp": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     "pfg_shape_vjp": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),

@@ -19,9 +19,9 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import PFG_FP32, PFG_FP64, PFG_MEM_DEVICE, PFG_MEM_HOST, PFG_SPLIT32, check, lib
+from ._lib import PFG_FP32, PFG_FP64, PFG_MEM_DEVICE, PFG_MEM_HOST, PFG_SPLIT32, PFG_SPLIT32_SIMT, check, lib
 
-PRECISIONS = {"fp64": PFG_FP64, "fp32": PFG_FP32, "split32": PFG_SPLIT32}
+PRECISIONS = {"fp64": PFG_FP64, "fp32": PFG_FP32, "split32": PFG_SPLIT32, "split32_simt": PFG_SPLIT32_SIMT}
 
 
 def _prec(p) -> int:
@@ -210,6 +210,29 @@ class NeoHookeanAssembler:
         import scipy.sparse as sp
         outer, inner = self.hessian_pattern()
         return sp.csc_matrix((vals, inner, outer), shape=(self.n_dofs, self.n_dofs))
+
+    def hessian_apply(self, p, values=None):
+        """q = H p with the library's SpMV (pfg_hessian_apply): H from `values` (a CUDA
+        float64 tensor of nnz entries) or, when None, the last Hessian assembled into
+        the context (assemble_hessian_into_context).  Deterministic."""
+        self._check_len(p, self.n_dofs, "p")
+        mem, ptrs, keep = self._prepare(p)
+        vptr = None
+        if values is not None:
+            if not _is_device(values):
+                raise ValueError("values must be a CUDA tensor")
+            vptr = ctypes.c_void_p(values.data_ptr())
+        out, optr = self._alloc(mem, self.n_dofs)
+        check(lib().pfg_hessian_apply(self._h, vptr, ptrs[0], mem, optr), self._h, "pfg_hessian_apply")
+        return out
+
+    def assemble_hessian_into_context(self, u, precision="fp64", project_to_psd: bool = False):
+        """Assemble the Hessian into the context's own device buffer (no copy out)."""
+        self._check_len(u, self.n_dofs, "u")
+        self.hessian_nnz()
+        mem, ptrs, keep = self._prepare(u)
+        check(lib().pfg_hessian(self._h, ptrs[0], mem, _prec(precision), int(bool(project_to_psd)), None),
+              self._h, "pfg_hessian")
 
     def inverted_count(self) -> int:
         c = ctypes.c_longlong()

@@ -11,7 +11,8 @@ backward(p) returns the vector-Jacobian products of f:
   d(p.f)/dX                  : ElasticForceDerivative::force_shape_derivative
       (ElasticForceDerivative.cpp:207-260), which equals +p . df/dX_rest;
   d(p.f)/du                  : H p, the assembled Hessian (structurally and
-      numerically symmetric) times p.
+      numerically symmetric) times p, by the library's own SpMV
+      (pfg_hessian_apply): bitwise deterministic.
 Each backward term recomputes F and the basis gradients per quadrature point
 from (u, lambda, mu, X); nothing from the forward pass is stored on the device
 beyond the four inputs.
@@ -57,8 +58,8 @@ class ElasticForce(torch.autograd.Function):
         if ctx.needs_input_grad[3]:
             g_X = asm.force_shape_derivative(u, p, ctx.precision).reshape(X.shape)
         if ctx.needs_input_grad[0]:
-            H = asm.assemble_hessian(u, ctx.precision)
-            g_u = (H @ p.unsqueeze(1)).squeeze(1)
+            asm.assemble_hessian_into_context(u, ctx.precision)
+            g_u = asm.hessian_apply(p)
         return g_u, g_lam, g_mu, g_X, None, None
 
 

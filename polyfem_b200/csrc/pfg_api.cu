@@ -79,6 +79,7 @@ struct pfg_context
 	// (pfg_set_elasticity_tensor): 36 doubles
 	double *d_hooke = nullptr;
 	double *h_cg_sc = nullptr;
+	int *d_err = nullptr; // set by a kernel whose bounded wait gave up (DevMesh::err)
 	std::string err;
 };
 
@@ -170,7 +171,7 @@ int check_material_prec(pfg_context *c, int prec)
 		return fail(c, PFG_ERR_STATE, "the elasticity tensor is not set (pfg_set_elasticity_tensor)");
 	return PFG_OK;
 }
-int check_prec(int prec) { return prec == PFG_FP64 || prec == PFG_FP32 || prec == PFG_SPLIT32; }
+int check_prec(int prec) { return prec == PFG_FP64 || prec == PFG_FP32 || prec == PFG_SPLIT32 || prec == PFG_SPLIT32_SIMT; }
 
 int ensure_staging(pfg_context *c, size_t out_doubles)
 {
@@ -229,11 +230,26 @@ int stage_in(pfg_context *c, const double *src, int mem, double *dst, size_t n, 
 	return PFG_OK;
 }
 
+// After a stream synchronisation: a kernel that gave up a bounded wait left the
+// flag set; report it once and clear it.
+int check_kernel_flag(pfg_context *c)
+{
+	int v = 0;
+	PFG_CUDA(c, cudaMemcpy(&v, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+	if (v)
+	{
+		PFG_CUDA(c, cudaMemset(c->d_err, 0, sizeof(int)));
+		return fail(c, PFG_ERR_CUDA, "a tensor-core kernel gave up waiting for its MMA or bulk copy; the results of "
+									 "the calls since the last synchronisation are invalid");
+	}
+	return PFG_OK;
+}
+
 int finish_host(pfg_context *c, double *host_dst, const double *dev_src, size_t n)
 {
 	if (n) PFG_CUDA(c, cudaMemcpyAsync(host_dst, dev_src, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
 	PFG_CUDA(c, cudaStreamSynchronize(c->stream));
-	return PFG_OK;
+	return check_kernel_flag(c);
 }
 
 // Host build of the CSC pattern (Eigen ColMajor semantics: per column the sorted
@@ -535,6 +551,7 @@ void free_all(pfg_context *c)
 	if (c->d_hooke) cudaFree(c->d_hooke);
 	if (c->d_rho) cudaFree(c->d_rho);
 	if (c->d_mpar) cudaFree(c->d_mpar);
+	if (c->d_err) cudaFree(c->d_err);
 }
 } // namespace
 
@@ -670,6 +687,8 @@ int pfg_create(const pfg_mesh_desc *d, pfg_context **out)
 	CREATE_CUDA(cudaMalloc(&c->sc.inverted, sizeof(unsigned long long)));
 	CREATE_CUDA(cudaMemset(c->sc.inverted, 0, sizeof(unsigned long long)));
 	CREATE_CUDA(cudaMalloc(&c->d_result, sizeof(double)));
+	CREATE_CUDA(cudaMalloc(&c->d_err, sizeof(int)));
+	CREATE_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
 	CREATE_CUDA(hessian_kernel_setup(c->device));
 #undef CREATE_CUDA
 	c->m.conn = c->d_conn;
@@ -682,6 +701,7 @@ int pfg_create(const pfg_mesh_desc *d, pfg_context **out)
 	c->m.g_eb_inc = c->d_g_eb_inc ? c->d_g_eb_inc : c->d_eb_inc;
 	c->m.X = c->d_X;
 	c->m.lame = c->d_lame;
+	c->m.err = c->d_err;
 	*out = c;
 	return PFG_OK;
 }
@@ -896,7 +916,27 @@ int pfg_hessian(pfg_context *c, const double *u, int mem, int prec, int project_
 	if (values && mem == PFG_MEM_DEVICE) p.values = values;
 	PFG_CUDA(c, launch_hessian(c->m, p, du, prec, project_psd, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
 	if (values && mem == PFG_MEM_HOST) return finish_host(c, values, c->d_values, c->pat.nnz);
-	if (mem == PFG_MEM_HOST) PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	if (mem == PFG_MEM_HOST)
+	{
+		PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+		return check_kernel_flag(c);
+	}
+	return PFG_OK;
+}
+
+int pfg_hessian_apply(pfg_context *c, const double *values, const double *p, int mem, double *q)
+{
+	if (!c || !check_mem(mem) || (c->m.N && (!p || !q))) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (!c->has_pattern) return fail(c, PFG_ERR_STATE, "no Hessian assembled yet (pattern not built)");
+	DeviceGuard g(c->device);
+	const size_t ndof = 3 * (size_t)c->m.N;
+	int st = ensure_staging(c, std::max<size_t>(ndof, 1));
+	if (st) return st;
+	const double *dp;
+	if ((st = stage_in(c, p, mem, c->d_p, ndof, &dp))) return st;
+	double *dq = mem == PFG_MEM_DEVICE ? q : c->d_out;
+	PFG_CUDA(c, launch_hessian_apply(c->m.N, c->d_outer, c->d_inner, values ? values : c->d_values, dp, dq, c->stream));
+	if (mem == PFG_MEM_HOST) return finish_host(c, q, c->d_out, ndof);
 	return PFG_OK;
 }
 
@@ -969,7 +1009,7 @@ int pfg_synchronize(pfg_context *c)
 	if (!c) return PFG_ERR_INVALID;
 	DeviceGuard g(c->device);
 	PFG_CUDA(c, cudaStreamSynchronize(c->stream));
-	return PFG_OK;
+	return check_kernel_flag(c);
 }
 
 /* ---------------------------------------------------------------------------

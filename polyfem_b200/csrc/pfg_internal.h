@@ -36,6 +36,7 @@ struct DevMesh
 	const int *ginc_off = nullptr;
 	const int *ginc_eb = nullptr;
 	const int *g_eb_inc = nullptr; // [E*n_g] inverse of ginc_eb (aliases eb_inc when isoparametric)
+	int *err = nullptr; // set to 1 by a kernel whose bounded wait gave up (the context reports it)
 };
 
 // Element Hessian staging: element e's symmetric node blocks (a, b), a <= b, as one
@@ -88,7 +89,8 @@ struct Scratch
 
 constexpr int PREC_FP64 = 0;
 constexpr int PREC_FP32 = 1;
-constexpr int PREC_SPLIT32 = 2;
+constexpr int PREC_SPLIT32 = 2;      // tensor cores (P2, Q1); CUDA cores for P1
+constexpr int PREC_SPLIT32_SIMT = 3; // the same split with the contraction on CUDA cores
 
 // Elements per thread block of the total-energy kernel for an element type (the
 // number of per-block partial sums is ceil(E / this)).
@@ -133,6 +135,12 @@ cudaError_t launch_material_vjp(const DevMesh &m, const double *u, const double 
 cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *adj, int prec, double *out,
 							 const Scratch &sc, cudaStream_t s);
 cudaError_t hessian_kernel_setup(int device);
+// Tensor-core element blocks of the split mode (pfg_tc.cu): the Phi tables of the
+// current device and the kernels' shared-memory limits (called by hessian_kernel_setup);
+// the packed FP32 block triangles of all elements into `stage` (P2 and Q1 only)
+cudaError_t tc_tables_setup(int device);
+cudaError_t launch_hessian_blocks_tc(const DevMesh &m, const double *u, float *stage, cudaStream_t s);
+size_t tc_smem_bytes(int et);
 
 // Device conjugate gradient (pfg_solve.cu).  Work vectors of n doubles (r, z, p, q,
 // invd), cg_partials_doubles() per-block partial sums and the scalars sc[CG_NSC].
@@ -159,6 +167,10 @@ cudaError_t launch_cg_diag_inv(int n, const int *outer, const int *inner, const 
 // The SpMV takes the columns in groups of m <= 3 consecutive columns with the same
 // rows (a node's dofs): groups[g] = first column * 4 + m, or, with groups == NULL,
 // group g = columns 3g .. 3g+2.
+// q = H p over the full pattern (a node's three columns share their rows), one warp
+// per node, every entry summed in a fixed order (bitwise deterministic)
+cudaError_t launch_hessian_apply(int n_nodes, const int *outer, const int *inner, const double *vals, const double *p,
+								 double *q, cudaStream_t s);
 // r = b - H x (x = 0 unless guess), p = D^-1 r; sc: r.z, |r|^2, |b|^2, the threshold
 // max(tol^2 |b|^2, smallest normal), done (|b| = 0 or |r|^2 below it), 0 iterations
 cudaError_t launch_cg_start(int n, int ngroups, const int *groups, const int *outer, const int *inner,

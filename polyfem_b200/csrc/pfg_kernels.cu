@@ -1885,7 +1885,30 @@ static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const
 	return cudaGetLastError();
 }
 
-cudaError_t hessian_kernel_setup(int) { return cudaSuccess; }
+cudaError_t hessian_kernel_setup(int device) { return tc_tables_setup(device); }
+
+// split mode on the tensor cores: element blocks by tcgen05 (FP32 triangles), then
+// the optional projection and the same reduction as the other modes
+template <class EL>
+static cudaError_t hessian_tc(const DevMesh &m, const DevPattern &p, const double *u, void *stage_v, bool project_psd,
+							  cudaStream_t s)
+{
+	constexpr int WARPS = 8;
+	float *stage = static_cast<float *>(stage_v);
+	cudaError_t e = launch_hessian_blocks_tc(m, u, stage, s);
+	if (e != cudaSuccess) return e;
+	if (project_psd && m.E > 0)
+	{
+		constexpr int PW = 4;
+		const size_t bytes_p = PW * sizeof(PsdWarp<EL>);
+		e = cudaFuncSetAttribute(k_project_psd<EL, float, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
+		if (e != cudaSuccess) return e;
+		k_project_psd<EL, float, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
+	}
+	const int ng = (m.N + WARPS - 1) / WARPS;
+	if (ng > 0) k_hessian_reduce<EL, float, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+	return cudaGetLastError();
+}
 
 cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *u, int prec, int project_psd,
 						   void *stage, cudaStream_t s)
@@ -1917,8 +1940,9 @@ cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *
 		return cudaErrorInvalidValue;
 	}
 	// FP64: everything in FP64.  FP32: everything in FP32 except det/log J.
-	// SPLIT32: kinematics (J^-T, F^-T, det/log J, g, d) in FP64, contraction and
-	// records in FP32, per-entry sums in FP64.
+	// SPLIT32_SIMT: kinematics (J^-T, F^-T, det/log J, g, d) in FP64, contraction and
+	// records in FP32 on CUDA cores, per-entry sums in FP64.  SPLIT32: the same
+	// kinematics, the contraction on the tensor cores (3xTF32) for P2 and Q1.
 	switch (m.et)
 	{
 	case 1:
@@ -1926,13 +1950,15 @@ cudaError_t launch_hessian(const DevMesh &m, const DevPattern &p, const double *
 			 : prec == PREC_FP32 ? hessian_two_pass<P1Tet, float, float>(m, p, u, stage, psd, s)
 								 : hessian_two_pass<P1Tet, double, float>(m, p, u, stage, psd, s);
 	case 2:
-		return prec == PREC_FP64 ? hessian_two_pass<P2Tet, double, double>(m, p, u, stage, psd, s)
-			 : prec == PREC_FP32 ? hessian_two_pass<P2Tet, float, float>(m, p, u, stage, psd, s)
-								 : hessian_two_pass<P2Tet, double, float>(m, p, u, stage, psd, s);
+		return prec == PREC_FP64	? hessian_two_pass<P2Tet, double, double>(m, p, u, stage, psd, s)
+			 : prec == PREC_FP32	? hessian_two_pass<P2Tet, float, float>(m, p, u, stage, psd, s)
+			 : prec == PREC_SPLIT32 ? hessian_tc<P2Tet>(m, p, u, stage, psd, s)
+									: hessian_two_pass<P2Tet, double, float>(m, p, u, stage, psd, s);
 	case 3:
-		return prec == PREC_FP64 ? hessian_two_pass<Q1Hex, double, double>(m, p, u, stage, psd, s)
-			 : prec == PREC_FP32 ? hessian_two_pass<Q1Hex, float, float>(m, p, u, stage, psd, s)
-								 : hessian_two_pass<Q1Hex, double, float>(m, p, u, stage, psd, s);
+		return prec == PREC_FP64	? hessian_two_pass<Q1Hex, double, double>(m, p, u, stage, psd, s)
+			 : prec == PREC_FP32	? hessian_two_pass<Q1Hex, float, float>(m, p, u, stage, psd, s)
+			 : prec == PREC_SPLIT32 ? hessian_tc<Q1Hex>(m, p, u, stage, psd, s)
+									: hessian_two_pass<Q1Hex, double, float>(m, p, u, stage, psd, s);
 	}
 	return cudaErrorInvalidValue;
 }

@@ -23,6 +23,7 @@
 #include "../../include/pfgpu.h"
 #include "pfg_internal.h"
 
+#include <cstdint>
 #include <mutex>
 #include <string>
 
@@ -86,6 +87,22 @@ extern "C" int pfg_energy_noalloc(int elem_type, int n_elements, int n_nodes, in
 	if (n_elements > 0 && (!conn_soa || !X || !lame || !u)) return noalloc_fail(PFG_ERR_INVALID, "NULL input array");
 	if (elem_type == PFG_P2_TET && n_elements > 0 && !gconn_soa)
 		return noalloc_fail(PFG_ERR_INVALID, "gconn_soa is required for P2 elements");
+	// the size limits pfg_create applies to the same inputs
+	if ((long long)n_nodes * 3 > 0x7fffffffLL) return noalloc_fail(PFG_ERR_UNSUPPORTED, "too many nodes (3 * n_nodes > 2^31-1)");
+	if ((long long)n_geom_nodes * 3 > 0x7fffffffLL)
+		return noalloc_fail(PFG_ERR_UNSUPPORTED, "too many geometric nodes (3 * n_geom_nodes > 2^31-1)");
+	const int n_per = elem_type == PFG_P1_TET ? 4 : (elem_type == PFG_P2_TET ? 10 : 8);
+	if ((long long)n_elements * n_per > 0x7fffffffLL) return noalloc_fail(PFG_ERR_UNSUPPORTED, "E * n exceeds 2^31-1");
+	// The caller owns these pointers, so nothing guarantees the alignment the kernel's
+	// loads assume: (lambda, mu) is read as one 16-byte pair per element, the other
+	// arrays element by element.  A misaligned pointer would fault on the device and
+	// lose the CUDA context, so it is refused here, before any CUDA call.
+	auto misaligned = [](const void *p, unsigned a) { return p && (reinterpret_cast<uintptr_t>(p) & (a - 1)) != 0; };
+	if (misaligned(lame, 16)) return noalloc_fail(PFG_ERR_INVALID, "lame must be 16-byte aligned ((lambda, mu) pairs are read as one 16-byte load)");
+	if (misaligned(u, 8) || misaligned(X, 8) || misaligned(out, 8))
+		return noalloc_fail(PFG_ERR_INVALID, "u, X and out must be 8-byte aligned");
+	if (misaligned(conn_soa, 4) || misaligned(gconn_soa, 4))
+		return noalloc_fail(PFG_ERR_INVALID, "conn_soa and gconn_soa must be 4-byte aligned");
 	const long long per_block = pfg::energy_elems_per_block(elem_type);
 	const long long blocks = ((long long)n_elements + per_block - 1) / per_block;
 	if (blocks > PFG_NOALLOC_MAX_BLOCKS)

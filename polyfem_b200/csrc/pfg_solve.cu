@@ -264,6 +264,14 @@ int grid_spmv(int ngroups) { return ngroups <= 0 ? 1 : (int)std::min<long long>(
 
 size_t cg_partials_doubles() { return (size_t)(CG_NT / 32) * CG_MAX_GRID; } // one per SpMV warp, >= 3 per vector block
 
+cudaError_t launch_hessian_apply(int n_nodes, const int *outer, const int *inner, const double *vals, const double *p,
+								 double *q, cudaStream_t s)
+{
+	if (n_nodes > 0)
+		k_spmv<<<grid_spmv(n_nodes), CG_NT, 0, s>>>(n_nodes, nullptr, outer, inner, vals, p, q, nullptr, nullptr);
+	return cudaGetLastError();
+}
+
 cudaError_t launch_cg_diag_inv(int n, const int *outer, const int *inner, const double *vals, double *invd,
 							   cudaStream_t s)
 {

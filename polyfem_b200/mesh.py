@@ -203,3 +203,45 @@ def smooth_displacement(mesh: Mesh, amp: float, noise: float, seed: int) -> np.n
     s = amp * np.sin(2.0 * np.pi * mesh.node_pos[:, 0])
     u = np.repeat(s[:, None], 3, axis=1).reshape(-1)
     return u + noise * mesh.h * rng.standard_normal(mesh.n_dofs)
+
+
+# ---------------------------------------------------------------------------
+# The five benchmark workloads (seeded; the same inputs for the tests, the
+# benchmark and the CPU baseline)
+# ---------------------------------------------------------------------------
+WORKLOADS = {
+    1: "P1 tets 20^3 x 6 (48,000), homogeneous E=1e5 nu=0.35, u = 0.02 h N(0,1)",
+    2: "P2 tets 40^3 x 6 (384,000), lognormal Lame, u = 0.02 h N(0,1)",
+    3: "Q1 hexes 96^3 (884,736), jittered 0.1 h, lognormal Lame, u = 0.05 sin(2 pi x)[1,1,1] + 0.005 h N(0,1)",
+    4: "P1 tets 48^3 x 6 (663,552), lognormal Lame, u = 0.02 h N(0,1), adjoint p = N(0,1)",
+    5: "P2 tets 32^3 x 6 (196,608), jittered 0.1 h, homogeneous E=1e5 nu=0.35, u = 0.02 h N(0,1), adjoint p = N(0,1)",
+}
+SEED_JITTER, SEED_LAME, SEED_U, SEED_P = 3, 5, 2, 7
+
+
+def workload(k: int, grid: int | None = None):
+    """(mesh, lam, mu, u, p) of benchmark workload k (1..5); `grid` overrides the
+    cells per axis (same generators, for smaller cases of the same kind)."""
+    if k == 1:
+        mesh = structured_tet_mesh(grid or 20, 1)
+        lam, mu = homogeneous_lame(mesh.n_elements)
+    elif k == 2:
+        mesh = structured_tet_mesh(grid or 40, 2)
+        lam, mu = lognormal_lame(mesh.n_elements, SEED_LAME)
+    elif k == 3:
+        mesh = structured_hex_mesh(grid or 96, jitter=0.1, seed=SEED_JITTER)
+        lam, mu = lognormal_lame(mesh.n_elements, SEED_LAME)
+    elif k == 4:
+        mesh = structured_tet_mesh(grid or 48, 1)
+        lam, mu = lognormal_lame(mesh.n_elements, SEED_LAME)
+    elif k == 5:
+        mesh = structured_tet_mesh(grid or 32, 2, jitter=0.1, seed=SEED_JITTER)
+        lam, mu = homogeneous_lame(mesh.n_elements)
+    else:
+        raise ValueError("workload must be 1..5")
+    if k == 3:
+        u = smooth_displacement(mesh, 0.05, 0.005, SEED_U)
+    else:
+        u = random_displacement(mesh, 0.02, SEED_U)
+    p = np.random.default_rng(SEED_P).standard_normal(mesh.n_dofs)
+    return mesh, lam, mu, u, p

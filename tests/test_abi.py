@@ -107,3 +107,23 @@ def test_python_wrapper_raises_on_failure():
     from polyfem_b200 import NeoHookeanAssembler, PfgError
     with pytest.raises(PfgError):
         NeoHookeanAssembler(M.P1_TET, bad, mesh.X, lam, mu, n_nodes=mesh.n_nodes)
+
+
+def test_noalloc_refuses_misaligned_caller_pointers_before_any_launch():
+    """pfg_energy_noalloc takes caller-owned device pointers; (lambda, mu) is read as
+    one 16-byte pair, so a pointer 8 bytes off (a slice of a larger pool) is refused
+    on the host with PFG_ERR_INVALID.  The pointers are never dereferenced: the
+    check runs before any CUDA call, so this needs no GPU."""
+    L = _lib.lib()
+    base = 1 << 20  # a 256-byte aligned fake device address, never touched
+    p = lambda off: ctypes.c_void_p(base + off)
+    st = L.pfg_energy_noalloc(M.P1_TET, 6, 8, 8, p(0), None, p(0), p(8), p(0), 0, p(0), None)
+    assert st == 1
+    assert b"16-byte aligned" in L.pfg_last_error(None)
+    st = L.pfg_energy_noalloc(M.P1_TET, 6, 8, 8, p(0), None, p(4), p(0), p(0), 0, p(0), None)
+    assert st == 1 and b"8-byte aligned" in L.pfg_last_error(None)
+    st = L.pfg_energy_noalloc(M.P1_TET, 6, 8, 8, p(2), None, p(0), p(0), p(0), 0, p(0), None)
+    assert st == 1 and b"4-byte aligned" in L.pfg_last_error(None)
+    # the size limits pfg_create applies
+    st = L.pfg_energy_noalloc(M.P1_TET, 6, 1 << 30, 8, p(0), None, p(0), p(0), p(0), 0, p(0), None)
+    assert st == 4 and b"too many nodes" in L.pfg_last_error(None)

@@ -85,10 +85,13 @@ def test_fp32_paths_within_stated_bounds(case):
     assert rel_err(asm.force_shape_derivative(u, case["p"], "fp32"), orc.shape_vjp(u, case["p"])) <= 1e-4
 
 
-def test_split32_hessian_within_bound(case):
+@pytest.mark.parametrize("prec", ["split32", "split32_simt"])
+def test_split32_hessian_within_bound(case, prec):
+    """split32 (tensor cores for P2 and Q1) and split32_simt (CUDA cores) both
+    within the 1e-6 relative Frobenius bound of the split mode."""
     u, orc, asm = case["u"], case["orc"], case["asm"]
     _, _, v_ref = orc.hessian(u)
-    assert rel_err(asm.assemble_hessian_values(u, "split32"), v_ref) <= 1e-6
+    assert rel_err(asm.assemble_hessian_values(u, prec), v_ref) <= 1e-6
 
 
 def test_device_mode_matches_host_mode(case):
@@ -258,7 +261,8 @@ def test_medium_mesh_hessian_against_oracle(require_gpu, et, g):
     h64 = asm.assemble_hessian_values(u, "fp64")
     assert rel_err(h64, v) <= TOL64
     assert np.array_equal(h64, asm.assemble_hessian_values(u, "fp64"))
-    hs = asm.assemble_hessian_values(u, "split32")
-    assert rel_err(hs, v) <= 1e-6
-    assert np.array_equal(hs, asm.assemble_hessian_values(u, "split32"))
+    for prec in ("split32", "split32_simt"):
+        hs = asm.assemble_hessian_values(u, prec)
+        assert rel_err(hs, v) <= 1e-6, prec
+        assert np.array_equal(hs, asm.assemble_hessian_values(u, prec)), prec
     asm.close()
