@@ -376,14 +376,25 @@ def run_gpu(args):
     achieved = bytes_alg / (ms_split * 1e-3) / 1e9
     traffic = _profiled_traffic(args.grid)
 
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = measure_configs(stream, peak)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nt = cpu_threads_for(nnz)
-        times, t_first = time_cpu_reference(mesh, lam, mu, u, nt, 2)
-        t = min(times)
-        cpu = {"value": E / t, "unit": UNIT, "cores": nt, "kind": "port",
-               "sample": f"full {args.grid}^3 P2 Hessian ({E:,} elements), best of 2 steady-state calls "
-                         f"of the oracle's std::thread port; pattern build {t_first:.1f} s"}
+        times, t_first = time_cpu_reference(mesh, lam, mu, u, nt, 5)
+        t = statistics.median(times)
+        # one host thread on a bounded sample of the same kind (P2 12^3, seeded alike)
+        ms_, ls_, mus_, us_ = _workload(12)
+        t1, _ = time_cpu_reference(ms_, ls_, mus_, us_, 1, 5)
+        t1 = statistics.median(t1)
+        cpu = {"value": E / t, "unit": UNIT, "cores": nt, "kind": "port", "host_cores": os.cpu_count(),
+               "sample": f"full {args.grid}^3 P2 Hessian ({E:,} elements), median of 5 steady-state calls "
+                         f"of the oracle's std::thread port on {nt} threads (host has {os.cpu_count()} cores); "
+                         f"pattern build {t_first:.1f} s",
+               "one_thread": {"value": ms_.n_elements / t1, "unit": UNIT, "cores": 1,
+                              "sample": f"P2 12^3 ({ms_.n_elements:,} elements), median of 5 steady-state calls"}}
 
     if rank == 0:
         line = {
@@ -411,6 +422,7 @@ def run_gpu(args):
                                  "on the context's stream; frac of measured HBM copy bandwidth; traffic = ncu "
                                  "DRAM bytes per element of the 24^3 capture x elements"},
             "cpu_baseline": cpu,
+            "configs": configs,
             "clocks": clocks,
             "gpu_launches": 2 * args.steps,
         }
@@ -420,6 +432,99 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+# ----------------------------------------------------------------- the other four workloads
+def measure_configs(stream, peak):
+    """Device times of the operations the other workloads name, inputs resident in
+    HBM, L2 flushed before every timed launch (CUDA events on the context's stream):
+      1  P1 20^3: FP64 energy, gradient, Hessian (L2-resident sizes: the flush makes
+         every launch read from DRAM)
+      1L P1 48^3: FP64 and FP32 energy and gradient (the HBM roofline of P1)
+      3  Q1 96^3 jittered: FP32 energy and gradient (FP64 det and reduction), split32
+         Hessian on the tensor cores, FP64 Hessian, split error vs FP64
+      4  P1 48^3: material VJP
+      5  P2 32^3 jittered: shape VJP, FP64 and FP32
+    Algorithmic bytes: conn + gconn (when distinct) + Lame + X + u (+ p) read once,
+    outputs written once (+ the Hessian's one int32 per element node pair)."""
+    import ctypes
+
+    import torch
+
+    from polyfem_b200 import NeoHookeanAssembler
+    from polyfem_b200 import mesh as M
+    from polyfem_b200._lib import lib
+
+    L = lib()
+    vp = ctypes.c_void_p
+    flush = torch.zeros(128 << 20, dtype=torch.float32, device="cuda")
+    out = {}
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        return _events_ms_flushed(stream, fn, reps, flush)
+
+    def entry(ms, E, nbytes):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        return {"ms": round(ms, 4), "elements_per_s": E / (ms * 1e-3), "alg_bytes": int(nbytes),
+                "alg_GBps": round(gbs, 1), "frac_hbm": round(gbs / peak, 4)}
+
+    plan = [("1_p1_20", 1, None), ("1L_p1_48", 4, None), ("3_q1_96", 3, None), ("4_p1_48", 4, None),
+            ("5_p2_32", 5, None)]
+    for key, k, grid in plan:
+        mesh, lam, mu, u, p = M.workload(k, grid)
+        E, n, ng = mesh.n_elements, mesh.conn.shape[1], mesh.gconn.shape[1]
+        asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+        h = asm.handle
+        L.pfg_set_stream(h, vp(stream.cuda_stream))
+        ud = torch.tensor(u, dtype=torch.float64, device="cuda")
+        pd = torch.tensor(p, dtype=torch.float64, device="cuda")
+        o = torch.empty(max(mesh.n_dofs, 2 * E, 3 * mesh.n_geom_nodes), dtype=torch.float64, device="cuda")
+        U, P, O = vp(ud.data_ptr()), vp(pd.data_ptr()), vp(o.data_ptr())
+        ins = (E * n * 4 + (E * ng * 4 if mesh.gconn is not mesh.conn else 0) + E * 16
+               + mesh.n_geom_nodes * 24 + mesh.n_nodes * 24)
+        res = {"workload": M.WORKLOADS[k] if grid is None else f"workload {k} at {grid}^3", "E": E}
+        if key == "1_p1_20":
+            nnz = asm.hessian_nnz()
+            res["energy_fp64"] = entry(timed(lambda: L.pfg_energy(h, U, 1, 0, O), 50), E, ins + 8)
+            res["gradient_fp64"] = entry(timed(lambda: L.pfg_gradient(h, U, 1, 0, O), 50), E, ins + mesh.n_dofs * 8)
+            res["hessian_fp64"] = entry(timed(lambda: L.pfg_hessian(h, U, 1, 0, 0, None), 20), E,
+                                        algorithmic_bytes(mesh, nnz))
+        elif key == "1L_p1_48":
+            for prec, name in ((0, "fp64"), (1, "fp32")):
+                res[f"energy_{name}"] = entry(timed(lambda: L.pfg_energy(h, U, 1, prec, O), 50), E, ins + 8)
+                res[f"gradient_{name}"] = entry(timed(lambda: L.pfg_gradient(h, U, 1, prec, O), 50), E,
+                                                ins + mesh.n_dofs * 8)
+        elif key == "3_q1_96":
+            nnz = asm.hessian_nnz()
+            res["energy_fp32"] = entry(timed(lambda: L.pfg_energy(h, U, 1, 1, O), 30), E, ins + 8)
+            res["gradient_fp32"] = entry(timed(lambda: L.pfg_gradient(h, U, 1, 1, O), 30), E, ins + mesh.n_dofs * 8)
+            v64 = torch.empty(nnz, dtype=torch.float64, device="cuda")
+            vs = torch.empty(nnz, dtype=torch.float64, device="cuda")
+            V64, VS = vp(v64.data_ptr()), vp(vs.data_ptr())
+            res["hessian_split32"] = entry(timed(lambda: L.pfg_hessian(h, U, 1, 2, 0, VS), 10), E,
+                                           algorithmic_bytes(mesh, nnz))
+            res["hessian_fp64"] = entry(timed(lambda: L.pfg_hessian(h, U, 1, 0, 0, V64), 10), E,
+                                        algorithmic_bytes(mesh, nnz))
+            torch.cuda.synchronize()
+            res["hessian_split32"]["rel_err_vs_fp64"] = float(torch.linalg.vector_norm(vs - v64)
+                                                              / torch.linalg.vector_norm(v64))
+            res["split_over_fp64"] = res["hessian_fp64"]["ms"] / res["hessian_split32"]["ms"]
+            del v64, vs
+        elif key == "4_p1_48":
+            res["material_vjp"] = entry(timed(lambda: L.pfg_material_vjp(h, U, P, 1, O), 50), E,
+                                        ins + mesh.n_nodes * 24 + 2 * E * 8)
+        elif key == "5_p2_32":
+            for prec, name in ((0, "fp64"), (1, "fp32")):
+                res[f"shape_vjp_{name}"] = entry(timed(lambda: L.pfg_shape_vjp(h, U, P, 1, prec, O), 30), E,
+                                                 ins + mesh.n_nodes * 24 + 3 * mesh.n_geom_nodes * 8)
+            torch.cuda.synchronize()
+        out[key] = res
+        asm.close()
+        torch.cuda.empty_cache()
+    return out
 
 
 # ----------------------------------------------------------------- per-operation suite
@@ -574,6 +679,36 @@ def run_suite(args):
     return 0
 
 
+def run_profile_case(args):
+    """The Hessian assembly of one precision alone on a G^3 P2 cube (the command the
+    ncu captures run): warm-up calls, then `steps` timed calls; prints one line."""
+    import torch
+
+    from polyfem_b200 import NeoHookeanAssembler
+    from polyfem_b200._lib import check, lib
+    from polyfem_b200.assembler import PRECISIONS
+
+    prec = PRECISIONS[args.profile]
+    mesh, lam, mu, u = _workload(args.grid)
+    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
+    asm.hessian_nnz()
+    L = lib()
+    h = asm.handle
+    stream = torch.cuda.Stream()
+    check(L.pfg_set_stream(h, ctypes_ptr(stream.cuda_stream)), h, "pfg_set_stream")
+    ud = torch.tensor(u, device="cuda", dtype=torch.float64)
+    fn = lambda: check(L.pfg_hessian(h, ctypes_ptr(ud.data_ptr()), 1, prec, 0, None), h, "pfg_hessian")
+    for _ in range(args.warmup):
+        fn()
+    torch.cuda.synchronize()
+    ms = _events_ms(stream, fn, args.steps)
+    check(L.pfg_synchronize(h), h, "pfg_synchronize")
+    print(json.dumps({"profile_case": workload_name(args.grid), "precision": args.profile, "ms": ms,
+                      "elements_per_s": mesh.n_elements / (ms * 1e-3)}), flush=True)
+    asm.close()
+    return 0
+
+
 def ctypes_ptr(p):
     import ctypes
     return ctypes.c_void_p(int(p))
@@ -614,11 +749,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", type=int, default=40, help="P2 cube cells per axis (40 = the benchmark workload)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-configs", action="store_true", help="skip the per-workload timings of configs 1, 3, 4, 5")
     ap.add_argument("--suite", action="store_true", help="per-operation timings on all workloads")
+    ap.add_argument("--profile", default="", choices=["", "fp64", "fp32", "split32", "split32_simt"],
+                    help="time only this precision's Hessian on the --grid cube (the ncu capture command)")
     ap.add_argument("--only", default="", help="comma-separated suite workload keys (" + ",".join(SUITE) + ")")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.profile:
+        return run_profile_case(args)
     if args.suite:
         return run_suite(args)
     if args.impl == "reference":

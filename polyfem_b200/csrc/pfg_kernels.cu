@@ -857,6 +857,135 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 	}
 }
 
+// Column form of the reduction (used whenever a node's column block fits the
+// per-warp buffer).  One warp per column node B: the warp zeroes a shared-memory
+// copy of B's 9 deg(B) CSC values, laid out exactly as the CSC stores them
+// (column c at c * 3 deg, row 3 rank + r), then walks B's incidences in ascending
+// order and adds every incidence's n blocks H_e(a, b) at the ranks of their row
+// nodes (pat.strip_rank, one uint16 per (incidence, local node)), and finally
+// copies the buffer out in 16-byte stores.  Every CSC entry receives its
+// contributions in incidence order, exactly as in k_hessian_reduce: the two
+// kernels give bitwise identical values.  Within an incidence the 9 n values are
+// spread over the lanes (distinct buffer entries, so no atomics); the staged
+// values and ranks of KB incidences are loaded before any of them is added, so
+// that their loads overlap.
+template <class EL, class T, int WARPS, int KB>
+__global__ void __launch_bounds__(WARPS * 32, 32 / WARPS)
+	k_hessian_columns(DevMesh m, DevPattern pat, const T *__restrict__ stage, int buf_doubles)
+{
+	constexpr int N = EL::N, TP = tri_pad(EL::N), NV = 9 * EL::N, R = (NV + 31) / 32;
+	extern __shared__ __align__(16) double colbuf[];
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int B = blockIdx.x * WARPS + warp;
+	if (B >= m.N) return;
+	double *buf = colbuf + (size_t)warp * buf_doubles;
+	const int o0 = __ldg(pat.outer + 3 * B);
+	const int stride = __ldg(pat.outer + 3 * B + 1) - o0; // 3 deg(B)
+	const int nval = 3 * stride;                          // 9 deg(B)
+	for (int i = lane; i < nval; i += 32) buf[i] = 0.0;
+	// this lane's values of an incidence: t = lane + 32 i -> local row node a, (r, c)
+	int la[R], lr[R], lc[R];
+#pragma unroll
+	for (int i = 0; i < R; ++i)
+	{
+		const int t = lane + 32 * i;
+		const int tt = t < NV ? t : 0;
+		la[i] = tt / 9;
+		lr[i] = (tt % 9) % 3;
+		lc[i] = (tt % 9) / 3;
+	}
+	__syncwarp();
+	const int s0 = __ldg(m.inc_off + B), s1 = __ldg(m.inc_off + B + 1);
+	for (int k0 = s0; k0 < s1; k0 += KB)
+	{
+		T v[KB][R];
+		int idx[KB][R];
+#pragma unroll
+		for (int j = 0; j < KB; ++j)
+		{
+			const int k = k0 + j;
+			const bool kin = k < s1;
+			const int eb = kin ? __ldg(m.inc_eb + k) : 0;
+			const int e = eb / N, b = eb - e * N;
+			const T *tri = stage + (size_t)e * TP;
+#pragma unroll
+			for (int i = 0; i < R; ++i)
+			{
+				const bool on = kin && (lane + 32 * i < NV);
+				const int a = la[i], r = lr[i], c = lc[i];
+				// H_e(3a+r, 3b+c): block (a, b) value [c][r] when a <= b, else block (b, a) value [r][c]
+				const int off = a <= b ? 9 * tri_index(N, a, b) + 3 * c + r : 9 * tri_index(N, b, a) + 3 * r + c;
+				const int rank = on ? (int)__ldg(pat.strip_rank + (size_t)k * N + a) : 0;
+				v[j][i] = on ? __ldg(tri + off) : T(0);
+				idx[j][i] = on ? c * stride + 3 * rank + r : -1;
+			}
+		}
+#pragma unroll
+		for (int j = 0; j < KB; ++j)
+		{
+#pragma unroll
+			for (int i = 0; i < R; ++i)
+				if (idx[j][i] >= 0) buf[idx[j][i]] += double(v[j][i]);
+			__syncwarp();
+		}
+	}
+	if (pat.red_col_start == nullptr)
+	{
+		// 9 deg doubles, contiguous in the CSC; o0 is a multiple of 9, so the start is
+		// 8-byte aligned only: peel to a 16-byte boundary, then double2 stores
+		double *dst = pat.values + o0;
+		const int head = (reinterpret_cast<uintptr_t>(dst) & 15) ? 1 : 0;
+		if (head && lane == 0) dst[0] = buf[0];
+		const int nv2 = (nval - head) / 2;
+		double2 *d2 = reinterpret_cast<double2 *>(dst + head);
+		for (int i = lane; i < nv2; i += 32) d2[i] = make_double2(buf[head + 2 * i], buf[head + 2 * i + 1]);
+		if (lane == 0 && head + 2 * nv2 < nval) dst[nval - 1] = buf[nval - 1];
+	}
+	else
+	{
+		for (int i = lane; i < nval; i += 32)
+		{
+			const int c = i / stride, rr = i - c * stride; // rr = 3 rank + r
+			const int cs = __ldg(pat.red_col_start + 3 * B + c);
+			if (cs < 0) continue;
+			const unsigned short ro = __ldg(pat.red_row_off + o0 / 3 + rr);
+			if (ro != 0xFFFF) pat.values[cs + ro] = buf[i];
+		}
+	}
+}
+
+// Pass 2 of every Hessian-pattern assembly: the column kernel when the largest
+// column block fits its per-warp shared buffer (9 max_deg doubles per warp),
+// else the plan-driven k_hessian_reduce.  Both give the same values bit for bit.
+#ifndef PFG_COLUMNS_WARPS
+#define PFG_COLUMNS_WARPS 8
+#endif
+#ifndef PFG_COLUMNS_KB
+#define PFG_COLUMNS_KB 4
+#endif
+template <class EL, class T>
+static cudaError_t launch_reduce(const DevMesh &m, const DevPattern &p, const T *stage, cudaStream_t s)
+{
+	if (m.N <= 0) return cudaSuccess;
+	constexpr int W = PFG_COLUMNS_WARPS;
+	const int buf = ((9 * p.max_deg + 1) / 2) * 2; // doubles per warp, kept 16-byte aligned
+	const size_t smem = (size_t)W * buf * sizeof(double);
+	if (p.strip_rank && smem <= 96 * 1024)
+	{
+		auto kern = k_hessian_columns<EL, T, W, PFG_COLUMNS_KB>;
+		if (smem > 48 * 1024)
+		{
+			cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+			if (e != cudaSuccess) return e;
+		}
+		kern<<<(m.N + W - 1) / W, W * 32, smem, s>>>(m, p, stage, buf);
+		return cudaGetLastError();
+	}
+	constexpr int WARPS = 8;
+	k_hessian_reduce<EL, T, WARPS><<<(m.N + WARPS - 1) / WARPS, WARPS * 32, 0, s>>>(m, p, stage);
+	return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // ipc::project_to_psd (PSDProjectionMethod::CLAMP), applied to every element
 // matrix before the scatter when NLAssembler::assemble_hessian is called with
@@ -1714,7 +1843,7 @@ static cudaError_t finish_fp64_hessian(const DevMesh &m, const DevPattern &p, do
 		k_project_psd<EL, double, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
 	}
 	const int ng = (m.N + WARPS - 1) / WARPS;
-	if (ng > 0) k_hessian_reduce<EL, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+	if (ng > 0) return launch_reduce<EL, double>(m, p, stage, s);
 	return cudaGetLastError();
 }
 
@@ -1845,15 +1974,15 @@ cudaError_t launch_mass(const DevMesh &m, const DevPattern &p, const double *rho
 	{
 	case 1:
 		if (nb) k_mass_blocks<P1Tet, WPB><<<nb, WPB * 32, 0, s>>>(m, rho, stage);
-		if (ng) k_hessian_reduce<P1Tet, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+		if (ng) return launch_reduce<P1Tet, double>(m, p, stage, s);
 		break;
 	case 2:
 		if (nb) k_mass_blocks<P2Tet, WPB><<<nb, WPB * 32, 0, s>>>(m, rho, stage);
-		if (ng) k_hessian_reduce<P2Tet, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+		if (ng) return launch_reduce<P2Tet, double>(m, p, stage, s);
 		break;
 	case 3:
 		if (nb) k_mass_blocks<Q1Hex, WPB><<<nb, WPB * 32, 0, s>>>(m, rho, stage);
-		if (ng) k_hessian_reduce<Q1Hex, double, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+		if (ng) return launch_reduce<Q1Hex, double>(m, p, stage, s);
 		break;
 	default: return cudaErrorInvalidValue;
 	}
@@ -1881,7 +2010,7 @@ static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const
 		k_project_psd<EL, T, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
 	}
 	const int ng = (m.N + WARPS - 1) / WARPS;
-	if (ng > 0) k_hessian_reduce<EL, T, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+	if (ng > 0) return launch_reduce<EL, T>(m, p, stage, s);
 	return cudaGetLastError();
 }
 
@@ -1906,7 +2035,7 @@ static cudaError_t hessian_tc(const DevMesh &m, const DevPattern &p, const doubl
 		k_project_psd<EL, float, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
 	}
 	const int ng = (m.N + WARPS - 1) / WARPS;
-	if (ng > 0) k_hessian_reduce<EL, float, WARPS><<<ng, WARPS * 32, 0, s>>>(m, p, stage);
+	if (ng > 0) return launch_reduce<EL, float>(m, p, stage, s);
 	return cudaGetLastError();
 }
 

@@ -418,7 +418,11 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 				rec[18] = (float)(lm.y * da);
 				rec[19] = (float)(lm.x * da);
 				rec[20] = (float)((lm.y - lm.x * lj) * da);
-				rec[21] = rec[22] = rec[23] = 0.f;
+				// J <= 0 (log J is NaN or -inf, as in the reference): the whole element
+				// matrix must come out NaN.  The tensor cores do not carry a NaN operand
+				// through a zero factor of Phi, so the epilogue writes the NaNs itself.
+				rec[21] = (J > 0.0 && isfinite(lj)) ? 0.f : 1.f;
+				rec[22] = rec[23] = 0.f;
 			}
 			named_arrive(BAR_FULL0 + buf, TC_THREADS);
 		}
@@ -443,6 +447,7 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 			const int buf = it & 1;
 			const int e0 = t * TE, ne = min(TE, m.E - e0);
 			named_sync(BAR_FULL0 + buf, TC_THREADS);
+			bool bad = false; // the row's element has a point with J <= 0
 			if (row < C::ROWS)
 			{
 				const int el = row / 9, rc = row % 9, r = rc / 3, c = rc % 3;
@@ -461,6 +466,7 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 #pragma unroll
 					for (int k = 0; k < 9; ++k) g[k] = R[9 + k];
 					const float dmu = (r == c) ? R[18] : 0.f, dl = R[19], dw = R[20];
+					bad |= R[21] != 0.f;
 #pragma unroll
 					for (int k = 0; k < 3; ++k)
 					{
@@ -533,6 +539,11 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 			{
 #pragma unroll
 				for (int i = 0; i < C::NPAD; ++i) v[i] = __int_as_float(0x7fc00000); // NaN: the result is invalid
+			}
+			if (bad)
+			{
+#pragma unroll
+				for (int i = 0; i < C::NPAD; ++i) v[i] = __int_as_float(0x7fc00000);
 			}
 			if (row < 9 * ne)
 			{
