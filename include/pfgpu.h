@@ -310,10 +310,10 @@ int pfg_mass_matrix(pfg_context *ctx, const double *rho, int mem, double *values
 int pfg_lump_matrix(pfg_context *ctx, const double *values, int mem, double *diag);
 
 /* ---------------------------------------------------------------------------
- * Linear solve on the device.  After every assembly NewtonMethod hands the
- * Hessian to its linear solver through polysolve's linear::Solver
- * (analyze_pattern, factorize, solve; called from solver/NLProblem.cpp:261-262,
- * 419-420).  pfg_cg_solve is that hand-off without a host round trip: the
+ * Linear solve on the device.  After every assembly the Newton step hands the
+ * Hessian that NLProblem::hessian returns (solver/NLProblem.cpp:615-621) to its
+ * linear solver through polysolve's linear::Solver (analyze_pattern, factorize,
+ * solve; called inside the Newton solver of polysolve@47dc48d, external).  pfg_cg_solve is that hand-off without a host round trip: the
  * conjugate gradient of Eigen's ConjugateGradient<..., Lower|Upper,
  * DiagonalPreconditioner>, the "Eigen::ConjugateGradient" choice of polysolve,
  * run on the context's assembled Hessian:

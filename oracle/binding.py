@@ -315,7 +315,7 @@ def lump_matrix(outer, inner, values):
 def conjugate_gradient(outer, inner, values, b, tol, max_iter, x0=None):
     """Eigen 3.4's ConjugateGradient<SparseMatrix, Lower|Upper, DiagonalPreconditioner>
     (the "Eigen::ConjugateGradient" choice of polysolve's linear::Solver, which
-    NewtonMethod calls after every assembly, solver/NLProblem.cpp:261-262,419-420),
+    the Newton step of polysolve@47dc48d (external) applies to the Hessian NLProblem::hessian returns, solver/NLProblem.cpp:615-621),
     restated on a ColMajor CSC matrix.  Eigen is a dependency absent from the
     reference tree (cmake/recipes/eigen.cmake pins 3.4.0); its published iteration:
     r = b - A x, stop when |r|^2 < max(tol^2 |b|^2, smallest normal double),

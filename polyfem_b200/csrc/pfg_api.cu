@@ -38,7 +38,6 @@ struct pfg_context
 	double *d_values = nullptr;
 	unsigned int *d_contrib = nullptr;
 	unsigned short *d_blk_rel = nullptr;
-	unsigned short *d_strip_rank = nullptr;
 	// Dirichlet reduction (pfg_set_dirichlet)
 	bool has_dirichlet = false;
 	std::vector<int> h_constrained;      // sorted unique constrained dofs
@@ -385,10 +384,6 @@ int build_pattern(pfg_context *c)
 	PFG_CUDA(c, cudaMalloc(&c->d_values, sizeof(double) * std::max<long long>(nnz, 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_contrib, sizeof(unsigned int) * std::max<size_t>(contrib.size(), 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_blk_rel, sizeof(unsigned short) * std::max<size_t>(blk_rel.size(), 1)));
-	PFG_CUDA(c, cudaMalloc(&c->d_strip_rank, sizeof(unsigned short) * std::max<size_t>(strip_rank.size(), 1)));
-	if (!strip_rank.empty())
-		PFG_CUDA(c, cudaMemcpy(c->d_strip_rank, strip_rank.data(), sizeof(unsigned short) * strip_rank.size(),
-							   cudaMemcpyHostToDevice));
 	PFG_CUDA(c, cudaMemcpy(c->d_outer, outer.data(), sizeof(int) * (ndof + 1), cudaMemcpyHostToDevice));
 	if (nnz) PFG_CUDA(c, cudaMemcpy(c->d_inner, inner.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice));
 	if (!contrib.empty())
@@ -403,7 +398,6 @@ int build_pattern(pfg_context *c)
 	c->pat.inner = c->d_inner;
 	c->pat.contrib = c->d_contrib;
 	c->pat.blk_rel = c->d_blk_rel;
-	c->pat.strip_rank = c->d_strip_rank;
 	c->pat.values = c->d_values;
 	c->has_pattern = true;
 	return PFG_OK;
@@ -541,7 +535,7 @@ int build_dirichlet(pfg_context *c)
 
 void free_all(pfg_context *c)
 {
-	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_contrib, c->d_blk_rel, c->d_strip_rank, c->d_eb_inc, c->d_g_eb_inc,
+	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_contrib, c->d_blk_rel, c->d_eb_inc, c->d_g_eb_inc,
 					c->d_inc_off, c->d_inc_eb, c->d_ginc_off, c->d_ginc_eb, c->d_vec_stage, c->d_hess_stage[0],
 					c->d_hess_stage[1], c->sc.partials, c->sc.ticket, c->sc.inverted, c->d_result, c->d_u, c->d_p, c->d_out};
 	for (void *p : ptrs)

@@ -68,9 +68,6 @@ struct DevPattern
 	const int *inner = nullptr;
 	const unsigned int *contrib = nullptr;
 	const unsigned short *blk_rel = nullptr;
-	// rank of the row node of local a in the column of incidence k's node, at
-	// strip_rank[k * n + a] (incidences in inc_eb order): the column kernel's plan
-	const unsigned short *strip_rank = nullptr;
 	double *values = nullptr;
 	// Dirichlet-reduced output (BCLagrangianForm::project_hessian): when red_col_start
 	// is set the reduction writes only entries whose row and column are free, at

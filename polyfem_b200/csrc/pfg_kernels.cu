@@ -141,11 +141,15 @@ __global__ void __launch_bounds__(NT, EL::ET == 1 ? 8 : 1) k_gradient(DevMesh m,
 {
 	const int e = blockIdx.x * NT + threadIdx.x;
 	if (e >= m.E) return;
-	T Xg[EL::NG][3];
-	T U[EL::N][3];
+	// The displacement gradient grad u = sum_a u_a (x) grad(phi_a) is formed in FP64
+	// in every mode: it is a difference of nearby nodal values, and rounding u or
+	// J^-T to FP32 first costs ~3x in the FP32 gradient's error on smooth fields.
+	// The stress and its contraction then run in T.
+	double Xg[EL::NG][3];
+	double U[EL::N][3];
 	int nodes[EL::N];
-	load_geom<EL, T>(m, e, Xg);
-	load_nodal<EL, T>(m, e, u, U, nodes);
+	load_geom<EL, double>(m, e, Xg);
+	load_nodal<EL, double>(m, e, u, U, nodes);
 	const double2 lm = __ldg(m.lame + e);
 	const double lambda = lm.x, mu = lm.y;
 	// element gradient, accumulated as G[a][d] = sum_q sum_r gref(q,a,r) (da P J^-1)[d][r]
@@ -153,26 +157,31 @@ __global__ void __launch_bounds__(NT, EL::ET == 1 ? 8 : 1) k_gradient(DevMesh m,
 	T Gacc[EL::N][3];
 #pragma unroll
 	for (int a = 0; a < EL::N; ++a) Gacc[a][0] = Gacc[a][1] = Gacc[a][2] = T(0);
-	T Jit[3][3];
+	double Jitd[3][3];
 	double detJ = 0.0;
-	if constexpr (EL::AFFINE) geometry<EL, T>(0, Xg, Jit, detJ);
+	if constexpr (EL::AFFINE) geometry<EL, double>(0, Xg, Jitd, detJ);
 	bool bad = false;
 #pragma unroll
 	for (int q = 0; q < EL::NQ; ++q)
 	{
-		if constexpr (!EL::AFFINE) geometry<EL, T>(q, Xg, Jit, detJ);
-		T A[3][3];
+		if constexpr (!EL::AFFINE) geometry<EL, double>(q, Xg, Jitd, detJ);
+		T Jit[3][3];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) Jit[r][c] = T(Jitd[r][c]);
+		double A[3][3];
 #pragma unroll
 		for (int r = 0; r < 3; ++r)
 #pragma unroll
 			for (int c = 0; c < 3; ++c)
 			{
-				T s = T(0);
+				double s = 0.0;
 #pragma unroll
 				for (int a = 0; a < EL::N; ++a)
 				{
 					const double gr = gref<EL>(q, a, c);
-					if (gr != 0.0) s += U[a][r] * T(gr);
+					if (gr != 0.0) s += U[a][r] * gr;
 				}
 				A[r][c] = s;
 			}
@@ -181,7 +190,7 @@ __global__ void __launch_bounds__(NT, EL::ET == 1 ? 8 : 1) k_gradient(DevMesh m,
 		for (int r = 0; r < 3; ++r)
 #pragma unroll
 			for (int c = 0; c < 3; ++c)
-				F[r][c] = A[r][0] * Jit[0][c] + A[r][1] * Jit[1][c] + A[r][2] * Jit[2][c] + (r == c ? T(1) : T(0));
+				F[r][c] = T(A[r][0] * Jitd[0][c] + A[r][1] * Jitd[1][c] + A[r][2] * Jitd[2][c]) + (r == c ? T(1) : T(0));
 		double J;
 		if constexpr (sizeof(T) == 8)
 			J = det3(F);
@@ -775,13 +784,35 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 // order, the three values (rows 3*rank .. 3*rank+2 of column 3B+c) of every
 // staged block that lands on its rank, read through the reduction plan
 // (consecutive values of block (a, b); for a flagged transposed block (b, a), the
-// values c, c+3, c+6), and writes them once.  No shared memory, no atomics: the
-// sum order of every entry is fixed.
+// values c, c+3, c+6), and writes them once.  No atomics: the sum order of every
+// entry is fixed.
+//
+// The warp first copies B's plan (its n * #incidences entries) and group starts
+// into shared memory with coalesced loads, so that an item reads its
+// contributions' offsets without a global round trip and issues the block-value
+// loads of RED_UNROLL contributions back to back.  Nodes whose plan exceeds the
+// shared copy (more than RED_PLAN entries or RED_DEG neighbours) read it from
+// global memory, two entries ahead.
+constexpr int RED_PLAN = 256, RED_DEG = 128, RED_UNROLL = 4;
+
+template <class T>
+__device__ __forceinline__ void red_load3(const T *__restrict__ stage, unsigned q, int c, T (&x)[3])
+{
+	const bool tr = q & TRI_TRANSPOSED;
+	const T *p = stage + (q & ~TRI_TRANSPOSED) + (tr ? c : 3 * c);
+	const int st = tr ? 3 : 1;
+	x[0] = __ldg(p);
+	x[1] = __ldg(p + st);
+	x[2] = __ldg(p + 2 * st);
+}
+
 template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 8)
+__global__ void __launch_bounds__(WARPS * 32, sizeof(T) == 8 ? 4 : 6)
 	k_hessian_reduce(DevMesh m, DevPattern pat, const T *__restrict__ stage)
 {
 	constexpr int N = EL::N;
+	__shared__ unsigned s_plan[WARPS][RED_PLAN];
+	__shared__ unsigned short s_rel[WARPS][RED_DEG + 1];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int B = blockIdx.x * WARPS + warp;
 	if (B >= m.N) return;
@@ -793,45 +824,65 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 	const unsigned *cl = pat.contrib + (size_t)s0 * N;
 	const unsigned short *br = pat.blk_rel + o0 / 9;
 	double *dst = pat.values + o0;
+	const bool local = tot <= RED_PLAN && deg <= RED_DEG;
+	if (local)
+	{
+		for (int i = lane; i < tot; i += 32) s_plan[warp][i] = __ldg(cl + i);
+		for (int i = lane; i < deg; i += 32) s_rel[warp][i] = __ldg(br + i);
+		if (lane == 0) s_rel[warp][deg] = (unsigned short)tot;
+		__syncwarp();
+	}
 	for (int it = lane; it < stride; it += 32)
 	{
 		// (rank, column) items rank-major: the three items of the diagonal block,
 		// which has the longest contribution list, share one pass of the warp
 		const int r = it / 3, c = it - 3 * r;
-		const int k0 = __ldg(br + r);
-		const int k1 = (r + 1 < deg) ? (int)__ldg(br + r + 1) : tot;
 		double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-		// two contributions per step, the next step's plan entries loaded ahead;
-		// the sum order stays k ascending
-		unsigned qa = k0 < k1 ? __ldg(cl + k0) : 0u;
-		unsigned qb = k0 + 1 < k1 ? __ldg(cl + k0 + 1) : 0u;
-		for (int k = k0; k < k1; k += 2)
+		if (local)
 		{
-			const unsigned q0 = qa, q1 = qb;
-			const bool two = k + 1 < k1;
-			qa = k + 2 < k1 ? __ldg(cl + k + 2) : 0u;
-			qb = k + 3 < k1 ? __ldg(cl + k + 3) : 0u;
-			// (a, b): values 3c, 3c+1, 3c+2 of the block; transposed (b, a): c, c+3, c+6
-			const bool t0 = q0 & TRI_TRANSPOSED, t1 = q1 & TRI_TRANSPOSED;
-			const T *p0 = stage + (q0 & ~TRI_TRANSPOSED) + (t0 ? c : 3 * c);
-			const T *p1 = stage + (q1 & ~TRI_TRANSPOSED) + (t1 ? c : 3 * c);
-			const int s0_ = t0 ? 3 : 1, s1_ = t1 ? 3 : 1;
-			const T x0 = __ldg(p0), x1 = __ldg(p0 + s0_), x2 = __ldg(p0 + 2 * s0_);
-			T y0 = T(0), y1 = T(0), y2 = T(0);
-			if (two)
+			const int k0 = s_rel[warp][r], k1 = s_rel[warp][r + 1];
+			for (int k = k0; k < k1; k += RED_UNROLL)
 			{
-				y0 = __ldg(p1);
-				y1 = __ldg(p1 + s1_);
-				y2 = __ldg(p1 + 2 * s1_);
+				T x[RED_UNROLL][3];
+#pragma unroll
+				for (int j = 0; j < RED_UNROLL; ++j)
+					if (k + j < k1) red_load3(stage, s_plan[warp][k + j], c, x[j]);
+#pragma unroll
+				for (int j = 0; j < RED_UNROLL; ++j)
+					if (k + j < k1)
+					{
+						a0 += double(x[j][0]);
+						a1 += double(x[j][1]);
+						a2 += double(x[j][2]);
+					}
 			}
-			a0 += double(x0);
-			a1 += double(x1);
-			a2 += double(x2);
-			if (two)
+		}
+		else
+		{
+			const int k0 = __ldg(br + r);
+			const int k1 = (r + 1 < deg) ? (int)__ldg(br + r + 1) : tot;
+			// two contributions per step, the next step's plan entries loaded ahead;
+			// the sum order stays k ascending
+			unsigned qa = k0 < k1 ? __ldg(cl + k0) : 0u;
+			unsigned qb = k0 + 1 < k1 ? __ldg(cl + k0 + 1) : 0u;
+			for (int k = k0; k < k1; k += 2)
 			{
-				a0 += double(y0);
-				a1 += double(y1);
-				a2 += double(y2);
+				const unsigned q0 = qa, q1 = qb;
+				const bool two = k + 1 < k1;
+				qa = k + 2 < k1 ? __ldg(cl + k + 2) : 0u;
+				qb = k + 3 < k1 ? __ldg(cl + k + 3) : 0u;
+				T x[3], y[3] = {T(0), T(0), T(0)};
+				red_load3(stage, q0, c, x);
+				if (two) red_load3(stage, q1, c, y);
+				a0 += double(x[0]);
+				a1 += double(x[1]);
+				a2 += double(x[2]);
+				if (two)
+				{
+					a0 += double(y[0]);
+					a1 += double(y[1]);
+					a2 += double(y[2]);
+				}
 			}
 		}
 		if (pat.red_col_start == nullptr)
@@ -857,130 +908,11 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 	}
 }
 
-// Column form of the reduction (used whenever a node's column block fits the
-// per-warp buffer).  One warp per column node B: the warp zeroes a shared-memory
-// copy of B's 9 deg(B) CSC values, laid out exactly as the CSC stores them
-// (column c at c * 3 deg, row 3 rank + r), then walks B's incidences in ascending
-// order and adds every incidence's n blocks H_e(a, b) at the ranks of their row
-// nodes (pat.strip_rank, one uint16 per (incidence, local node)), and finally
-// copies the buffer out in 16-byte stores.  Every CSC entry receives its
-// contributions in incidence order, exactly as in k_hessian_reduce: the two
-// kernels give bitwise identical values.  Within an incidence the 9 n values are
-// spread over the lanes (distinct buffer entries, so no atomics); the staged
-// values and ranks of KB incidences are loaded before any of them is added, so
-// that their loads overlap.
-template <class EL, class T, int WARPS, int KB>
-__global__ void __launch_bounds__(WARPS * 32, 32 / WARPS)
-	k_hessian_columns(DevMesh m, DevPattern pat, const T *__restrict__ stage, int buf_doubles)
-{
-	constexpr int N = EL::N, TP = tri_pad(EL::N), NV = 9 * EL::N, R = (NV + 31) / 32;
-	extern __shared__ __align__(16) double colbuf[];
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int B = blockIdx.x * WARPS + warp;
-	if (B >= m.N) return;
-	double *buf = colbuf + (size_t)warp * buf_doubles;
-	const int o0 = __ldg(pat.outer + 3 * B);
-	const int stride = __ldg(pat.outer + 3 * B + 1) - o0; // 3 deg(B)
-	const int nval = 3 * stride;                          // 9 deg(B)
-	for (int i = lane; i < nval; i += 32) buf[i] = 0.0;
-	// this lane's values of an incidence: t = lane + 32 i -> local row node a, (r, c)
-	int la[R], lr[R], lc[R];
-#pragma unroll
-	for (int i = 0; i < R; ++i)
-	{
-		const int t = lane + 32 * i;
-		const int tt = t < NV ? t : 0;
-		la[i] = tt / 9;
-		lr[i] = (tt % 9) % 3;
-		lc[i] = (tt % 9) / 3;
-	}
-	__syncwarp();
-	const int s0 = __ldg(m.inc_off + B), s1 = __ldg(m.inc_off + B + 1);
-	for (int k0 = s0; k0 < s1; k0 += KB)
-	{
-		T v[KB][R];
-		int idx[KB][R];
-#pragma unroll
-		for (int j = 0; j < KB; ++j)
-		{
-			const int k = k0 + j;
-			const bool kin = k < s1;
-			const int eb = kin ? __ldg(m.inc_eb + k) : 0;
-			const int e = eb / N, b = eb - e * N;
-			const T *tri = stage + (size_t)e * TP;
-#pragma unroll
-			for (int i = 0; i < R; ++i)
-			{
-				const bool on = kin && (lane + 32 * i < NV);
-				const int a = la[i], r = lr[i], c = lc[i];
-				// H_e(3a+r, 3b+c): block (a, b) value [c][r] when a <= b, else block (b, a) value [r][c]
-				const int off = a <= b ? 9 * tri_index(N, a, b) + 3 * c + r : 9 * tri_index(N, b, a) + 3 * r + c;
-				const int rank = on ? (int)__ldg(pat.strip_rank + (size_t)k * N + a) : 0;
-				v[j][i] = on ? __ldg(tri + off) : T(0);
-				idx[j][i] = on ? c * stride + 3 * rank + r : -1;
-			}
-		}
-#pragma unroll
-		for (int j = 0; j < KB; ++j)
-		{
-#pragma unroll
-			for (int i = 0; i < R; ++i)
-				if (idx[j][i] >= 0) buf[idx[j][i]] += double(v[j][i]);
-			__syncwarp();
-		}
-	}
-	if (pat.red_col_start == nullptr)
-	{
-		// 9 deg doubles, contiguous in the CSC; o0 is a multiple of 9, so the start is
-		// 8-byte aligned only: peel to a 16-byte boundary, then double2 stores
-		double *dst = pat.values + o0;
-		const int head = (reinterpret_cast<uintptr_t>(dst) & 15) ? 1 : 0;
-		if (head && lane == 0) dst[0] = buf[0];
-		const int nv2 = (nval - head) / 2;
-		double2 *d2 = reinterpret_cast<double2 *>(dst + head);
-		for (int i = lane; i < nv2; i += 32) d2[i] = make_double2(buf[head + 2 * i], buf[head + 2 * i + 1]);
-		if (lane == 0 && head + 2 * nv2 < nval) dst[nval - 1] = buf[nval - 1];
-	}
-	else
-	{
-		for (int i = lane; i < nval; i += 32)
-		{
-			const int c = i / stride, rr = i - c * stride; // rr = 3 rank + r
-			const int cs = __ldg(pat.red_col_start + 3 * B + c);
-			if (cs < 0) continue;
-			const unsigned short ro = __ldg(pat.red_row_off + o0 / 3 + rr);
-			if (ro != 0xFFFF) pat.values[cs + ro] = buf[i];
-		}
-	}
-}
-
-// Pass 2 of every Hessian-pattern assembly: the column kernel when the largest
-// column block fits its per-warp shared buffer (9 max_deg doubles per warp),
-// else the plan-driven k_hessian_reduce.  Both give the same values bit for bit.
-#ifndef PFG_COLUMNS_WARPS
-#define PFG_COLUMNS_WARPS 8
-#endif
-#ifndef PFG_COLUMNS_KB
-#define PFG_COLUMNS_KB 4
-#endif
+// Pass 2 of every Hessian-pattern assembly.
 template <class EL, class T>
 static cudaError_t launch_reduce(const DevMesh &m, const DevPattern &p, const T *stage, cudaStream_t s)
 {
 	if (m.N <= 0) return cudaSuccess;
-	constexpr int W = PFG_COLUMNS_WARPS;
-	const int buf = ((9 * p.max_deg + 1) / 2) * 2; // doubles per warp, kept 16-byte aligned
-	const size_t smem = (size_t)W * buf * sizeof(double);
-	if (p.strip_rank && smem <= 96 * 1024)
-	{
-		auto kern = k_hessian_columns<EL, T, W, PFG_COLUMNS_KB>;
-		if (smem > 48 * 1024)
-		{
-			cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-			if (e != cudaSuccess) return e;
-		}
-		kern<<<(m.N + W - 1) / W, W * 32, smem, s>>>(m, p, stage, buf);
-		return cudaGetLastError();
-	}
 	constexpr int WARPS = 8;
 	k_hessian_reduce<EL, T, WARPS><<<(m.N + WARPS - 1) / WARPS, WARPS * 32, 0, s>>>(m, p, stage);
 	return cudaGetLastError();

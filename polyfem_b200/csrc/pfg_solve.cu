@@ -1,8 +1,9 @@
 // Linear solve on the device: conjugate gradient with the diagonal (Jacobi)
 // preconditioner on the context's assembled Hessian (full or Dirichlet-reduced
-// CSC), the hand-off NewtonMethod makes to its linear solver after every
-// assembly (polysolve's linear::Solver: analyze_pattern / factorize / solve, as
-// called from solver/NLProblem.cpp:261-262,419-420).
+// CSC), the hand-off the Newton step makes to its linear solver after every
+// assembly: the Hessian NLProblem::hessian returns (solver/NLProblem.cpp:615-621)
+// goes to polysolve's linear::Solver (analyze_pattern / factorize / solve),
+// called inside the Newton solver of polysolve@47dc48d (external).
 //
 // The iteration is Eigen's ConjugateGradient with DiagonalPreconditioner (Eigen
 // 3.4, the version the reference pins in cmake/recipes/eigen.cmake), restated:

@@ -71,6 +71,7 @@ struct TcCfg
 	static_assert(NPAD <= (int)TMEM_COLS, "accumulator must fit the TMEM allocation");
 	static_assert(KD <= KP && KP % 8 == 0, "K padding");
 	static_assert(NQ == 4 || NQ == 8, "K order groups the points of one (k, l) in 16-byte chunks");
+	static_assert(TE * TP <= 2 * KC * 128 * 4, "the block triangles must fit the A operand's bytes");
 };
 
 // Shared memory of one CTA.  A and B use the canonical K-major layout without
@@ -81,19 +82,29 @@ template <class EL>
 struct TcSmem
 {
 	using C = TcCfg<EL>;
-	alignas(1024) float Ah[C::KC][128][4];
-	alignas(1024) float Al[C::KC][128][4];
+	// A operand (hi, lo); once the tile's MMAs have completed the same bytes hold
+	// the tile's block triangles for the bulk store ([TE][TP] floats)
+	union
+	{
+		struct
+		{
+			alignas(1024) float Ah[C::KC][128][4];
+			alignas(1024) float Al[C::KC][128][4];
+		};
+		alignas(1024) float out[C::TE * C::TP];
+	};
 	alignas(1024) float Bh[C::KC][C::NPAD][4]; // Bh then Bl, contiguous: one bulk copy
 	float Bl[C::KC][C::NPAD][4];
-	alignas(16) float out[C::TE * C::TP];       // the tile's block triangles, copied out in one bulk store
 	alignas(16) float kin[2][C::TE][C::NQ][C::KIN];
-	double U[C::TE][C::N][3];
-	double X[C::TE][C::NG][3];
+	// gathered inputs, two tiles: the next tile's copies are in flight while this
+	// tile's kinematics run
+	double U[2][C::TE][C::N][3];
+	double X[2][C::TE][C::NG][3];
+	double2 lame[2][C::TE];
+	int nodes[2][C::TE][C::N + C::NG];
 	double gtab[C::NQ][C::N][3];
 	double ggtab[EL::AFFINE ? 1 : C::NQ][C::NG][3];
 	double wq[C::NQ];
-	double2 lame[C::TE];
-	int nodes[C::TE][C::N + C::NG];
 	alignas(8) unsigned long long bar_b;   // Phi bulk copy
 	unsigned long long bar_mma;            // MMA completion (tcgen05.commit)
 	uint32_t tmem_base;
@@ -195,6 +206,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 #pragma unroll
 	for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+
+__device__ __forceinline__ void cp_async8(void *dst_smem, const void *src)
+{
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst_smem)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src)
+{
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst_smem)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void named_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 __device__ __forceinline__ void named_arrive(int id, int n) { asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory"); }
@@ -331,33 +353,81 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 	if (warp >= 4)
 	{
 		// ================= load group: nodes, gathers, kinematics =================
+		// Pipeline per tile t (buffers by tile parity): the node ids of the tile after
+		// next are loaded into registers and the next tile's u / X / Lame gathers are
+		// in flight (cp.async) while this tile's kinematics run.
 		const int lt = tid - 128;
-		int it = 0;
-		for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it)
-		{
-			const int buf = it & 1;
-			if (it >= 2) named_sync(BAR_EMPTY0 + buf, TC_THREADS);
-			const int e0 = t * TE, ne = min(TE, m.E - e0);
-			for (int i = lt; i < TE * (N + NG); i += 128)
+		constexpr int NJ = N + NG, NR = (TE * NJ + 127) / 128;
+		int nr[NR];
+		auto load_nodes = [&](int tt) {
+			const int e0 = tt * TE, ne = min(TE, m.E - e0);
+#pragma unroll
+			for (int k = 0; k < NR; ++k)
 			{
-				const int j = i / TE, el = i % TE, e = e0 + el;
+				const int i = lt + 128 * k, j = i / TE, el = i % TE, e = e0 + el;
 				int v = 0;
-				if (el < ne) v = (j < N) ? __ldg(m.conn + (size_t)j * m.E + e) : __ldg(m.gconn + (size_t)(j - N) * m.E + e);
-				S.nodes[el][j] = v;
+				if (i < TE * NJ && el < ne)
+					v = (j < N) ? __ldg(m.conn + (size_t)j * m.E + e) : __ldg(m.gconn + (size_t)(j - N) * m.E + e);
+				nr[k] = v;
 			}
-			if (lt < TE) S.lame[lt] = lt < ne ? __ldg(m.lame + e0 + lt) : make_double2(0.0, 0.0);
-			named_sync(BAR_LOAD, 128);
+		};
+		auto store_nodes = [&](int g) {
+#pragma unroll
+			for (int k = 0; k < NR; ++k)
+			{
+				const int i = lt + 128 * k;
+				if (i < TE * NJ) S.nodes[g][i % TE][i / TE] = nr[k];
+			}
+		};
+		auto issue_gathers = [&](int g, int tt) {
+			const int e0 = tt * TE, ne = min(TE, m.E - e0);
 			for (int i = lt; i < TE * N * 3; i += 128)
 			{
 				const int el = i / (N * 3), a = (i / 3) % N, d = i % 3;
-				S.U[el][a][d] = el < ne ? __ldg(u + (size_t)S.nodes[el][a] * 3 + d) : 0.0;
+				if (el < ne)
+					cp_async8(&S.U[g][el][a][d], u + (size_t)S.nodes[g][el][a] * 3 + d);
+				else
+					S.U[g][el][a][d] = 0.0;
 			}
 			for (int i = lt; i < TE * NG * 3; i += 128)
 			{
 				const int el = i / (NG * 3), j = (i / 3) % NG, d = i % 3;
-				S.X[el][j][d] = el < ne ? __ldg(m.X + (size_t)S.nodes[el][N + j] * 3 + d) : 0.0;
+				if (el < ne)
+					cp_async8(&S.X[g][el][j][d], m.X + (size_t)S.nodes[g][el][N + j] * 3 + d);
+				else
+					S.X[g][el][j][d] = 0.0;
 			}
+			if (lt < TE)
+			{
+				if (lt < ne)
+					cp_async16(&S.lame[g][lt], m.lame + e0 + lt);
+				else
+					S.lame[g][lt] = make_double2(0.0, 0.0);
+			}
+			cp_async_commit();
+		};
+		int t = blockIdx.x;
+		if (t < ntiles)
+		{
+			load_nodes(t);
+			store_nodes(0);
+		}
+		named_sync(BAR_LOAD, 128);
+		if (t < ntiles) issue_gathers(0, t);
+		if (t + (int)gridDim.x < ntiles) load_nodes(t + gridDim.x);
+		int it = 0;
+		for (; t < ntiles; t += gridDim.x, ++it)
+		{
+			const int buf = it & 1, g = it & 1;
+			const int tn = t + gridDim.x, tnn = tn + gridDim.x;
+			cp_async_wait_all();
+			named_sync(BAR_LOAD, 128); // this tile's gathers have landed; the other buffers are free
+			if (tn < ntiles) store_nodes(g ^ 1);
 			named_sync(BAR_LOAD, 128);
+			if (tn < ntiles) issue_gathers(g ^ 1, tn);
+			if (tnn < ntiles) load_nodes(tnn);
+			if (it >= 2) named_sync(BAR_EMPTY0 + buf, TC_THREADS);
+			const int e0 = t * TE, ne = min(TE, m.E - e0);
 			for (int i = lt; i < TE * NQ; i += 128)
 			{
 				const int el = i / NQ, q = i % NQ;
@@ -378,7 +448,7 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 					{
 						double s = 0.0;
 #pragma unroll
-						for (int j = 0; j < NG; ++j) s += gg[j][r] * S.X[el][j][c];
+						for (int j = 0; j < NG; ++j) s += gg[j][r] * S.X[g][el][j][c];
 						Jac[r][c] = s;
 					}
 				const double detJ = det3(Jac);
@@ -392,7 +462,7 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 					{
 						double s = 0.0;
 #pragma unroll
-						for (int a = 0; a < N; ++a) s += S.U[el][a][r] * gq[a][c];
+						for (int a = 0; a < N; ++a) s += S.U[g][el][a][r] * gq[a][c];
 						Ar[r][c] = s;
 					}
 				double F[3][3];
@@ -406,7 +476,7 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 				double FmT[3][3];
 				inv_transpose3(F, J, FmT);
 				const double da = detJ * S.wq[q];
-				const double2 lm = S.lame[el]; // (lambda, mu)
+				const double2 lm = S.lame[g][el]; // (lambda, mu)
 #pragma unroll
 				for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -447,6 +517,8 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 			const int buf = it & 1;
 			const int e0 = t * TE, ne = min(TE, m.E - e0);
 			named_sync(BAR_FULL0 + buf, TC_THREADS);
+			if (tid == 0) bulk_wait_read_all(); // the previous tile's store has left the A bytes
+			named_sync(BAR_MATH, 128);
 			bool bad = false; // the row's element has a point with J <= 0
 			if (row < C::ROWS)
 			{
@@ -494,7 +566,6 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 			}
 			named_arrive(BAR_EMPTY0 + buf, TC_THREADS); // kin[buf] consumed
 			fence_proxy_async_smem();
-			if (tid == 0) bulk_wait_read_all(); // the previous tile's store has left `out`
 			named_sync(BAR_MATH, 128);
 			if (tid == 0 && !S.abort)
 			{
@@ -580,10 +651,17 @@ struct TcLaunch
 		if (device < 0 || device >= 64) return 148;
 		if (!cached[device])
 		{
-			int sms = 0, per_sm = 0;
+			// CTAs per SM from the kernel's own footprint: shared memory (plus the 1 KB
+			// the runtime reserves per CTA) and registers
+			int sms = 0, smem_sm = 0, regs_sm = 0;
 			cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-			cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hessian_blocks_tc<EL>, TC_THREADS, sizeof(TcSmem<EL>));
-			cached[device] = std::max(1, sms * std::max(1, per_sm));
+			cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+			cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device);
+			cudaFuncAttributes fa{};
+			cudaFuncGetAttributes(&fa, k_hessian_blocks_tc<EL>);
+			const int by_smem = smem_sm / (int)(sizeof(TcSmem<EL>) + 1024);
+			const int by_regs = fa.numRegs > 0 ? regs_sm / (fa.numRegs * TC_THREADS) : 1;
+			cached[device] = std::max(1, sms) * std::max(1, std::min(std::min(by_smem, by_regs), 4));
 		}
 		return cached[device];
 	}

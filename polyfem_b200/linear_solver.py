@@ -2,8 +2,10 @@
 
 PolyFEM's Newton solver hands every assembled Hessian to a polysolve
 linear::Solver -- ``analyze_pattern(A, precond_num)``, ``factorize(A)``,
-``solve(b, x)``, ``get_info(info)`` (the call sequence of
-solver/NLProblem.cpp:261-262,419-420).  ``ConjugateGradient`` mirrors that
+``solve(b, x)``, ``get_info(info)``: the Hessian NLProblem::hessian returns
+(solver/NLProblem.cpp:615-621) is solved inside the Newton step of polysolve@47dc48d
+(cmake/recipes/polysolve.cmake:11; external, not in the reference tree), which owns
+that call sequence.  ``ConjugateGradient`` mirrors that
 interface for the solver polysolve names "Eigen::ConjugateGradient" (Eigen's
 conjugate gradient with the diagonal preconditioner), run by libpfgpu on the
 matrix the assembler left on the device, so the Hessian never leaves the GPU.
