@@ -779,35 +779,41 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 	}
 }
 
-// One warp per column node B; the warp's 3*deg(B) work items are the (row rank,
-// column c) pairs of B's column block.  Each item sums, in FP64 and in incidence
-// order, the three values (rows 3*rank .. 3*rank+2 of column 3B+c) of every
-// staged block that lands on its rank, read through the reduction plan
-// (consecutive values of block (a, b); for a flagged transposed block (b, a), the
-// values c, c+3, c+6), and writes them once.  No atomics: the sum order of every
-// entry is fixed.
+// One warp per column node B; the warp's work items are the row ranks of B's
+// column block, one lane per rank (the node block (A, B) of every neighbour A).
+// An item sums, in FP64 and in incidence order, the whole 3x3 staged blocks that
+// land on its rank, read through the reduction plan: block (a, b) gives
+// H(3a+r, 3b+c) at value 3c + r; a flagged block (b, a) is read transposed, value
+// 3r + c.  The nine sums go to rows 3 rank .. 3 rank + 2 of B's three columns,
+// written once.  No atomics: the sum order of every entry is fixed.
 //
 // The warp first copies B's plan (its n * #incidences entries) and group starts
 // into shared memory with coalesced loads, so that an item reads its
-// contributions' offsets without a global round trip and issues the block-value
-// loads of RED_UNROLL contributions back to back.  Nodes whose plan exceeds the
+// contributions' offsets without a global round trip; the nine values of two
+// contributions are loaded before either is added.  Nodes whose plan exceeds the
 // shared copy (more than RED_PLAN entries or RED_DEG neighbours) read it from
-// global memory, two entries ahead.
-constexpr int RED_PLAN = 256, RED_DEG = 128, RED_UNROLL = 4;
+// global memory.
+constexpr int RED_PLAN = 256, RED_DEG = 128;
 
 template <class T>
-__device__ __forceinline__ void red_load3(const T *__restrict__ stage, unsigned q, int c, T (&x)[3])
+__device__ __forceinline__ void red_block(const T *__restrict__ stage, unsigned q, T (&v)[9])
 {
-	const bool tr = q & TRI_TRANSPOSED;
-	const T *p = stage + (q & ~TRI_TRANSPOSED) + (tr ? c : 3 * c);
-	const int st = tr ? 3 : 1;
-	x[0] = __ldg(p);
-	x[1] = __ldg(p + st);
-	x[2] = __ldg(p + 2 * st);
+	const T *p = stage + (q & ~TRI_TRANSPOSED);
+#pragma unroll
+	for (int i = 0; i < 9; ++i) v[i] = __ldg(p + i);
+}
+template <class T>
+__device__ __forceinline__ void red_add(double (&acc)[9], const T (&v)[9], bool tr)
+{
+	// acc[3c + r] accumulates H(3A+r, 3B+c)
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) acc[3 * c + r] += double(tr ? v[3 * r + c] : v[3 * c + r]);
 }
 
 template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, sizeof(T) == 8 ? 4 : 6)
+__global__ void __launch_bounds__(WARPS * 32, 4)
 	k_hessian_reduce(DevMesh m, DevPattern pat, const T *__restrict__ stage)
 {
 	constexpr int N = EL::N;
@@ -832,77 +838,55 @@ __global__ void __launch_bounds__(WARPS * 32, sizeof(T) == 8 ? 4 : 6)
 		if (lane == 0) s_rel[warp][deg] = (unsigned short)tot;
 		__syncwarp();
 	}
-	for (int it = lane; it < stride; it += 32)
+	for (int r = lane; r < deg; r += 32)
 	{
-		// (rank, column) items rank-major: the three items of the diagonal block,
-		// which has the longest contribution list, share one pass of the warp
-		const int r = it / 3, c = it - 3 * r;
-		double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-		if (local)
+		const int k0 = local ? (int)s_rel[warp][r] : (int)__ldg(br + r);
+		const int k1 = local ? (int)s_rel[warp][r + 1] : (r + 1 < deg ? (int)__ldg(br + r + 1) : tot);
+		double acc[9];
+#pragma unroll
+		for (int i = 0; i < 9; ++i) acc[i] = 0.0;
+		int k = k0;
+		for (; k + 1 < k1; k += 2)
 		{
-			const int k0 = s_rel[warp][r], k1 = s_rel[warp][r + 1];
-			for (int k = k0; k < k1; k += RED_UNROLL)
-			{
-				T x[RED_UNROLL][3];
-#pragma unroll
-				for (int j = 0; j < RED_UNROLL; ++j)
-					if (k + j < k1) red_load3(stage, s_plan[warp][k + j], c, x[j]);
-#pragma unroll
-				for (int j = 0; j < RED_UNROLL; ++j)
-					if (k + j < k1)
-					{
-						a0 += double(x[j][0]);
-						a1 += double(x[j][1]);
-						a2 += double(x[j][2]);
-					}
-			}
+			const unsigned q0 = local ? s_plan[warp][k] : __ldg(cl + k);
+			const unsigned q1 = local ? s_plan[warp][k + 1] : __ldg(cl + k + 1);
+			T v0[9], v1[9];
+			red_block(stage, q0, v0);
+			red_block(stage, q1, v1);
+			red_add(acc, v0, q0 & TRI_TRANSPOSED);
+			red_add(acc, v1, q1 & TRI_TRANSPOSED);
 		}
-		else
+		if (k < k1)
 		{
-			const int k0 = __ldg(br + r);
-			const int k1 = (r + 1 < deg) ? (int)__ldg(br + r + 1) : tot;
-			// two contributions per step, the next step's plan entries loaded ahead;
-			// the sum order stays k ascending
-			unsigned qa = k0 < k1 ? __ldg(cl + k0) : 0u;
-			unsigned qb = k0 + 1 < k1 ? __ldg(cl + k0 + 1) : 0u;
-			for (int k = k0; k < k1; k += 2)
-			{
-				const unsigned q0 = qa, q1 = qb;
-				const bool two = k + 1 < k1;
-				qa = k + 2 < k1 ? __ldg(cl + k + 2) : 0u;
-				qb = k + 3 < k1 ? __ldg(cl + k + 3) : 0u;
-				T x[3], y[3] = {T(0), T(0), T(0)};
-				red_load3(stage, q0, c, x);
-				if (two) red_load3(stage, q1, c, y);
-				a0 += double(x[0]);
-				a1 += double(x[1]);
-				a2 += double(x[2]);
-				if (two)
-				{
-					a0 += double(y[0]);
-					a1 += double(y[1]);
-					a2 += double(y[2]);
-				}
-			}
+			const unsigned q0 = local ? s_plan[warp][k] : __ldg(cl + k);
+			T v0[9];
+			red_block(stage, q0, v0);
+			red_add(acc, v0, q0 & TRI_TRANSPOSED);
 		}
 		if (pat.red_col_start == nullptr)
 		{
-			double *d = dst + c * stride + 3 * r;
-			d[0] = a0;
-			d[1] = a1;
-			d[2] = a2;
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+			{
+				double *d = dst + c * stride + 3 * r;
+				d[0] = acc[3 * c];
+				d[1] = acc[3 * c + 1];
+				d[2] = acc[3 * c + 2];
+			}
 		}
 		else
 		{
 			// Dirichlet-reduced output: free rows of free columns only
-			const int cs = __ldg(pat.red_col_start + 3 * B + c);
-			if (cs >= 0)
+			const unsigned short *ro = pat.red_row_off + o0 / 3 + 3 * r;
+			const unsigned short r0 = __ldg(ro), r1 = __ldg(ro + 1), r2 = __ldg(ro + 2);
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
 			{
-				const unsigned short *ro = pat.red_row_off + o0 / 3 + 3 * r;
-				const unsigned short r0 = __ldg(ro), r1 = __ldg(ro + 1), r2 = __ldg(ro + 2);
-				if (r0 != 0xFFFF) pat.values[cs + r0] = a0;
-				if (r1 != 0xFFFF) pat.values[cs + r1] = a1;
-				if (r2 != 0xFFFF) pat.values[cs + r2] = a2;
+				const int cs = __ldg(pat.red_col_start + 3 * B + c);
+				if (cs < 0) continue;
+				if (r0 != 0xFFFF) pat.values[cs + r0] = acc[3 * c];
+				if (r1 != 0xFFFF) pat.values[cs + r1] = acc[3 * c + 1];
+				if (r2 != 0xFFFF) pat.values[cs + r2] = acc[3 * c + 2];
 			}
 		}
 	}

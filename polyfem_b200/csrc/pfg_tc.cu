@@ -102,6 +102,7 @@ struct TcSmem
 	double X[2][C::TE][C::NG][3];
 	double2 lame[2][C::TE];
 	int nodes[2][C::TE][C::N + C::NG];
+	double geo[C::TE][20]; // affine elements: J (9), G = J^-T J^-1 (9), det J
 	double gtab[C::NQ][C::N][3];
 	double ggtab[EL::AFFINE ? 1 : C::NQ][C::NG][3];
 	double wq[C::NQ];
@@ -191,8 +192,24 @@ __device__ __forceinline__ void mma_commit(unsigned long long *bar)
 				 : "memory");
 }
 
-// 16 consecutive accumulator columns of the warp's 32 lanes, waited on in the
-// same statement so that no use of the registers can be scheduled before the wait
+// 32 (or 16) consecutive accumulator columns of the warp's 32 lanes, waited on in
+// the same statement so that no use of the registers can be scheduled before the wait
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
+{
+	uint32_t r[32];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+				 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+				 "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
+				 "tcgen05.wait::ld.sync.aligned;"
+				 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+				   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+				   "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+				   "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+				 : "r"(taddr)
+				 : "memory");
+#pragma unroll
+	for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 {
 	uint32_t r[16];
@@ -426,8 +443,40 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 			named_sync(BAR_LOAD, 128);
 			if (tn < ntiles) issue_gathers(g ^ 1, tn);
 			if (tnn < ntiles) load_nodes(tnn);
-			if (it >= 2) named_sync(BAR_EMPTY0 + buf, TC_THREADS);
 			const int e0 = t * TE, ne = min(TE, m.E - e0);
+			if constexpr (EL::AFFINE)
+			{
+				// the geometric map is affine: J, det J and G = J^-T J^-1 once per element
+				if (lt < TE)
+				{
+					double *geo = S.geo[lt];
+					double Jac[3][3];
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+#pragma unroll
+						for (int c = 0; c < 3; ++c)
+						{
+							double s_ = 0.0;
+#pragma unroll
+							for (int j = 0; j < NG; ++j) s_ += S.ggtab[0][j][r] * S.X[g][lt][j][c];
+							Jac[r][c] = s_;
+						}
+					const double detJ = det3(Jac);
+					double Jit[3][3];
+					inv_transpose3(Jac, detJ, Jit);
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+#pragma unroll
+						for (int c = 0; c < 3; ++c)
+						{
+							geo[3 * r + c] = Jac[r][c];
+							geo[9 + 3 * r + c] = Jit[r][0] * Jit[c][0] + Jit[r][1] * Jit[c][1] + Jit[r][2] * Jit[c][2];
+						}
+					geo[18] = detJ;
+				}
+				named_sync(BAR_LOAD, 128);
+			}
+			if (it >= 2) named_sync(BAR_EMPTY0 + buf, TC_THREADS);
 			for (int i = lt; i < TE * NQ; i += 128)
 			{
 				const int el = i / NQ, q = i % NQ;
@@ -438,43 +487,61 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 					for (int k = 0; k < C::KIN; ++k) rec[k] = 0.f;
 					continue;
 				}
+				// With M = J^T + sum_a u_a (x) grad_ref(phi_a) (the deformed map's gradient,
+				// rows spatial, columns reference): F = M J^-T, so det F = det M / det J and
+				// Kt = F^-T J^-1 = M^-T; and G = J^-T J^-1 depends on the geometry only.
 				const double(*gq)[3] = S.gtab[q];
-				const double(*gg)[3] = S.ggtab[EL::AFFINE ? 0 : q];
-				double Jac[3][3];
+				double Jac[3][3], G[3][3], detJ;
+				if constexpr (EL::AFFINE)
+				{
+					const double *geo = S.geo[el];
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+#pragma unroll
+						for (int c = 0; c < 3; ++c)
+						{
+							Jac[r][c] = geo[3 * r + c];
+							G[r][c] = geo[9 + 3 * r + c];
+						}
+					detJ = geo[18];
+				}
+				else
+				{
+					const double(*gg)[3] = S.ggtab[q];
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+#pragma unroll
+						for (int c = 0; c < 3; ++c)
+						{
+							double s_ = 0.0;
+#pragma unroll
+							for (int j = 0; j < NG; ++j) s_ += gg[j][r] * S.X[g][el][j][c];
+							Jac[r][c] = s_;
+						}
+					detJ = det3(Jac);
+					double Jit[3][3];
+					inv_transpose3(Jac, detJ, Jit);
+#pragma unroll
+					for (int r = 0; r < 3; ++r)
+#pragma unroll
+						for (int c = 0; c < 3; ++c) G[r][c] = Jit[r][0] * Jit[c][0] + Jit[r][1] * Jit[c][1] + Jit[r][2] * Jit[c][2];
+				}
+				double M[3][3];
 #pragma unroll
 				for (int r = 0; r < 3; ++r)
 #pragma unroll
 					for (int c = 0; c < 3; ++c)
 					{
-						double s = 0.0;
+						double s_ = Jac[c][r];
 #pragma unroll
-						for (int j = 0; j < NG; ++j) s += gg[j][r] * S.X[g][el][j][c];
-						Jac[r][c] = s;
+						for (int a = 0; a < N; ++a) s_ += S.U[g][el][a][r] * gq[a][c];
+						M[r][c] = s_;
 					}
-				const double detJ = det3(Jac);
-				double Jit[3][3];
-				inv_transpose3(Jac, detJ, Jit);
-				double Ar[3][3];
-#pragma unroll
-				for (int r = 0; r < 3; ++r)
-#pragma unroll
-					for (int c = 0; c < 3; ++c)
-					{
-						double s = 0.0;
-#pragma unroll
-						for (int a = 0; a < N; ++a) s += S.U[g][el][a][r] * gq[a][c];
-						Ar[r][c] = s;
-					}
-				double F[3][3];
-#pragma unroll
-				for (int r = 0; r < 3; ++r)
-#pragma unroll
-					for (int c = 0; c < 3; ++c)
-						F[r][c] = Ar[r][0] * Jit[0][c] + Ar[r][1] * Jit[1][c] + Ar[r][2] * Jit[2][c] + (r == c ? 1.0 : 0.0);
-				const double J = det3(F);
+				const double detM = det3(M);
+				const double J = detM / detJ;
 				const double lj = log(J);
-				double FmT[3][3];
-				inv_transpose3(F, J, FmT);
+				double Kt[3][3];
+				inv_transpose3(M, detM, Kt);
 				const double da = detJ * S.wq[q];
 				const double2 lm = S.lame[g][el]; // (lambda, mu)
 #pragma unroll
@@ -482,8 +549,8 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 #pragma unroll
 					for (int k = 0; k < 3; ++k)
 					{
-						rec[3 * r + k] = (float)(FmT[r][0] * Jit[k][0] + FmT[r][1] * Jit[k][1] + FmT[r][2] * Jit[k][2]);
-						rec[9 + 3 * r + k] = (float)(Jit[r][0] * Jit[k][0] + Jit[r][1] * Jit[k][1] + Jit[r][2] * Jit[k][2]);
+						rec[3 * r + k] = (float)Kt[r][k];
+						rec[9 + 3 * r + k] = (float)G[r][k];
 					}
 				rec[18] = (float)(lm.y * da);
 				rec[19] = (float)(lm.x * da);
@@ -598,12 +665,22 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 			if (got)
 			{
 #pragma unroll
-				for (int c0 = 0; c0 < C::NPAD; c0 += 16)
+				for (int c0 = 0; c0 < C::NPAD; c0 += 32)
 				{
-					float x[16];
-					tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, x);
+					if (c0 + 32 <= C::NPAD)
+					{
+						float x[32];
+						tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + c0, x);
 #pragma unroll
-					for (int i = 0; i < 16; ++i) v[c0 + i] = x[i];
+						for (int i = 0; i < 32; ++i) v[c0 + i] = x[i];
+					}
+					else
+					{
+						float x[16];
+						tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, x);
+#pragma unroll
+						for (int i = 0; i < 16; ++i) v[c0 + i] = x[i];
+					}
 				}
 			}
 			else
