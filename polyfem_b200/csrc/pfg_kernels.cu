@@ -779,46 +779,18 @@ __global__ void __launch_bounds__(128, blocks_min_ctas<EL, K, T>())
 	}
 }
 
-// One warp per column node B; the warp's work items are the row ranks of B's
-// column block, one lane per rank (the node block (A, B) of every neighbour A).
-// An item sums, in FP64 and in incidence order, the whole 3x3 staged blocks that
-// land on its rank, read through the reduction plan: block (a, b) gives
-// H(3a+r, 3b+c) at value 3c + r; a flagged block (b, a) is read transposed, value
-// 3r + c.  The nine sums go to rows 3 rank .. 3 rank + 2 of B's three columns,
-// written once.  No atomics: the sum order of every entry is fixed.
-//
-// The warp first copies B's plan (its n * #incidences entries) and group starts
-// into shared memory with coalesced loads, so that an item reads its
-// contributions' offsets without a global round trip; the nine values of two
-// contributions are loaded before either is added.  Nodes whose plan exceeds the
-// shared copy (more than RED_PLAN entries or RED_DEG neighbours) read it from
-// global memory.
-constexpr int RED_PLAN = 256, RED_DEG = 128;
-
-template <class T>
-__device__ __forceinline__ void red_block(const T *__restrict__ stage, unsigned q, T (&v)[9])
-{
-	const T *p = stage + (q & ~TRI_TRANSPOSED);
-#pragma unroll
-	for (int i = 0; i < 9; ++i) v[i] = __ldg(p + i);
-}
-template <class T>
-__device__ __forceinline__ void red_add(double (&acc)[9], const T (&v)[9], bool tr)
-{
-	// acc[3c + r] accumulates H(3A+r, 3B+c)
-#pragma unroll
-	for (int c = 0; c < 3; ++c)
-#pragma unroll
-		for (int r = 0; r < 3; ++r) acc[3 * c + r] += double(tr ? v[3 * r + c] : v[3 * c + r]);
-}
-
+// One warp per column node B; the warp's 3*deg(B) work items are the (row rank,
+// column c) pairs of B's column block.  Each item sums, in FP64 and in incidence
+// order, the three values (rows 3*rank .. 3*rank+2 of column 3B+c) of every
+// staged block that lands on its rank, read through the reduction plan
+// (consecutive values of block (a, b); for a flagged transposed block (b, a), the
+// values c, c+3, c+6), and writes them once.  No shared memory, no atomics: the
+// sum order of every entry is fixed.
 template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 4)
+__global__ void __launch_bounds__(WARPS * 32, 8)
 	k_hessian_reduce(DevMesh m, DevPattern pat, const T *__restrict__ stage)
 {
 	constexpr int N = EL::N;
-	__shared__ unsigned s_plan[WARPS][RED_PLAN];
-	__shared__ unsigned short s_rel[WARPS][RED_DEG + 1];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int B = blockIdx.x * WARPS + warp;
 	if (B >= m.N) return;
@@ -830,63 +802,65 @@ __global__ void __launch_bounds__(WARPS * 32, 4)
 	const unsigned *cl = pat.contrib + (size_t)s0 * N;
 	const unsigned short *br = pat.blk_rel + o0 / 9;
 	double *dst = pat.values + o0;
-	const bool local = tot <= RED_PLAN && deg <= RED_DEG;
-	if (local)
+	for (int it = lane; it < stride; it += 32)
 	{
-		for (int i = lane; i < tot; i += 32) s_plan[warp][i] = __ldg(cl + i);
-		for (int i = lane; i < deg; i += 32) s_rel[warp][i] = __ldg(br + i);
-		if (lane == 0) s_rel[warp][deg] = (unsigned short)tot;
-		__syncwarp();
-	}
-	for (int r = lane; r < deg; r += 32)
-	{
-		const int k0 = local ? (int)s_rel[warp][r] : (int)__ldg(br + r);
-		const int k1 = local ? (int)s_rel[warp][r + 1] : (r + 1 < deg ? (int)__ldg(br + r + 1) : tot);
-		double acc[9];
-#pragma unroll
-		for (int i = 0; i < 9; ++i) acc[i] = 0.0;
-		int k = k0;
-		for (; k + 1 < k1; k += 2)
+		// (rank, column) items rank-major: the three items of the diagonal block,
+		// which has the longest contribution list, share one pass of the warp
+		const int r = it / 3, c = it - 3 * r;
+		const int k0 = __ldg(br + r);
+		const int k1 = (r + 1 < deg) ? (int)__ldg(br + r + 1) : tot;
+		double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+		// two contributions per step, the next step's plan entries loaded ahead;
+		// the sum order stays k ascending
+		unsigned qa = k0 < k1 ? __ldg(cl + k0) : 0u;
+		unsigned qb = k0 + 1 < k1 ? __ldg(cl + k0 + 1) : 0u;
+		for (int k = k0; k < k1; k += 2)
 		{
-			const unsigned q0 = local ? s_plan[warp][k] : __ldg(cl + k);
-			const unsigned q1 = local ? s_plan[warp][k + 1] : __ldg(cl + k + 1);
-			T v0[9], v1[9];
-			red_block(stage, q0, v0);
-			red_block(stage, q1, v1);
-			red_add(acc, v0, q0 & TRI_TRANSPOSED);
-			red_add(acc, v1, q1 & TRI_TRANSPOSED);
-		}
-		if (k < k1)
-		{
-			const unsigned q0 = local ? s_plan[warp][k] : __ldg(cl + k);
-			T v0[9];
-			red_block(stage, q0, v0);
-			red_add(acc, v0, q0 & TRI_TRANSPOSED);
+			const unsigned q0 = qa, q1 = qb;
+			const bool two = k + 1 < k1;
+			qa = k + 2 < k1 ? __ldg(cl + k + 2) : 0u;
+			qb = k + 3 < k1 ? __ldg(cl + k + 3) : 0u;
+			// (a, b): values 3c, 3c+1, 3c+2 of the block; transposed (b, a): c, c+3, c+6
+			const bool t0 = q0 & TRI_TRANSPOSED, t1 = q1 & TRI_TRANSPOSED;
+			const T *p0 = stage + (q0 & ~TRI_TRANSPOSED) + (t0 ? c : 3 * c);
+			const T *p1 = stage + (q1 & ~TRI_TRANSPOSED) + (t1 ? c : 3 * c);
+			const int s0_ = t0 ? 3 : 1, s1_ = t1 ? 3 : 1;
+			const T x0 = __ldg(p0), x1 = __ldg(p0 + s0_), x2 = __ldg(p0 + 2 * s0_);
+			T y0 = T(0), y1 = T(0), y2 = T(0);
+			if (two)
+			{
+				y0 = __ldg(p1);
+				y1 = __ldg(p1 + s1_);
+				y2 = __ldg(p1 + 2 * s1_);
+			}
+			a0 += double(x0);
+			a1 += double(x1);
+			a2 += double(x2);
+			if (two)
+			{
+				a0 += double(y0);
+				a1 += double(y1);
+				a2 += double(y2);
+			}
 		}
 		if (pat.red_col_start == nullptr)
 		{
-#pragma unroll
-			for (int c = 0; c < 3; ++c)
-			{
-				double *d = dst + c * stride + 3 * r;
-				d[0] = acc[3 * c];
-				d[1] = acc[3 * c + 1];
-				d[2] = acc[3 * c + 2];
-			}
+			double *d = dst + c * stride + 3 * r;
+			d[0] = a0;
+			d[1] = a1;
+			d[2] = a2;
 		}
 		else
 		{
 			// Dirichlet-reduced output: free rows of free columns only
-			const unsigned short *ro = pat.red_row_off + o0 / 3 + 3 * r;
-			const unsigned short r0 = __ldg(ro), r1 = __ldg(ro + 1), r2 = __ldg(ro + 2);
-#pragma unroll
-			for (int c = 0; c < 3; ++c)
+			const int cs = __ldg(pat.red_col_start + 3 * B + c);
+			if (cs >= 0)
 			{
-				const int cs = __ldg(pat.red_col_start + 3 * B + c);
-				if (cs < 0) continue;
-				if (r0 != 0xFFFF) pat.values[cs + r0] = acc[3 * c];
-				if (r1 != 0xFFFF) pat.values[cs + r1] = acc[3 * c + 1];
-				if (r2 != 0xFFFF) pat.values[cs + r2] = acc[3 * c + 2];
+				const unsigned short *ro = pat.red_row_off + o0 / 3 + 3 * r;
+				const unsigned short r0 = __ldg(ro), r1 = __ldg(ro + 1), r2 = __ldg(ro + 2);
+				if (r0 != 0xFFFF) pat.values[cs + r0] = a0;
+				if (r1 != 0xFFFF) pat.values[cs + r1] = a1;
+				if (r2 != 0xFFFF) pat.values[cs + r2] = a2;
 			}
 		}
 	}

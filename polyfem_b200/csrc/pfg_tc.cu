@@ -102,7 +102,7 @@ struct TcSmem
 	double X[2][C::TE][C::NG][3];
 	double2 lame[2][C::TE];
 	int nodes[2][C::TE][C::N + C::NG];
-	double geo[C::TE][20]; // affine elements: J (9), G = J^-T J^-1 (9), det J
+	double geo[2][C::TE][20]; // affine elements: J (9), G = J^-T J^-1 (9), det J
 	double gtab[C::NQ][C::N][3];
 	double ggtab[EL::AFFINE ? 1 : C::NQ][C::NG][3];
 	double wq[C::NQ];
@@ -223,17 +223,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 #pragma unroll
 	for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
-
-__device__ __forceinline__ void cp_async8(void *dst_smem, const void *src)
-{
-	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst_smem)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src)
-{
-	asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst_smem)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void named_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 __device__ __forceinline__ void named_arrive(int id, int n) { asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory"); }
@@ -370,12 +359,18 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 	if (warp >= 4)
 	{
 		// ================= load group: nodes, gathers, kinematics =================
-		// Pipeline per tile t (buffers by tile parity): the node ids of the tile after
-		// next are loaded into registers and the next tile's u / X / Lame gathers are
-		// in flight (cp.async) while this tile's kinematics run.
+		// Pipeline over this CTA's tiles (buffers by tile parity, loads in flight in
+		// registers): while tile t's kinematics run, the u / X / Lame values of the next
+		// tile and the node ids of the tile after it are in flight, and (affine
+		// elements) the otherwise idle warps compute the next tile's geometry.
 		const int lt = tid - 128;
 		constexpr int NJ = N + NG, NR = (TE * NJ + 127) / 128;
+		constexpr int NU = TE * N * 3, NX = TE * NG * 3, NV = (NU + NX + 127) / 128;
+		constexpr int GEO0 = ((TE * NQ + 31) / 32) * 32; // first thread of the geometry group
+		static_assert(!EL::AFFINE || GEO0 + TE <= 128, "the geometry group needs idle producer threads");
 		int nr[NR];
+		double gv[NV];
+		double2 glm = make_double2(0.0, 0.0);
 		auto load_nodes = [&](int tt) {
 			const int e0 = tt * TE, ne = min(TE, m.E - e0);
 #pragma unroll
@@ -388,40 +383,87 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 				nr[k] = v;
 			}
 		};
-		auto store_nodes = [&](int g) {
+		auto store_nodes = [&](int b) {
 #pragma unroll
 			for (int k = 0; k < NR; ++k)
 			{
 				const int i = lt + 128 * k;
-				if (i < TE * NJ) S.nodes[g][i % TE][i / TE] = nr[k];
+				if (i < TE * NJ) S.nodes[b][i % TE][i / TE] = nr[k];
 			}
 		};
-		auto issue_gathers = [&](int g, int tt) {
+		auto load_values = [&](int b, int tt) { // node ids of tile tt in nodes[b]
 			const int e0 = tt * TE, ne = min(TE, m.E - e0);
-			for (int i = lt; i < TE * N * 3; i += 128)
+#pragma unroll
+			for (int k = 0; k < NV; ++k)
 			{
-				const int el = i / (N * 3), a = (i / 3) % N, d = i % 3;
-				if (el < ne)
-					cp_async8(&S.U[g][el][a][d], u + (size_t)S.nodes[g][el][a] * 3 + d);
-				else
-					S.U[g][el][a][d] = 0.0;
+				const int i = lt + 128 * k;
+				double v = 0.0;
+				if (i < NU)
+				{
+					const int el = i / (N * 3), a = (i / 3) % N, d = i % 3;
+					if (el < ne) v = __ldg(u + (size_t)S.nodes[b][el][a] * 3 + d);
+				}
+				else if (i < NU + NX)
+				{
+					const int i2 = i - NU, el = i2 / (NG * 3), j = (i2 / 3) % NG, d = i2 % 3;
+					if (el < ne) v = __ldg(m.X + (size_t)S.nodes[b][el][N + j] * 3 + d);
+				}
+				gv[k] = v;
 			}
-			for (int i = lt; i < TE * NG * 3; i += 128)
+			if (lt < TE) glm = lt < ne ? __ldg(m.lame + e0 + lt) : make_double2(0.0, 0.0);
+		};
+		auto store_values = [&](int b) {
+#pragma unroll
+			for (int k = 0; k < NV; ++k)
 			{
-				const int el = i / (NG * 3), j = (i / 3) % NG, d = i % 3;
-				if (el < ne)
-					cp_async8(&S.X[g][el][j][d], m.X + (size_t)S.nodes[g][el][N + j] * 3 + d);
-				else
-					S.X[g][el][j][d] = 0.0;
+				const int i = lt + 128 * k;
+				if (i < NU)
+					S.U[b][i / (N * 3)][(i / 3) % N][i % 3] = gv[k];
+				else if (i < NU + NX)
+				{
+					const int i2 = i - NU;
+					S.X[b][i2 / (NG * 3)][(i2 / 3) % NG][i2 % 3] = gv[k];
+				}
 			}
-			if (lt < TE)
+			if (lt < TE) S.lame[b][lt] = glm;
+		};
+		// affine elements: J, det J and G = J^-T J^-1 of element el of the tile whose
+		// node ids are in nodes[b], read straight from X
+		auto geometry = [&](int b, int el, bool valid) {
+			double *geo = S.geo[b][el];
+			if (!valid)
 			{
-				if (lt < ne)
-					cp_async16(&S.lame[g][lt], m.lame + e0 + lt);
-				else
-					S.lame[g][lt] = make_double2(0.0, 0.0);
+				for (int k = 0; k < 19; ++k) geo[k] = k == 18 ? 1.0 : 0.0;
+				return;
 			}
-			cp_async_commit();
+			double Xe[NG][3];
+#pragma unroll
+			for (int j = 0; j < NG; ++j)
+#pragma unroll
+				for (int d = 0; d < 3; ++d) Xe[j][d] = __ldg(m.X + (size_t)S.nodes[b][el][N + j] * 3 + d);
+			double Jac[3][3];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+				{
+					double s_ = 0.0;
+#pragma unroll
+					for (int j = 0; j < NG; ++j) s_ += S.ggtab[0][j][r] * Xe[j][c];
+					Jac[r][c] = s_;
+				}
+			const double detJ = det3(Jac);
+			double Jit[3][3];
+			inv_transpose3(Jac, detJ, Jit);
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c)
+				{
+					geo[3 * r + c] = Jac[r][c];
+					geo[9 + 3 * r + c] = Jit[r][0] * Jit[c][0] + Jit[r][1] * Jit[c][1] + Jit[r][2] * Jit[c][2];
+				}
+			geo[18] = detJ;
 		};
 		int t = blockIdx.x;
 		if (t < ntiles)
@@ -430,52 +472,27 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 			store_nodes(0);
 		}
 		named_sync(BAR_LOAD, 128);
-		if (t < ntiles) issue_gathers(0, t);
+		if (t < ntiles)
+		{
+			load_values(0, t);
+			if constexpr (EL::AFFINE)
+				if (lt >= GEO0 && lt < GEO0 + TE) geometry(0, lt - GEO0, lt - GEO0 < min(TE, m.E - t * TE));
+		}
 		if (t + (int)gridDim.x < ntiles) load_nodes(t + gridDim.x);
 		int it = 0;
 		for (; t < ntiles; t += gridDim.x, ++it)
 		{
 			const int buf = it & 1, g = it & 1;
 			const int tn = t + gridDim.x, tnn = tn + gridDim.x;
-			cp_async_wait_all();
-			named_sync(BAR_LOAD, 128); // this tile's gathers have landed; the other buffers are free
+			store_values(g);
 			if (tn < ntiles) store_nodes(g ^ 1);
-			named_sync(BAR_LOAD, 128);
-			if (tn < ntiles) issue_gathers(g ^ 1, tn);
+			named_sync(BAR_LOAD, 128); // this tile's inputs and geometry are in place; the other buffers are free
+			if (tn < ntiles) load_values(g ^ 1, tn);
 			if (tnn < ntiles) load_nodes(tnn);
 			const int e0 = t * TE, ne = min(TE, m.E - e0);
 			if constexpr (EL::AFFINE)
-			{
-				// the geometric map is affine: J, det J and G = J^-T J^-1 once per element
-				if (lt < TE)
-				{
-					double *geo = S.geo[lt];
-					double Jac[3][3];
-#pragma unroll
-					for (int r = 0; r < 3; ++r)
-#pragma unroll
-						for (int c = 0; c < 3; ++c)
-						{
-							double s_ = 0.0;
-#pragma unroll
-							for (int j = 0; j < NG; ++j) s_ += S.ggtab[0][j][r] * S.X[g][lt][j][c];
-							Jac[r][c] = s_;
-						}
-					const double detJ = det3(Jac);
-					double Jit[3][3];
-					inv_transpose3(Jac, detJ, Jit);
-#pragma unroll
-					for (int r = 0; r < 3; ++r)
-#pragma unroll
-						for (int c = 0; c < 3; ++c)
-						{
-							geo[3 * r + c] = Jac[r][c];
-							geo[9 + 3 * r + c] = Jit[r][0] * Jit[c][0] + Jit[r][1] * Jit[c][1] + Jit[r][2] * Jit[c][2];
-						}
-					geo[18] = detJ;
-				}
-				named_sync(BAR_LOAD, 128);
-			}
+				if (lt >= GEO0 && lt < GEO0 + TE && tn < ntiles)
+					geometry(g ^ 1, lt - GEO0, lt - GEO0 < min(TE, m.E - tn * TE));
 			if (it >= 2) named_sync(BAR_EMPTY0 + buf, TC_THREADS);
 			for (int i = lt; i < TE * NQ; i += 128)
 			{
@@ -494,7 +511,7 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 				double Jac[3][3], G[3][3], detJ;
 				if constexpr (EL::AFFINE)
 				{
-					const double *geo = S.geo[el];
+					const double *geo = S.geo[g][el];
 #pragma unroll
 					for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -594,13 +611,25 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 #pragma unroll
 				for (int q = 0; q < NQ; ++q)
 				{
-					const float *R = S.kin[buf][el][q];
+					// the (element, point) record as six 16-byte loads; rows r and c of Kt
+					// picked by selects (no indexed register access)
+					float R[24];
+					const float4 *R4 = reinterpret_cast<const float4 *>(S.kin[buf][el][q]);
+#pragma unroll
+					for (int k = 0; k < 6; ++k)
+					{
+						const float4 x = R4[k];
+						R[4 * k] = x.x;
+						R[4 * k + 1] = x.y;
+						R[4 * k + 2] = x.z;
+						R[4 * k + 3] = x.w;
+					}
 					float kr[3], kc[3], g[9];
 #pragma unroll
 					for (int k = 0; k < 3; ++k)
 					{
-						kr[k] = R[3 * r + k];
-						kc[k] = R[3 * c + k];
+						kr[k] = r == 0 ? R[k] : (r == 1 ? R[3 + k] : R[6 + k]);
+						kc[k] = c == 0 ? R[k] : (c == 1 ? R[3 + k] : R[6 + k]);
 					}
 #pragma unroll
 					for (int k = 0; k < 9; ++k) g[k] = R[9 + k];
