@@ -137,8 +137,23 @@ __device__ void reduce_to_result(double v, double *partials, double *result, uns
 	__syncthreads();
 	if (!s_last) return;
 	__threadfence();
+	// the partials this thread sums, in index order; up to eight loads (from L2,
+	// where the other blocks' writes are visible after their fences) are in flight
+	// before the first add, so the tail is one round trip instead of one per partial
 	double acc = 0.0;
-	for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) acc += *((volatile double *)partials + i);
+	for (int i0 = threadIdx.x; i0 < (int)gridDim.x; i0 += 8 * NT)
+	{
+		double x[8];
+#pragma unroll
+		for (int j = 0; j < 8; ++j)
+		{
+			const int i = i0 + j * NT;
+			x[j] = i < (int)gridDim.x ? __ldcg(partials + i) : 0.0;
+		}
+#pragma unroll
+		for (int j = 0; j < 8; ++j)
+			if (i0 + j * NT < (int)gridDim.x) acc += x[j];
+	}
 	acc = warp_sum(acc);
 	if (lane == 0) s_w[wid] = acc;
 	__syncthreads();
