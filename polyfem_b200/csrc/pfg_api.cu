@@ -394,12 +394,6 @@ int build_pattern(pfg_context *c)
 							   cudaMemcpyHostToDevice));
 	c->pat.nnz = nnz;
 	c->pat.max_deg = max_deg;
-	{
-		long long mi = 0;
-		for (int B = 0; B < N; ++B) mi = std::max(mi, ioff[B + 1] - ioff[B]);
-		c->pat.max_inc = (int)mi;
-		c->pat.max_plan = (int)(mi * n);
-	}
 	c->pat.outer = c->d_outer;
 	c->pat.inner = c->d_inner;
 	c->pat.contrib = c->d_contrib;

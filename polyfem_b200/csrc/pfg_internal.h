@@ -62,9 +62,7 @@ constexpr unsigned TRI_TRANSPOSED = 0x80000000u;
 struct DevPattern
 {
 	long long nnz = 0;
-	int max_deg = 0;  // largest number of neighbour nodes of a node
-	int max_inc = 0;  // largest number of incidences of a node
-	int max_plan = 0; // largest reduction plan of a node (n * incidences)
+	int max_deg = 0; // largest number of neighbour nodes of a node
 
 	const int *outer = nullptr;
 	const int *inner = nullptr;

@@ -866,125 +866,13 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 	}
 }
 
-// Windowed form of the reduction (the default; k_hessian_reduce remains for
-// nodes whose plan does not fit the shared copies).  One warp per column node B.
-// The warp copies B's plan and group starts to shared memory, then walks B's
-// row ranks in windows whose contributions fit WCH staged blocks: it loads the
-// window's blocks whole (nine consecutive values per block, consecutive lanes on
-// consecutive values, so each load instruction touches few sectors) into its
-// shared buffer, and the window's (rank, column) items sum their three values per
-// contribution from there, in FP64 and in incidence order -- the order of
-// k_hessian_reduce, so both give the same values bit for bit.  A rank group never
-// spans two windows.
-constexpr int RW_PLAN = 256, RW_DEG = 128;
-
-template <class T>
-__host__ __device__ constexpr int reduce_window_blocks()
-{
-	return sizeof(T) == 8 ? 64 : 128;
-}
-
-template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 4)
-	k_hessian_reduce_windows(DevMesh m, DevPattern pat, const T *__restrict__ stage)
-{
-	constexpr int N = EL::N, WCH = reduce_window_blocks<T>();
-	__shared__ unsigned s_plan[WARPS][RW_PLAN];
-	__shared__ unsigned short s_rel[WARPS][RW_DEG + 1];
-	__shared__ T s_blk[WARPS][WCH * 9];
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int B = blockIdx.x * WARPS + warp;
-	if (B >= m.N) return;
-	const int o0 = __ldg(pat.outer + 3 * B);
-	const int stride = __ldg(pat.outer + 3 * B + 1) - o0; // 3 * deg(B)
-	const int deg = stride / 3;
-	const int s0 = __ldg(m.inc_off + B), s1 = __ldg(m.inc_off + B + 1);
-	const int tot = (s1 - s0) * N;
-	if (tot > RW_PLAN || deg > RW_DEG || (s1 - s0) > WCH) return; // left to k_hessian_reduce (host checks)
-	const unsigned *cl = pat.contrib + (size_t)s0 * N;
-	const unsigned short *br = pat.blk_rel + o0 / 9;
-	unsigned *plan = s_plan[warp];
-	unsigned short *rel = s_rel[warp];
-	T *blk = s_blk[warp];
-	for (int i = lane; i < tot; i += 32) plan[i] = __ldg(cl + i);
-	for (int i = lane; i < deg; i += 32) rel[i] = __ldg(br + i);
-	if (lane == 0) rel[deg] = (unsigned short)tot;
-	__syncwarp();
-	double *dst = pat.values + o0;
-	for (int r0 = 0; r0 < deg;)
-	{
-		// the largest window [r0, r1) of rank groups with at most WCH blocks (a group
-		// has at most one block per incidence, so at least one group fits)
-		int lo = r0 + 1, hi = deg;
-		const int lim = rel[r0] + WCH;
-		while (lo < hi)
-		{
-			const int mid = (lo + hi + 1) >> 1;
-			if (rel[mid] <= lim)
-				lo = mid;
-			else
-				hi = mid - 1;
-		}
-		const int r1 = lo;
-		const int b0 = rel[r0], nb = rel[r1] - b0;
-		for (int f = lane; f < nb * 9; f += 32)
-		{
-			const int kb = f / 9, v = f - 9 * kb;
-			blk[f] = __ldg(stage + (plan[b0 + kb] & ~TRI_TRANSPOSED) + v);
-		}
-		__syncwarp();
-		for (int it = lane; it < 3 * (r1 - r0); it += 32)
-		{
-			const int r = r0 + it / 3, c = it - 3 * (it / 3);
-			const int k0 = rel[r], k1 = rel[r + 1];
-			double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-			for (int k = k0; k < k1; ++k)
-			{
-				const bool tr = plan[k] & TRI_TRANSPOSED;
-				const T *p = blk + 9 * (k - b0) + (tr ? c : 3 * c);
-				const int st = tr ? 3 : 1;
-				a0 += double(p[0]);
-				a1 += double(p[st]);
-				a2 += double(p[2 * st]);
-			}
-			if (pat.red_col_start == nullptr)
-			{
-				double *d = dst + c * stride + 3 * r;
-				d[0] = a0;
-				d[1] = a1;
-				d[2] = a2;
-			}
-			else
-			{
-				const int cs = __ldg(pat.red_col_start + 3 * B + c);
-				if (cs >= 0)
-				{
-					const unsigned short *ro = pat.red_row_off + o0 / 3 + 3 * r;
-					const unsigned short q0 = __ldg(ro), q1 = __ldg(ro + 1), q2 = __ldg(ro + 2);
-					if (q0 != 0xFFFF) pat.values[cs + q0] = a0;
-					if (q1 != 0xFFFF) pat.values[cs + q1] = a1;
-					if (q2 != 0xFFFF) pat.values[cs + q2] = a2;
-				}
-			}
-		}
-		__syncwarp();
-		r0 = r1;
-	}
-}
-
-// Pass 2 of every Hessian-pattern assembly: the windowed kernel when every node's
-// plan fits its shared copies (the pattern build records that), else the
-// plan-driven kernel for all nodes.
+// Pass 2 of every Hessian-pattern assembly.
 template <class EL, class T>
 static cudaError_t launch_reduce(const DevMesh &m, const DevPattern &p, const T *stage, cudaStream_t s)
 {
 	if (m.N <= 0) return cudaSuccess;
 	constexpr int WARPS = 8;
-	const bool windows = p.max_plan <= RW_PLAN && p.max_deg <= RW_DEG && p.max_inc <= reduce_window_blocks<T>();
-	if (windows)
-		k_hessian_reduce_windows<EL, T, WARPS><<<(m.N + WARPS - 1) / WARPS, WARPS * 32, 0, s>>>(m, p, stage);
-	else
-		k_hessian_reduce<EL, T, WARPS><<<(m.N + WARPS - 1) / WARPS, WARPS * 32, 0, s>>>(m, p, stage);
+	k_hessian_reduce<EL, T, WARPS><<<(m.N + WARPS - 1) / WARPS, WARPS * 32, 0, s>>>(m, p, stage);
 	return cudaGetLastError();
 }
 
