@@ -6,12 +6,15 @@ split 6 tets/hex (384,000 elements, 531,441 nodes, 1,594,323 dofs, 134,475,849
 CSC nonzeros), 4-point quadrature, per-element lognormal Lame parameters, seeded
 synthetic displacement u = 0.02 h N(0,1).  One step = one assembly of the global
 Hessian CSC values through the path's C ABI (pfg_hessian), which launches two
-kernels: k_hessian_blocks (element blocks -> one packed block triangle per element)
-and a reduction kernel (blocks -> CSC columns, summed per entry in a fixed order).
+kernels: the element blocks (split32: k_hessian_blocks_tc on the tensor cores; FP64:
+k_hessian_blocks on CUDA cores) -> one packed block triangle per element, and the
+reduction kernel (blocks -> CSC columns, summed per entry in a fixed order).
 
   value     : split-precision Hessian assembly, inputs resident in HBM (elements/s)
   e2e       : the same call with host buffers (pinned u in, CSC values out) (elements/s)
   fp64      : the plain FP64 drop-in kernel, same workload (elements/s)
+  split32_simt : the same split with the element contraction on CUDA cores
+  configs   : the other four workloads' operations (energy, gradient, Hessian, adjoint terms)
   cpu_baseline / --impl reference : the CPU oracle port of the reference's TBB
               assembly (NLAssembler::assemble_hessian) on the host cores.
 
@@ -39,9 +42,9 @@ sys.path.insert(0, REPO)
 METRIC = "NeoHookean elem Hessians/s on 1 B200: split-FP32 vs FP64, rel err vs FP64"
 UNIT = "elements/s"
 SEED_LAME, SEED_U = 5, 2
-PRECISION_NOTE = ("split32 = FP64 kinematics (J^-T, F, det/log J, F^-T, basis gradients) + FP32 "
-                  "block contraction and FP32 staged element blocks + FP64 per-entry sums and CSC values "
-                  "(CUDA cores)")
+PRECISION_NOTE = ("split32 = FP64 kinematics (J^-T, M = dx/dxi, det/log J, M^-T) + element contraction on the "
+                  "tensor cores (tcgen05 kind::tf32, each FP32 operand split into two TF32 halves, 3 products, FP32 "
+                  "accumulation in TMEM) + FP32 staged element blocks + FP64 per-entry sums and CSC values")
 
 
 def workload_name(grid: int) -> str:
@@ -418,7 +421,7 @@ def run_gpu(args):
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "bytes_alg_per_launch": bytes_alg,
                          "staged_bytes_per_launch": staged_bytes(mesh, nnz, tri_bytes),
-                         "note": "one pfg_hessian call = k_hessian_blocks + the reduction kernel, CUDA events "
+                         "note": "one pfg_hessian call = k_hessian_blocks_tc + the reduction kernel, CUDA events "
                                  "on the context's stream; frac of measured HBM copy bandwidth; traffic = ncu "
                                  "DRAM bytes per element of the 24^3 capture x elements"},
             "cpu_baseline": cpu,
