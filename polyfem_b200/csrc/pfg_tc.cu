@@ -57,8 +57,12 @@ struct TcCfg
 	static constexpr int N = EL::N, NG = EL::NG, NQ = EL::NQ;
 	static constexpr int NP = N * (N + 1) / 2;         // node pairs a <= b
 	static constexpr int NPAD = (NP + 15) / 16 * 16;   // MMA N (multiple of 16 for M = 128)
-	static constexpr int KD = 9 * NQ;                  // (k, l, q)
-	static constexpr int KP = (KD + 7) / 8 * 8;        // MMA K, padded to the TF32 K step of 8
+	// The K dimension runs in parts of four points (Q1: two parts) through one A
+	// buffer, so that the A operand of an 8-point element fits two CTAs per SM.
+	static constexpr int NQH = NQ < 4 ? NQ : 4;        // points per part
+	static constexpr int KH = NQ / NQH;                // parts
+	static constexpr int KD = 9 * NQH;                 // (k, l, q) of one part
+	static constexpr int KP = (KD + 7) / 8 * 8;        // MMA K of a part, padded to the TF32 K step of 8
 	static constexpr int KC = KP / 4;                  // 16-byte K chunks (4 TF32 values)
 	static constexpr int TE = 14;                      // elements per 128-row tile (9 rows each)
 	static constexpr int ROWS = 9 * TE;                // 126 valid rows of 128
@@ -67,17 +71,18 @@ struct TcCfg
 	static constexpr uint32_t TMEM_COLS = 64;          // power of two >= NPAD
 	static constexpr uint32_t A_CHUNK = 128 * 16;      // bytes of one K chunk of A (128 rows)
 	static constexpr uint32_t B_CHUNK = NPAD * 16;     // bytes of one K chunk of B
-	static constexpr uint32_t B_BYTES = 2u * KC * B_CHUNK; // hi and lo halves of Phi
+	static constexpr uint32_t B_PART = 2u * KC * B_CHUNK;   // hi and lo halves of one part of Phi
+	static constexpr uint32_t B_BYTES = KH * B_PART;
 	static_assert(NPAD <= (int)TMEM_COLS, "accumulator must fit the TMEM allocation");
 	static_assert(KD <= KP && KP % 8 == 0, "K padding");
-	static_assert(NQ == 4 || NQ == 8, "K order groups the points of one (k, l) in 16-byte chunks");
+	static_assert(NQH == 4 && NQ % NQH == 0, "K order groups four points of one (k, l) in a 16-byte chunk");
 	static_assert(TE * TP <= 2 * KC * 128 * 4, "the block triangles must fit the A operand's bytes");
 };
 
 // Shared memory of one CTA.  A and B use the canonical K-major layout without
 // swizzle: a K chunk is 16 bytes (4 TF32) of every row, rows 16 bytes apart,
 // consecutive chunks A_CHUNK / B_CHUNK bytes apart (LBO), 8-row groups 128
-// bytes apart (SBO).  K index j = (3k + l) * NQ + q.
+// bytes apart (SBO).  K index within part h: j = (3k + l) * 4 + (q - 4h).
 template <class EL>
 struct TcSmem
 {
@@ -93,8 +98,7 @@ struct TcSmem
 		};
 		alignas(1024) float out[C::TE * C::TP];
 	};
-	alignas(1024) float Bh[C::KC][C::NPAD][4]; // Bh then Bl, contiguous: one bulk copy
-	float Bl[C::KC][C::NPAD][4];
+	alignas(1024) float B[C::KH][2][C::KC][C::NPAD][4]; // Phi per part: hi then lo, all parts contiguous (one bulk copy)
 	alignas(16) float kin[2][C::TE][C::NQ][C::KIN];
 	// gathered inputs, two tiles: the next tile's copies are in flight while this
 	// tile's kinematics run
@@ -102,7 +106,7 @@ struct TcSmem
 	double X[2][C::TE][C::NG][3];
 	double2 lame[2][C::TE];
 	int nodes[2][C::TE][C::N + C::NG];
-	double geo[2][C::TE][20]; // affine elements: J (9), G = J^-T J^-1 (9), det J
+	double geo[EL::AFFINE ? 2 : 1][C::TE][20]; // affine elements: J (9), G = J^-T J^-1 (9), det J
 	double gtab[C::NQ][C::N][3];
 	double ggtab[EL::AFFINE ? 1 : C::NQ][C::NG][3];
 	double wq[C::NQ];
@@ -268,7 +272,6 @@ std::vector<float> build_phi()
 {
 	using C = TcCfg<EL>;
 	std::vector<float> t(C::B_BYTES / 4, 0.f);
-	float *hi = t.data(), *lo = t.data() + C::KC * C::NPAD * 4;
 	int p = 0;
 	for (int a = 0; a < C::N; ++a)
 		for (int b = a; b < C::N; ++b, ++p)
@@ -279,7 +282,9 @@ std::vector<float> build_phi()
 						const double x = gref<EL>(q, a, k) * gref<EL>(q, b, l);
 						const float h = tf32_round((float)x);
 						const float r = tf32_round((float)(x - (double)h));
-						const int j = (3 * k + l) * C::NQ + q;
+						const int part = q / C::NQH, j = (3 * k + l) * C::NQH + (q - part * C::NQH);
+						float *hi = t.data() + (size_t)part * (C::B_PART / 4);
+						float *lo = hi + C::KC * C::NPAD * 4;
 						const size_t off = ((size_t)(j / 4) * C::NPAD + p) * 4 + (j % 4);
 						hi[off] = h;
 						lo[off] = r;
@@ -352,7 +357,7 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 	if (tid == 0)
 	{
 		mbar_expect_tx(&S.bar_b, C::B_BYTES);
-		bulk_load(&S.Bh[0][0][0], phi, C::B_BYTES, &S.bar_b);
+		bulk_load(&S.B[0][0][0][0][0], phi, C::B_BYTES, &S.bar_b);
 	}
 	const uint32_t tmem = S.tmem_base;
 
@@ -596,96 +601,112 @@ __global__ void __launch_bounds__(TC_THREADS, tc_min_ctas<EL>())
 			if (m.err) atomicExch(m.err, 1);
 		}
 		int it = 0;
+		unsigned mma_phase = 0; // completed phases of bar_mma waited on so far (one per part of every tile)
 		for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it)
 		{
 			const int buf = it & 1;
 			const int e0 = t * TE, ne = min(TE, m.E - e0);
 			named_sync(BAR_FULL0 + buf, TC_THREADS);
-			if (tid == 0) bulk_wait_read_all(); // the previous tile's store has left the A bytes
-			named_sync(BAR_MATH, 128);
 			bool bad = false; // the row's element has a point with J <= 0
-			if (row < C::ROWS)
+#pragma unroll 1
+			for (int h = 0; h < C::KH; ++h)
 			{
-				const int el = row / 9, rc = row % 9, r = rc / 3, c = rc % 3;
-				float w[9][NQ];
-#pragma unroll
-				for (int q = 0; q < NQ; ++q)
+				if (h == 0)
 				{
-					// the (element, point) record as six 16-byte loads; rows r and c of Kt
-					// picked by selects (no indexed register access)
-					float R[24];
-					const float4 *R4 = reinterpret_cast<const float4 *>(S.kin[buf][el][q]);
-#pragma unroll
-					for (int k = 0; k < 6; ++k)
+					if (tid == 0) bulk_wait_read_all(); // the previous tile's store has left the A bytes
+				}
+				else if (tid == 0 && !S.abort)
+				{
+					// the previous part's MMAs must be done with A before it is rewritten
+					if (!mbar_wait(&S.bar_mma, mma_phase & 1))
 					{
-						const float4 x = R4[k];
-						R[4 * k] = x.x;
-						R[4 * k + 1] = x.y;
-						R[4 * k + 2] = x.z;
-						R[4 * k + 3] = x.w;
-					}
-					float kr[3], kc[3], g[9];
-#pragma unroll
-					for (int k = 0; k < 3; ++k)
-					{
-						kr[k] = r == 0 ? R[k] : (r == 1 ? R[3 + k] : R[6 + k]);
-						kc[k] = c == 0 ? R[k] : (c == 1 ? R[3 + k] : R[6 + k]);
-					}
-#pragma unroll
-					for (int k = 0; k < 9; ++k) g[k] = R[9 + k];
-					const float dmu = (r == c) ? R[18] : 0.f, dl = R[19], dw = R[20];
-					bad |= R[21] != 0.f;
-#pragma unroll
-					for (int k = 0; k < 3; ++k)
-					{
-						const float a1 = dl * kr[k], a2 = dw * kc[k];
-#pragma unroll
-						for (int l = 0; l < 3; ++l) w[3 * k + l][q] = fmaf(a1, kc[l], fmaf(a2, kr[l], dmu * g[3 * k + l]));
+						S.abort = 1;
+						if (m.err) atomicExch(m.err, 1);
 					}
 				}
+				if (h > 0) ++mma_phase;
+				named_sync(BAR_MATH, 128);
+				if (row < C::ROWS)
+				{
+					const int el = row / 9, rc = row % 9, r = rc / 3, c = rc % 3;
+					float w[9][C::NQH];
 #pragma unroll
-				for (int kl = 0; kl < 9; ++kl)
-#pragma unroll
-					for (int q0 = 0; q0 < NQ; q0 += 4)
+					for (int qh = 0; qh < C::NQH; ++qh)
 					{
-						float h[4], l4[4];
+						// the (element, point) record as six 16-byte loads; rows r and c of Kt
+						// picked by selects (no indexed register access)
+						float R[24];
+						const float4 *R4 = reinterpret_cast<const float4 *>(S.kin[buf][el][h * C::NQH + qh]);
+#pragma unroll
+						for (int k = 0; k < 6; ++k)
+						{
+							const float4 x = R4[k];
+							R[4 * k] = x.x;
+							R[4 * k + 1] = x.y;
+							R[4 * k + 2] = x.z;
+							R[4 * k + 3] = x.w;
+						}
+						float kr[3], kc[3], g[9];
+#pragma unroll
+						for (int k = 0; k < 3; ++k)
+						{
+							kr[k] = r == 0 ? R[k] : (r == 1 ? R[3 + k] : R[6 + k]);
+							kc[k] = c == 0 ? R[k] : (c == 1 ? R[3 + k] : R[6 + k]);
+						}
+#pragma unroll
+						for (int k = 0; k < 9; ++k) g[k] = R[9 + k];
+						const float dmu = (r == c) ? R[18] : 0.f, dl = R[19], dw = R[20];
+						bad |= R[21] != 0.f;
+#pragma unroll
+						for (int k = 0; k < 3; ++k)
+						{
+							const float a1 = dl * kr[k], a2 = dw * kc[k];
+#pragma unroll
+							for (int l = 0; l < 3; ++l) w[3 * k + l][qh] = fmaf(a1, kc[l], fmaf(a2, kr[l], dmu * g[3 * k + l]));
+						}
+					}
+#pragma unroll
+					for (int kl = 0; kl < 9; ++kl)
+					{
+						float hh[4], ll[4];
 #pragma unroll
 						for (int i = 0; i < 4; ++i)
 						{
-							h[i] = tf32_round(w[kl][q0 + i]);
-							l4[i] = tf32_round(w[kl][q0 + i] - h[i]);
+							hh[i] = tf32_round(w[kl][i]);
+							ll[i] = tf32_round(w[kl][i] - hh[i]);
 						}
-						const int kc4 = (kl * NQ + q0) / 4;
-						*reinterpret_cast<float4 *>(S.Ah[kc4][row]) = make_float4(h[0], h[1], h[2], h[3]);
-						*reinterpret_cast<float4 *>(S.Al[kc4][row]) = make_float4(l4[0], l4[1], l4[2], l4[3]);
+						*reinterpret_cast<float4 *>(S.Ah[kl][row]) = make_float4(hh[0], hh[1], hh[2], hh[3]);
+						*reinterpret_cast<float4 *>(S.Al[kl][row]) = make_float4(ll[0], ll[1], ll[2], ll[3]);
 					}
-			}
-			named_arrive(BAR_EMPTY0 + buf, TC_THREADS); // kin[buf] consumed
-			fence_proxy_async_smem();
-			named_sync(BAR_MATH, 128);
-			if (tid == 0 && !S.abort)
-			{
-				tc_fence_after();
-				const uint32_t idesc = idesc_tf32(128, C::NPAD);
-				const uint32_t a_h = smem_u32(&S.Ah[0][0][0]), a_l = smem_u32(&S.Al[0][0][0]);
-				const uint32_t b_h = smem_u32(&S.Bh[0][0][0]), b_l = smem_u32(&S.Bl[0][0][0]);
+				}
+				if (h == C::KH - 1) named_arrive(BAR_EMPTY0 + buf, TC_THREADS); // kin[buf] consumed
+				fence_proxy_async_smem();
+				named_sync(BAR_MATH, 128);
+				if (tid == 0 && !S.abort)
+				{
+					tc_fence_after();
+					const uint32_t idesc = idesc_tf32(128, C::NPAD);
+					const uint32_t a_h = smem_u32(&S.Ah[0][0][0]), a_l = smem_u32(&S.Al[0][0][0]);
+					const uint32_t b_h = smem_u32(&S.B[h][0][0][0][0]), b_l = smem_u32(&S.B[h][1][0][0][0]);
 #pragma unroll 1
-				for (int s = 0; s < C::KP / 8; ++s)
-				{
-					const uint32_t ao = s * 2 * C::A_CHUNK, bo = s * 2 * C::B_CHUNK;
-					const uint64_t dah = smem_desc(a_h + ao, C::A_CHUNK, 128), dal = smem_desc(a_l + ao, C::A_CHUNK, 128);
-					const uint64_t dbh = smem_desc(b_h + bo, C::B_CHUNK, 128), dbl = smem_desc(b_l + bo, C::B_CHUNK, 128);
-					mma_tf32(tmem, dal, dbh, idesc, s > 0 ? 1u : 0u);
-					mma_tf32(tmem, dah, dbl, idesc, 1u);
-					mma_tf32(tmem, dah, dbh, idesc, 1u);
-				}
-				mma_commit(&S.bar_mma);
-				if (!mbar_wait(&S.bar_mma, it & 1))
-				{
-					S.abort = 1;
-					if (m.err) atomicExch(m.err, 1);
+					for (int ks = 0; ks < C::KP / 8; ++ks)
+					{
+						const uint32_t ao = ks * 2 * C::A_CHUNK, bo = ks * 2 * C::B_CHUNK;
+						const uint64_t dah = smem_desc(a_h + ao, C::A_CHUNK, 128), dal = smem_desc(a_l + ao, C::A_CHUNK, 128);
+						const uint64_t dbh = smem_desc(b_h + bo, C::B_CHUNK, 128), dbl = smem_desc(b_l + bo, C::B_CHUNK, 128);
+						mma_tf32(tmem, dal, dbh, idesc, (h > 0 || ks > 0) ? 1u : 0u);
+						mma_tf32(tmem, dah, dbl, idesc, 1u);
+						mma_tf32(tmem, dah, dbh, idesc, 1u);
+					}
+					mma_commit(&S.bar_mma);
 				}
 			}
+			if (tid == 0 && !S.abort && !mbar_wait(&S.bar_mma, mma_phase & 1))
+			{
+				S.abort = 1;
+				if (m.err) atomicExch(m.err, 1);
+			}
+			++mma_phase;
 			tc_fence_before();
 			named_sync(BAR_MATH, 128);
 			tc_fence_after();
