@@ -791,81 +791,76 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 	k_hessian_reduce(DevMesh m, DevPattern pat, const T *__restrict__ stage)
 {
 	constexpr int N = EL::N;
-	const int lane = threadIdx.x & 31;
-	// persistent warps: node B = warp id, then every total_warps-th node, so that a
-	// warp's nodes mix long (vertex) and short (edge) columns and no block waits for
-	// its slowest warp
-	const int total_warps = gridDim.x * WARPS;
-	for (int B = blockIdx.x * WARPS + (threadIdx.x >> 5); B < m.N; B += total_warps)
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int B = blockIdx.x * WARPS + warp;
+	if (B >= m.N) return;
+	const int o0 = __ldg(pat.outer + 3 * B);
+	const int stride = __ldg(pat.outer + 3 * B + 1) - o0; // 3 * deg(B)
+	const int deg = stride / 3;
+	const int s0 = __ldg(m.inc_off + B), s1 = __ldg(m.inc_off + B + 1);
+	const int tot = (s1 - s0) * N;
+	const unsigned *cl = pat.contrib + (size_t)s0 * N;
+	const unsigned short *br = pat.blk_rel + o0 / 9;
+	double *dst = pat.values + o0;
+	for (int it = lane; it < stride; it += 32)
 	{
-		const int o0 = __ldg(pat.outer + 3 * B);
-		const int stride = __ldg(pat.outer + 3 * B + 1) - o0; // 3 * deg(B)
-		const int deg = stride / 3;
-		const int s0 = __ldg(m.inc_off + B), s1 = __ldg(m.inc_off + B + 1);
-		const int tot = (s1 - s0) * N;
-		const unsigned *cl = pat.contrib + (size_t)s0 * N;
-		const unsigned short *br = pat.blk_rel + o0 / 9;
-		double *dst = pat.values + o0;
-		for (int it = lane; it < stride; it += 32)
+		// (rank, column) items rank-major: the three items of the diagonal block,
+		// which has the longest contribution list, share one pass of the warp
+		const int r = it / 3, c = it - 3 * r;
+		const int k0 = __ldg(br + r);
+		const int k1 = (r + 1 < deg) ? (int)__ldg(br + r + 1) : tot;
+		double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+		// two contributions per step, the next step's plan entries loaded ahead;
+		// the sum order stays k ascending
+		unsigned qa = k0 < k1 ? __ldg(cl + k0) : 0u;
+		unsigned qb = k0 + 1 < k1 ? __ldg(cl + k0 + 1) : 0u;
+		for (int k = k0; k < k1; k += 2)
 		{
-			// (rank, column) items rank-major: the three items of the diagonal block,
-			// which has the longest contribution list, share one pass of the warp
-			const int r = it / 3, c = it - 3 * r;
-			const int k0 = __ldg(br + r);
-			const int k1 = (r + 1 < deg) ? (int)__ldg(br + r + 1) : tot;
-			double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-			// two contributions per step, the next step's plan entries loaded ahead;
-			// the sum order stays k ascending
-			unsigned qa = k0 < k1 ? __ldg(cl + k0) : 0u;
-			unsigned qb = k0 + 1 < k1 ? __ldg(cl + k0 + 1) : 0u;
-			for (int k = k0; k < k1; k += 2)
+			const unsigned q0 = qa, q1 = qb;
+			const bool two = k + 1 < k1;
+			qa = k + 2 < k1 ? __ldg(cl + k + 2) : 0u;
+			qb = k + 3 < k1 ? __ldg(cl + k + 3) : 0u;
+			// (a, b): values 3c, 3c+1, 3c+2 of the block; transposed (b, a): c, c+3, c+6
+			const bool t0 = q0 & TRI_TRANSPOSED, t1 = q1 & TRI_TRANSPOSED;
+			const T *p0 = stage + (q0 & ~TRI_TRANSPOSED) + (t0 ? c : 3 * c);
+			const T *p1 = stage + (q1 & ~TRI_TRANSPOSED) + (t1 ? c : 3 * c);
+			const int s0_ = t0 ? 3 : 1, s1_ = t1 ? 3 : 1;
+			const T x0 = __ldg(p0), x1 = __ldg(p0 + s0_), x2 = __ldg(p0 + 2 * s0_);
+			T y0 = T(0), y1 = T(0), y2 = T(0);
+			if (two)
 			{
-				const unsigned q0 = qa, q1 = qb;
-				const bool two = k + 1 < k1;
-				qa = k + 2 < k1 ? __ldg(cl + k + 2) : 0u;
-				qb = k + 3 < k1 ? __ldg(cl + k + 3) : 0u;
-				// (a, b): values 3c, 3c+1, 3c+2 of the block; transposed (b, a): c, c+3, c+6
-				const bool t0 = q0 & TRI_TRANSPOSED, t1 = q1 & TRI_TRANSPOSED;
-				const T *p0 = stage + (q0 & ~TRI_TRANSPOSED) + (t0 ? c : 3 * c);
-				const T *p1 = stage + (q1 & ~TRI_TRANSPOSED) + (t1 ? c : 3 * c);
-				const int s0_ = t0 ? 3 : 1, s1_ = t1 ? 3 : 1;
-				const T x0 = __ldg(p0), x1 = __ldg(p0 + s0_), x2 = __ldg(p0 + 2 * s0_);
-				T y0 = T(0), y1 = T(0), y2 = T(0);
-				if (two)
-				{
-					y0 = __ldg(p1);
-					y1 = __ldg(p1 + s1_);
-					y2 = __ldg(p1 + 2 * s1_);
-				}
-				a0 += double(x0);
-				a1 += double(x1);
-				a2 += double(x2);
-				if (two)
-				{
-					a0 += double(y0);
-					a1 += double(y1);
-					a2 += double(y2);
-				}
+				y0 = __ldg(p1);
+				y1 = __ldg(p1 + s1_);
+				y2 = __ldg(p1 + 2 * s1_);
 			}
-			if (pat.red_col_start == nullptr)
+			a0 += double(x0);
+			a1 += double(x1);
+			a2 += double(x2);
+			if (two)
 			{
-				double *d = dst + c * stride + 3 * r;
-				d[0] = a0;
-				d[1] = a1;
-				d[2] = a2;
+				a0 += double(y0);
+				a1 += double(y1);
+				a2 += double(y2);
 			}
-			else
+		}
+		if (pat.red_col_start == nullptr)
+		{
+			double *d = dst + c * stride + 3 * r;
+			d[0] = a0;
+			d[1] = a1;
+			d[2] = a2;
+		}
+		else
+		{
+			// Dirichlet-reduced output: free rows of free columns only
+			const int cs = __ldg(pat.red_col_start + 3 * B + c);
+			if (cs >= 0)
 			{
-				// Dirichlet-reduced output: free rows of free columns only
-				const int cs = __ldg(pat.red_col_start + 3 * B + c);
-				if (cs >= 0)
-				{
-					const unsigned short *ro = pat.red_row_off + o0 / 3 + 3 * r;
-					const unsigned short r0 = __ldg(ro), r1 = __ldg(ro + 1), r2 = __ldg(ro + 2);
-					if (r0 != 0xFFFF) pat.values[cs + r0] = a0;
-					if (r1 != 0xFFFF) pat.values[cs + r1] = a1;
-					if (r2 != 0xFFFF) pat.values[cs + r2] = a2;
-				}
+				const unsigned short *ro = pat.red_row_off + o0 / 3 + 3 * r;
+				const unsigned short r0 = __ldg(ro), r1 = __ldg(ro + 1), r2 = __ldg(ro + 2);
+				if (r0 != 0xFFFF) pat.values[cs + r0] = a0;
+				if (r1 != 0xFFFF) pat.values[cs + r1] = a1;
+				if (r2 != 0xFFFF) pat.values[cs + r2] = a2;
 			}
 		}
 	}
@@ -877,16 +872,7 @@ static cudaError_t launch_reduce(const DevMesh &m, const DevPattern &p, const T 
 {
 	if (m.N <= 0) return cudaSuccess;
 	constexpr int WARPS = 8;
-	static int sms = 0;
-	if (!sms)
-	{
-		int dev = 0;
-		cudaGetDevice(&dev);
-		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-		if (sms <= 0) sms = 148;
-	}
-	const int grid = std::min((m.N + WARPS - 1) / WARPS, sms * 8); // 8 CTAs of 8 warps per SM
-	k_hessian_reduce<EL, T, WARPS><<<grid, WARPS * 32, 0, s>>>(m, p, stage);
+	k_hessian_reduce<EL, T, WARPS><<<(m.N + WARPS - 1) / WARPS, WARPS * 32, 0, s>>>(m, p, stage);
 	return cudaGetLastError();
 }
 
