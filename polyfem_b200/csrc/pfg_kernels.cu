@@ -118,9 +118,10 @@ __global__ void __launch_bounds__(NT, elem_kernel_min_ctas<EL>()) k_energy(DevMe
 											   double *__restrict__ result, unsigned int *ticket,
 											   unsigned long long *inverted)
 {
-	const int e = blockIdx.x * NT + threadIdx.x;
+	// grid-stride: a resident grid, each thread summing its elements in order, so the
+	// block reduction and the partials' tail are paid once per resident block
 	double en = 0.0;
-	if (e < m.E) en = element_energy<EL, T>(m, u, e, inverted);
+	for (int e = blockIdx.x * NT + threadIdx.x; e < m.E; e += gridDim.x * NT) en += element_energy<EL, T>(m, u, e, inverted);
 	reduce_to_result<NT>(en, partials, result, ticket);
 }
 
@@ -281,6 +282,66 @@ __global__ void __launch_bounds__(NT) k_vec_gather(int n_nodes, const int *__res
 	out[(size_t)B * 3 + 0] = t0;
 	out[(size_t)B * 3 + 1] = t1;
 	out[(size_t)B * 3 + 2] = t2;
+}
+
+// The same sums with G lanes per node: lane l loads slots l, l + G, ... of the
+// node's contiguous run (consecutive lanes on consecutive 32-byte slots), sums
+// them in that order, and the G partial sums meet in a fixed butterfly.  The
+// order is fixed, so the result is deterministic.  Used when a node has many
+// incidences on average (P1: ~19), where one thread per node queues too many
+// loads per thread.
+template <int G, int NT>
+__global__ void __launch_bounds__(NT) k_vec_gather_group(int n_nodes, const int *__restrict__ off,
+														 const double *__restrict__ stage, double *__restrict__ out)
+{
+	static_assert(G == 8 || G == 16 || G == 32, "node groups are aligned parts of a warp");
+	const int t = blockIdx.x * NT + threadIdx.x;
+	const int B = t / G, l = t % G;
+	if (B >= n_nodes) return; // whole groups leave together: n_nodes is per group
+	const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+	const int k0 = __ldg(off + B), k1 = __ldg(off + B + 1);
+	const double2 *slots = reinterpret_cast<const double2 *>(stage);
+	double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+	for (int k = k0 + l; k < k1; k += G)
+	{
+		const double2 x = __ldg(slots + 2 * (size_t)k);
+		const double2 y = __ldg(slots + 2 * (size_t)k + 1);
+		t0 += x.x;
+		t1 += x.y;
+		t2 += y.x;
+	}
+#pragma unroll
+	for (int o = G / 2; o > 0; o >>= 1)
+	{
+		t0 += __shfl_xor_sync(mask, t0, o);
+		t1 += __shfl_xor_sync(mask, t1, o);
+		t2 += __shfl_xor_sync(mask, t2, o);
+	}
+	if (l == 0)
+	{
+		out[(size_t)B * 3 + 0] = t0;
+		out[(size_t)B * 3 + 1] = t1;
+		out[(size_t)B * 3 + 2] = t2;
+	}
+}
+
+__host__ __device__ constexpr int nodes_of(int et) { return et == 1 ? 4 : et == 2 ? 10 : 8; }
+__host__ __device__ constexpr int geom_nodes_of(int et) { return et == 3 ? 8 : 4; }
+
+// Per-node sums of one 32-byte slot per incidence: a G-lane group per node when
+// nodes average more than 12 incidences, else one thread per node.
+static void launch_vec_gather(int n_nodes, const int *off, long long n_inc, const double *stage, double *out,
+							  cudaStream_t s)
+{
+	if (n_nodes <= 0) return;
+	constexpr int NT = 128;
+	if (n_inc > 12LL * n_nodes)
+	{
+		constexpr int G = 32;
+		k_vec_gather_group<G, NT><<<(int)(((long long)n_nodes * G + NT - 1) / NT), NT, 0, s>>>(n_nodes, off, stage, out);
+	}
+	else
+		k_vec_gather<NT><<<(n_nodes + NT - 1) / NT, NT, 0, s>>>(n_nodes, off, stage, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -2170,7 +2231,20 @@ static void energy_t(const DevMesh &m, const double *u, bool per_element, double
 	if (per_element)
 		k_energy_per_element<EL, T, NT><<<nb, NT, 0, s>>>(m, u, out, sc.inverted);
 	else
-		k_energy<EL, T, NT><<<nb, NT, 0, s>>>(m, u, sc.partials, out, sc.ticket, sc.inverted);
+	{
+		// as many blocks as stay resident (never more than one per 256 elements, the
+		// partials' capacity)
+		static int resident = 0;
+		if (!resident)
+		{
+			int dev = 0, sms = 0, per_sm = 0;
+			cudaGetDevice(&dev);
+			cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+			cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_energy<EL, T, NT>, NT, 0);
+			resident = std::max(1, sms) * std::max(1, per_sm);
+		}
+		k_energy<EL, T, NT><<<std::min(nb, resident), NT, 0, s>>>(m, u, sc.partials, out, sc.ticket, sc.inverted);
+	}
 }
 
 template <class EL, int MAT>
@@ -2266,8 +2340,7 @@ cudaError_t launch_gradient(const DevMesh &m, const double *u, int prec, double 
 		case 3: f32 ? gradient_t<Q1Hex, float>(m, u, sc, s) : gradient_t<Q1Hex, double>(m, u, sc, s); break;
 		default: return cudaErrorInvalidValue;
 		}
-	constexpr int NTG = 128;
-	if (m.N > 0) k_vec_gather<NTG><<<blocks_for(m.N, NTG), NTG, 0, s>>>(m.N, m.inc_off, sc.vec_stage, g);
+	launch_vec_gather(m.N, m.inc_off, (long long)m.E * nodes_of(m.et), sc.vec_stage, g, s);
 	return cudaGetLastError();
 }
 
@@ -2308,8 +2381,7 @@ cudaError_t launch_shape_vjp(const DevMesh &m, const double *u, const double *ad
 		case 3: f32 ? k_shape_vjp<Q1Hex, float, NT><<<nb, NT, 0, s>>>(m, u, adj, st) : k_shape_vjp<Q1Hex, double, NT><<<nb, NT, 0, s>>>(m, u, adj, st); break;
 		default: return cudaErrorInvalidValue;
 		}
-	constexpr int NTG = 128;
-	if (m.Ng > 0) k_vec_gather<NTG><<<blocks_for(m.Ng, NTG), NTG, 0, s>>>(m.Ng, m.ginc_off, st, out);
+	launch_vec_gather(m.Ng, m.ginc_off, (long long)m.E * geom_nodes_of(m.et), st, out, s);
 	return cudaGetLastError();
 }
 
