@@ -38,7 +38,6 @@ struct pfg_context
 	double *d_values = nullptr;
 	unsigned int *d_contrib = nullptr;
 	unsigned short *d_blk_rel = nullptr;
-	unsigned short *d_self_rank = nullptr, *d_rev_rank = nullptr;
 	// Dirichlet reduction (pfg_set_dirichlet)
 	bool has_dirichlet = false;
 	std::vector<int> h_constrained;      // sorted unique constrained dofs
@@ -380,27 +379,6 @@ int build_pattern(pfg_context *c)
 		}
 	});
 
-	// the symmetric walk's ranks: B in its own list, and B in each neighbour's list
-	std::vector<unsigned short> self_rank(N), rev_rank((size_t)noff[N]);
-	parallel_ranges(N, [&](long long s0, long long s1, int) {
-		for (long long B = s0; B < s1; ++B)
-		{
-			const int *lo = nbr.data() + noff[B], *hi = nbr.data() + noff[B + 1];
-			self_rank[B] = (unsigned short)(std::lower_bound(lo, hi, (int)B) - lo);
-			for (long long k = noff[B]; k < noff[B + 1]; ++k)
-			{
-				const int A = nbr[k];
-				const int *la = nbr.data() + noff[A], *ha = nbr.data() + noff[A + 1];
-				rev_rank[k] = (unsigned short)(std::lower_bound(la, ha, (int)B) - la);
-			}
-		}
-	});
-	PFG_CUDA(c, cudaMalloc(&c->d_self_rank, sizeof(unsigned short) * std::max<size_t>(self_rank.size(), 1)));
-	PFG_CUDA(c, cudaMalloc(&c->d_rev_rank, sizeof(unsigned short) * std::max<size_t>(rev_rank.size(), 1)));
-	if (N) PFG_CUDA(c, cudaMemcpy(c->d_self_rank, self_rank.data(), sizeof(unsigned short) * N, cudaMemcpyHostToDevice));
-	if (!rev_rank.empty())
-		PFG_CUDA(c, cudaMemcpy(c->d_rev_rank, rev_rank.data(), sizeof(unsigned short) * rev_rank.size(),
-							   cudaMemcpyHostToDevice));
 	PFG_CUDA(c, cudaMalloc(&c->d_outer, sizeof(int) * (ndof + 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_inner, sizeof(int) * std::max<long long>(nnz, 1)));
 	PFG_CUDA(c, cudaMalloc(&c->d_values, sizeof(double) * std::max<long long>(nnz, 1)));
@@ -420,8 +398,6 @@ int build_pattern(pfg_context *c)
 	c->pat.inner = c->d_inner;
 	c->pat.contrib = c->d_contrib;
 	c->pat.blk_rel = c->d_blk_rel;
-	c->pat.self_rank = c->d_self_rank;
-	c->pat.rev_rank = c->d_rev_rank;
 	c->pat.values = c->d_values;
 	c->has_pattern = true;
 	return PFG_OK;
@@ -559,7 +535,7 @@ int build_dirichlet(pfg_context *c)
 
 void free_all(pfg_context *c)
 {
-	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_contrib, c->d_blk_rel, c->d_self_rank, c->d_rev_rank, c->d_eb_inc, c->d_g_eb_inc,
+	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_contrib, c->d_blk_rel, c->d_eb_inc, c->d_g_eb_inc,
 					c->d_inc_off, c->d_inc_eb, c->d_ginc_off, c->d_ginc_eb, c->d_vec_stage, c->d_hess_stage[0],
 					c->d_hess_stage[1], c->sc.partials, c->sc.ticket, c->sc.inverted, c->d_result, c->d_u, c->d_p, c->d_out};
 	for (void *p : ptrs)

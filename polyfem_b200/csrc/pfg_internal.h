@@ -68,11 +68,6 @@ struct DevPattern
 	const int *inner = nullptr;
 	const unsigned int *contrib = nullptr;
 	const unsigned short *blk_rel = nullptr;
-	// symmetric walk: rank of every node in its own column block, and for every
-	// node block (B, rank r) with neighbour A the rank of B in A's column block
-	// (indexed like blk_rel); NULL = every warp walks its whole column
-	const unsigned short *self_rank = nullptr;
-	const unsigned short *rev_rank = nullptr;
 	double *values = nullptr;
 	// Dirichlet-reduced output (BCLagrangianForm::project_hessian): when red_col_start
 	// is set the reduction writes only entries whose row and column are free, at

@@ -863,14 +863,7 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 	const unsigned *cl = pat.contrib + (size_t)s0 * N;
 	const unsigned short *br = pat.blk_rel + o0 / 9;
 	double *dst = pat.values + o0;
-	// With the symmetric plan the warp sums only the blocks of neighbours A >= B
-	// (ranks from B's own onwards) and also writes each off-diagonal block,
-	// transposed, into column block A at B's rank there (pat.rev_rank).  Every
-	// entry of H(B, A) = H(A, B)^T then gets the same contributions in the same
-	// order (elements holding both nodes, ascending) as A's own warp would sum:
-	// the values are bitwise those of the full walk, with half the block reads.
-	const int r_first = pat.self_rank ? (int)__ldg(pat.self_rank + B) : 0;
-	for (int it = 3 * r_first + lane; it < stride; it += 32)
+	for (int it = lane; it < stride; it += 32)
 	{
 		// (rank, column) items rank-major: the three items of the diagonal block,
 		// which has the longest contribution list, share one pass of the warp
@@ -911,31 +904,12 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 				a2 += double(y2);
 			}
 		}
-		// the partner column block (A, B) of the symmetric plan: A's three columns,
-		// row 3 rank_A(B) + c; none for the diagonal block
-		const bool mirror = pat.self_rank && r != r_first;
-		int oA = 0, strideA = 0, rA = 0, A = 0;
-		if (mirror)
-		{
-			A = __ldg(pat.inner + o0 + 3 * r) / 3;
-			oA = __ldg(pat.outer + 3 * A);
-			strideA = __ldg(pat.outer + 3 * A + 1) - oA;
-			rA = __ldg(pat.rev_rank + o0 / 9 + r);
-		}
 		if (pat.red_col_start == nullptr)
 		{
 			double *d = dst + c * stride + 3 * r;
 			d[0] = a0;
 			d[1] = a1;
 			d[2] = a2;
-			if (mirror)
-			{
-				// H(3B+c, 3A+j) = H(3A+j, 3B+c): column 3A+j, row 3 rA + c
-				double *dA = pat.values + oA + 3 * rA + c;
-				dA[0] = a0;
-				dA[strideA] = a1;
-				dA[2 * strideA] = a2;
-			}
 		}
 		else
 		{
@@ -948,20 +922,6 @@ __global__ void __launch_bounds__(WARPS * 32, 8)
 				if (r0 != 0xFFFF) pat.values[cs + r0] = a0;
 				if (r1 != 0xFFFF) pat.values[cs + r1] = a1;
 				if (r2 != 0xFFFF) pat.values[cs + r2] = a2;
-			}
-			if (mirror)
-			{
-				const unsigned short roA = __ldg(pat.red_row_off + oA / 3 + 3 * rA + c);
-				if (roA != 0xFFFF)
-				{
-					const double v[3] = {a0, a1, a2};
-#pragma unroll
-					for (int j = 0; j < 3; ++j)
-					{
-						const int csA = __ldg(pat.red_col_start + 3 * A + j);
-						if (csA >= 0) pat.values[csA + roA] = v[j];
-					}
-				}
 			}
 		}
 	}
