@@ -310,6 +310,19 @@ int pfg_mass_matrix(pfg_context *ctx, const double *rho, int mem, double *values
 int pfg_lump_matrix(pfg_context *ctx, const double *values, int mem, double *diag);
 
 /* ---------------------------------------------------------------------------
+ * Dense assembly: polyfem::utils::DenseMatrixCache (utils/MatrixCache.hpp:136-177,
+ * MatrixCache.cpp:326-403), whose mat() the assembler merges densely
+ * (assembler/Assembler.cpp:306-316) before taking its sparseView().
+ * dense[col * ndof + row] (column-major, ndof = 3 N, Eigen's default storage) =
+ * the value of (row, col) in `values` (nnz doubles in the Hessian pattern, e.g.
+ * pfg_hessian or pfg_mass_matrix output) and 0 outside the pattern.  values and
+ * dense in `mem`; PFG_ERR_UNSUPPORTED when ndof^2 > PFG_DENSE_MAX_ENTRIES.  A
+ * host-mode call allocates device staging for the values and the dense matrix
+ * for the duration of the call. */
+#define PFG_DENSE_MAX_ENTRIES (1LL << 29)
+int pfg_dense_matrix(pfg_context *ctx, const double *values, int mem, double *dense);
+
+/* ---------------------------------------------------------------------------
  * Linear solve on the device.  After every assembly the Newton step hands the
  * Hessian that NLProblem::hessian returns (solver/NLProblem.cpp:615-621) to its
  * linear solver through polysolve's linear::Solver (analyze_pattern, factorize,

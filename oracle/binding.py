@@ -249,6 +249,35 @@ class SparseMatrixCache:
             self.h = None
 
 
+class DenseMatrixCache:
+    """DenseMatrixCache restated (utils/MatrixCache.cpp:326-403): add_value sums into a
+    dense matrix (MatrixCache.cpp:371-374); get_matrix is its sparseView(), which keeps
+    the nonzero entries only (MatrixCache.cpp:378-381)."""
+
+    def __init__(self, rows: int, cols: int | None = None):
+        self.mat = np.zeros((rows, rows if cols is None else cols))
+
+    def add_value(self, e, i, j, v):
+        self.mat[i, j] += v
+
+    def get_matrix(self):
+        import scipy.sparse as sp
+        return sp.csc_matrix(self.mat)  # stores the nonzeros only, like Eigen's sparseView()
+
+
+def dense_hessian(orc, mesh, u):
+    """The global Hessian through DenseMatrixCache: every element matrix of the oracle
+    added entry by entry at its global dofs, elements in order (the serial order of
+    Assembler.cpp:306-316's merge of one thread's cache)."""
+    n = mesh.conn.shape[1]
+    cache = DenseMatrixCache(mesh.n_dofs)
+    for e in range(mesh.n_elements):
+        H = orc.element(e, u)[2]
+        dofs = (3 * mesh.conn[e][:, None] + np.arange(3)[None, :]).ravel()
+        cache.mat[np.ix_(dofs, dofs)] += H
+    return cache
+
+
 def free_dofs(ndof: int, constrained):
     """not_constraints_ / old_to_new_ of BCLagrangianForm (BCLagrangianForm.cpp:122-137)."""
     is_c = np.zeros(ndof, dtype=bool)

@@ -125,6 +125,7 @@ SIGNATURES = {
     "pfg_set_elasticity_tensor": (ctypes.c_int, [_vp, _vp]),
     "pfg_mass_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
     "pfg_lump_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
+    "pfg_dense_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
     "pfg_cg_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
 }

@@ -281,6 +281,23 @@ class NeoHookeanAssembler:
         check(lib().pfg_lump_matrix(self._h, ptrs[0], mem, optr), self._h, "pfg_lump_matrix")
         return out
 
+    def dense_matrix(self, values):
+        """DenseMatrixCache::mat() (utils/MatrixCache.hpp:136-177) of a matrix in the
+        Hessian pattern: the dense ndof x ndof array, zeros outside the pattern.
+        numpy in, numpy out (C-contiguous, element [row, col]); a CUDA tensor gives a
+        CUDA tensor."""
+        self._check_len(values, self.hessian_nnz(), "values")
+        mem, ptrs, keep = self._prepare(values)
+        out, optr = self._alloc(mem, self.n_dofs * self.n_dofs)
+        check(lib().pfg_dense_matrix(self._h, ptrs[0], mem, optr), self._h, "pfg_dense_matrix")
+        # the library writes column-major: the flat array is the transpose's rows
+        return out.reshape(self.n_dofs, self.n_dofs).T
+
+    def assemble_hessian_dense(self, u, precision="fp64", project_to_psd=False):
+        """assemble_hessian with a DenseMatrixCache: the Hessian as a dense array
+        (Assembler.cpp:306-316 merges the dense caches before its sparseView())."""
+        return self.dense_matrix(self.assemble_hessian_values(u, precision, project_to_psd=project_to_psd))
+
     def assemble_lumped_mass(self, rho=None):
         """The lumped mass matrix's diagonal, lump_matrix(mass), as BCLagrangianForm
         builds it (BCLagrangianForm.cpp:68) and State does for

@@ -1147,6 +1147,36 @@ int pfg_lump_matrix(pfg_context *c, const double *values, int mem, double *diag)
 	return PFG_OK;
 }
 
+int pfg_dense_matrix(pfg_context *c, const double *values, int mem, double *dense)
+{
+	if (!c || !check_mem(mem) || !values || !dense) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	DeviceGuard g(c->device);
+	int st;
+	if (!c->has_pattern && (st = build_pattern(c))) return st;
+	const long long nnz = c->pat.nnz;
+	const long long ndof = 3LL * c->m.N;
+	if (ndof * ndof > PFG_DENSE_MAX_ENTRIES)
+		return fail(c, PFG_ERR_UNSUPPORTED, "dense matrix larger than PFG_DENSE_MAX_ENTRIES entries");
+	if (mem == PFG_MEM_DEVICE)
+	{
+		PFG_CUDA(c, launch_csc_to_dense((int)ndof, c->d_outer, c->d_inner, values, dense, c->stream));
+		return PFG_OK;
+	}
+	// host mode: the values and the dense matrix are staged in device buffers of this call
+	double *dv = nullptr, *dd = nullptr;
+	cudaError_t e = cudaMalloc(&dv, sizeof(double) * std::max<long long>(nnz, 1));
+	if (e == cudaSuccess) e = cudaMalloc(&dd, sizeof(double) * std::max<long long>(ndof * ndof, 1));
+	if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(dv, values, sizeof(double) * nnz, cudaMemcpyHostToDevice, c->stream);
+	if (e == cudaSuccess) e = launch_csc_to_dense((int)ndof, c->d_outer, c->d_inner, dv, dd, c->stream);
+	if (e == cudaSuccess && ndof)
+		e = cudaMemcpyAsync(dense, dd, sizeof(double) * ndof * ndof, cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+	cudaFree(dv);
+	cudaFree(dd);
+	if (e != cudaSuccess) return cuda_fail(c, e, "pfg_dense_matrix");
+	return PFG_OK;
+}
+
 int pfg_cg_solve(pfg_context *c, int system, const double *values, const double *b, int mem, double tol, int max_iter,
 				 int guess, double *x, int *iters, double *rel_res)
 {

@@ -112,6 +112,10 @@ cudaError_t launch_mass(const DevMesh &m, const DevPattern &p, const double *rho
 // pattern (outer, inner), each summed in ascending column order
 cudaError_t launch_lump_rows(int n_nodes, const int *outer, const int *inner, const double *vals, double *diag,
 							 cudaStream_t s);
+// DenseMatrixCache: the values of the Hessian pattern into a dense column-major
+// ndof x ndof array (zeros outside the pattern)
+cudaError_t launch_csc_to_dense(int ndof, const int *outer, const int *inner, const double *vals, double *dense,
+								cudaStream_t s);
 // Dirichlet reduction helpers: dof maps of the free dofs (old_to_new[dof] = index
 // among the free dofs or -1, free[i] = dof of the i-th free dof)
 cudaError_t launch_gather_free(const double *full, const int *free, int n_free, double *out, cudaStream_t s);

@@ -2458,6 +2458,28 @@ cudaError_t launch_lump_rows(int n_nodes, const int *outer, const int *inner, co
 	return cudaGetLastError();
 }
 
+// DenseMatrixCache (utils/MatrixCache.hpp:136-177): the matrix in the Hessian pattern
+// as a dense column-major ndof x ndof array.  One warp per column; every entry of
+// the pattern is written once, the rest of the column is zero (cleared before).
+__global__ void k_csc_to_dense(int ndof, const int *__restrict__ outer, const int *__restrict__ inner,
+							   const double *__restrict__ vals, double *__restrict__ dense)
+{
+	const int col = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+	if (col >= ndof) return;
+	double *d = dense + (size_t)col * ndof;
+	for (int k = __ldg(outer + col) + lane; k < __ldg(outer + col + 1); k += 32) d[__ldg(inner + k)] = __ldg(vals + k);
+}
+
+cudaError_t launch_csc_to_dense(int ndof, const int *outer, const int *inner, const double *vals, double *dense,
+								cudaStream_t s)
+{
+	if (ndof <= 0) return cudaSuccess;
+	cudaError_t e = cudaMemsetAsync(dense, 0, sizeof(double) * (size_t)ndof * (size_t)ndof, s);
+	if (e != cudaSuccess) return e;
+	k_csc_to_dense<<<(int)(((size_t)ndof * 32 + 255) / 256), 256, 0, s>>>(ndof, outer, inner, vals, dense);
+	return cudaGetLastError();
+}
+
 cudaError_t launch_gather_free(const double *full, const int *free, int n_free, double *out, cudaStream_t s)
 {
 	if (n_free > 0) k_gather_free<<<(n_free + 255) / 256, 256, 0, s>>>(full, free, n_free, out);

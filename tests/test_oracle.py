@@ -376,3 +376,18 @@ def test_project_hessian_known_answer():
     assert list(o) == [0, 2, 4, 7] and list(i) == [0, 2, 1, 2, 0, 1, 2]
     assert np.array_equal(project_gradient(np.arange(4.0), [1]), [0.0, 2.0, 3.0])
     assert np.array_equal(reduced_to_full([10.0, 20.0, 30.0], [-1.0, -2.0, -3.0, -4.0], [1]), [10.0, -2.0, 20.0, 30.0])
+
+
+def test_dense_matrix_cache_restatement():
+    """DenseMatrixCache (MatrixCache.cpp:326-403): add_value sums duplicates, and
+    get_matrix is the sparseView that drops exact zeros."""
+    from oracle.binding import DenseMatrixCache
+    c = DenseMatrixCache(3)
+    c.add_value(0, 0, 0, 1.5)
+    c.add_value(1, 0, 0, 2.0)
+    c.add_value(0, 1, 2, 4.0)
+    c.add_value(1, 1, 2, -4.0)  # cancels to an exact zero: not stored
+    c.add_value(0, 2, 1, 7.0)
+    assert c.mat[0, 0] == 3.5 and c.mat[1, 2] == 0.0
+    m = c.get_matrix()
+    assert m.nnz == 2 and m[0, 0] == 3.5 and m[2, 1] == 7.0
