@@ -204,7 +204,15 @@ int pfg_version(void);
  *                                 (pfg_set_elasticity_tensor), eps the small strain;
  *   PFG_MAT_SAINT_VENANT_TENSOR : SaintVenantElasticity with that anisotropic tensor
  *                                 (SaintVenantElasticity.cpp:209-267), psi = 1/2 S:E,
- *                                 S = C E in Voigt form, E = (F^T F - I)/2.
+ *                                 S = C E in Voigt form, E = (F^T F - I)/2;
+ *   PFG_MAT_UNCONSTRAINED_OGDEN : UnconstrainedOgdenElasticity (OgdenElasticity.tpp:8-57),
+ *                                 psi = sum_t 2 mu_t/alpha_t^2 (sum_i s_i^alpha_t - 3)
+ *                                       + sum_t (J - 1)^(2(t+1)) / D_t,
+ *                                 s_i = J^(-1/3) x the principal stretches of F;
+ *                                 parameters (alpha_0.., mu_0.., D_0..), 1 or 2 terms;
+ *   PFG_MAT_INCOMPRESSIBLE_OGDEN: IncompressibleOgdenElasticity (OgdenElasticity.tpp:
+ *                                 59-94), psi = sum_t c_t/m_t^2 (sum_i s_i^m_t - 3)
+ *                                 + k/2 ln^2 J; parameters (c_0.., m_0.., k), 1 to 3 terms.
  * Energy, gradient and Hessian (with project_psd and the Dirichlet reduction) then
  * follow the chosen material in PFG_FP64 (other precisions return
  * PFG_ERR_UNSUPPORTED).  The adjoint terms follow the reference's assemblers:
@@ -227,7 +235,9 @@ enum pfg_material
 	PFG_MAT_MOONEY_RIVLIN_3PARAM = 5,
 	PFG_MAT_VOLUME_PENALTY = 6,
 	PFG_MAT_HOOKE = 7,
-	PFG_MAT_SAINT_VENANT_TENSOR = 8
+	PFG_MAT_SAINT_VENANT_TENSOR = 8,
+	PFG_MAT_UNCONSTRAINED_OGDEN = 9,
+	PFG_MAT_INCOMPRESSIBLE_OGDEN = 10
 };
 int pfg_set_material(pfg_context *ctx, int material);
 
@@ -241,12 +251,15 @@ int pfg_set_material(pfg_context *ctx, int material);
 int pfg_set_elasticity_tensor(pfg_context *ctx, const double *c21);
 
 /* Per-element parameters of PFG_MAT_MOONEY_RIVLIN (n_params 3: c1, c2, k),
- * PFG_MAT_MOONEY_RIVLIN_3PARAM (4: c1, c2, c3, d1) and PFG_MAT_VOLUME_PENALTY
- * (1: k): the reference's GenericMatParam values (MatParams.cpp), one per element,
- * parameter-major: params[k * n_elements + e] is parameter k of element e.
- * 1 <= n_params <= 4.  The energy, gradient and Hessian calls of these materials
- * return PFG_ERR_STATE until parameters of the material's count are set; the
- * parameters stay with the context when the material changes. */
+ * PFG_MAT_MOONEY_RIVLIN_3PARAM (4: c1, c2, c3, d1), PFG_MAT_VOLUME_PENALTY
+ * (1: k), PFG_MAT_UNCONSTRAINED_OGDEN (3 K: alpha_0..alpha_K-1, mu_0.., D_0.., with
+ * K = 1 or 2 terms, as GenericMatParams alphas, mus, Ds, OgdenElasticity.cpp:12-20)
+ * and PFG_MAT_INCOMPRESSIBLE_OGDEN (2 K + 1: c_0.., m_0.., k, K = 1 to 3,
+ * OgdenElasticity.cpp:53-60): the reference's GenericMatParam values (MatParams.cpp),
+ * one per element, parameter-major: params[k * n_elements + e] is parameter k of
+ * element e.  1 <= n_params <= 8.  The energy, gradient and Hessian calls of these
+ * materials return PFG_ERR_STATE until parameters of a count the material takes
+ * are set; the parameters stay with the context when the material changes. */
 int pfg_set_material_params(pfg_context *ctx, const double *params, int n_params, int mem);
 
 /* ---------------------------------------------------------------------------

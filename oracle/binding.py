@@ -90,7 +90,9 @@ class Oracle:
 
     MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2, "LinearElasticity": 3,
                  "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6, "HookeLinearElasticity": 7,
-                 "SaintVenantTensor": 8}
+                 "SaintVenantTensor": 8, "UnconstrainedOgden": 9, "IncompressibleOgden": 10}
+    # lists of one value per term (alphas, mus, Ds; c, m), then IncompressibleOgden's k
+    OGDEN_PARAMS = {"UnconstrainedOgden": ("alphas", "mus", "Ds"), "IncompressibleOgden": ("c", "m", "k")}
     MATERIAL_PARAMS = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
                        "VolumePenalty": ("k",)}
 
@@ -119,7 +121,15 @@ class Oracle:
                 raise ValueError("the elasticity tensor takes 21 entries")
             L.orc_set_elasticity_tensor(self.h, _dp(self._hooke))
             params = None
-        names = self.MATERIAL_PARAMS.get(material, ())
+        if material in self.OGDEN_PARAMS:
+            keys = self.OGDEN_PARAMS[material]
+            if set(params or {}) != set(keys):
+                raise ValueError(f"{material} takes the parameters {list(keys)}")
+            flat = [v for k in keys for v in (params[k] if isinstance(params[k], (list, tuple)) else [params[k]])]
+            params = {f"p{i}": v for i, v in enumerate(flat)}
+            names = tuple(params)
+        else:
+            names = self.MATERIAL_PARAMS.get(material, ())
         if set(params or {}) != set(names):
             raise ValueError(f"{material} takes the parameters {list(names)}")
         if names:

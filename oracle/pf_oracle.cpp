@@ -499,10 +499,13 @@ enum
 	MAT_MOONEY_RIVLIN_3PARAM = 5,
 	MAT_VOLUME_PENALTY = 6,
 	MAT_HOOKE = 7,
-	MAT_SAINT_VENANT_TENSOR = 8
+	MAT_SAINT_VENANT_TENSOR = 8,
+	MAT_UNCONSTRAINED_OGDEN = 9,
+	MAT_INCOMPRESSIBLE_OGDEN = 10
 };
 constexpr int PRM_MAX = 21; // material parameters of an element: 21 tensor entries for MAT_HOOKE and
                             // MAT_SAINT_VENANT_TENSOR
+constexpr int PRM_COUNT = PRM_MAX - 1; // the Ogden formulations: prm[PRM_COUNT] = number of values set
 
 // value, gradient and Hessian with respect to the 9 entries F(r, c) (index 3r + c)
 struct D2
@@ -568,6 +571,22 @@ static D2 operator/(const D2 &a, const D2 &b) { return a * dpow(b, -1.0); }
 static double dpow(double a, double p) { return std::pow(a, p); }
 static D2 dlog(const D2 &a) { return chain(a, std::log(a.v), 1.0 / a.v, -1.0 / (a.v * a.v)); }
 static double dlog(double a) { return std::log(a); }
+static D2 dsqrt(const D2 &a)
+{
+	const double f = std::sqrt(a.v);
+	return chain(a, f, 0.5 / f, -0.25 / (f * a.v));
+}
+static double dsqrt(double a) { return std::sqrt(a); }
+static D2 dacos(const D2 &a)
+{
+	const double d = 1.0 - a.v * a.v;
+	return chain(a, std::acos(a.v), -1.0 / std::sqrt(d), -a.v / (d * std::sqrt(d)));
+}
+static double dacos(double a) { return std::acos(a); }
+static D2 dcos(const D2 &a) { return chain(a, std::cos(a.v), -std::sin(a.v), -std::cos(a.v)); }
+static double dcos(double a) { return std::cos(a); }
+static double dval(const D2 &a) { return a.v; }
+static double dval(double a) { return a; }
 
 template <class S>
 static S det3s(const S (&F)[3][3])
@@ -743,6 +762,99 @@ static S psi_hooke(const S (&F)[3][3], const double *c21)
 	return 0.5 * tr;
 }
 
+// utils::autogen::eigs_3d (autogen/auto_eigs.hpp:33-76): the eigenvalues of a symmetric
+// 3 x 3 matrix by the trigonometric solution of its characteristic cubic, from the
+// entries m(0,0), m(1,1), m(2,2), m(0,1), m(0,2), m(1,2); all three the trace / 3 when
+// the deviator vanishes (below 1e-10), the arc cosine's argument clamped to [-1, 1].
+template <class S>
+static void eigs_3d(const S (&m)[3][3], S (&res)[3])
+{
+	const S t01 = m[0][0] + m[1][1];
+	const S tr = t01 + m[2][2];
+	const S off = m[0][1] * m[0][1] + m[0][2] * m[0][2] + m[1][2] * m[1][2];
+	const S d02 = m[0][0] - m[2][2], d12 = m[1][1] - m[2][2], d01 = m[0][0] - m[1][1];
+	// 9 p: three times the sum of squared off-diagonal entries plus half the squared diagonal differences
+	const S p9 = 3.0 * off + 0.5 * (d02 * d02) + 0.5 * (d12 * d12) + 0.5 * (d01 * d01);
+	const S sp9 = dsqrt(p9);
+	if (2.0 * dval(sp9) < 1e-10)
+	{
+		res[0] = res[1] = res[2] = (1.0 / 3.0) * tr;
+		return;
+	}
+	// 27 det(m - tr/3 I) / 2 over (9 p)^(3/2): the cosine of three times the angle
+	const S num = -1.5 * (t01 * (m[0][0] + m[2][2]) * (m[1][1] + m[2][2])) + 4.5 * (tr * off) -
+				  13.5 * (m[0][1] * m[0][1] * m[2][2]) - 13.5 * (m[0][2] * m[0][2] * m[1][1]) -
+				  13.5 * (m[1][2] * m[1][2] * m[0][0]) + m[0][0] * m[0][0] * m[0][0] + 9.0 * (m[0][0] * m[1][1] * m[2][2]) +
+				  27.0 * (m[0][1] * m[0][2] * m[1][2]) + m[1][1] * m[1][1] * m[1][1] + m[2][2] * m[2][2] * m[2][2];
+	const S c3 = num / dpow(p9, 1.5);
+	const S ang = (1.0 / 3.0) * (dval(c3) >= 1.0 ? S(0.0) : dval(c3) <= -1.0 ? S(M_PI) : dacos(c3));
+	const S r = (2.0 / 3.0) * sp9, mean = (1.0 / 3.0) * tr;
+	res[0] = r * dcos(ang) + mean;
+	res[1] = r * dcos(ang + S(2.0 * M_PI / 3.0)) + mean;
+	res[2] = r * dcos(ang - S(2.0 * M_PI / 3.0)) + mean;
+}
+
+// UnconstrainedOgden (OgdenElasticity.tpp:8-57): the principal stretches sqrt(eig(F^T F)),
+// scaled by J^(-1/3), K terms (alpha_t, mu_t, D_t) in prm = alphas, mus, Ds:
+//   psi = sum_t 2 mu_t / alpha_t^2 (sum_i s_i^alpha_t - 3) + sum_t (J - 1)^(2(t+1)) / D_t
+template <class S>
+static S psi_unconstrained_ogden(const S (&F)[3][3], const double *prm, int K)
+{
+	S C[3][3], ev[3];
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c)
+		{
+			C[r][c] = S(0.0);
+			for (int k = 0; k < 3; ++k) C[r][c] = C[r][c] + F[k][r] * F[k][c];
+		}
+	eigs_3d(C, ev);
+	for (int i = 0; i < 3; ++i) ev[i] = dsqrt(ev[i]);
+	const S J = det3s(F);
+	const S jd = dpow(J, -1.0 / 3.0);
+	for (int i = 0; i < 3; ++i) ev[i] = ev[i] * jd;
+	S val = S(0.0);
+	for (int t = 0; t < K; ++t)
+	{
+		const double alpha = prm[t], mu = prm[K + t];
+		S tmp = S(-3.0);
+		for (int i = 0; i < 3; ++i) tmp = tmp + dpow(ev[i], alpha);
+		val = val + (2.0 * mu / (alpha * alpha)) * tmp;
+	}
+	for (int t = 0; t < K; ++t) val = val + (1.0 / prm[2 * K + t]) * dpow(J - S(1.0), 2.0 * (t + 1));
+	return val;
+}
+
+// IncompressibleOgden (OgdenElasticity.tpp:59-94): F~ = F / J^(1/3), the stretches
+// sqrt(eig(F~ F~^T)), K terms (c_t, m_t) and k in prm = cs, ms, k:
+//   psi = sum_t c_t / m_t^2 (sum_j s_j^m_t - 3) + k/2 ln^2 J
+template <class S>
+static S psi_incompressible_ogden(const S (&F)[3][3], const double *prm, int K)
+{
+	const S J = det3s(F);
+	const S lj = dlog(J);
+	const S s = dpow(J, 1.0 / 3.0);
+	S Ft[3][3], Ct[3][3], ev[3];
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c) Ft[r][c] = F[r][c] / s;
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c)
+		{
+			Ct[r][c] = S(0.0);
+			for (int k = 0; k < 3; ++k) Ct[r][c] = Ct[r][c] + Ft[r][k] * Ft[c][k];
+		}
+	eigs_3d(Ct, ev);
+	for (int i = 0; i < 3; ++i) ev[i] = dsqrt(ev[i]);
+	S val = S(0.0);
+	for (int t = 0; t < K; ++t)
+	{
+		const double c = prm[t], m = prm[K + t];
+		S tmp = S(-3.0);
+		for (int j = 0; j < 3; ++j) tmp = tmp + dpow(ev[j], m);
+		val = val + (c / (m * m)) * tmp;
+	}
+	return val + (0.5 * prm[2 * K]) * (lj * lj);
+}
+
 template <class S>
 static S psi_material(int mat, const S (&F)[3][3], const double *prm)
 {
@@ -761,6 +873,8 @@ static S psi_material(int mat, const S (&F)[3][3], const double *prm)
 	case MAT_LINEAR_ELASTICITY: return psi_linear_elasticity(F, prm[0], prm[1]);
 	case MAT_MOONEY_RIVLIN: return psi_mooney_rivlin(F, prm[0], prm[1], prm[2]);
 	case MAT_MOONEY_RIVLIN_3PARAM: return psi_mooney_rivlin_3param(F, prm[0], prm[1], prm[2], prm[3]);
+	case MAT_UNCONSTRAINED_OGDEN: return psi_unconstrained_ogden(F, prm, (int)prm[PRM_COUNT] / 3);
+	case MAT_INCOMPRESSIBLE_OGDEN: return psi_incompressible_ogden(F, prm, ((int)prm[PRM_COUNT] - 1) / 2);
 	default: return psi_volume_penalty(F, prm[0]);
 	}
 }
@@ -1089,7 +1203,10 @@ struct Context
 		if (material == MAT_HOOKE || material == MAT_SAINT_VENANT_TENSOR)
 			for (int k = 0; k < PRM_MAX; ++k) prm[k] = hooke[k];
 		else if (material >= MAT_MOONEY_RIVLIN)
-			for (int k = 0; k < 4; ++k) prm[k] = k < n_mparams ? mparams[(size_t)k * E + e] : 0.0;
+		{
+			for (int k = 0; k < 8; ++k) prm[k] = k < n_mparams ? mparams[(size_t)k * E + e] : 0.0;
+			prm[PRM_COUNT] = n_mparams;
+		}
 	}
 	CSC last;                  // last assembled Hessian
 	CSC mass;                  // last assembled mass matrix
@@ -1727,7 +1844,7 @@ extern "C"
 	void orc_set_project_psd(void *h, int on) { static_cast<Context *>(h)->project_psd = on != 0; }
 	// later calls use another material of the GenericElastic family (MAT_*); 0 = NeoHookean
 	void orc_set_material(void *h, int mat) { static_cast<Context *>(h)->material = mat; }
-	// per-element GenericMatParam values, parameter-major (params[k * E + e]), 1..4 of them
+	// per-element GenericMatParam values, parameter-major (params[k * E + e]), 1..8 of them
 	void orc_set_material_params(void *h, const double *params, int n_params)
 	{
 		Context &c = *static_cast<Context *>(h);

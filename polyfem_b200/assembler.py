@@ -313,11 +313,16 @@ class NeoHookeanAssembler:
 
     # -- material (AssemblerUtils::make_assembler's formulation name) ------------------
     MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2, "LinearElasticity": 3,
-                 "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6, "HookeLinearElasticity": 7}
+                 "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6, "HookeLinearElasticity": 7,
+                 "UnconstrainedOgden": 9, "IncompressibleOgden": 10}
     SAINT_VENANT_TENSOR = 8  # "SaintVenant" with an elasticity_tensor
     # the GenericMatParam names of the parameterised formulations, in pfg_set_material_params order
     MATERIAL_PARAMS = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
                        "VolumePenalty": ("k",)}
+    # the Ogden formulations' GenericMatParams (OgdenElasticity.cpp:7-10, 48-51): one value
+    # per term for each list; IncompressibleOgden's k is one GenericMatParam
+    OGDEN_PARAMS = {"UnconstrainedOgden": ("alphas", "mus", "Ds"), "IncompressibleOgden": ("c", "m", "k")}
+    OGDEN_MAX_TERMS = {"UnconstrainedOgden": 2, "IncompressibleOgden": 3}
 
     def set_material(self, formulation: str, **params):
         """Switch the elastic formulation (AssemblerUtils::make_assembler's name).
@@ -326,7 +331,9 @@ class NeoHookeanAssembler:
         "LinearElasticity" use the per-element lambda/mu.  "MooneyRivlin" (c1, c2, k),
         "MooneyRivlin3Param" (c1, c2, c3, d1) and "VolumePenalty" (k) take their
         parameters as keywords, each a scalar or one value per element (host arrays
-        or CUDA tensors).  "HookeLinearElasticity" takes ``elasticity_tensor``: the 21
+        or CUDA tensors).  "UnconstrainedOgden" takes alphas, mus, Ds (lists of one
+        entry per term, 1 or 2 terms) and "IncompressibleOgden" c, m (1 to 3 terms)
+        and k, each entry again a scalar or one value per element.  "HookeLinearElasticity" takes ``elasticity_tensor``: the 21
         entries C(i, j), i <= j, of its 6 x 6 Voigt tensor, row by row (the reference's
         material key; ``isotropic_elasticity_tensor`` gives the lambda/mu one); so does
         "SaintVenant" given ``elasticity_tensor``, which is then anisotropic.  Every
@@ -344,6 +351,11 @@ class NeoHookeanAssembler:
             params = {}
             if formulation == "SaintVenant":
                 mat_id = self.SAINT_VENANT_TENSOR
+        if formulation in self.OGDEN_PARAMS:
+            self.set_material_params(*self._ogden_params(formulation, params))
+            check(lib().pfg_set_material(self._h, mat_id), self._h, "pfg_set_material")
+            self.material = formulation
+            return
         names = self.MATERIAL_PARAMS.get(formulation, ())
         if set(params) != set(names):
             raise ValueError(f"{formulation} takes the parameters {list(names)}, got {sorted(params)}")
@@ -351,6 +363,25 @@ class NeoHookeanAssembler:
             self.set_material_params(*(params[n] for n in names))
         check(lib().pfg_set_material(self._h, mat_id), self._h, "pfg_set_material")
         self.material = formulation
+
+    def _ogden_params(self, formulation, params):
+        """The flat pfg_set_material_params list of an Ogden formulation: alphas, mus, Ds
+        (three lists of K terms), or c, m (two lists of K terms) and k."""
+        keys = self.OGDEN_PARAMS[formulation]
+        if set(params) != set(keys):
+            raise ValueError(f"{formulation} takes the parameters {list(keys)}, got {sorted(params)}")
+        lists = [list(params[k]) if isinstance(params[k], (list, tuple)) else [params[k]] for k in keys]
+        if formulation == "IncompressibleOgden":
+            if len(lists[2]) != 1:
+                raise ValueError("IncompressibleOgden takes one k")
+            terms = lists[:2]
+        else:
+            terms = lists
+        K = len(terms[0])
+        if any(len(t) != K for t in terms) or not 1 <= K <= self.OGDEN_MAX_TERMS[formulation]:
+            raise ValueError(f"{formulation} takes 1 to {self.OGDEN_MAX_TERMS[formulation]} terms, "
+                             f"the same number in {list(keys[:len(terms)])}")
+        return [v for lst in lists for v in lst]
 
     def set_elasticity_tensor(self, c21):
         """ElasticityTensor::set_from_entries with 21 entries (MatParams.cpp:180-205):
@@ -374,8 +405,8 @@ class NeoHookeanAssembler:
         """Per-element parameters of the current or next parameterised formulation, in
         MATERIAL_PARAMS order (pfg_set_material_params)."""
         E = self.n_elements
-        if not 1 <= len(params) <= 4:
-            raise ValueError("1 to 4 parameters")
+        if not 1 <= len(params) <= 8:
+            raise ValueError("1 to 8 parameters")
         if any(_is_device(p) for p in params):
             import torch
             cols = [p if _is_device(p) else torch.tensor(p, dtype=torch.float64) for p in params]

@@ -72,7 +72,7 @@ struct pfg_context
 	// lumped diagonal for host-mode pfg_lump_matrix calls (3N doubles)
 	double *d_lump = nullptr;
 	// parameters of the automatically differentiated materials (pfg_set_material_params):
-	// one zero-padded double4 per element; n_mpar = the count last set (0: none)
+	// eight zero-padded doubles (two double4) per element; n_mpar = the count last set (0: none)
 	double4 *d_mpar = nullptr;
 	int n_mpar = 0;
 	// elasticity tensor of HookeLinearElasticity and the anisotropic SaintVenant
@@ -147,15 +147,28 @@ void parallel_ranges(long long n, F &&f)
 }
 
 int check_mem(int mem) { return mem == PFG_MEM_HOST || mem == PFG_MEM_DEVICE; }
-// number of pfg_set_material_params parameters a material takes (0: none, or Lame)
-int material_param_count(int mat)
+// Whether a material takes pfg_set_material_params parameters, and whether n of them
+// fit it; for the Ogden formulations also the number of terms n gives.
+bool material_takes_params(int mat)
 {
+	return mat == PFG_MAT_MOONEY_RIVLIN || mat == PFG_MAT_MOONEY_RIVLIN_3PARAM || mat == PFG_MAT_VOLUME_PENALTY ||
+		   mat == PFG_MAT_UNCONSTRAINED_OGDEN || mat == PFG_MAT_INCOMPRESSIBLE_OGDEN;
+}
+bool material_params_fit(int mat, int n, int *terms)
+{
+	*terms = 0;
 	switch (mat)
 	{
-	case PFG_MAT_MOONEY_RIVLIN: return 3;
-	case PFG_MAT_MOONEY_RIVLIN_3PARAM: return 4;
-	case PFG_MAT_VOLUME_PENALTY: return 1;
-	default: return 0;
+	case PFG_MAT_MOONEY_RIVLIN: return n == 3;
+	case PFG_MAT_MOONEY_RIVLIN_3PARAM: return n == 4;
+	case PFG_MAT_VOLUME_PENALTY: return n == 1;
+	case PFG_MAT_UNCONSTRAINED_OGDEN: // alphas, mus, Ds: three per term
+		*terms = n / 3;
+		return n == 3 || n == 6;
+	case PFG_MAT_INCOMPRESSIBLE_OGDEN: // cs, ms: two per term, then k
+		*terms = (n - 1) / 2;
+		return n == 3 || n == 5 || n == 7;
+	default: return true;
 	}
 }
 // The other materials (pfg_set_material) are assembled in FP64 only, and the
@@ -164,9 +177,10 @@ int check_material_prec(pfg_context *c, int prec)
 {
 	if (c->m.mat != PFG_MAT_NEOHOOKEAN && prec != PFG_FP64)
 		return fail(c, PFG_ERR_UNSUPPORTED, "only PFG_FP64 is implemented for materials other than NeoHookean");
-	const int np = material_param_count(c->m.mat);
-	if (np && c->m.E && c->n_mpar != np)
+	int terms = 0;
+	if (material_takes_params(c->m.mat) && c->m.E && !(c->n_mpar > 0 && material_params_fit(c->m.mat, c->n_mpar, &terms)))
 		return fail(c, PFG_ERR_STATE, "the material's parameters are not set (pfg_set_material_params)");
+	c->m.mterms = terms;
 	if ((c->m.mat == PFG_MAT_HOOKE || c->m.mat == PFG_MAT_SAINT_VENANT_TENSOR) && !c->d_hooke)
 		return fail(c, PFG_ERR_STATE, "the elasticity tensor is not set (pfg_set_elasticity_tensor)");
 	return PFG_OK;
@@ -727,7 +741,7 @@ int pfg_set_stream(pfg_context *c, void *stream)
 
 int pfg_set_material(pfg_context *c, int material)
 {
-	if (!c || material < PFG_MAT_NEOHOOKEAN || material > PFG_MAT_SAINT_VENANT_TENSOR)
+	if (!c || material < PFG_MAT_NEOHOOKEAN || material > PFG_MAT_INCOMPRESSIBLE_OGDEN)
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
 	c->m.mat = material;
 	return PFG_OK;
@@ -751,34 +765,33 @@ int pfg_set_elasticity_tensor(pfg_context *c, const double *c21)
 
 int pfg_set_material_params(pfg_context *c, const double *params, int n_params, int mem)
 {
-	if (!c || !check_mem(mem) || n_params < 1 || n_params > 4) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (!c || !check_mem(mem) || n_params < 1 || n_params > 8) return fail(c, PFG_ERR_INVALID, "bad arguments");
 	if (c->m.E && !params) return fail(c, PFG_ERR_INVALID, "params NULL");
 	DeviceGuard g(c->device);
 	const size_t E = c->m.E;
+	constexpr size_t PER = 8; // doubles per element on the device (two double4)
 	if (E)
 	{
 		if (!c->d_mpar)
 		{
-			PFG_CUDA(c, cudaMalloc(&c->d_mpar, sizeof(double4) * E));
+			PFG_CUDA(c, cudaMalloc(&c->d_mpar, sizeof(double) * PER * E));
 			c->m.mpar = c->d_mpar;
 		}
 		if (mem == PFG_MEM_HOST)
 		{
-			std::vector<double4> pv(E, make_double4(0.0, 0.0, 0.0, 0.0));
+			std::vector<double> pv(PER * E, 0.0);
 			for (size_t e = 0; e < E; ++e)
-			{
-				double *d = &pv[e].x;
-				for (int k = 0; k < n_params; ++k) d[k] = params[(size_t)k * E + e];
-			}
-			PFG_CUDA(c, cudaMemcpyAsync(c->d_mpar, pv.data(), sizeof(double4) * E, cudaMemcpyHostToDevice, c->stream));
+				for (int k = 0; k < n_params; ++k) pv[PER * e + k] = params[(size_t)k * E + e];
+			PFG_CUDA(c, cudaMemcpyAsync(c->d_mpar, pv.data(), sizeof(double) * PER * E, cudaMemcpyHostToDevice, c->stream));
 			PFG_CUDA(c, cudaStreamSynchronize(c->stream));
 		}
 		else
 		{
-			PFG_CUDA(c, cudaMemsetAsync(c->d_mpar, 0, sizeof(double4) * E, c->stream));
+			PFG_CUDA(c, cudaMemsetAsync(c->d_mpar, 0, sizeof(double) * PER * E, c->stream));
 			for (int k = 0; k < n_params; ++k)
-				PFG_CUDA(c, cudaMemcpy2DAsync((char *)c->d_mpar + k * sizeof(double), sizeof(double4), params + (size_t)k * E,
-											  sizeof(double), sizeof(double), E, cudaMemcpyDeviceToDevice, c->stream));
+				PFG_CUDA(c, cudaMemcpy2DAsync((char *)c->d_mpar + k * sizeof(double), sizeof(double) * PER,
+											  params + (size_t)k * E, sizeof(double), sizeof(double), E,
+											  cudaMemcpyDeviceToDevice, c->stream));
 		}
 	}
 	c->n_mpar = n_params;

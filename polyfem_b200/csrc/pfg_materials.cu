@@ -50,6 +50,11 @@
 //                                          (HookeLinearElasticity.cpp:372-421)
 //   8 SaintVenant         (one tensor)     psi = 1/2 S:E, S = T E in Voigt form, E the Green strain
 //                                          (SaintVenantElasticity.cpp:209-267)
+//   9 UnconstrainedOgden  (alphas, mus, Ds; 1-2 terms)   psi of the principal stretches
+//  10 IncompressibleOgden (cs, ms, k; 1-3 terms)          (OgdenElasticity.tpp:8-94)
+// The Ogden densities are functions of the invariants too: the stretches are the
+// square roots of the eigenvalues of F^T F, which the characteristic cubic gives from
+// (I1, I2, J^2) (cauchy_green_eigs).
 // with I1~ = J^-2/3 I1 and I2~ = J^-4/3 I2 (the invariants of F~ F~^T, F~ = J^-1/3 F).
 #include "pfg_device.cuh"
 
@@ -60,13 +65,27 @@ namespace pfg
 {
 
 constexpr int MAT_LINEAR_ELASTICITY = 3, MAT_MOONEY_RIVLIN = 4, MAT_MOONEY_RIVLIN_3PARAM = 5, MAT_VOLUME_PENALTY = 6,
-			  MAT_HOOKE = 7, MAT_SAINT_VENANT_TENSOR = 8;
+			  MAT_HOOKE = 7, MAT_SAINT_VENANT_TENSOR = 8, MAT_UNCONSTRAINED_OGDEN = 9, MAT_INCOMPRESSIBLE_OGDEN = 10;
+// An element's material parameters: up to eight values (pfg_set_material_params)
+// and, for the Ogden formulations, the number of terms.
+struct MatP
+{
+	double x, y, z, w, x2, y2, z2, w2;
+	int nt;
+};
 // the quadratic densities: constant tangent, no invariants
 template <int MAT>
 __host__ __device__ constexpr bool quadratic_mat() { return MAT == MAT_LINEAR_ELASTICITY || MAT == MAT_HOOKE; }
+// the densities of the principal stretches (Ogden), differentiated by dual and
+// hyper-dual numbers over the nine entries of F as the reference differentiates them
+template <int MAT>
+__host__ __device__ constexpr bool entry_mat() { return MAT == MAT_UNCONSTRAINED_OGDEN || MAT == MAT_INCOMPRESSIBLE_OGDEN; }
 // the densities of (I1, I2, J), differentiated by hyper-dual numbers
 template <int MAT>
-__host__ __device__ constexpr bool invariant_mat() { return !quadratic_mat<MAT>() && MAT != MAT_SAINT_VENANT_TENSOR; }
+__host__ __device__ constexpr bool invariant_mat()
+{
+	return !quadratic_mat<MAT>() && MAT != MAT_SAINT_VENANT_TENSOR && !entry_mat<MAT>();
+}
 // Voigt index of F(r, c) in HookeLinearElasticity's strain (e00, e11, e22, 2e12, 2e02, 2e01)
 __host__ __device__ constexpr int voigt(int r, int c) { return r == c ? r : 6 - r - c; }
 // IsochoricNeoHookean (hand-derived tangent in pfg_kernels.cu) is also an invariant
@@ -127,12 +146,180 @@ __device__ __forceinline__ S ad_pow(S x, double p)
 
 template <class S>
 __device__ __forceinline__ S sq(S x) { return x * x; }
+__device__ __forceinline__ double ad_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ double ad_recip(double x) { return 1.0 / x; }
+__device__ __forceinline__ double ad_acos(double x) { return acos(x); }
+__device__ __forceinline__ double ad_cos(double x) { return cos(x); }
+// sqrt: f' = 1/(2f), f'' = -f'/(2x)
+template <class S>
+__device__ __forceinline__ S ad_sqrt(S x)
+{
+	const double f = sqrt(x.v), f1 = 0.5 / f;
+	return chain(x, f, f1, -0.5 * f1 / x.v);
+}
+template <class S>
+__device__ __forceinline__ S ad_recip(S x)
+{
+	const double r = 1.0 / x.v;
+	return chain(x, r, -r * r, 2.0 * r * r * r);
+}
+// acos: f' = -(1 - x^2)^(-1/2), f'' = -x (1 - x^2)^(-3/2)
+template <class S>
+__device__ __forceinline__ S ad_acos(S x)
+{
+	const double d = 1.0 - x.v * x.v, rs = 1.0 / sqrt(d);
+	return chain(x, acos(x.v), -rs, -x.v * rs / d);
+}
+template <class S>
+__device__ __forceinline__ S ad_cos(S x)
+{
+	const double c = cos(x.v);
+	return chain(x, c, -sin(x.v), -c);
+}
+__device__ __forceinline__ double ad_val(double x) { return x; }
+__device__ __forceinline__ double ad_val(Dual1 x) { return x.v; }
+__device__ __forceinline__ double ad_val(HDual x) { return x.v; }
+template <class S>
+__device__ __forceinline__ S ad_const(double c);
+template <>
+__device__ __forceinline__ double ad_const<double>(double c) { return c; }
+template <>
+__device__ __forceinline__ Dual1 ad_const<Dual1>(double c) { return {c, 0.0}; }
+template <>
+__device__ __forceinline__ HDual ad_const<HDual>(double c) { return {c, 0.0, 0.0, 0.0}; }
+
+
+// The Ogden sums of K terms over the three stretches st; pv holds alphas, mus, Ds
+// (unconstrained) or cs, ms, k (incompressible), K values per group.
+template <int K, bool INC, class S>
+__device__ __forceinline__ S ogden_terms(const S (&st)[3], S J, const double (&pv)[8])
+{
+	S val = ad_const<S>(0.0);
+#pragma unroll
+	for (int t = 0; t < K; ++t)
+	{
+		const double ex = INC ? pv[K + t] : pv[t];
+		const double co = INC ? pv[t] / (ex * ex) : 2.0 * pv[K + t] / (ex * ex);
+		S tmp = ad_const<S>(-3.0);
+#pragma unroll
+		for (int i = 0; i < 3; ++i) tmp = tmp + ad_pow(st[i], ex);
+		val = val + co * tmp;
+	}
+	if constexpr (INC)
+		val = val + (0.5 * pv[2 * K]) * sq(ad_log(J));
+	else
+	{
+		const S jm2 = sq(J - 1.0);
+		S w = jm2;
+#pragma unroll
+		for (int t = 0; t < K; ++t)
+		{
+			val = val + (1.0 / pv[2 * K + t]) * w; // (J - 1)^(2(t+1)) / D_t
+			w = w * jm2;
+		}
+	}
+	return val;
+}
+
+// The eigenvalues of a symmetric 3 x 3 matrix m, the closed form that
+// utils::autogen::eigs_3d (autogen/auto_eigs.hpp:33-76) evaluates from the entries
+// m00, m11, m22, m01, m02, m12: with 9p = 3 (m01^2 + m02^2 + m12^2) + ((m00 - m22)^2 +
+// (m11 - m22)^2 + (m00 - m11)^2) / 2 and the angle t = acos(27 det(m - tr/3 I) / (2 (9p)^(3/2))) / 3,
+//   eig = tr/3 + (2/3) sqrt(9p) cos(t + {0, 2pi/3, -2pi/3});
+// all three tr/3 when 2 sqrt(9p) < 1e-10, t the constant 0 or pi/3 when the cosine's
+// argument leaves [-1, 1], as there.
+template <class S>
+__device__ __forceinline__ void sym_eigs3(const S (&m)[3][3], S (&res)[3])
+{
+	const S t01 = m[0][0] + m[1][1];
+	const S tr = t01 + m[2][2];
+	const S off = m[0][1] * m[0][1] + m[0][2] * m[0][2] + m[1][2] * m[1][2];
+	const S d02 = m[0][0] - m[2][2], d12 = m[1][1] - m[2][2], d01 = m[0][0] - m[1][1];
+	const S p9 = 3.0 * off + 0.5 * (d02 * d02) + 0.5 * (d12 * d12) + 0.5 * (d01 * d01);
+	if (2.0 * sqrt(ad_val(p9)) < 1e-10)
+	{
+		res[0] = res[1] = res[2] = (1.0 / 3.0) * tr;
+		return;
+	}
+	const S sp9 = ad_sqrt(p9);
+	const S num = -1.5 * (t01 * (m[0][0] + m[2][2]) * (m[1][1] + m[2][2])) + 4.5 * (tr * off) -
+				  13.5 * (m[0][1] * m[0][1] * m[2][2]) - 13.5 * (m[0][2] * m[0][2] * m[1][1]) -
+				  13.5 * (m[1][2] * m[1][2] * m[0][0]) + m[0][0] * m[0][0] * m[0][0] + 9.0 * (m[0][0] * m[1][1] * m[2][2]) +
+				  27.0 * (m[0][1] * m[0][2] * m[1][2]) + m[1][1] * m[1][1] * m[1][1] + m[2][2] * m[2][2] * m[2][2];
+	const S c3 = num * ad_recip(p9 * sp9);
+	const double c3v = ad_val(c3);
+	const S ang = (1.0 / 3.0) * (c3v >= 1.0 ? ad_const<S>(0.0) : c3v <= -1.0 ? ad_const<S>(M_PI) : ad_acos(c3));
+	const S r = (2.0 / 3.0) * sp9, mean = (1.0 / 3.0) * tr;
+	res[0] = r * ad_cos(ang) + mean;
+	res[1] = r * ad_cos(ang + 2.0 * M_PI / 3.0) + mean;
+	res[2] = r * ad_cos(ang - 2.0 * M_PI / 3.0) + mean;
+}
+
+template <class S>
+__device__ __forceinline__ S det3s(const S (&F)[3][3])
+{
+	return F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) - F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+		   F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+}
+
+// The Ogden densities of F, generic in the number type:
+//   UnconstrainedOgden (OgdenElasticity.tpp:8-57): the stretches sqrt(eig(F^T F)) J^(-1/3);
+//   IncompressibleOgden (OgdenElasticity.tpp:59-94): F~ = F / J^(1/3), the stretches
+//   sqrt(eig(F~ F~^T)); both then ogden_terms.
+template <int MAT, class S>
+__device__ __forceinline__ S ogden_psi(const S (&F)[3][3], const MatP &p)
+{
+	constexpr bool inc = MAT == MAT_INCOMPRESSIBLE_OGDEN;
+	const double pv[8] = {p.x, p.y, p.z, p.w, p.x2, p.y2, p.z2, p.w2};
+	const S J = det3s(F);
+	S Cm[3][3], st[3];
+	if constexpr (inc)
+	{
+		const S is = ad_recip(ad_pow(J, 1.0 / 3.0));
+		S Ft[3][3];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) Ft[r][c] = F[r][c] * is;
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) Cm[r][c] = Ft[r][0] * Ft[c][0] + Ft[r][1] * Ft[c][1] + Ft[r][2] * Ft[c][2];
+		sym_eigs3(Cm, st);
+#pragma unroll
+		for (int i = 0; i < 3; ++i) st[i] = ad_sqrt(st[i]);
+	}
+	else
+	{
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) Cm[r][c] = F[0][r] * F[0][c] + F[1][r] * F[1][c] + F[2][r] * F[2][c];
+		sym_eigs3(Cm, st);
+		const S jd = ad_pow(J, -1.0 / 3.0);
+#pragma unroll
+		for (int i = 0; i < 3; ++i) st[i] = ad_sqrt(st[i]) * jd;
+	}
+	if (p.nt == 1) return ogden_terms<1, inc>(st, J, pv);
+	if (p.nt == 2) return ogden_terms<2, inc>(st, J, pv);
+	return ogden_terms<3, inc>(st, J, pv);
+}
+
+// F with the dual parts of two directions: entry (r, c) carries d/de1 = [3r+c == i],
+// d/de2 = W(r, c) (W may be a unit direction e_j)
+__device__ __forceinline__ void hd_def_grad(const double F[3][3], int i, const double (&W)[9], HDual (&Fh)[3][3])
+{
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) Fh[r][c] = {F[r][c], (3 * r + c) == i ? 1.0 : 0.0, W[3 * r + c], 0.0};
+}
 
 // ---------------------------------------------------------------------------
 // energy densities of the invariant materials, generic in the number type
 // ---------------------------------------------------------------------------
 template <int MAT, class S>
-__device__ __forceinline__ S inv_psi(S I1, S I2, S J, const double4 &p)
+__device__ __forceinline__ S inv_psi(S I1, S I2, S J, const MatP &p)
 {
 	if constexpr (MAT == MAT_ISO_NEOHOOKEAN) // psi = mu/2 (J^-2/3 I1 - 3), IsochoricNeoHookean.hpp:19-33
 		return (0.5 * p.y) * (ad_pow(J, -2.0 / 3.0) * I1 - 3.0);
@@ -189,7 +376,7 @@ __device__ __forceinline__ void invariants(const double F[3][3], Invariants &v)
 
 // psi_x (x = I1, I2, J) by three dual evaluations
 template <int MAT>
-__device__ __forceinline__ void inv_psi_first(const Invariants &v, const double4 &p, double d[3])
+__device__ __forceinline__ void inv_psi_first(const Invariants &v, const MatP &p, double d[3])
 {
 #pragma unroll 1
 	for (int x = 0; x < 3; ++x)
@@ -197,20 +384,36 @@ __device__ __forceinline__ void inv_psi_first(const Invariants &v, const double4
 }
 
 template <int MAT>
-__device__ __forceinline__ double4 ad_params(const DevMesh &m, int e)
+__device__ __forceinline__ MatP ad_params(const DevMesh &m, int e)
 {
+	MatP p{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, m.mterms};
 	if constexpr (MAT == MAT_HOOKE || MAT == MAT_SAINT_VENANT_TENSOR) // their one tensor is m.hooke
-		return make_double4(0.0, 0.0, 0.0, 0.0);
+		return p;
 	else if constexpr (MAT == MAT_LINEAR_ELASTICITY || MAT == MAT_ISO_NEOHOOKEAN)
 	{
 		const double2 lm = __ldg(m.lame + e);
-		return make_double4(lm.x, lm.y, 0.0, 0.0);
+		p.x = lm.x;
+		p.y = lm.y;
+		return p;
 	}
 	else
 	{
-		const double2 *q = reinterpret_cast<const double2 *>(m.mpar + e);
+		// eight values per element, 64 bytes: the Ogden formulations read all of them
+		const double2 *q = reinterpret_cast<const double2 *>(m.mpar + 2 * (size_t)e);
 		const double2 x = __ldg(q), y = __ldg(q + 1);
-		return make_double4(x.x, x.y, y.x, y.y);
+		p.x = x.x;
+		p.y = x.y;
+		p.z = y.x;
+		p.w = y.y;
+		if constexpr (MAT == MAT_UNCONSTRAINED_OGDEN || MAT == MAT_INCOMPRESSIBLE_OGDEN)
+		{
+			const double2 z = __ldg(q + 2), w = __ldg(q + 3);
+			p.x2 = z.x;
+			p.y2 = z.y;
+			p.z2 = w.x;
+			p.w2 = w.y;
+		}
+		return p;
 	}
 }
 
@@ -263,9 +466,18 @@ __device__ __forceinline__ void right_cauchy_green(const double F[3][3], double 
 }
 
 template <int MAT>
-__device__ __forceinline__ double mat_energy(const double F[3][3], const double4 &p, const double *T)
+__device__ __forceinline__ double mat_energy(const double F[3][3], const MatP &p, const double *T)
 {
-	if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
+	if constexpr (entry_mat<MAT>())
+	{
+		double Fc[3][3];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) Fc[r][c] = F[r][c];
+		return ogden_psi<MAT, double>(Fc, p);
+	}
+	else if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
 	{
 		double Cr[9], e[6], sv[6];
 		right_cauchy_green(F, Cr);
@@ -296,9 +508,23 @@ __device__ __forceinline__ double mat_energy(const double F[3][3], const double4
 
 // P = dpsi/dF (row-major 9)
 template <int MAT>
-__device__ __forceinline__ void mat_stress(const double F[3][3], const double4 &p, const double *T, double P[9])
+__device__ __forceinline__ void mat_stress(const double F[3][3], const MatP &p, const double *T, double P[9])
 {
-	if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
+	if constexpr (entry_mat<MAT>())
+	{
+		// one dual evaluation per entry of F
+#pragma unroll 1
+		for (int i = 0; i < 9; ++i)
+		{
+			Dual1 Fd[3][3];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c) Fd[r][c] = {F[r][c], (3 * r + c) == i ? 1.0 : 0.0};
+			P[i] = ogden_psi<MAT, Dual1>(Fd, p).d;
+		}
+	}
+	else if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
 	{
 		double Cr[9], e[6], sv[6];
 		right_cauchy_green(F, Cr);
@@ -349,7 +575,7 @@ __device__ __forceinline__ double ad_element_energy(const DevMesh &m, const doub
 	int nodes[EL::N];
 	load_geom<EL, double>(m, e, Xg);
 	load_nodal<EL, double>(m, e, u, U, nodes);
-	const double4 prm = ad_params<MAT>(m, e);
+	const MatP prm = ad_params<MAT>(m, e);
 	double en = 0.0;
 	bool bad = false;
 #pragma unroll
@@ -396,7 +622,7 @@ __global__ void __launch_bounds__(NT) k_ad_gradient(DevMesh m, const double *__r
 	int nodes[EL::N];
 	load_geom<EL, double>(m, e, Xg);
 	load_nodal<EL, double>(m, e, u, U, nodes);
-	const double4 prm = ad_params<MAT>(m, e);
+	const MatP prm = ad_params<MAT>(m, e);
 #pragma unroll
 	for (int a = 0; a < EL::N; ++a) Gacc[a][0] = Gacc[a][1] = Gacc[a][2] = 0.0;
 	bool bad = false;
@@ -574,7 +800,7 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 		for (int i = lane; i < NG * 3; i += 32)
 			S.X[i / 3][i % 3] = __ldg(m.X + (size_t)__ldg(m.gconn + (size_t)(i / 3) * m.E + e) * 3 + i % 3);
 		__syncwarp();
-		const double4 prm = ad_params<MAT>(m, e);
+		const MatP prm = ad_params<MAT>(m, e);
 		if (lane < NQ)
 		{
 			const int q = lane;
@@ -586,7 +812,7 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 #pragma unroll
 				for (int c = 0; c < 3; ++c) S.Jit[q][3 * r + c] = Jit[r][c];
 			S.da[q] = detJ * qweight<EL>(q);
-			if constexpr (!quadratic_mat<MAT>()) invariants(F, S.inv[q]);
+			if constexpr (!quadratic_mat<MAT>()) invariants(F, S.inv[q]); // entry_mat: F = dI1/dF / 2
 			if constexpr (MAT == MAT_SAINT_VENANT_TENSOR)
 			{
 				// the point's Voigt stress, shared by its 45 tangent entries (psi is unused here)
@@ -632,6 +858,20 @@ __global__ void __launch_bounds__(WPB * 32) k_ad_blocks(DevMesh m, const double 
 				h = __ldg(m.hooke + 6 * voigt(ce.i / 3, ce.i % 3) + voigt(ce.j / 3, ce.j % 3));
 			else if constexpr (MAT == MAT_LINEAR_ELASTICITY)
 				h = prm.y * (ce.dab * ce.dAB + ce.le_aBbA) + prm.x * ce.le_aAbB;
+			else if constexpr (entry_mat<MAT>())
+			{
+				// one hyper-dual evaluation over the entries (i, j) of F
+				double F[3][3], ej[9];
+#pragma unroll
+				for (int r = 0; r < 3; ++r)
+#pragma unroll
+					for (int c = 0; c < 3; ++c) F[r][c] = 0.5 * S.inv[q].dx[0][3 * r + c];
+#pragma unroll
+				for (int l = 0; l < 9; ++l) ej[l] = l == ce.j ? 1.0 : 0.0;
+				HDual Fh[3][3];
+				hd_def_grad(F, ce.i, ej, Fh);
+				h = ogden_psi<MAT, HDual>(Fh, prm).ab;
+			}
 			else
 				h = inv_hessian_entry(S.inv[q], S.psi[q], ce);
 			S.C[q][k] = S.da[q] * h;
@@ -712,7 +952,7 @@ __device__ __forceinline__ void stress_invariants(const S F[3][3], S &I1, S &I2,
 // Q = sum_x (psi_x' dx/dF + psi_x (dx/dF)'), with ' the derivative along W; psi_x and
 // psi_x' = sum_y psi_xy y' come from one hyper-dual evaluation per invariant x.
 template <int MAT>
-__device__ __forceinline__ void stress_and_directional(const double F[3][3], const double W[3][3], const double4 &p,
+__device__ __forceinline__ void stress_and_directional(const double F[3][3], const double W[3][3], const MatP &p,
 													   double P[9], double Q[9])
 {
 	if constexpr (MAT == MAT_LINEAR_ELASTICITY)
@@ -726,6 +966,24 @@ __device__ __forceinline__ void stress_and_directional(const double F[3][3], con
 				P[3 * r + c] = p.y * ((F[r][c] - (r == c)) + (F[c][r] - (r == c))) + (r == c ? p.x * trG : 0.0);
 				Q[3 * r + c] = p.y * (W[r][c] + W[c][r]) + (r == c ? p.x * trW : 0.0);
 			}
+	}
+	else if constexpr (entry_mat<MAT>())
+	{
+		// one hyper-dual evaluation per entry i of F, along e_i and W: P_i and (C W)_i
+		double w9[9];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) w9[3 * r + c] = W[r][c];
+#pragma unroll 1
+		for (int i = 0; i < 9; ++i)
+		{
+			HDual Fh[3][3];
+			hd_def_grad(F, i, w9, Fh);
+			const HDual h = ogden_psi<MAT, HDual>(Fh, p);
+			P[i] = h.a;
+			Q[i] = h.ab;
+		}
 	}
 	else
 	{
@@ -804,7 +1062,7 @@ __global__ void __launch_bounds__(NT) k_ad_shape_vjp(DevMesh m, const double *__
 	load_geom<EL, double>(m, e, Xg);
 	load_nodal<EL, double>(m, e, u, U, nodes);
 	load_nodal<EL, double>(m, e, adj, Pn, nodes);
-	const double4 prm = ad_params<MAT>(m, e);
+	const MatP prm = ad_params<MAT>(m, e);
 #pragma unroll
 	for (int j = 0; j < EL::NG; ++j) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
 #pragma unroll 1
@@ -876,6 +1134,8 @@ static cudaError_t with_ad_material(const DevMesh &m, Fn &&f)
 		case MAT_VOLUME_PENALTY: f(EL{}, std::integral_constant<int, MAT_VOLUME_PENALTY>{}); break;
 		case MAT_HOOKE: f(EL{}, std::integral_constant<int, MAT_HOOKE>{}); break;
 		case MAT_SAINT_VENANT_TENSOR: f(EL{}, std::integral_constant<int, MAT_SAINT_VENANT_TENSOR>{}); break;
+		case MAT_UNCONSTRAINED_OGDEN: f(EL{}, std::integral_constant<int, MAT_UNCONSTRAINED_OGDEN>{}); break;
+		case MAT_INCOMPRESSIBLE_OGDEN: f(EL{}, std::integral_constant<int, MAT_INCOMPRESSIBLE_OGDEN>{}); break;
 		default: return cudaErrorInvalidValue;
 		}
 		return cudaGetLastError();
@@ -974,6 +1234,8 @@ cudaError_t launch_ad_shape_vjp_stage(const DevMesh &m, const double *u, const d
 	case MAT_MOONEY_RIVLIN: return by_el(std::integral_constant<int, MAT_MOONEY_RIVLIN>{});
 	case MAT_MOONEY_RIVLIN_3PARAM: return by_el(std::integral_constant<int, MAT_MOONEY_RIVLIN_3PARAM>{});
 	case MAT_VOLUME_PENALTY: return by_el(std::integral_constant<int, MAT_VOLUME_PENALTY>{});
+	case MAT_UNCONSTRAINED_OGDEN: return by_el(std::integral_constant<int, MAT_UNCONSTRAINED_OGDEN>{});
+	case MAT_INCOMPRESSIBLE_OGDEN: return by_el(std::integral_constant<int, MAT_INCOMPRESSIBLE_OGDEN>{});
 	}
 	return cudaErrorInvalidValue;
 }

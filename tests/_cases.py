@@ -85,4 +85,10 @@ def material_params(mat, n_elements, seed=0):
     if mat in ("HookeLinearElasticity", "SaintVenantTensor"):
         return {"elasticity_tensor": hooke_tensor(seed)}
     rng = np.random.default_rng(seed)
+    if mat == "UnconstrainedOgden":  # two terms (alpha, mu, D), a rubber-like fit
+        f = lambda v: v * rng.uniform(0.8, 1.2, n_elements)
+        return {"alphas": [f(1.3), f(5.0)], "mus": [f(1.2e5), f(2.0e3)], "Ds": [f(2e-6), f(5e-5)]}
+    if mat == "IncompressibleOgden":  # three terms (c, m) with a negative exponent, and k
+        f = lambda v: v * rng.uniform(0.8, 1.2, n_elements)
+        return {"c": [f(1.5e5), f(4.0e3), f(-3.0e3)], "m": [f(1.3), f(5.0), f(-2.0)], "k": f(8e5)}
     return {n: 1e5 * rng.uniform(0.5, 1.5, n_elements) for n in MATERIAL_PARAM_NAMES.get(mat, ())}

@@ -1,5 +1,6 @@
 """Energy-defined formulations on the GPU (pfg_materials.cu): LinearElasticity,
-MooneyRivlin, MooneyRivlin3Param and VolumePenalty, differentiated on the device by
+MooneyRivlin, MooneyRivlin3Param, VolumePenalty and the two Ogden formulations
+(principal stretches from the invariants' characteristic cubic), differentiated on the device by
 dual and hyper-dual numbers.  FP64 energy, gradient and Hessian (with
 project_to_psd and the Dirichlet reduction) against the oracle, which
 differentiates the same energies with second-order dual numbers over F as the
@@ -16,7 +17,8 @@ from _cases import make_case, material_params, rel_err
 
 pytestmark = pytest.mark.gpu
 
-MATS = ["LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty"]
+MATS = ["LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty", "UnconstrainedOgden",
+        "IncompressibleOgden"]
 ELEMS = [(M.P1_TET, 3), (M.P2_TET, 2), (M.Q1_HEX, 3)]
 
 
@@ -45,7 +47,7 @@ def test_energy_gradient_hessian_match_oracle(require_gpu, mat, et, g):
     asm.close()
 
 
-@pytest.mark.parametrize("mat", ["MooneyRivlin", "MooneyRivlin3Param"])
+@pytest.mark.parametrize("mat", ["MooneyRivlin", "MooneyRivlin3Param", "UnconstrainedOgden", "IncompressibleOgden"])
 def test_projected_and_reduced_hessian(require_gpu, mat):
     mesh, asm, orc, _, _ = setup(M.P2_TET, 2, mat, seed=5)
     rng = np.random.default_rng(6)
@@ -136,7 +138,8 @@ def test_inverted_element(require_gpu, mat):
     asm.close()
 
 
-SHAPE_MATS = ["IsochoricNeoHookean", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty"]
+SHAPE_MATS = ["IsochoricNeoHookean", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty",
+              "UnconstrainedOgden", "IncompressibleOgden"]
 
 
 @pytest.mark.parametrize("mat", SHAPE_MATS)

@@ -1,6 +1,6 @@
 """The oracle's restatement of the other elastic formulations (IsochoricNeoHookean,
 SaintVenant, LinearElasticity, MooneyRivlin, MooneyRivlin3Param, VolumePenalty,
-HookeLinearElasticity):
+HookeLinearElasticity, UnconstrainedOgden, IncompressibleOgden):
 derivatives by central finite differences, as the reference checks its forms
 (tests/test_form_derivatives.cpp:166-226), and closed-form known answers."""
 import numpy as np
@@ -13,7 +13,7 @@ from polyfem_b200 import mesh as M
 from _cases import make_case, material_params
 
 MATS = ["IsochoricNeoHookean", "SaintVenant", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param",
-        "VolumePenalty", "HookeLinearElasticity", "SaintVenantTensor"]
+        "VolumePenalty", "HookeLinearElasticity", "SaintVenantTensor", "UnconstrainedOgden", "IncompressibleOgden"]
 ELEMS = [(M.P1_TET, "P1"), (M.P2_TET, "P2"), (M.Q1_HEX, "Q1")]
 
 
@@ -223,7 +223,8 @@ def test_oracle_p1_mass_closed_form():
 
 
 # ----------------------------------------------------------- adjoint terms
-SHAPE_MATS = ["IsochoricNeoHookean", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty"]
+SHAPE_MATS = ["IsochoricNeoHookean", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty",
+              "UnconstrainedOgden", "IncompressibleOgden"]
 
 
 def _moved(mesh, v, d, h):
@@ -271,3 +272,29 @@ def test_linear_elasticity_material_vjp_finite_differences():
             fm = Oracle(mesh, lm, mm, material="LinearElasticity").gradient(u) @ p
             fd = (fp - fm) / (2 * h)
             assert abs(-term[e + which * E] - fd) <= 1e-6 * max(abs(fd), 1e-12) + 1e-9
+
+
+def test_ogden_known_answers():
+    """Homogeneous deformations F = R diag(a, b, c) of the unit cube: the principal
+    stretches are (a, b, c), so both Ogden energies are known in closed form; zero
+    energy and gradient at rest, and under a rotation."""
+    a, b, c = 1.15, 0.93, 1.04
+    J = a * b * c
+    th = 0.5
+    R = np.array([[np.cos(th), 0, np.sin(th)], [0, 1, 0], [-np.sin(th), 0, np.cos(th)]])
+    F = R @ np.diag([a, b, c])
+    st = np.array([a, b, c]) * J ** (-1 / 3)
+    al, mu_, D = [1.3, 5.0], [1.2e5, 2.0e3], [2e-6, 5e-5]
+    cs, ms, k = [1.5e5, 4.0e3, -3.0e3], [1.3, 5.0, -2.0], 8e5
+    psi_u = sum(2 * m_ / x ** 2 * ((st ** x).sum() - 3) for x, m_ in zip(al, mu_)) + \
+        sum((J - 1) ** (2 * (t + 1)) / D[t] for t in range(2))
+    psi_i = sum(c_ / m_ ** 2 * ((st ** m_).sum() - 3) for c_, m_ in zip(cs, ms)) + 0.5 * k * np.log(J) ** 2
+    for et in (M.P1_TET, M.P2_TET, M.Q1_HEX):
+        mesh, lam, mu, _, _ = make_case(et, 2, seed=4)
+        for mat, prm, psi in (("UnconstrainedOgden", {"alphas": al, "mus": mu_, "Ds": D}, psi_u),
+                              ("IncompressibleOgden", {"c": cs, "m": ms, "k": k}, psi_i)):
+            o = Oracle(mesh, lam, mu, material=mat, params=prm)
+            assert abs(o.energy(np.zeros(mesh.n_dofs))) <= 1e-12 * 1e5
+            assert np.abs(o.gradient(np.zeros(mesh.n_dofs))).max() <= 1e-9 * 1e5
+            assert abs(o.energy(_uniform(mesh, R))) <= 1e-9 * 1e5
+            assert abs(o.energy(_uniform(mesh, F)) - psi) <= 1e-10 * abs(psi), (mat, et)
