@@ -647,7 +647,10 @@ def run_suite(args):
         # the other materials (FP64): energy, gradient and the Hessian; the
         # parameterised ones with (c1, c2, k), (c1, c2, c3, d1), (k) of stress scale mu
         mu_s = float(np.median(mu))
-        mpar = {4: [mu_s, 0.5 * mu_s, 10 * mu_s], 5: [mu_s, 0.5 * mu_s, 0.2 * mu_s, 10 * mu_s], 6: [10 * mu_s]}
+        mpar = {4: [mu_s, 0.5 * mu_s, 10 * mu_s], 5: [mu_s, 0.5 * mu_s, 0.2 * mu_s, 10 * mu_s], 6: [10 * mu_s],
+                # Ogden: two terms (alpha, mu, D) / three terms (c, m) and k
+                9: [1.3, 5.0, mu_s, 0.02 * mu_s, 0.1 / mu_s, 1.0 / mu_s],
+                10: [mu_s, 0.03 * mu_s, -0.02 * mu_s, 1.3, 5.0, -2.0, 10 * mu_s]}
         # HookeLinearElasticity and the anisotropic SaintVenant: the isotropic tensor of
         # (2.333 mu, mu) (nu = 0.35) plus a seeded symmetric positive semi-definite part
         Ct = np.zeros((6, 6))
@@ -660,7 +663,8 @@ def run_suite(args):
         check(L.pfg_set_elasticity_tensor(h, vp(c21.ctypes.data)), h, "pfg_set_elasticity_tensor")
         for mname, mid in (("iso_neohookean", 1), ("saint_venant", 2), ("linear_elasticity", 3),
                            ("mooney_rivlin", 4), ("mooney_rivlin_3param", 5), ("volume_penalty", 6),
-                           ("hooke", 7), ("saint_venant_tensor", 8)):
+                           ("hooke", 7), ("saint_venant_tensor", 8), ("unconstrained_ogden", 9),
+                           ("incompressible_ogden", 10)):
             if mid in mpar:
                 pv = np.ascontiguousarray(np.repeat(np.asarray(mpar[mid], dtype=np.float64)[:, None], E, axis=1))
                 check(L.pfg_set_material_params(h, vp(pv.ctypes.data), len(mpar[mid]), 0), h,
