@@ -212,7 +212,10 @@ int pfg_version(void);
  *                                 parameters (alpha_0.., mu_0.., D_0..), 1 or 2 terms;
  *   PFG_MAT_INCOMPRESSIBLE_OGDEN: IncompressibleOgdenElasticity (OgdenElasticity.tpp:
  *                                 59-94), psi = sum_t c_t/m_t^2 (sum_i s_i^m_t - 3)
- *                                 + k/2 ln^2 J; parameters (c_0.., m_0.., k), 1 to 3 terms.
+ *                                 + k/2 ln^2 J; parameters (c_0.., m_0.., k), 1 to 3 terms;
+ *   PFG_MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC: MooneyRivlin3ParamSymbolic (MooneyRivlin3ParamSymbolic.cpp:
+ *                                 317-340), psi = c1 (I1~ - 3) + c2 (I2~ - 3)
+ *                                 + c3 (I1~ - 3)(I2~ - 3) + d1 ln^2 J, (c1, c2, c3, d1).
  * Energy, gradient and Hessian (with project_psd and the Dirichlet reduction) then
  * follow the chosen material in PFG_FP64 (other precisions return
  * PFG_ERR_UNSUPPORTED).  The adjoint terms follow the reference's assemblers:
@@ -237,7 +240,8 @@ enum pfg_material
 	PFG_MAT_HOOKE = 7,
 	PFG_MAT_SAINT_VENANT_TENSOR = 8,
 	PFG_MAT_UNCONSTRAINED_OGDEN = 9,
-	PFG_MAT_INCOMPRESSIBLE_OGDEN = 10
+	PFG_MAT_INCOMPRESSIBLE_OGDEN = 10,
+	PFG_MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC = 11
 };
 int pfg_set_material(pfg_context *ctx, int material);
 
@@ -251,7 +255,8 @@ int pfg_set_material(pfg_context *ctx, int material);
 int pfg_set_elasticity_tensor(pfg_context *ctx, const double *c21);
 
 /* Per-element parameters of PFG_MAT_MOONEY_RIVLIN (n_params 3: c1, c2, k),
- * PFG_MAT_MOONEY_RIVLIN_3PARAM (4: c1, c2, c3, d1), PFG_MAT_VOLUME_PENALTY
+ * PFG_MAT_MOONEY_RIVLIN_3PARAM and PFG_MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC (4: c1, c2,
+ * c3, d1), PFG_MAT_VOLUME_PENALTY
  * (1: k), PFG_MAT_UNCONSTRAINED_OGDEN (3 K: alpha_0..alpha_K-1, mu_0.., D_0.., with
  * K = 1 or 2 terms, as GenericMatParams alphas, mus, Ds, OgdenElasticity.cpp:12-20)
  * and PFG_MAT_INCOMPRESSIBLE_OGDEN (2 K + 1: c_0.., m_0.., k, K = 1 to 3,

@@ -90,11 +90,12 @@ class Oracle:
 
     MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2, "LinearElasticity": 3,
                  "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6, "HookeLinearElasticity": 7,
-                 "SaintVenantTensor": 8, "UnconstrainedOgden": 9, "IncompressibleOgden": 10}
+                 "SaintVenantTensor": 8, "UnconstrainedOgden": 9, "IncompressibleOgden": 10,
+                 "MooneyRivlin3ParamSymbolic": 11}
     # lists of one value per term (alphas, mus, Ds; c, m), then IncompressibleOgden's k
     OGDEN_PARAMS = {"UnconstrainedOgden": ("alphas", "mus", "Ds"), "IncompressibleOgden": ("c", "m", "k")}
     MATERIAL_PARAMS = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
-                       "VolumePenalty": ("k",)}
+                       "VolumePenalty": ("k",), "MooneyRivlin3ParamSymbolic": ("c1", "c2", "c3", "d1")}
 
     def __init__(self, mesh, lam, mu, n_threads: int = 1, cache_size: int = 900000,
                  fast_pattern: bool = False, material: str = "NeoHookean", params=None):

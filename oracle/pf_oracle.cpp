@@ -501,7 +501,8 @@ enum
 	MAT_HOOKE = 7,
 	MAT_SAINT_VENANT_TENSOR = 8,
 	MAT_UNCONSTRAINED_OGDEN = 9,
-	MAT_INCOMPRESSIBLE_OGDEN = 10
+	MAT_INCOMPRESSIBLE_OGDEN = 10,
+	MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC = 11
 };
 constexpr int PRM_MAX = 21; // material parameters of an element: 21 tensor entries for MAT_HOOKE and
                             // MAT_SAINT_VENANT_TENSOR
@@ -725,6 +726,28 @@ static S psi_mooney_rivlin_3param(const S (&F)[3][3], double c1, double c2, doub
 	return c1 * I1t + (S(c2) + c3 * I1t) * I2t + d1 * (jm * jm);
 }
 
+// MooneyRivlin3ParamSymbolic (MooneyRivlin3ParamSymbolic.cpp:317-340): B = F F^T,
+// I1~ = J^(-2/3) tr B, I2~ = J^(-4/3) I2(B),
+// psi = c1 (I1~ - 3) + c2 (I2~ - 3) + c3 (I1~ - 3)(I2~ - 3) + d1 ln^2 J
+template <class S>
+static S psi_mooney_rivlin_3param_symbolic(const S (&F)[3][3], double c1, double c2, double c3, double d1)
+{
+	const S J = det3s(F);
+	const S lj = dlog(J);
+	S B[3][3];
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c)
+		{
+			B[r][c] = S(0.0);
+			for (int m = 0; m < 3; ++m) B[r][c] = B[r][c] + F[r][m] * F[c][m];
+		}
+	S trB, i2;
+	invariants12(B, trB, i2);
+	const S I1t = dpow(J, -2.0 / 3.0) * trB;
+	const S I2t = dpow(J, -4.0 / 3.0) * i2;
+	return c1 * (I1t - S(3.0)) + c2 * (I2t - S(3.0)) + c3 * ((I1t - S(3.0)) * (I2t - S(3.0))) + d1 * (lj * lj);
+}
+
 // VolumePenalty: psi = k/2 ((J^2 - 1)/2 - ln J)
 template <class S>
 static S psi_volume_penalty(const S (&F)[3][3], double k)
@@ -873,6 +896,7 @@ static S psi_material(int mat, const S (&F)[3][3], const double *prm)
 	case MAT_LINEAR_ELASTICITY: return psi_linear_elasticity(F, prm[0], prm[1]);
 	case MAT_MOONEY_RIVLIN: return psi_mooney_rivlin(F, prm[0], prm[1], prm[2]);
 	case MAT_MOONEY_RIVLIN_3PARAM: return psi_mooney_rivlin_3param(F, prm[0], prm[1], prm[2], prm[3]);
+	case MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC: return psi_mooney_rivlin_3param_symbolic(F, prm[0], prm[1], prm[2], prm[3]);
 	case MAT_UNCONSTRAINED_OGDEN: return psi_unconstrained_ogden(F, prm, (int)prm[PRM_COUNT] / 3);
 	case MAT_INCOMPRESSIBLE_OGDEN: return psi_incompressible_ogden(F, prm, ((int)prm[PRM_COUNT] - 1) / 2);
 	default: return psi_volume_penalty(F, prm[0]);

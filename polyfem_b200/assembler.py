@@ -314,11 +314,11 @@ class NeoHookeanAssembler:
     # -- material (AssemblerUtils::make_assembler's formulation name) ------------------
     MATERIALS = {"NeoHookean": 0, "IsochoricNeoHookean": 1, "SaintVenant": 2, "LinearElasticity": 3,
                  "MooneyRivlin": 4, "MooneyRivlin3Param": 5, "VolumePenalty": 6, "HookeLinearElasticity": 7,
-                 "UnconstrainedOgden": 9, "IncompressibleOgden": 10}
+                 "UnconstrainedOgden": 9, "IncompressibleOgden": 10, "MooneyRivlin3ParamSymbolic": 11}
     SAINT_VENANT_TENSOR = 8  # "SaintVenant" with an elasticity_tensor
     # the GenericMatParam names of the parameterised formulations, in pfg_set_material_params order
     MATERIAL_PARAMS = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
-                       "VolumePenalty": ("k",)}
+                       "VolumePenalty": ("k",), "MooneyRivlin3ParamSymbolic": ("c1", "c2", "c3", "d1")}
     # the Ogden formulations' GenericMatParams (OgdenElasticity.cpp:7-10, 48-51): one value
     # per term for each list; IncompressibleOgden's k is one GenericMatParam
     OGDEN_PARAMS = {"UnconstrainedOgden": ("alphas", "mus", "Ds"), "IncompressibleOgden": ("c", "m", "k")}
@@ -329,7 +329,7 @@ class NeoHookeanAssembler:
 
         "NeoHookean" (default), "IsochoricNeoHookean", "SaintVenant" (isotropic) and
         "LinearElasticity" use the per-element lambda/mu.  "MooneyRivlin" (c1, c2, k),
-        "MooneyRivlin3Param" (c1, c2, c3, d1) and "VolumePenalty" (k) take their
+        "MooneyRivlin3Param" and "MooneyRivlin3ParamSymbolic" (c1, c2, c3, d1) and "VolumePenalty" (k) take their
         parameters as keywords, each a scalar or one value per element (host arrays
         or CUDA tensors).  "UnconstrainedOgden" takes alphas, mus, Ds (lists of one
         entry per term, 1 or 2 terms) and "IncompressibleOgden" c, m (1 to 3 terms)

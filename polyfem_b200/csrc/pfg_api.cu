@@ -152,7 +152,8 @@ int check_mem(int mem) { return mem == PFG_MEM_HOST || mem == PFG_MEM_DEVICE; }
 bool material_takes_params(int mat)
 {
 	return mat == PFG_MAT_MOONEY_RIVLIN || mat == PFG_MAT_MOONEY_RIVLIN_3PARAM || mat == PFG_MAT_VOLUME_PENALTY ||
-		   mat == PFG_MAT_UNCONSTRAINED_OGDEN || mat == PFG_MAT_INCOMPRESSIBLE_OGDEN;
+		   mat == PFG_MAT_UNCONSTRAINED_OGDEN || mat == PFG_MAT_INCOMPRESSIBLE_OGDEN ||
+		   mat == PFG_MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC;
 }
 bool material_params_fit(int mat, int n, int *terms)
 {
@@ -160,7 +161,8 @@ bool material_params_fit(int mat, int n, int *terms)
 	switch (mat)
 	{
 	case PFG_MAT_MOONEY_RIVLIN: return n == 3;
-	case PFG_MAT_MOONEY_RIVLIN_3PARAM: return n == 4;
+	case PFG_MAT_MOONEY_RIVLIN_3PARAM:
+	case PFG_MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC: return n == 4;
 	case PFG_MAT_VOLUME_PENALTY: return n == 1;
 	case PFG_MAT_UNCONSTRAINED_OGDEN: // alphas, mus, Ds: three per term
 		*terms = n / 3;
@@ -741,7 +743,7 @@ int pfg_set_stream(pfg_context *c, void *stream)
 
 int pfg_set_material(pfg_context *c, int material)
 {
-	if (!c || material < PFG_MAT_NEOHOOKEAN || material > PFG_MAT_INCOMPRESSIBLE_OGDEN)
+	if (!c || material < PFG_MAT_NEOHOOKEAN || material > PFG_MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC)
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
 	c->m.mat = material;
 	return PFG_OK;

@@ -23,13 +23,13 @@ struct DevMesh
 	int et = 0, E = 0, N = 0, Ng = 0;
 	int mat = 0; // pfg_material: 0 NeoHookean, 1 IsochoricNeoHookean, 2 SaintVenant, 3 LinearElasticity,
 	             // 4 MooneyRivlin, 5 MooneyRivlin3Param, 6 VolumePenalty, 7 HookeLinearElasticity,
-	             // 8 SaintVenant with an anisotropic tensor, 9 UnconstrainedOgden, 10 IncompressibleOgden
-	             // (pfg_set_material)
+	             // 8 SaintVenant with an anisotropic tensor, 9 UnconstrainedOgden, 10 IncompressibleOgden,
+	             // 11 MooneyRivlin3ParamSymbolic (pfg_set_material)
 	const int *conn = nullptr;
 	const int *gconn = nullptr;
 	const double *X = nullptr;
 	const double2 *lame = nullptr;
-	const double4 *mpar = nullptr; // per-element parameters of materials 4..6, 9, 10 (pfg_set_material_params):
+	const double4 *mpar = nullptr; // per-element parameters of materials 4..6, 9..11 (pfg_set_material_params):
 	                               // eight zero-padded values (two double4) per element
 	int mterms = 0;                // number of terms of the Ogden formulations (9, 10)
 	const double *hooke = nullptr; // materials 7, 8: the full symmetric 6 x 6 Voigt elasticity tensor, row-major

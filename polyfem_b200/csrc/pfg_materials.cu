@@ -45,6 +45,8 @@
 //                                          (MooneyRivlinElasticity.hpp:25-46)
 //   5 MooneyRivlin3Param  (c1, c2, c3, d1) psi = c1 (I1~ - 3) + (c2 + c3 (I1~ - 3)) (I2~ - 3) + d1 (J - 1)^2
 //                                          (MooneyRivlin3ParamElasticity.hpp:26-49)
+//  11 MooneyRivlin3ParamSymbolic (c1, c2, c3, d1): the same with d1 ln^2 J
+//                                          (MooneyRivlin3ParamSymbolic.cpp:317-340)
 //   6 VolumePenalty       (k)              psi = k/2 ((J^2 - 1)/2 - ln J)   (VolumePenalty.hpp:20-34)
 //   7 HookeLinearElasticity (one tensor)  psi = 1/2 sigma:eps, sigma = T eps in Voigt form
 //                                          (HookeLinearElasticity.cpp:372-421)
@@ -65,7 +67,8 @@ namespace pfg
 {
 
 constexpr int MAT_LINEAR_ELASTICITY = 3, MAT_MOONEY_RIVLIN = 4, MAT_MOONEY_RIVLIN_3PARAM = 5, MAT_VOLUME_PENALTY = 6,
-			  MAT_HOOKE = 7, MAT_SAINT_VENANT_TENSOR = 8, MAT_UNCONSTRAINED_OGDEN = 9, MAT_INCOMPRESSIBLE_OGDEN = 10;
+			  MAT_HOOKE = 7, MAT_SAINT_VENANT_TENSOR = 8, MAT_UNCONSTRAINED_OGDEN = 9, MAT_INCOMPRESSIBLE_OGDEN = 10,
+			  MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC = 11;
 // An element's material parameters: up to eight values (pfg_set_material_params)
 // and, for the Ogden formulations, the number of terms.
 struct MatP
@@ -331,6 +334,8 @@ __device__ __forceinline__ S inv_psi(S I1, S I2, S J, const MatP &p)
 		const S I1t = j23 * I1 - 3.0, I2t = sq(j23) * I2 - 3.0;
 		if constexpr (MAT == MAT_MOONEY_RIVLIN)
 			return p.x * I1t + p.y * I2t + (0.5 * p.z) * sq(ad_log(J));
+		else if constexpr (MAT == MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC) // its volumetric term is d1 ln^2 J
+			return p.x * I1t + (p.z * I1t + p.y) * I2t + p.w * sq(ad_log(J));
 		else // MAT_MOONEY_RIVLIN_3PARAM
 			return p.x * I1t + (p.z * I1t + p.y) * I2t + p.w * sq(J - 1.0);
 	}
@@ -1136,6 +1141,9 @@ static cudaError_t with_ad_material(const DevMesh &m, Fn &&f)
 		case MAT_SAINT_VENANT_TENSOR: f(EL{}, std::integral_constant<int, MAT_SAINT_VENANT_TENSOR>{}); break;
 		case MAT_UNCONSTRAINED_OGDEN: f(EL{}, std::integral_constant<int, MAT_UNCONSTRAINED_OGDEN>{}); break;
 		case MAT_INCOMPRESSIBLE_OGDEN: f(EL{}, std::integral_constant<int, MAT_INCOMPRESSIBLE_OGDEN>{}); break;
+		case MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC:
+			f(EL{}, std::integral_constant<int, MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC>{});
+			break;
 		default: return cudaErrorInvalidValue;
 		}
 		return cudaGetLastError();
@@ -1236,6 +1244,7 @@ cudaError_t launch_ad_shape_vjp_stage(const DevMesh &m, const double *u, const d
 	case MAT_VOLUME_PENALTY: return by_el(std::integral_constant<int, MAT_VOLUME_PENALTY>{});
 	case MAT_UNCONSTRAINED_OGDEN: return by_el(std::integral_constant<int, MAT_UNCONSTRAINED_OGDEN>{});
 	case MAT_INCOMPRESSIBLE_OGDEN: return by_el(std::integral_constant<int, MAT_INCOMPRESSIBLE_OGDEN>{});
+	case MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC: return by_el(std::integral_constant<int, MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC>{});
 	}
 	return cudaErrorInvalidValue;
 }

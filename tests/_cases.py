@@ -61,7 +61,7 @@ def permuted(mesh, u, seed=0):
 # GenericMatParam names of the parameterised formulations (MooneyRivlinElasticity.hpp,
 # MooneyRivlin3ParamElasticity.hpp, VolumePenalty.hpp)
 MATERIAL_PARAM_NAMES = {"MooneyRivlin": ("c1", "c2", "k"), "MooneyRivlin3Param": ("c1", "c2", "c3", "d1"),
-                        "VolumePenalty": ("k",)}
+                        "VolumePenalty": ("k",), "MooneyRivlin3ParamSymbolic": ("c1", "c2", "c3", "d1")}
 
 
 def hooke_tensor(seed=0, lam=86419.75, mu=37037.04):

@@ -74,7 +74,7 @@ def test_material_switch_and_unsupported_calls(require_gpu):
         with pytest.raises(PfgError) as ei:
             call()
         assert ei.value.status == 4  # PFG_ERR_UNSUPPORTED
-    assert lib().pfg_set_material(asm.handle, 11) == 1  # PFG_ERR_INVALID
+    assert lib().pfg_set_material(asm.handle, 12) == 1  # PFG_ERR_INVALID
     asm.set_material("NeoHookean")
     assert asm.assemble_energy(u) == e_nh  # back on the NeoHookean path, bit for bit
     with pytest.raises(ValueError):

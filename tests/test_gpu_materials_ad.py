@@ -18,7 +18,7 @@ from _cases import make_case, material_params, rel_err
 pytestmark = pytest.mark.gpu
 
 MATS = ["LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty", "UnconstrainedOgden",
-        "IncompressibleOgden"]
+        "IncompressibleOgden", "MooneyRivlin3ParamSymbolic"]
 ELEMS = [(M.P1_TET, 3), (M.P2_TET, 2), (M.Q1_HEX, 3)]
 
 
@@ -47,7 +47,8 @@ def test_energy_gradient_hessian_match_oracle(require_gpu, mat, et, g):
     asm.close()
 
 
-@pytest.mark.parametrize("mat", ["MooneyRivlin", "MooneyRivlin3Param", "UnconstrainedOgden", "IncompressibleOgden"])
+@pytest.mark.parametrize("mat", ["MooneyRivlin", "MooneyRivlin3Param", "UnconstrainedOgden", "IncompressibleOgden",
+        "MooneyRivlin3ParamSymbolic"])
 def test_projected_and_reduced_hessian(require_gpu, mat):
     mesh, asm, orc, _, _ = setup(M.P2_TET, 2, mat, seed=5)
     rng = np.random.default_rng(6)
@@ -139,7 +140,7 @@ def test_inverted_element(require_gpu, mat):
 
 
 SHAPE_MATS = ["IsochoricNeoHookean", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty",
-              "UnconstrainedOgden", "IncompressibleOgden"]
+              "UnconstrainedOgden", "IncompressibleOgden", "MooneyRivlin3ParamSymbolic"]
 
 
 @pytest.mark.parametrize("mat", SHAPE_MATS)

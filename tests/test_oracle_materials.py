@@ -13,7 +13,8 @@ from polyfem_b200 import mesh as M
 from _cases import make_case, material_params
 
 MATS = ["IsochoricNeoHookean", "SaintVenant", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param",
-        "VolumePenalty", "HookeLinearElasticity", "SaintVenantTensor", "UnconstrainedOgden", "IncompressibleOgden"]
+        "VolumePenalty", "HookeLinearElasticity", "SaintVenantTensor", "UnconstrainedOgden", "IncompressibleOgden",
+        "MooneyRivlin3ParamSymbolic"]
 ELEMS = [(M.P1_TET, "P1"), (M.P2_TET, "P2"), (M.Q1_HEX, "Q1")]
 
 
@@ -91,6 +92,9 @@ def test_energy_defined_materials_known_answers():
                                    [(dil, d1 * (s_ ** 3 - 1) ** 2), (rot, 0.0),
                                     (iso, c1 * (I1 - 3) + (c2 + c3 * (I1 - 3)) * (I2 - 3))]),
             "VolumePenalty": ({"k": k}, [(dil, k / 2 * ((s_ ** 6 - 1) / 2 - 3 * np.log(s_))), (rot, 0.0), (iso, 0.0)]),
+            "MooneyRivlin3ParamSymbolic": ({"c1": c1, "c2": c2, "c3": c3, "d1": d1},
+                                           [(dil, d1 * (3 * np.log(s_)) ** 2), (rot, 0.0),
+                                            (iso, c1 * (I1 - 3) + c2 * (I2 - 3) + c3 * (I1 - 3) * (I2 - 3))]),
         }
         for mat, (prm, checks) in cases.items():
             o = Oracle(mesh, lam, mu, material=mat, params=prm)
@@ -224,7 +228,7 @@ def test_oracle_p1_mass_closed_form():
 
 # ----------------------------------------------------------- adjoint terms
 SHAPE_MATS = ["IsochoricNeoHookean", "LinearElasticity", "MooneyRivlin", "MooneyRivlin3Param", "VolumePenalty",
-              "UnconstrainedOgden", "IncompressibleOgden"]
+              "UnconstrainedOgden", "IncompressibleOgden", "MooneyRivlin3ParamSymbolic"]
 
 
 def _moved(mesh, v, d, h):
