@@ -373,6 +373,14 @@ def run_gpu(args):
     e2e_ms = _events_ms(stream, lambda: call(PFG_SPLIT32, PFG_MEM_HOST, hptr_u, hptr_v), args.steps)
     e2e_ms = max_over_ranks(e2e_ms)
 
+    # one Newton step that keeps the matrix on the device: pinned u in; the reduced
+    # (x = 0 face clamped) gradient and PSD-projected FP64 Hessian, the device CG on it
+    # (relative residual 1e-6), the full step; pinned step out.  Times the whole step
+    # and each part with CUDA events on the context's stream.
+    newton = None
+    if rank == 0 and world == 1 and not args.no_newton:
+        newton = time_newton_step(asm, h, mesh, u_host, stream, min(args.steps, 5))
+
     tri_bytes = 4 * 8 * ((9 * 55 + 7) // 8)  # P2 block triangle in FP32
     bytes_alg = algorithmic_bytes(mesh, nnz)
     peak, peak_src = _peaks()
@@ -425,6 +433,7 @@ def run_gpu(args):
                                  "on the context's stream; frac of measured HBM copy bandwidth; traffic = ncu "
                                  "DRAM bytes per element of the 24^3 capture x elements"},
             "cpu_baseline": cpu,
+            "e2e_newton_step": newton,
             "configs": configs,
             "clocks": clocks,
             "gpu_launches": 2 * args.steps,
@@ -435,6 +444,59 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def time_newton_step(asm, h, mesh, u_host, stream, steps):
+    """One Newton step of the device-resident path (NLProblem with the projecting
+    Dirichlet form: NLProblem::gradient / hessian reduced, the linear solve, the step
+    reduced_to_full): H2D of u and D2H of the step inside the timed region."""
+    import ctypes
+
+    import torch
+    from polyfem_b200._lib import check, lib
+    L = lib()
+    face = np.flatnonzero(mesh.node_pos[:, 0] <= 1e-12)
+    asm.set_dirichlet((3 * face[:, None] + np.arange(3)).ravel())
+    L.pfg_set_stream(h, ctypes_ptr(stream.cuda_stream))
+    nf, ndof = asm.n_free, mesh.n_dofs
+    ud = torch.empty(ndof, dtype=torch.float64, device="cuda")
+    g = torch.empty(nf, dtype=torch.float64, device="cuda")
+    x = torch.empty(nf, dtype=torch.float64, device="cuda")
+    dx = torch.empty(ndof, dtype=torch.float64, device="cuda")
+    dx_host = torch.empty(ndof, dtype=torch.float64).pin_memory()
+    it, rr = ctypes.c_int(), ctypes.c_double()
+    P = ctypes_ptr
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+
+    def step():
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            ud.copy_(u_host, non_blocking=True)
+            check(L.pfg_gradient_reduced(h, P(ud.data_ptr()), 1, 0, P(g.data_ptr())), h, "pfg_gradient_reduced")
+            ev[1].record(stream)
+            check(L.pfg_hessian_reduced(h, P(ud.data_ptr()), 1, 0, 1, None), h, "pfg_hessian_reduced")
+            ev[2].record(stream)
+            check(L.pfg_cg_solve(h, 1, None, P(g.data_ptr()), 1, 1e-6, 5000, 0, P(x.data_ptr()), ctypes.byref(it),
+                                 ctypes.byref(rr)), h, "pfg_cg_solve")
+            ev[3].record(stream)
+            check(L.pfg_reduced_to_full(h, P(x.data_ptr()), None, 1, P(dx.data_ptr())), h, "pfg_reduced_to_full")
+            dx_host.copy_(dx, non_blocking=True)
+            ev[4].record(stream)
+        torch.cuda.synchronize()
+        return [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
+
+    step()
+    parts = [step() for _ in range(steps)]
+    med = [statistics.median(p[i] for p in parts) for i in range(4)]
+    total = sum(med)
+    E = mesh.n_elements
+    return {"value": E / (total * 1e-3), "unit": UNIT, "ms_per_step": total,
+            "h2d_bytes_per_step": ndof * 8, "d2h_bytes_per_step": ndof * 8,
+            "ms_gradient": med[0], "ms_hessian_psd": med[1], "ms_cg": med[2], "ms_step_out": med[3],
+            "cg_iterations": it.value, "cg_rel_residual": rr.value, "n_free": nf,
+            "note": "NLProblem's Newton step with the matrix kept on the device: reduced gradient, reduced "
+                    "PSD-projected FP64 Hessian, Jacobi-preconditioned CG to 1e-6, reduced_to_full; "
+                    "median of the timed steps"}
 
 
 # ----------------------------------------------------------------- the other four workloads
@@ -758,6 +820,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-configs", action="store_true", help="skip the per-workload timings of configs 1, 3, 4, 5")
     ap.add_argument("--suite", action="store_true", help="per-operation timings on all workloads")
+    ap.add_argument("--no-newton", action="store_true", help="skip the device-resident Newton step")
     ap.add_argument("--profile", default="", choices=["", "fp64", "fp32", "split32", "split32_simt"],
                     help="time only this precision's Hessian on the --grid cube (the ncu capture command)")
     ap.add_argument("--only", default="", help="comma-separated suite workload keys (" + ",".join(SUITE) + ")")
