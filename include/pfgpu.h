@@ -268,6 +268,29 @@ int pfg_set_elasticity_tensor(pfg_context *ctx, const double *c21);
 int pfg_set_material_params(pfg_context *ctx, const double *params, int n_params, int mem);
 
 /* ---------------------------------------------------------------------------
+ * Compositions of formulations.  MaterialSum (SumModel.cpp:43-78) adds the element
+ * energies, gradients and Hessians of several formulations, each with its own
+ * parameters; MultiModels (MultiModel.cpp:35-58) assembles every element with the
+ * formulation of its body.  pfg_set_component sets component k (< PFG_MAX_COMPONENTS):
+ * its material (any PFG_MAT_*), its per-element (lambda, mu) (NULL: the context's
+ * pfg_set_lame values), its per-element parameters as pfg_set_material_params takes
+ * them (params[q * n_elements + e], NULL / 0 for materials without), and the 21
+ * tensor entries of PFG_MAT_HOOKE / PFG_MAT_SAINT_VENANT_TENSOR (host memory; NULL
+ * otherwise); arrays in `mem`.  pfg_set_composite then switches the context to the
+ * composition of components 0 .. n_components-1: element_component (host, n_elements
+ * entries in [0, n_components)) gives each element's component (MultiModels), NULL
+ * adds all components on every element (MaterialSum).  The element blocks are
+ * combined per element before the PSD projection, as the reference projects the
+ * composed element matrix.  Energy, per-element energy, gradient and Hessian, full
+ * and Dirichlet-reduced, in PFG_FP64; the adjoint terms return PFG_ERR_UNSUPPORTED
+ * (SumModel and MultiModel have none).  pfg_set_material leaves the composition.
+ * ------------------------------------------------------------------------- */
+#define PFG_MAX_COMPONENTS 4
+int pfg_set_component(pfg_context *ctx, int k, int material, const double *lambda, const double *mu,
+                      const double *params, int n_params, const double *c21, int mem);
+int pfg_set_composite(pfg_context *ctx, int n_components, const int *element_component);
+
+/* ---------------------------------------------------------------------------
  * Dirichlet reduction.  When the only constraint form of the nonlinear problem
  * is the Dirichlet one (BCLagrangianForm::can_project), NLProblem reduces the
  * full quantities by dropping the constrained dofs:

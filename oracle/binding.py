@@ -289,6 +289,34 @@ def dense_hessian(orc, mesh, u):
     return cache
 
 
+def composite_reference(mesh, components, element_component, u, project=False):
+    """MaterialSum (SumModel.cpp:43-78) and MultiModels (MultiModel.cpp:35-58) restated
+    from the oracle's element quantities: per element the sum over the components (or
+    only the element's own component) of energy, gradient and Hessian, the Hessian
+    projected after the sum (NLAssembler projects the element matrix the composition
+    returns), then assembled.  components: (oracle material name, lam, mu, params) per
+    component.  Returns (per-element energies, gradient, dense Hessian)."""
+    orcs = [Oracle(mesh, lam, mu, material=mat, params=prm) for mat, lam, mu, prm in components]
+    n = mesh.conn.shape[1]
+    E = mesh.n_elements
+    per = np.zeros(E)
+    g = np.zeros(mesh.n_dofs)
+    H = np.zeros((mesh.n_dofs, mesh.n_dofs))
+    for e in range(E):
+        ks = range(len(orcs)) if element_component is None else [int(element_component[e])]
+        en, ge, He = 0.0, np.zeros(3 * n), np.zeros((3 * n, 3 * n))
+        for k in ks:
+            a, b, c = orcs[k].element(e, u)
+            en, ge, He = en + a, ge + b, He + c
+        if project:
+            He = project_psd(He)
+        dofs = (3 * mesh.conn[e][:, None] + np.arange(3)[None, :]).ravel()
+        per[e] = en
+        g[dofs] += ge
+        H[np.ix_(dofs, dofs)] += He
+    return per, g, H
+
+
 def free_dofs(ndof: int, constrained):
     """not_constraints_ / old_to_new_ of BCLagrangianForm (BCLagrangianForm.cpp:122-137)."""
     is_c = np.zeros(ndof, dtype=bool)

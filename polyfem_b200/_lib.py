@@ -126,6 +126,8 @@ SIGNATURES = {
     "pfg_mass_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
     "pfg_lump_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
     "pfg_dense_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
+    "pfg_set_component": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "pfg_set_composite": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "pfg_cg_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
 }

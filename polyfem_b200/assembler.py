@@ -364,6 +364,58 @@ class NeoHookeanAssembler:
         check(lib().pfg_set_material(self._h, mat_id), self._h, "pfg_set_material")
         self.material = formulation
 
+    def set_composite(self, components, element_component=None):
+        """MaterialSum (SumModel.cpp:43-78) or MultiModels (MultiModel.cpp:35-58).
+
+        components: a list (at most 4) of dicts, each {"formulation": name, ...} with the
+        formulation's parameters as set_material takes them, and optionally "lam" / "mu"
+        (per-element or scalar Lame parameters of that component; default: the
+        assembler's).  element_component: None adds all components on every element
+        (MaterialSum); else one component index per element (MultiModels).  Assembled
+        in FP64; set_material leaves the composition."""
+        E = self.n_elements
+        if not 1 <= len(components) <= 4:
+            raise ValueError("1 to 4 components")
+        for k, comp in enumerate(components):
+            comp = dict(comp)
+            name = comp.pop("formulation")
+            lam = comp.pop("lam", None)
+            mu = comp.pop("mu", None)
+            if (lam is None) != (mu is None):
+                raise ValueError("give both lam and mu of a component, or neither")
+            mat = self.MATERIALS.get(name)
+            if mat is None and name != "NeoHookean":
+                raise ValueError(f"unknown formulation {name!r}")
+            c21 = None
+            if name == "HookeLinearElasticity" or (name == "SaintVenant" and "elasticity_tensor" in comp):
+                c21 = np.ascontiguousarray(np.asarray(comp.pop("elasticity_tensor"), dtype=np.float64).ravel())
+                if c21.size != 21:
+                    raise ValueError("the elasticity tensor takes 21 entries")
+                if name == "SaintVenant":
+                    mat = self.SAINT_VENANT_TENSOR
+            if name in self.OGDEN_PARAMS:
+                vals = self._ogden_params(name, comp)
+            else:
+                names = self.MATERIAL_PARAMS.get(name, ())
+                if set(comp) != set(names):
+                    raise ValueError(f"{name} takes the parameters {list(names)}, got {sorted(comp)}")
+                vals = [comp[n] for n in names]
+            packed = (np.ascontiguousarray(np.stack([np.broadcast_to(np.asarray(v, dtype=np.float64), (E,))
+                                                     for v in vals])) if vals else None)
+            lv = None if lam is None else np.ascontiguousarray(np.broadcast_to(np.asarray(lam, dtype=np.float64), (E,)))
+            mv = None if mu is None else np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (E,)))
+            ptr = lambda a: None if a is None else ctypes.c_void_p(a.ctypes.data)
+            check(lib().pfg_set_component(self._h, k, mat, ptr(lv), ptr(mv), ptr(packed), len(vals), ptr(c21),
+                                          PFG_MEM_HOST), self._h, "pfg_set_component")
+        sel = None
+        if element_component is not None:
+            sel = np.ascontiguousarray(np.asarray(element_component, dtype=np.int32).ravel())
+            if sel.size != E:
+                raise ValueError(f"element_component must have {E} entries")
+        check(lib().pfg_set_composite(self._h, len(components), None if sel is None else ctypes.c_void_p(sel.ctypes.data)),
+              self._h, "pfg_set_composite")
+        self.material = "MultiModels" if sel is not None else "MaterialSum"
+
     def _ogden_params(self, formulation, params):
         """The flat pfg_set_material_params list of an Ogden formulation: alphas, mus, Ds
         (three lists of K terms), or c, m (two lists of K terms) and k."""

@@ -80,6 +80,25 @@ struct pfg_context
 	double *d_hooke = nullptr;
 	double *h_cg_sc = nullptr;
 	int *d_err = nullptr; // set by a kernel whose bounded wait gave up (DevMesh::err)
+	// compositions of formulations (pfg_set_component / pfg_set_composite): each
+	// component's material and parameters; the component of every element (MultiModels)
+	// or none (MaterialSum); per-component scratch of the element kernels
+	struct Component
+	{
+		int mat = -1;
+		double2 *lame = nullptr; // NULL: the context's Lame parameters
+		double4 *mpar = nullptr;
+		int n_mpar = 0, terms = 0;
+		double *hooke = nullptr;
+	};
+	Component comps[PFG_MAX_COMPONENTS];
+	int n_comps = 0;
+	bool composite = false;
+	int *d_elem_comp = nullptr;
+	double *d_comp_e = nullptr, *d_comp_eacc = nullptr; // per-element energies: one component's, combined
+	double *d_comp_vec = nullptr;                       // one component's gradient slots
+	double *d_comp_stage = nullptr;                     // one component's FP64 block triangles
+	unsigned long long *d_comp_inverted = nullptr;      // inverted counts of components after the first
 	std::string err;
 };
 
@@ -177,6 +196,9 @@ bool material_params_fit(int mat, int n, int *terms)
 // parameterised ones need their parameters.
 int check_material_prec(pfg_context *c, int prec)
 {
+	if (c->composite)
+		return prec == PFG_FP64 ? PFG_OK
+								: fail(c, PFG_ERR_UNSUPPORTED, "compositions of formulations are assembled in PFG_FP64 only");
 	if (c->m.mat != PFG_MAT_NEOHOOKEAN && prec != PFG_FP64)
 		return fail(c, PFG_ERR_UNSUPPORTED, "only PFG_FP64 is implemented for materials other than NeoHookean");
 	int terms = 0;
@@ -549,6 +571,92 @@ int build_dirichlet(pfg_context *c)
 	return PFG_OK;
 }
 
+// the DevMesh of component k: the context's mesh with the component's material
+DevMesh component_mesh(const pfg_context *c, int k)
+{
+	DevMesh mk = c->m;
+	const auto &comp = c->comps[k];
+	mk.mat = comp.mat;
+	if (comp.lame) mk.lame = comp.lame;
+	mk.mpar = comp.mpar;
+	mk.mterms = comp.terms;
+	mk.hooke = comp.hooke;
+	return mk;
+}
+
+int ensure_composite_scratch(pfg_context *c, bool energy, bool gradient, bool hessian)
+{
+	const size_t E = std::max(c->m.E, 1);
+	if (!c->d_comp_inverted) PFG_CUDA(c, cudaMalloc(&c->d_comp_inverted, sizeof(unsigned long long)));
+	if (energy && !c->d_comp_e)
+	{
+		PFG_CUDA(c, cudaMalloc(&c->d_comp_e, sizeof(double) * E));
+		PFG_CUDA(c, cudaMalloc(&c->d_comp_eacc, sizeof(double) * E));
+	}
+	if (gradient && !c->d_comp_vec)
+		PFG_CUDA(c, cudaMalloc(&c->d_comp_vec, sizeof(double) * E * std::max(c->n, c->ng) * 4));
+	if (hessian && !c->d_comp_stage) PFG_CUDA(c, cudaMalloc(&c->d_comp_stage, sizeof(double) * E * tri_pad(c->n)));
+	return PFG_OK;
+}
+
+// Scratch of component k: components after the first count their inverted elements
+// elsewhere (every component evaluates every element)
+Scratch component_scratch(const pfg_context *c, int k)
+{
+	Scratch sk = c->sc;
+	if (k > 0) sk.inverted = c->d_comp_inverted;
+	return sk;
+}
+
+// composite energies: per element (per_element) or their deterministic total, into dst
+int composite_energy(pfg_context *c, const double *du, bool per_element, double *dst)
+{
+	int st;
+	if ((st = ensure_composite_scratch(c, true, false, false))) return st;
+	double *acc = per_element ? dst : c->d_comp_eacc;
+	for (int k = 0; k < c->n_comps; ++k)
+	{
+		PFG_CUDA(c, launch_energy(component_mesh(c, k), du, PFG_FP64, true, c->d_comp_e, component_scratch(c, k), c->stream));
+		PFG_CUDA(c, launch_combine_elements(acc, c->d_comp_e, 1, c->m.E, c->d_elem_comp, k, k == 0, c->stream));
+	}
+	if (!per_element) PFG_CUDA(c, launch_sum_array(acc, c->m.E, dst, c->sc, c->stream));
+	return PFG_OK;
+}
+
+// composite gradient (3N) into dst
+int composite_gradient(pfg_context *c, const double *du, double *dst)
+{
+	int st;
+	if ((st = ensure_composite_scratch(c, false, true, false))) return st;
+	const long long n_inc = (long long)c->m.E * c->n;
+	for (int k = 0; k < c->n_comps; ++k)
+	{
+		Scratch sk = component_scratch(c, k);
+		sk.vec_stage = c->d_comp_vec;
+		PFG_CUDA(c, launch_gradient_stage(component_mesh(c, k), du, sk, c->stream));
+		PFG_CUDA(c, launch_combine_slots(c->d_vec_stage, c->d_comp_vec, n_inc, c->n, c->m.inc_eb, c->d_elem_comp, k, k == 0,
+										 c->stream));
+	}
+	PFG_CUDA(c, launch_gradient_gather(c->m, c->d_vec_stage, dst, c->stream));
+	return PFG_OK;
+}
+
+// composite Hessian into the pattern p: every component's FP64 block triangles combined
+// per element, then projected (optionally) and scattered
+int composite_hessian(pfg_context *c, const DevPattern &p, const double *du, int project_psd)
+{
+	int st;
+	if ((st = ensure_composite_scratch(c, false, false, true))) return st;
+	double *acc = static_cast<double *>(c->d_hess_stage[0]);
+	for (int k = 0; k < c->n_comps; ++k)
+	{
+		PFG_CUDA(c, launch_fp64_blocks(component_mesh(c, k), du, c->d_comp_stage, c->stream));
+		PFG_CUDA(c, launch_combine_elements(acc, c->d_comp_stage, tri_pad(c->n), c->m.E, c->d_elem_comp, k, k == 0, c->stream));
+	}
+	PFG_CUDA(c, launch_fp64_finish(c->m, p, acc, project_psd != 0, c->stream));
+	return PFG_OK;
+}
+
 void free_all(pfg_context *c)
 {
 	void *ptrs[] = {c->d_conn, c->d_gconn, c->d_X, c->d_lame, c->d_outer, c->d_inner, c->d_values, c->d_contrib, c->d_blk_rel, c->d_eb_inc, c->d_g_eb_inc,
@@ -568,6 +676,15 @@ void free_all(pfg_context *c)
 	if (c->d_rho) cudaFree(c->d_rho);
 	if (c->d_mpar) cudaFree(c->d_mpar);
 	if (c->d_err) cudaFree(c->d_err);
+	for (auto &k : c->comps)
+	{
+		if (k.lame) cudaFree(k.lame);
+		if (k.mpar) cudaFree(k.mpar);
+		if (k.hooke) cudaFree(k.hooke);
+	}
+	void *cptrs[] = {c->d_elem_comp, c->d_comp_e, c->d_comp_eacc, c->d_comp_vec, c->d_comp_stage, c->d_comp_inverted};
+	for (void *p : cptrs)
+		if (p) cudaFree(p);
 }
 } // namespace
 
@@ -746,6 +863,7 @@ int pfg_set_material(pfg_context *c, int material)
 	if (!c || material < PFG_MAT_NEOHOOKEAN || material > PFG_MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC)
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
 	c->m.mat = material;
+	c->composite = false;
 	return PFG_OK;
 }
 
@@ -800,6 +918,96 @@ int pfg_set_material_params(pfg_context *c, const double *params, int n_params, 
 	return PFG_OK;
 }
 
+int pfg_set_component(pfg_context *c, int k, int material, const double *lambda, const double *mu, const double *params,
+					  int n_params, const double *c21, int mem)
+{
+	if (!c || !check_mem(mem) || k < 0 || k >= PFG_MAX_COMPONENTS || material < PFG_MAT_NEOHOOKEAN ||
+		material > PFG_MAT_MOONEY_RIVLIN_3PARAM_SYMBOLIC || (lambda == nullptr) != (mu == nullptr) || n_params < 0 ||
+		n_params > 8)
+		return fail(c, PFG_ERR_INVALID, "bad arguments");
+	int terms = 0;
+	if (material_takes_params(material) && !(n_params > 0 && params && material_params_fit(material, n_params, &terms)))
+		return fail(c, PFG_ERR_INVALID, "the component's material takes parameters of another count");
+	const bool tensor = material == PFG_MAT_HOOKE || material == PFG_MAT_SAINT_VENANT_TENSOR;
+	if (tensor && !c21) return fail(c, PFG_ERR_INVALID, "the component's material takes an elasticity tensor");
+	DeviceGuard g(c->device);
+	auto &comp = c->comps[k];
+	const size_t E = c->m.E;
+	comp.mat = material;
+	comp.terms = terms;
+	comp.n_mpar = material_takes_params(material) ? n_params : 0;
+	if (lambda && E)
+	{
+		if (!comp.lame) PFG_CUDA(c, cudaMalloc(&comp.lame, sizeof(double2) * E));
+		std::vector<double2> lm(E);
+		std::vector<double> hl, hm;
+		const double *pl = lambda, *pm = mu;
+		if (mem == PFG_MEM_DEVICE)
+		{
+			hl.resize(E);
+			hm.resize(E);
+			PFG_CUDA(c, cudaMemcpy(hl.data(), lambda, sizeof(double) * E, cudaMemcpyDeviceToHost));
+			PFG_CUDA(c, cudaMemcpy(hm.data(), mu, sizeof(double) * E, cudaMemcpyDeviceToHost));
+			pl = hl.data();
+			pm = hm.data();
+		}
+		for (size_t e = 0; e < E; ++e) lm[e] = make_double2(pl[e], pm[e]);
+		PFG_CUDA(c, cudaMemcpy(comp.lame, lm.data(), sizeof(double2) * E, cudaMemcpyHostToDevice));
+	}
+	else if (comp.lame)
+	{
+		cudaFree(comp.lame);
+		comp.lame = nullptr;
+	}
+	if (comp.n_mpar && E)
+	{
+		constexpr size_t PER = 8;
+		if (!comp.mpar) PFG_CUDA(c, cudaMalloc(&comp.mpar, sizeof(double) * PER * E));
+		std::vector<double> src((size_t)n_params * E), pv(PER * E, 0.0);
+		if (mem == PFG_MEM_DEVICE)
+			PFG_CUDA(c, cudaMemcpy(src.data(), params, sizeof(double) * src.size(), cudaMemcpyDeviceToHost));
+		else
+			std::copy(params, params + src.size(), src.begin());
+		for (size_t e = 0; e < E; ++e)
+			for (int q = 0; q < n_params; ++q) pv[PER * e + q] = src[(size_t)q * E + e];
+		PFG_CUDA(c, cudaMemcpy(comp.mpar, pv.data(), sizeof(double) * PER * E, cudaMemcpyHostToDevice));
+	}
+	if (tensor)
+	{
+		double full[36];
+		for (int i = 0, q = 0; i < 6; ++i)
+			for (int j = i; j < 6; ++j, ++q) full[6 * i + j] = full[6 * j + i] = c21[q];
+		if (!comp.hooke) PFG_CUDA(c, cudaMalloc(&comp.hooke, sizeof(full)));
+		PFG_CUDA(c, cudaMemcpy(comp.hooke, full, sizeof(full), cudaMemcpyHostToDevice));
+	}
+	return PFG_OK;
+}
+
+int pfg_set_composite(pfg_context *c, int n_components, const int *element_component)
+{
+	if (!c || n_components < 1 || n_components > PFG_MAX_COMPONENTS) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	for (int k = 0; k < n_components; ++k)
+		if (c->comps[k].mat < 0) return fail(c, PFG_ERR_STATE, "a component is not set (pfg_set_component)");
+	DeviceGuard g(c->device);
+	const int E = c->m.E;
+	if (element_component)
+	{
+		for (int e = 0; e < E; ++e)
+			if (element_component[e] < 0 || element_component[e] >= n_components)
+				return fail(c, PFG_ERR_INVALID, "element_component out of range");
+		if (!c->d_elem_comp) PFG_CUDA(c, cudaMalloc(&c->d_elem_comp, sizeof(int) * std::max(E, 1)));
+		if (E) PFG_CUDA(c, cudaMemcpy(c->d_elem_comp, element_component, sizeof(int) * E, cudaMemcpyHostToDevice));
+	}
+	else if (c->d_elem_comp)
+	{
+		cudaFree(c->d_elem_comp);
+		c->d_elem_comp = nullptr;
+	}
+	c->n_comps = n_components;
+	c->composite = true;
+	return PFG_OK;
+}
+
 int pfg_set_lame(pfg_context *c, const double *lambda, const double *mu, int mem)
 {
 	if (!c || !check_mem(mem)) return fail(c, PFG_ERR_INVALID, "bad arguments");
@@ -849,7 +1057,12 @@ int pfg_energy(pfg_context *c, const double *u, int mem, int prec, double *out)
 	if ((st = stage_in(c, u, mem, c->d_u, 3 * (size_t)c->m.N, &du))) return st;
 	PFG_CUDA(c, cudaMemsetAsync(c->sc.inverted, 0, sizeof(unsigned long long), c->stream));
 	double *dst = mem == PFG_MEM_DEVICE ? out : c->d_result;
-	PFG_CUDA(c, launch_energy(c->m, du, prec, false, dst, c->sc, c->stream));
+	if (c->composite)
+	{
+		if ((st = composite_energy(c, du, false, dst))) return st;
+	}
+	else
+		PFG_CUDA(c, launch_energy(c->m, du, prec, false, dst, c->sc, c->stream));
 	if (mem == PFG_MEM_HOST) return finish_host(c, out, c->d_result, 1);
 	return PFG_OK;
 }
@@ -866,7 +1079,12 @@ int pfg_energy_per_element(pfg_context *c, const double *u, int mem, int prec, d
 	if ((st = stage_in(c, u, mem, c->d_u, 3 * (size_t)c->m.N, &du))) return st;
 	PFG_CUDA(c, cudaMemsetAsync(c->sc.inverted, 0, sizeof(unsigned long long), c->stream));
 	double *dst = mem == PFG_MEM_DEVICE ? out : c->d_out;
-	PFG_CUDA(c, launch_energy(c->m, du, prec, true, dst, c->sc, c->stream));
+	if (c->composite)
+	{
+		if ((st = composite_energy(c, du, true, dst))) return st;
+	}
+	else
+		PFG_CUDA(c, launch_energy(c->m, du, prec, true, dst, c->sc, c->stream));
 	if (mem == PFG_MEM_HOST) return finish_host(c, out, c->d_out, c->m.E);
 	return PFG_OK;
 }
@@ -884,7 +1102,12 @@ int pfg_gradient(pfg_context *c, const double *u, int mem, int prec, double *gou
 	PFG_CUDA(c, cudaMemsetAsync(c->sc.inverted, 0, sizeof(unsigned long long), c->stream));
 	double *dst = mem == PFG_MEM_DEVICE ? gout : c->d_out;
 	if ((st = ensure_vec_stage(c))) return st;
-	PFG_CUDA(c, launch_gradient(c->m, du, prec, dst, c->sc, c->stream));
+	if (c->composite)
+	{
+		if ((st = composite_gradient(c, du, dst))) return st;
+	}
+	else
+		PFG_CUDA(c, launch_gradient(c->m, du, prec, dst, c->sc, c->stream));
 	if (mem == PFG_MEM_HOST) return finish_host(c, gout, c->d_out, ndof);
 	return PFG_OK;
 }
@@ -929,7 +1152,12 @@ int pfg_hessian(pfg_context *c, const double *u, int mem, int prec, int project_
 	// device output goes straight into the caller's array; otherwise into the context's
 	DevPattern p = c->pat;
 	if (values && mem == PFG_MEM_DEVICE) p.values = values;
-	PFG_CUDA(c, launch_hessian(c->m, p, du, prec, project_psd, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
+	if (c->composite)
+	{
+		if ((st = composite_hessian(c, p, du, project_psd))) return st;
+	}
+	else
+		PFG_CUDA(c, launch_hessian(c->m, p, du, prec, project_psd, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
 	if (values && mem == PFG_MEM_HOST) return finish_host(c, values, c->d_values, c->pat.nnz);
 	if (mem == PFG_MEM_HOST)
 	{
@@ -970,7 +1198,7 @@ int pfg_material_vjp(pfg_context *c, const double *u, const double *p, int mem, 
 	if (!c || !check_mem(mem) || (c->m.E && !out) || (c->m.N && (!u || !p))) return fail(c, PFG_ERR_INVALID, "bad arguments");
 	// compute_dstress_dmu_dlambda exists for NeoHookean and LinearElasticity (and
 	// FixedCorotational, not built); the reference throws for the others
-	if (c->m.mat != PFG_MAT_NEOHOOKEAN && c->m.mat != PFG_MAT_LINEAR_ELASTICITY)
+	if (c->composite || (c->m.mat != PFG_MAT_NEOHOOKEAN && c->m.mat != PFG_MAT_LINEAR_ELASTICITY))
 		return fail(c, PFG_ERR_UNSUPPORTED, "the material derivative exists for NeoHookean and LinearElasticity only");
 	DeviceGuard g(c->device);
 	const size_t ndof = 3 * (size_t)c->m.N;
@@ -991,7 +1219,8 @@ int pfg_shape_vjp(pfg_context *c, const double *u, const double *p, int mem, int
 		return fail(c, PFG_ERR_INVALID, "bad arguments");
 	// compute_stress_grad_multiply_mat exists for every formulation built here but
 	// SaintVenant and HookeLinearElasticity, whose reference assemblers throw
-	if (c->m.mat == PFG_MAT_SAINT_VENANT || c->m.mat == PFG_MAT_SAINT_VENANT_TENSOR || c->m.mat == PFG_MAT_HOOKE)
+	if (c->composite || c->m.mat == PFG_MAT_SAINT_VENANT || c->m.mat == PFG_MAT_SAINT_VENANT_TENSOR ||
+		c->m.mat == PFG_MAT_HOOKE)
 		return fail(c, PFG_ERR_UNSUPPORTED, "the shape derivative does not exist for SaintVenant and HookeLinearElasticity");
 	if (int st_m = check_material_prec(c, prec)) return st_m;
 	DeviceGuard g(c->device);
@@ -1084,7 +1313,12 @@ int pfg_hessian_reduced(pfg_context *c, const double *u, int mem, int prec, int 
 	p.values = (values && mem == PFG_MEM_DEVICE) ? values : c->d_red_values;
 	p.red_col_start = c->d_red_col_start;
 	p.red_row_off = c->d_red_row_off;
-	PFG_CUDA(c, launch_hessian(c->m, p, du, prec, project_psd, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
+	if (c->composite)
+	{
+		if ((st = composite_hessian(c, p, du, project_psd))) return st;
+	}
+	else
+		PFG_CUDA(c, launch_hessian(c->m, p, du, prec, project_psd, c->d_hess_stage[prec == PFG_FP64 ? 0 : 1], c->stream));
 	if (values && mem == PFG_MEM_HOST) return finish_host(c, values, c->d_red_values, c->red_nnz);
 	if (mem == PFG_MEM_HOST) PFG_CUDA(c, cudaStreamSynchronize(c->stream));
 	return PFG_OK;
@@ -1104,7 +1338,12 @@ int pfg_gradient_reduced(pfg_context *c, const double *u, int mem, int prec, dou
 	if ((st = stage_in(c, u, mem, c->d_u, ndof, &du))) return st;
 	PFG_CUDA(c, cudaMemsetAsync(c->sc.inverted, 0, sizeof(unsigned long long), c->stream));
 	if ((st = ensure_vec_stage(c))) return st;
-	PFG_CUDA(c, launch_gradient(c->m, du, prec, c->d_full_tmp, c->sc, c->stream));
+	if (c->composite)
+	{
+		if ((st = composite_gradient(c, du, c->d_full_tmp))) return st;
+	}
+	else
+		PFG_CUDA(c, launch_gradient(c->m, du, prec, c->d_full_tmp, c->sc, c->stream));
 	double *dst = mem == PFG_MEM_DEVICE ? g_out : c->d_out;
 	PFG_CUDA(c, launch_gather_free(c->d_full_tmp, c->d_free, c->n_free, dst, c->stream));
 	if (mem == PFG_MEM_HOST) return finish_host(c, g_out, c->d_out, c->n_free);

@@ -115,6 +115,20 @@ cudaError_t launch_mass(const DevMesh &m, const DevPattern &p, const double *rho
 // pattern (outer, inner), each summed in ascending column order
 cudaError_t launch_lump_rows(int n_nodes, const int *outer, const int *inner, const double *vals, double *diag,
 							 cudaStream_t s);
+// Compositions of formulations (MaterialSum, MultiModels): FP64 pass 1 alone and the
+// projection + scatter alone; the gradient's slots alone and their gather; per-element
+// and per-slot combination of a component's buffer into the accumulated one (sel:
+// component of every element, NULL = all elements; first: start from zero); the
+// deterministic sum of an array (Scratch partials and ticket)
+cudaError_t launch_fp64_blocks(const DevMesh &m, const double *u, double *stage, cudaStream_t s);
+cudaError_t launch_fp64_finish(const DevMesh &m, const DevPattern &p, double *stage, bool project_psd, cudaStream_t s);
+cudaError_t launch_gradient_stage(const DevMesh &m, const double *u, const Scratch &sc, cudaStream_t s);
+cudaError_t launch_gradient_gather(const DevMesh &m, const double *stage, double *g, cudaStream_t s);
+cudaError_t launch_combine_elements(double *acc, const double *src, long long per, int E, const int *sel, int comp,
+									bool first, cudaStream_t s);
+cudaError_t launch_combine_slots(double *acc, const double *src, long long n_inc, int n, const int *inc_eb, const int *sel,
+								 int comp, bool first, cudaStream_t s);
+cudaError_t launch_sum_array(const double *x, int n, double *out, const Scratch &sc, cudaStream_t s);
 // DenseMatrixCache: the values of the Hessian pattern into a dense column-major
 // ndof x ndof array (zeros outside the pattern)
 cudaError_t launch_csc_to_dense(int ndof, const int *outer, const int *inner, const double *vals, double *dense,

@@ -2458,6 +2458,169 @@ cudaError_t launch_lump_rows(int n_nodes, const int *outer, const int *inner, co
 	return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Compositions of formulations: MaterialSum (SumModel.cpp:43-78, the element
+// energies, gradients and Hessians of several formulations added) and MultiModels
+// (MultiModel.cpp:35-58, the formulation chosen per element).  Each component runs
+// its own FP64 element kernels into its own per-element buffers; the combination
+// below adds them per element (components ascending), keeping of a MultiModels
+// element only its own component's values; the usual tail (energy reduction,
+// incidence gather, PSD projection, scatter) then runs on the combined buffers.
+// ---------------------------------------------------------------------------
+// acc[e * per + i] (=|+=) src[e * per + i] for elements e whose component is comp
+// (every element when sel is NULL); first: acc starts from zero
+__global__ void k_combine_elements(double *__restrict__ acc, const double *__restrict__ src, long long per, int E,
+								   const int *__restrict__ sel, int comp, int first)
+{
+	const long long total = per * (long long)E;
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
+	{
+		const int e = (int)(i / per);
+		const bool on = sel == nullptr || __ldg(sel + e) == comp;
+		const double v = on ? __ldg(src + i) : 0.0;
+		acc[i] = first ? v : acc[i] + v;
+	}
+}
+
+// the same over the 32-byte incidence slots of the gradient stage (slot k belongs to
+// element inc_eb[k] / n)
+__global__ void k_combine_slots(double *__restrict__ acc, const double *__restrict__ src, long long n_inc, int n,
+								const int *__restrict__ inc_eb, const int *__restrict__ sel, int comp, int first)
+{
+	for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n_inc; k += (long long)gridDim.x * blockDim.x)
+	{
+		const bool on = sel == nullptr || __ldg(sel + __ldg(inc_eb + k) / n) == comp;
+#pragma unroll
+		for (int c = 0; c < 4; ++c)
+		{
+			const double v = on ? __ldg(src + 4 * k + c) : 0.0;
+			acc[4 * k + c] = first ? v : acc[4 * k + c] + v;
+		}
+	}
+}
+
+// the sum of x[0..n), fixed order (grid-stride per thread, block tree, block
+// partials in index order by the last block): deterministic
+template <int NT>
+__global__ void __launch_bounds__(NT) k_sum_array(const double *__restrict__ x, int n, double *__restrict__ partials,
+												  double *__restrict__ result, unsigned int *ticket)
+{
+	double v = 0.0;
+	for (int i = blockIdx.x * NT + threadIdx.x; i < n; i += gridDim.x * NT) v += __ldg(x + i);
+	reduce_to_result<NT>(v, partials, result, ticket);
+}
+
+static inline int combine_blocks(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 16); }
+
+cudaError_t launch_combine_elements(double *acc, const double *src, long long per, int E, const int *sel, int comp,
+									bool first, cudaStream_t s)
+{
+	if (per * (long long)E > 0)
+		k_combine_elements<<<combine_blocks(per * (long long)E), 256, 0, s>>>(acc, src, per, E, sel, comp, first ? 1 : 0);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_combine_slots(double *acc, const double *src, long long n_inc, int n, const int *inc_eb, const int *sel,
+								 int comp, bool first, cudaStream_t s)
+{
+	if (n_inc > 0) k_combine_slots<<<combine_blocks(n_inc), 256, 0, s>>>(acc, src, n_inc, n, inc_eb, sel, comp, first ? 1 : 0);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_sum_array(const double *x, int n, double *out, const Scratch &sc, cudaStream_t s)
+{
+	constexpr int NT = 256;
+	if (n <= 0) return cudaMemsetAsync(out, 0, sizeof(double), s);
+	const int nb = std::min(blocks_for(n, NT), sc.max_blocks);
+	k_sum_array<NT><<<nb, NT, 0, s>>>(x, n, sc.partials, out, sc.ticket);
+	return cudaGetLastError();
+}
+
+// pass 1 alone in FP64: the element block triangles of the context's material
+cudaError_t launch_fp64_blocks(const DevMesh &m, const double *u, double *stage, cudaStream_t s)
+{
+	if (m.E <= 0) return cudaSuccess;
+	if (m.mat >= MAT_FIRST_AD) return launch_ad_blocks(m, u, stage, s);
+	auto gen = [&](auto el) -> cudaError_t {
+		using EL = decltype(el);
+		constexpr int WPB = 4;
+		const size_t bytes = WPB * sizeof(GenWarp<EL>);
+		const int nb = std::min((m.E + WPB - 1) / WPB, 148 * 32);
+		cudaError_t e;
+		if (m.mat == MAT_ISO_NEOHOOKEAN)
+		{
+			e = cudaFuncSetAttribute(k_gen_blocks<EL, MAT_ISO_NEOHOOKEAN, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+			if (e == cudaSuccess) k_gen_blocks<EL, MAT_ISO_NEOHOOKEAN, WPB><<<nb, WPB * 32, bytes, s>>>(m, u, stage);
+		}
+		else
+		{
+			e = cudaFuncSetAttribute(k_gen_blocks<EL, MAT_SAINT_VENANT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+			if (e == cudaSuccess) k_gen_blocks<EL, MAT_SAINT_VENANT, WPB><<<nb, WPB * 32, bytes, s>>>(m, u, stage);
+		}
+		return e != cudaSuccess ? e : cudaGetLastError();
+	};
+	auto nh = [&](auto el) -> cudaError_t {
+		using EL = decltype(el);
+		using TL = EcTile<EL, double>;
+		const size_t bytes1 = sizeof(EcSmem<EL, double, double>);
+		cudaError_t e = cudaFuncSetAttribute(k_hessian_blocks<EL, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes1);
+		if (e != cudaSuccess) return e;
+		k_hessian_blocks<EL, double, double><<<(m.E + TL::TE - 1) / TL::TE, TL::NT, bytes1, s>>>(m, u, stage, 0, m.E);
+		return cudaGetLastError();
+	};
+	switch (m.et)
+	{
+	case 1: return m.mat ? gen(P1Tet{}) : nh(P1Tet{});
+	case 2: return m.mat ? gen(P2Tet{}) : nh(P2Tet{});
+	case 3: return m.mat ? gen(Q1Hex{}) : nh(Q1Hex{});
+	}
+	return cudaErrorInvalidValue;
+}
+
+// projection (optional) and scatter of FP64 block triangles
+cudaError_t launch_fp64_finish(const DevMesh &m, const DevPattern &p, double *stage, bool project_psd, cudaStream_t s)
+{
+	if (p.nnz == 0) return cudaSuccess;
+	switch (m.et)
+	{
+	case 1: return finish_fp64_hessian<P1Tet>(m, p, stage, project_psd, s);
+	case 2: return finish_fp64_hessian<P2Tet>(m, p, stage, project_psd, s);
+	case 3: return finish_fp64_hessian<Q1Hex>(m, p, stage, project_psd, s);
+	}
+	return cudaErrorInvalidValue;
+}
+
+// the gradient's incidence slots alone (FP64), and their gather
+cudaError_t launch_gradient_stage(const DevMesh &m, const double *u, const Scratch &sc, cudaStream_t s)
+{
+	if (m.E == 0) return cudaSuccess;
+	if (m.mat >= MAT_FIRST_AD) return launch_ad_gradient_stage(m, u, sc, s);
+	if (m.mat != 0)
+		switch (m.et)
+		{
+		case 1: gen_gradient_mat<P1Tet>(m, u, sc, s); break;
+		case 2: gen_gradient_mat<P2Tet>(m, u, sc, s); break;
+		case 3: gen_gradient_mat<Q1Hex>(m, u, sc, s); break;
+		default: return cudaErrorInvalidValue;
+		}
+	else
+		switch (m.et)
+		{
+		case 1: gradient_t<P1Tet, double>(m, u, sc, s); break;
+		case 2: gradient_t<P2Tet, double>(m, u, sc, s); break;
+		case 3: gradient_t<Q1Hex, double>(m, u, sc, s); break;
+		default: return cudaErrorInvalidValue;
+		}
+	return cudaGetLastError();
+}
+
+cudaError_t launch_gradient_gather(const DevMesh &m, const double *stage, double *g, cudaStream_t s)
+{
+	if (m.E == 0) return cudaMemsetAsync(g, 0, sizeof(double) * 3 * (size_t)m.N, s);
+	launch_vec_gather(m.N, m.inc_off, (long long)m.E * nodes_of(m.et), stage, g, s);
+	return cudaGetLastError();
+}
+
 // DenseMatrixCache (utils/MatrixCache.hpp:136-177): the matrix in the Hessian pattern
 // as a dense column-major ndof x ndof array.  One warp per column; every entry of
 // the pattern is written once, the rest of the column is zero (cleared before).
