@@ -1157,7 +1157,7 @@ __device__ __forceinline__ void psd_reflect(const PW &S, double (&y)[M], int i)
 
 // 3 CTAs of 4 warps per SM: at most 168 registers a thread (a few spill for P2)
 template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 3) k_project_psd(DevMesh m, T *__restrict__ stage)
+__global__ void __launch_bounds__(WARPS * 32, EL::ET == 1 ? 5 : 3) k_project_psd(DevMesh m, T *__restrict__ stage)
 {
 	using W = PsdWarp<EL>;
 	constexpr int N = EL::N, M = W::M;
