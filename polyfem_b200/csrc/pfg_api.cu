@@ -80,6 +80,7 @@ struct pfg_context
 	double *d_hooke = nullptr;
 	double *h_cg_sc = nullptr;
 	int *d_err = nullptr; // set by a kernel whose bounded wait gave up (DevMesh::err)
+	int *d_work = nullptr; // DevMesh::work
 	// compositions of formulations (pfg_set_component / pfg_set_composite): each
 	// component's material and parameters; the component of every element (MultiModels)
 	// or none (MaterialSum); per-component scratch of the element kernels
@@ -676,6 +677,7 @@ void free_all(pfg_context *c)
 	if (c->d_rho) cudaFree(c->d_rho);
 	if (c->d_mpar) cudaFree(c->d_mpar);
 	if (c->d_err) cudaFree(c->d_err);
+	if (c->d_work) cudaFree(c->d_work);
 	for (auto &k : c->comps)
 	{
 		if (k.lame) cudaFree(k.lame);
@@ -822,6 +824,7 @@ int pfg_create(const pfg_mesh_desc *d, pfg_context **out)
 	CREATE_CUDA(cudaMalloc(&c->d_result, sizeof(double)));
 	CREATE_CUDA(cudaMalloc(&c->d_err, sizeof(int)));
 	CREATE_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+	CREATE_CUDA(cudaMalloc(&c->d_work, sizeof(int)));
 	CREATE_CUDA(hessian_kernel_setup(c->device));
 #undef CREATE_CUDA
 	c->m.conn = c->d_conn;
@@ -835,6 +838,7 @@ int pfg_create(const pfg_mesh_desc *d, pfg_context **out)
 	c->m.X = c->d_X;
 	c->m.lame = c->d_lame;
 	c->m.err = c->d_err;
+	c->m.work = c->d_work;
 	*out = c;
 	return PFG_OK;
 }

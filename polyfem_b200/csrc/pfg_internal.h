@@ -40,6 +40,7 @@ struct DevMesh
 	const int *ginc_eb = nullptr;
 	const int *g_eb_inc = nullptr; // [E*n_g] inverse of ginc_eb (aliases eb_inc when isoparametric)
 	int *err = nullptr; // set to 1 by a kernel whose bounded wait gave up (the context reports it)
+	int *work = nullptr; // element counter of the PSD projection's persistent warps (cleared before each launch)
 };
 
 // Element Hessian staging: element e's symmetric node blocks (a, b), a <= b, as one

@@ -1155,19 +1155,15 @@ __device__ __forceinline__ void psd_reflect(const PW &S, double (&y)[M], int i)
 	}
 }
 
-// 3 CTAs of 4 warps per SM: at most 168 registers a thread (a few spill for P2)
-template <class EL, class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, EL::ET == 1 ? 5 : 3) k_project_psd(DevMesh m, T *__restrict__ stage)
+// The projection of element e by one warp (all 32 lanes, converged on entry and
+// on every return; S is the warp's shared workspace)
+template <class EL, class T>
+__device__ __forceinline__ void psd_element(PsdWarp<EL> &S, T *__restrict__ stage, int e, int lane)
 {
 	using W = PsdWarp<EL>;
 	constexpr int N = EL::N, M = W::M;
 	constexpr unsigned FULL = 0xffffffffu;
 	static_assert(M <= 32, "one lane per row");
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	W &S = reinterpret_cast<W *>(smem_raw)[threadIdx.x >> 5];
-	const int lane = threadIdx.x & 31;
-	const int e = blockIdx.x * WARPS + (threadIdx.x >> 5);
-	if (e >= m.E) return;
 	// lane i = 3a + r < M owns row i of the element matrix: A[3a+r][3b+c] is value
 	// 3c + r of staged block (a, b) for a <= b, value 3r + c of block (b, a) for a > b
 	T *tri = stage + (size_t)e * tri_pad(N);
@@ -1404,6 +1400,47 @@ __global__ void __launch_bounds__(WARPS * 32, EL::ET == 1 ? 5 : 3) k_project_psd
 #pragma unroll
 			for (int c = 0; c < 3; ++c)
 				if (b >= ra) tri[at(b, c)] = T(r[3 * b + c]); // each stored value once
+	}
+}
+
+// One warp per element, 3 CTAs of 4 warps per SM for P2 and Q1 and 5 for P1 (at most
+// 168 registers a thread, a few spill for P2).  For P1 the warps are persistent:
+// each takes the next element from the counter m.work (zero at launch) until none
+// is left, so a warp whose element is already PSD, or has few negative eigenvalues,
+// goes on to the next one instead of idling until the other warps of its CTA
+// finish (P1 48^3: 5.51 -> 4.97 ms).  The larger P2 and Q1 kernels run one element
+// per warp: persistent warps drift apart in phase and were slower there (P2 40^3
+// 16.3 -> 17.6 ms).  Each element's arithmetic does not depend on which warp
+// projects it.
+template <class EL>
+__host__ __device__ constexpr bool psd_persistent() { return EL::ET == 1; }
+
+template <class EL, class T, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, EL::ET == 1 ? 5 : 3) k_project_psd(DevMesh m, T *__restrict__ stage)
+{
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	PsdWarp<EL> &S = reinterpret_cast<PsdWarp<EL> *>(smem_raw)[threadIdx.x >> 5];
+	const int lane = threadIdx.x & 31;
+	if constexpr (!psd_persistent<EL>())
+	{
+		const int e = blockIdx.x * WARPS + (threadIdx.x >> 5);
+		if (e < m.E) psd_element<EL, T>(S, stage, e, lane);
+	}
+	else
+	{
+		for (;;)
+		{
+			int e = 0;
+			if (lane == 0) e = atomicAdd(m.work, 1);
+			e = __shfl_sync(0xffffffffu, e, 0);
+			if (e >= m.E) return;
+			// an opaque copy of the lane keeps the lane-dependent offsets inside the
+			// element (hoisted out of the loop they would stay live and spill)
+			int ln = lane;
+			asm volatile("" : "+r"(ln));
+			psd_element<EL, T>(S, stage, e, ln);
+			__syncwarp();
+		}
 	}
 }
 
@@ -1778,6 +1815,39 @@ __global__ void __launch_bounds__(WPB * 32, gen_blocks_min_ctas<EL, MAT>())
 	}
 }
 
+// P1: one resident grid of persistent warps over all elements, m.work cleared on
+// the stream first; P2 and Q1: one warp per element
+template <class EL, class T>
+static cudaError_t launch_project_psd(const DevMesh &m, T *stage, cudaStream_t s)
+{
+	constexpr int PW = 4;
+	if (m.E <= 0) return cudaSuccess;
+	const size_t bytes_p = PW * sizeof(PsdWarp<EL>);
+	cudaError_t e = cudaFuncSetAttribute(k_project_psd<EL, T, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
+	if (e != cudaSuccess) return e;
+	const long long need = (m.E + PW - 1) / PW;
+	int grid = (int)need;
+	if constexpr (psd_persistent<EL>())
+	{
+		if (!m.work) return cudaErrorInvalidValue;
+		static int per_sm = 0; // resident CTAs per SM of this instance (the same on every B200)
+		if (per_sm == 0)
+		{
+			int nb = 0;
+			e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_project_psd<EL, T, PW>, PW * 32, bytes_p);
+			if (e != cudaSuccess) return e;
+			per_sm = nb > 0 ? nb : 1;
+		}
+		int dev = 0, sms = 0;
+		if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+		if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+		grid = (int)std::min<long long>(need, (long long)per_sm * sms);
+		if ((e = cudaMemsetAsync(m.work, 0, sizeof(int), s)) != cudaSuccess) return e;
+	}
+	k_project_psd<EL, T, PW><<<grid, PW * 32, bytes_p, s>>>(m, stage);
+	return cudaGetLastError();
+}
+
 // FP64 staged element triangles -> (PSD projection) -> CSC values: the tail of the
 // Hessian for every material other than NeoHookean
 template <class EL>
@@ -1785,13 +1855,10 @@ static cudaError_t finish_fp64_hessian(const DevMesh &m, const DevPattern &p, do
 									   cudaStream_t s)
 {
 	constexpr int WARPS = 8;
-	if (project_psd && m.E > 0)
+	if (project_psd)
 	{
-		constexpr int PW = 4;
-		const size_t bytes_p = PW * sizeof(PsdWarp<EL>);
-		cudaError_t e = cudaFuncSetAttribute(k_project_psd<EL, double, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
+		const cudaError_t e = launch_project_psd<EL, double>(m, stage, s);
 		if (e != cudaSuccess) return e;
-		k_project_psd<EL, double, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
 	}
 	const int ng = (m.N + WARPS - 1) / WARPS;
 	if (ng > 0) return launch_reduce<EL, double>(m, p, stage, s);
@@ -1952,13 +2019,10 @@ static cudaError_t hessian_two_pass(const DevMesh &m, const DevPattern &p, const
 	if (e != cudaSuccess) return e;
 	const int nb = (m.E + TL::TE - 1) / TL::TE;
 	if (nb > 0) k_hessian_blocks<EL, K, T><<<nb, TL::NT, bytes1, s>>>(m, u, stage, 0, m.E);
-	if (project_psd && m.E > 0)
+	if (project_psd)
 	{
-		constexpr int PW = 4;
-		const size_t bytes_p = PW * sizeof(PsdWarp<EL>);
-		e = cudaFuncSetAttribute(k_project_psd<EL, T, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
+		e = launch_project_psd<EL, T>(m, stage, s);
 		if (e != cudaSuccess) return e;
-		k_project_psd<EL, T, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
 	}
 	const int ng = (m.N + WARPS - 1) / WARPS;
 	if (ng > 0) return launch_reduce<EL, T>(m, p, stage, s);
@@ -1977,13 +2041,10 @@ static cudaError_t hessian_tc(const DevMesh &m, const DevPattern &p, const doubl
 	float *stage = static_cast<float *>(stage_v);
 	cudaError_t e = launch_hessian_blocks_tc(m, u, stage, s);
 	if (e != cudaSuccess) return e;
-	if (project_psd && m.E > 0)
+	if (project_psd)
 	{
-		constexpr int PW = 4;
-		const size_t bytes_p = PW * sizeof(PsdWarp<EL>);
-		e = cudaFuncSetAttribute(k_project_psd<EL, float, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes_p);
+		e = launch_project_psd<EL, float>(m, stage, s);
 		if (e != cudaSuccess) return e;
-		k_project_psd<EL, float, PW><<<(m.E + PW - 1) / PW, PW * 32, bytes_p, s>>>(m, stage);
 	}
 	const int ng = (m.N + WARPS - 1) / WARPS;
 	if (ng > 0) return launch_reduce<EL, float>(m, p, stage, s);
