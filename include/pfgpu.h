@@ -41,7 +41,8 @@ enum pfg_status
 	PFG_ERR_CUDA = 2,        /* a CUDA runtime call failed; see pfg_last_error */
 	PFG_ERR_OOM = 3,         /* device or host allocation failed */
 	PFG_ERR_UNSUPPORTED = 4, /* beyond an implementation limit (e.g. the 32-bit reduction plan) */
-	PFG_ERR_STATE = 5        /* call made in the wrong state (e.g. pattern not built) */
+	PFG_ERR_STATE = 5,       /* call made in the wrong state (e.g. pattern not built) */
+	PFG_ERR_NUMERIC = 6      /* the matrix is not positive definite (pfg_direct_factorize) */
 };
 
 enum pfg_elem_type
@@ -392,6 +393,33 @@ enum pfg_system
 };
 int pfg_cg_solve(pfg_context *ctx, int system, const double *values, const double *b, int mem, double tol,
                  int max_iter, int guess, double *x, int *iters, double *rel_res);
+
+/* Sparse direct solve on the device: the factorisation polysolve's direct choices
+ * compute for the Newton step's SPD system (Eigen::SimplicialLDLT, Cholmod or
+ * Pardiso at the reference's call sites: mesh/remesh/L2Projection.cpp:25-29,
+ * State.cpp:1562-1565), as a multifrontal Cholesky P A P^T = L L^T with a nested
+ * dissection ordering, in the three calls of polysolve's linear::Solver:
+ *   pfg_direct_analyze   (analyzePattern): orders and analyses the pattern of
+ *       `system` (PFG_SYS_FULL after pfg_hessian, PFG_SYS_REDUCED after
+ *       pfg_set_dirichlet; host work, then the maps go to the device).  Repeat it
+ *       when the pattern changes: pfg_set_dirichlet discards the reduced system's
+ *       analysis.  PFG_ERR_OOM when the dense fronts do not fit in device memory;
+ *   pfg_direct_factorize (factorize): factorises `values` (device memory, nnz
+ *       doubles of the analysed pattern, both triangles stored; the lower one is
+ *       read) or, with values == NULL, the system's values the last assembly left
+ *       in the context.  PFG_ERR_NUMERIC when the matrix is not positive definite
+ *       (Eigen's NumericalIssue): a non-positive or non-finite pivot;
+ *   pfg_direct_solve     (solve): x = A^-1 b for b and x in `mem` (x may be b).
+ * Every sum is taken in a fixed order, so factor and solution are bitwise
+ * deterministic.  pfg_direct_stats (after analyze) and pfg_direct_symbolic (any
+ * host pattern: full symmetric CSC of n columns with sorted rows; host only, no
+ * device) write six values: n, fronts, tree levels, doubles of the dense fronts,
+ * entries of L, largest front order. */
+int pfg_direct_analyze(pfg_context *ctx, int system);
+int pfg_direct_factorize(pfg_context *ctx, int system, const double *values);
+int pfg_direct_solve(pfg_context *ctx, int system, const double *b, int mem, double *x);
+int pfg_direct_stats(const pfg_context *ctx, long long *stats);
+int pfg_direct_symbolic(int n, const int *outer, const int *inner, long long *stats);
 
 /* ---------------------------------------------------------------------------
  * Allocation-free energy.  No counterpart in the reference: PolyFEM always

@@ -13,10 +13,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB_PATH = os.path.join(HERE, "libpfgpu.so")
-SOURCES = ["pfg_api.cu", "pfg_kernels.cu", "pfg_materials.cu", "pfg_solve.cu", "pfg_noalloc.cu", "pfg_tc.cu"]
+SOURCES = ["pfg_api.cu", "pfg_kernels.cu", "pfg_materials.cu", "pfg_solve.cu", "pfg_noalloc.cu", "pfg_tc.cu", "pfg_direct.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 PFG_OK = 0
+PFG_ERR_INVALID = 1
+PFG_ERR_STATE = 5
+PFG_ERR_NUMERIC = 6
 PFG_MEM_HOST = 0
 PFG_MEM_DEVICE = 1
 PFG_FP64 = 0
@@ -130,6 +133,11 @@ SIGNATURES = {
     "pfg_set_composite": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "pfg_cg_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
+    "pfg_direct_analyze": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pfg_direct_factorize": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "pfg_direct_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
+    "pfg_direct_stats": (ctypes.c_int, [_vp, _vp]),
+    "pfg_direct_symbolic": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp]),
 }
 
 

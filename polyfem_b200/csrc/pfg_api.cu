@@ -100,6 +100,9 @@ struct pfg_context
 	double *d_comp_vec = nullptr;                       // one component's gradient slots
 	double *d_comp_stage = nullptr;                     // one component's FP64 block triangles
 	unsigned long long *d_comp_inverted = nullptr;      // inverted counts of components after the first
+	// sparse direct solve (pfg_direct_*): the analysed (and factorised) system
+	pfg::DirectFactor *direct = nullptr;
+	int direct_system = -1;
 	std::string err;
 };
 
@@ -461,8 +464,16 @@ void build_incidence(const int *conn, int E, int n, int N, std::vector<long long
 		}
 }
 
+void free_direct(pfg_context *c)
+{
+	direct_destroy(c->direct);
+	c->direct = nullptr;
+	c->direct_system = -1;
+}
+
 void free_dirichlet(pfg_context *c)
 {
+	if (c->direct_system == PFG_SYS_REDUCED) free_direct(c);
 	void *rptrs[] = {c->d_old_to_new, c->d_free, c->d_red_col_start, c->d_red_outer, c->d_red_inner, c->d_red_row_off,
 					 c->d_red_values, c->d_red_groups};
 	for (void *p : rptrs)
@@ -670,6 +681,7 @@ void free_all(pfg_context *c)
 	for (void *p : rptrs)
 		if (p) cudaFree(p);
 	if (c->d_cg) cudaFree(c->d_cg);
+	free_direct(c);
 	if (c->h_cg_sc) cudaFreeHost(c->h_cg_sc);
 	if (c->d_mass) cudaFree(c->d_mass);
 	if (c->d_lump) cudaFree(c->d_lump);
@@ -704,6 +716,7 @@ const char *pfg_status_string(int s)
 	case PFG_ERR_OOM: return "out of memory";
 	case PFG_ERR_UNSUPPORTED: return "unsupported";
 	case PFG_ERR_STATE: return "invalid state";
+	case PFG_ERR_NUMERIC: return "matrix not positive definite";
 	}
 	return "unknown status";
 }
@@ -1528,6 +1541,129 @@ int pfg_cg_solve(pfg_context *c, int system, const double *values, const double 
 	if (iters) *iters = it;
 	if (rel_res) *rel_res = res;
 	if (mem == PFG_MEM_HOST) return finish_host(c, x, dx, n);
+	return PFG_OK;
+}
+
+// the system's device pattern: n, nnz, outer, inner, values; PFG_OK or a state error
+static int system_pattern(pfg_context *c, int system, int &n, long long &nnz, const int *&outer, const int *&inner,
+						  const double *&vals)
+{
+	if (system == PFG_SYS_FULL)
+	{
+		if (!c->has_pattern) return fail(c, PFG_ERR_STATE, "no Hessian assembled (pfg_hessian)");
+		n = 3 * c->m.N;
+		nnz = c->pat.nnz;
+		outer = c->d_outer;
+		inner = c->d_inner;
+		vals = c->d_values;
+		return PFG_OK;
+	}
+	if (system == PFG_SYS_REDUCED)
+	{
+		if (!c->has_dirichlet) return fail(c, PFG_ERR_STATE, "no Dirichlet set (pfg_set_dirichlet)");
+		n = c->n_free;
+		nnz = c->red_nnz;
+		outer = c->d_red_outer;
+		inner = c->d_red_inner;
+		vals = c->d_red_values;
+		return PFG_OK;
+	}
+	return fail(c, PFG_ERR_INVALID, "bad system");
+}
+
+int pfg_direct_analyze(pfg_context *c, int system)
+{
+	if (!c) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	int n;
+	long long nnz;
+	const int *d_outer, *d_inner;
+	const double *vals;
+	if (int st = system_pattern(c, system, n, nnz, d_outer, d_inner, vals)) return st;
+	DeviceGuard g(c->device);
+	free_direct(c);
+	std::vector<int> outer((size_t)n + 1), inner((size_t)std::max<long long>(nnz, 1));
+	PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	PFG_CUDA(c, cudaMemcpy(outer.data(), d_outer, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost));
+	if (nnz) PFG_CUDA(c, cudaMemcpy(inner.data(), d_inner, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost));
+	pfg::DirectFactor *f = nullptr;
+	std::string msg;
+	if (int st = direct_symbolic(n, outer.data(), inner.data(), &f, msg)) return fail(c, st, msg);
+	if (int st = direct_upload(f, msg))
+	{
+		direct_destroy(f);
+		return fail(c, st, msg);
+	}
+	c->direct = f;
+	c->direct_system = system;
+	return PFG_OK;
+}
+
+int pfg_direct_factorize(pfg_context *c, int system, const double *values)
+{
+	if (!c) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	int n;
+	long long nnz;
+	const int *d_outer, *d_inner;
+	const double *vals;
+	if (int st = system_pattern(c, system, n, nnz, d_outer, d_inner, vals)) return st;
+	if (!c->direct || c->direct_system != system || direct_n(c->direct) != n || direct_nnz(c->direct) != nnz)
+		return fail(c, PFG_ERR_STATE, "pattern not analysed (pfg_direct_analyze)");
+	if (values) vals = values;
+	if (nnz && !vals) return fail(c, PFG_ERR_STATE, "no values assembled");
+	DeviceGuard g(c->device);
+	cudaError_t ce = cudaSuccess;
+	const int r = direct_factorize(c->direct, vals, c->stream, &ce);
+	if (r == 1) return fail(c, PFG_ERR_NUMERIC, "matrix not positive definite (non-positive pivot)");
+	if (r) return cuda_fail(c, ce, "direct_factorize");
+	return PFG_OK;
+}
+
+int pfg_direct_solve(pfg_context *c, int system, const double *b, int mem, double *x)
+{
+	if (!c || !check_mem(mem)) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	if (!c->direct || c->direct_system != system || !direct_factorized(c->direct))
+		return fail(c, PFG_ERR_STATE, "not factorised (pfg_direct_factorize)");
+	const int n = direct_n(c->direct);
+	if (n == 0) return PFG_OK;
+	if (!b || !x) return fail(c, PFG_ERR_INVALID, "b or x NULL");
+	DeviceGuard g(c->device);
+	if (mem == PFG_MEM_HOST)
+	{
+		double *io = direct_io(c->direct);
+		PFG_CUDA(c, cudaMemcpyAsync(io, b, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+		PFG_CUDA(c, direct_solve(c->direct, io, io, c->stream));
+		PFG_CUDA(c, cudaMemcpyAsync(x, io, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+		PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+		return PFG_OK;
+	}
+	PFG_CUDA(c, direct_solve(c->direct, b, x, c->stream));
+	return PFG_OK;
+}
+
+int pfg_direct_stats(const pfg_context *c, long long *stats)
+{
+	if (!c || !stats) return fail(const_cast<pfg_context *>(c), PFG_ERR_INVALID, "bad arguments");
+	if (!c->direct) return fail(const_cast<pfg_context *>(c), PFG_ERR_STATE, "pattern not analysed (pfg_direct_analyze)");
+	direct_stats(c->direct, stats);
+	return PFG_OK;
+}
+
+int pfg_direct_symbolic(int n, const int *outer, const int *inner, long long *stats)
+{
+	if (n < 0 || !outer || !stats || (n > 0 && outer[n] > 0 && !inner)) return fail(nullptr, PFG_ERR_INVALID, "bad arguments");
+	if (outer[0] != 0) return fail(nullptr, PFG_ERR_INVALID, "outer[0] must be 0");
+	for (int j = 0; j < n; ++j)
+	{
+		if (outer[j + 1] < outer[j]) return fail(nullptr, PFG_ERR_INVALID, "outer not monotone");
+		for (int t = outer[j]; t < outer[j + 1]; ++t)
+			if (inner[t] < 0 || inner[t] >= n || (t > outer[j] && inner[t] <= inner[t - 1]))
+				return fail(nullptr, PFG_ERR_INVALID, "rows out of range or not strictly ascending");
+	}
+	pfg::DirectFactor *f = nullptr;
+	std::string msg;
+	if (int st = direct_symbolic(n, outer, inner, &f, msg)) return fail(nullptr, st, msg);
+	direct_stats(f, stats);
+	direct_destroy(f);
 	return PFG_OK;
 }
 

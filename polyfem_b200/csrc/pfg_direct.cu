@@ -1,0 +1,943 @@
+// Sparse direct solve on the device: a multifrontal Cholesky factorisation
+// P A P^T = L L^T of a symmetric positive definite matrix in the assembler's CSC
+// pattern, and the triangular solves.  PolyFEM's Newton step hands each assembled
+// Hessian to a polysolve linear::Solver (analyzePattern, factorize, solve) inside
+// the Newton solver of polysolve@47dc48d (external); the direct choices its call
+// sites name are sparse LDL^T / Cholesky factorisations (Eigen::SimplicialLDLT,
+// Cholmod, Pardiso: mesh/remesh/L2Projection.cpp:25-29, State.cpp:1562-1565).
+// This is that family's algorithm laid out for the GPU:
+//   analysis (host, once per pattern): columns with identical patterns (the dofs
+//     of one node) are grouped; the group graph is ordered by nested dissection
+//     with breadth-first level separators; the dissection tree is the assembly
+//     tree: every separator (and every leaf part) is one front whose columns are
+//     eliminated together, after its two halves.  Row structures, front sizes,
+//     the scatter of A's entries into the fronts and the extend-add maps are
+//     precomputed.
+//   factorisation (device): fronts of equal height in the tree are processed by
+//     the same launches, leaves first: A's lower entries are scattered into the
+//     zeroed fronts, the children's update matrices are added in child order,
+//     and each front is partially factorised (32-column panels: Cholesky of the
+//     diagonal block, triangular solve of the rows below, rank-32 update of the
+//     trailing lower triangle in 64 x 64 tiles); the trailing block is the update
+//     matrix the parent adds.
+//   solve (device): forward substitution leaves first (each front adds its
+//     children's update vectors in child order), backward substitution from the
+//     root, then the inverse permutation.
+// Every sum is taken in a fixed order, so factor and solution are bitwise
+// deterministic.  Fronts are dense column-major m x m blocks (lower triangle
+// used), all resident for the factor's lifetime.
+#include "pfg_internal.h"
+#include "pfgpu.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace pfg
+{
+
+namespace
+{
+
+constexpr int NB = 32;          // panel width of the partial factorisation
+constexpr int LEAF_DOFS = 96;   // dissection stops at parts of at most this many dofs
+constexpr int TRSM_ROWS = 128;  // rows per CTA of the panel solve
+constexpr int TILE = 64;        // trailing-update tile
+
+struct DevFront
+{
+	long long foff; // front block in the front buffer (doubles), m x m column-major
+	long long woff; // m doubles of solve workspace
+	long long roff; // rows of this front's update in the parent (relpos), m - k entries
+	long long ioff; // permuted positions of the m - k rows below the front's columns
+	int col0;       // first permuted column
+	int k;          // columns eliminated in this front
+	int m;          // k + rows below
+	int child0;     // children in child_list[child0 .. child0 + nchild)
+	int nchild;
+	int pad;
+};
+
+struct Panel
+{
+	int lvl, j0, rows_grid, tiles_grid;
+};
+
+} // namespace
+
+struct DirectFactor
+{
+	int n = 0;
+	long long nnz = 0;
+	int ns = 0;
+	std::vector<int> perm;             // permuted position -> dof
+	std::vector<DevFront> fr;          // fronts in postorder
+	std::vector<int> lvl_start;        // fronts of height h: lvl_list[lvl_start[h] .. lvl_start[h+1])
+	std::vector<int> lvl_list;
+	std::vector<long long> lvl_fbeg;   // front doubles of each level [lvl_fbeg[h], lvl_fbeg[h+1])
+	std::vector<long long> lvl_abeg;   // A-map entries of each level
+	std::vector<int> lvl_maxchild, lvl_maxrc;
+	std::vector<Panel> panels;         // factorisation launches in order
+	long long front_doubles = 0, work_doubles = 0, amap_n = 0;
+	// host maps between the analysis and the upload
+	std::vector<int> h_child, h_relpos, h_rows, h_amap_src;
+	std::vector<long long> h_amap_dst;
+	// device
+	DevFront *d_fr = nullptr;
+	int *d_lvl_list = nullptr, *d_child = nullptr, *d_relpos = nullptr, *d_rows = nullptr, *d_perm = nullptr;
+	int *d_amap_src = nullptr;
+	long long *d_amap_dst = nullptr;
+	double *d_front = nullptr, *d_work = nullptr, *d_vec = nullptr; // d_vec: 2 n (permuted rhs, solution)
+	double *d_io = nullptr;                                          // n: b and x of a host-memory solve
+	int *d_err = nullptr;
+	bool factorized = false;
+};
+
+// ------------------------------------------------------------------ analysis
+
+namespace
+{
+
+struct NdBuilder
+{
+	// group graph
+	int nv = 0;
+	std::vector<int> off, adj, wt;
+	// dissection tree (created in postorder: every node after its descendants)
+	std::vector<std::vector<int>> cols;     // groups of each node
+	std::vector<std::vector<int>> children;
+	std::vector<int> mark, vis, lev;
+	int label = 0, stamp = 0;
+
+	int make_node(std::vector<int> g, std::vector<int> ch)
+	{
+		std::sort(g.begin(), g.end());
+		cols.push_back(std::move(g));
+		children.push_back(std::move(ch));
+		return (int)cols.size() - 1;
+	}
+
+	// breadth-first levels from root over vertices marked `lab`; returns the visit
+	// order and fills level starts; vis[] = stamp for visited, lev[] = level
+	void bfs(int root, int lab, std::vector<int> &order, std::vector<int> &ls)
+	{
+		++stamp;
+		order.clear();
+		ls.clear();
+		order.push_back(root);
+		vis[root] = stamp;
+		lev[root] = 0;
+		ls.push_back(0);
+		size_t head = 0;
+		int cur = 0;
+		while (head < order.size())
+		{
+			const int v = order[head];
+			if (lev[v] != cur)
+			{
+				cur = lev[v];
+				ls.push_back((int)head);
+			}
+			++head;
+			for (int t = off[v]; t < off[v + 1]; ++t)
+			{
+				const int u = adj[t];
+				if (mark[u] == lab && vis[u] != stamp)
+				{
+					vis[u] = stamp;
+					lev[u] = lev[v] + 1;
+					order.push_back(u);
+				}
+			}
+		}
+		ls.push_back((int)order.size());
+	}
+
+	int degree_in(int v, int lab) const
+	{
+		int d = 0;
+		for (int t = off[v]; t < off[v + 1]; ++t) d += mark[adj[t]] == lab;
+		return d;
+	}
+
+	// nested dissection of the vertex set S; returns the roots of its subtrees
+	std::vector<int> build(std::vector<int> S)
+	{
+		std::vector<int> roots;
+		if (S.empty()) return roots;
+		const int lab = ++label;
+		for (int v : S) mark[v] = lab;
+		std::vector<int> order, ls;
+		bfs(S[0], lab, order, ls);
+		if (order.size() < S.size())
+		{
+			// disconnected: every component is its own subtree
+			std::vector<std::vector<int>> comps;
+			comps.push_back(order);
+			for (int v : order) mark[v] = -1;
+			for (int v : S)
+				if (mark[v] == lab)
+				{
+					bfs(v, lab, order, ls);
+					comps.push_back(order);
+					for (int u : order) mark[u] = -1;
+				}
+			for (auto &c : comps)
+			{
+				std::vector<int> r = build(std::move(c));
+				roots.insert(roots.end(), r.begin(), r.end());
+			}
+			return roots;
+		}
+		long long w = 0;
+		for (int v : S) w += wt[v];
+		if (w <= LEAF_DOFS)
+		{
+			roots.push_back(make_node(std::move(S), {}));
+			return roots;
+		}
+		// pseudo-peripheral root: restart from a minimum-degree vertex of the last
+		// level while the eccentricity grows
+		int r = S[0], h = (int)ls.size() - 1;
+		for (int it = 0; it < 4; ++it)
+		{
+			int best = -1, bd = 1 << 30;
+			for (int q = ls[h - 1]; q < ls[h]; ++q)
+			{
+				const int d = degree_in(order[q], lab);
+				if (d < bd) bd = d, best = order[q];
+			}
+			std::vector<int> o2, l2;
+			bfs(best, lab, o2, l2);
+			const int h2 = (int)l2.size() - 1;
+			if (h2 <= h)
+			{
+				bfs(r, lab, order, ls); // restore r's levels
+				break;
+			}
+			r = best;
+			h = h2;
+			order.swap(o2);
+			ls.swap(l2);
+		}
+		if (h < 3)
+		{
+			roots.push_back(make_node(std::move(S), {}));
+			return roots;
+		}
+		// separator level: the first level where the weight before it reaches half
+		long long acc = 0;
+		int mid = 1;
+		for (int q = 0; q < h; ++q)
+		{
+			long long lw = 0;
+			for (int t = ls[q]; t < ls[q + 1]; ++t) lw += wt[order[t]];
+			if (acc + lw > w / 2)
+			{
+				mid = q;
+				break;
+			}
+			acc += lw;
+		}
+		mid = std::min(std::max(mid, 1), h - 2);
+		std::vector<int> A, B, Sep;
+		for (int q = 0; q < h; ++q)
+			for (int t = ls[q]; t < ls[q + 1]; ++t)
+			{
+				const int v = order[t];
+				if (q < mid) A.push_back(v);
+				else if (q > mid) B.push_back(v);
+				else
+				{
+					// a level-mid vertex with no neighbour beyond the separator joins A
+					bool beyond = false;
+					for (int e = off[v]; e < off[v + 1] && !beyond; ++e)
+					{
+						const int u = adj[e];
+						beyond = mark[u] == lab && vis[u] == stamp && lev[u] == mid + 1;
+					}
+					(beyond ? Sep : A).push_back(v);
+				}
+			}
+		std::vector<int> ch = build(std::move(A));
+		std::vector<int> cb = build(std::move(B));
+		ch.insert(ch.end(), cb.begin(), cb.end());
+		if (Sep.empty())
+		{
+			roots = ch;
+			return roots;
+		}
+		roots.push_back(make_node(std::move(Sep), std::move(ch)));
+		return roots;
+	}
+};
+
+template <class T>
+static cudaError_t upload(T **d, const std::vector<T> &h)
+{
+	*d = nullptr;
+	const size_t bytes = sizeof(T) * std::max<size_t>(h.size(), 1);
+	cudaError_t e = cudaMalloc(reinterpret_cast<void **>(d), bytes);
+	if (e != cudaSuccess) return e;
+	if (!h.empty()) e = cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
+	return e;
+}
+
+} // namespace
+
+void direct_destroy(DirectFactor *f)
+{
+	if (!f) return;
+	void *ptrs[] = {f->d_fr,       f->d_lvl_list, f->d_child, f->d_relpos, f->d_rows, f->d_perm, f->d_amap_src,
+					f->d_amap_dst, f->d_front,    f->d_work,  f->d_vec,    f->d_io,   f->d_err};
+	for (void *p : ptrs)
+		if (p) cudaFree(p); // a host-only analysis never touches the runtime
+	delete f;
+}
+
+int direct_n(const DirectFactor *f) { return f ? f->n : 0; }
+long long direct_nnz(const DirectFactor *f) { return f ? f->nnz : 0; }
+long long direct_front_bytes(const DirectFactor *f) { return f ? f->front_doubles * 8 : 0; }
+int direct_fronts(const DirectFactor *f) { return f ? f->ns : 0; }
+bool direct_factorized(const DirectFactor *f) { return f && f->factorized; }
+double *direct_io(DirectFactor *f) { return f ? f->d_io : nullptr; }
+
+// Host analysis of a pattern (full symmetric CSC, sorted rows, n > 0 columns):
+// ordering, fronts and every index map, each checked against the front it
+// addresses before anything reaches the device.  0 ok, else a PFG error code
+// with msg; *out owns the host arrays (and the maps until direct_upload).
+int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **out, std::string &msg)
+{
+	*out = nullptr;
+	auto *f = new DirectFactor();
+	f->n = n;
+	f->nnz = n > 0 ? outer[n] : 0;
+	// 1. groups of consecutive columns with identical patterns
+	std::vector<int> gof(n), gfirst;
+	for (int j = 0; j < n; ++j)
+	{
+		bool same = false;
+		if (j > 0)
+		{
+			const int a0 = outer[j - 1], a1 = outer[j], b0 = outer[j], b1 = outer[j + 1];
+			same = (a1 - a0) == (b1 - b0) && std::equal(inner + a0, inner + a1, inner + b0);
+		}
+		if (same) gof[j] = gof[j - 1];
+		else
+		{
+			gof[j] = (int)gfirst.size();
+			gfirst.push_back(j);
+		}
+	}
+	const int ng = (int)gfirst.size();
+	gfirst.push_back(n);
+	NdBuilder nd;
+	nd.nv = ng;
+	nd.off.assign(ng + 1, 0);
+	nd.wt.assign(ng, 0);
+	for (int g = 0; g < ng; ++g)
+	{
+		nd.wt[g] = gfirst[g + 1] - gfirst[g];
+		const int j = gfirst[g];
+		int last = -1;
+		for (int t = outer[j]; t < outer[j + 1]; ++t)
+		{
+			const int h = gof[inner[t]];
+			if (h != g && h != last) nd.adj.push_back(h);
+			last = h;
+		}
+		nd.off[g + 1] = (int)nd.adj.size();
+	}
+	nd.mark.assign(ng, 0);
+	nd.vis.assign(ng, 0);
+	nd.lev.assign(ng, 0);
+	std::vector<int> all(ng);
+	std::iota(all.begin(), all.end(), 0);
+	nd.build(std::move(all));
+	const int ns = (int)nd.cols.size();
+	f->ns = ns;
+	// 2. permutation: columns in node (postorder) order
+	std::vector<int> parent(ns, -1), col0(ns), kc(ns);
+	for (int s = 0; s < ns; ++s)
+		for (int c : nd.children[s]) parent[c] = s;
+	f->perm.resize(n);
+	std::vector<int> iperm(n);
+	int pos = 0;
+	for (int s = 0; s < ns; ++s)
+	{
+		col0[s] = pos;
+		for (int g : nd.cols[s])
+			for (int j = gfirst[g]; j < gfirst[g + 1]; ++j)
+			{
+				f->perm[pos] = j;
+				iperm[j] = pos++;
+			}
+		kc[s] = pos - col0[s];
+	}
+	if (pos != n)
+	{
+		msg = "direct solver analysis lost columns";
+		direct_destroy(f);
+		return PFG_ERR_STATE;
+	}
+	// 3. row structures below each front's columns
+	std::vector<std::vector<int>> rows(ns);
+	for (int s = 0; s < ns; ++s)
+	{
+		const int last = col0[s] + kc[s] - 1;
+		std::vector<int> R;
+		for (int q = col0[s]; q <= last; ++q)
+		{
+			const int j = f->perm[q];
+			for (int t = outer[j]; t < outer[j + 1]; ++t)
+			{
+				const int p = iperm[inner[t]];
+				if (p > last) R.push_back(p);
+			}
+		}
+		for (int c : nd.children[s])
+			for (int p : rows[c])
+				if (p > last) R.push_back(p);
+		std::sort(R.begin(), R.end());
+		R.erase(std::unique(R.begin(), R.end()), R.end());
+		rows[s] = std::move(R);
+	}
+	// 4. heights and levels
+	std::vector<int> height(ns, 0);
+	int maxh = 0;
+	for (int s = 0; s < ns; ++s)
+	{
+		for (int c : nd.children[s]) height[s] = std::max(height[s], height[c] + 1);
+		maxh = std::max(maxh, height[s]);
+	}
+	const int nl = ns > 0 ? maxh + 1 : 0;
+	f->lvl_start.assign(nl + 1, 0);
+	for (int s = 0; s < ns; ++s) f->lvl_start[height[s] + 1]++;
+	for (int h = 0; h < nl; ++h) f->lvl_start[h + 1] += f->lvl_start[h];
+	f->lvl_list.resize(ns);
+	{
+		std::vector<int> fill(f->lvl_start.begin(), f->lvl_start.end() - 1);
+		for (int s = 0; s < ns; ++s) f->lvl_list[fill[height[s]]++] = s;
+	}
+	// 5. fronts (allocated level by level), maps
+	f->fr.resize(ns);
+	std::vector<int> child_list, relpos, rowsflat;
+	f->lvl_fbeg.assign(nl + 1, 0);
+	f->lvl_abeg.assign(nl + 1, 0);
+	f->lvl_maxchild.assign(nl, 0);
+	f->lvl_maxrc.assign(nl, 0);
+	long long fo = 0, wo = 0;
+	std::vector<int> amap_src;
+	std::vector<long long> amap_dst;
+	// local index of permuted position p in front s's list, -1 if absent
+	auto local = [&](int s, int p) -> int {
+		const int last = col0[s] + kc[s] - 1;
+		if (p <= last) return p >= col0[s] ? p - col0[s] : -1;
+		const auto &R = rows[s];
+		const auto it = std::lower_bound(R.begin(), R.end(), p);
+		return it != R.end() && *it == p ? kc[s] + (int)(it - R.begin()) : -1;
+	};
+	bool broken = false;
+	for (int s = 0; s < ns; ++s)
+	{
+		DevFront &d = f->fr[s];
+		d.col0 = col0[s];
+		d.k = kc[s];
+		d.m = kc[s] + (int)rows[s].size();
+		d.child0 = (int)child_list.size();
+		d.nchild = (int)nd.children[s].size();
+		d.pad = 0;
+		for (int c : nd.children[s]) child_list.push_back(c);
+		d.ioff = (long long)rowsflat.size();
+		rowsflat.insert(rowsflat.end(), rows[s].begin(), rows[s].end());
+		d.woff = wo;
+		wo += d.m;
+	}
+	for (int s = 0; s < ns; ++s)
+	{
+		DevFront &d = f->fr[s];
+		d.roff = (long long)relpos.size();
+		if (parent[s] >= 0)
+		{
+			int prev = -1;
+			for (int p : rows[s])
+			{
+				const int l = local(parent[s], p);
+				broken |= l <= prev; // present in the parent, increasing
+				relpos.push_back(l);
+				prev = l;
+			}
+		}
+		else broken |= !rows[s].empty();
+	}
+	for (int h = 0; h < nl; ++h)
+	{
+		f->lvl_fbeg[h] = fo;
+		f->lvl_abeg[h] = (long long)amap_src.size();
+		for (int t = f->lvl_start[h]; t < f->lvl_start[h + 1]; ++t)
+		{
+			const int s = f->lvl_list[t];
+			DevFront &d = f->fr[s];
+			d.foff = fo;
+			fo += (long long)d.m * d.m;
+			f->lvl_maxchild[h] = std::max(f->lvl_maxchild[h], d.nchild);
+			for (int c : nd.children[s]) f->lvl_maxrc[h] = std::max(f->lvl_maxrc[h], f->fr[c].m - f->fr[c].k);
+			for (int q = d.col0; q < d.col0 + d.k; ++q)
+			{
+				const int j = f->perm[q], cl = q - d.col0;
+				for (int t2 = outer[j]; t2 < outer[j + 1]; ++t2)
+				{
+					const int p = iperm[inner[t2]];
+					if (p < q) continue; // the upper entry of the pair
+					const int lr = local(s, p);
+					broken |= lr < cl || lr >= d.m; // lower triangle of this front
+					amap_src.push_back(t2);
+					amap_dst.push_back(d.foff + lr + (long long)cl * d.m);
+				}
+			}
+		}
+	}
+	f->lvl_fbeg[nl] = fo;
+	f->lvl_abeg[nl] = (long long)amap_src.size();
+	f->front_doubles = fo;
+	f->work_doubles = wo;
+	f->amap_n = (long long)amap_src.size();
+	// 6. panel launches of the factorisation
+	for (int h = 0; h < nl; ++h)
+	{
+		int maxk = 0;
+		for (int t = f->lvl_start[h]; t < f->lvl_start[h + 1]; ++t) maxk = std::max(maxk, f->fr[f->lvl_list[t]].k);
+		for (int j0 = 0; j0 < maxk; j0 += NB)
+		{
+			long long rg = 0, tg = 0;
+			for (int t = f->lvl_start[h]; t < f->lvl_start[h + 1]; ++t)
+			{
+				const DevFront &d = f->fr[f->lvl_list[t]];
+				if (d.k <= j0) continue;
+				const int nb = std::min(NB, d.k - j0);
+				const long long below = d.m - j0 - nb;
+				rg = std::max(rg, (below + TRSM_ROWS - 1) / TRSM_ROWS);
+				const long long nt = (below + TILE - 1) / TILE;
+				tg = std::max(tg, nt * (nt + 1) / 2);
+			}
+			if (tg > 0x7fffffffLL)
+			{
+				msg = "direct solver front too large";
+				direct_destroy(f);
+				return PFG_ERR_UNSUPPORTED;
+			}
+			f->panels.push_back({h, j0, (int)rg, (int)tg});
+		}
+	}
+	for (int h = 0; h < nl; ++h)
+		if (f->lvl_start[h + 1] - f->lvl_start[h] > 65535)
+		{
+			msg = "direct solver: more than 65535 fronts of one height";
+			direct_destroy(f);
+			return PFG_ERR_UNSUPPORTED;
+		}
+	for (int s2 = 0; s2 < ns && !broken; ++s2)
+	{
+		const DevFront &d = f->fr[s2];
+		broken |= d.k < 1 || d.m < d.k || d.foff < 0 || d.foff + (long long)d.m * d.m > fo;
+		const int last = d.col0 + d.k - 1;
+		for (int q = 0; q < d.m - d.k && !broken; ++q)
+		{
+			const int p = rowsflat[d.ioff + q];
+			broken |= p <= last || p >= n || (q > 0 && p <= rowsflat[d.ioff + q - 1]);
+		}
+	}
+	if (broken)
+	{
+		msg = "direct solver analysis produced an inconsistent front structure";
+		direct_destroy(f);
+		return PFG_ERR_STATE;
+	}
+	f->h_child = std::move(child_list);
+	f->h_relpos = std::move(relpos);
+	f->h_rows = std::move(rowsflat);
+	f->h_amap_src = std::move(amap_src);
+	f->h_amap_dst = std::move(amap_dst);
+	*out = f;
+	return PFG_OK;
+}
+
+// the analysed maps to the device (the host copies are released); 0 ok, else a
+// PFG error code with msg (f is left for direct_destroy)
+int direct_upload(DirectFactor *f, std::string &msg)
+{
+	const int n = f->n;
+	const long long fo = f->front_doubles, wo = f->work_doubles;
+	// the fronts must fit beside what is already allocated
+	size_t fre = 0, tot = 0;
+	cudaError_t e = cudaMemGetInfo(&fre, &tot);
+	if (e != cudaSuccess)
+	{
+		msg = cudaGetErrorString(e);
+		return PFG_ERR_CUDA;
+	}
+	const double need = 8.0 * (double)fo + 8.0 * (double)wo + 12.0 * (double)f->amap_n + 24.0 * n;
+	if (need > 0.85 * (double)fre)
+	{
+		msg = "direct solver needs " + std::to_string((long long)(need / 1e6)) + " MB of device memory for its fronts, " +
+			  std::to_string((long long)(fre / 1000000)) + " MB free";
+		return PFG_ERR_OOM;
+	}
+	if ((e = upload(&f->d_fr, f->fr)) != cudaSuccess || (e = upload(&f->d_lvl_list, f->lvl_list)) != cudaSuccess ||
+		(e = upload(&f->d_child, f->h_child)) != cudaSuccess || (e = upload(&f->d_relpos, f->h_relpos)) != cudaSuccess ||
+		(e = upload(&f->d_rows, f->h_rows)) != cudaSuccess || (e = upload(&f->d_perm, f->perm)) != cudaSuccess ||
+		(e = upload(&f->d_amap_src, f->h_amap_src)) != cudaSuccess ||
+		(e = upload(&f->d_amap_dst, f->h_amap_dst)) != cudaSuccess ||
+		(e = cudaMalloc(&f->d_front, 8 * std::max<long long>(fo, 1))) != cudaSuccess ||
+		(e = cudaMalloc(&f->d_work, 8 * std::max<long long>(wo, 1))) != cudaSuccess ||
+		(e = cudaMalloc(&f->d_vec, 16 * (size_t)std::max(n, 1))) != cudaSuccess ||
+		(e = cudaMalloc(&f->d_io, 8 * (size_t)std::max(n, 1))) != cudaSuccess ||
+		(e = cudaMalloc(&f->d_err, sizeof(int))) != cudaSuccess)
+	{
+		msg = cudaGetErrorString(e);
+		return e == cudaErrorMemoryAllocation ? PFG_ERR_OOM : PFG_ERR_CUDA;
+	}
+	f->h_child = {};
+	f->h_relpos = {};
+	f->h_rows = {};
+	f->h_amap_src = {};
+	f->h_amap_dst = {};
+	return PFG_OK;
+}
+
+void direct_stats(const DirectFactor *f, long long *st)
+{
+	// [n, fronts, levels, front doubles, nnz of L (columns of the fronts), largest front]
+	long long nnzl = 0, mx = 0;
+	for (const DevFront &d : f->fr)
+	{
+		nnzl += (long long)d.k * (d.k + 1) / 2 + (long long)d.k * (d.m - d.k);
+		mx = std::max<long long>(mx, d.m);
+	}
+	st[0] = f->n;
+	st[1] = f->ns;
+	st[2] = (long long)f->lvl_start.size() - 1;
+	st[3] = f->front_doubles;
+	st[4] = nnzl;
+	st[5] = mx;
+}
+
+// ------------------------------------------------------------------ kernels
+
+namespace
+{
+
+__global__ void k_dir_assemble(long long n, const int *__restrict__ src, const long long *__restrict__ dst,
+							   const double *__restrict__ vals, double *__restrict__ F)
+{
+	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t < n) F[dst[t]] = vals[src[t]];
+}
+
+// child ci of every front of the level: F_s[relpos a, relpos b] += U_c[a, b] (a >= b);
+// warp w of CTA x takes column b = 8 x + w of the child's update
+__global__ void __launch_bounds__(256) k_dir_extend_add(const DevFront *__restrict__ fr, const int *__restrict__ list,
+														const int *__restrict__ child, const int *__restrict__ relpos,
+														double *__restrict__ F, int ci)
+{
+	const DevFront f = fr[list[blockIdx.y]];
+	if (ci >= f.nchild) return;
+	const DevFront c = fr[child[f.child0 + ci]];
+	const int rc = c.m - c.k;
+	const int b = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+	if (b >= rc) return;
+	const int *rp = relpos + c.roff;
+	const double *U = F + c.foff + c.k + (size_t)c.k * c.m + (size_t)b * c.m;
+	double *P = F + f.foff + (size_t)rp[b] * f.m;
+	for (int a = b + lane; a < rc; a += 32) P[rp[a]] += U[a];
+}
+
+// Cholesky of the diagonal block of panel j0 (one warp per front)
+__global__ void __launch_bounds__(32) k_dir_potrf(const DevFront *__restrict__ fr, const int *__restrict__ list,
+												  double *__restrict__ F, int j0, int *__restrict__ err)
+{
+	const DevFront f = fr[list[blockIdx.x]];
+	if (j0 >= f.k) return;
+	const int nb = min(NB, f.k - j0), lane = threadIdx.x;
+	__shared__ double D[NB][NB + 1];
+	double *Fb = F + f.foff;
+	for (int c = 0; c < nb; ++c)
+		if (lane < nb && lane >= c) D[lane][c] = Fb[(size_t)(j0 + lane) + (size_t)(j0 + c) * f.m];
+	__syncwarp();
+	bool bad = false;
+	for (int c = 0; c < nb; ++c)
+	{
+		double d = D[c][c];
+		if (!(d > 0.0) || !(d <= 1.7976931348623157e308))
+		{
+			bad = true;
+			d = 1.0;
+		}
+		d = sqrt(d);
+		__syncwarp();
+		if (lane == c) D[c][c] = d;
+		if (lane > c && lane < nb) D[lane][c] /= d;
+		__syncwarp();
+		if (lane > c && lane < nb)
+		{
+			const double lc = D[lane][c];
+			for (int l = c + 1; l <= lane; ++l) D[lane][l] -= lc * D[l][c];
+		}
+		__syncwarp();
+	}
+	if (bad && lane == 0) atomicExch(err, 1);
+	for (int c = 0; c < nb; ++c)
+		if (lane < nb && lane >= c) Fb[(size_t)(j0 + lane) + (size_t)(j0 + c) * f.m] = D[lane][c];
+}
+
+// rows below the panel: X L_d^T = B, one row per thread
+__global__ void __launch_bounds__(TRSM_ROWS) k_dir_trsm(const DevFront *__restrict__ fr, const int *__restrict__ list,
+														double *__restrict__ F, int j0)
+{
+	const DevFront f = fr[list[blockIdx.y]];
+	if (j0 >= f.k) return;
+	const int nb = min(NB, f.k - j0);
+	__shared__ double D[NB][NB + 1];
+	double *Fb = F + f.foff;
+	for (int t = threadIdx.x; t < nb * nb; t += TRSM_ROWS)
+	{
+		const int r = t % nb, c = t / nb;
+		if (r >= c) D[r][c] = Fb[(size_t)(j0 + r) + (size_t)(j0 + c) * f.m];
+	}
+	__syncthreads();
+	const long long i = (long long)j0 + nb + (long long)blockIdx.x * TRSM_ROWS + threadIdx.x;
+	if (i >= f.m) return;
+	double x[NB];
+#pragma unroll
+	for (int l = 0; l < NB; ++l)
+		if (l < nb) x[l] = Fb[i + (size_t)(j0 + l) * f.m];
+#pragma unroll
+	for (int l = 0; l < NB; ++l)
+		if (l < nb)
+		{
+			double s = x[l];
+#pragma unroll
+			for (int t = 0; t < l; ++t) s = fma(-x[t], D[l][t], s);
+			x[l] = s / D[l][l];
+		}
+#pragma unroll
+	for (int l = 0; l < NB; ++l)
+		if (l < nb) Fb[i + (size_t)(j0 + l) * f.m] = x[l];
+}
+
+// trailing lower triangle -= P P^T for the panel's rows P below it, 64 x 64 tiles
+__global__ void __launch_bounds__(256) k_dir_syrk(const DevFront *__restrict__ fr, const int *__restrict__ list,
+												  double *__restrict__ F, int j0)
+{
+	const DevFront f = fr[list[blockIdx.y]];
+	if (j0 >= f.k) return;
+	const int nb = min(NB, f.k - j0);
+	const int o = j0 + nb, t = f.m - o;
+	if (t <= 0) return;
+	const long long nt = (t + TILE - 1) / TILE;
+	const long long tile = blockIdx.x;
+	if (tile >= nt * (nt + 1) / 2) return;
+	long long ti = (long long)((sqrt(8.0 * (double)tile + 1.0) - 1.0) * 0.5);
+	while (ti * (ti + 1) / 2 > tile) --ti;
+	while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
+	const long long tj = tile - ti * (ti + 1) / 2;
+	__shared__ double Pi[NB][TILE + 1], Pj[NB][TILE + 1];
+	double *Fb = F + f.foff;
+	for (int q = threadIdx.x; q < NB * TILE; q += 256)
+	{
+		const int r = q % TILE, l = q / TILE;
+		const long long gi = ti * TILE + r, gj = tj * TILE + r;
+		const bool ok = l < nb;
+		Pi[l][r] = ok && gi < t ? Fb[(size_t)(o + gi) + (size_t)(j0 + l) * f.m] : 0.0;
+		Pj[l][r] = ok && gj < t ? Fb[(size_t)(o + gj) + (size_t)(j0 + l) * f.m] : 0.0;
+	}
+	__syncthreads();
+	const int tr = (threadIdx.x % 16) * 4, tc = (threadIdx.x / 16) * 4;
+	double acc[4][4] = {};
+#pragma unroll 4
+	for (int l = 0; l < NB; ++l)
+	{
+		double a[4], b[4];
+#pragma unroll
+		for (int q = 0; q < 4; ++q)
+		{
+			a[q] = Pi[l][tr + q];
+			b[q] = Pj[l][tc + q];
+		}
+#pragma unroll
+		for (int p = 0; p < 4; ++p)
+#pragma unroll
+			for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], b[q], acc[p][q]);
+	}
+#pragma unroll
+	for (int q = 0; q < 4; ++q)
+	{
+		const long long gc = tj * TILE + tc + q;
+#pragma unroll
+		for (int p = 0; p < 4; ++p)
+		{
+			const long long gr = ti * TILE + tr + p;
+			if (gr < t && gc < t && gr >= gc) Fb[(size_t)(o + gr) + (size_t)(o + gc) * f.m] -= acc[p][q];
+		}
+	}
+}
+
+__global__ void k_dir_permute_in(int n, const int *__restrict__ perm, const double *__restrict__ b, double *__restrict__ bp)
+{
+	const int q = blockIdx.x * blockDim.x + threadIdx.x;
+	if (q < n) bp[q] = b[perm[q]];
+}
+
+__global__ void k_dir_permute_out(int n, const int *__restrict__ perm, const double *__restrict__ xp, double *__restrict__ x)
+{
+	const int q = blockIdx.x * blockDim.x + threadIdx.x;
+	if (q < n) x[perm[q]] = xp[q];
+}
+
+// forward substitution of the level's fronts (one CTA each): w = [b_cols; 0] plus
+// the children's update vectors, then L11 w1 = w1 with w2 -= L21 w1
+__global__ void __launch_bounds__(256) k_dir_forward(const DevFront *__restrict__ fr, const int *__restrict__ list,
+													 const int *__restrict__ child, const int *__restrict__ relpos,
+													 const double *__restrict__ F, const double *__restrict__ bp,
+													 double *__restrict__ W)
+{
+	const DevFront f = fr[list[blockIdx.x]];
+	double *w = W + f.woff;
+	const double *L = F + f.foff;
+	for (int i = threadIdx.x; i < f.m; i += 256) w[i] = i < f.k ? bp[f.col0 + i] : 0.0;
+	__syncthreads();
+	for (int ci = 0; ci < f.nchild; ++ci)
+	{
+		const DevFront c = fr[child[f.child0 + ci]];
+		const int rc = c.m - c.k;
+		const int *rp = relpos + c.roff;
+		const double *wc = W + c.woff + c.k;
+		for (int i = threadIdx.x; i < rc; i += 256) w[rp[i]] += wc[i];
+		__syncthreads();
+	}
+	for (int j = 0; j < f.k; ++j)
+	{
+		if (threadIdx.x == 0) w[j] /= L[(size_t)j * f.m + j];
+		__syncthreads();
+		const double v = w[j];
+		const double *Lj = L + (size_t)j * f.m;
+		for (int i = j + 1 + threadIdx.x; i < f.m; i += 256) w[i] = fma(-Lj[i], v, w[i]);
+		__syncthreads();
+	}
+}
+
+__device__ __forceinline__ double warp_sum_d(double v)
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+// backward substitution of the level's fronts (one CTA each): the rows' solution
+// (ancestors, already solved) is gathered into w2, w1 -= L21^T w2, then
+// L11^T x1 = w1 by warp 0
+__global__ void __launch_bounds__(256) k_dir_backward(const DevFront *__restrict__ fr, const int *__restrict__ list,
+													  const int *__restrict__ rows, const double *__restrict__ F,
+													  double *__restrict__ W, double *__restrict__ X)
+{
+	const DevFront f = fr[list[blockIdx.x]];
+	double *w = W + f.woff;
+	const double *L = F + f.foff;
+	const int r = f.m - f.k, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int i = threadIdx.x; i < r; i += 256) w[f.k + i] = X[rows[f.ioff + i]];
+	__syncthreads();
+	for (int j = warp; j < f.k; j += 8)
+	{
+		const double *Lj = L + (size_t)j * f.m + f.k;
+		double s = 0.0;
+		for (int i = lane; i < r; i += 32) s = fma(Lj[i], w[f.k + i], s);
+		s = warp_sum_d(s);
+		if (lane == 0) w[j] -= s;
+	}
+	__syncthreads();
+	if (warp == 0)
+		for (int j = f.k - 1; j >= 0; --j)
+		{
+			const double *Lj = L + (size_t)j * f.m;
+			double s = 0.0;
+			for (int i = j + 1 + lane; i < f.k; i += 32) s = fma(Lj[i], w[i], s);
+			s = warp_sum_d(s);
+			const double xj = (w[j] - s) / Lj[j];
+			__syncwarp();
+			if (lane == 0) w[j] = xj;
+			__syncwarp();
+		}
+	__syncthreads();
+	for (int j = threadIdx.x; j < f.k; j += 256) X[f.col0 + j] = w[j];
+}
+
+} // namespace
+
+// values (device, the analysed pattern's nnz) -> factor; 0 ok, 1 not positive
+// definite, else a CUDA error through *ce
+int direct_factorize(DirectFactor *f, const double *vals, cudaStream_t s, cudaError_t *ce)
+{
+	*ce = cudaSuccess;
+	f->factorized = false;
+	const int nl = (int)f->lvl_start.size() - 1;
+	if ((*ce = cudaMemsetAsync(f->d_err, 0, sizeof(int), s)) != cudaSuccess) return 2;
+	size_t pi = 0;
+	for (int h = 0; h < nl; ++h)
+	{
+		const int nf = f->lvl_start[h + 1] - f->lvl_start[h];
+		const int *list = f->d_lvl_list + f->lvl_start[h];
+		const long long fb = f->lvl_fbeg[h], fe = f->lvl_fbeg[h + 1];
+		if ((*ce = cudaMemsetAsync(f->d_front + fb, 0, 8 * (size_t)(fe - fb), s)) != cudaSuccess) return 2;
+		const long long ab = f->lvl_abeg[h], na = f->lvl_abeg[h + 1] - ab;
+		if (na > 0)
+			k_dir_assemble<<<(unsigned)((na + 255) / 256), 256, 0, s>>>(na, f->d_amap_src + ab, f->d_amap_dst + ab, vals,
+																		 f->d_front);
+		for (int ci = 0; ci < f->lvl_maxchild[h]; ++ci)
+			if (f->lvl_maxrc[h] > 0)
+				k_dir_extend_add<<<dim3((f->lvl_maxrc[h] + 7) / 8, nf), 256, 0, s>>>(f->d_fr, list, f->d_child,
+																					 f->d_relpos, f->d_front, ci);
+		for (; pi < f->panels.size() && f->panels[pi].lvl == h; ++pi)
+		{
+			const Panel &p = f->panels[pi];
+			k_dir_potrf<<<nf, 32, 0, s>>>(f->d_fr, list, f->d_front, p.j0, f->d_err);
+			if (p.rows_grid > 0) k_dir_trsm<<<dim3(p.rows_grid, nf), TRSM_ROWS, 0, s>>>(f->d_fr, list, f->d_front, p.j0);
+			if (p.tiles_grid > 0) k_dir_syrk<<<dim3(p.tiles_grid, nf), 256, 0, s>>>(f->d_fr, list, f->d_front, p.j0);
+		}
+		if ((*ce = cudaGetLastError()) != cudaSuccess) return 2;
+	}
+	int bad = 0;
+	if ((*ce = cudaMemcpyAsync(&bad, f->d_err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return 2;
+	if ((*ce = cudaStreamSynchronize(s)) != cudaSuccess) return 2;
+	if (bad) return 1;
+	f->factorized = true;
+	return 0;
+}
+
+// x = A^-1 b for device vectors b, x of n entries (x may alias b)
+cudaError_t direct_solve(DirectFactor *f, const double *b, double *x, cudaStream_t s)
+{
+	const int n = f->n;
+	if (n == 0) return cudaSuccess;
+	double *bp = f->d_vec, *xp = f->d_vec + n;
+	const int nl = (int)f->lvl_start.size() - 1;
+	k_dir_permute_in<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_perm, b, bp);
+	for (int h = 0; h < nl; ++h)
+	{
+		const int nf = f->lvl_start[h + 1] - f->lvl_start[h];
+		k_dir_forward<<<nf, 256, 0, s>>>(f->d_fr, f->d_lvl_list + f->lvl_start[h], f->d_child, f->d_relpos, f->d_front,
+										 bp, f->d_work);
+	}
+	for (int h = nl - 1; h >= 0; --h)
+	{
+		const int nf = f->lvl_start[h + 1] - f->lvl_start[h];
+		k_dir_backward<<<nf, 256, 0, s>>>(f->d_fr, f->d_lvl_list + f->lvl_start[h], f->d_rows, f->d_front, f->d_work,
+										  xp);
+	}
+	k_dir_permute_out<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_perm, xp, x);
+	return cudaGetLastError();
+}
+
+} // namespace pfg

@@ -206,4 +206,22 @@ cudaError_t launch_cg_iterations(int n, int count, int ngroups, const int *group
 // Sets the message pfg_last_error(NULL) returns on this host thread.
 void set_global_error(const std::string &msg);
 
+// Sparse direct solve (pfg_direct.cu): multifrontal Cholesky of an SPD matrix in a
+// CSC pattern.  direct_symbolic analyses a host pattern (0 or a PFG error code),
+// direct_upload moves its maps to the device, direct_factorize factorises device
+// values (0 ok, 1 not positive definite, 2 CUDA error in *ce), direct_solve
+// solves for device vectors (x may alias b).  direct_stats: n, fronts, levels,
+// front doubles, entries of L, largest front.
+struct DirectFactor;
+int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **out, std::string &msg);
+int direct_upload(DirectFactor *f, std::string &msg);
+int direct_factorize(DirectFactor *f, const double *vals, cudaStream_t s, cudaError_t *ce);
+cudaError_t direct_solve(DirectFactor *f, const double *b, double *x, cudaStream_t s);
+void direct_destroy(DirectFactor *f);
+void direct_stats(const DirectFactor *f, long long *st);
+int direct_n(const DirectFactor *f);
+long long direct_nnz(const DirectFactor *f);
+bool direct_factorized(const DirectFactor *f);
+double *direct_io(DirectFactor *f);
+
 } // namespace pfg
