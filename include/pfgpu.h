@@ -413,8 +413,8 @@ int pfg_cg_solve(pfg_context *ctx, int system, const double *values, const doubl
  * Every sum is taken in a fixed order, so factor and solution are bitwise
  * deterministic.  pfg_direct_stats (after analyze) and pfg_direct_symbolic (any
  * host pattern: full symmetric CSC of n columns with sorted rows; host only, no
- * device) write six values: n, fronts, tree levels, doubles of the dense fronts,
- * entries of L, largest front order. */
+ * device) write seven values: n, fronts, tree levels, doubles of the dense
+ * fronts, entries of L, largest front order, flops of the factorisation. */
 int pfg_direct_analyze(pfg_context *ctx, int system);
 int pfg_direct_factorize(pfg_context *ctx, int system, const double *values);
 int pfg_direct_solve(pfg_context *ctx, int system, const double *b, int mem, double *x);

@@ -610,13 +610,22 @@ int direct_upload(DirectFactor *f, std::string &msg)
 
 void direct_stats(const DirectFactor *f, long long *st)
 {
-	// [n, fronts, levels, front doubles, nnz of L (columns of the fronts), largest front]
+	// [n, fronts, levels, front doubles, nnz of L (columns of the fronts), largest
+	// front, flops of the factorisation: column j of a front of order m updates the
+	// (m-j-1)(m-j)/2 entries of its trailing lower triangle, one multiply-add each]
 	long long nnzl = 0, mx = 0;
+	double fl = 0.0;
+	auto s2 = [](double t) { return t * (t + 1.0) * (2.0 * t + 1.0) / 6.0; }; // sum of squares 1..t
+	auto s1 = [](double t) { return t * (t + 1.0) / 2.0; };
 	for (const DevFront &d : f->fr)
 	{
 		nnzl += (long long)d.k * (d.k + 1) / 2 + (long long)d.k * (d.m - d.k);
 		mx = std::max<long long>(mx, d.m);
+		// sum over t = m-k .. m-1 of t (t + 1)
+		const double hi = d.m - 1.0, lo = d.m - d.k - 1.0;
+		fl += (s2(hi) - s2(lo)) + (s1(hi) - s1(lo));
 	}
+	st[6] = (long long)fl;
 	st[0] = f->n;
 	st[1] = f->ns;
 	st[2] = (long long)f->lvl_start.size() - 1;
@@ -798,7 +807,9 @@ __global__ void k_dir_permute_out(int n, const int *__restrict__ perm, const dou
 }
 
 // forward substitution of the level's fronts (one CTA each): w = [b_cols; 0] plus
-// the children's update vectors, then L11 w1 = w1 with w2 -= L21 w1
+// the children's update vectors, then L11 w1 = w1 with w2 -= L21 w1, in 32-column
+// blocks: warp 0 solves the diagonal block in registers, then every thread takes
+// rows below it (coalesced column reads of L)
 __global__ void __launch_bounds__(256) k_dir_forward(const DevFront *__restrict__ fr, const int *__restrict__ list,
 													 const int *__restrict__ child, const int *__restrict__ relpos,
 													 const double *__restrict__ F, const double *__restrict__ bp,
@@ -807,6 +818,7 @@ __global__ void __launch_bounds__(256) k_dir_forward(const DevFront *__restrict_
 	const DevFront f = fr[list[blockIdx.x]];
 	double *w = W + f.woff;
 	const double *L = F + f.foff;
+	const int lane = threadIdx.x & 31;
 	for (int i = threadIdx.x; i < f.m; i += 256) w[i] = i < f.k ? bp[f.col0 + i] : 0.0;
 	__syncthreads();
 	for (int ci = 0; ci < f.nchild; ++ci)
@@ -818,13 +830,32 @@ __global__ void __launch_bounds__(256) k_dir_forward(const DevFront *__restrict_
 		for (int i = threadIdx.x; i < rc; i += 256) w[rp[i]] += wc[i];
 		__syncthreads();
 	}
-	for (int j = 0; j < f.k; ++j)
+	__shared__ double yb[NB];
+	for (int j0 = 0; j0 < f.k; j0 += NB)
 	{
-		if (threadIdx.x == 0) w[j] /= L[(size_t)j * f.m + j];
+		const int nb = min(NB, f.k - j0);
+		if (threadIdx.x < 32)
+		{
+			double v = lane < nb ? w[j0 + lane] : 0.0;
+			for (int c = 0; c < nb; ++c)
+			{
+				const double yc = __shfl_sync(0xffffffffu, v, c) / L[(size_t)(j0 + c) * f.m + j0 + c];
+				if (lane == c) v = yc;
+				if (lane > c && lane < nb) v = fma(-L[(size_t)(j0 + c) * f.m + j0 + lane], yc, v);
+			}
+			if (lane < nb)
+			{
+				w[j0 + lane] = v;
+				yb[lane] = v;
+			}
+		}
 		__syncthreads();
-		const double v = w[j];
-		const double *Lj = L + (size_t)j * f.m;
-		for (int i = j + 1 + threadIdx.x; i < f.m; i += 256) w[i] = fma(-Lj[i], v, w[i]);
+		for (int i = j0 + nb + threadIdx.x; i < f.m; i += 256)
+		{
+			double a = w[i];
+			for (int c = 0; c < nb; ++c) a = fma(-L[(size_t)(j0 + c) * f.m + i], yb[c], a);
+			w[i] = a;
+		}
 		__syncthreads();
 	}
 }
@@ -837,8 +868,10 @@ __device__ __forceinline__ double warp_sum_d(double v)
 }
 
 // backward substitution of the level's fronts (one CTA each): the rows' solution
-// (ancestors, already solved) is gathered into w2, w1 -= L21^T w2, then
-// L11^T x1 = w1 by warp 0
+// (ancestors, already solved) is gathered into w2 and w1 -= L21^T w2; then
+// L11^T x1 = w1 in 32-column blocks from the last: each column of the block takes
+// the solved part below it (a warp per column, coalesced), then warp 0 solves the
+// block's transposed diagonal in registers
 __global__ void __launch_bounds__(256) k_dir_backward(const DevFront *__restrict__ fr, const int *__restrict__ list,
 													  const int *__restrict__ rows, const double *__restrict__ F,
 													  double *__restrict__ W, double *__restrict__ X)
@@ -858,19 +891,35 @@ __global__ void __launch_bounds__(256) k_dir_backward(const DevFront *__restrict
 		if (lane == 0) w[j] -= s;
 	}
 	__syncthreads();
-	if (warp == 0)
-		for (int j = f.k - 1; j >= 0; --j)
+	const int nblk = (f.k + NB - 1) / NB;
+	for (int bi = nblk - 1; bi >= 0; --bi)
+	{
+		const int j0 = bi * NB, nb = min(NB, f.k - j0), e = j0 + nb;
+		for (int c = warp; c < nb; c += 8)
 		{
-			const double *Lj = L + (size_t)j * f.m;
+			const double *Lj = L + (size_t)(j0 + c) * f.m;
 			double s = 0.0;
-			for (int i = j + 1 + lane; i < f.k; i += 32) s = fma(Lj[i], w[i], s);
+			for (int i = e + lane; i < f.k; i += 32) s = fma(Lj[i], w[i], s);
 			s = warp_sum_d(s);
-			const double xj = (w[j] - s) / Lj[j];
-			__syncwarp();
-			if (lane == 0) w[j] = xj;
-			__syncwarp();
+			if (lane == 0) w[j0 + c] -= s;
 		}
-	__syncthreads();
+		__syncthreads();
+		if (threadIdx.x < 32)
+		{
+			double v = lane < nb ? w[j0 + lane] : 0.0;
+			for (int c = nb - 1; c >= 0; --c)
+			{
+				// x_c = (v_c - sum_{c' > c} L[c'][c] x_c') / L[c][c]; lanes c' > c hold x_c'
+				const double *Lc = L + (size_t)(j0 + c) * f.m + j0;
+				const double t = lane > c && lane < nb ? Lc[lane] * v : 0.0;
+				const double sum = warp_sum_d(t);
+				const double xc = (__shfl_sync(0xffffffffu, v, c) - sum) / Lc[c];
+				if (lane == c) v = xc;
+			}
+			if (lane < nb) w[j0 + lane] = v;
+		}
+		__syncthreads();
+	}
 	for (int j = threadIdx.x; j < f.k; j += 256) X[f.col0 + j] = w[j];
 }
 

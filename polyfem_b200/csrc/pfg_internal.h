@@ -211,7 +211,7 @@ void set_global_error(const std::string &msg);
 // direct_upload moves its maps to the device, direct_factorize factorises device
 // values (0 ok, 1 not positive definite, 2 CUDA error in *ce), direct_solve
 // solves for device vectors (x may alias b).  direct_stats: n, fronts, levels,
-// front doubles, entries of L, largest front.
+// front doubles, entries of L, largest front, flops of the factorisation.
 struct DirectFactor;
 int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **out, std::string &msg);
 int direct_upload(DirectFactor *f, std::string &msg);

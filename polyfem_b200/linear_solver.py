@@ -114,11 +114,11 @@ class DirectSolver:
     assembly's, or a float64 CUDA tensor in the same pattern), ``solve`` returns
     x = A^-1 b for numpy arrays or CUDA tensors.  A matrix that is not positive
     definite raises PfgError with status PFG_ERR_NUMERIC from ``factorize``.
-    ``get_info()`` reports the analysis: fronts, tree levels, entries of L and
-    the largest front.
+    ``get_info()`` reports the analysis: fronts, tree levels, entries of L, the
+    largest front and the factorisation's flops.
     """
 
-    STATS = ("n", "fronts", "levels", "front_doubles", "nnz_L", "max_front")
+    STATS = ("n", "fronts", "levels", "front_doubles", "nnz_L", "max_front", "flops")
 
     def __init__(self, assembler: NeoHookeanAssembler, system: str = "reduced"):
         if system not in ("full", "reduced"):
@@ -144,7 +144,7 @@ class DirectSolver:
         """Orders and analyses the system's pattern (the assembler's; `A` is not read)."""
         h = self.asm.handle
         check(lib().pfg_direct_analyze(h, self.system), h, "pfg_direct_analyze")
-        st = (ctypes.c_longlong * 6)()
+        st = (ctypes.c_longlong * 7)()
         check(lib().pfg_direct_stats(h, st), h, "pfg_direct_stats")
         self._info = dict(zip(self.STATS, (int(v) for v in st)))
 
@@ -189,12 +189,12 @@ class DirectSolver:
 
 def direct_symbolic(outer, inner) -> dict:
     """Host-only analysis of a symmetric CSC pattern (full storage, sorted rows):
-    the fronts, tree levels, entries of L and largest front the device
+    the fronts, tree levels, entries of L, largest front and flops the device
     factorisation of that pattern would have.  Needs no GPU."""
     outer = np.ascontiguousarray(outer, dtype=np.int32)
     inner = np.ascontiguousarray(inner, dtype=np.int32)
     n = outer.size - 1
-    st = (ctypes.c_longlong * 6)()
+    st = (ctypes.c_longlong * 7)()
     check(lib().pfg_direct_symbolic(n, ctypes.c_void_p(outer.ctypes.data), ctypes.c_void_p(inner.ctypes.data), st),
           None, "pfg_direct_symbolic")
     return dict(zip(DirectSolver.STATS, (int(v) for v in st)))
