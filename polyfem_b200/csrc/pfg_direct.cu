@@ -46,6 +46,8 @@ constexpr int NB = 32;          // panel width of the partial factorisation
 constexpr int LEAF_DOFS = 96;   // dissection stops at parts of at most this many dofs
 constexpr int TRSM_ROWS = 128;  // rows per CTA of the panel solve
 constexpr int TILE = 64;        // trailing-update tile
+constexpr int FWD_ROWS = 256;   // rows per CTA of the forward solve's panel update
+constexpr int BWD_ROWS = 512;   // rows per CTA of the backward solve's panel sums
 
 struct DevFront
 {
@@ -64,6 +66,7 @@ struct DevFront
 struct Panel
 {
 	int lvl, j0, rows_grid, tiles_grid;
+	int fwd_grid, bwd_grid; // CTAs per front of the solve's panel steps
 };
 
 } // namespace
@@ -79,7 +82,8 @@ struct DirectFactor
 	std::vector<int> lvl_list;
 	std::vector<long long> lvl_fbeg;   // front doubles of each level [lvl_fbeg[h], lvl_fbeg[h+1])
 	std::vector<long long> lvl_abeg;   // A-map entries of each level
-	std::vector<int> lvl_maxchild, lvl_maxrc;
+	std::vector<int> lvl_maxchild, lvl_maxrc, lvl_maxk;
+	int max_bwd_part = 0; // doubles of backward partial sums for one panel step
 	std::vector<Panel> panels;         // factorisation launches in order
 	long long front_doubles = 0, work_doubles = 0, amap_n = 0;
 	// host maps between the analysis and the upload
@@ -92,6 +96,7 @@ struct DirectFactor
 	long long *d_amap_dst = nullptr;
 	double *d_front = nullptr, *d_work = nullptr, *d_vec = nullptr; // d_vec: 2 n (permuted rhs, solution)
 	double *d_io = nullptr;                                          // n: b and x of a host-memory solve
+	double *d_part = nullptr;                                        // backward panel partial sums
 	int *d_err = nullptr;
 	bool factorized = false;
 };
@@ -292,7 +297,7 @@ void direct_destroy(DirectFactor *f)
 {
 	if (!f) return;
 	void *ptrs[] = {f->d_fr,       f->d_lvl_list, f->d_child, f->d_relpos, f->d_rows, f->d_perm, f->d_amap_src,
-					f->d_amap_dst, f->d_front,    f->d_work,  f->d_vec,    f->d_io,   f->d_err};
+					f->d_amap_dst, f->d_front,    f->d_work,  f->d_vec,    f->d_io,   f->d_err, f->d_part};
 	for (void *p : ptrs)
 		if (p) cudaFree(p); // a host-only analysis never touches the runtime
 	delete f;
@@ -510,9 +515,10 @@ int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **ou
 	{
 		int maxk = 0;
 		for (int t = f->lvl_start[h]; t < f->lvl_start[h + 1]; ++t) maxk = std::max(maxk, f->fr[f->lvl_list[t]].k);
+		f->lvl_maxk.push_back(maxk);
 		for (int j0 = 0; j0 < maxk; j0 += NB)
 		{
-			long long rg = 0, tg = 0;
+			long long rg = 0, tg = 0, fg = 0, bg = 1;
 			for (int t = f->lvl_start[h]; t < f->lvl_start[h + 1]; ++t)
 			{
 				const DevFront &d = f->fr[f->lvl_list[t]];
@@ -522,6 +528,8 @@ int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **ou
 				rg = std::max(rg, (below + TRSM_ROWS - 1) / TRSM_ROWS);
 				const long long nt = (below + TILE - 1) / TILE;
 				tg = std::max(tg, nt * (nt + 1) / 2);
+				fg = std::max(fg, (below + FWD_ROWS - 1) / FWD_ROWS);
+				bg = std::max(bg, ((long long)d.k - j0 - nb + BWD_ROWS - 1) / BWD_ROWS);
 			}
 			if (tg > 0x7fffffffLL)
 			{
@@ -529,7 +537,9 @@ int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **ou
 				direct_destroy(f);
 				return PFG_ERR_UNSUPPORTED;
 			}
-			f->panels.push_back({h, j0, (int)rg, (int)tg});
+			f->panels.push_back({h, j0, (int)rg, (int)tg, (int)fg, (int)bg});
+			const long long nfl = f->lvl_start[h + 1] - f->lvl_start[h];
+			f->max_bwd_part = (int)std::max<long long>(f->max_bwd_part, nfl * bg * NB);
 		}
 	}
 	for (int h = 0; h < nl; ++h)
@@ -579,7 +589,7 @@ int direct_upload(DirectFactor *f, std::string &msg)
 		msg = cudaGetErrorString(e);
 		return PFG_ERR_CUDA;
 	}
-	const double need = 8.0 * (double)fo + 8.0 * (double)wo + 12.0 * (double)f->amap_n + 24.0 * n;
+	const double need = 8.0 * (double)fo + 8.0 * (double)wo + 12.0 * (double)f->amap_n + 24.0 * n + 8.0 * f->max_bwd_part;
 	if (need > 0.85 * (double)fre)
 	{
 		msg = "direct solver needs " + std::to_string((long long)(need / 1e6)) + " MB of device memory for its fronts, " +
@@ -595,6 +605,7 @@ int direct_upload(DirectFactor *f, std::string &msg)
 		(e = cudaMalloc(&f->d_work, 8 * std::max<long long>(wo, 1))) != cudaSuccess ||
 		(e = cudaMalloc(&f->d_vec, 16 * (size_t)std::max(n, 1))) != cudaSuccess ||
 		(e = cudaMalloc(&f->d_io, 8 * (size_t)std::max(n, 1))) != cudaSuccess ||
+		(e = cudaMalloc(&f->d_part, 8 * (size_t)std::max(f->max_bwd_part, 1))) != cudaSuccess ||
 		(e = cudaMalloc(&f->d_err, sizeof(int))) != cudaSuccess)
 	{
 		msg = cudaGetErrorString(e);
@@ -664,42 +675,45 @@ __global__ void __launch_bounds__(256) k_dir_extend_add(const DevFront *__restri
 	for (int a = b + lane; a < rc; a += 32) P[rp[a]] += U[a];
 }
 
-// Cholesky of the diagonal block of panel j0 (one warp per front)
+// Cholesky of the diagonal block of panel j0 (one warp per front): lane i holds row
+// i of the block in registers; column c's entries reach the other lanes by shuffle
 __global__ void __launch_bounds__(32) k_dir_potrf(const DevFront *__restrict__ fr, const int *__restrict__ list,
 												  double *__restrict__ F, int j0, int *__restrict__ err)
 {
+	constexpr unsigned FULL = 0xffffffffu;
 	const DevFront f = fr[list[blockIdx.x]];
 	if (j0 >= f.k) return;
 	const int nb = min(NB, f.k - j0), lane = threadIdx.x;
-	__shared__ double D[NB][NB + 1];
 	double *Fb = F + f.foff;
-	for (int c = 0; c < nb; ++c)
-		if (lane < nb && lane >= c) D[lane][c] = Fb[(size_t)(j0 + lane) + (size_t)(j0 + c) * f.m];
-	__syncwarp();
+	const bool row = lane < nb;
+	double v[NB];
+#pragma unroll
+	for (int c = 0; c < NB; ++c) v[c] = row && c <= lane && c < nb ? Fb[(size_t)(j0 + lane) + (size_t)(j0 + c) * f.m] : 0.0;
 	bool bad = false;
-	for (int c = 0; c < nb; ++c)
+#pragma unroll
+	for (int c = 0; c < NB; ++c)
 	{
-		double d = D[c][c];
+		if (c >= nb) break;
+		double d = __shfl_sync(FULL, v[c], c);
 		if (!(d > 0.0) || !(d <= 1.7976931348623157e308))
 		{
 			bad = true;
 			d = 1.0;
 		}
 		d = sqrt(d);
-		__syncwarp();
-		if (lane == c) D[c][c] = d;
-		if (lane > c && lane < nb) D[lane][c] /= d;
-		__syncwarp();
-		if (lane > c && lane < nb)
+		const double lc = lane == c ? d : (lane > c ? v[c] / d : 0.0); // L[lane][c]
+		if (lane >= c) v[c] = lc;
+#pragma unroll
+		for (int l = c + 1; l < NB; ++l)
 		{
-			const double lc = D[lane][c];
-			for (int l = c + 1; l <= lane; ++l) D[lane][l] -= lc * D[l][c];
+			const double llc = __shfl_sync(FULL, lc, l); // L[l][c]
+			if (lane >= l && l < nb) v[l] = fma(-lc, llc, v[l]);
 		}
-		__syncwarp();
 	}
 	if (bad && lane == 0) atomicExch(err, 1);
-	for (int c = 0; c < nb; ++c)
-		if (lane < nb && lane >= c) Fb[(size_t)(j0 + lane) + (size_t)(j0 + c) * f.m] = D[lane][c];
+#pragma unroll
+	for (int c = 0; c < NB; ++c)
+		if (row && c <= lane && c < nb) Fb[(size_t)(j0 + lane) + (size_t)(j0 + c) * f.m] = v[c];
 }
 
 // rows below the panel: X L_d^T = B, one row per thread
@@ -806,19 +820,17 @@ __global__ void k_dir_permute_out(int n, const int *__restrict__ perm, const dou
 	if (q < n) x[perm[q]] = xp[q];
 }
 
-// forward substitution of the level's fronts (one CTA each): w = [b_cols; 0] plus
-// the children's update vectors, then L11 w1 = w1 with w2 -= L21 w1, in 32-column
-// blocks: warp 0 solves the diagonal block in registers, then every thread takes
-// rows below it (coalesced column reads of L)
-__global__ void __launch_bounds__(256) k_dir_forward(const DevFront *__restrict__ fr, const int *__restrict__ list,
-													 const int *__restrict__ child, const int *__restrict__ relpos,
-													 const double *__restrict__ F, const double *__restrict__ bp,
-													 double *__restrict__ W)
+// Forward substitution, level by level from the leaves, in the factorisation's
+// 32-column panels.  k_fwd_init: w = [b_cols; 0] plus the children's update
+// vectors (one CTA per front, children in order); per panel, k_fwd_diag (one warp
+// per front) solves the diagonal block in registers and k_fwd_rows updates the
+// rows below it (a thread per row, several CTAs per front, coalesced columns of L).
+__global__ void __launch_bounds__(256) k_fwd_init(const DevFront *__restrict__ fr, const int *__restrict__ list,
+												  const int *__restrict__ child, const int *__restrict__ relpos,
+												  const double *__restrict__ bp, double *__restrict__ W)
 {
 	const DevFront f = fr[list[blockIdx.x]];
 	double *w = W + f.woff;
-	const double *L = F + f.foff;
-	const int lane = threadIdx.x & 31;
 	for (int i = threadIdx.x; i < f.m; i += 256) w[i] = i < f.k ? bp[f.col0 + i] : 0.0;
 	__syncthreads();
 	for (int ci = 0; ci < f.nchild; ++ci)
@@ -830,34 +842,42 @@ __global__ void __launch_bounds__(256) k_dir_forward(const DevFront *__restrict_
 		for (int i = threadIdx.x; i < rc; i += 256) w[rp[i]] += wc[i];
 		__syncthreads();
 	}
-	__shared__ double yb[NB];
-	for (int j0 = 0; j0 < f.k; j0 += NB)
+}
+
+__global__ void __launch_bounds__(32) k_fwd_diag(const DevFront *__restrict__ fr, const int *__restrict__ list,
+												 const double *__restrict__ F, double *__restrict__ W, int j0)
+{
+	const DevFront f = fr[list[blockIdx.x]];
+	if (j0 >= f.k) return;
+	const int nb = min(NB, f.k - j0), lane = threadIdx.x;
+	double *w = W + f.woff;
+	const double *L = F + f.foff;
+	double v = lane < nb ? w[j0 + lane] : 0.0;
+	for (int c = 0; c < nb; ++c)
 	{
-		const int nb = min(NB, f.k - j0);
-		if (threadIdx.x < 32)
-		{
-			double v = lane < nb ? w[j0 + lane] : 0.0;
-			for (int c = 0; c < nb; ++c)
-			{
-				const double yc = __shfl_sync(0xffffffffu, v, c) / L[(size_t)(j0 + c) * f.m + j0 + c];
-				if (lane == c) v = yc;
-				if (lane > c && lane < nb) v = fma(-L[(size_t)(j0 + c) * f.m + j0 + lane], yc, v);
-			}
-			if (lane < nb)
-			{
-				w[j0 + lane] = v;
-				yb[lane] = v;
-			}
-		}
-		__syncthreads();
-		for (int i = j0 + nb + threadIdx.x; i < f.m; i += 256)
-		{
-			double a = w[i];
-			for (int c = 0; c < nb; ++c) a = fma(-L[(size_t)(j0 + c) * f.m + i], yb[c], a);
-			w[i] = a;
-		}
-		__syncthreads();
+		const double yc = __shfl_sync(0xffffffffu, v, c) / L[(size_t)(j0 + c) * f.m + j0 + c];
+		if (lane == c) v = yc;
+		if (lane > c && lane < nb) v = fma(-L[(size_t)(j0 + c) * f.m + j0 + lane], yc, v);
 	}
+	if (lane < nb) w[j0 + lane] = v;
+}
+
+__global__ void __launch_bounds__(FWD_ROWS) k_fwd_rows(const DevFront *__restrict__ fr, const int *__restrict__ list,
+													   const double *__restrict__ F, double *__restrict__ W, int j0)
+{
+	const DevFront f = fr[list[blockIdx.y]];
+	if (j0 >= f.k) return;
+	const int nb = min(NB, f.k - j0);
+	double *w = W + f.woff;
+	const double *L = F + f.foff;
+	__shared__ double yb[NB];
+	if (threadIdx.x < nb) yb[threadIdx.x] = w[j0 + threadIdx.x];
+	__syncthreads();
+	const long long i = (long long)j0 + nb + (long long)blockIdx.x * FWD_ROWS + threadIdx.x;
+	if (i >= f.m) return;
+	double a = w[i];
+	for (int c = 0; c < nb; ++c) a = fma(-L[(size_t)(j0 + c) * f.m + i], yb[c], a);
+	w[i] = a;
 }
 
 __device__ __forceinline__ double warp_sum_d(double v)
@@ -867,59 +887,97 @@ __device__ __forceinline__ double warp_sum_d(double v)
 	return v;
 }
 
-// backward substitution of the level's fronts (one CTA each): the rows' solution
-// (ancestors, already solved) is gathered into w2 and w1 -= L21^T w2; then
-// L11^T x1 = w1 in 32-column blocks from the last: each column of the block takes
-// the solved part below it (a warp per column, coalesced), then warp 0 solves the
-// block's transposed diagonal in registers
-__global__ void __launch_bounds__(256) k_dir_backward(const DevFront *__restrict__ fr, const int *__restrict__ list,
-													  const int *__restrict__ rows, const double *__restrict__ F,
-													  double *__restrict__ W, double *__restrict__ X)
+// Backward substitution, level by level from the root.  k_bwd_gather: w2 = the
+// rows' solution (ancestors, already solved); k_bwd_l21: w1 -= L21^T w2 (a warp
+// per column); per panel from the last, k_bwd_cols sums L[i][j] x_i over the
+// solved columns i below the panel in row chunks of BWD_ROWS (one partial per
+// chunk and column) and k_bwd_diag (one warp per front) adds the partials in chunk
+// order and solves the transposed diagonal block in registers; k_bwd_store writes
+// x1.
+__global__ void __launch_bounds__(256) k_bwd_gather(const DevFront *__restrict__ fr, const int *__restrict__ list,
+													const int *__restrict__ rows, const double *__restrict__ X,
+													double *__restrict__ W)
 {
 	const DevFront f = fr[list[blockIdx.x]];
 	double *w = W + f.woff;
-	const double *L = F + f.foff;
-	const int r = f.m - f.k, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int r = f.m - f.k;
 	for (int i = threadIdx.x; i < r; i += 256) w[f.k + i] = X[rows[f.ioff + i]];
-	__syncthreads();
-	for (int j = warp; j < f.k; j += 8)
+}
+
+__global__ void __launch_bounds__(256) k_bwd_l21(const DevFront *__restrict__ fr, const int *__restrict__ list,
+												 const double *__restrict__ F, double *__restrict__ W)
+{
+	const DevFront f = fr[list[blockIdx.y]];
+	const int j = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+	if (j >= f.k) return;
+	double *w = W + f.woff;
+	const int r = f.m - f.k;
+	const double *Lj = F + f.foff + (size_t)j * f.m + f.k;
+	double s = 0.0;
+	for (int i = lane; i < r; i += 32) s = fma(Lj[i], w[f.k + i], s);
+	s = warp_sum_d(s);
+	if (lane == 0) w[j] -= s;
+}
+
+__global__ void __launch_bounds__(256) k_bwd_cols(const DevFront *__restrict__ fr, const int *__restrict__ list,
+												  const double *__restrict__ F, const double *__restrict__ W,
+												  double *__restrict__ part, int j0)
+{
+	const DevFront f = fr[list[blockIdx.y]];
+	if (j0 >= f.k) return;
+	const int nb = min(NB, f.k - j0), e = j0 + nb;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const double *w = W + f.woff;
+	const double *L = F + f.foff;
+	const int i0 = e + blockIdx.x * BWD_ROWS, i1 = min(f.k, i0 + BWD_ROWS);
+	double *pp = part + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * NB;
+	for (int c = warp; c < NB; c += 8)
 	{
-		const double *Lj = L + (size_t)j * f.m + f.k;
 		double s = 0.0;
-		for (int i = lane; i < r; i += 32) s = fma(Lj[i], w[f.k + i], s);
+		if (c < nb)
+		{
+			const double *Lc = L + (size_t)(j0 + c) * f.m;
+			for (int i = i0 + lane; i < i1; i += 32) s = fma(Lc[i], w[i], s);
+		}
 		s = warp_sum_d(s);
-		if (lane == 0) w[j] -= s;
+		if (lane == 0) pp[c] = s;
 	}
-	__syncthreads();
-	const int nblk = (f.k + NB - 1) / NB;
-	for (int bi = nblk - 1; bi >= 0; --bi)
+}
+
+__global__ void __launch_bounds__(32) k_bwd_diag(const DevFront *__restrict__ fr, const int *__restrict__ list,
+												 const double *__restrict__ F, double *__restrict__ W,
+												 const double *__restrict__ part, int nchunk, int j0)
+{
+	const DevFront f = fr[list[blockIdx.x]];
+	if (j0 >= f.k) return;
+	const int nb = min(NB, f.k - j0), lane = threadIdx.x;
+	double *w = W + f.woff;
+	const double *L = F + f.foff;
+	double v = 0.0;
+	if (lane < nb)
 	{
-		const int j0 = bi * NB, nb = min(NB, f.k - j0), e = j0 + nb;
-		for (int c = warp; c < nb; c += 8)
-		{
-			const double *Lj = L + (size_t)(j0 + c) * f.m;
-			double s = 0.0;
-			for (int i = e + lane; i < f.k; i += 32) s = fma(Lj[i], w[i], s);
-			s = warp_sum_d(s);
-			if (lane == 0) w[j0 + c] -= s;
-		}
-		__syncthreads();
-		if (threadIdx.x < 32)
-		{
-			double v = lane < nb ? w[j0 + lane] : 0.0;
-			for (int c = nb - 1; c >= 0; --c)
-			{
-				// x_c = (v_c - sum_{c' > c} L[c'][c] x_c') / L[c][c]; lanes c' > c hold x_c'
-				const double *Lc = L + (size_t)(j0 + c) * f.m + j0;
-				const double t = lane > c && lane < nb ? Lc[lane] * v : 0.0;
-				const double sum = warp_sum_d(t);
-				const double xc = (__shfl_sync(0xffffffffu, v, c) - sum) / Lc[c];
-				if (lane == c) v = xc;
-			}
-			if (lane < nb) w[j0 + lane] = v;
-		}
-		__syncthreads();
+		const double *pp = part + (size_t)blockIdx.x * nchunk * NB + lane;
+		double s = 0.0;
+		for (int q = 0; q < nchunk; ++q) s += pp[(size_t)q * NB];
+		v = w[j0 + lane] - s;
 	}
+	for (int c = nb - 1; c >= 0; --c)
+	{
+		// x_c = (v_c - sum_{c' > c} L[c'][c] x_c') / L[c][c]; lanes c' > c hold x_c'
+		const double *Lc = L + (size_t)(j0 + c) * f.m + j0;
+		const double t = lane > c && lane < nb ? Lc[lane] * v : 0.0;
+		const double sum = warp_sum_d(t);
+		const double xc = (__shfl_sync(0xffffffffu, v, c) - sum) / Lc[c];
+		if (lane == c) v = xc;
+	}
+	if (lane < nb) w[j0 + lane] = v;
+}
+
+__global__ void __launch_bounds__(256) k_bwd_store(const DevFront *__restrict__ fr, const int *__restrict__ list,
+												   const double *__restrict__ W, double *__restrict__ X)
+{
+	const DevFront f = fr[list[blockIdx.x]];
+	const double *w = W + f.woff;
 	for (int j = threadIdx.x; j < f.k; j += 256) X[f.col0 + j] = w[j];
 }
 
@@ -973,17 +1031,39 @@ cudaError_t direct_solve(DirectFactor *f, const double *b, double *x, cudaStream
 	double *bp = f->d_vec, *xp = f->d_vec + n;
 	const int nl = (int)f->lvl_start.size() - 1;
 	k_dir_permute_in<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_perm, b, bp);
+	size_t pi = 0;
 	for (int h = 0; h < nl; ++h)
 	{
 		const int nf = f->lvl_start[h + 1] - f->lvl_start[h];
-		k_dir_forward<<<nf, 256, 0, s>>>(f->d_fr, f->d_lvl_list + f->lvl_start[h], f->d_child, f->d_relpos, f->d_front,
-										 bp, f->d_work);
+		const int *list = f->d_lvl_list + f->lvl_start[h];
+		k_fwd_init<<<nf, 256, 0, s>>>(f->d_fr, list, f->d_child, f->d_relpos, bp, f->d_work);
+		for (; pi < f->panels.size() && f->panels[pi].lvl == h; ++pi)
+		{
+			const Panel &p = f->panels[pi];
+			k_fwd_diag<<<nf, 32, 0, s>>>(f->d_fr, list, f->d_front, f->d_work, p.j0);
+			if (p.fwd_grid > 0)
+				k_fwd_rows<<<dim3(p.fwd_grid, nf), FWD_ROWS, 0, s>>>(f->d_fr, list, f->d_front, f->d_work, p.j0);
+		}
 	}
 	for (int h = nl - 1; h >= 0; --h)
 	{
 		const int nf = f->lvl_start[h + 1] - f->lvl_start[h];
-		k_dir_backward<<<nf, 256, 0, s>>>(f->d_fr, f->d_lvl_list + f->lvl_start[h], f->d_rows, f->d_front, f->d_work,
-										  xp);
+		const int *list = f->d_lvl_list + f->lvl_start[h];
+		k_bwd_gather<<<nf, 256, 0, s>>>(f->d_fr, list, f->d_rows, xp, f->d_work);
+		if (f->lvl_maxk[h] > 0)
+			k_bwd_l21<<<dim3((f->lvl_maxk[h] + 7) / 8, nf), 256, 0, s>>>(f->d_fr, list, f->d_front, f->d_work);
+		// this level's panels, last first
+		size_t p1 = 0;
+		while (p1 < f->panels.size() && f->panels[p1].lvl < h) ++p1;
+		size_t p2 = p1;
+		while (p2 < f->panels.size() && f->panels[p2].lvl == h) ++p2;
+		for (size_t q = p2; q > p1; --q)
+		{
+			const Panel &p = f->panels[q - 1];
+			k_bwd_cols<<<dim3(p.bwd_grid, nf), 256, 0, s>>>(f->d_fr, list, f->d_front, f->d_work, f->d_part, p.j0);
+			k_bwd_diag<<<nf, 32, 0, s>>>(f->d_fr, list, f->d_front, f->d_work, f->d_part, p.bwd_grid, p.j0);
+		}
+		k_bwd_store<<<nf, 256, 0, s>>>(f->d_fr, list, f->d_work, xp);
 	}
 	k_dir_permute_out<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_perm, xp, x);
 	return cudaGetLastError();
