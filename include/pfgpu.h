@@ -408,8 +408,10 @@ int pfg_cg_solve(pfg_context *ctx, int system, const double *values, const doubl
  *       doubles of the analysed pattern, both triangles stored; the lower one is
  *       read) or, with values == NULL, the system's values the last assembly left
  *       in the context.  PFG_ERR_NUMERIC when the matrix is not positive definite
- *       (Eigen's NumericalIssue): a non-positive or non-finite pivot;
- *   pfg_direct_solve     (solve): x = A^-1 b for b and x in `mem` (x may be b).
+ *       (Eigen's NumericalIssue): a non-positive or non-finite pivot.  The call
+ *       waits for the factorisation to finish (it reads the pivot check);
+ *   pfg_direct_solve     (solve): x = A^-1 b for b and x in `mem` (x may be b);
+ *       with PFG_MEM_DEVICE it is asynchronous on the context's stream.
  * Every sum is taken in a fixed order, so factor and solution are bitwise
  * deterministic.  pfg_direct_stats (after analyze) and pfg_direct_symbolic (any
  * host pattern: full symmetric CSC of n columns with sorted rows; host only, no
