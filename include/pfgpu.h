@@ -403,7 +403,8 @@ int pfg_cg_solve(pfg_context *ctx, int system, const double *values, const doubl
  *       `system` (PFG_SYS_FULL after pfg_hessian, PFG_SYS_REDUCED after
  *       pfg_set_dirichlet; host work, then the maps go to the device).  Repeat it
  *       when the pattern changes: pfg_set_dirichlet discards the reduced system's
- *       analysis.  PFG_ERR_OOM when the dense fronts do not fit in device memory;
+ *       analysis.  PFG_ERR_OOM when the dense fronts do not fit in device memory,
+ *       PFG_ERR_UNSUPPORTED beyond 65,535 fronts at one height of the tree;
  *   pfg_direct_factorize (factorize): factorises `values` (device memory, nnz
  *       doubles of the analysed pattern, both triangles stored; the lower one is
  *       read) or, with values == NULL, the system's values the last assembly left
