@@ -16,10 +16,11 @@
 //   factorisation (device): fronts of equal height in the tree are processed by
 //     the same launches, leaves first: A's lower entries are scattered into the
 //     zeroed fronts, the children's update matrices are added in child order,
-//     and each front is partially factorised (32-column panels: Cholesky of the
-//     diagonal block, triangular solve of the rows below, rank-32 update of the
-//     trailing lower triangle in 64 x 64 tiles); the trailing block is the update
-//     matrix the parent adds.
+//     and each front is partially factorised in pairs of 32-column panels
+//     (Cholesky of each diagonal block, triangular solve of the rows below, the
+//     first panel's update of the second, then one rank-64 update of the trailing
+//     lower triangle in 64 x 64 tiles); the trailing block is the update matrix
+//     the parent adds.
 //   solve (device): forward substitution leaves first (each front adds its
 //     children's update vectors in child order), backward substitution from the
 //     root, then the inverse permutation.
@@ -42,7 +43,8 @@ namespace pfg
 namespace
 {
 
-constexpr int NB = 32;          // panel width of the partial factorisation
+constexpr int NB = 32;          // panel width of the triangular solves
+constexpr int NBF = 64;         // panel width of the partial factorisation
 constexpr int LEAF_DOFS = 96;   // dissection stops at parts of at most this many dofs
 constexpr int TRSM_ROWS = 128;  // rows per CTA of the panel solve
 constexpr int TILE = 64;        // trailing-update tile
@@ -84,7 +86,8 @@ struct DirectFactor
 	std::vector<long long> lvl_abeg;   // A-map entries of each level
 	std::vector<int> lvl_maxchild, lvl_maxrc, lvl_maxk;
 	int max_bwd_part = 0; // doubles of backward partial sums for one panel step
-	std::vector<Panel> panels;         // factorisation launches in order
+	std::vector<Panel> panels;         // solve panels (NB columns) in order
+	std::vector<Panel> fpanels;        // factorisation panels (NBF columns) in order
 	long long front_doubles = 0, work_doubles = 0, amap_n = 0;
 	// host maps between the analysis and the upload
 	std::vector<int> h_child, h_relpos, h_rows, h_amap_src;
@@ -516,6 +519,37 @@ int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **ou
 		int maxk = 0;
 		for (int t = f->lvl_start[h]; t < f->lvl_start[h + 1]; ++t) maxk = std::max(maxk, f->fr[f->lvl_list[t]].k);
 		f->lvl_maxk.push_back(maxk);
+		for (int j0 = 0; j0 < maxk; j0 += NBF)
+		{
+			// rows_grid: panel A's rows below; fwd_grid: rows of A's update of B (0 when
+			// no front has a panel B); bwd_grid: panel B's rows below; tiles_grid: the
+			// rank-64 trailing update
+			long long ra = 0, ru = 0, rb = 0, tg = 0;
+			for (int t = f->lvl_start[h]; t < f->lvl_start[h + 1]; ++t)
+			{
+				const DevFront &d = f->fr[f->lvl_list[t]];
+				if (d.k <= j0) continue;
+				const int na = std::min(NB, d.k - j0);
+				ra = std::max(ra, ((long long)d.m - j0 - na + TRSM_ROWS - 1) / TRSM_ROWS);
+				if (d.k > j0 + NB)
+				{
+					const int nbb = std::min(NB, d.k - j0 - NB);
+					ru = std::max(ru, ((long long)d.m - j0 - NB + TRSM_ROWS - 1) / TRSM_ROWS);
+					rb = std::max(rb, ((long long)d.m - j0 - NB - nbb + TRSM_ROWS - 1) / TRSM_ROWS);
+				}
+				const int nb = std::min(NBF, d.k - j0);
+				const long long below = d.m - j0 - nb;
+				const long long nt = (below + TILE - 1) / TILE;
+				tg = std::max(tg, nt * (nt + 1) / 2);
+			}
+			if (tg > 0x7fffffffLL)
+			{
+				msg = "direct solver front too large";
+				direct_destroy(f);
+				return PFG_ERR_UNSUPPORTED;
+			}
+			f->fpanels.push_back({h, j0, (int)ra, (int)tg, (int)ru, (int)rb});
+		}
 		for (int j0 = 0; j0 < maxk; j0 += NB)
 		{
 			long long rg = 0, tg = 0, fg = 0, bg = 1;
@@ -751,13 +785,54 @@ __global__ void __launch_bounds__(TRSM_ROWS) k_dir_trsm(const DevFront *__restri
 		if (l < nb) Fb[i + (size_t)(j0 + l) * f.m] = x[l];
 }
 
-// trailing lower triangle -= P P^T for the panel's rows P below it, 64 x 64 tiles
-__global__ void __launch_bounds__(256) k_dir_syrk(const DevFront *__restrict__ fr, const int *__restrict__ list,
-												  double *__restrict__ F, int j0)
+// The factorisation runs in pairs of 32-column panels A = [j0, j0+32) and
+// B = [j0+32, j0+64): A is factorised (k_dir_potrf, k_dir_trsm), its update is
+// applied to B's columns alone (k_dir_panel_update), B is factorised, and one
+// rank-64 update of the trailing lower triangle by both panels follows
+// (k_dir_syrk64), so the trailing matrix is read and written once per 64 columns.
+// k_dir_panel_update: F[i][j0+32+c] -= sum_l F[i][j0+l] F[j0+32+c][j0+l] for the
+// rows i >= j0+32+c, a thread per row, A's rows of B's columns in shared memory.
+__global__ void __launch_bounds__(TRSM_ROWS) k_dir_panel_update(const DevFront *__restrict__ fr,
+																const int *__restrict__ list, double *__restrict__ F,
+																int j0)
+{
+	const DevFront f = fr[list[blockIdx.y]];
+	const int jb = j0 + NB;
+	if (jb >= f.k) return;
+	const int nc = min(NB, f.k - jb);
+	__shared__ double M[NB][NB + 1]; // M[c][l] = F[jb + c][j0 + l]
+	double *Fb = F + f.foff;
+	for (int t = threadIdx.x; t < NB * NB; t += TRSM_ROWS)
+	{
+		const int c = t % NB, l = t / NB;
+		M[c][l] = c < nc ? Fb[(size_t)(jb + c) + (size_t)(j0 + l) * f.m] : 0.0;
+	}
+	__syncthreads();
+	const long long i = (long long)jb + (long long)blockIdx.x * TRSM_ROWS + threadIdx.x;
+	if (i >= f.m) return;
+	double x[NB];
+#pragma unroll
+	for (int l = 0; l < NB; ++l) x[l] = Fb[i + (size_t)(j0 + l) * f.m];
+	for (int c = 0; c < nc; ++c)
+	{
+		if (i < jb + c) break; // upper part of B's block
+		double a = 0.0;
+#pragma unroll
+		for (int l = 0; l < NB; ++l) a = fma(x[l], M[c][l], a);
+		Fb[i + (size_t)(jb + c) * f.m] -= a;
+	}
+}
+
+// trailing lower triangle -= P P^T for the pair's rows P below it (up to 64 columns),
+// 64 x 64 tiles of the lower triangle, the two 64 x 64 row blocks of P in shared
+// memory, 4 x 4 entries per thread
+constexpr size_t SYRK64_SMEM = 2 * NBF * (TILE + 1) * sizeof(double);
+__global__ void __launch_bounds__(256) k_dir_syrk64(const DevFront *__restrict__ fr, const int *__restrict__ list,
+													double *__restrict__ F, int j0)
 {
 	const DevFront f = fr[list[blockIdx.y]];
 	if (j0 >= f.k) return;
-	const int nb = min(NB, f.k - j0);
+	const int nb = min(NBF, f.k - j0);
 	const int o = j0 + nb, t = f.m - o;
 	if (t <= 0) return;
 	const long long nt = (t + TILE - 1) / TILE;
@@ -767,9 +842,11 @@ __global__ void __launch_bounds__(256) k_dir_syrk(const DevFront *__restrict__ f
 	while (ti * (ti + 1) / 2 > tile) --ti;
 	while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
 	const long long tj = tile - ti * (ti + 1) / 2;
-	__shared__ double Pi[NB][TILE + 1], Pj[NB][TILE + 1];
+	extern __shared__ __align__(16) double sy[];
+	double(*Pi)[TILE + 1] = reinterpret_cast<double(*)[TILE + 1]>(sy);
+	double(*Pj)[TILE + 1] = reinterpret_cast<double(*)[TILE + 1]>(sy + NBF * (TILE + 1));
 	double *Fb = F + f.foff;
-	for (int q = threadIdx.x; q < NB * TILE; q += 256)
+	for (int q = threadIdx.x; q < NBF * TILE; q += 256)
 	{
 		const int r = q % TILE, l = q / TILE;
 		const long long gi = ti * TILE + r, gj = tj * TILE + r;
@@ -781,7 +858,7 @@ __global__ void __launch_bounds__(256) k_dir_syrk(const DevFront *__restrict__ f
 	const int tr = (threadIdx.x % 16) * 4, tc = (threadIdx.x / 16) * 4;
 	double acc[4][4] = {};
 #pragma unroll 4
-	for (int l = 0; l < NB; ++l)
+	for (int l = 0; l < NBF; ++l)
 	{
 		double a[4], b[4];
 #pragma unroll
@@ -991,6 +1068,9 @@ int direct_factorize(DirectFactor *f, const double *vals, cudaStream_t s, cudaEr
 	f->factorized = false;
 	const int nl = (int)f->lvl_start.size() - 1;
 	if ((*ce = cudaMemsetAsync(f->d_err, 0, sizeof(int), s)) != cudaSuccess) return 2;
+	if ((*ce = cudaFuncSetAttribute(k_dir_syrk64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SYRK64_SMEM)) !=
+		cudaSuccess)
+		return 2;
 	size_t pi = 0;
 	for (int h = 0; h < nl; ++h)
 	{
@@ -1006,12 +1086,22 @@ int direct_factorize(DirectFactor *f, const double *vals, cudaStream_t s, cudaEr
 			if (f->lvl_maxrc[h] > 0)
 				k_dir_extend_add<<<dim3((f->lvl_maxrc[h] + 7) / 8, nf), 256, 0, s>>>(f->d_fr, list, f->d_child,
 																					 f->d_relpos, f->d_front, ci);
-		for (; pi < f->panels.size() && f->panels[pi].lvl == h; ++pi)
+		for (; pi < f->fpanels.size() && f->fpanels[pi].lvl == h; ++pi)
 		{
-			const Panel &p = f->panels[pi];
+			const Panel &p = f->fpanels[pi];
+			// panel A
 			k_dir_potrf<<<nf, 32, 0, s>>>(f->d_fr, list, f->d_front, p.j0, f->d_err);
 			if (p.rows_grid > 0) k_dir_trsm<<<dim3(p.rows_grid, nf), TRSM_ROWS, 0, s>>>(f->d_fr, list, f->d_front, p.j0);
-			if (p.tiles_grid > 0) k_dir_syrk<<<dim3(p.tiles_grid, nf), 256, 0, s>>>(f->d_fr, list, f->d_front, p.j0);
+			// A's update of B, then panel B
+			if (p.fwd_grid > 0)
+			{
+				k_dir_panel_update<<<dim3(p.fwd_grid, nf), TRSM_ROWS, 0, s>>>(f->d_fr, list, f->d_front, p.j0);
+				k_dir_potrf<<<nf, 32, 0, s>>>(f->d_fr, list, f->d_front, p.j0 + NB, f->d_err);
+				if (p.bwd_grid > 0)
+					k_dir_trsm<<<dim3(p.bwd_grid, nf), TRSM_ROWS, 0, s>>>(f->d_fr, list, f->d_front, p.j0 + NB);
+			}
+			if (p.tiles_grid > 0)
+				k_dir_syrk64<<<dim3(p.tiles_grid, nf), 256, SYRK64_SMEM, s>>>(f->d_fr, list, f->d_front, p.j0);
 		}
 		if ((*ce = cudaGetLastError()) != cudaSuccess) return 2;
 	}
