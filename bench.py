@@ -380,7 +380,7 @@ def run_gpu(args):
     newton = newton_direct = None
     if rank == 0 and world == 1 and not args.no_newton:
         newton = time_newton_step(asm, h, mesh, u_host, stream, min(args.steps, 5))
-        newton_direct = time_newton_step_direct(stream, DIRECT_GRID, 3)
+        newton_direct = time_newton_step_direct(asm, h, mesh, u_host, stream, 2)
 
     tri_bytes = 4 * 8 * ((9 * 55 + 7) // 8)  # P2 block triangle in FP32
     bytes_alg = algorithmic_bytes(mesh, nnz)
@@ -501,33 +501,24 @@ def time_newton_step(asm, h, mesh, u_host, stream, steps):
                     "median of the timed steps"}
 
 
-DIRECT_GRID = 24  # P2 24^3: the largest P2 cube whose dense fronts (33 GB) sit comfortably in HBM
-
-
-def time_newton_step_direct(stream, grid, steps):
+def time_newton_step_direct(asm, h, mesh, u_host, stream, steps):
     """The same Newton step with the sparse direct solve (pfg_direct_*) in place of
-    CG, on P2 grid^3 (the analysis is made once, as polysolve's analyzePattern, and
-    timed apart): pinned u in, reduced gradient, reduced PSD-projected FP64
-    Hessian, factorisation, solve, reduced_to_full, pinned step out.  The CG solve
-    of the same system (to 1e-6) is timed beside it."""
+    CG, on the same context and Dirichlet set (the analysis is made once, as
+    polysolve's analyzePattern, and timed apart): pinned u in, reduced gradient,
+    reduced PSD-projected FP64 Hessian, factorisation, solve, reduced_to_full,
+    pinned step out.  The CG solve of the same system (to 1e-6) is timed beside it.
+    The factor is released afterwards."""
     import ctypes
     import time
 
     import torch
 
-    from polyfem_b200 import NeoHookeanAssembler
-    from polyfem_b200 import mesh as M
-    from polyfem_b200._lib import check, lib
+    from polyfem_b200 import PfgError
+    from polyfem_b200._lib import PFG_ERR_OOM, check, lib
     L = lib()
     P = ctypes_ptr
-    mesh, lam, mu, u, _ = M.workload(2, grid)
-    asm = NeoHookeanAssembler.from_mesh(mesh, lam, mu)
-    h = asm.handle
-    face = np.flatnonzero(mesh.node_pos[:, 0] <= 1e-12)
-    asm.set_dirichlet((3 * face[:, None] + np.arange(3)).ravel())
     L.pfg_set_stream(h, P(stream.cuda_stream))
     nf, ndof = asm.n_free, mesh.n_dofs
-    u_host = torch.tensor(u, dtype=torch.float64).pin_memory()
     ud = torch.empty(ndof, dtype=torch.float64, device="cuda")
     g = torch.empty(nf, dtype=torch.float64, device="cuda")
     x = torch.empty(nf, dtype=torch.float64, device="cuda")
@@ -539,7 +530,12 @@ def time_newton_step_direct(stream, grid, steps):
         check(L.pfg_hessian_reduced(h, P(ud.data_ptr()), 1, 0, 1, None), h, "pfg_hessian_reduced")
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    check(L.pfg_direct_analyze(h, 1), h, "pfg_direct_analyze")
+    try:
+        check(L.pfg_direct_analyze(h, 1), h, "pfg_direct_analyze")
+    except PfgError as e:
+        if e.status != PFG_ERR_OOM:
+            raise
+        return {"unavailable": str(e)}
     t_an = time.perf_counter() - t0
     st = (ctypes.c_longlong * 7)()
     check(L.pfg_direct_stats(h, st), h, "pfg_direct_stats")
@@ -566,6 +562,7 @@ def time_newton_step_direct(stream, grid, steps):
     step()
     parts = [step() for _ in range(steps)]
     med = [statistics.median(p[i] for p in parts) for i in range(5)]
+    check(L.pfg_direct_free(h), h, "pfg_direct_free")
     it, rr = ctypes.c_int(), ctypes.c_double()
     with torch.cuda.stream(stream):
         ev[5].record(stream)
@@ -577,17 +574,16 @@ def time_newton_step_direct(stream, grid, steps):
     diff = float((x - xc).norm() / x.norm())
     total = sum(med)
     E = mesh.n_elements
-    asm.close()
-    return {"value": E / (total * 1e-3), "unit": UNIT, "ms_per_step": total, "workload": workload_name(grid),
-            "h2d_bytes_per_step": ndof * 8, "d2h_bytes_per_step": ndof * 8, "n_free": nf,
+    return {"value": E / (total * 1e-3), "unit": UNIT, "ms_per_step": total, "n_free": nf,
+            "h2d_bytes_per_step": ndof * 8, "d2h_bytes_per_step": ndof * 8,
             "ms_gradient": med[0], "ms_hessian_psd": med[1], "ms_factorize": med[2], "ms_solve": med[3],
             "ms_step_out": med[4], "s_analyze": t_an, "fronts": st[1], "nnz_L": st[4], "max_front": st[5],
             "front_GB": st[3] * 8e-9, "factorize_flops": st[6],
             "factorize_tflops": st[6] / (med[2] * 1e-3) / 1e12,
             "cg_ms_same_system": cg_ms, "cg_iterations": it.value, "rel_diff_vs_cg_1e-6": diff,
             "note": "NLProblem's Newton step with the sparse direct solve on the device (multifrontal "
-                    "Cholesky, nested dissection); the analysis is made once per pattern; median of the "
-                    "timed steps"}
+                    "Cholesky, nested dissection) on the workload's own reduced system; the analysis is made "
+                    "once per pattern; median of the timed steps"}
 
 
 # ----------------------------------------------------------------- the other four workloads

@@ -413,6 +413,7 @@ int pfg_cg_solve(pfg_context *ctx, int system, const double *values, const doubl
  *       waits for the factorisation to finish (it reads the pivot check);
  *   pfg_direct_solve     (solve): x = A^-1 b for b and x in `mem` (x may be b);
  *       with PFG_MEM_DEVICE it is asynchronous on the context's stream.
+ * pfg_direct_free releases the analysis and the factor (pfg_destroy does too).
  * Every sum is taken in a fixed order, so factor and solution are bitwise
  * deterministic.  pfg_direct_stats (after analyze) and pfg_direct_symbolic (any
  * host pattern: full symmetric CSC of n columns with sorted rows; host only, no
@@ -421,6 +422,7 @@ int pfg_cg_solve(pfg_context *ctx, int system, const double *values, const doubl
 int pfg_direct_analyze(pfg_context *ctx, int system);
 int pfg_direct_factorize(pfg_context *ctx, int system, const double *values);
 int pfg_direct_solve(pfg_context *ctx, int system, const double *b, int mem, double *x);
+int pfg_direct_free(pfg_context *ctx);
 int pfg_direct_stats(const pfg_context *ctx, long long *stats);
 int pfg_direct_symbolic(int n, const int *outer, const int *inner, long long *stats);
 

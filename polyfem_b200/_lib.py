@@ -18,6 +18,7 @@ ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 PFG_OK = 0
 PFG_ERR_INVALID = 1
+PFG_ERR_OOM = 3
 PFG_ERR_STATE = 5
 PFG_ERR_NUMERIC = 6
 PFG_MEM_HOST = 0
@@ -137,6 +138,7 @@ SIGNATURES = {
     "pfg_direct_factorize": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "pfg_direct_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
     "pfg_direct_stats": (ctypes.c_int, [_vp, _vp]),
+    "pfg_direct_free": (ctypes.c_int, [_vp]),
     "pfg_direct_symbolic": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp]),
 }
 

@@ -1640,6 +1640,15 @@ int pfg_direct_solve(pfg_context *c, int system, const double *b, int mem, doubl
 	return PFG_OK;
 }
 
+int pfg_direct_free(pfg_context *c)
+{
+	if (!c) return fail(c, PFG_ERR_INVALID, "bad arguments");
+	DeviceGuard g(c->device);
+	PFG_CUDA(c, cudaStreamSynchronize(c->stream));
+	free_direct(c);
+	return PFG_OK;
+}
+
 int pfg_direct_stats(const pfg_context *c, long long *stats)
 {
 	if (!c || !stats) return fail(const_cast<pfg_context *>(c), PFG_ERR_INVALID, "bad arguments");

@@ -25,8 +25,8 @@
 //     children's update vectors in child order), backward substitution from the
 //     root, then the inverse permutation.
 // Every sum is taken in a fixed order, so factor and solution are bitwise
-// deterministic.  Fronts are dense column-major m x m blocks (lower triangle
-// used), all resident for the factor's lifetime.
+// deterministic.  Fronts are dense lower triangles of m (m + 1) / 2 doubles
+// (packed columns), all resident for the factor's lifetime.
 #include "pfg_internal.h"
 #include "pfgpu.h"
 
@@ -53,7 +53,7 @@ constexpr int BWD_ROWS = 512;   // rows per CTA of the backward solve's panel su
 
 struct DevFront
 {
-	long long foff; // front block in the front buffer (doubles), m x m column-major
+	long long foff; // front in the front buffer (doubles): m (m + 1) / 2, packed lower columns
 	long long woff; // m doubles of solve workspace
 	long long roff; // rows of this front's update in the parent (relpos), m - k entries
 	long long ioff; // permuted positions of the m - k rows below the front's columns
@@ -64,6 +64,10 @@ struct DevFront
 	int nchild;
 	int pad;
 };
+
+// Fronts are stored as packed lower columns: column j of an order-m front holds
+// rows j .. m-1, and entry (i, j), i >= j, sits at pk(m, j) + i.
+__host__ __device__ __forceinline__ long long pk(int m, int j) { return (long long)j * m - (long long)j * (j + 1) / 2; }
 
 struct Panel
 {
@@ -490,7 +494,7 @@ int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **ou
 			const int s = f->lvl_list[t];
 			DevFront &d = f->fr[s];
 			d.foff = fo;
-			fo += (long long)d.m * d.m;
+			fo += (long long)d.m * (d.m + 1) / 2;
 			f->lvl_maxchild[h] = std::max(f->lvl_maxchild[h], d.nchild);
 			for (int c : nd.children[s]) f->lvl_maxrc[h] = std::max(f->lvl_maxrc[h], f->fr[c].m - f->fr[c].k);
 			for (int q = d.col0; q < d.col0 + d.k; ++q)
@@ -503,7 +507,7 @@ int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **ou
 					const int lr = local(s, p);
 					broken |= lr < cl || lr >= d.m; // lower triangle of this front
 					amap_src.push_back(t2);
-					amap_dst.push_back(d.foff + lr + (long long)cl * d.m);
+					amap_dst.push_back(d.foff + pk(d.m, cl) + lr);
 				}
 			}
 		}
@@ -586,7 +590,7 @@ int direct_symbolic(int n, const int *outer, const int *inner, DirectFactor **ou
 	for (int s2 = 0; s2 < ns && !broken; ++s2)
 	{
 		const DevFront &d = f->fr[s2];
-		broken |= d.k < 1 || d.m < d.k || d.foff < 0 || d.foff + (long long)d.m * d.m > fo;
+		broken |= d.k < 1 || d.m < d.k || d.foff < 0 || d.foff + (long long)d.m * (d.m + 1) / 2 > fo;
 		const int last = d.col0 + d.k - 1;
 		for (int q = 0; q < d.m - d.k && !broken; ++q)
 		{
@@ -704,8 +708,8 @@ __global__ void __launch_bounds__(256) k_dir_extend_add(const DevFront *__restri
 	const int b = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
 	if (b >= rc) return;
 	const int *rp = relpos + c.roff;
-	const double *U = F + c.foff + c.k + (size_t)c.k * c.m + (size_t)b * c.m;
-	double *P = F + f.foff + (size_t)rp[b] * f.m;
+	const double *U = F + c.foff + pk(c.m, c.k + b) + c.k; // U[a] = entry (k + a, k + b), a >= b
+	double *P = F + f.foff + pk(f.m, rp[b]);
 	for (int a = b + lane; a < rc; a += 32) P[rp[a]] += U[a];
 }
 
@@ -721,8 +725,15 @@ __global__ void __launch_bounds__(32) k_dir_potrf(const DevFront *__restrict__ f
 	double *Fb = F + f.foff;
 	const bool row = lane < nb;
 	double v[NB];
+	{
+		long long cb = pk(f.m, j0) + j0 + lane; // entry (j0 + lane, j0 + c)
 #pragma unroll
-	for (int c = 0; c < NB; ++c) v[c] = row && c <= lane && c < nb ? Fb[(size_t)(j0 + lane) + (size_t)(j0 + c) * f.m] : 0.0;
+		for (int c = 0; c < NB; ++c)
+		{
+			v[c] = row && c <= lane && c < nb ? Fb[cb] : 0.0;
+			cb += f.m - (j0 + c) - 1;
+		}
+	}
 	bool bad = false;
 #pragma unroll
 	for (int c = 0; c < NB; ++c)
@@ -745,9 +756,15 @@ __global__ void __launch_bounds__(32) k_dir_potrf(const DevFront *__restrict__ f
 		}
 	}
 	if (bad && lane == 0) atomicExch(err, 1);
+	{
+		long long cb = pk(f.m, j0) + j0 + lane;
 #pragma unroll
-	for (int c = 0; c < NB; ++c)
-		if (row && c <= lane && c < nb) Fb[(size_t)(j0 + lane) + (size_t)(j0 + c) * f.m] = v[c];
+		for (int c = 0; c < NB; ++c)
+		{
+			if (row && c <= lane && c < nb) Fb[cb] = v[c];
+			cb += f.m - (j0 + c) - 1;
+		}
+	}
 }
 
 // rows below the panel: X L_d^T = B, one row per thread
@@ -762,15 +779,22 @@ __global__ void __launch_bounds__(TRSM_ROWS) k_dir_trsm(const DevFront *__restri
 	for (int t = threadIdx.x; t < nb * nb; t += TRSM_ROWS)
 	{
 		const int r = t % nb, c = t / nb;
-		if (r >= c) D[r][c] = Fb[(size_t)(j0 + r) + (size_t)(j0 + c) * f.m];
+		if (r >= c) D[r][c] = Fb[(size_t)(j0 + r) + pk(f.m, j0 + c)];
 	}
 	__syncthreads();
 	const long long i = (long long)j0 + nb + (long long)blockIdx.x * TRSM_ROWS + threadIdx.x;
 	if (i >= f.m) return;
 	double x[NB];
+	const long long c0 = pk(f.m, j0) + i; // entry (i, j0); column j0 + l + 1 starts m - (j0 + l) - 1 later
+	{
+		long long cb = c0;
 #pragma unroll
-	for (int l = 0; l < NB; ++l)
-		if (l < nb) x[l] = Fb[i + (size_t)(j0 + l) * f.m];
+		for (int l = 0; l < NB; ++l)
+		{
+			if (l < nb) x[l] = Fb[cb];
+			cb += f.m - (j0 + l) - 1;
+		}
+	}
 #pragma unroll
 	for (int l = 0; l < NB; ++l)
 		if (l < nb)
@@ -780,9 +804,15 @@ __global__ void __launch_bounds__(TRSM_ROWS) k_dir_trsm(const DevFront *__restri
 			for (int t = 0; t < l; ++t) s = fma(-x[t], D[l][t], s);
 			x[l] = s / D[l][l];
 		}
+	{
+		long long cb = c0;
 #pragma unroll
-	for (int l = 0; l < NB; ++l)
-		if (l < nb) Fb[i + (size_t)(j0 + l) * f.m] = x[l];
+		for (int l = 0; l < NB; ++l)
+		{
+			if (l < nb) Fb[cb] = x[l];
+			cb += f.m - (j0 + l) - 1;
+		}
+	}
 }
 
 // The factorisation runs in pairs of 32-column panels A = [j0, j0+32) and
@@ -801,25 +831,30 @@ __global__ void __launch_bounds__(TRSM_ROWS) k_dir_panel_update(const DevFront *
 	if (jb >= f.k) return;
 	const int nc = min(NB, f.k - jb);
 	__shared__ double M[NB][NB + 1]; // M[c][l] = F[jb + c][j0 + l]
+	__shared__ long long cofs[NB];   // pk of columns j0 + l
 	double *Fb = F + f.foff;
+	if (threadIdx.x < NB) cofs[threadIdx.x] = pk(f.m, j0 + threadIdx.x);
+	__syncthreads();
 	for (int t = threadIdx.x; t < NB * NB; t += TRSM_ROWS)
 	{
 		const int c = t % NB, l = t / NB;
-		M[c][l] = c < nc ? Fb[(size_t)(jb + c) + (size_t)(j0 + l) * f.m] : 0.0;
+		M[c][l] = c < nc ? Fb[cofs[l] + jb + c] : 0.0;
 	}
 	__syncthreads();
 	const long long i = (long long)jb + (long long)blockIdx.x * TRSM_ROWS + threadIdx.x;
 	if (i >= f.m) return;
 	double x[NB];
 #pragma unroll
-	for (int l = 0; l < NB; ++l) x[l] = Fb[i + (size_t)(j0 + l) * f.m];
+	for (int l = 0; l < NB; ++l) x[l] = Fb[cofs[l] + i];
+	long long cb = pk(f.m, jb) + i; // entry (i, jb + c)
 	for (int c = 0; c < nc; ++c)
 	{
 		if (i < jb + c) break; // upper part of B's block
 		double a = 0.0;
 #pragma unroll
 		for (int l = 0; l < NB; ++l) a = fma(x[l], M[c][l], a);
-		Fb[i + (size_t)(jb + c) * f.m] -= a;
+		Fb[cb] -= a;
+		cb += f.m - (jb + c) - 1;
 	}
 }
 
@@ -846,13 +881,16 @@ __global__ void __launch_bounds__(256) k_dir_syrk64(const DevFront *__restrict__
 	double(*Pi)[TILE + 1] = reinterpret_cast<double(*)[TILE + 1]>(sy);
 	double(*Pj)[TILE + 1] = reinterpret_cast<double(*)[TILE + 1]>(sy + NBF * (TILE + 1));
 	double *Fb = F + f.foff;
+	__shared__ long long cofs[NBF]; // pk of columns j0 + l
+	if (threadIdx.x < NBF) cofs[threadIdx.x] = pk(f.m, j0 + threadIdx.x);
+	__syncthreads();
 	for (int q = threadIdx.x; q < NBF * TILE; q += 256)
 	{
 		const int r = q % TILE, l = q / TILE;
 		const long long gi = ti * TILE + r, gj = tj * TILE + r;
 		const bool ok = l < nb;
-		Pi[l][r] = ok && gi < t ? Fb[(size_t)(o + gi) + (size_t)(j0 + l) * f.m] : 0.0;
-		Pj[l][r] = ok && gj < t ? Fb[(size_t)(o + gj) + (size_t)(j0 + l) * f.m] : 0.0;
+		Pi[l][r] = ok && gi < t ? Fb[cofs[l] + o + gi] : 0.0;
+		Pj[l][r] = ok && gj < t ? Fb[cofs[l] + o + gj] : 0.0;
 	}
 	__syncthreads();
 	const int tr = (threadIdx.x % 16) * 4, tc = (threadIdx.x / 16) * 4;
@@ -872,6 +910,7 @@ __global__ void __launch_bounds__(256) k_dir_syrk64(const DevFront *__restrict__
 #pragma unroll
 			for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], b[q], acc[p][q]);
 	}
+	long long cb = pk(f.m, (int)(o + tj * TILE + tc)) + o + ti * TILE + tr; // entry (o + gr, o + gc) at p = q = 0
 #pragma unroll
 	for (int q = 0; q < 4; ++q)
 	{
@@ -880,8 +919,9 @@ __global__ void __launch_bounds__(256) k_dir_syrk64(const DevFront *__restrict__
 		for (int p = 0; p < 4; ++p)
 		{
 			const long long gr = ti * TILE + tr + p;
-			if (gr < t && gc < t && gr >= gc) Fb[(size_t)(o + gr) + (size_t)(o + gc) * f.m] -= acc[p][q];
+			if (gr < t && gc < t && gr >= gc) Fb[cb + p] -= acc[p][q];
 		}
+		cb += f.m - (o + gc) - 1;
 	}
 }
 
@@ -930,11 +970,13 @@ __global__ void __launch_bounds__(32) k_fwd_diag(const DevFront *__restrict__ fr
 	double *w = W + f.woff;
 	const double *L = F + f.foff;
 	double v = lane < nb ? w[j0 + lane] : 0.0;
+	long long cb = pk(f.m, j0) + j0; // column j0 + c, row j0
 	for (int c = 0; c < nb; ++c)
 	{
-		const double yc = __shfl_sync(0xffffffffu, v, c) / L[(size_t)(j0 + c) * f.m + j0 + c];
+		const double yc = __shfl_sync(0xffffffffu, v, c) / L[cb + c];
 		if (lane == c) v = yc;
-		if (lane > c && lane < nb) v = fma(-L[(size_t)(j0 + c) * f.m + j0 + lane], yc, v);
+		if (lane > c && lane < nb) v = fma(-L[cb + lane], yc, v);
+		cb += f.m - (j0 + c) - 1;
 	}
 	if (lane < nb) w[j0 + lane] = v;
 }
@@ -953,7 +995,12 @@ __global__ void __launch_bounds__(FWD_ROWS) k_fwd_rows(const DevFront *__restric
 	const long long i = (long long)j0 + nb + (long long)blockIdx.x * FWD_ROWS + threadIdx.x;
 	if (i >= f.m) return;
 	double a = w[i];
-	for (int c = 0; c < nb; ++c) a = fma(-L[(size_t)(j0 + c) * f.m + i], yb[c], a);
+	long long cb = pk(f.m, j0) + i;
+	for (int c = 0; c < nb; ++c)
+	{
+		a = fma(-L[cb], yb[c], a);
+		cb += f.m - (j0 + c) - 1;
+	}
 	w[i] = a;
 }
 
@@ -989,7 +1036,7 @@ __global__ void __launch_bounds__(256) k_bwd_l21(const DevFront *__restrict__ fr
 	if (j >= f.k) return;
 	double *w = W + f.woff;
 	const int r = f.m - f.k;
-	const double *Lj = F + f.foff + (size_t)j * f.m + f.k;
+	const double *Lj = F + f.foff + pk(f.m, j) + f.k;
 	double s = 0.0;
 	for (int i = lane; i < r; i += 32) s = fma(Lj[i], w[f.k + i], s);
 	s = warp_sum_d(s);
@@ -1013,7 +1060,7 @@ __global__ void __launch_bounds__(256) k_bwd_cols(const DevFront *__restrict__ f
 		double s = 0.0;
 		if (c < nb)
 		{
-			const double *Lc = L + (size_t)(j0 + c) * f.m;
+			const double *Lc = L + pk(f.m, j0 + c);
 			for (int i = i0 + lane; i < i1; i += 32) s = fma(Lc[i], w[i], s);
 		}
 		s = warp_sum_d(s);
@@ -1041,7 +1088,7 @@ __global__ void __launch_bounds__(32) k_bwd_diag(const DevFront *__restrict__ fr
 	for (int c = nb - 1; c >= 0; --c)
 	{
 		// x_c = (v_c - sum_{c' > c} L[c'][c] x_c') / L[c][c]; lanes c' > c hold x_c'
-		const double *Lc = L + (size_t)(j0 + c) * f.m + j0;
+		const double *Lc = L + pk(f.m, j0 + c) + j0;
 		const double t = lane > c && lane < nb ? Lc[lane] * v : 0.0;
 		const double sum = warp_sum_d(t);
 		const double xc = (__shfl_sync(0xffffffffu, v, c) - sum) / Lc[c];

@@ -161,6 +161,12 @@ class DirectSolver:
                   "pfg_set_stream")
         check(lib().pfg_direct_factorize(h, self.system, vp), h, "pfg_direct_factorize")
 
+    def free(self):
+        """Releases the analysis and the factor's device memory (the dense fronts)."""
+        h = self.asm.handle
+        check(lib().pfg_direct_free(h), h, "pfg_direct_free")
+        self._info = {}
+
     def solve(self, b, x=None):
         """x with A x = b (``x``, in b's memory space, receives it).  Returns x."""
         n = self.size()

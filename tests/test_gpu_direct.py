@@ -136,6 +136,14 @@ def test_state_errors(require_gpu):
     assert np.array_equal(ds.solve(-grad), x)
     with pytest.raises(ValueError):
         ds.solve(np.zeros(H2.shape[0] + 1))
+    # released: the factor is gone until the next analysis
+    ds.free()
+    with pytest.raises(PfgError) as ei:
+        ds.solve(-grad)
+    assert ei.value.status == PFG_ERR_STATE
+    ds.analyze_pattern()
+    ds.factorize()
+    assert np.array_equal(ds.solve(-grad), x)
     asm.close()
 
 
