@@ -862,7 +862,7 @@ __global__ void __launch_bounds__(TRSM_ROWS) k_dir_panel_update(const DevFront *
 // 64 x 64 tiles of the lower triangle, the two 64 x 64 row blocks of P in shared
 // memory, 4 x 4 entries per thread
 constexpr size_t SYRK64_SMEM = 2 * NBF * (TILE + 1) * sizeof(double);
-__global__ void __launch_bounds__(256) k_dir_syrk64(const DevFront *__restrict__ fr, const int *__restrict__ list,
+__global__ void __launch_bounds__(256, 3) k_dir_syrk64(const DevFront *__restrict__ fr, const int *__restrict__ list,
 													double *__restrict__ F, int j0)
 {
 	const DevFront f = fr[list[blockIdx.y]];
@@ -884,13 +884,25 @@ __global__ void __launch_bounds__(256) k_dir_syrk64(const DevFront *__restrict__
 	__shared__ long long cofs[NBF]; // pk of columns j0 + l
 	if (threadIdx.x < NBF) cofs[threadIdx.x] = pk(f.m, j0 + threadIdx.x);
 	__syncthreads();
-	for (int q = threadIdx.x; q < NBF * TILE; q += 256)
+	// all of a thread's staging loads are issued before any is stored
+	constexpr int SQ = NBF * TILE / 256;
+	double vi[SQ], vj[SQ];
+	const int r = threadIdx.x % TILE, l0 = threadIdx.x / TILE;
+	const long long gi = ti * TILE + r, gj = tj * TILE + r;
+#pragma unroll
+	for (int q = 0; q < SQ; ++q)
 	{
-		const int r = q % TILE, l = q / TILE;
-		const long long gi = ti * TILE + r, gj = tj * TILE + r;
+		const int l = l0 + q * (256 / TILE);
 		const bool ok = l < nb;
-		Pi[l][r] = ok && gi < t ? Fb[cofs[l] + o + gi] : 0.0;
-		Pj[l][r] = ok && gj < t ? Fb[cofs[l] + o + gj] : 0.0;
+		vi[q] = ok && gi < t ? Fb[cofs[l] + o + gi] : 0.0;
+		vj[q] = ok && gj < t ? Fb[cofs[l] + o + gj] : 0.0;
+	}
+#pragma unroll
+	for (int q = 0; q < SQ; ++q)
+	{
+		const int l = l0 + q * (256 / TILE);
+		Pi[l][r] = vi[q];
+		Pj[l][r] = vj[q];
 	}
 	__syncthreads();
 	const int tr = (threadIdx.x % 16) * 4, tc = (threadIdx.x / 16) * 4;
